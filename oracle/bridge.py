@@ -1,0 +1,193 @@
+"""ctypes bridge to the CPU oracles (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/_ref/libftk2ref.so (the reference engine, built from the
+reference's own headers) and oracle/_build/libcporacle.so (our C restatement,
+cp_oracle.c).  Only tests/, the smoke check and bench.py's CPU-baseline leg
+import this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libftk2ref.so")
+ORC_LIB = os.path.join(HERE, "_build", "libcporacle.so")
+
+MESH_REGULAR, MESH_EXTRUDED = 0, 1
+F32, F64 = 0, 1
+LAYOUT_MULTI, LAYOUT_SEPARATE, LAYOUT_PER_VERTEX = 0, 1, 2
+
+
+class OrcMesh(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("ndims", C.c_int),
+        ("local_dims", C.c_uint64 * 4), ("offset", C.c_uint64 * 4), ("global_dims", C.c_uint64 * 4),
+        ("n_base_verts", C.c_uint64), ("base_coords", C.c_void_p),
+        ("n_base_cells", C.c_uint64), ("base_cells", C.c_void_p),
+        ("base_cell_dim", C.c_int), ("n_layers", C.c_uint64),
+    ]
+
+
+class OrcField(C.Structure):
+    _fields_ = [
+        ("dtype", C.c_int), ("ncomp", C.c_int), ("layout", C.c_int),
+        ("comp", C.c_void_p * 4), ("nd", C.c_int), ("dims", C.c_uint64 * 4),
+        ("scalar", C.c_void_p), ("scalar_nd", C.c_int), ("scalar_dims", C.c_uint64 * 4),
+        ("sos_q", C.c_double), ("n_threads", C.c_int),
+    ]
+
+
+class OrcResult(C.Structure):
+    _fields_ = [
+        ("m", C.c_int), ("n", C.c_uint64),
+        ("simplices", C.POINTER(C.c_uint64)), ("bary", C.POINTER(C.c_float)),
+        ("lambda_", C.POINTER(C.c_double)), ("track_id", C.POINTER(C.c_uint64)),
+        ("type", C.POINTER(C.c_uint32)), ("scalar", C.POINTER(C.c_float)),
+        ("n_edges", C.c_uint64), ("edges", C.POINTER(C.c_uint32)),
+        ("n_tested", C.c_uint64),
+    ]
+
+
+@dataclass
+class CPResult:
+    """Flattened FeatureComplex: features in canonical order plus edges."""
+    simplices: np.ndarray   # (n, m+1) uint64
+    bary: np.ndarray        # (n, m+1) float32
+    lam: np.ndarray         # (n, m+1) float64
+    track_id: np.ndarray    # (n,) uint64
+    type: np.ndarray        # (n,) uint32
+    scalar: np.ndarray      # (n,) float32
+    edges: np.ndarray       # (e, 2) uint32
+    n_tested: int = 0
+
+
+_libs: dict[str, C.CDLL] = {}
+
+
+def _load(path: str, prefix: str) -> C.CDLL:
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path} (run __graft_entry__.build())")
+        lib = C.CDLL(path)
+        run = getattr(lib, prefix + "_run")
+        run.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.POINTER(OrcResult)]
+        run.restype = C.c_int
+        free = getattr(lib, prefix + "_free")
+        free.argtypes = [C.POINTER(OrcResult)]
+        free.restype = None
+        _libs[path] = lib
+    return _libs[path]
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def make_regular_mesh(local_dims, offset=None, global_dims=None) -> OrcMesh:
+    nd = len(local_dims)
+    offset = list(offset) if offset is not None else [0] * nd
+    global_dims = list(global_dims) if global_dims is not None else list(local_dims)
+    m = OrcMesh()
+    m.kind = MESH_REGULAR
+    m.ndims = nd
+    for i in range(nd):
+        m.local_dims[i] = int(local_dims[i])
+        m.offset[i] = int(offset[i])
+        m.global_dims[i] = int(global_dims[i])
+    return m
+
+
+def make_extruded_mesh(coords: np.ndarray, cells: np.ndarray, n_layers: int, keep: list) -> OrcMesh:
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    cells = np.ascontiguousarray(cells, dtype=np.uint64)
+    keep += [coords, cells]
+    m = OrcMesh()
+    m.kind = MESH_EXTRUDED
+    m.ndims = cells.shape[1]  # base cell dim + 1 (time)
+    m.n_base_verts = coords.shape[0]
+    m.base_coords = coords.ctypes.data
+    m.n_base_cells = cells.shape[0]
+    m.base_cells = cells.ctypes.data
+    m.base_cell_dim = cells.shape[1] - 1
+    m.n_layers = int(n_layers)
+    return m
+
+
+def make_field(arrays, layout: int, ncomp: int, scalar=None, sos_q: float = 1e6,
+               n_threads: int = 0, keep: list | None = None) -> OrcField:
+    """arrays: MULTI -> one numpy array whose memory is [M, dims...] Fortran
+    (C-order shape (..reversed dims.., M)); SEPARATE / PER_VERTEX -> list of M
+    arrays (C-order shape reversed dims)."""
+    keep = keep if keep is not None else []
+    f = OrcField()
+    first = arrays if layout == LAYOUT_MULTI else arrays[0]
+    f.dtype = F64 if first.dtype == np.float64 else F32
+    f.ncomp = ncomp
+    f.layout = layout
+    if layout == LAYOUT_MULTI:
+        a = np.ascontiguousarray(arrays)
+        keep.append(a)
+        f.comp[0] = a.ctypes.data
+        dims = a.shape[::-1][1:]
+    else:
+        dims = None
+        for j, a in enumerate(arrays):
+            a = np.ascontiguousarray(a)
+            keep.append(a)
+            f.comp[j] = a.ctypes.data
+            dims = a.shape[::-1]
+    f.nd = len(dims)
+    for i, d in enumerate(dims):
+        f.dims[i] = int(d)
+    if scalar is not None:
+        s = np.ascontiguousarray(scalar)
+        keep.append(s)
+        f.scalar = s.ctypes.data
+        f.scalar_nd = s.ndim
+        for i, d in enumerate(s.shape[::-1]):
+            f.scalar_dims[i] = int(d)
+    f.sos_q = float(sos_q)
+    f.n_threads = int(n_threads)
+    return f
+
+
+def _run(path: str, prefix: str, mesh: OrcMesh, field: OrcField) -> CPResult:
+    lib = _load(path, prefix)
+    res = OrcResult()
+    rc = getattr(lib, prefix + "_run")(C.byref(mesh), C.byref(field), C.byref(res))
+    if rc != 0:
+        raise RuntimeError(f"{prefix}_run failed with status {rc}")
+    try:
+        n, k, e = int(res.n), int(res.m) + 1, int(res.n_edges)
+
+        def arr(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        return CPResult(
+            simplices=arr(res.simplices, n * k, np.uint64).reshape(n, k),
+            bary=arr(res.bary, n * k, np.float32).reshape(n, k),
+            lam=arr(res.lambda_, n * k, np.float64).reshape(n, k),
+            track_id=arr(res.track_id, n, np.uint64),
+            type=arr(res.type, n, np.uint32),
+            scalar=arr(res.scalar, n, np.float32),
+            edges=arr(res.edges, 2 * e, np.uint32).reshape(e, 2),
+            n_tested=int(res.n_tested),
+        )
+    finally:
+        getattr(lib, prefix + "_free")(C.byref(res))
+
+
+def run_reference(mesh: OrcMesh, field: OrcField) -> CPResult:
+    """The reference's own engine (execute + get_complex)."""
+    return _run(REF_LIB, "ftk2ref", mesh, field)
+
+
+def run_restatement(mesh: OrcMesh, field: OrcField) -> CPResult:
+    """Our exact C restatement of the same algorithm."""
+    return _run(ORC_LIB, "cporacle", mesh, field)

@@ -1,0 +1,90 @@
+/*
+ * Plain-C interface shared by the two CPU oracles of the critical-point path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, the smoke check and the CPU-baseline
+ * leg of bench.py may load the libraries built from oracle/; the product never
+ * links them.
+ *
+ *   oracle/_ref/libftk2ref.so   the reference's own CPU engine
+ *                               (SimplicialEngine<T, CriticalPointPredicate<M,T>>
+ *                               ::execute() + get_complex(), engine.hpp:96-99 and
+ *                               822-996), compiled unmodified from its headers
+ *                               against the ndarray shim in oracle/shim.
+ *   oracle/_build/libcporacle.so our own exact, multithreaded C restatement
+ *                               of the same algorithm (cp_oracle.c), used where
+ *                               the reference is too slow.
+ *
+ * Both fill the same orc_result, whose content mirrors the reference's
+ * FeatureComplex (complex.hpp:14-58): features in Simplex::operator< order,
+ * float barycentrics, track_id, type, scalar, and the sorted unique edge list.
+ */
+#ifndef FTK2B_ORACLE_API_H
+#define FTK2B_ORACLE_API_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_MESH_REGULAR = 0, ORC_MESH_EXTRUDED = 1 };
+enum { ORC_F32 = 0, ORC_F64 = 1 };
+enum { ORC_LAYOUT_MULTI = 0, ORC_LAYOUT_SEPARATE = 1, ORC_LAYOUT_PER_VERTEX = 2 };
+
+typedef struct {
+  int kind;                 /* ORC_MESH_* */
+  int ndims;                /* regular: dims incl. time (3 = 2D+t, 4 = 3D+t) */
+  uint64_t local_dims[4];   /* RegularSimplicialMesh(dims, offset, global)   */
+  uint64_t offset[4];
+  uint64_t global_dims[4];
+  /* extruded: UnstructuredSimplicialMesh(3, cell_dim, coords, cells) wrapped in
+   * ExtrudedSimplicialMesh(base, n_layers) */
+  uint64_t n_base_verts;
+  const double* base_coords;   /* 3 per base vertex */
+  uint64_t n_base_cells;
+  const uint64_t* base_cells;  /* (base_cell_dim + 1) per cell */
+  int base_cell_dim;           /* 2 = triangles, 3 = tets */
+  uint64_t n_layers;
+} orc_mesh;
+
+typedef struct {
+  int dtype;                /* ORC_F32 / ORC_F64 */
+  int ncomp;                /* M: 2 or 3 */
+  int layout;               /* ORC_LAYOUT_* */
+  const void* comp[4];      /* MULTI: comp[0] = [M, dims...]; else one array per component */
+  int nd;                   /* array rank, not counting MULTI's leading component dim */
+  uint64_t dims[4];         /* Fortran dims (first fastest) */
+  const void* scalar;       /* optional scalar field (same dtype) or NULL */
+  int scalar_nd;
+  uint64_t scalar_dims[4];
+  double sos_q;             /* Predicate::sos_q (predicate.hpp:25) */
+  int n_threads;            /* restatement only: worker threads (0 = all cores) */
+} orc_field;
+
+typedef struct {
+  int m;                    /* feature simplices have m+1 vertices */
+  uint64_t n;               /* number of features */
+  uint64_t* simplices;      /* n*(m+1) sorted vertex ids */
+  float* bary;              /* n*(m+1) barycentrics as the reference stores them */
+  double* lambda;           /* n*(m+1) solver output in the field precision, widened */
+  uint64_t* track_id;       /* n */
+  uint32_t* type;           /* n (always 0 in the reference) */
+  float* scalar;            /* n */
+  uint64_t n_edges;
+  uint32_t* edges;          /* 2*n_edges, sorted, unique, (lo, hi) */
+  uint64_t n_tested;        /* m-simplices evaluated (restatement only) */
+} orc_result;
+
+/* reference engine build */
+int ftk2ref_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);
+void ftk2ref_free(orc_result* r);
+
+/* own restatement */
+int cporacle_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);
+void cporacle_free(orc_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

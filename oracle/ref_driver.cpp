@@ -1,0 +1,172 @@
+// Driver that runs the reference's own CPU critical-point engine.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by oracle/Makefile into
+// oracle/_ref/libftk2ref.so from the reference headers where they lie (the
+// reference's include/ tree) plus the ndarray shim in oracle/shim; no reference
+// source is copied into this repository.
+//
+// Per call it builds the mesh and predicate exactly as the reference's own
+// tests and examples do (tests/test_examples.cpp:79-100, 162-184;
+// examples/critical_point_2d.cpp:65-84), runs
+// SimplicialEngine<T, CriticalPointPredicate<M,T>>::execute() and
+// get_complex() (engine.hpp:96-99, 822-996) and flattens the returned
+// FeatureComplex.  As a side channel it re-runs the reference's
+// ZeroCrossingSolver<M,T>::solve (zero_crossing.hpp:20-47) on every returned
+// simplex, gathering values the way extract_simplex does
+// (engine.hpp:1096-1124, get_value 999-1009), so double-precision barycentrics
+// can be compared even though FeatureElement stores floats (feature.hpp:26).
+#include <ftk2/core/engine.hpp>
+#include <ftk2/core/mesh.hpp>
+#include <ftk2/core/predicate.hpp>
+#include <ftk2/core/unstructured_mesh.hpp>
+
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "oracle_api.h"
+
+namespace {
+
+template <typename T>
+ftk::ndarray<T> make_array(const void* src, int nd, const uint64_t* dims, size_t lead = 0) {
+  std::vector<size_t> shape;
+  if (lead) shape.push_back(lead);
+  for (int i = 0; i < nd; ++i) shape.push_back((size_t)dims[i]);
+  ftk::ndarray<T> a(shape);
+  std::memcpy(a.data(), src, a.nelem() * sizeof(T));
+  return a;
+}
+
+template <typename T, int M>
+int run(const orc_mesh* mesh, const orc_field* field, orc_result* out) {
+  using namespace ftk2;
+  std::shared_ptr<Mesh> mesh_ptr;
+  std::shared_ptr<RegularSimplicialMesh> reg;
+  if (mesh->kind == ORC_MESH_REGULAR) {
+    std::vector<uint64_t> dims, off, glob;
+    for (int i = 0; i < mesh->ndims; ++i) {
+      dims.push_back(mesh->local_dims[i]);
+      off.push_back(mesh->offset[i]);
+      glob.push_back(mesh->global_dims[i]);
+    }
+    reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
+    mesh_ptr = reg;
+  } else {
+    std::vector<double> coords(mesh->base_coords, mesh->base_coords + 3 * mesh->n_base_verts);
+    size_t nc = (size_t)mesh->n_base_cells * (mesh->base_cell_dim + 1);
+    std::vector<uint64_t> cells(mesh->base_cells, mesh->base_cells + nc);
+    auto base = std::make_shared<UnstructuredSimplicialMesh>(
+        mesh->base_cell_dim, mesh->base_cell_dim, coords, cells);
+    mesh_ptr = std::make_shared<ExtrudedSimplicialMesh>(base, mesh->n_layers);
+  }
+
+  CriticalPointPredicate<M, T> pred;
+  pred.sos_q = field->sos_q;
+  std::map<std::string, ftk::ndarray<T>> data;
+  static const char* names[4] = {"U", "V", "W", "S"};
+  if (field->layout == ORC_LAYOUT_MULTI) {
+    pred.use_multicomponent = true;
+    pred.vector_var_name = "vec";
+    data["vec"] = make_array<T>(field->comp[0], field->nd, field->dims, (size_t)M);
+  } else {
+    pred.use_multicomponent = false;
+    for (int j = 0; j < M; ++j) {
+      pred.var_names[j] = names[j];
+      data[names[j]] = make_array<T>(field->comp[j], field->nd, field->dims);
+    }
+  }
+  if (field->scalar) {
+    pred.scalar_var_name = "S";
+    data["S"] = make_array<T>(field->scalar, field->scalar_nd, field->scalar_dims);
+  }
+
+  SimplicialEngine<T, CriticalPointPredicate<M, T>> engine(mesh_ptr, pred);
+  // The engine reports progress on stdout; keep it out of the caller's stream.
+  std::streambuf* saved = std::cout.rdbuf();
+  std::ostringstream sink;
+  std::cout.rdbuf(sink.rdbuf());
+  engine.execute(data);
+  FeatureComplex complex = engine.get_complex();
+  std::cout.rdbuf(saved);
+
+  const uint64_t n = complex.vertices.size();
+  out->m = M;
+  out->n = n;
+  out->simplices = (uint64_t*)std::malloc(sizeof(uint64_t) * (n * (M + 1) + 1));
+  out->bary = (float*)std::malloc(sizeof(float) * (n * (M + 1) + 1));
+  out->lambda = (double*)std::malloc(sizeof(double) * (n * (M + 1) + 1));
+  out->track_id = (uint64_t*)std::malloc(sizeof(uint64_t) * (n + 1));
+  out->type = (uint32_t*)std::malloc(sizeof(uint32_t) * (n + 1));
+  out->scalar = (float*)std::malloc(sizeof(float) * (n + 1));
+  out->n_tested = 0;
+
+  for (uint64_t i = 0; i < n; ++i) {
+    const FeatureElement& el = complex.vertices[i];
+    T values[M + 1][M];
+    for (int v = 0; v <= M; ++v) {
+      out->simplices[i * (M + 1) + v] = el.simplex.vertices[v];
+      out->bary[i * (M + 1) + v] = el.barycentric_coords[0][v];
+      std::vector<double> coords = mesh_ptr->get_vertex_coordinates(el.simplex.vertices[v]);
+      for (int j = 0; j < M; ++j) {
+        if (field->layout == ORC_LAYOUT_MULTI) {
+          const auto& a = data.at("vec");
+          if (coords.size() == 3) values[v][j] = a.f(j, coords[0], coords[1], coords[2]);
+          else values[v][j] = a.f(j, coords[0], coords[1], coords[2], coords[3]);
+        } else {
+          const auto& a = data.at(names[j]);
+          if (a.nd() == 1) { values[v][j] = a[el.simplex.vertices[v]]; continue; }
+          std::vector<double> lc = coords;
+          if (reg) for (size_t k = 0; k < lc.size(); ++k) lc[k] -= (double)reg->get_offset()[k];
+          if (lc.size() == 3) values[v][j] = a.f(lc[0], lc[1], lc[2]);
+          else values[v][j] = a.f(lc[0], lc[1], lc[2], lc[3]);
+        }
+      }
+    }
+    T lambda[M + 1];
+    bool ok = ZeroCrossingSolver<M, T>::solve(values, lambda);
+    for (int v = 0; v <= M; ++v) out->lambda[i * (M + 1) + v] = ok ? (double)lambda[v] : NAN;
+    out->track_id[i] = el.track_id;
+    out->type[i] = el.type;
+    out->scalar[i] = el.scalar;
+  }
+
+  std::vector<uint32_t> edges;
+  for (const auto& conn : complex.connectivity)
+    if (conn.dimension == 1) edges = conn.indices;
+  out->n_edges = edges.size() / 2;
+  out->edges = (uint32_t*)std::malloc(sizeof(uint32_t) * (edges.size() + 2));
+  if (!edges.empty()) std::memcpy(out->edges, edges.data(), sizeof(uint32_t) * edges.size());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int ftk2ref_run(const orc_mesh* mesh, const orc_field* field, orc_result* out) {
+  std::memset(out, 0, sizeof(*out));
+  try {
+    const bool f64 = field->dtype == ORC_F64;
+    if (field->ncomp == 2) return f64 ? run<double, 2>(mesh, field, out) : run<float, 2>(mesh, field, out);
+    if (field->ncomp == 3) return f64 ? run<double, 3>(mesh, field, out) : run<float, 3>(mesh, field, out);
+    return 2;
+  } catch (const std::exception& e) {
+    std::cerr << "ftk2ref_run: " << e.what() << std::endl;
+    return 1;
+  }
+}
+
+extern "C" void ftk2ref_free(orc_result* r) {
+  std::free(r->simplices);
+  std::free(r->bary);
+  std::free(r->lambda);
+  std::free(r->track_id);
+  std::free(r->type);
+  std::free(r->scalar);
+  std::free(r->edges);
+  std::memset(r, 0, sizeof(*r));
+}
