@@ -1,0 +1,316 @@
+"""Benchmark of the critical-point tracking path (one JSON line on rank 0).
+
+Workload: 3D flow critical points, plain drop-in -- a 128^3 x 16 float64
+3-component Gaussian-sum gradient field (32 seeded blobs, sigma U[4,12]
+voxels, drift U[-0.5,0.5] voxel/step), tetrahedra of the 4D Kuhn spacetime mesh
+tested with the exact integer SoS at Q = 2^20, then canonical ordering, star
+edges and trajectories.
+
+A step = one full extraction (execute + get_complex equivalent) of the field.
+  value : simplices/s with the field resident in HBM (ftk2b_cp_run), device
+          timed with CUDA events on the context's stream, max over ranks.
+  e2e   : the same through ftk2b_cp_extract with pinned host input and host
+          output (H2D + D2H inside the timed region).
+The field (805 MB) is larger than L2 (126 MB), so no flush is needed.
+
+--impl reference times the reference's own CPU engine (oracle/_ref, built from
+the reference's headers) on bounded sub-boxes of the same field.
+With --gpus N > 1 every rank runs an independent replica on its own field
+(weak scaling); there is no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D CP tracking simplices/s & HBM GB/s, batched vs plain; serve p50/p99 ms"
+UNIT = "simplices/s"
+DIMS = (128, 128, 128)
+NT = 16
+SOS_Q = 2.0 ** 20
+CONFIG = {"workload": "3D flow critical points, plain drop-in: 128^3 x 16 float64 3-component "
+                      "Gaussian-sum gradient (32 blobs), 4D Kuhn tets, SoS Q=2^20",
+          "grid": [128, 128, 128, 16], "ncomp": 3, "field_dtype": "float64", "sos_q": SOS_Q,
+          "l2": "inputs larger than L2 (805 MB field vs 126 MB L2)"}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """DRAM bytes of one extraction launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "extract_regular_c2_traffic.json")
+    try:
+        return float(json.load(open(p))["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def cpu_baseline_sample(field_np, steps_budget_s=20.0):
+    """The reference's CPU engine on sub-boxes of the same field, run until
+    ~steps_budget_s seconds have been spent; returns (simplices/s, sample)."""
+    from oracle import bridge
+    import numpy as np
+    sub = (14, 14, 14, 4)
+    total_s, total_n, boxes = 0.0, 0, 0
+    rng = np.random.default_rng(0)
+    while total_s < steps_budget_s and boxes < 64:
+        lo = [int(rng.integers(0, DIMS[i] - sub[i])) for i in range(3)] + [int(rng.integers(0, NT - sub[3]))]
+        keep: list = []
+        mesh = bridge.make_regular_mesh(list(sub), lo, list(DIMS) + [NT])
+        fld = bridge.make_field(field_np, bridge.LAYOUT_MULTI, 3, sos_q=SOS_Q, keep=keep)
+        t = time.perf_counter()
+        bridge.run_reference(mesh, fld)
+        total_s += time.perf_counter() - t
+        from ftk2_b200 import api
+        total_n += api.simplex_count(api.regular_mesh_desc(list(sub), lo, list(DIMS) + [NT]), 3)
+        boxes += 1
+    sample = (f"{boxes} sub-boxes of {sub[0]}x{sub[1]}x{sub[2]}x{sub[3]} vertices of the same "
+              f"field, reference engine (oracle/_ref) execute+get_complex, {total_s:.1f} s")
+    return total_n / total_s, sample
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import bridge
+    import numpy as np
+    from ftk2_b200 import synthetic
+    if not bridge.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference engine build oracle/_ref missing"}))
+        return 0
+    # the reference's CPU engine on the same field definition; sub-boxes are
+    # drawn from a 40^3 x 16 corner of the field, generated on the host
+    corner = (40, 40, 40)
+    field = synthetic.gaussian_sum_gradient(corner, NT, seed=1234, n_blobs=32, box=DIMS)
+    sub = (12, 12, 12, 4)
+    rng = np.random.default_rng(1)
+    from ftk2_b200 import api
+
+    def one():
+        lo = [int(rng.integers(0, corner[i] - sub[i])) for i in range(3)] + [int(rng.integers(0, NT - sub[3]))]
+        keep: list = []
+        mesh = bridge.make_regular_mesh(list(sub), lo, list(corner) + [NT])
+        fld = bridge.make_field(field, bridge.LAYOUT_MULTI, 3, sos_q=SOS_Q, keep=keep)
+        n = api.simplex_count(api.regular_mesh_desc(list(sub), lo, list(corner) + [NT]), 3)
+        t = time.perf_counter()
+        bridge.run_reference(mesh, fld)
+        return n, time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        one()
+    tot_n, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        n, t = one()
+        tot_n += n
+        tot_t += t
+    value = tot_n / tot_t
+    cores = os.cpu_count() or 1
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": dict(CONFIG, reference_sample=f"{sub[0]}x{sub[1]}x{sub[2]}x{sub[3]} sub-box per step"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"one {sub[0]}x{sub[1]}x{sub[2]}x{sub[3]}-vertex sub-box of the "
+                                       f"workload field per step through the reference engine "
+                                       f"(std::thread parallel_for; phase 1 serial)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ftk2b", choices=["ftk2b", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    from ftk2_b200 import api, generate
+
+    ctx = api.Context(local)
+    # independent replica per rank: seed offset by rank
+    field = generate.gaussian_field_device(DIMS, NT, seed=1234 + rank, n_blobs=32,
+                                           dtype=torch.float64)
+    torch.cuda.synchronize()
+    keep: list = []
+    mesh = api.regular_mesh_desc(list(DIMS) + [NT])
+    fdev = api.field_desc(field, api.LAYOUT_MULTICOMPONENT, 3, keep=keep)
+    prm = api.params(SOS_Q)
+    nsimp = api.simplex_count(mesh, 3)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+    for _ in range(max(args.warmup, 3)):
+        ctx.run(mesh, fdev, prm)
+    _, _, launches0 = ctx.last_timing()
+
+    # ---- device-resident timed region
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    extract_ms = []
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            nf, ne = ctx.run(mesh, fdev, prm)
+            xms, _, _ = ctx.last_timing()
+            extract_ms.append(xms)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    _, _, launches1 = ctx.last_timing()
+    ms_total = ev0.elapsed_time(ev1)
+    if pg:
+        t = torch.tensor([ms_total], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * nsimp / (ms_step / 1000.0)
+
+    # ---- end to end through the public API with host buffers
+    host = field.cpu().numpy()
+    pinned = torch.from_numpy(host).pin_memory()
+    fhost = api.field_desc(pinned.numpy(), api.LAYOUT_MULTICOMPONENT, 3, keep=keep)
+    res = ctx.extract(mesh, fhost, prm)  # warm the host path
+    # bytes ftk2b_cp_fetch copies back: vertex ids, float barycentrics, four
+    # double lambdas, scalar and track id per feature, plus the edge list
+    nfe = len(res.track_id)
+    d2h = nfe * (8 * 4 + 4 * 4 + 8 * 4 + 4 + 8) + res.edges.nbytes
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e2e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        res = ctx.extract(mesh, fhost, prm)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if pg:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * nsimp / e2e_s
+
+    # ---- roofline of the dominant kernel (fused extraction)
+    peak, peak_kind = measured_peak()
+    alg_bytes = 3 * 8 * DIMS[0] * DIMS[1] * DIMS[2] * NT
+    xms = statistics.mean(extract_ms)
+    achieved = alg_bytes / (xms / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic_per_launch(),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6650 GB/s", "kernel": "extract_regular_kernel<double,4>",
+            "kernel_ms": xms, "algorithmic_bytes": alg_bytes}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(CONFIG, parallelism=f"replicas{world}", features=int(nf), edges=int(ne),
+                           simplices=int(nsimp)),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.nbytes),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1000.0},
+            "roofline": roof, "clocks": clocks.summary(),
+            "gpu_launches": int(launches1 - launches0)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample = cpu_baseline_sample(host)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1,
+                                "kind": "reference", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

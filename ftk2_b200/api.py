@@ -1,0 +1,427 @@
+"""Python binding of the C ABI in include/ftk2b.h (ctypes), plus a mirror of
+the reference's engine interface for this path:
+
+    mesh   = RegularSimplicialMesh([nx, ny, nt])              # mesh.hpp:256-265
+    pred   = CriticalPointPredicate(2, vector_var_name="v")   # predicate.hpp:49-64
+    engine = SimplicialEngine(mesh, pred)                     # engine.hpp:84-85
+    engine.execute({"v": array})                              # engine.hpp:96-99
+    fc     = engine.get_complex()                             # engine.hpp:822-996
+
+Arrays follow the reference's ndarray memory layout (Fortran order, first
+index fastest): a numpy array of C-order shape (nt, ny, nx, M) holds the
+reference's [M, nx, ny, nt] multicomponent array.  CUDA tensors (torch) are
+passed by device pointer without a copy.
+
+There is no CPU fallback: without the built library or a CUDA device every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libftk2b.so")
+
+# enums of include/ftk2b.h
+OK, INVALID_ARG, OOM, CUDA_ERROR, TIMEOUT, OVERFLOW_RETRY, NO_DEVICE, UNSUPPORTED, BUSY = range(9)
+STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "CUDA_ERROR", "TIMEOUT", "OVERFLOW_RETRY", "NO_DEVICE",
+                "UNSUPPORTED", "BUSY"]
+MESH_REGULAR, MESH_EXTRUDED = 0, 1
+F32, F64 = 0, 1
+LAYOUT_MULTICOMPONENT, LAYOUT_SEPARATE, LAYOUT_PER_VERTEX = 0, 1, 2
+HOST, DEVICE = 0, 1
+PRECISION_EXACT, PRECISION_REFINED = 0, 1
+OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK = 1, 2
+CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
+               "center"]
+
+
+class Ftk2bError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"{name}: {msg}")
+        self.status = status
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("ndims", C.c_int),
+        ("local_dims", C.c_uint64 * 4), ("offset", C.c_uint64 * 4), ("global_dims", C.c_uint64 * 4),
+        ("n_base_verts", C.c_uint64), ("base_cells", C.c_void_p), ("n_base_cells", C.c_uint64),
+        ("base_cell_dim", C.c_int), ("n_layers", C.c_uint64),
+    ]
+
+
+class FieldDesc(C.Structure):
+    _fields_ = [
+        ("dtype", C.c_int), ("ncomp", C.c_int), ("layout", C.c_int), ("location", C.c_int),
+        ("comp", C.c_void_p * 3), ("nd", C.c_int), ("dims", C.c_uint64 * 4),
+        ("scalar", C.c_void_p), ("scalar_nd", C.c_int), ("scalar_dims", C.c_uint64 * 4),
+    ]
+
+
+class CPParams(C.Structure):
+    _fields_ = [("sos_q", C.c_double), ("precision", C.c_int), ("want_edges", C.c_int),
+                ("classify", C.c_int)]
+
+
+class CPResultC(C.Structure):
+    _fields_ = [
+        ("m", C.c_int), ("n_features", C.c_uint64),
+        ("simplices", C.POINTER(C.c_uint64)), ("lambda_", C.POINTER(C.c_double)),
+        ("barycentric", C.POINTER(C.c_float)), ("track_id", C.POINTER(C.c_uint64)),
+        ("type", C.POINTER(C.c_uint32)), ("cp_class", C.POINTER(C.c_uint32)),
+        ("scalar", C.POINTER(C.c_float)),
+        ("n_edges", C.c_uint64), ("edges", C.POINTER(C.c_uint32)),
+        ("n_tracks", C.c_uint64), ("n_simplices", C.c_uint64), ("device_ms", C.c_double),
+    ]
+
+
+# name -> (restype, argtypes); every symbol include/ftk2b.h declares
+SIGNATURES = {
+    "ftk2b_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "ftk2b_ctx_destroy": (None, [C.c_void_p]),
+    "ftk2b_last_error": (C.c_char_p, [C.c_void_p]),
+    "ftk2b_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "ftk2b_cp_params_default": (CPParams, []),
+    "ftk2b_ctx_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
+    "ftk2b_mesh_simplex_count": (C.c_uint64, [C.POINTER(MeshDesc), C.c_int]),
+    "ftk2b_cp_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                   C.POINTER(CPParams), C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_cp_result_free": (None, [C.POINTER(CPResultC)]),
+    "ftk2b_cp_run": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                               C.POINTER(CPParams), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_ctx_last_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_uint64)]),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libftk2b.so and bind every exported entry point.  Raises if the
+    library has not been built: the path has no CPU fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library not built: {path} (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+# ---------------------------------------------------------------------------
+# descriptors
+
+
+def regular_mesh_desc(local_dims, offset=None, global_dims=None) -> MeshDesc:
+    nd = len(local_dims)
+    offset = list(offset) if offset is not None else [0] * nd
+    global_dims = list(global_dims) if global_dims is not None else list(local_dims)
+    m = MeshDesc()
+    m.kind = MESH_REGULAR
+    m.ndims = nd
+    for i in range(nd):
+        m.local_dims[i] = int(local_dims[i])
+        m.offset[i] = int(offset[i])
+        m.global_dims[i] = int(global_dims[i])
+    return m
+
+
+def extruded_mesh_desc(n_base_verts: int, cells: np.ndarray, n_layers: int, keep: list) -> MeshDesc:
+    cells = np.ascontiguousarray(cells, dtype=np.uint64)
+    keep.append(cells)
+    m = MeshDesc()
+    m.kind = MESH_EXTRUDED
+    m.ndims = cells.shape[1]
+    m.n_base_verts = int(n_base_verts)
+    m.base_cells = cells.ctypes.data
+    m.n_base_cells = cells.shape[0]
+    m.base_cell_dim = cells.shape[1] - 1
+    m.n_layers = int(n_layers)
+    return m
+
+
+def _is_torch_cuda(a) -> bool:
+    return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
+
+
+def _ptr_dtype_shape(a, keep: list):
+    if _is_torch_cuda(a):
+        if not a.is_contiguous():
+            raise ValueError("device arrays must be contiguous")
+        import torch
+        dt = {torch.float64: F64, torch.float32: F32}.get(a.dtype)
+        if dt is None:
+            raise ValueError(f"unsupported dtype {a.dtype}")
+        keep.append(a)
+        return a.data_ptr(), dt, tuple(a.shape), DEVICE
+    a = np.ascontiguousarray(a)
+    if a.dtype not in (np.float64, np.float32):
+        raise ValueError(f"unsupported dtype {a.dtype}")
+    keep.append(a)
+    return a.ctypes.data, (F64 if a.dtype == np.float64 else F32), a.shape, HOST
+
+
+def field_desc(arrays, layout: int, ncomp: int, scalar=None, keep: Optional[list] = None) -> FieldDesc:
+    """MULTICOMPONENT: one array of C-order shape (..reversed dims.., M).
+    SEPARATE / PER_VERTEX: a sequence of M arrays of C-order shape reversed dims."""
+    keep = keep if keep is not None else []
+    f = FieldDesc()
+    f.ncomp = ncomp
+    f.layout = layout
+    if layout == LAYOUT_MULTICOMPONENT:
+        p, dt, shape, loc = _ptr_dtype_shape(arrays, keep)
+        if shape[-1] != ncomp:
+            raise ValueError("multicomponent arrays carry the component axis last (fastest)")
+        f.comp[0] = p
+        dims = tuple(shape[::-1][1:])
+    else:
+        dims = None
+        loc = dt = None
+        for j, a in enumerate(arrays):
+            p, dtj, shape, locj = _ptr_dtype_shape(a, keep)
+            f.comp[j] = p
+            dims = tuple(shape[::-1])
+            dt, loc = dtj, locj
+    f.dtype, f.location = dt, loc
+    f.nd = len(dims)
+    for i, d in enumerate(dims):
+        f.dims[i] = int(d)
+    if scalar is not None:
+        p, _, shape, _ = _ptr_dtype_shape(scalar, keep)
+        f.scalar = p
+        f.scalar_nd = len(shape)
+        for i, d in enumerate(shape[::-1]):
+            f.scalar_dims[i] = int(d)
+    return f
+
+
+def params(sos_q: float = 1e6, precision: int = PRECISION_EXACT, want_edges: bool = True,
+           classify: bool = False) -> CPParams:
+    p = CPParams()
+    p.sos_q = float(sos_q)
+    p.precision = int(precision)
+    p.want_edges = int(bool(want_edges))
+    p.classify = int(bool(classify))
+    return p
+
+
+@dataclass
+class CPResult:
+    """Flattened FeatureComplex (complex.hpp:14-58) of one extraction."""
+    simplices: np.ndarray      # (n, m+1) uint64 sorted vertex ids, canonical order
+    lam: np.ndarray            # (n, m+1) float64 barycentrics
+    bary: np.ndarray           # (n, m+1) float32 as FeatureElement stores them
+    track_id: np.ndarray       # (n,) uint64
+    type: np.ndarray           # (n,) uint32 (0)
+    cp_class: np.ndarray       # (n,) uint32
+    scalar: np.ndarray         # (n,) float32
+    edges: np.ndarray          # (e, 2) uint32
+    n_tracks: int = 0
+    n_simplices: int = 0
+    device_ms: float = 0.0
+
+
+def _result_from_c(r: CPResultC) -> CPResult:
+    n, k, e = int(r.n_features), int(r.m) + 1, int(r.n_edges)
+
+    def arr(ptr, count, dt):
+        if count == 0:
+            return np.zeros(0, dtype=dt)
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+    return CPResult(
+        simplices=arr(r.simplices, n * k, np.uint64).reshape(n, k),
+        lam=arr(r.lambda_, n * k, np.float64).reshape(n, k),
+        bary=arr(r.barycentric, n * k, np.float32).reshape(n, k),
+        track_id=arr(r.track_id, n, np.uint64),
+        type=arr(r.type, n, np.uint32),
+        cp_class=arr(r.cp_class, n, np.uint32),
+        scalar=arr(r.scalar, n, np.float32),
+        edges=arr(r.edges, 2 * e, np.uint32).reshape(e, 2),
+        n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
+
+
+class Context:
+    """One ftk2b_ctx: a device, a CUDA stream and reusable device buffers."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.ftk2b_ctx_create(int(device), C.byref(h))
+        if st != OK:
+            raise Ftk2bError(st, "ftk2b_ctx_create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ftk2b_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.lib.ftk2b_ctx_stream(self.h) or 0)
+
+    def set_option(self, option: int, value: int):
+        self._check(self.lib.ftk2b_ctx_set_option(self.h, int(option), int(value)))
+
+    def last_error(self) -> str:
+        return (self.lib.ftk2b_last_error(self.h) or b"").decode()
+
+    def _check(self, st: int):
+        if st != OK:
+            raise Ftk2bError(st, self.last_error())
+
+    def extract(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None) -> CPResult:
+        prm = prm or params()
+        out = C.POINTER(CPResultC)()
+        self._check(self.lib.ftk2b_cp_extract(self.h, C.byref(mesh), C.byref(field), C.byref(prm),
+                                              C.byref(out)))
+        try:
+            return _result_from_c(out.contents)
+        finally:
+            self.lib.ftk2b_cp_result_free(out)
+
+    def run(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None):
+        """Device pipeline only; results stay on the device until fetch()."""
+        prm = prm or params()
+        n, ne = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.ftk2b_cp_run(self.h, C.byref(mesh), C.byref(field), C.byref(prm),
+                                          C.byref(n), C.byref(ne)))
+        return int(n.value), int(ne.value)
+
+    def last_timing(self):
+        """(extraction kernel ms, whole pipeline ms, kernels launched so far)."""
+        x, t, k = C.c_double(), C.c_double(), C.c_uint64()
+        self._check(self.lib.ftk2b_ctx_last_timing(self.h, C.byref(x), C.byref(t), C.byref(k)))
+        return float(x.value), float(t.value), int(k.value)
+
+    def fetch(self) -> CPResult:
+        out = C.POINTER(CPResultC)()
+        self._check(self.lib.ftk2b_cp_fetch(self.h, C.byref(out)))
+        try:
+            return _result_from_c(out.contents)
+        finally:
+            self.lib.ftk2b_cp_result_free(out)
+
+
+def simplex_count(mesh: MeshDesc, m: int) -> int:
+    return int(load_library().ftk2b_mesh_simplex_count(C.byref(mesh), int(m)))
+
+
+# ---------------------------------------------------------------------------
+# mirror of the reference's engine interface
+
+
+class RegularSimplicialMesh:
+    """RegularSimplicialMesh(dims, offset, global_dims) (mesh.hpp:256-265)."""
+
+    def __init__(self, dims: Sequence[int], offset: Optional[Sequence[int]] = None,
+                 global_dims: Optional[Sequence[int]] = None):
+        self.dims = list(dims)
+        self.offset = list(offset) if offset else [0] * len(dims)
+        self.global_dims = list(global_dims) if global_dims else list(dims)
+
+    def get_total_dimension(self) -> int:
+        return len(self.dims)
+
+    def desc(self, keep: list) -> MeshDesc:
+        return regular_mesh_desc(self.dims, self.offset, self.global_dims)
+
+
+class UnstructuredSimplicialMesh:
+    """UnstructuredSimplicialMesh(spatial_dim, cell_dim, coords, cells)
+    (unstructured_mesh.hpp:16-76); coords are (n, 3), cells (n_cells, cell_dim+1)."""
+
+    def __init__(self, spatial_dim: int, cell_dim: int, coords: np.ndarray, cells: np.ndarray):
+        self.spatial_dim = spatial_dim
+        self.cell_dim = cell_dim
+        self.coords = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+        self.cells = np.asarray(cells, dtype=np.uint64).reshape(-1, cell_dim + 1)
+
+    def get_total_dimension(self) -> int:
+        return self.cell_dim
+
+
+class ExtrudedSimplicialMesh:
+    """ExtrudedSimplicialMesh(base, n_layers) (mesh.hpp:542-562)."""
+
+    def __init__(self, base: UnstructuredSimplicialMesh, n_layers: int):
+        self.base = base
+        self.n_layers = int(n_layers)
+
+    def get_total_dimension(self) -> int:
+        return self.base.get_total_dimension() + 1
+
+    def desc(self, keep: list) -> MeshDesc:
+        return extruded_mesh_desc(self.base.coords.shape[0], self.base.cells, self.n_layers, keep)
+
+
+@dataclass
+class CriticalPointPredicate:
+    """CriticalPointPredicate<M,T> knobs (predicate.hpp:22-64)."""
+    M: int
+    vector_var_name: str = ""
+    var_names: list = field(default_factory=list)
+    scalar_var_name: str = ""
+    use_multicomponent: bool = True
+    sos_q: float = 1e6
+    precision: int = PRECISION_EXACT
+    classify: bool = False
+
+
+class SimplicialEngine:
+    """SimplicialEngine<T, CriticalPointPredicate<M,T>> (engine.hpp:79-996) on the GPU."""
+
+    def __init__(self, mesh, pred: CriticalPointPredicate, ctx: Optional[Context] = None):
+        self.mesh = mesh
+        self.pred = pred
+        self.ctx = ctx or Context(0)
+        self._result: Optional[CPResult] = None
+
+    def _field(self, data: dict, keep: list) -> FieldDesc:
+        p = self.pred
+        scalar = data[p.scalar_var_name] if p.scalar_var_name else None
+        if p.use_multicomponent and p.vector_var_name:
+            return field_desc(data[p.vector_var_name], LAYOUT_MULTICOMPONENT, p.M, scalar, keep)
+        arrays = [data[n] for n in p.var_names[:p.M]]
+        layout = LAYOUT_PER_VERTEX if isinstance(self.mesh, ExtrudedSimplicialMesh) else LAYOUT_SEPARATE
+        return field_desc(arrays, layout, p.M, scalar, keep)
+
+    def execute(self, data: dict, var_names=None):
+        keep: list = []
+        mesh = self.mesh.desc(keep)
+        fld = self._field(data, keep)
+        prm = params(self.pred.sos_q, self.pred.precision, True, self.pred.classify)
+        self._result = self.ctx.extract(mesh, fld, prm)
+
+    execute_cuda = execute
+
+    def get_complex(self) -> CPResult:
+        if self._result is None:
+            raise RuntimeError("execute() has not run")
+        return self._result

@@ -1,0 +1,66 @@
+// Context object and cross-file declarations of the C-ABI layer.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/ftk2b.h"
+#include "cp_internal.h"
+#include "cp_post.h"
+
+namespace ftk2b {
+
+// grow-only device allocation owned by a context
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want);
+  void release();
+};
+
+enum { kCountFeatures = 0, kCountEdges = 1, kCountRoots = 2, kCountErr = 3, kNumCounters = 8 };
+
+struct LastRun {
+  int kind = 0, m = 0;
+  uint64_t n = 0, ne = 0, n_roots = 0, n_simplices = 0;
+  double device_ms = 0;
+  int classify = 0, want_edges = 1;
+};
+
+}  // namespace ftk2b
+
+struct ftk2b_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_x = nullptr;
+  unsigned long long launches = 0;
+  double last_extract_ms = 0;
+  std::string err;
+  unsigned cap_hint = 0;
+  int tune_tchunk = 0;
+  ftk2b::DevBuf stage[3], stage_scalar;
+  ftk2b::DevBuf key, lam, bary4, scalar, key_alt, perm0, perm1, hist, lam_s, bary4_s, scalar_s,
+      simplices, bary, track, edge_cnt, edges, parent, counters, cls;
+  std::vector<ftk2b::DevBuf> extra;
+  ftk2b::LastRun last;
+
+  int sort_grid() const { return num_sms * 2; }
+  void release_all();
+  std::vector<ftk2b::DevBuf*> all_bufs();
+  ftk2b::PostBuffers post_buffers(unsigned cap, unsigned edge_cap, int key_bits);
+};
+
+namespace ftk2b {
+
+ftk2b_status prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int mesh_d,
+                           const uint64_t* need_global_hi, const uint64_t* need_local_hi,
+                           uint64_t n_vertices, FieldAccess& fa);
+ftk2b_status ensure_feature_buffers(ftk2b_ctx* ctx, unsigned cap, unsigned edge_cap, int m);
+
+}  // namespace ftk2b
+
+// extruded meshes (cp_extruded.cu)
+ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                          const ftk2b_cp_params* prm);
+uint64_t extruded_simplex_count(const ftk2b_mesh_desc* mesh, int m);

@@ -1,0 +1,73 @@
+// Internal launch descriptors shared by the kernel translation units and the
+// C-ABI layer.  Plain structs passed to kernels by value.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ftk2b {
+
+constexpr int kMaxChains = 64;
+
+// Value access for a field sampled on a regular grid or per vertex.
+//   multicomponent [M, d0, d1, ...] (Fortran):  comp[j] = base + j,
+//       estride = {M, M*d0, M*d0*d1, ...}, shift = 0 (global coordinates,
+//       engine.hpp:1101-1124)
+//   separate arrays [d0, d1, ...]:             comp[j] = array j,
+//       estride = {1, d0, d0*d1, ...}, shift = mesh offset (engine.hpp:999-1009)
+//   per-vertex 1D arrays:                      index = vertex id
+struct FieldAccess {
+  const void* comp[3];
+  long long estride[4];
+  long long shift[4];
+  int per_vertex;
+  // optional scalar (interpolated only for separate-array fields,
+  // predicate.hpp:81-92 with the arrays the engine passes, engine.hpp:1125-1139)
+  const void* scalar;
+  long long sstride[4];
+  int scalar_per_vertex;
+  int has_scalar;
+};
+
+// Regular spacetime mesh: RegularSimplicialMesh(local, offset, global)
+// (mesh.hpp:256-265).  Corners range over the local box; vertex ids use the
+// global dims (mesh.hpp:439-451).
+struct RegularMesh {
+  int d;                       // 3 (2D + t) or 4 (3D + t)
+  long long ld[4];             // local dims
+  long long off[4];            // offset of the local box in global coordinates
+  long long gd[4];             // global dims
+  unsigned long long gstride[4];
+};
+
+// Output of the extraction stage (unsorted, capacity-bounded)
+struct FeatureSink {
+  unsigned long long* key;     // canonical key: corner vertex id * n_chains + chain rank
+  double* lam;                 // 4 per feature: reported barycentrics
+  float* bary4;                // 4 per feature: (float) of the exact-path barycentrics
+  float* scalar;
+  unsigned int* count;         // number found (may exceed cap: overflow)
+  unsigned int cap;
+};
+
+struct ExtractConfig {
+  double Q;                    // sos_q
+  int refined;                 // 1: report FP32 + one FP64 refinement step
+  int tchunk;                  // corner time steps per block
+  int tiles[3];                // tiles along x, y, z (z = 1 for 2D)
+};
+
+// chain tables: masks of vertices 1..m of every m-simplex type of a
+// d-hypercube, in canonical (vertex-id) order
+struct ChainTable {
+  int n;
+  unsigned char mask[kMaxChains][4];
+};
+
+void upload_chain_tables();
+
+cudaError_t launch_extract_regular(int dtype_f64, const RegularMesh& mesh, const FieldAccess& fa,
+                                   const ExtractConfig& cfg, const FeatureSink& sink,
+                                   cudaStream_t st);
+
+}  // namespace ftk2b

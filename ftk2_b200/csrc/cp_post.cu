@@ -1,0 +1,476 @@
+// Post-extraction stages of the critical-point path, all on the device and
+// driven by device-resident counts (so the whole pipeline can be enqueued, and
+// captured in a CUDA graph, without a host round trip):
+//
+//   1. canonical order: LSD radix sort of the feature keys.  Key order equals
+//      the reference's Simplex::operator< order (mesh.hpp:36-42), so sorted
+//      position = canonical id (engine.hpp:838-850).
+//   2. star edges: for every feature, the top cells it is a face of (the two
+//      Kuhn cofaces of a codimension-1 simplex), their other faces looked up by
+//      binary search; the smallest active face of a cell is the star centre and
+//      links to every other active face (engine.hpp:1342-1387; for regular
+//      meshes encode_simplex_id order equals key order, mesh.hpp:736-749).
+//   3. trajectories: lock-free union-find that always hooks the larger root
+//      under the smaller one, so every component's root is its smallest
+//      canonical id = the reference's track_id (engine.hpp:46-74, 965-983).
+#include "cp_post.h"
+
+namespace ftk2b {
+
+__constant__ ChainTable c_post_chains[2];
+__constant__ signed char c_rank3[64];     // (m1 | m2 << 3) -> chain rank, d = 3
+__constant__ signed char c_rank4[4096];   // (m1 | m2 << 4 | m3 << 8) -> chain rank, d = 4
+
+// ---------------------------------------------------------------------------
+// radix sort (keys u64, payload u32), stable, device-resident count
+
+constexpr int kRsThreads = 256;
+
+__global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
+                               unsigned cap, int shift, unsigned* __restrict__ hist) {
+  __shared__ unsigned h[256];
+  const unsigned n = min(*n_ptr, cap);
+  const unsigned G = gridDim.x, b = blockIdx.x;
+  const unsigned chunk = (n + G - 1) / G;
+  const unsigned start = min(b * chunk, n), end = min(start + chunk, n);
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  for (unsigned i = start + threadIdx.x; i < end; i += kRsThreads)
+    atomicAdd(&h[(keys[i] >> shift) & 255], 1u);
+  __syncthreads();
+  hist[threadIdx.x * G + b] = h[threadIdx.x];
+}
+
+// exclusive scan of `total` counters in place, one block of 1024 threads
+__global__ void scan_inplace_kernel(unsigned* __restrict__ a, unsigned total, unsigned* total_out,
+                                    const unsigned* n_ptr) {
+  __shared__ unsigned part[1024];
+  const unsigned t = threadIdx.x;
+  if (n_ptr) total = min(total, *n_ptr);
+  const unsigned seg = (total + 1023) / 1024;
+  const unsigned s0 = min(t * seg, total), s1 = min(s0 + seg, total);
+  unsigned sum = 0;
+  for (unsigned i = s0; i < s1; ++i) sum += a[i];
+  part[t] = sum;
+  __syncthreads();
+  for (unsigned off = 1; off < 1024; off <<= 1) {
+    unsigned v = (t >= off) ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  unsigned run = part[t] - sum;
+  for (unsigned i = s0; i < s1; ++i) {
+    unsigned v = a[i];
+    a[i] = run;
+    run += v;
+  }
+  if (total_out && t == 1023) *total_out = part[1023];
+}
+
+__global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
+                                  const unsigned* __restrict__ vin,
+                                  unsigned long long* __restrict__ kout, unsigned* __restrict__ vout,
+                                  const unsigned* n_ptr, unsigned cap, int shift,
+                                  const unsigned* __restrict__ hist) {
+  __shared__ unsigned base[256];
+  __shared__ unsigned wcnt[kRsThreads / 32][256];
+  const unsigned n = min(*n_ptr, cap);
+  const unsigned G = gridDim.x, b = blockIdx.x;
+  const unsigned chunk = (n + G - 1) / G;
+  const unsigned start = min(b * chunk, n), end = min(start + chunk, n);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  base[tid] = hist[tid * G + b];
+  for (unsigned t0 = start; t0 < end; t0 += kRsThreads) {
+    const unsigned i = t0 + tid;
+    const bool valid = i < end;
+    const unsigned long long key = valid ? kin[i] : 0ull;
+    const unsigned val = valid ? vin[i] : 0u;
+    const unsigned dig = valid ? (unsigned)((key >> shift) & 255) : 256u;
+#pragma unroll
+    for (int w = 0; w < kRsThreads / 32; ++w) wcnt[w][tid] = 0;
+    __syncthreads();
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
+    const unsigned rank = __popc(peers & ((1u << lane) - 1));
+    if (valid && lane == __ffs(peers) - 1) wcnt[warp][dig] = __popc(peers);
+    __syncthreads();
+    unsigned run = 0;
+#pragma unroll
+    for (int w = 0; w < kRsThreads / 32; ++w) {
+      const unsigned c = wcnt[w][tid];
+      wcnt[w][tid] = run;
+      run += c;
+    }
+    __syncthreads();
+    if (valid) {
+      const unsigned pos = base[dig] + wcnt[warp][dig] + rank;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+    base[tid] += run;
+    __syncthreads();
+  }
+}
+
+__global__ void iota_kernel(unsigned* v, const unsigned* n_ptr, unsigned cap) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+// Sorts (keys, vals) of device count *n_ptr (clamped to cap) over the low
+// `bits` bits.  Result lands in whichever buffer pair the pass parity selects;
+// returns true when it is the alternate pair.
+bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, unsigned* v1,
+                const unsigned* n_ptr, unsigned cap, int bits, unsigned* hist, int grid,
+                cudaStream_t st, unsigned long long* launches) {
+  bool alt = false;
+  for (int shift = 0; shift < bits; shift += 8) {
+    const unsigned long long* ki = alt ? k1 : k0;
+    const unsigned* vi = alt ? v1 : v0;
+    unsigned long long* ko = alt ? k0 : k1;
+    unsigned* vo = alt ? v0 : v1;
+    rs_hist_kernel<<<grid, kRsThreads, 0, st>>>(ki, n_ptr, cap, shift, hist);
+    scan_inplace_kernel<<<1, 1024, 0, st>>>(hist, 256u * grid, nullptr, nullptr);
+    rs_scatter_kernel<<<grid, kRsThreads, 0, st>>>(ki, vi, ko, vo, n_ptr, cap, shift, hist);
+    if (launches) *launches += 3;
+    alt = !alt;
+  }
+  return alt;
+}
+
+// ---------------------------------------------------------------------------
+// gather features into canonical order
+
+__global__ void gather_kernel(const unsigned* n_ptr, unsigned cap, const unsigned* __restrict__ perm,
+                              const double* __restrict__ lam_in, const float* __restrict__ sc_in,
+                              const float* __restrict__ bary_in, double* __restrict__ lam_out,
+                              float* __restrict__ sc_out, float* __restrict__ bary_out) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned p = perm[i];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      lam_out[4 * (size_t)i + k] = lam_in[4 * (size_t)p + k];
+      bary_out[4 * (size_t)i + k] = bary_in[4 * (size_t)p + k];
+    }
+    sc_out[i] = sc_in[p];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// regular-mesh geometry helpers
+
+struct Decoded {
+  long long g[4];  // global coords of the corner
+  int mk[5];       // masks of the m+1 vertices (mk[0] = 0)
+};
+
+__device__ __forceinline__ void decode_key(const RegularMesh& mesh, int nch, unsigned long long key,
+                                           Decoded& dc) {
+  const ChainTable& CT = c_post_chains[mesh.d - 3];
+  const int m = mesh.d - 1;
+  unsigned long long vid = key / (unsigned long long)nch;
+  const int ch = (int)(key % (unsigned long long)nch);
+  for (int k = 0; k < mesh.d; ++k) {
+    dc.g[k] = (long long)(vid % (unsigned long long)mesh.gd[k]);
+    vid /= (unsigned long long)mesh.gd[k];
+  }
+  dc.mk[0] = 0;
+  for (int i = 0; i < m; ++i) dc.mk[i + 1] = CT.mask[ch][i];
+}
+
+__device__ __forceinline__ int chain_rank(int d, const int* rel /* m masks */) {
+  if (d == 3) return c_rank3[rel[0] | (rel[1] << 3)];
+  return c_rank4[rel[0] | (rel[1] << 4) | (rel[2] << 8)];
+}
+
+__device__ __forceinline__ long long find_key(const unsigned long long* keys, unsigned n,
+                                              unsigned long long k) {
+  unsigned lo = 0, hi = n;
+  while (lo < hi) {
+    const unsigned mid = (lo + hi) >> 1;
+    const unsigned long long v = keys[mid];
+    if (v == k) return mid;
+    if (v < k) lo = mid + 1;
+    else hi = mid;
+  }
+  return -1;
+}
+
+// Cofaces (top cells) of the feature's simplex inside the local box, each as
+// corner + d+1 vertex masks.  A codimension-1 simplex of a Kuhn triangulation
+// has exactly two: if one axis a never steps, prepend (corner - e_a) or append
+// (full mask); otherwise split the one two-axis step in either order.
+__device__ int top_cells(const RegularMesh& mesh, const Decoded& dc, long long cc[2][4],
+                         int cm[2][5]) {
+  const int d = mesh.d, m = d - 1, full = (1 << d) - 1;
+  int nc = 0;
+  const int missing = full & ~dc.mk[m];
+  if (missing) {
+    const int a = __ffs(missing) - 1;
+    if (dc.g[a] - mesh.off[a] >= 1) {
+      for (int k = 0; k < 4; ++k) cc[nc][k] = dc.g[k];
+      cc[nc][a] -= 1;
+      cm[nc][0] = 0;
+      for (int j = 0; j <= m; ++j) cm[nc][j + 1] = dc.mk[j] | (1 << a);
+      ++nc;
+    }
+    if (dc.g[a] - mesh.off[a] + 1 < mesh.ld[a]) {
+      for (int k = 0; k < 4; ++k) cc[nc][k] = dc.g[k];
+      for (int j = 0; j <= m; ++j) cm[nc][j] = dc.mk[j];
+      cm[nc][m + 1] = full;
+      ++nc;
+    }
+  } else {
+    for (int j = 1; j <= m; ++j) {
+      const int step = dc.mk[j] & ~dc.mk[j - 1];
+      if (__popc(step) == 2) {
+        const int lo = step & -step, hi = step & ~lo;
+        const int ins[2] = {lo, hi};
+        for (int q = 0; q < 2; ++q) {
+          for (int k = 0; k < 4; ++k) cc[nc][k] = dc.g[k];
+          int w = 0;
+          for (int jj = 0; jj <= m; ++jj) {
+            if (jj == j) cm[nc][w++] = dc.mk[j - 1] | ins[q];
+            cm[nc][w++] = dc.mk[jj];
+          }
+          ++nc;
+        }
+        break;
+      }
+    }
+  }
+  return nc;
+}
+
+// Indices of the active faces of a top cell, ascending.
+__device__ int active_faces(const RegularMesh& mesh, int nch, const unsigned long long* keys,
+                            unsigned n, const long long cc[4], const int cm[5], long long out[5]) {
+  const int d = mesh.d, m = d - 1;
+  int na = 0;
+  for (int r = 0; r <= d; ++r) {
+    // face without vertex r: corner = cell vertex (r == 0 ? 1 : 0)
+    const int basem = (r == 0) ? cm[1] : 0;
+    int rel[4];
+    int w = 0;
+    for (int i = 0; i <= d; ++i) {
+      if (i == r || (r == 0 && i == 1) || (r != 0 && i == 0)) continue;
+      rel[w++] = cm[i] & ~basem;
+    }
+    unsigned long long vid = 0;
+    for (int k = 0; k < d; ++k)
+      vid += (unsigned long long)(cc[k] + ((basem >> k) & 1)) * mesh.gstride[k];
+    const int rk = chain_rank(d, rel);
+    const long long idx = find_key(keys, n, vid * (unsigned long long)nch + (unsigned long long)rk);
+    if (idx >= 0) out[na++] = idx;
+    (void)m;
+  }
+  // insertion sort (at most 5)
+  for (int i = 1; i < na; ++i)
+    for (int j = i; j > 0 && out[j - 1] > out[j]; --j) {
+      long long t = out[j];
+      out[j] = out[j - 1];
+      out[j - 1] = t;
+    }
+  return na;
+}
+
+// pass 0: count edges per feature (as star centre); pass 1: write them
+template <int PASS>
+__global__ void edges_regular_kernel(RegularMesh mesh, int nch, const unsigned long long* __restrict__ keys,
+                                     const unsigned* n_ptr, unsigned cap, unsigned* __restrict__ cnt,
+                                     const unsigned* __restrict__ off, unsigned* __restrict__ edges,
+                                     unsigned edge_cap) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Decoded dc;
+    decode_key(mesh, nch, keys[i], dc);
+    long long cc[2][4];
+    int cm[2][5];
+    const int nc = top_cells(mesh, dc, cc, cm);
+    long long others[8];
+    int no = 0;
+    for (int q = 0; q < nc; ++q) {
+      long long act[5];
+      const int na = active_faces(mesh, nch, keys, n, cc[q], cm[q], act);
+      if (na >= 2 && act[0] == (long long)i)
+        for (int t = 1; t < na; ++t) others[no++] = act[t];
+    }
+    if (PASS == 0) {
+      cnt[i] = no;
+    } else {
+      for (int a = 1; a < no; ++a)
+        for (int b = a; b > 0 && others[b - 1] > others[b]; --b) {
+          long long t = others[b];
+          others[b] = others[b - 1];
+          others[b - 1] = t;
+        }
+      const unsigned o = off[i];
+      for (int t = 0; t < no; ++t)
+        if (o + t < edge_cap) {
+          edges[2 * (size_t)(o + t)] = i;
+          edges[2 * (size_t)(o + t) + 1] = (unsigned)others[t];
+        }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// union-find
+
+__global__ void uf_init_kernel(unsigned* parent, const unsigned* n_ptr, unsigned cap) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    parent[i] = i;
+}
+
+__device__ __forceinline__ unsigned uf_root(unsigned* parent, unsigned x) {
+  // follow parents to the root, halving the path on the way; parents only
+  // ever decrease, so the halving writes (atomicMin) never undo a hook
+  unsigned p = __ldcg(&parent[x]);
+  while (p != x) {
+    const unsigned gp = __ldcg(&parent[p]);
+    if (gp < p) atomicMin(&parent[x], gp);
+    x = p;
+    p = gp;
+  }
+  return x;
+}
+
+__global__ void uf_hook_kernel(unsigned* parent, const unsigned* __restrict__ edges,
+                               const unsigned* ne_ptr, unsigned edge_cap, unsigned* err) {
+  const unsigned ne = min(*ne_ptr, edge_cap);
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    unsigned a = edges[2 * (size_t)e], b = edges[2 * (size_t)e + 1];
+    // every retry follows a successful hook by another thread, and links only
+    // go to smaller indices, so this terminates; the bound is a safety net
+    int it = 0;
+    for (; it < (1 << 20); ++it) {
+      const unsigned ra = uf_root(parent, a), rb = uf_root(parent, b);
+      if (ra == rb) break;
+      const unsigned lo = min(ra, rb), hi = max(ra, rb);
+      if (atomicCAS(&parent[hi], hi, lo) == hi) break;
+      a = ra;
+      b = rb;
+    }
+    if (it == (1 << 20)) atomicOr(err, 1u);
+  }
+}
+
+__global__ void uf_label_kernel(unsigned* parent, const unsigned* n_ptr, unsigned cap,
+                                unsigned long long* __restrict__ track, unsigned* n_roots) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned x = uf_root(parent, i);
+    track[i] = x;
+    if (x == i) atomicAdd(n_roots, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// output expansion: vertex ids and float barycentrics
+
+__global__ void expand_regular_kernel(RegularMesh mesh, int nch, const unsigned long long* __restrict__ keys,
+                                      const unsigned* n_ptr, unsigned cap,
+                                      const float* __restrict__ bary4,
+                                      unsigned long long* __restrict__ simplices,
+                                      float* __restrict__ bary) {
+  const unsigned n = min(*n_ptr, cap);
+  const int m = mesh.d - 1;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Decoded dc;
+    decode_key(mesh, nch, keys[i], dc);
+    for (int v = 0; v <= m; ++v) {
+      unsigned long long vid = 0;
+      for (int k = 0; k < mesh.d; ++k)
+        vid += (unsigned long long)(dc.g[k] + ((dc.mk[v] >> k) & 1)) * mesh.gstride[k];
+      simplices[(size_t)i * (m + 1) + v] = vid;
+      bary[(size_t)i * (m + 1) + v] = bary4[4 * (size_t)i + v];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+
+void upload_post_tables() {
+  ChainTable h[2];
+  // same construction as the extraction tables (canonical chain order)
+  auto build = [](ChainTable& t, int d, int m) {
+    t.n = 0;
+    const int full = (1 << d) - 1;
+    int cur[5] = {0, 0, 0, 0, 0}, next[5] = {0, 0, 0, 0, 0};
+    int depth = 1;
+    while (depth > 0) {
+      const int prev = cur[depth - 1];
+      int nx = next[depth] + 1;
+      while (nx <= full && !(((nx & prev) == prev) && nx != prev)) ++nx;
+      if (nx > full) {
+        next[depth] = 0;
+        --depth;
+        continue;
+      }
+      next[depth] = nx;
+      cur[depth] = nx;
+      if (depth == m) {
+        for (int k = 0; k < m; ++k) t.mask[t.n][k] = (unsigned char)cur[k + 1];
+        t.n++;
+      } else {
+        ++depth;
+        next[depth] = 0;
+      }
+    }
+  };
+  build(h[0], 3, 2);
+  build(h[1], 4, 3);
+  cudaMemcpyToSymbol(c_post_chains, h, sizeof(h));
+  signed char r3[64], r4[4096];
+  for (int i = 0; i < 64; ++i) r3[i] = -1;
+  for (int i = 0; i < 4096; ++i) r4[i] = -1;
+  for (int c = 0; c < h[0].n; ++c) r3[h[0].mask[c][0] | (h[0].mask[c][1] << 3)] = (signed char)c;
+  for (int c = 0; c < h[1].n; ++c)
+    r4[h[1].mask[c][0] | (h[1].mask[c][1] << 4) | (h[1].mask[c][2] << 8)] = (signed char)c;
+  cudaMemcpyToSymbol(c_rank3, r3, sizeof(r3));
+  cudaMemcpyToSymbol(c_rank4, r4, sizeof(r4));
+}
+
+static int grid_for(unsigned cap, int threads, int max_blocks) {
+  long long b = ((long long)cap + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuffers& B,
+                                int want_edges, cudaStream_t st, unsigned long long* launches) {
+  const unsigned cap = B.cap;
+  const int gsort = B.sort_grid;
+  const int g = grid_for(cap, 256, 4096);
+  // keys in canonical order
+  iota_kernel<<<g, 256, 0, st>>>(B.perm0, B.count, cap);
+  const bool alt = radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits,
+                              B.hist, gsort, st, launches);
+  *launches += 3;  // iota, gather, expand
+  const unsigned long long* skey = alt ? B.key_alt : B.key;
+  const unsigned* perm = alt ? B.perm1 : B.perm0;
+  gather_kernel<<<g, 256, 0, st>>>(B.count, cap, perm, B.lam, B.scalar, B.bary4, B.lam_sorted,
+                                   B.scalar_sorted, B.bary4_sorted);
+  expand_regular_kernel<<<g, 256, 0, st>>>(mesh, nch, skey, B.count, cap, B.bary4_sorted,
+                                           B.simplices, B.bary);
+  if (!want_edges) return cudaGetLastError();
+  // star edges, written in (centre, other) order: already sorted and unique
+  edges_regular_kernel<0><<<g, 128, 0, st>>>(mesh, nch, skey, B.count, cap, B.edge_cnt, nullptr,
+                                             nullptr, 0);
+  scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count);
+  edges_regular_kernel<1><<<g, 128, 0, st>>>(mesh, nch, skey, B.count, cap, nullptr, B.edge_cnt,
+                                             B.edges, B.edge_cap);
+  // trajectories
+  uf_init_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap);
+  const int ge = grid_for(B.edge_cap, 256, 4096);
+  uf_hook_kernel<<<ge, 256, 0, st>>>(B.parent, B.edges, B.n_edges, B.edge_cap, B.err);
+  uf_label_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap, B.track, B.n_roots);
+  *launches += 6;  // edge count, scan, edge write, uf init, hook, label
+  return cudaGetLastError();
+}
+
+}  // namespace ftk2b

@@ -1,0 +1,49 @@
+// Device buffers and launchers of the post-extraction stages.
+#pragma once
+
+#include "cp_internal.h"
+
+namespace ftk2b {
+
+struct PostBuffers {
+  unsigned cap;                     // feature capacity
+  unsigned edge_cap;
+  int key_bits;                     // significant bits of the canonical keys
+  int sort_grid;
+  // extraction output (unsorted)
+  unsigned long long* key;
+  double* lam;                      // 4 per feature
+  float* bary4;                     // 4 per feature: (float) of the exact-path lambda
+  float* scalar;
+  unsigned* count;                  // device count of features
+  // sort scratch
+  unsigned long long* key_alt;
+  unsigned* perm0;
+  unsigned* perm1;
+  unsigned* hist;                   // 256 * sort_grid
+  // canonical-order outputs
+  double* lam_sorted;
+  float* bary4_sorted;
+  float* scalar_sorted;
+  unsigned long long* simplices;    // (m+1) per feature
+  float* bary;                      // (m+1) per feature
+  unsigned long long* track;
+  unsigned* edge_cnt;               // per feature, scanned in place into offsets
+  unsigned* edges;                  // 2 per edge
+  unsigned* n_edges;
+  unsigned* parent;
+  unsigned* n_roots;
+  unsigned* err;
+  unsigned* cls;                    // per feature classification (FTK2B_CLASS_*)
+};
+
+void upload_post_tables();
+cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuffers& B,
+                                int want_edges, cudaStream_t st, unsigned long long* launches);
+cudaError_t launch_classify_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa, int nch,
+                                    const PostBuffers& B, cudaStream_t st);
+bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, unsigned* v1,
+                const unsigned* n_ptr, unsigned cap, int bits, unsigned* hist, int grid,
+                cudaStream_t st, unsigned long long* launches);
+
+}  // namespace ftk2b

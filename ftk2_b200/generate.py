@@ -1,0 +1,69 @@
+"""Device-side synthetic fields for full-size runs (bench, large tests).
+
+Same definitions as ftk2_b200.synthetic (blob parameters drawn from the same
+seeded numpy generator), evaluated on the GPU with torch so that 10^8-vertex
+fields take milliseconds instead of minutes.  Values agree with the numpy
+version to rounding; tests that compare against the oracle copy the device
+field back to the host, so both sides always read identical bytes.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .synthetic import gaussian_blobs
+
+
+def gaussian_field_device(dims, nt: int, seed: int = 1234, n_blobs: int = 32, dtype=None,
+                          noise: float = 0.0, noise_seed: int | None = None, sigma=(4.0, 12.0),
+                          drift: float = 0.5, scale: float = 1.0, device: str = "cuda"):
+    """Analytic gradient of a drifting Gaussian sum, shape (nt, [nz,] ny, nx, ndim),
+    multiplied by ``scale`` (e.g. the box side for gradients per box length),
+    plus ``noise`` * N(0,1)."""
+    import torch
+    dtype = dtype or torch.float64
+    ndim = len(dims)
+    blobs = gaussian_blobs(seed, n_blobs, dims, sigma, drift)
+    axes = [torch.arange(n, dtype=torch.float64, device=device) for n in dims]
+    shape = tuple(dims[::-1])
+    out = torch.empty((nt,) + shape + (ndim,), dtype=dtype, device=device)
+    gen = None
+    if noise:
+        gen = torch.Generator(device=device)
+        gen.manual_seed(int(seed + 1 if noise_seed is None else noise_seed))
+    for k in range(nt):
+        acc = torch.zeros(shape + (ndim,), dtype=torch.float64, device=device)
+        for b in range(n_blobs):
+            c = blobs["centers"][b] + blobs["vel"][b] * k
+            s2 = float(blobs["sigma"][b]) ** 2
+            d = []
+            for i in range(ndim):
+                view = [1] * ndim
+                view[ndim - 1 - i] = dims[i]
+                d.append((axes[i] - float(c[i])).view(view))
+            r2 = d[0] * d[0]
+            for i in range(1, ndim):
+                r2 = r2 + d[i] * d[i]
+            e = float(blobs["amps"][b]) * torch.exp(-r2 / (2.0 * s2)) / s2
+            for i in range(ndim):
+                acc[..., i] -= (e * d[i]).expand(shape)
+        if scale != 1.0:
+            acc *= scale
+        if noise:
+            acc += noise * torch.randn(acc.shape, dtype=torch.float64, device=device, generator=gen)
+        out[k] = acc.to(dtype)
+    return out
+
+
+def c2_field(device: str = "cuda"):
+    """3D flow critical points, plain drop-in: 128^3 x 16, 32 blobs, float64."""
+    import torch
+    return gaussian_field_device((128, 128, 128), 16, seed=1234, n_blobs=32, dtype=torch.float64,
+                                 device=device)
+
+
+def c4_field(device: str = "cuda"):
+    """Precision workload: 256^3 x 8 float32, 64 blobs of width U[16,48] voxels,
+    gradient per box length (x256) plus 1e-3 N(0,1) noise."""
+    import torch
+    return gaussian_field_device((256, 256, 256), 8, seed=4321, n_blobs=64, dtype=torch.float32,
+                                 noise=1e-3, sigma=(16.0, 48.0), scale=256.0, device=device)

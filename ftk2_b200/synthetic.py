@@ -56,15 +56,20 @@ def gaussian_blobs(seed: int, n_blobs: int, box, sigma=(4.0, 12.0), drift=0.5):
 
 def gaussian_sum_gradient(dims, nt: int, seed: int = 1234, n_blobs: int = 32,
                           dtype=np.float64, noise: float = 0.0, noise_seed: int | None = None,
-                          sigma=(4.0, 12.0), drift=0.5) -> np.ndarray:
+                          sigma=(4.0, 12.0), drift=0.5, box=None, origin=None,
+                          t0: int = 0) -> np.ndarray:
     """Analytic gradient of a drifting Gaussian sum on a regular grid.
 
-    dims: spatial dims (nx, ny) or (nx, ny, nz).  Returns array of shape
+    dims: spatial dims (nx, ny) or (nx, ny, nz) of the evaluated region.
+    Blob centres are drawn over ``box`` (default ``dims``); ``origin`` and
+    ``t0`` place the evaluated region inside a larger field, so a corner of a
+    big field can be generated alone.  Returns array of shape
     (nt, [nz,] ny, nx, ncomp) in ``dtype``; computed in float64 and rounded.
     """
     ndim = len(dims)
-    blobs = gaussian_blobs(seed, n_blobs, dims, sigma, drift)
-    axes = [np.arange(n, dtype=np.float64) for n in dims]
+    blobs = gaussian_blobs(seed, n_blobs, box if box is not None else dims, sigma, drift)
+    origin = origin if origin is not None else [0] * ndim
+    axes = [origin[i] + np.arange(n, dtype=np.float64) for i, n in enumerate(dims)]
     # grids in (.., y, x) order
     grids = np.meshgrid(*axes[::-1], indexing="ij")[::-1]  # grids[k] is coord k, shape rev(dims)
     shape = tuple(dims[::-1])
@@ -72,7 +77,7 @@ def gaussian_sum_gradient(dims, nt: int, seed: int = 1234, n_blobs: int = 32,
     for k in range(nt):
         acc = [np.zeros(shape) for _ in range(ndim)]
         for b in range(n_blobs):
-            c = blobs["centers"][b] + blobs["vel"][b] * k
+            c = blobs["centers"][b] + blobs["vel"][b] * (k + t0)
             s2 = blobs["sigma"][b] ** 2
             d = [grids[i] - c[i] for i in range(ndim)]
             r2 = sum(di * di for di in d)

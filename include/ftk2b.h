@@ -1,0 +1,177 @@
+/*
+ * ftk2b.h - C ABI of the B200-native critical-point tracking path.
+ *
+ * Drop-in replacement for the reference's
+ *   SimplicialEngine<T, CriticalPointPredicate<M,T>>::execute() / execute_cuda()
+ *   followed by get_complex()
+ * (include/ftk2/core/engine.hpp:96-99, 273-282, 822-996), callable from any
+ * language through plain pointers and sizes.  Every function returns a status
+ * code; nothing throws or exits across this boundary, and there is no CPU
+ * fallback: without a usable CUDA device the calls fail with FTK2B_NO_DEVICE.
+ *
+ * Results follow the reference's FeatureComplex (complex.hpp:14-58):
+ * features in Simplex order (sorted vertex ids), float barycentrics as
+ * FeatureElement stores them (feature.hpp:26), track_id = canonical id of the
+ * smallest feature of the trajectory, type = 0 (predicate.hpp:80), and the
+ * sorted, de-duplicated edge list of the trajectories.
+ *
+ * Threading: a context is used by one host thread at a time; create one
+ * context per thread for concurrency.  All device work of a context runs on
+ * its own CUDA stream.
+ */
+#ifndef FTK2B_H
+#define FTK2B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FTK2B_OK = 0,
+  FTK2B_INVALID_ARG = 1,     /* malformed descriptor (the reference throws or reads out of bounds) */
+  FTK2B_OOM = 2,             /* device allocation failed */
+  FTK2B_CUDA_ERROR = 3,      /* a CUDA call failed (the reference calls exit(), engine.hpp:29-37) */
+  FTK2B_TIMEOUT = 4,         /* a bounded device-side wait gave up */
+  FTK2B_OVERFLOW_RETRY = 5,  /* an output buffer overflowed and retries were exhausted */
+  FTK2B_NO_DEVICE = 6,       /* no usable CUDA device: there is no CPU fallback */
+  FTK2B_UNSUPPORTED = 7,     /* a combination the path does not implement */
+  FTK2B_BUSY = 8             /* the serving queue is full */
+} ftk2b_status;
+
+enum { FTK2B_MESH_REGULAR = 0, FTK2B_MESH_EXTRUDED = 1 };
+enum { FTK2B_F32 = 0, FTK2B_F64 = 1 };
+enum {
+  FTK2B_LAYOUT_MULTICOMPONENT = 0, /* one [M, d0, d1, ...] array, component fastest (engine.hpp:1101-1124) */
+  FTK2B_LAYOUT_SEPARATE = 1,       /* M arrays [d0, d1, ...] indexed by global - offset (engine.hpp:999-1009) */
+  FTK2B_LAYOUT_PER_VERTEX = 2      /* M 1-D arrays indexed by vertex id (engine.hpp:1000) */
+};
+enum { FTK2B_HOST = 0, FTK2B_DEVICE = 1 };
+enum {
+  FTK2B_PRECISION_EXACT = 0,   /* solve in the field precision, operation for operation (zero_crossing.hpp:20-90) */
+  FTK2B_PRECISION_REFINED = 1  /* same accepted set; reported lambda = FP32 solve + one FP64 refinement step */
+};
+enum {
+  FTK2B_CLASS_NONE = 0,        /* classification not requested */
+  FTK2B_CLASS_DEGENERATE = 1,
+  FTK2B_CLASS_SOURCE = 2,      /* gradient fields: minimum */
+  FTK2B_CLASS_SINK = 3,        /* gradient fields: maximum */
+  FTK2B_CLASS_SADDLE = 4,
+  FTK2B_CLASS_SPIRAL_SOURCE = 5,
+  FTK2B_CLASS_SPIRAL_SINK = 6,
+  FTK2B_CLASS_CENTER = 7
+};
+
+typedef struct ftk2b_ctx ftk2b_ctx;
+
+/* Spacetime mesh.
+ * REGULAR  = RegularSimplicialMesh(local_dims, offset, global_dims)
+ *            (mesh.hpp:256-265); ndims counts time (3 = 2D+t, 4 = 3D+t).
+ * EXTRUDED = ExtrudedSimplicialMesh(UnstructuredSimplicialMesh(cells), n_layers)
+ *            (mesh.hpp:542-562, unstructured_mesh.hpp:16-76): base cells are
+ *            triangles (base_cell_dim 2) or tets (3) over n_base_verts vertices. */
+typedef struct {
+  int kind;
+  int ndims;
+  uint64_t local_dims[4];
+  uint64_t offset[4];
+  uint64_t global_dims[4];
+  uint64_t n_base_verts;
+  const uint64_t* base_cells;  /* host memory, (base_cell_dim + 1) ids per cell */
+  uint64_t n_base_cells;
+  int base_cell_dim;
+  uint64_t n_layers;
+} ftk2b_mesh_desc;
+
+/* Vector field (CriticalPointPredicate<M,T>, predicate.hpp:49-64).
+ * MULTICOMPONENT: comp[0] = [M, d0, d1, ...] with nd = number of mesh dims.
+ * SEPARATE:       comp[0..M-1] = [d0, d1, ...]; nd == 1 means per-vertex.
+ * PER_VERTEX:     comp[0..M-1] of length dims[0].
+ * scalar: optional scalar field, interpolated at features only for SEPARATE
+ * layouts, as the reference does (predicate.hpp:81-92). */
+typedef struct {
+  int dtype;
+  int ncomp;
+  int layout;
+  int location;       /* FTK2B_HOST or FTK2B_DEVICE (for every pointer below) */
+  const void* comp[3];
+  int nd;
+  uint64_t dims[4];   /* Fortran order, first fastest, excluding the component dim */
+  const void* scalar;
+  int scalar_nd;
+  uint64_t scalar_dims[4];
+} ftk2b_field_desc;
+
+typedef struct {
+  double sos_q;       /* Predicate::sos_q, default 1e6 (predicate.hpp:25) */
+  int precision;      /* FTK2B_PRECISION_* */
+  int want_edges;     /* 1 (default): connectivity and track ids */
+  int classify;       /* 1: fill cp_class from the Jacobian of the coface top cell */
+} ftk2b_cp_params;
+
+/* Result of one extraction; owned by the library until ftk2b_cp_result_free. */
+typedef struct {
+  int m;                  /* feature simplices have m+1 vertices */
+  uint64_t n_features;
+  uint64_t* simplices;    /* n*(m+1) sorted vertex ids */
+  double* lambda;         /* n*(m+1) barycentrics (exact: field precision widened) */
+  float* barycentric;     /* n*(m+1) as FeatureElement::barycentric_coords[0] */
+  uint64_t* track_id;     /* n */
+  uint32_t* type;         /* n, always 0 like the reference */
+  uint32_t* cp_class;     /* n, FTK2B_CLASS_* */
+  float* scalar;          /* n */
+  uint64_t n_edges;
+  uint32_t* edges;        /* 2*n_edges, (lo, hi) indices into the features */
+  uint64_t n_tracks;
+  uint64_t n_simplices;   /* m-simplices of the mesh: the unit of work */
+  double device_ms;       /* device time of the extraction pipeline */
+} ftk2b_cp_result;
+
+/* --- context (replaces the engine object; engine.hpp:84-85) --------------- */
+ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out);
+void ftk2b_ctx_destroy(ftk2b_ctx* ctx);
+const char* ftk2b_last_error(const ftk2b_ctx* ctx);
+void* ftk2b_ctx_stream(ftk2b_ctx* ctx); /* the context's cudaStream_t */
+
+ftk2b_cp_params ftk2b_cp_params_default(void);
+
+/* Tuning knobs of a context (no reference counterpart: the reference sizes
+ * its buffers with fixed guesses, engine.hpp:351-385). */
+enum {
+  FTK2B_OPT_FEATURE_CAPACITY = 1, /* initial feature capacity; grows on overflow */
+  FTK2B_OPT_TIME_CHUNK = 2        /* time steps per extraction block (0 = all) */
+};
+ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
+
+/* m-simplices a mesh holds for codimension m (2 or 3): the unit of work. */
+uint64_t ftk2b_mesh_simplex_count(const ftk2b_mesh_desc* mesh, int m);
+
+/* --- one-shot extraction: execute() + get_complex() ----------------------- */
+/* Replaces SimplicialEngine::execute / execute_cuda (engine.hpp:96-99,
+ * 273-282) plus get_complex (engine.hpp:822-996). */
+ftk2b_status ftk2b_cp_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
+                              const ftk2b_field_desc* field, const ftk2b_cp_params* params,
+                              ftk2b_cp_result** out);
+void ftk2b_cp_result_free(ftk2b_cp_result* r);
+
+/* Two-step form of ftk2b_cp_extract: run leaves the results in the context's
+ * device buffers (valid until the next call on the context); fetch copies
+ * them to a host result.  Used to time the device pipeline alone. */
+ftk2b_status ftk2b_cp_run(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
+                          const ftk2b_field_desc* field, const ftk2b_cp_params* params,
+                          uint64_t* n_features, uint64_t* n_edges);
+ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out);
+
+/* Device timing of the last run on the context's stream (CUDA events):
+ * the fused extraction kernel alone and the whole pipeline, in ms, and the
+ * number of kernels the context has launched so far. */
+ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* total_ms,
+                                   uint64_t* kernels_launched);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FTK2B_H */

@@ -914,3 +914,56 @@ void cporacle_free(orc_result* r) {
   free(r->edges);
   memset(r, 0, sizeof(*r));
 }
+
+/* ------------------------------------------------------------------------ */
+/* Primitive entry points, checked against the reference's unit-test vectors */
+
+/* sos::sign (sos.hpp:12-20) */
+int cporacle_sos_sign(double v, uint64_t index, double Q) {
+  i128 q = quant(v, Q);
+  if (q > 0) return 1;
+  if (q < 0) return -1;
+  return (index % 2 == 0) ? 1 : -1;
+}
+
+int cporacle_det2(const double* v0, const double* v1, uint64_t i0, uint64_t i1, double Q) {
+  return sos_det2(v0, v1, i0, i1, Q);
+}
+
+int cporacle_det3(const double* v0, const double* v1, const double* v2, double Q) {
+  return sos_det3(v0, v1, v2, Q);
+}
+
+/* origin_inside<M> on (M+1) x M values, row-major */
+int cporacle_inside(int M, const double* vals, const uint64_t* idx, double Q) {
+  double v[4][3];
+  for (int i = 0; i <= M; ++i)
+    for (int j = 0; j < M; ++j) v[i][j] = vals[i * M + j];
+  return sos_inside(M, v, idx, Q);
+}
+
+/* ZeroCrossingSolver<K,T>::solve for K = 2, 3 in double (f64 != 0) or float */
+int cporacle_solve(int K, int f64, const double* vals, double* lam) {
+  if (f64) {
+    double v[4][3], l[4];
+    for (int i = 0; i <= K; ++i)
+      for (int j = 0; j < K; ++j) v[i][j] = vals[i * K + j];
+    int ok = solve_f64(K, v, l);
+    for (int i = 0; i <= K; ++i) lam[i] = l[i];
+    return ok;
+  }
+  float v[4][3], l[4];
+  for (int i = 0; i <= K; ++i)
+    for (int j = 0; j < K; ++j) v[i][j] = (float)vals[i * K + j];
+  int ok = solve_f32(K, v, l);
+  for (int i = 0; i <= K; ++i) lam[i] = l[i];
+  return ok;
+}
+
+/* number of m-simplex types per d-hypercube (cpu_get_num_simplex_types) */
+int cporacle_chain_count(int d, int m) {
+  chains_t c;
+  if (d < 1 || d > 4 || m < 1 || m > d) return 0;
+  build_chains(&c, d, m);
+  return c.n;
+}

@@ -1,0 +1,214 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the oracle.
+
+* every golden case: identical to the reference engine's own output
+  (simplex ids, float barycentrics, lambdas, track ids, edges, scalars);
+* seeded medium cases: identical to the exact C restatement;
+* full-size configuration: size-independent invariants of the result plus
+  windows of it against the restatement;
+* host and device inputs give the same bytes; repeated runs are identical;
+* buffer overflow is recovered by the retry path.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from ftk2_b200 import api
+from ftk2_b200 import synthetic as S
+from oracle import bridge
+import cases
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def gpu_run(ctx, case, **kw):
+    keep: list = []
+    mesh, fld = cases.gpu_inputs(case, keep)
+    return ctx.extract(mesh, fld, api.params(case.sos_q, **kw))
+
+
+def oracle_run(case):
+    keep: list = []
+    mesh, fld = cases.oracle_inputs(case, keep)
+    return bridge.run_restatement(mesh, fld)
+
+
+def assert_identical(g, o, lam=True):
+    assert g.simplices.shape == o.simplices.shape, (g.simplices.shape, o.simplices.shape)
+    assert np.array_equal(g.simplices, o.simplices)
+    assert np.array_equal(g.track_id, o.track_id)
+    assert np.array_equal(g.edges, o.edges)
+    assert np.array_equal(g.bary, o.bary)
+    assert np.array_equal(g.scalar, o.scalar)
+    assert np.array_equal(g.type, o.type)
+    if lam:
+        assert np.array_equal(g.lam, o.lam)
+
+
+REGULAR_GOLDEN = [n for n in sorted(cases.GOLDEN_CASES) if not n.startswith("extruded")]
+EXTRUDED_GOLDEN = [n for n in sorted(cases.GOLDEN_CASES) if n.startswith("extruded")]
+
+
+@pytest.mark.parametrize("name", REGULAR_GOLDEN)
+def test_golden_regular(ctx, name):
+    case = cases.GOLDEN_CASES[name]()
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    assert str(z["input_sha256"]) == case.input_digest()
+    g = gpu_run(ctx, case)
+    ref = bridge.CPResult(simplices=z["simplices"], bary=z["bary"], lam=z["lam"],
+                          track_id=z["track_id"], type=z["type"], scalar=z["scalar"],
+                          edges=z["edges"])
+    assert_identical(g, ref)
+    assert g.n_tracks == len(np.unique(ref.track_id))
+
+
+def _medium_cases():
+    out = []
+    for seed in (1, 2):
+        g = S.gaussian_sum_gradient((48, 40, 36), 6, seed=seed, n_blobs=24)
+        out.append(cases.Case(f"g3d_f64_s{seed}", "regular", 3, cases.MULTI, g, 2.0 ** 20,
+                              [48, 40, 36, 6]))
+    g = S.gaussian_sum_gradient((40, 36, 32), 5, seed=7, n_blobs=24, dtype=np.float32, noise=1e-3,
+                                sigma=(3, 8))
+    out.append(cases.Case("g3d_f32_noise", "regular", 3, cases.MULTI, g, 2.0 ** 20, [40, 36, 32, 5]))
+    g = S.gaussian_sum_gradient((200, 150), 12, seed=3, n_blobs=40, sigma=(3, 9))
+    out.append(cases.Case("g2d_f64", "regular", 2, cases.MULTI, g, 1e6, [200, 150, 12]))
+    g = S.gaussian_sum_gradient((130, 97), 9, seed=4, n_blobs=30, dtype=np.float32, sigma=(2, 6))
+    U, V = np.ascontiguousarray(g[..., 0]), np.ascontiguousarray(g[..., 1])
+    sc = np.random.default_rng(5).standard_normal(U.shape).astype(np.float32)
+    out.append(cases.Case("g2d_f32_sep_offset", "regular", 2, cases.SEPARATE, [U, V], 1e6,
+                          [120, 90, 8], [5, 4, 1], [130, 97, 9], scalar=sc))
+    g = S.gaussian_sum_gradient((34, 33, 35), 5, seed=11, n_blobs=20)
+    comps = [np.ascontiguousarray(g[..., j]) for j in range(3)]
+    out.append(cases.Case("g3d_sep_offset", "regular", 3, cases.SEPARATE, comps, 2.0 ** 20,
+                          [30, 29, 31, 4], [2, 3, 1, 1], [34, 33, 35, 5]))
+    return out
+
+
+@pytest.mark.parametrize("case", _medium_cases(), ids=lambda c: c.name)
+def test_medium_vs_restatement(ctx, case):
+    g = gpu_run(ctx, case)
+    o = oracle_run(case)
+    assert len(o.track_id) > 0
+    assert_identical(g, o)
+    assert g.n_simplices == o.n_tested
+
+
+def test_device_input_matches_host_input(ctx):
+    torch = pytest.importorskip("torch")
+    g = S.gaussian_sum_gradient((40, 40, 40), 5, seed=13, n_blobs=24)
+    keep: list = []
+    mesh = api.regular_mesh_desc([40, 40, 40, 5])
+    host = ctx.extract(mesh, api.field_desc(g, api.LAYOUT_MULTICOMPONENT, 3, keep=keep),
+                       api.params(2.0 ** 20))
+    dev = torch.from_numpy(g).cuda()
+    devr = ctx.extract(mesh, api.field_desc(dev, api.LAYOUT_MULTICOMPONENT, 3, keep=keep),
+                       api.params(2.0 ** 20))
+    assert_identical(host, devr)
+    again = ctx.extract(mesh, api.field_desc(dev, api.LAYOUT_MULTICOMPONENT, 3, keep=keep),
+                        api.params(2.0 ** 20))
+    assert_identical(devr, again)
+
+
+def test_overflow_retry(ctx):
+    case = cases.c1_analytic_2d()
+    ctx.set_option(api.OPT_FEATURE_CAPACITY, 100)  # far below the 3697 features
+    try:
+        g = gpu_run(ctx, case)
+    finally:
+        ctx.set_option(api.OPT_FEATURE_CAPACITY, 0)
+    z = np.load(os.path.join(GOLDEN, "c1_analytic_2d.npz"))
+    assert np.array_equal(g.simplices, z["simplices"])
+    assert np.array_equal(g.edges, z["edges"])
+
+
+@pytest.mark.parametrize("tchunk", [1, 3])
+def test_time_chunking_is_invisible(ctx, tchunk):
+    case = cases.GOLDEN_CASES["gauss3d_16"]()
+    base = gpu_run(ctx, case)
+    ctx.set_option(api.OPT_TIME_CHUNK, tchunk)
+    try:
+        g = gpu_run(ctx, case)
+    finally:
+        ctx.set_option(api.OPT_TIME_CHUNK, 0)
+    assert_identical(base, g)
+
+
+def check_invariants(r):
+    n = len(r.track_id)
+    # canonical order: strictly increasing tuples (Simplex::operator<)
+    s = r.simplices
+    if n > 1:
+        a, b = s[:-1], s[1:]
+        diff = a != b
+        first = diff.argmax(axis=1)
+        rows = np.arange(n - 1)
+        assert diff.any(axis=1).all()
+        assert (a[rows, first] < b[rows, first]).all()
+    assert (np.diff(s, axis=1) > 0).all()              # sorted vertex ids
+    # track ids: root of the component = smallest member, idempotent
+    t = r.track_id.astype(np.int64)
+    assert (t <= np.arange(n)).all()
+    assert (t[t] == t).all()
+    # edges: sorted, unique, lo < hi, endpoints in one track
+    e = r.edges.astype(np.int64)
+    if len(e):
+        assert (e[:, 0] < e[:, 1]).all()
+        key = e[:, 0] * (n + 1) + e[:, 1]
+        assert (np.diff(key) > 0).all()
+        assert (t[e[:, 0]] == t[e[:, 1]]).all()
+    # barycentrics in range and summing to one
+    assert (r.lam >= -1e-9).all() and (r.lam <= 1 + 1e-9).all()
+    np.testing.assert_allclose(r.lam.sum(axis=1), 1.0, atol=1e-12)
+
+
+def test_full_size_3d_config_invariants_and_windows(ctx):
+    """128^3 x 16 float64 Gaussian-sum gradient (the 3D plain drop-in
+    configuration): invariants at full size, and sub-box meshes of the same
+    field identical to the restatement."""
+    torch = pytest.importorskip("torch")
+    from ftk2_b200 import generate
+    dev = generate.gaussian_field_device((128, 128, 128), 16, seed=1234, n_blobs=32,
+                                         dtype=torch.float64)
+    keep: list = []
+    mesh = api.regular_mesh_desc([128, 128, 128, 16])
+    r = ctx.extract(mesh, api.field_desc(dev, api.LAYOUT_MULTICOMPONENT, 3, keep=keep),
+                    api.params(2.0 ** 20))
+    assert len(r.track_id) > 100
+    check_invariants(r)
+    host = dev.cpu().numpy()
+    rng = np.random.default_rng(0)
+    for _ in range(2):
+        lo = [int(rng.integers(0, 128 - 40)) for _ in range(3)] + [int(rng.integers(0, 8))]
+        local = [40, 40, 40, 8]
+        case = cases.Case("win", "regular", 3, cases.MULTI, host, 2.0 ** 20, local, lo,
+                          [128, 128, 128, 16])
+        g = gpu_run(ctx, case)
+        o = oracle_run(case)
+        assert_identical(g, o)
+
+
+def test_refined_precision_same_set_smaller_error(ctx):
+    g32 = S.gaussian_sum_gradient((40, 36, 32), 5, seed=7, n_blobs=24, dtype=np.float32, noise=1e-3,
+                                  sigma=(3, 8))
+    case = cases.Case("p", "regular", 3, cases.MULTI, g32, 2.0 ** 20, [40, 36, 32, 5])
+    exact = gpu_run(ctx, case)
+    refined = gpu_run(ctx, case, precision=api.PRECISION_REFINED)
+    # the accepted set, tracks and stored float barycentrics are unchanged
+    assert np.array_equal(exact.simplices, refined.simplices)
+    assert np.array_equal(exact.track_id, refined.track_id)
+    assert np.array_equal(exact.bary, refined.bary)
+    # position error against an FP64 solve of the promoted values
+    case64 = cases.Case("p64", "regular", 3, cases.MULTI, g32.astype(np.float64), 2.0 ** 20,
+                        [40, 36, 32, 5])
+    o64 = oracle_run(case64)
+    idx = {tuple(s): i for i, s in enumerate(o64.simplices.tolist())}
+    common = [(i, idx[tuple(s)]) for i, s in enumerate(refined.simplices.tolist()) if tuple(s) in idx]
+    assert len(common) > 0.9 * len(refined.simplices)
+    a = np.array([refined.lam[i] for i, _ in common])
+    b = np.array([o64.lam[j] for _, j in common])
+    c = np.array([exact.lam[i] for i, _ in common])
+    err_ref = np.abs(a - b).max()
+    err_f32 = np.abs(c - b).max()
+    assert err_ref <= 1e-9 or err_ref < 1e-3 * err_f32, (err_ref, err_f32)
