@@ -36,7 +36,8 @@ F32, F64 = 0, 1
 LAYOUT_MULTICOMPONENT, LAYOUT_SEPARATE, LAYOUT_PER_VERTEX = 0, 1, 2
 HOST, DEVICE = 0, 1
 PRECISION_EXACT, PRECISION_REFINED = 0, 1
-OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK = 1, 2
+OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA = 1, 2, 3
+INFO_LAST_TMA = 100
 CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
                "center"]
 
@@ -90,6 +91,7 @@ SIGNATURES = {
     "ftk2b_ctx_stream": (C.c_void_p, [C.c_void_p]),
     "ftk2b_cp_params_default": (CPParams, []),
     "ftk2b_ctx_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
+    "ftk2b_ctx_get_option": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "ftk2b_mesh_simplex_count": (C.c_uint64, [C.POINTER(MeshDesc), C.c_int]),
     "ftk2b_cp_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                    C.POINTER(CPParams), C.POINTER(C.POINTER(CPResultC))]),
@@ -288,6 +290,11 @@ class Context:
 
     def set_option(self, option: int, value: int):
         self._check(self.lib.ftk2b_ctx_set_option(self.h, int(option), int(value)))
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int64()
+        self._check(self.lib.ftk2b_ctx_get_option(self.h, int(option), C.byref(v)))
+        return int(v.value)
 
     def last_error(self) -> str:
         return (self.lib.ftk2b_last_error(self.h) or b"").decode()

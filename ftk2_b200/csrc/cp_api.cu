@@ -82,7 +82,7 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
   ctx->device = device;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
-      cudaEventCreate(&ctx->ev_x) != cudaSuccess) {
+      cudaEventCreate(&ctx->ev_x) != cudaSuccess || cudaEventCreate(&ctx->ev_r) != cudaSuccess) {
     delete ctx;
     return FTK2B_CUDA_ERROR;
   }
@@ -121,6 +121,7 @@ extern "C" void ftk2b_ctx_destroy(ftk2b_ctx* ctx) {
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaEventDestroy(ctx->ev_x);
+  cudaEventDestroy(ctx->ev_r);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -151,8 +152,22 @@ extern "C" ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t
       if (value < 0 || value > (1 << 30)) return fail(ctx, FTK2B_INVALID_ARG, "time chunk out of range");
       ctx->tune_tchunk = (int)value;
       return FTK2B_OK;
+    case FTK2B_OPT_DISABLE_TMA:
+      ctx->disable_tma = value != 0;
+      return FTK2B_OK;
     default:
       return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
+  }
+}
+
+extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t* value) {
+  if (!ctx || !value) return FTK2B_INVALID_ARG;
+  switch (option) {
+    case FTK2B_OPT_FEATURE_CAPACITY: *value = ctx->cap_hint; return FTK2B_OK;
+    case FTK2B_OPT_TIME_CHUNK: *value = ctx->tune_tchunk; return FTK2B_OK;
+    case FTK2B_OPT_DISABLE_TMA: *value = ctx->disable_tma ? 1 : 0; return FTK2B_OK;
+    case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
+    default: return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
 }
 
@@ -164,7 +179,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   std::vector<DevBuf*> v = {&stage[0], &stage[1], &stage[2], &stage_scalar, &key, &lam, &bary4,
                             &scalar, &key_alt, &perm0, &perm1, &hist, &lam_s, &bary4_s, &scalar_s,
                             &simplices, &bary, &track, &edge_cnt, &edges, &parent, &counters,
-                            &cls};
+                            &cls, &cand_corner, &cand_chains};
   for (auto& b : extra) v.push_back(&b);
   return v;
 }
@@ -266,6 +281,7 @@ ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int
         return fail(ctx, FTK2B_INVALID_ARG, "field dim %d (%llu) smaller than offset+local (%llu)", k,
                     (unsigned long long)f->dims[k], (unsigned long long)need_global_hi[k]);
     nelem = prod(f->dims, f->nd) * (uint64_t)M;
+    for (int k = 0; k < mesh_d; ++k) fa.adims[k] = (long long)f->dims[k];
     long long s = M;
     for (int k = 0; k < mesh_d; ++k) {
       fa.estride[k] = s;
@@ -277,6 +293,7 @@ ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int
                   (unsigned long long)f->dims[0], (unsigned long long)n_vertices);
     nelem = f->dims[0];
     fa.per_vertex = 1;
+    fa.adims[0] = (long long)f->dims[0];
   } else if (f->layout == FTK2B_LAYOUT_SEPARATE) {
     if (f->nd != mesh_d) return fail(ctx, FTK2B_INVALID_ARG, "separate arrays need nd == mesh dims");
     for (int k = 0; k < mesh_d; ++k)
@@ -284,6 +301,7 @@ ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int
         return fail(ctx, FTK2B_INVALID_ARG, "array dim %d (%llu) smaller than local dim (%llu)", k,
                     (unsigned long long)f->dims[k], (unsigned long long)need_local_hi[k]);
     nelem = prod(f->dims, f->nd);
+    for (int k = 0; k < mesh_d; ++k) fa.adims[k] = (long long)f->dims[k];
     long long s = 1;
     for (int k = 0; k < mesh_d; ++k) {
       fa.estride[k] = s;
@@ -365,7 +383,7 @@ ftk2b_status ftk2b::ensure_feature_buffers(ftk2b_ctx* ctx, unsigned cap, unsigne
   CUDA_TRY(ctx, ctx->cls.ensure(sizeof(unsigned) * cap));
   CUDA_TRY(ctx, ctx->edges.ensure(sizeof(unsigned) * 2 * (size_t)edge_cap));
   CUDA_TRY(ctx, ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
-  const int grid = ctx->sort_grid();
+  const int grid = ctx->sort_grid(cap);
   CUDA_TRY(ctx, ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)grid));
   return FTK2B_OK;
 }
@@ -376,7 +394,7 @@ PostBuffers ftk2b_ctx::post_buffers(unsigned cap_, unsigned edge_cap_, int key_b
   B.cap = cap_;
   B.edge_cap = edge_cap_;
   B.key_bits = key_bits;
-  B.sort_grid = sort_grid();
+  B.sort_grid = sort_grid(cap_);
   B.key = (unsigned long long*)key.p;
   B.lam = (double*)lam.p;
   B.bary4 = (float*)bary4.p;
@@ -417,7 +435,8 @@ static ftk2b_status build_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, R
       return fail(ctx, FTK2B_INVALID_ARG, "mesh dim %d is zero", k);
     if (mesh->offset[k] + mesh->local_dims[k] > mesh->global_dims[k])
       return fail(ctx, FTK2B_INVALID_ARG, "offset + local exceeds global along dim %d", k);
-    if (mesh->local_dims[k] > (1ull << 30)) return fail(ctx, FTK2B_INVALID_ARG, "mesh dim %d too large", k);
+    if (mesh->local_dims[k] >= (1ull << 16))
+      return fail(ctx, FTK2B_UNSUPPORTED, "local mesh dim %d exceeds 65535", k);
     rm.ld[k] = (long long)mesh->local_dims[k];
     rm.off[k] = (long long)mesh->offset[k];
     rm.gd[k] = (long long)mesh->global_dims[k];
@@ -456,23 +475,22 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   cfg.refined = prm->precision == FTK2B_PRECISION_REFINED;
   cfg.tchunk = (int)rm.ld[d - 1];
   if (ctx->tune_tchunk > 0) cfg.tchunk = ctx->tune_tchunk;
-  const int TX = 32, TY = (d == 4) ? 4 : 16, TZ = (d == 4) ? 4 : 1;
+  int TX, TY, TZ;
+  regular_tile(d, &TX, &TY, &TZ);
   cfg.tiles[0] = (int)((rm.ld[0] + TX - 1) / TX);
   cfg.tiles[1] = (int)((rm.ld[1] + TY - 1) / TY);
   cfg.tiles[2] = (d == 4) ? (int)((rm.ld[2] + TZ - 1) / TZ) : 1;
 
-  // feature capacity: grows on overflow and is remembered by the context
-  unsigned cap = ctx->cap_hint;
-  if (cap == 0) {
-    uint64_t guess = nsimp / 2048;
-    if (guess < 65536) guess = 65536;
-    if (guess > (1u << 28)) guess = 1u << 28;
-    cap = (unsigned)guess;
-  }
+  // feature capacity: starts small (sorting cost scales with it) and grows
+  // on overflow; the context remembers the grown value
+  unsigned cap = ctx->cap_hint ? ctx->cap_hint : 65536u;
+  unsigned ccap = ctx->cand_cap_hint ? ctx->cand_cap_hint : 65536u;
   for (int attempt = 0; attempt < 4; ++attempt) {
     const unsigned edge_cap = cap * 2;
     st = ensure_feature_buffers(ctx, cap, edge_cap, m);
     if (st) return st;
+    CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
+    CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream));
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
@@ -483,9 +501,18 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     sink.scalar = B.scalar;
     sink.count = B.count;
     sink.cap = cap;
-    CUDA_TRY(ctx, launch_extract_regular(field->dtype == FTK2B_F64, rm, fa, cfg, sink, ctx->stream));
+    CandidateQueue cq;
+    cq.corner = (unsigned long long*)ctx->cand_corner.p;
+    cq.chains = (unsigned long long*)ctx->cand_chains.p;
+    cq.count = (unsigned*)ctx->counters.p + kCountCand;
+    cq.cap = ccap;
+    CUDA_TRY(ctx, launch_extract_regular(field->dtype == FTK2B_F64, rm, fa, cfg, cq, B.err,
+                                         ctx->stream, !ctx->disable_tma, &ctx->last_used_tma));
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
-    ctx->launches += 1;
+    CUDA_TRY(ctx, launch_refine_regular(field->dtype == FTK2B_F64, rm, fa, cfg, cq, sink, ctx->num_sms,
+                                        ctx->stream));
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev_r, ctx->stream));
+    ctx->launches += 2;
     CUDA_TRY(ctx, launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, &ctx->launches));
     if (prm->classify) {
       CUDA_TRY(ctx, launch_classify_regular(field->dtype == FTK2B_F64, rm, fa, nch, B, ctx->stream));
@@ -495,11 +522,21 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     unsigned h[kNumCounters];
     CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->counters.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    float ms = 0.f, xms = 0.f;
+    float ms = 0.f, xms = 0.f, rms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     cudaEventElapsedTime(&xms, ctx->ev0, ctx->ev_x);
+    cudaEventElapsedTime(&rms, ctx->ev_x, ctx->ev_r);
     ctx->last_extract_ms = xms;
+    ctx->last_refine_ms = rms;
+    if (h[kCountErr] & 2u) return fail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return fail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
+    if (h[kCountCand] > ccap) {
+      const uint64_t want = (uint64_t)h[kCountCand] + h[kCountCand] / 4 + 1024;
+      if (want > 0xFFFFFFF0ull) return fail(ctx, FTK2B_OVERFLOW_RETRY, "candidate count exceeds 2^32");
+      ccap = (unsigned)want;
+      ctx->cand_cap_hint = ccap;
+      continue;
+    }
     if (h[kCountFeatures] > cap || h[kCountEdges] > edge_cap) {
       uint64_t want = (uint64_t)h[kCountFeatures] + h[kCountFeatures] / 4 + 1024;
       const uint64_t want_e = ((uint64_t)h[kCountEdges] + 1) / 2 + 1024;

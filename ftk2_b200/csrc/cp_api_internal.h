@@ -18,7 +18,7 @@ struct DevBuf {
   void release();
 };
 
-enum { kCountFeatures = 0, kCountEdges = 1, kCountRoots = 2, kCountErr = 3, kNumCounters = 8 };
+enum { kCountFeatures = 0, kCountEdges = 1, kCountRoots = 2, kCountErr = 3, kCountCand = 4, kNumCounters = 8 };
 
 struct LastRun {
   int kind = 0, m = 0;
@@ -36,16 +36,28 @@ struct ftk2b_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_x = nullptr;
   unsigned long long launches = 0;
   double last_extract_ms = 0;
+  double last_refine_ms = 0;
+  cudaEvent_t ev_r = nullptr;
   std::string err;
   unsigned cap_hint = 0;
+  unsigned cand_cap_hint = 0;
   int tune_tchunk = 0;
+  bool disable_tma = false;
+  int last_used_tma = 0;
   ftk2b::DevBuf stage[3], stage_scalar;
   ftk2b::DevBuf key, lam, bary4, scalar, key_alt, perm0, perm1, hist, lam_s, bary4_s, scalar_s,
-      simplices, bary, track, edge_cnt, edges, parent, counters, cls;
+      simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains;
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::LastRun last;
 
-  int sort_grid() const { return num_sms * 2; }
+  // blocks of the radix sort: enough to stream the feature capacity, few
+  // enough that the per-pass digit-histogram scan stays short
+  int sort_grid(unsigned cap) const {
+    int g = (int)(cap / 4096u);
+    if (g < 1) g = 1;
+    if (g > 2 * num_sms) g = 2 * num_sms;
+    return g;
+  }
   void release_all();
   std::vector<ftk2b::DevBuf*> all_bufs();
   ftk2b::PostBuffers post_buffers(unsigned cap, unsigned edge_cap, int key_bits);

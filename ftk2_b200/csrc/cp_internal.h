@@ -20,6 +20,7 @@ struct FieldAccess {
   const void* comp[3];
   long long estride[4];
   long long shift[4];
+  long long adims[4];          // array dims (Fortran, excluding the component dim)
   int per_vertex;
   // optional scalar (interpolated only for separate-array fields,
   // predicate.hpp:81-92 with the arrays the engine passes, engine.hpp:1125-1139)
@@ -50,6 +51,15 @@ struct FeatureSink {
   unsigned int cap;
 };
 
+// Hypercubes that survive the cull, with the chains (simplex types) whose
+// vertices also survive it; consumed by the exact-test kernel.
+struct CandidateQueue {
+  unsigned long long* corner;  // local corner coords, 16 bits each: x | y << 16 | z << 32 | t << 48
+  unsigned long long* chains;  // bit c: chain c still needs the exact test
+  unsigned* count;             // number queued (may exceed cap: overflow)
+  unsigned cap;
+};
+
 struct ExtractConfig {
   double Q;                    // sos_q
   int refined;                 // 1: report FP32 + one FP64 refinement step
@@ -66,8 +76,15 @@ struct ChainTable {
 
 void upload_chain_tables();
 
-cudaError_t launch_extract_regular(int dtype_f64, const RegularMesh& mesh, const FieldAccess& fa,
-                                   const ExtractConfig& cfg, const FeatureSink& sink,
-                                   cudaStream_t st);
+// Launches the fused extraction; uses TMA tensor-tile staging when allowed
+// and the array satisfies the 16-byte alignment rules (reported in used_tma).
+cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
+                                   const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
+                                   cudaStream_t st, bool allow_tma, int* used_tma);
+// Exact SoS + solve of the queued candidates, compacted into the sink.
+cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
+                                  const ExtractConfig& cfg, const CandidateQueue& cq,
+                                  const FeatureSink& sink, int num_sms, cudaStream_t st);
+void regular_tile(int d, int* tx, int* ty, int* tz);
 
 }  // namespace ftk2b

@@ -7,12 +7,21 @@
 // once, as (corner vertex, chain type), with the corner ranging over every
 // vertex so that the upper-boundary simplices phase 2 discovers are included.
 //
-// One thread block owns a spatial tile of corners and marches through time,
-// keeping one 64-bit cull word per vertex of the previous and current time
-// slice in shared memory.  A hypercube is rejected as a whole when the AND of
-// its vertices' words proves that every simplex in it fails the barycentric
-// solve (see vertex_word); only the rare surviving hypercubes are enumerated
-// simplex by simplex, with the exact integer SoS test and the bit-exact solve.
+// One thread block owns a spatial tile of corners (32 along x, one warp lane
+// each) and marches through time.  Each time slice of the tile (plus a
+// one-vertex halo) is brought into shared memory by one TMA tensor-tile copy
+// per array, double-buffered so the next slice streams in while the current
+// step is culled.  Every vertex gets a 64-bit cull word; a hypercube is
+// rejected when the AND of its vertices' words proves that no simplex in it
+// can pass the barycentric solve (see vertex_word).  Only the rare surviving
+// hypercubes are enumerated simplex by simplex with the exact integer SoS test
+// and the bit-exact solve, and accepted simplices are compacted by warp ballot.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
+#include <mutex>
+
 #include "cp_device.cuh"
 #include "cp_internal.h"
 
@@ -78,8 +87,7 @@ __device__ __forceinline__ unsigned long long vertex_word(const T v[M]) {
     w |= (unsigned long long)(v[j] < -thr) << (3 + j);
   }
   w |= (unsigned long long)(b < T(4e-13)) << 6;
-  const int e = exponent_of(b);
-  const int rel = e - kElo;
+  const int rel = exponent_of(b) - kElo;
   if (rel >= 0 && rel < kBands * CullParams<T>::band && b > T(0)) {
     const int n = rel / CullParams<T>::band;
     unsigned long long band = (7ull << n) >> 1;  // bits n-1, n, n+1
@@ -121,31 +129,110 @@ __device__ __forceinline__ T scalar_at(const FieldAccess& fa, const long long g[
 }
 
 // ---------------------------------------------------------------------------
+// TMA / mbarrier primitives (inline PTX)
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait for the phase of the given parity; false if it never completed.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  const unsigned a = smem_addr(bar);
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            int c3, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// ---------------------------------------------------------------------------
 
 template <int D> struct Tile;
 template <> struct Tile<4> {
-  static constexpr int TX = 32, TY = 4, TZ = 4;
+  // warp w owns corner row cy = w % 8 and corner z levels 2 (w / 8) .. +1
+  static constexpr int TX = 32, TY = 8, TZ = 4;
 };
 template <> struct Tile<3> {
-  static constexpr int TX = 32, TY = 16, TZ = 1;
+  // warp w owns corner rows cy = 2w, 2w + 1
+  static constexpr int TX = 32, TY = 32, TZ = 1;
 };
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRows = 2;  // corner rows a warp culls per step
+constexpr int kMaxVXBox = 36;
 
-template <typename T, int D>
-__global__ void __launch_bounds__(kThreads, 4)
-    extract_regular_kernel(RegularMesh mesh, FieldAccess fa, ExtractConfig cfg, FeatureSink sink) {
+// Shape of one time slice of a tile in shared memory, as the TMA box lays it
+// out: multicomponent [VZ][VY][VXBOX * M], separate arrays [M][VZ][VY][VXBOX].
+struct BoxShape {
+  int vxbox;       // x extent of the box (>= TX + 1, padded to 16-byte rows)
+  int multi;       // 1: interleaved components
+  unsigned comp;   // bytes of one component box (separate arrays)
+  unsigned bytes;  // bytes of one slice buffer (all components, 128-byte padded)
+  unsigned tx;     // bytes the TMA copies of one slice deliver
+};
+
+__device__ __forceinline__ unsigned long long pack_corner(long long x, long long y, long long z,
+                                                          long long t) {
+  return (unsigned long long)x | ((unsigned long long)y << 16) | ((unsigned long long)z << 32) |
+         ((unsigned long long)t << 48);
+}
+
+// Stage 1: stream the field through shared memory, cull hypercubes, queue
+// the survivors with the chains whose own vertices survive the cull.
+template <typename T, int D, bool TMA>
+__global__ void __launch_bounds__(kThreads, 2)
+    extract_regular_kernel(const __grid_constant__ CUtensorMap map0,
+                           const __grid_constant__ CUtensorMap map1,
+                           const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa,
+                           ExtractConfig cfg, CandidateQueue cq, BoxShape bs, unsigned* err) {
   constexpr int M = D - 1;
   constexpr int TX = Tile<D>::TX, TY = Tile<D>::TY, TZ = Tile<D>::TZ;
   constexpr int VX = TX + 1, VY = TY + 1, VZ = (D == 4) ? TZ + 1 : 1;
   constexpr int VS = VX * VY * VZ;
-  constexpr int NC = TX * TY * TZ;
-  constexpr int TBIT = 1 << (D - 1);  // mask bit of the time axis
-  constexpr int NV = 1 << D;          // vertices per hypercube
+  constexpr int VPT = (VS + kThreads - 1) / kThreads;  // vertices per thread
+  constexpr int TBIT = 1 << (D - 1);                  // mask bit of the time axis
+  static_assert(D == 3 ? kWarps * kRows == TY : kWarps == TY * (TZ / kRows),
+                "every corner row of the tile belongs to exactly one warp");
 
-  __shared__ unsigned long long W[2][VS];
-  __shared__ unsigned short surv[NC];
-  __shared__ int nsurv;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T* raw[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + bs.bytes)};
+  unsigned long long* W0 = reinterpret_cast<unsigned long long*>(smem + 2 * (size_t)bs.bytes);
+  __shared__ unsigned long long bar[2];
 
   const ChainTable& CT = c_chains[D - 3];
   const int tid = threadIdx.x;
@@ -161,172 +248,323 @@ __global__ void __launch_bounds__(kThreads, 4)
   const long long lt = mesh.ld[D - 1];
   const long long t0 = (long long)blockIdx.y * cfg.tchunk;
   const long long t1 = min(t0 + (long long)cfg.tchunk, lt);
+  const long long s_end = min(t1, lt - 1);  // last vertex slice this block reads
+  // array coordinates of local (0,0,0,0): global for multicomponent arrays,
+  // local for separate arrays
+  long long aoff[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) aoff[k] = (k < D) ? mesh.off[k] - fa.shift[k] : 0;
 
-  auto load_slice = [&](unsigned long long* dst, long long ts) {
-    for (int i = tid; i < VS; i += kThreads) {
-      const int vx = i % VX;
-      const int r = i / VX;
-      const int vy = r % VY;
-      const int vz = r / VY;
-      long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : ts, ts};
-      bool in = l[0] < mesh.ld[0] && l[1] < mesh.ld[1] && (D == 3 || l[2] < mesh.ld[2]);
-      unsigned long long w = kAbsent;
-      if (in) {
-        long long g[4];
-        unsigned long long vid = 0;
+  // per-thread vertex slots of a slice, fixed for the whole time march
+  int voff[VPT];    // element offset of component 0 in a raw slice buffer (-1: absent)
 #pragma unroll
-        for (int k = 0; k < D; ++k) {
-          g[k] = l[k] + mesh.off[k];
-          vid += (unsigned long long)g[k] * mesh.gstride[k];
+  for (int u = 0; u < VPT; ++u) {
+    const int i = tid + u * kThreads;
+    voff[u] = -1;
+    if (i < VS) {
+      const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
+      const bool in = x0 + vx < mesh.ld[0] && y0 + vy < mesh.ld[1] && (D == 3 || z0 + vz < mesh.ld[2]);
+      if (in) voff[u] = bs.multi ? ((vz * VY + vy) * bs.vxbox + vx) * M : (vz * VY + vy) * bs.vxbox + vx;
+    }
+  }
+  const int comp_elems = (int)(bs.comp / sizeof(T));
+
+  // ---- slice staging
+  auto issue = [&](long long s, int buf) {
+    if constexpr (TMA) {
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[buf], bs.tx);
+        const int cx = (int)((x0 + aoff[0]) * (bs.multi ? M : 1));
+        const int cy = (int)(y0 + aoff[1]);
+        const CUtensorMap* maps[3] = {&map0, &map1, &map2};
+        for (int j = 0; j < (bs.multi ? 1 : M); ++j) {
+          unsigned char* dst = reinterpret_cast<unsigned char*>(raw[buf]) + j * bs.comp;
+          if constexpr (D == 4)
+            tma_load_4d(dst, maps[j], cx, cy, (int)(z0 + aoff[2]), (int)(s + aoff[3]), &bar[buf]);
+          else
+            tma_load_3d(dst, maps[j], cx, cy, (int)(s + aoff[2]), &bar[buf]);
         }
-        T v[M];
-#pragma unroll
-        for (int j = 0; j < M; ++j) v[j] = field_at<T>(fa, j, g, D, vid);
-        w = vertex_word<T, M>(v);
       }
-      dst[i] = w;
+    } else {
+      // plain cooperative loads into the same layout (zero outside the array)
+      const int nper = bs.vxbox * VY * VZ;
+      for (int e = tid; e < nper * M; e += kThreads) {
+        int j, r;
+        if (bs.multi) {
+          j = e % M;
+          r = e / M;
+        } else {
+          j = e / nper;
+          r = e % nper;
+        }
+        const int vx = r % bs.vxbox;
+        const int vy = (r / bs.vxbox) % VY;
+        const int vz = r / (bs.vxbox * VY);
+        const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : s, s};
+        bool in = true;
+        long long o = 0;
+        if (fa.per_vertex) {
+          // 1-D per-vertex arrays: index by vertex id, only inside the mesh
+#pragma unroll
+          for (int k = 0; k < D; ++k) {
+            in &= l[k] < mesh.ld[k];
+            o += (l[k] + mesh.off[k]) * (long long)mesh.gstride[k];
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < D; ++k) {
+            const long long a = l[k] + aoff[k];
+            in &= a >= 0 && a < fa.adims[k];
+            o += a * fa.estride[k];
+          }
+        }
+        T v = T(0);
+        if (in) v = static_cast<const T*>(fa.comp[j])[o];
+        if (bs.multi) raw[buf][((vz * VY + vy) * bs.vxbox + vx) * M + j] = v;
+        else raw[buf][j * comp_elems + (vz * VY + vy) * bs.vxbox + vx] = v;
+      }
     }
   };
-
-  int cur = 0;
-  load_slice(W[0], t0);
-  for (long long ct = t0; ct < t1; ++ct) {
-    const int nxt = cur ^ 1;
-    if (ct + 1 < lt) {
-      load_slice(W[nxt], ct + 1);
+  auto wait = [&](long long s, int buf) -> bool {
+    if constexpr (TMA) {
+      const unsigned parity = (unsigned)(((s - t0) >> 1) & 1);
+      const bool ok = mbar_wait(&bar[buf], parity);
+      return !__syncthreads_or(!ok);
     } else {
-      for (int i = tid; i < VS; i += kThreads) W[nxt][i] = kAbsent;
+      __syncthreads();
+      return true;
     }
-    if (tid == 0) nsurv = 0;
-    __syncthreads();
-
-    // ---- hypercube cull
-    for (int c = tid; c < NC; c += kThreads) {
-      const int cx = c % TX;
-      const int cy = (c / TX) % TY;
-      const int cz = c / (TX * TY);
-      if (x0 + cx >= mesh.ld[0] || y0 + cy >= mesh.ld[1] || (D == 4 && z0 + cz >= mesh.ld[2])) continue;
-      unsigned long long acc = kAbsent;
+  };
+  auto words = [&](int buf, unsigned long long* dst) {
+    const T* r = raw[buf];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        const int dx = v & 1, dy = (v >> 1) & 1, dz = (D == 4) ? (v >> 2) & 1 : 0;
-        const int slot = ((cz + dz) * VY + (cy + dy)) * VX + (cx + dx);
-        acc &= ((v & TBIT) ? W[nxt] : W[cur])[slot];
+    for (int u = 0; u < VPT; ++u) {
+      const int i = tid + u * kThreads;
+      if (i < VS) {
+        unsigned long long w = kAbsent;
+        if (voff[u] >= 0) {
+          T v[M];
+#pragma unroll
+          for (int j = 0; j < M; ++j) v[j] = bs.multi ? r[voff[u] + j] : r[voff[u] + j * comp_elems];
+          w = vertex_word<T, M>(v);
+        }
+        dst[i] = w;
       }
-      if (!word_culled(acc)) surv[atomicAdd(&nsurv, 1)] = (unsigned short)c;
+    }
+  };
+  auto W = [&](long long s) -> unsigned long long* { return W0 + (size_t)((s - t0) % 3) * VS; };
+
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    issue(t0, 0);
+    if (t0 + 1 <= s_end) issue(t0 + 1, 1);
+  } else {
+    issue(t0, 0);
+  }
+  if (!wait(t0, 0)) {
+    // give the other copy in flight a bounded chance to land before leaving
+    if (TMA && t0 + 1 <= s_end) mbar_wait(&bar[1], 0);
+    if (tid == 0) atomicOr(err, 2u);
+    return;
+  }
+  words(0, W(t0));
+  __syncthreads();
+  if (TMA && t0 + 2 <= s_end) issue(t0 + 2, 0);
 
-    // ---- surviving hypercubes: enumerate chains, exact tests
-    const int ns = nsurv;
-    for (int s = warp; s < ns; s += kThreads / 32) {
-      const int c = surv[s];
-      const int cx = c % TX;
-      const int cy = (c / TX) % TY;
-      const int cz = c / (TX * TY);
-      const long long l[4] = {x0 + cx, y0 + cy, (D == 4) ? z0 + cz : ct, ct};
-      int valid = 0;  // axes along which the corner can step by +1
-#pragma unroll
-      for (int k = 0; k < D; ++k)
-        if (l[k] + 1 < mesh.ld[k]) valid |= 1 << k;
-      long long g0[4];
-      unsigned long long vid0 = 0;
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        g0[k] = l[k] + mesh.off[k];
-        vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
+  for (long long ct = t0; ct < t1; ++ct) {
+    const long long s = ct + 1;
+    unsigned long long* B = W(s);
+    if (s <= s_end) {
+      const int buf = (int)((s - t0) & 1);
+      if (!TMA) issue(s, buf);
+      if (!wait(s, buf)) {
+        if (TMA && s + 1 <= s_end) mbar_wait(&bar[buf ^ 1], (unsigned)(((s + 1 - t0) >> 1) & 1));
+        if (tid == 0) atomicOr(err, 2u);
+        return;
       }
-      for (int base = 0; base < CT.n; base += 32) {
-        const int ch = base + lane;
-        bool acc = false;
-        double lam_out[4] = {0, 0, 0, 0};
-        float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-        float sc_out = 0.f;
-        if (ch < CT.n) {
-          int mk[M + 1];
-          mk[0] = 0;
+      words(buf, B);
+    } else {
+      for (int i = tid; i < VS; i += kThreads) B[i] = kAbsent;
+    }
+    __syncthreads();
+    if (TMA && s + 2 <= s_end) issue(s + 2, (int)((s - t0) & 1));
+
+    // ---- hypercube cull: lanes along x, kRows corner rows per warp
+    const unsigned long long* A = W(ct);
+    const int cyw = (D == 4) ? warp % TY : warp * kRows;
+    const int czw = (D == 4) ? (warp / TY) * kRows : 0;
+    unsigned long long R[kRows + 1];
 #pragma unroll
-          for (int i = 0; i < M; ++i) mk[i + 1] = CT.mask[ch][i];
-          if ((mk[M] & ~valid) == 0) {
-            unsigned long long wacc = kAbsent;
+    for (int q = 0; q <= kRows; ++q) {
+      unsigned long long r, e = kAbsent;
+      if constexpr (D == 4) {
+        const int i0 = ((czw + q) * VY + cyw) * VX + lane, i1 = i0 + VX;
+        r = A[i0] & A[i1] & B[i0] & B[i1];
+        if (lane == 31) e = A[i0 + 1] & A[i1 + 1] & B[i0 + 1] & B[i1 + 1];
+      } else {
+        const int i0 = (cyw + q) * VX + lane;
+        r = A[i0] & B[i0];
+        if (lane == 31) e = A[i0 + 1] & B[i0 + 1];
+      }
+      const unsigned long long nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
+      R[q] = r & (lane == 31 ? e : nb);
+    }
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      const int cy = (D == 4) ? cyw : cyw + q;
+      const int cz = (D == 4) ? czw + q : 0;
+      const bool valid = x0 + lane < mesh.ld[0] && y0 + cy < mesh.ld[1] &&
+                         (D == 3 || z0 + cz < mesh.ld[2]);
+      unsigned ball = __ballot_sync(0xFFFFFFFFu, valid && !word_culled(R[q] & R[q + 1]));
+      while (ball) {
+        // one surviving hypercube at a time: lanes test its chains
+        const int cx = __ffs(ball) - 1;
+        ball &= ball - 1;
+        const long long l[4] = {x0 + cx, y0 + cy, (D == 4) ? z0 + cz : ct, ct};
+        int vmask = 0;  // axes along which the corner can step by +1
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+          if (l[k] + 1 < mesh.ld[k]) vmask |= 1 << k;
+        unsigned long long chains = 0;
+        for (int base = 0; base < CT.n; base += 32) {
+          const int ch = base + lane;
+          bool ok = false;
+          if (ch < CT.n && (CT.mask[ch][M - 1] & ~vmask) == 0) {
+            unsigned long long wacc = (A[((cz * VY) + cy) * VX + cx]);
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+              const int mk = CT.mask[ch][i];
+              const int dx = mk & 1, dy = (mk >> 1) & 1, dz = (D == 4) ? (mk >> 2) & 1 : 0;
+              const int slot = ((cz + dz) * VY + (cy + dy)) * VX + (cx + dx);
+              wacc &= ((mk & TBIT) ? B : A)[slot];
+            }
+            ok = !word_culled(wacc);
+          }
+          chains |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, ok) << base;
+        }
+        if (chains && lane == 0) {
+          const unsigned idx = atomicAdd(cq.count, 1u);
+          if (idx < cq.cap) {
+            cq.corner[idx] = pack_corner(l[0], l[1], (D == 4) ? l[2] : 0, ct);
+            cq.chains[idx] = chains;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Stage 2: exact SoS test and bit-exact solve of every queued chain, one warp
+// per candidate hypercube, accepted simplices compacted by warp ballot.
+template <typename T, int D>
+__global__ void __launch_bounds__(256)
+    refine_regular_kernel(RegularMesh mesh, FieldAccess fa, ExtractConfig cfg, CandidateQueue cq,
+                          FeatureSink sink) {
+  constexpr int M = D - 1;
+  const ChainTable& CT = c_chains[D - 3];
+  const int lane = threadIdx.x & 31;
+  const unsigned n = min(*cq.count, cq.cap);
+  const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned c = gw; c < n; c += nw) {
+    const unsigned long long pc = cq.corner[c];
+    const unsigned long long chains = cq.chains[c];
+    const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                            (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+    long long g0[4];
+    unsigned long long vid0 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      // D = 3: the time coordinate sits in slot 2
+      const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+      g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+      if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
+    }
+    for (int base = 0; base < CT.n; base += 32) {
+      const int ch = base + lane;
+      bool acc = false;
+      double lam_out[4] = {0, 0, 0, 0};
+      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+      float sc_out = 0.f;
+      if (ch < CT.n && ((chains >> ch) & 1ull)) {
+        int mk[M + 1];
+        mk[0] = 0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) mk[i + 1] = CT.mask[ch][i];
+        T vals[M + 1][M];
+        long long gv[M + 1][4];
+        unsigned long long vid[M + 1];
+#pragma unroll
+        for (int i = 0; i <= M; ++i) {
+          vid[i] = 0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            gv[i][k] = (k < D) ? g0[k] + ((mk[i] >> k) & 1) : 0;
+            if (k < D) vid[i] += (unsigned long long)gv[i][k] * mesh.gstride[k];
+          }
+#pragma unroll
+          for (int j = 0; j < M; ++j) vals[i][j] = field_at<T>(fa, j, gv[i], D, vid[i]);
+        }
+        bool inside;
+        if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
+        else inside = sos_inside3<T>(vals, cfg.Q);
+        if (inside) {
+          T lam[M + 1];
+          if (solve_exact<M, T>(vals, lam)) {
+            acc = true;
 #pragma unroll
             for (int i = 0; i <= M; ++i) {
-              const int dx = mk[i] & 1, dy = (mk[i] >> 1) & 1, dz = (D == 4) ? (mk[i] >> 2) & 1 : 0;
-              const int slot = ((cz + dz) * VY + (cy + dy)) * VX + (cx + dx);
-              wacc &= ((mk[i] & TBIT) ? W[nxt] : W[cur])[slot];
+              lam_out[i] = (double)lam[i];
+              bary_out[i] = (float)lam[i];
             }
-            if (!word_culled(wacc)) {
-              T vals[M + 1][M];
-              long long gv[M + 1][4];
-              unsigned long long vid[M + 1];
+            if (fa.has_scalar) {
+              using F = fp<T>;
+              T sc = T(0);
 #pragma unroll
-              for (int i = 0; i <= M; ++i) {
-                vid[i] = 0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                  gv[i][k] = (k < D) ? g0[k] + ((mk[i] >> k) & 1) : 0;
-                  if (k < D) vid[i] += (unsigned long long)gv[i][k] * mesh.gstride[k];
-                }
-#pragma unroll
-                for (int j = 0; j < M; ++j) vals[i][j] = field_at<T>(fa, j, gv[i], D, vid[i]);
-              }
-              bool inside;
-              if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
-              else inside = sos_inside3<T>(vals, cfg.Q);
-              if (inside) {
-                T lam[M + 1];
-                if (solve_exact<M, T>(vals, lam)) {
-                  acc = true;
-#pragma unroll
-                  for (int i = 0; i <= M; ++i) {
-                    lam_out[i] = (double)lam[i];
-                    bary_out[i] = (float)lam[i];
-                  }
-                  if (fa.has_scalar) {
-                    using F = fp<T>;
-                    T s = T(0);
-#pragma unroll
-                    for (int i = 0; i <= M; ++i) s = F::add(s, F::mul(lam[i], scalar_at<T>(fa, gv[i], D, vid[i])));
-                    sc_out = (float)s;
-                  }
-                  if (cfg.refined) {
-                    double r[M + 1];
-                    if (solve_refined<M, T>(vals, r))
-#pragma unroll
-                      for (int i = 0; i <= M; ++i) lam_out[i] = r[i];
-                  }
-                }
-              }
+              for (int i = 0; i <= M; ++i)
+                sc = F::add(sc, F::mul(lam[i], scalar_at<T>(fa, gv[i], D, vid[i])));
+              sc_out = (float)sc;
             }
-          }
-        }
-        const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
-        if (ball) {
-          unsigned int basei = 0;
-          const int leader = __ffs(ball) - 1;
-          if (lane == leader) basei = atomicAdd(sink.count, (unsigned)__popc(ball));
-          basei = __shfl_sync(0xFFFFFFFFu, basei, leader);
-          if (acc) {
-            const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
-            if (idx < sink.cap) {
-              sink.key[idx] = vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
+            if (cfg.refined) {
+              double rr[M + 1];
+              if (solve_refined<M, T>(vals, rr))
 #pragma unroll
-              for (int i = 0; i < 4; ++i) {
-                sink.lam[4 * (size_t)idx + i] = lam_out[i];
-                sink.bary4[4 * (size_t)idx + i] = bary_out[i];
-              }
-              sink.scalar[idx] = sc_out;
+                for (int i = 0; i <= M; ++i) lam_out[i] = rr[i];
             }
           }
         }
       }
+      const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
+      if (ball) {
+        unsigned int basei = 0;
+        const int leader = __ffs(ball) - 1;
+        if (lane == leader) basei = atomicAdd(sink.count, (unsigned)__popc(ball));
+        basei = __shfl_sync(0xFFFFFFFFu, basei, leader);
+        if (acc) {
+          const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
+          if (idx < sink.cap) {
+            sink.key[idx] = vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              sink.lam[4 * (size_t)idx + i] = lam_out[i];
+              sink.bary4[4 * (size_t)idx + i] = bary_out[i];
+            }
+            sink.scalar[idx] = sc_out;
+          }
+        }
+      }
     }
-    __syncthreads();
-    cur = nxt;
   }
 }
 
 // ---------------------------------------------------------------------------
+// host side
 
 static void build_chains(ChainTable& t, int d, int m) {
   // strictly increasing non-empty masks m1 < ... < mm (each a superset of the
@@ -366,19 +604,154 @@ void upload_chain_tables() {
   cudaMemcpyToSymbol(c_chains, h, sizeof(h));
 }
 
-cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
-                                   const ExtractConfig& cfg, const FeatureSink& sink,
-                                   cudaStream_t st) {
-  const long long lt = mesh.ld[mesh.d - 1];
+static int vxbox_for(int multi, int m, size_t es) {
+  // smallest box width >= 33 whose row is a multiple of 16 bytes
+  for (int v = 33; v <= kMaxVXBox; ++v)
+    if (((size_t)v * (multi ? m : 1) * es) % 16 == 0) return v;
+  return kMaxVXBox;
+}
+
+// cuTensorMapEncodeTiled is a driver API entry point; it is resolved through
+// the runtime so that the library carries no link-time libcuda dependency.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+static bool encode_map(CUtensorMap* map, bool f64, const void* base, int rank, const uint64_t* dims,
+                       const uint64_t* strides_bytes, const uint32_t* box) {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return false;
+  cuuint64_t gd[5], gs[4];
+  cuuint32_t bx[5], es[5];
+  for (int i = 0; i < rank; ++i) {
+    gd[i] = dims[i];
+    bx[i] = box[i];
+    es[i] = 1;
+    if (i) gs[i - 1] = strides_bytes[i - 1];
+  }
+  CUresult r = encode(
+      map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank,
+      const_cast<void*>(base), gd, gs, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename T, int D>
+static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                            const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
+                            int* used_tma) {
+  constexpr int M = D - 1;
+  constexpr int VY = Tile<D>::TY + 1, VZ = (D == 4) ? Tile<D>::TZ + 1 : 1;
+  const size_t es = sizeof(T);
+  const int multi = (!fa.per_vertex && fa.estride[0] == M) ? 1 : 0;  // interleaved components
+  BoxShape bs;
+  bs.multi = multi;
+  bs.vxbox = vxbox_for(multi, M, es);
+  const size_t comp_bytes = (size_t)bs.vxbox * VY * VZ * es;
+  bs.comp = (unsigned)((comp_bytes + 127) & ~(size_t)127);
+  bs.tx = (unsigned)(comp_bytes * M);
+  bs.bytes = multi ? (unsigned)((comp_bytes * M + 127) & ~(size_t)127) : bs.comp * M;
+
+  // TMA applies when every box starts on a 16-byte boundary and the array
+  // strides are multiples of 16 bytes: inner coordinate = array x * (M or 1)
+  CUtensorMap maps[3];
+  memset(maps, 0, sizeof(maps));
+  bool tma = allow_tma && !fa.per_vertex;
+  const long long ax0 = mesh.off[0] - fa.shift[0];
+  const size_t inner_es = (multi ? M : 1) * es;
+  if (tma) {
+    if (((size_t)ax0 * inner_es) % 16 != 0) tma = false;
+    if (((size_t)fa.adims[0] * inner_es) % 16 != 0) tma = false;
+    for (int j = 0; j < (multi ? 1 : M); ++j)
+      if (((uintptr_t)fa.comp[j]) % 16 != 0) tma = false;
+    for (int k = 0; k < D; ++k)
+      if (fa.adims[k] * (k == 0 ? (multi ? M : 1) : 1) > 0x7FFFFFFFll) tma = false;
+  }
+  if (tma) {
+    uint64_t dims[4], strides[3];
+    uint32_t box[4];
+    dims[0] = (uint64_t)fa.adims[0] * (multi ? M : 1);
+    box[0] = (uint32_t)(bs.vxbox * (multi ? M : 1));
+    uint64_t s = dims[0] * es;
+    for (int k = 1; k < D; ++k) {
+      dims[k] = (uint64_t)fa.adims[k];
+      strides[k - 1] = s;
+      s *= dims[k];
+    }
+    box[1] = VY;
+    if (D == 4) {
+      box[2] = VZ;
+      box[3] = 1;
+    } else {
+      box[2] = 1;
+    }
+    for (int j = 0; j < (multi ? 1 : M) && tma; ++j)
+      tma = encode_map(&maps[j], sizeof(T) == 8, fa.comp[j], D, dims, strides, box);
+  }
+  if (used_tma) *used_tma = tma ? 1 : 0;
+  const size_t words = 3 * sizeof(unsigned long long) * (size_t)(Tile<D>::TX + 1) * VY * VZ;
+  const size_t shm = 2 * (size_t)bs.bytes + words;
+  const long long lt = mesh.ld[D - 1];
   const unsigned nchunks = (unsigned)((lt + cfg.tchunk - 1) / cfg.tchunk);
   const unsigned ntiles = (unsigned)cfg.tiles[0] * cfg.tiles[1] * cfg.tiles[2];
   dim3 grid(ntiles, nchunks);
-  if (mesh.d == 4) {
-    if (f64) extract_regular_kernel<double, 4><<<grid, kThreads, 0, st>>>(mesh, fa, cfg, sink);
-    else extract_regular_kernel<float, 4><<<grid, kThreads, 0, st>>>(mesh, fa, cfg, sink);
+  cudaError_t e;
+  if (tma) {
+    auto k = extract_regular_kernel<T, D, true>;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e) return e;
+    k<<<grid, kThreads, shm, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, bs, err);
   } else {
-    if (f64) extract_regular_kernel<double, 3><<<grid, kThreads, 0, st>>>(mesh, fa, cfg, sink);
-    else extract_regular_kernel<float, 3><<<grid, kThreads, 0, st>>>(mesh, fa, cfg, sink);
+    auto k = extract_regular_kernel<T, D, false>;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e) return e;
+    k<<<grid, kThreads, shm, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, bs, err);
+  }
+  return cudaGetLastError();
+}
+
+void regular_tile(int d, int* tx, int* ty, int* tz) {
+  if (d == 4) {
+    *tx = Tile<4>::TX;
+    *ty = Tile<4>::TY;
+    *tz = Tile<4>::TZ;
+  } else {
+    *tx = Tile<3>::TX;
+    *ty = Tile<3>::TY;
+    *tz = Tile<3>::TZ;
+  }
+}
+
+cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
+                                   const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
+                                   cudaStream_t st, bool allow_tma, int* used_tma) {
+  if (mesh.d == 4)
+    return f64 ? launch_t<double, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
+               : launch_t<float, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
+  return f64 ? launch_t<double, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
+             : launch_t<float, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
+}
+
+cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
+                                  const ExtractConfig& cfg, const CandidateQueue& cq,
+                                  const FeatureSink& sink, int num_sms, cudaStream_t st) {
+  const int blocks = num_sms * 4;
+  if (mesh.d == 4) {
+    if (f64) refine_regular_kernel<double, 4><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
+    else refine_regular_kernel<float, 4><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
+  } else {
+    if (f64) refine_regular_kernel<double, 3><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
+    else refine_regular_kernel<float, 3><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
   }
   return cudaGetLastError();
 }

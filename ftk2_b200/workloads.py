@@ -1,0 +1,69 @@
+"""Named workloads of the critical-point path, runnable from the command line
+(used for profiling runs; the field is generated on the device):
+
+    python -m ftk2_b200.workloads --case c2 --steps 3
+    python -m ftk2_b200.workloads --case c2_small --steps 2 --no-tma
+
+c2        3D flow CPs, plain drop-in: 128^3 x 16 float64, 32 blobs, Q = 2^20
+c2_small  the same field definition on 128^3 x 4 (200 MB, larger than L2)
+c4        precision workload: 256^3 x 8 float32 with 1e-3 noise
+c4_small  the same on 256^3 x 2
+c1        2D analytic 64 x 64 x 10 float64, Q = 1e6
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+from . import api, generate, synthetic
+
+
+def make(case: str):
+    import torch
+    if case == "c2":
+        return generate.c2_field(), [128, 128, 128, 16], 3, 2.0 ** 20
+    if case == "c2_small":
+        f = generate.gaussian_field_device((128, 128, 128), 4, seed=1234, n_blobs=32,
+                                           dtype=torch.float64)
+        return f, [128, 128, 128, 4], 3, 2.0 ** 20
+    if case == "c4":
+        return generate.c4_field(), [256, 256, 256, 8], 3, 2.0 ** 20
+    if case == "c4_small":
+        f = generate.gaussian_field_device((256, 256, 256), 2, seed=4321, n_blobs=64,
+                                           dtype=torch.float32, noise=1e-3, sigma=(16.0, 48.0),
+                                           scale=256.0)
+        return f, [256, 256, 256, 2], 3, 2.0 ** 20
+    if case == "c1":
+        f = torch.from_numpy(synthetic.analytic_2d()).cuda()
+        return f, [64, 64, 10], 2, 1e6
+    raise ValueError(case)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="c2_small")
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--no-tma", action="store_true")
+    ap.add_argument("--refined", action="store_true")
+    args = ap.parse_args()
+    import torch
+    field, dims, m, q = make(args.case)
+    torch.cuda.synchronize()
+    with api.Context(0) as ctx:
+        if args.no_tma:
+            ctx.set_option(api.OPT_DISABLE_TMA, 1)
+        keep: list = []
+        mesh = api.regular_mesh_desc(dims)
+        fd = api.field_desc(field, api.LAYOUT_MULTICOMPONENT, m, keep=keep)
+        prm = api.params(q, precision=api.PRECISION_REFINED if args.refined else api.PRECISION_EXACT)
+        for i in range(args.steps):
+            t = time.perf_counter()
+            n, ne = ctx.run(mesh, fd, prm)
+            x, tot, _ = ctx.last_timing()
+            print(f"step {i}: {n} features {ne} edges  extract {x:.3f} ms  pipeline {tot:.3f} ms  "
+                  f"host {1e3 * (time.perf_counter() - t):.3f} ms  tma={ctx.get_option(api.INFO_LAST_TMA)}",
+                  flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -141,9 +141,14 @@ ftk2b_cp_params ftk2b_cp_params_default(void);
  * its buffers with fixed guesses, engine.hpp:351-385). */
 enum {
   FTK2B_OPT_FEATURE_CAPACITY = 1, /* initial feature capacity; grows on overflow */
-  FTK2B_OPT_TIME_CHUNK = 2        /* time steps per extraction block (0 = all) */
+  FTK2B_OPT_TIME_CHUNK = 2,       /* time steps per extraction block (0 = all) */
+  FTK2B_OPT_DISABLE_TMA = 3       /* 1: stage slices with plain loads instead of TMA */
 };
 ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
+/* Reads an option back, or FTK2B_INFO_LAST_TMA: 1 when the last regular-mesh
+ * extraction staged its slices with TMA tensor copies. */
+enum { FTK2B_INFO_LAST_TMA = 100 };
+ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t* value);
 
 /* m-simplices a mesh holds for codimension m (2 or 3): the unit of work. */
 uint64_t ftk2b_mesh_simplex_count(const ftk2b_mesh_desc* mesh, int m);

@@ -50,12 +50,19 @@ REGULAR_GOLDEN = [n for n in sorted(cases.GOLDEN_CASES) if not n.startswith("ext
 EXTRUDED_GOLDEN = [n for n in sorted(cases.GOLDEN_CASES) if n.startswith("extruded")]
 
 
+@pytest.mark.parametrize("staging", ["tma", "plain"])
 @pytest.mark.parametrize("name", REGULAR_GOLDEN)
-def test_golden_regular(ctx, name):
+def test_golden_regular(ctx, name, staging):
     case = cases.GOLDEN_CASES[name]()
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     assert str(z["input_sha256"]) == case.input_digest()
-    g = gpu_run(ctx, case)
+    ctx.set_option(api.OPT_DISABLE_TMA, 1 if staging == "plain" else 0)
+    try:
+        g = gpu_run(ctx, case)
+        if staging == "plain":
+            assert ctx.get_option(api.INFO_LAST_TMA) == 0
+    finally:
+        ctx.set_option(api.OPT_DISABLE_TMA, 0)
     ref = bridge.CPResult(simplices=z["simplices"], bary=z["bary"], lam=z["lam"],
                           track_id=z["track_id"], type=z["type"], scalar=z["scalar"],
                           edges=z["edges"])
@@ -93,6 +100,26 @@ def test_medium_vs_restatement(ctx, case):
     assert len(o.track_id) > 0
     assert_identical(g, o)
     assert g.n_simplices == o.n_tested
+    ctx.set_option(api.OPT_DISABLE_TMA, 1)
+    try:
+        p = gpu_run(ctx, case)
+    finally:
+        ctx.set_option(api.OPT_DISABLE_TMA, 0)
+    assert_identical(p, o)
+
+
+def test_tma_used_when_aligned_and_skipped_when_not(ctx):
+    g = S.gaussian_sum_gradient((40, 36, 32), 4, seed=2, n_blobs=10)
+    # aligned multicomponent float64 array: TMA staging
+    gpu_run(ctx, cases.Case("a", "regular", 3, cases.MULTI, g, 2.0 ** 20, [40, 36, 32, 4]))
+    assert ctx.get_option(api.INFO_LAST_TMA) == 1
+    # odd x offset: a box would start 24 bytes into a 16-byte line, so the
+    # kernel falls back to plain loads, with identical results
+    case = cases.Case("b", "regular", 3, cases.MULTI, g, 2.0 ** 20, [36, 30, 28, 3], [3, 1, 2, 1],
+                      [40, 36, 32, 4])
+    r = gpu_run(ctx, case)
+    assert ctx.get_option(api.INFO_LAST_TMA) == 0
+    assert_identical(r, oracle_run(case))
 
 
 def test_device_input_matches_host_input(ctx):
