@@ -36,7 +36,7 @@ F32, F64 = 0, 1
 LAYOUT_MULTICOMPONENT, LAYOUT_SEPARATE, LAYOUT_PER_VERTEX = 0, 1, 2
 HOST, DEVICE = 0, 1
 PRECISION_EXACT, PRECISION_REFINED = 0, 1
-OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA = 1, 2, 3
+OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA, OPT_USE_GRAPHS = 1, 2, 3, 4
 INFO_LAST_TMA = 100
 CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
                "center"]

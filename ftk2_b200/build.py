@@ -60,5 +60,26 @@ def build(verbose: bool = False) -> str:
     return LIB
 
 
+DROPIN_SRC = os.path.join(ROOT, "tests", "cpp", "dropin_c1.cpp")
+DROPIN_BIN = os.path.join(OUT_DIR, "dropin_c1")
+
+
+def build_dropin_test(verbose: bool = False) -> str:
+    """C++ program using include/ftk2b/engine.hpp exactly like the reference's
+    examples use engine.hpp; linked against libftk2b.so (rpath = _lib)."""
+    lib = build(verbose)
+    if os.path.exists(DROPIN_BIN) and os.path.getmtime(DROPIN_BIN) >= max(
+            os.path.getmtime(DROPIN_SRC), os.path.getmtime(lib),
+            os.path.getmtime(os.path.join(ROOT, "include", "ftk2b", "engine.hpp"))):
+        return DROPIN_BIN
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(ROOT, "oracle", "shim"), DROPIN_SRC, "-o", DROPIN_BIN,
+           "-L", OUT_DIR, "-lftk2b", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return DROPIN_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))

@@ -23,6 +23,7 @@ namespace ftk2b {
 
 cudaError_t DevBuf::ensure(size_t want) {
   if (bytes >= want && p) return cudaSuccess;
+  ++generation;
   if (p) cudaFree(p);
   p = nullptr;
   bytes = 0;
@@ -86,6 +87,10 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
     delete ctx;
     return FTK2B_CUDA_ERROR;
   }
+  if (cudaMallocHost((void**)&ctx->h_counters, sizeof(unsigned) * kNumCounters) != cudaSuccess) {
+    delete ctx;
+    return FTK2B_OOM;
+  }
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   ctx->num_sms = prop.multiProcessorCount;
@@ -118,6 +123,9 @@ extern "C" void ftk2b_ctx_destroy(ftk2b_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->release_all();
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->gexec2) cudaGraphExecDestroy(ctx->gexec2);
+  if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaEventDestroy(ctx->ev_x);
@@ -155,6 +163,10 @@ extern "C" ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_DISABLE_TMA:
       ctx->disable_tma = value != 0;
       return FTK2B_OK;
+    case FTK2B_OPT_USE_GRAPHS:
+      ctx->use_graphs = value != 0;
+      ctx->graph_valid = false;
+      return FTK2B_OK;
     default:
       return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
@@ -167,11 +179,14 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_TIME_CHUNK: *value = ctx->tune_tchunk; return FTK2B_OK;
     case FTK2B_OPT_DISABLE_TMA: *value = ctx->disable_tma ? 1 : 0; return FTK2B_OK;
     case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
+    case FTK2B_OPT_USE_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return FTK2B_OK;
     default: return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
 }
 
 void ftk2b_ctx::release_all() {
+  // cached graphs point into these buffers
+  graph_valid = false;
   for (DevBuf* b : all_bufs()) b->release();
 }
 
@@ -492,8 +507,6 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
-    CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream));
-    CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     FeatureSink sink;
     sink.key = B.key;
     sink.lam = B.lam;
@@ -506,28 +519,96 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cq.chains = (unsigned long long*)ctx->cand_chains.p;
     cq.count = (unsigned*)ctx->counters.p + kCountCand;
     cq.cap = ccap;
-    CUDA_TRY(ctx, launch_extract_regular(field->dtype == FTK2B_F64, rm, fa, cfg, cq, B.err,
-                                         ctx->stream, !ctx->disable_tma, &ctx->last_used_tma));
-    CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
-    CUDA_TRY(ctx, launch_refine_regular(field->dtype == FTK2B_F64, rm, fa, cfg, cq, sink, ctx->num_sms,
-                                        ctx->stream));
-    CUDA_TRY(ctx, cudaEventRecord(ctx->ev_r, ctx->stream));
-    ctx->launches += 2;
-    CUDA_TRY(ctx, launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, &ctx->launches));
-    if (prm->classify) {
-      CUDA_TRY(ctx, launch_classify_regular(field->dtype == FTK2B_F64, rm, fa, nch, B, ctx->stream));
-      ctx->launches += 1;
+    const int f64 = field->dtype == FTK2B_F64;
+    // the device pipeline in two parts so that the fused cull kernel can be
+    // timed on its own: [counters reset, cull] and [exact tests, canonical
+    // order, star edges, trajectories, counters readback]
+    auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
+      cudaError_t e;
+      if ((e = cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream))) return e;
+      if ((e = launch_extract_regular(f64, rm, fa, cfg, cq, B.err, ctx->stream, !ctx->disable_tma,
+                                      &ctx->last_used_tma)))
+        return e;
+      *nl += 1;
+      return cudaSuccess;
+    };
+    auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
+      cudaError_t e;
+      if ((e = launch_refine_regular(f64, rm, fa, cfg, cq, sink, ctx->num_sms, ctx->stream))) return e;
+      *nl += 1;
+      if ((e = launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, nl))) return e;
+      if (prm->classify) {
+        if ((e = launch_classify_regular(f64, rm, fa, nch, B, ctx->stream))) return e;
+        *nl += 1;
+      }
+      return cudaMemcpyAsync(ctx->h_counters, ctx->counters.p, sizeof(unsigned) * kNumCounters,
+                             cudaMemcpyDeviceToHost, ctx->stream);
+    };
+    if (ctx->use_graphs) {
+      RegularGraphKey key;
+      memset(&key, 0, sizeof(key));
+      key.rm = rm;
+      key.fa = fa;
+      key.cfg = cfg;
+      key.cap = cap;
+      key.ccap = ccap;
+      key.edge_cap = edge_cap;
+      key.f64 = f64;
+      key.want_edges = prm->want_edges;
+      key.classify = prm->classify;
+      key.allow_tma = !ctx->disable_tma;
+      key.key_bits = key_bits;
+      key.nch = nch;
+      const unsigned long long gen = ctx->buffer_generation();
+      if (!(ctx->graph_valid && ctx->graph_gen == gen && memcmp(&key, &ctx->gkey, sizeof(key)) == 0)) {
+        ctx->graph_valid = false;
+        unsigned long long nl = 0;
+        cudaGraphExec_t* slots[2] = {&ctx->gexec, &ctx->gexec2};
+        for (int part = 0; part < 2; ++part) {
+          cudaGraph_t graph = nullptr;
+          CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+          cudaError_t ce = part == 0 ? enqueue1(&nl) : enqueue2(&nl);
+          cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
+          if (ce || ee) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return fail(ctx, FTK2B_CUDA_ERROR, "graph capture failed: %s",
+                        cudaGetErrorString(ce ? ce : ee));
+          }
+          if (*slots[part]) cudaGraphExecDestroy(*slots[part]);
+          *slots[part] = nullptr;
+          cudaError_t ie = cudaGraphInstantiate(slots[part], graph, 0);
+          cudaGraphDestroy(graph);
+          if (ie) return fail(ctx, FTK2B_CUDA_ERROR, "graph instantiate failed: %s", cudaGetErrorString(ie));
+        }
+        ctx->gkey = key;
+        ctx->graph_gen = gen;
+        ctx->graph_valid = true;
+        ctx->launches_per_run = nl;
+      }
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+      CUDA_TRY(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
+      CUDA_TRY(ctx, cudaGraphLaunch(ctx->gexec2, ctx->stream));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+      ctx->launches += ctx->launches_per_run;
+    } else {
+      unsigned long long nl = 0;
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+      CUDA_TRY(ctx, enqueue1(&nl));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
+      CUDA_TRY(ctx, enqueue2(&nl));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+      ctx->launches += nl;
     }
-    CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-    unsigned h[kNumCounters];
-    CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->counters.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    float ms = 0.f, xms = 0.f, rms = 0.f;
-    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    cudaEventElapsedTime(&xms, ctx->ev0, ctx->ev_x);
-    cudaEventElapsedTime(&rms, ctx->ev_x, ctx->ev_r);
+    unsigned h[kNumCounters];
+    memcpy(h, ctx->h_counters, sizeof(h));
+    float ms = 0.f, xms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) ms = 0.f;
+    if (cudaEventElapsedTime(&xms, ctx->ev0, ctx->ev_x) != cudaSuccess) xms = 0.f;
+    cudaGetLastError();  // a failed timing query must not linger in the error slot
     ctx->last_extract_ms = xms;
-    ctx->last_refine_ms = rms;
     if (h[kCountErr] & 2u) return fail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return fail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
     if (h[kCountCand] > ccap) {

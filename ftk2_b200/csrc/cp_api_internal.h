@@ -14,11 +14,22 @@ namespace ftk2b {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  unsigned long long generation = 0;  // bumped on every reallocation
   cudaError_t ensure(size_t want);
   void release();
 };
 
 enum { kCountFeatures = 0, kCountEdges = 1, kCountRoots = 2, kCountErr = 3, kCountCand = 4, kNumCounters = 8 };
+
+// Everything a regular-mesh run bakes into its kernel launches; a cached CUDA
+// graph is replayed only when the next run's key is byte-identical.
+struct RegularGraphKey {
+  RegularMesh rm;
+  FieldAccess fa;
+  ExtractConfig cfg;
+  unsigned cap, ccap, edge_cap;
+  int f64, want_edges, classify, allow_tma, key_bits, nch;
+};
 
 struct LastRun {
   int kind = 0, m = 0;
@@ -49,6 +60,20 @@ struct ftk2b_ctx {
       simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains;
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::LastRun last;
+  // CUDA graph of the last regular-mesh pipeline
+  bool use_graphs = true;
+  bool graph_valid = false;
+  ftk2b::RegularGraphKey gkey;
+  cudaGraphExec_t gexec = nullptr;   // counters reset + fused cull kernel
+  cudaGraphExec_t gexec2 = nullptr;  // exact tests + canonical order + trajectories
+  unsigned long long launches_per_run = 0;
+  unsigned* h_counters = nullptr;  // pinned
+  unsigned long long graph_gen = 0;
+  unsigned long long buffer_generation() {
+    unsigned long long g = 0;
+    for (ftk2b::DevBuf* b : all_bufs()) g += b->generation;
+    return g;
+  }
 
   // blocks of the radix sort: enough to stream the feature capacity, few
   // enough that the per-pass digit-histogram scan stays short

@@ -25,11 +25,15 @@ __constant__ signed char c_rank4[4096];   // (m1 | m2 << 4 | m3 << 8) -> chain r
 // radix sort (keys u64, payload u32), stable, device-resident count
 
 constexpr int kRsThreads = 256;
+// counts up to this size are sorted by one block in shared memory
+constexpr unsigned kSmallSort = 8192;
+constexpr int kSmallThreads = 512;
 
 __global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
                                unsigned cap, int shift, unsigned* __restrict__ hist) {
   __shared__ unsigned h[256];
   const unsigned n = min(*n_ptr, cap);
+  if (n <= kSmallSort) return;
   const unsigned G = gridDim.x, b = blockIdx.x;
   const unsigned chunk = (n + G - 1) / G;
   const unsigned start = min(b * chunk, n), end = min(start + chunk, n);
@@ -43,9 +47,10 @@ __global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, cons
 
 // exclusive scan of `total` counters in place, one block of 1024 threads
 __global__ void scan_inplace_kernel(unsigned* __restrict__ a, unsigned total, unsigned* total_out,
-                                    const unsigned* n_ptr) {
+                                    const unsigned* n_ptr, const unsigned* skip_small) {
   __shared__ unsigned part[1024];
   const unsigned t = threadIdx.x;
+  if (skip_small && min(*skip_small, total) <= kSmallSort) return;
   if (n_ptr) total = min(total, *n_ptr);
   const unsigned seg = (total + 1023) / 1024;
   const unsigned s0 = min(t * seg, total), s1 = min(s0 + seg, total);
@@ -76,6 +81,7 @@ __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
   __shared__ unsigned base[256];
   __shared__ unsigned wcnt[kRsThreads / 32][256];
   const unsigned n = min(*n_ptr, cap);
+  if (n <= kSmallSort) return;
   const unsigned G = gridDim.x, b = blockIdx.x;
   const unsigned chunk = (n + G - 1) / G;
   const unsigned start = min(b * chunk, n), end = min(start + chunk, n);
@@ -115,7 +121,88 @@ __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
 
 __global__ void iota_kernel(unsigned* v, const unsigned* n_ptr, unsigned cap) {
   const unsigned n = min(*n_ptr, cap);
+  if (n <= kSmallSort) return;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+// One block sorts up to kSmallSort keys in shared memory (stable LSD radix,
+// 8-bit digits), writing sorted keys and the permutation to (kout, vout),
+// which may alias the input keys.  Larger counts leave it to the multi-block
+// passes, which in turn return immediately for small counts.
+__global__ void __launch_bounds__(kSmallThreads)
+    small_sort_kernel(const unsigned long long* kin, const unsigned* n_ptr, unsigned cap, int bits,
+                      unsigned long long* kout, unsigned* vout) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  unsigned long long* ka = reinterpret_cast<unsigned long long*>(sm);
+  unsigned long long* kb = ka + kSmallSort;
+  unsigned* va = reinterpret_cast<unsigned*>(kb + kSmallSort);
+  unsigned* vb = va + kSmallSort;
+  __shared__ unsigned wcnt[kSmallThreads / 32][256];
+  __shared__ unsigned base[256];
+  const unsigned n = min(*n_ptr, cap);
+  if (n > kSmallSort) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (unsigned i = tid; i < n; i += kSmallThreads) {
+    ka[i] = kin[i];
+    va[i] = i;
+  }
+  __syncthreads();
+  for (int shift = 0; shift < bits; shift += 8) {
+    // digit totals -> exclusive bases
+    if (tid < 256) base[tid] = 0;
+    __syncthreads();
+    for (unsigned i = tid; i < n; i += kSmallThreads) atomicAdd(&base[(ka[i] >> shift) & 255], 1u);
+    __syncthreads();
+    if (tid == 0) {
+      unsigned run = 0;
+      for (int d = 0; d < 256; ++d) {
+        const unsigned c = base[d];
+        base[d] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    // stable scatter, one chunk of kSmallThreads items at a time
+    for (unsigned c0 = 0; c0 < n; c0 += kSmallThreads) {
+      const unsigned i = c0 + tid;
+      const bool valid = i < n;
+      const unsigned long long key = valid ? ka[i] : 0ull;
+      const unsigned dig = valid ? (unsigned)((key >> shift) & 255) : 256u;
+      for (int d = tid; d < (kSmallThreads / 32) * 256; d += kSmallThreads) (&wcnt[0][0])[d] = 0;
+      __syncthreads();
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
+      const unsigned rank = __popc(peers & ((1u << lane) - 1));
+      if (valid && lane == __ffs(peers) - 1) wcnt[warp][dig] = __popc(peers);
+      __syncthreads();
+      unsigned run = 0;
+      if (tid < 256) {
+        for (int w = 0; w < kSmallThreads / 32; ++w) {
+          const unsigned c = wcnt[w][tid];
+          wcnt[w][tid] = run;
+          run += c;
+        }
+      }
+      __syncthreads();
+      if (valid) {
+        const unsigned pos = base[dig] + wcnt[warp][dig] + rank;
+        kb[pos] = key;
+        vb[pos] = va[i];
+      }
+      __syncthreads();
+      if (tid < 256) base[tid] += run;
+      __syncthreads();
+    }
+    unsigned long long* tk = ka;
+    ka = kb;
+    kb = tk;
+    unsigned* tv = va;
+    va = vb;
+    vb = tv;
+  }
+  for (unsigned i = tid; i < n; i += kSmallThreads) {
+    kout[i] = ka[i];
+    vout[i] = va[i];
+  }
 }
 
 // Sorts (keys, vals) of device count *n_ptr (clamped to cap) over the low
@@ -131,7 +218,7 @@ bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, un
     unsigned long long* ko = alt ? k0 : k1;
     unsigned* vo = alt ? v0 : v1;
     rs_hist_kernel<<<grid, kRsThreads, 0, st>>>(ki, n_ptr, cap, shift, hist);
-    scan_inplace_kernel<<<1, 1024, 0, st>>>(hist, 256u * grid, nullptr, nullptr);
+    scan_inplace_kernel<<<1, 1024, 0, st>>>(hist, 256u * grid, nullptr, nullptr, n_ptr);
     rs_scatter_kernel<<<grid, kRsThreads, 0, st>>>(ki, vi, ko, vo, n_ptr, cap, shift, hist);
     if (launches) *launches += 3;
     alt = !alt;
@@ -446,11 +533,19 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
   const unsigned cap = B.cap;
   const int gsort = B.sort_grid;
   const int g = grid_for(cap, 256, 4096);
-  // keys in canonical order
+  // keys in canonical order: one shared-memory block for small counts,
+  // multi-block LSD passes otherwise (each returns at once when not needed)
+  const bool alt = ((B.key_bits + 7) / 8) % 2 == 1;
+  {
+    const size_t shm = kSmallSort * (2 * sizeof(unsigned long long) + 2 * sizeof(unsigned));
+    cudaFuncSetAttribute(small_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    small_sort_kernel<<<1, kSmallThreads, shm, st>>>(B.key, B.count, cap, B.key_bits,
+                                                    alt ? B.key_alt : B.key, alt ? B.perm1 : B.perm0);
+  }
   iota_kernel<<<g, 256, 0, st>>>(B.perm0, B.count, cap);
-  const bool alt = radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits,
-                              B.hist, gsort, st, launches);
-  *launches += 3;  // iota, gather, expand
+  radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits, B.hist, gsort, st,
+             launches);
+  *launches += 4;  // small sort, iota, gather, expand
   const unsigned long long* skey = alt ? B.key_alt : B.key;
   const unsigned* perm = alt ? B.perm1 : B.perm0;
   gather_kernel<<<g, 256, 0, st>>>(B.count, cap, perm, B.lam, B.scalar, B.bary4, B.lam_sorted,
@@ -461,7 +556,7 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
   // star edges, written in (centre, other) order: already sorted and unique
   edges_regular_kernel<0><<<g, 128, 0, st>>>(mesh, nch, skey, B.count, cap, B.edge_cnt, nullptr,
                                              nullptr, 0);
-  scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count);
+  scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count, nullptr);
   edges_regular_kernel<1><<<g, 128, 0, st>>>(mesh, nch, skey, B.count, cap, nullptr, B.edge_cnt,
                                              B.edges, B.edge_cap);
   // trajectories

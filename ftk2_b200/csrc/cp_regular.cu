@@ -30,12 +30,13 @@ namespace ftk2b {
 __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=3 (60)
 
 // ---------------------------------------------------------------------------
-// Per-vertex cull word.
+// Per-vertex cull word (32 bits), computed with integer operations on the
+// high 32 bits of each value (the whole value for float).
 //
 //   bits 0..2   component j strongly positive:  v_j >  kappa' * b,  b = max_k |v_k|
 //   bits 3..5   component j strongly negative:  v_j < -kappa' * b
 //   bit  6      tiny: b < 4e-13
-//   bits 8..63  magnitude-band mask {n-1, n, n+1}, n = (exponent(b) - E_LO) / B
+//   bits 7..31  magnitude-band mask {n-1, n, n+1}, n = (exponent(b) - E_LO) / B
 //
 // The AND of the words of a set S of vertices is "culled" when
 //   (a) a sign bit survives and the band mask is non-zero: then every vertex
@@ -48,57 +49,73 @@ __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=
 //       2^-12 (float) that is impossible, so no simplex inside S is accepted.
 //   (b) or the tiny bit survives: the first pivot of the solve is below 1e-12
 //       (zero_crossing.hpp:72), so the solve rejects.
-// Vertices outside the mesh get ~0 (neutral under AND).
+// Each predicate is evaluated on high words so that it can only err towards
+// "not strong" / "not tiny": a strictly larger high word of a non-negative
+// IEEE value implies a strictly larger value, and kappa' * b only shifts the
+// exponent field.  Infinite or NaN components give 0 (never culled).  Vertices
+// outside the mesh get ~0 (neutral under AND).
 template <typename T> struct CullParams;
 template <> struct CullParams<double> {
-  static constexpr double kappa_prime = 1.0 / 4096.0;  // 2^-12
-  static constexpr int band = 4;                       // exponents per band
+  static constexpr int mant = 20;          // mantissa bits in the high word
+  static constexpr unsigned expmask = 0x7FF00000u;
+  static constexpr int bias = 1023;
+  static constexpr int kappa_exp = 12;     // kappa' = 2^-12
+  static constexpr int band = 4;           // exponents per band: kappa = 2^-24
+  static constexpr unsigned tiny_hi = 0x3D5C25C2u;  // high word of 4e-13 (rounded down)
 };
 template <> struct CullParams<float> {
-  static constexpr float kappa_prime = 1.0f / 64.0f;   // 2^-6
-  static constexpr int band = 2;
+  static constexpr int mant = 23;
+  static constexpr unsigned expmask = 0x7F800000u;
+  static constexpr int bias = 127;
+  static constexpr int kappa_exp = 3;      // kappa' = 2^-3
+  static constexpr int band = 3;           // kappa = 2^-12
+  static constexpr unsigned tiny_hi = 0x2AE12E13u;  // 4e-13f (3.99999993e-13)
 };
 constexpr int kElo = -42;      // 2^-42 < 4e-13: smaller magnitudes are "tiny"
-constexpr int kBands = 56;
-constexpr unsigned long long kAbsent = ~0ull;
+constexpr int kBands = 25;
+constexpr unsigned kAbsent = ~0u;
 
-__device__ __forceinline__ int exponent_of(double b) {
-  return (int)((__double_as_longlong(b) >> 52) & 0x7FF) - 1023;
+template <typename T> __device__ __forceinline__ unsigned hi_word(T v);
+template <> __device__ __forceinline__ unsigned hi_word<double>(double v) {
+  return (unsigned)__double2hiint(v);
 }
-__device__ __forceinline__ int exponent_of(float b) {
-  return (int)((__float_as_int(b) >> 23) & 0xFF) - 127;
+template <> __device__ __forceinline__ unsigned hi_word<float>(float v) {
+  return __float_as_uint(v);
 }
 
 template <typename T, int M>
-__device__ __forceinline__ unsigned long long vertex_word(const T v[M]) {
-  bool nan = false;
-  T b = T(0);
+__device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M]) {
+  using P = CullParams<T>;
+  unsigned a[M];
+  unsigned b = 0;
 #pragma unroll
   for (int j = 0; j < M; ++j) {
-    nan |= (v[j] != v[j]);
-    b = fmax(b, fabs(v[j]));
+    a[j] = h[j] & 0x7FFFFFFFu;
+    b = max(b, a[j]);
   }
-  if (nan) return 0ull;  // never culled
-  const T thr = b * CullParams<T>::kappa_prime;  // exact power-of-two scaling
-  unsigned long long w = 0;
+  if (b >= P::expmask) return 0u;  // inf or nan somewhere: never culled
+  const unsigned kexp = (unsigned)P::kappa_exp << P::mant;
+  const unsigned thr = b > kexp ? b - kexp : 0u;  // high word of kappa' * b
+  unsigned w = 0;
 #pragma unroll
   for (int j = 0; j < M; ++j) {
-    w |= (unsigned long long)(v[j] > thr) << j;
-    w |= (unsigned long long)(v[j] < -thr) << (3 + j);
+    const unsigned strong = a[j] > thr ? 1u : 0u;
+    const unsigned neg = h[j] >> 31;
+    w |= (strong & (neg ^ 1u)) << j;
+    w |= (strong & neg) << (3 + j);
   }
-  w |= (unsigned long long)(b < T(4e-13)) << 6;
-  const int rel = exponent_of(b) - kElo;
-  if (rel >= 0 && rel < kBands * CullParams<T>::band && b > T(0)) {
-    const int n = rel / CullParams<T>::band;
-    unsigned long long band = (7ull << n) >> 1;  // bits n-1, n, n+1
-    band &= (1ull << kBands) - 1;
-    w |= band << 8;
+  w |= (b < P::tiny_hi ? 1u : 0u) << 6;
+  const int rel = (int)(b >> P::mant) - P::bias - kElo;
+  if (rel >= 0 && rel < kBands * P::band) {
+    const int n = rel / P::band;
+    const unsigned band = ((7u << n) >> 1) & ((1u << kBands) - 1u);  // bits n-1, n, n+1
+    w |= band << 7;
   }
   return w;
 }
 
-__device__ __forceinline__ bool word_culled(unsigned long long w) {
-  return (((w & 0x3Full) != 0) && ((w >> 8) != 0)) || ((w & 0x40ull) != 0);
+__device__ __forceinline__ bool word_culled(unsigned w) {
+  return (((w & 0x3Fu) != 0) && ((w >> 7) != 0)) || ((w & 0x40u) != 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -231,8 +248,9 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   extern __shared__ __align__(128) unsigned char smem[];
   T* raw[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + bs.bytes)};
-  unsigned long long* W0 = reinterpret_cast<unsigned long long*>(smem + 2 * (size_t)bs.bytes);
+  unsigned* W0 = reinterpret_cast<unsigned*>(smem + 2 * (size_t)bs.bytes);
   __shared__ unsigned long long bar[2];
+  __shared__ int wait_failed;
 
   const ChainTable& CT = c_chains[D - 3];
   const int tid = threadIdx.x;
@@ -245,10 +263,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int y0 = (tix % cfg.tiles[1]) * TY;
   tix /= cfg.tiles[1];
   const int z0 = (D == 4) ? tix * TZ : 0;
-  const long long lt = mesh.ld[D - 1];
-  const long long t0 = (long long)blockIdx.y * cfg.tchunk;
-  const long long t1 = min(t0 + (long long)cfg.tchunk, lt);
-  const long long s_end = min(t1, lt - 1);  // last vertex slice this block reads
+  // time in int: local dims are below 2^16
+  const int lt = (int)mesh.ld[D - 1];
+  const int t0 = (int)blockIdx.y * cfg.tchunk;
+  const int t1 = min(t0 + cfg.tchunk, lt);
+  const int s_end = min(t1, lt - 1);  // last vertex slice this block reads
   // array coordinates of local (0,0,0,0): global for multicomponent arrays,
   // local for separate arrays
   long long aoff[4];
@@ -270,7 +289,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int comp_elems = (int)(bs.comp / sizeof(T));
 
   // ---- slice staging
-  auto issue = [&](long long s, int buf) {
+  auto issue = [&](int s, int buf) {
     if constexpr (TMA) {
       if (tid == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -301,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int vx = r % bs.vxbox;
         const int vy = (r / bs.vxbox) % VY;
         const int vz = r / (bs.vxbox * VY);
-        const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : s, s};
+        const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : (long long)s, (long long)s};
         bool in = true;
         long long o = 0;
         if (fa.per_vertex) {
@@ -326,34 +345,42 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     }
   };
-  auto wait = [&](long long s, int buf) -> bool {
+  auto wait = [&](int s, int buf) -> bool {
     if constexpr (TMA) {
-      const unsigned parity = (unsigned)(((s - t0) >> 1) & 1);
-      const bool ok = mbar_wait(&bar[buf], parity);
-      return !__syncthreads_or(!ok);
+      // one warp polls the barrier; the rest of the block waits at the
+      // block barrier without issuing instructions
+      if (warp == 0) {
+        const bool ok = mbar_wait(&bar[buf], (unsigned)(((s - t0) >> 1) & 1));
+        if (lane == 0) wait_failed = ok ? 0 : 1;
+      }
+      __syncthreads();
+      return wait_failed == 0;
     } else {
       __syncthreads();
       return true;
     }
   };
-  auto words = [&](int buf, unsigned long long* dst) {
-    const T* r = raw[buf];
+  // high 32-bit word of each element (the element itself for float)
+  constexpr int HW = sizeof(T) / 4;
+  auto words = [&](int buf, unsigned* dst) {
+    const unsigned* r = reinterpret_cast<const unsigned*>(raw[buf]) + (HW - 1);
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
       const int i = tid + u * kThreads;
       if (i < VS) {
-        unsigned long long w = kAbsent;
+        unsigned w = kAbsent;
         if (voff[u] >= 0) {
-          T v[M];
+          unsigned h[M];
 #pragma unroll
-          for (int j = 0; j < M; ++j) v[j] = bs.multi ? r[voff[u] + j] : r[voff[u] + j * comp_elems];
-          w = vertex_word<T, M>(v);
+          for (int j = 0; j < M; ++j)
+            h[j] = r[HW * (bs.multi ? voff[u] + j : voff[u] + j * comp_elems)];
+          w = vertex_word_hi<T, M>(h);
         }
         dst[i] = w;
       }
     }
   };
-  auto W = [&](long long s) -> unsigned long long* { return W0 + (size_t)((s - t0) % 3) * VS; };
+  auto W = [&](int s) -> unsigned* { return W0 + ((s - t0) % 3) * VS; };
 
   if constexpr (TMA) {
     if (tid == 0) {
@@ -369,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
   if (!wait(t0, 0)) {
     // give the other copy in flight a bounded chance to land before leaving
-    if (TMA && t0 + 1 <= s_end) mbar_wait(&bar[1], 0);
+    if (TMA && t0 + 1 <= s_end && warp == 0) mbar_wait(&bar[1], 0);
     if (tid == 0) atomicOr(err, 2u);
     return;
   }
@@ -377,14 +404,26 @@ __global__ void __launch_bounds__(kThreads, 2)
   __syncthreads();
   if (TMA && t0 + 2 <= s_end) issue(t0 + 2, 0);
 
-  for (long long ct = t0; ct < t1; ++ct) {
-    const long long s = ct + 1;
-    unsigned long long* B = W(s);
+  // corner validity per (lane, row) does not change along time
+  const int cyw = (D == 4) ? warp % TY : warp * kRows;
+  const int czw = (D == 4) ? (warp / TY) * kRows : 0;
+  unsigned row_valid = 0;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const int cy = (D == 4) ? cyw : cyw + q;
+    const int cz = (D == 4) ? czw + q : 0;
+    if (x0 + lane < mesh.ld[0] && y0 + cy < mesh.ld[1] && (D == 3 || z0 + cz < mesh.ld[2]))
+      row_valid |= 1u << q;
+  }
+
+  for (int ct = t0; ct < t1; ++ct) {
+    const int s = ct + 1;
+    unsigned* B = W(s);
     if (s <= s_end) {
-      const int buf = (int)((s - t0) & 1);
+      const int buf = (s - t0) & 1;
       if (!TMA) issue(s, buf);
       if (!wait(s, buf)) {
-        if (TMA && s + 1 <= s_end) mbar_wait(&bar[buf ^ 1], (unsigned)(((s + 1 - t0) >> 1) & 1));
+        if (TMA && s + 1 <= s_end && warp == 0) mbar_wait(&bar[buf ^ 1], (unsigned)(((s + 1 - t0) >> 1) & 1));
         if (tid == 0) atomicOr(err, 2u);
         return;
       }
@@ -393,16 +432,14 @@ __global__ void __launch_bounds__(kThreads, 2)
       for (int i = tid; i < VS; i += kThreads) B[i] = kAbsent;
     }
     __syncthreads();
-    if (TMA && s + 2 <= s_end) issue(s + 2, (int)((s - t0) & 1));
+    if (TMA && s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
 
     // ---- hypercube cull: lanes along x, kRows corner rows per warp
-    const unsigned long long* A = W(ct);
-    const int cyw = (D == 4) ? warp % TY : warp * kRows;
-    const int czw = (D == 4) ? (warp / TY) * kRows : 0;
-    unsigned long long R[kRows + 1];
+    const unsigned* A = W(ct);
+    unsigned R[kRows + 1];
 #pragma unroll
     for (int q = 0; q <= kRows; ++q) {
-      unsigned long long r, e = kAbsent;
+      unsigned r, e = kAbsent;
       if constexpr (D == 4) {
         const int i0 = ((czw + q) * VY + cyw) * VX + lane, i1 = i0 + VX;
         r = A[i0] & A[i1] & B[i0] & B[i1];
@@ -412,21 +449,19 @@ __global__ void __launch_bounds__(kThreads, 2)
         r = A[i0] & B[i0];
         if (lane == 31) e = A[i0 + 1] & B[i0 + 1];
       }
-      const unsigned long long nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
+      const unsigned nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
       R[q] = r & (lane == 31 ? e : nb);
     }
 #pragma unroll
     for (int q = 0; q < kRows; ++q) {
       const int cy = (D == 4) ? cyw : cyw + q;
       const int cz = (D == 4) ? czw + q : 0;
-      const bool valid = x0 + lane < mesh.ld[0] && y0 + cy < mesh.ld[1] &&
-                         (D == 3 || z0 + cz < mesh.ld[2]);
-      unsigned ball = __ballot_sync(0xFFFFFFFFu, valid && !word_culled(R[q] & R[q + 1]));
+      unsigned ball = __ballot_sync(0xFFFFFFFFu, ((row_valid >> q) & 1u) && !word_culled(R[q] & R[q + 1]));
       while (ball) {
         // one surviving hypercube at a time: lanes test its chains
         const int cx = __ffs(ball) - 1;
         ball &= ball - 1;
-        const long long l[4] = {x0 + cx, y0 + cy, (D == 4) ? z0 + cz : ct, ct};
+        const long long l[4] = {x0 + cx, y0 + cy, (D == 4) ? z0 + cz : (long long)ct, (long long)ct};
         int vmask = 0;  // axes along which the corner can step by +1
 #pragma unroll
         for (int k = 0; k < D; ++k)
@@ -436,7 +471,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           const int ch = base + lane;
           bool ok = false;
           if (ch < CT.n && (CT.mask[ch][M - 1] & ~vmask) == 0) {
-            unsigned long long wacc = (A[((cz * VY) + cy) * VX + cx]);
+            unsigned wacc = A[((cz * VY) + cy) * VX + cx];
 #pragma unroll
             for (int i = 0; i < M; ++i) {
               const int mk = CT.mask[ch][i];
@@ -699,7 +734,7 @@ static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, cons
       tma = encode_map(&maps[j], sizeof(T) == 8, fa.comp[j], D, dims, strides, box);
   }
   if (used_tma) *used_tma = tma ? 1 : 0;
-  const size_t words = 3 * sizeof(unsigned long long) * (size_t)(Tile<D>::TX + 1) * VY * VZ;
+  const size_t words = 3 * sizeof(unsigned) * (size_t)(Tile<D>::TX + 1) * VY * VZ;
   const size_t shm = 2 * (size_t)bs.bytes + words;
   const long long lt = mesh.ld[D - 1];
   const unsigned nchunks = (unsigned)((lt + cfg.tchunk - 1) / cfg.tchunk);

@@ -142,7 +142,8 @@ ftk2b_cp_params ftk2b_cp_params_default(void);
 enum {
   FTK2B_OPT_FEATURE_CAPACITY = 1, /* initial feature capacity; grows on overflow */
   FTK2B_OPT_TIME_CHUNK = 2,       /* time steps per extraction block (0 = all) */
-  FTK2B_OPT_DISABLE_TMA = 3       /* 1: stage slices with plain loads instead of TMA */
+  FTK2B_OPT_DISABLE_TMA = 3,      /* 1: stage slices with plain loads instead of TMA */
+  FTK2B_OPT_USE_GRAPHS = 4        /* 1 (default): replay the device pipeline as a CUDA graph */
 };
 ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
 /* Reads an option back, or FTK2B_INFO_LAST_TMA: 1 when the last regular-mesh

@@ -138,6 +138,19 @@ def test_device_input_matches_host_input(ctx):
     assert_identical(devr, again)
 
 
+def test_graph_replay_and_eager_agree(ctx):
+    case = cases.GOLDEN_CASES["f32_3d_noise_offset"]()
+    a = gpu_run(ctx, case)
+    b = gpu_run(ctx, case)          # replayed graph
+    ctx.set_option(api.OPT_USE_GRAPHS, 0)
+    try:
+        c = gpu_run(ctx, case)      # eager launches
+    finally:
+        ctx.set_option(api.OPT_USE_GRAPHS, 1)
+    assert_identical(a, b)
+    assert_identical(a, c)
+
+
 def test_overflow_retry(ctx):
     case = cases.c1_analytic_2d()
     ctx.set_option(api.OPT_FEATURE_CAPACITY, 100)  # far below the 3697 features
