@@ -194,7 +194,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   std::vector<DevBuf*> v = {&stage[0], &stage[1], &stage[2], &stage_scalar, &key, &lam, &bary4,
                             &scalar, &key_alt, &perm0, &perm1, &hist, &lam_s, &bary4_s, &scalar_s,
                             &simplices, &bary, &track, &edge_cnt, &edges, &parent, &counters,
-                            &cls, &cand_corner, &cand_chains};
+                            &cls, &cand_corner, &cand_chains, &edge_slots};
   for (auto& b : extra) v.push_back(&b);
   return v;
 }
@@ -397,6 +397,7 @@ ftk2b_status ftk2b::ensure_feature_buffers(ftk2b_ctx* ctx, unsigned cap, unsigne
   CUDA_TRY(ctx, ctx->parent.ensure(sizeof(unsigned) * cap));
   CUDA_TRY(ctx, ctx->cls.ensure(sizeof(unsigned) * cap));
   CUDA_TRY(ctx, ctx->edges.ensure(sizeof(unsigned) * 2 * (size_t)edge_cap));
+  CUDA_TRY(ctx, ctx->edge_slots.ensure(sizeof(unsigned) * 8 * (size_t)cap));
   CUDA_TRY(ctx, ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
   const int grid = ctx->sort_grid(cap);
   CUDA_TRY(ctx, ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)grid));
@@ -431,6 +432,7 @@ PostBuffers ftk2b_ctx::post_buffers(unsigned cap_, unsigned edge_cap_, int key_b
   B.track = (unsigned long long*)track.p;
   B.edge_cnt = (unsigned*)edge_cnt.p;
   B.edges = (unsigned*)edges.p;
+  B.edge_slots = (unsigned*)edge_slots.p;
   B.parent = (unsigned*)parent.p;
   B.cls = (unsigned*)cls.p;
   return B;

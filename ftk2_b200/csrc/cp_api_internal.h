@@ -57,7 +57,7 @@ struct ftk2b_ctx {
   int last_used_tma = 0;
   ftk2b::DevBuf stage[3], stage_scalar;
   ftk2b::DevBuf key, lam, bary4, scalar, key_alt, perm0, perm1, hist, lam_s, bary4_s, scalar_s,
-      simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains;
+      simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains, edge_slots;
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::LastRun last;
   // CUDA graph of the last regular-mesh pipeline

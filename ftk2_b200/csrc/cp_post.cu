@@ -25,15 +25,11 @@ __constant__ signed char c_rank4[4096];   // (m1 | m2 << 4 | m3 << 8) -> chain r
 // radix sort (keys u64, payload u32), stable, device-resident count
 
 constexpr int kRsThreads = 256;
-// counts up to this size are sorted by one block in shared memory
-constexpr unsigned kSmallSort = 8192;
-constexpr int kSmallThreads = 512;
 
 __global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
                                unsigned cap, int shift, unsigned* __restrict__ hist) {
   __shared__ unsigned h[256];
   const unsigned n = min(*n_ptr, cap);
-  if (n <= kSmallSort) return;
   const unsigned G = gridDim.x, b = blockIdx.x;
   const unsigned chunk = (n + G - 1) / G;
   const unsigned start = min(b * chunk, n), end = min(start + chunk, n);
@@ -50,7 +46,7 @@ __global__ void scan_inplace_kernel(unsigned* __restrict__ a, unsigned total, un
                                     const unsigned* n_ptr, const unsigned* skip_small) {
   __shared__ unsigned part[1024];
   const unsigned t = threadIdx.x;
-  if (skip_small && min(*skip_small, total) <= kSmallSort) return;
+  (void)skip_small;
   if (n_ptr) total = min(total, *n_ptr);
   const unsigned seg = (total + 1023) / 1024;
   const unsigned s0 = min(t * seg, total), s1 = min(s0 + seg, total);
@@ -81,7 +77,6 @@ __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
   __shared__ unsigned base[256];
   __shared__ unsigned wcnt[kRsThreads / 32][256];
   const unsigned n = min(*n_ptr, cap);
-  if (n <= kSmallSort) return;
   const unsigned G = gridDim.x, b = blockIdx.x;
   const unsigned chunk = (n + G - 1) / G;
   const unsigned start = min(b * chunk, n), end = min(start + chunk, n);
@@ -121,88 +116,7 @@ __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
 
 __global__ void iota_kernel(unsigned* v, const unsigned* n_ptr, unsigned cap) {
   const unsigned n = min(*n_ptr, cap);
-  if (n <= kSmallSort) return;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
-}
-
-// One block sorts up to kSmallSort keys in shared memory (stable LSD radix,
-// 8-bit digits), writing sorted keys and the permutation to (kout, vout),
-// which may alias the input keys.  Larger counts leave it to the multi-block
-// passes, which in turn return immediately for small counts.
-__global__ void __launch_bounds__(kSmallThreads)
-    small_sort_kernel(const unsigned long long* kin, const unsigned* n_ptr, unsigned cap, int bits,
-                      unsigned long long* kout, unsigned* vout) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  unsigned long long* ka = reinterpret_cast<unsigned long long*>(sm);
-  unsigned long long* kb = ka + kSmallSort;
-  unsigned* va = reinterpret_cast<unsigned*>(kb + kSmallSort);
-  unsigned* vb = va + kSmallSort;
-  __shared__ unsigned wcnt[kSmallThreads / 32][256];
-  __shared__ unsigned base[256];
-  const unsigned n = min(*n_ptr, cap);
-  if (n > kSmallSort) return;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (unsigned i = tid; i < n; i += kSmallThreads) {
-    ka[i] = kin[i];
-    va[i] = i;
-  }
-  __syncthreads();
-  for (int shift = 0; shift < bits; shift += 8) {
-    // digit totals -> exclusive bases
-    if (tid < 256) base[tid] = 0;
-    __syncthreads();
-    for (unsigned i = tid; i < n; i += kSmallThreads) atomicAdd(&base[(ka[i] >> shift) & 255], 1u);
-    __syncthreads();
-    if (tid == 0) {
-      unsigned run = 0;
-      for (int d = 0; d < 256; ++d) {
-        const unsigned c = base[d];
-        base[d] = run;
-        run += c;
-      }
-    }
-    __syncthreads();
-    // stable scatter, one chunk of kSmallThreads items at a time
-    for (unsigned c0 = 0; c0 < n; c0 += kSmallThreads) {
-      const unsigned i = c0 + tid;
-      const bool valid = i < n;
-      const unsigned long long key = valid ? ka[i] : 0ull;
-      const unsigned dig = valid ? (unsigned)((key >> shift) & 255) : 256u;
-      for (int d = tid; d < (kSmallThreads / 32) * 256; d += kSmallThreads) (&wcnt[0][0])[d] = 0;
-      __syncthreads();
-      const unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
-      const unsigned rank = __popc(peers & ((1u << lane) - 1));
-      if (valid && lane == __ffs(peers) - 1) wcnt[warp][dig] = __popc(peers);
-      __syncthreads();
-      unsigned run = 0;
-      if (tid < 256) {
-        for (int w = 0; w < kSmallThreads / 32; ++w) {
-          const unsigned c = wcnt[w][tid];
-          wcnt[w][tid] = run;
-          run += c;
-        }
-      }
-      __syncthreads();
-      if (valid) {
-        const unsigned pos = base[dig] + wcnt[warp][dig] + rank;
-        kb[pos] = key;
-        vb[pos] = va[i];
-      }
-      __syncthreads();
-      if (tid < 256) base[tid] += run;
-      __syncthreads();
-    }
-    unsigned long long* tk = ka;
-    ka = kb;
-    kb = tk;
-    unsigned* tv = va;
-    va = vb;
-    vb = tv;
-  }
-  for (unsigned i = tid; i < n; i += kSmallThreads) {
-    kout[i] = ka[i];
-    vout[i] = va[i];
-  }
 }
 
 // Sorts (keys, vals) of device count *n_ptr (clamped to cap) over the low
@@ -361,6 +275,92 @@ __device__ int active_faces(const RegularMesh& mesh, int nch, const unsigned lon
       out[j - 1] = t;
     }
   return na;
+}
+
+constexpr int kEdgeSlots = 8;  // a codimension-1 simplex has 2 cofaces with <= 4 other faces each
+
+// Index of the face of top cell (cc, cm) without vertex r, or -1.
+__device__ __forceinline__ long long face_index(const RegularMesh& mesh, int nch,
+                                                const unsigned long long* keys, unsigned n,
+                                                const long long cc[4], const int cm[5], int r) {
+  const int d = mesh.d;
+  const int basem = (r == 0) ? cm[1] : 0;
+  int rel[4];
+  int w = 0;
+  for (int i = 0; i <= d; ++i) {
+    if (i == r || (r == 0 && i == 1) || (r != 0 && i == 0)) continue;
+    rel[w++] = cm[i] & ~basem;
+  }
+  unsigned long long vid = 0;
+  for (int k = 0; k < d; ++k) vid += (unsigned long long)(cc[k] + ((basem >> k) & 1)) * mesh.gstride[k];
+  return find_key(keys, n, vid * (unsigned long long)nch + (unsigned long long)chain_rank(d, rel));
+}
+
+// One warp per feature: lanes look up the faces of both cofaces in parallel;
+// when the feature is the smallest active face of a cell it writes the star
+// edges to its other active faces into padded slots (ascending), and its
+// edge count.
+__global__ void edges_regular_warp_kernel(RegularMesh mesh, int nch,
+                                          const unsigned long long* __restrict__ keys,
+                                          const unsigned* n_ptr, unsigned cap,
+                                          unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+  const unsigned n = min(*n_ptr, cap);
+  const int lane = threadIdx.x & 31;
+  const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  const int d = mesh.d;
+  for (unsigned i = gw; i < n; i += nw) {
+    Decoded dc;
+    decode_key(mesh, nch, keys[i], dc);
+    long long cc[2][4];
+    int cm[2][5];
+    const int nc = top_cells(mesh, dc, cc, cm);
+    long long idx = -1;
+    const int q = lane / (d + 1), r = lane % (d + 1);
+    if (lane < nc * (d + 1)) idx = face_index(mesh, nch, keys, n, cc[q], cm[q], r);
+    const unsigned act = __ballot_sync(0xFFFFFFFFu, idx >= 0);
+    unsigned others[kEdgeSlots];
+    int no = 0;
+    for (int qq = 0; qq < nc; ++qq) {
+      const unsigned cellmask = ((1u << (d + 1)) - 1u) << (qq * (d + 1));
+      const unsigned a = act & cellmask;
+      const unsigned v = ((a >> lane) & 1u) ? (unsigned)idx : 0xFFFFFFFFu;
+      const unsigned mn = __reduce_min_sync(0xFFFFFFFFu, v);
+      if (__popc(a) < 2 || mn != i) continue;
+      for (unsigned bits = a; bits; bits &= bits - 1) {
+        const unsigned val = __shfl_sync(0xFFFFFFFFu, (unsigned)idx, __ffs(bits) - 1);
+        if (val != i && no < kEdgeSlots) others[no++] = val;
+      }
+    }
+    if (lane == 0) {
+      for (int a2 = 1; a2 < no; ++a2)
+        for (int b2 = a2; b2 > 0 && others[b2 - 1] > others[b2]; --b2) {
+          const unsigned t = others[b2];
+          others[b2] = others[b2 - 1];
+          others[b2 - 1] = t;
+        }
+      cnt[i] = no;
+      for (int k = 0; k < no; ++k) slots[(size_t)i * kEdgeSlots + k] = others[k];
+    }
+  }
+}
+
+// After the exclusive scan of the counts (in place), copy every feature's
+// edges to their final positions: (centre, other) pairs, sorted and unique.
+__global__ void edges_compact_kernel(const unsigned* n_ptr, unsigned cap, const unsigned* __restrict__ off,
+                                     const unsigned* n_edges, const unsigned* __restrict__ slots,
+                                     unsigned* __restrict__ edges, unsigned edge_cap) {
+  const unsigned n = min(*n_ptr, cap);
+  const unsigned ne = *n_edges;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned o = off[i];
+    const unsigned c = (i + 1 < n ? off[i + 1] : ne) - o;
+    for (unsigned k = 0; k < c; ++k)
+      if (o + k < edge_cap) {
+        edges[2 * (size_t)(o + k)] = i;
+        edges[2 * (size_t)(o + k) + 1] = slots[(size_t)i * kEdgeSlots + k];
+      }
+  }
 }
 
 // pass 0: count edges per feature (as star centre); pass 1: write them
@@ -533,19 +533,11 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
   const unsigned cap = B.cap;
   const int gsort = B.sort_grid;
   const int g = grid_for(cap, 256, 4096);
-  // keys in canonical order: one shared-memory block for small counts,
-  // multi-block LSD passes otherwise (each returns at once when not needed)
-  const bool alt = ((B.key_bits + 7) / 8) % 2 == 1;
-  {
-    const size_t shm = kSmallSort * (2 * sizeof(unsigned long long) + 2 * sizeof(unsigned));
-    cudaFuncSetAttribute(small_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    small_sort_kernel<<<1, kSmallThreads, shm, st>>>(B.key, B.count, cap, B.key_bits,
-                                                    alt ? B.key_alt : B.key, alt ? B.perm1 : B.perm0);
-  }
+  // keys in canonical order: multi-block stable LSD radix passes
   iota_kernel<<<g, 256, 0, st>>>(B.perm0, B.count, cap);
-  radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits, B.hist, gsort, st,
-             launches);
-  *launches += 4;  // small sort, iota, gather, expand
+  const bool alt = radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits, B.hist,
+                              gsort, st, launches);
+  *launches += 3;  // iota, gather, expand
   const unsigned long long* skey = alt ? B.key_alt : B.key;
   const unsigned* perm = alt ? B.perm1 : B.perm0;
   gather_kernel<<<g, 256, 0, st>>>(B.count, cap, perm, B.lam, B.scalar, B.bary4, B.lam_sorted,
@@ -554,11 +546,14 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
                                            B.simplices, B.bary);
   if (!want_edges) return cudaGetLastError();
   // star edges, written in (centre, other) order: already sorted and unique
-  edges_regular_kernel<0><<<g, 128, 0, st>>>(mesh, nch, skey, B.count, cap, B.edge_cnt, nullptr,
-                                             nullptr, 0);
+  {
+    const int gw = grid_for(cap, 8, 8192);  // one warp per feature, 8 warps per block
+    edges_regular_warp_kernel<<<gw, 256, 0, st>>>(mesh, nch, skey, B.count, cap, B.edge_cnt,
+                                                  B.edge_slots);
+  }
   scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count, nullptr);
-  edges_regular_kernel<1><<<g, 128, 0, st>>>(mesh, nch, skey, B.count, cap, nullptr, B.edge_cnt,
-                                             B.edges, B.edge_cap);
+  edges_compact_kernel<<<g, 256, 0, st>>>(B.count, cap, B.edge_cnt, B.n_edges, B.edge_slots, B.edges,
+                                          B.edge_cap);
   // trajectories
   uf_init_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap);
   const int ge = grid_for(B.edge_cap, 256, 4096);

@@ -30,6 +30,7 @@ struct PostBuffers {
   unsigned long long* track;
   unsigned* edge_cnt;               // per feature, scanned in place into offsets
   unsigned* edges;                  // 2 per edge
+  unsigned* edge_slots;             // 8 per feature: star edges before compaction
   unsigned* n_edges;
   unsigned* parent;
   unsigned* n_roots;

@@ -83,35 +83,45 @@ template <> __device__ __forceinline__ unsigned hi_word<float>(float v) {
   return __float_as_uint(v);
 }
 
-template <typename T, int M>
-__device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M]) {
+// Band masks by magnitude exponent: band_table[rel + 1] for rel = biased
+// exponent - bias - E_LO; 0 outside the banded window (and at index 0).
+constexpr int kBandTable = 128;
+
+template <typename T>
+__device__ __forceinline__ void fill_band_table(unsigned* tbl, int tid, int nthreads) {
   using P = CullParams<T>;
-  unsigned a[M];
+  for (int i = tid; i < kBandTable; i += nthreads) {
+    const int rel = i - 1;
+    unsigned w = 0;
+    if (rel >= 0 && rel < kBands * P::band) {
+      const int n = rel / P::band;
+      w = (((7u << n) >> 1) & ((1u << kBands) - 1u)) << 7;  // bits n-1, n, n+1
+    }
+    tbl[i] = w;
+  }
+}
+
+template <typename T, int M>
+__device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M], const unsigned* band_tbl) {
+  using P = CullParams<T>;
   unsigned b = 0;
 #pragma unroll
-  for (int j = 0; j < M; ++j) {
-    a[j] = h[j] & 0x7FFFFFFFu;
-    b = max(b, a[j]);
-  }
-  if (b >= P::expmask) return 0u;  // inf or nan somewhere: never culled
+  for (int j = 0; j < M; ++j) b = max(b, h[j] & 0x7FFFFFFFu);
   const unsigned kexp = (unsigned)P::kappa_exp << P::mant;
   const unsigned thr = b > kexp ? b - kexp : 0u;  // high word of kappa' * b
   unsigned w = 0;
 #pragma unroll
   for (int j = 0; j < M; ++j) {
-    const unsigned strong = a[j] > thr ? 1u : 0u;
-    const unsigned neg = h[j] >> 31;
-    w |= (strong & (neg ^ 1u)) << j;
-    w |= (strong & neg) << (3 + j);
+    // positive and |v| > thr  <=>  (int)h > (int)thr  (thr >= 0)
+    // negative and |v| > thr  <=>  h > thr | sign bit   (unsigned)
+    w |= ((int)h[j] > (int)thr ? 1u : 0u) << j;
+    w |= (h[j] > (thr | 0x80000000u) ? 1u : 0u) << (3 + j);
   }
   w |= (b < P::tiny_hi ? 1u : 0u) << 6;
-  const int rel = (int)(b >> P::mant) - P::bias - kElo;
-  if (rel >= 0 && rel < kBands * P::band) {
-    const int n = rel / P::band;
-    const unsigned band = ((7u << n) >> 1) & ((1u << kBands) - 1u);  // bits n-1, n, n+1
-    w |= band << 7;
-  }
-  return w;
+  const int rel1 = (int)(b >> P::mant) - P::bias - kElo + 1;
+  w |= band_tbl[min((unsigned)rel1, (unsigned)(kBandTable - 1))];
+  // inf or nan somewhere: never culled
+  return b >= P::expmask ? 0u : w;
 }
 
 __device__ __forceinline__ bool word_culled(unsigned w) {
@@ -251,6 +261,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   unsigned* W0 = reinterpret_cast<unsigned*>(smem + 2 * (size_t)bs.bytes);
   __shared__ unsigned long long bar[2];
   __shared__ int wait_failed;
+  __shared__ unsigned band_tbl[kBandTable];
 
   const ChainTable& CT = c_chains[D - 3];
   const int tid = threadIdx.x;
@@ -287,6 +298,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
   }
   const int comp_elems = (int)(bs.comp / sizeof(T));
+  fill_band_table<T>(band_tbl, tid, kThreads);  // visible after the first barrier below
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
@@ -374,7 +386,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
           for (int j = 0; j < M; ++j)
             h[j] = r[HW * (bs.multi ? voff[u] + j : voff[u] + j * comp_elems)];
-          w = vertex_word_hi<T, M>(h);
+          w = vertex_word_hi<T, M>(h, band_tbl);
         }
         dst[i] = w;
       }
@@ -392,6 +404,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     issue(t0, 0);
     if (t0 + 1 <= s_end) issue(t0 + 1, 1);
   } else {
+    __syncthreads();
     issue(t0, 0);
   }
   if (!wait(t0, 0)) {
@@ -495,18 +508,24 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
-// Stage 2: exact SoS test and bit-exact solve of every queued chain, one warp
-// per candidate hypercube, accepted simplices compacted by warp ballot.
+// Stage 2: exact SoS test and bit-exact solve of the queued chains.  One warp
+// per candidate hypercube: its 2^D vertices' values are gathered once into
+// shared memory, then each lane tests one chain; accepted simplices are
+// compacted by warp ballot.
+constexpr int kRefineWarps = 8;
+
 template <typename T, int D>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kRefineWarps * 32, 2)
     refine_regular_kernel(RegularMesh mesh, FieldAccess fa, ExtractConfig cfg, CandidateQueue cq,
                           FeatureSink sink) {
   constexpr int M = D - 1;
+  constexpr int NV = 1 << D;
+  __shared__ T cube[kRefineWarps][NV][M];
   const ChainTable& CT = c_chains[D - 3];
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const unsigned n = min(*cq.count, cq.cap);
-  const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  const unsigned gw = blockIdx.x * kRefineWarps + wib;
+  const unsigned nw = gridDim.x * kRefineWarps;
   for (unsigned c = gw; c < n; c += nw) {
     const unsigned long long pc = cq.corner[c];
     const unsigned long long chains = cq.chains[c];
@@ -516,11 +535,28 @@ __global__ void __launch_bounds__(256)
     unsigned long long vid0 = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      // D = 3: the time coordinate sits in slot 2
+      // D = 3: the time coordinate is the third axis
       const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
       g0[k] = (k < D) ? lk + mesh.off[k] : 0;
       if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
     }
+    // gather the hypercube's vertex values (only vertices inside the mesh)
+    for (int e = lane; e < NV * M; e += 32) {
+      const int v = e / M, j = e % M;
+      long long g[4];
+      unsigned long long vid = 0;
+      bool in = true;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
+        if (k < D) {
+          in &= g[k] - mesh.off[k] < mesh.ld[k];
+          vid += (unsigned long long)g[k] * mesh.gstride[k];
+        }
+      }
+      cube[wib][v][j] = in ? field_at<T>(fa, j, g, D, vid) : T(0);
+    }
+    __syncwarp();
     for (int base = 0; base < CT.n; base += 32) {
       const int ch = base + lane;
       bool acc = false;
@@ -533,19 +569,10 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int i = 0; i < M; ++i) mk[i + 1] = CT.mask[ch][i];
         T vals[M + 1][M];
-        long long gv[M + 1][4];
-        unsigned long long vid[M + 1];
 #pragma unroll
-        for (int i = 0; i <= M; ++i) {
-          vid[i] = 0;
+        for (int i = 0; i <= M; ++i)
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            gv[i][k] = (k < D) ? g0[k] + ((mk[i] >> k) & 1) : 0;
-            if (k < D) vid[i] += (unsigned long long)gv[i][k] * mesh.gstride[k];
-          }
-#pragma unroll
-          for (int j = 0; j < M; ++j) vals[i][j] = field_at<T>(fa, j, gv[i], D, vid[i]);
-        }
+          for (int j = 0; j < M; ++j) vals[i][j] = cube[wib][mk[i]][j];
         bool inside;
         if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
         else inside = sos_inside3<T>(vals, cfg.Q);
@@ -562,8 +589,16 @@ __global__ void __launch_bounds__(256)
               using F = fp<T>;
               T sc = T(0);
 #pragma unroll
-              for (int i = 0; i <= M; ++i)
-                sc = F::add(sc, F::mul(lam[i], scalar_at<T>(fa, gv[i], D, vid[i])));
+              for (int i = 0; i <= M; ++i) {
+                long long gv[4];
+                unsigned long long vid = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                  gv[k] = (k < D) ? g0[k] + ((mk[i] >> k) & 1) : 0;
+                  if (k < D) vid += (unsigned long long)gv[k] * mesh.gstride[k];
+                }
+                sc = F::add(sc, F::mul(lam[i], scalar_at<T>(fa, gv, D, vid)));
+              }
               sc_out = (float)sc;
             }
             if (cfg.refined) {
@@ -595,6 +630,7 @@ __global__ void __launch_bounds__(256)
         }
       }
     }
+    __syncwarp();
   }
 }
 
@@ -780,13 +816,14 @@ cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const Field
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
                                   const ExtractConfig& cfg, const CandidateQueue& cq,
                                   const FeatureSink& sink, int num_sms, cudaStream_t st) {
-  const int blocks = num_sms * 4;
+  const int blocks = num_sms * 8;
+  const int thr = kRefineWarps * 32;
   if (mesh.d == 4) {
-    if (f64) refine_regular_kernel<double, 4><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
-    else refine_regular_kernel<float, 4><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
+    if (f64) refine_regular_kernel<double, 4><<<blocks, thr, 0, st>>>(mesh, fa, cfg, cq, sink);
+    else refine_regular_kernel<float, 4><<<blocks, thr, 0, st>>>(mesh, fa, cfg, cq, sink);
   } else {
-    if (f64) refine_regular_kernel<double, 3><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
-    else refine_regular_kernel<float, 3><<<blocks, 256, 0, st>>>(mesh, fa, cfg, cq, sink);
+    if (f64) refine_regular_kernel<double, 3><<<blocks, thr, 0, st>>>(mesh, fa, cfg, cq, sink);
+    else refine_regular_kernel<float, 3><<<blocks, thr, 0, st>>>(mesh, fa, cfg, cq, sink);
   }
   return cudaGetLastError();
 }
