@@ -28,6 +28,9 @@
 namespace ftk2b {
 
 __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=3 (60)
+// chains whose vertices all stay inside the mesh, by the mask of axes along
+// which a corner may step: [0][vmask] for d = 3, [1][vmask] for d = 4
+__constant__ unsigned long long c_chains_by_vmask[2][16];
 
 // ---------------------------------------------------------------------------
 // Per-vertex cull word (32 bits), computed with integer operations on the
@@ -221,16 +224,35 @@ template <> struct Tile<3> {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRows = 2;  // corner rows a warp culls per step
-constexpr int kMaxVXBox = 36;
 
-// Shape of one time slice of a tile in shared memory, as the TMA box lays it
-// out: multicomponent [VZ][VY][VXBOX * M], separate arrays [M][VZ][VY][VXBOX].
-struct BoxShape {
-  int vxbox;       // x extent of the box (>= TX + 1, padded to 16-byte rows)
-  int multi;       // 1: interleaved components
-  unsigned comp;   // bytes of one component box (separate arrays)
-  unsigned bytes;  // bytes of one slice buffer (all components, 128-byte padded)
-  unsigned tx;     // bytes the TMA copies of one slice deliver
+// Compile-time geometry of one block's time slice in shared memory, as the
+// TMA box lays it out: multicomponent [VZ][VY][VXBOX * M], separate arrays
+// [M][VZ][VY][VXBOX] (each component padded to 128 bytes).  VXBOX >= TX + 1
+// is padded so every box row is a multiple of 16 bytes.
+__host__ __device__ constexpr int vxbox_of(bool multi, int m, int es) {
+  return ((33 * (multi ? m : 1) * es) % 16 == 0)   ? 33
+         : ((34 * (multi ? m : 1) * es) % 16 == 0) ? 34
+         : ((35 * (multi ? m : 1) * es) % 16 == 0) ? 35
+                                                     : 36;
+}
+__host__ __device__ constexpr int round128(int b) { return (b + 127) & ~127; }
+
+template <typename T, int D, bool MULTI>
+struct Geo {
+  static constexpr int M = D - 1;
+  static constexpr int TX = Tile<D>::TX, TY = Tile<D>::TY, TZ = Tile<D>::TZ;
+  static constexpr int VX = TX + 1, VY = TY + 1, VZ = (D == 4) ? TZ + 1 : 1;
+  static constexpr int VS = VX * VY * VZ;                     // vertex slots of a slice
+  static constexpr int VPT = (VS + kThreads - 1) / kThreads;  // slots per thread
+  static constexpr int VSP = VPT * kThreads;                  // padded slots
+  static constexpr int VXBOX = vxbox_of(MULTI, M, (int)sizeof(T));
+  static constexpr int COMP_RAW = VXBOX * VY * VZ * (int)sizeof(T);  // bytes of one component box
+  static constexpr int COMP = round128(COMP_RAW);
+  static constexpr int BYTES = MULTI ? round128(COMP_RAW * M) : COMP * M;  // one slice buffer
+  static constexpr int TX_BYTES = COMP_RAW * M;                          // bytes TMA delivers
+  static constexpr int COMP_ELEMS = COMP / (int)sizeof(T);
+  static constexpr int WORDS = 2 * BYTES;                                // offset of the word slots
+  static constexpr int SMEM = WORDS + 3 * VSP * 4;
 };
 
 __device__ __forceinline__ unsigned long long pack_corner(long long x, long long y, long long z,
@@ -241,29 +263,26 @@ __device__ __forceinline__ unsigned long long pack_corner(long long x, long long
 
 // Stage 1: stream the field through shared memory, cull hypercubes, queue
 // the survivors with the chains whose own vertices survive the cull.
-template <typename T, int D, bool TMA>
+template <typename T, int D, bool MULTI, bool TMA>
 __global__ void __launch_bounds__(kThreads, 2)
     extract_regular_kernel(const __grid_constant__ CUtensorMap map0,
                            const __grid_constant__ CUtensorMap map1,
                            const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa,
-                           ExtractConfig cfg, CandidateQueue cq, BoxShape bs, unsigned* err) {
+                           ExtractConfig cfg, CandidateQueue cq, unsigned* err) {
+  using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
-  constexpr int TX = Tile<D>::TX, TY = Tile<D>::TY, TZ = Tile<D>::TZ;
-  constexpr int VX = TX + 1, VY = TY + 1, VZ = (D == 4) ? TZ + 1 : 1;
-  constexpr int VS = VX * VY * VZ;
-  constexpr int VPT = (VS + kThreads - 1) / kThreads;  // vertices per thread
-  constexpr int TBIT = 1 << (D - 1);                  // mask bit of the time axis
+  constexpr int TX = G::TX, TY = G::TY, TZ = G::TZ;
+  constexpr int VX = G::VX, VY = G::VY, VZ = G::VZ, VS = G::VS, VPT = G::VPT, VSP = G::VSP;
+  constexpr int TBIT = 1 << (D - 1);  // mask bit of the time axis
+  constexpr int HW = sizeof(T) / 4;   // the high 32-bit word of an element is its last
   static_assert(D == 3 ? kWarps * kRows == TY : kWarps == TY * (TZ / kRows),
                 "every corner row of the tile belongs to exactly one warp");
 
   extern __shared__ __align__(128) unsigned char smem[];
-  T* raw[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + bs.bytes)};
-  unsigned* W0 = reinterpret_cast<unsigned*>(smem + 2 * (size_t)bs.bytes);
   __shared__ unsigned long long bar[2];
-  __shared__ int wait_failed;
   __shared__ unsigned band_tbl[kBandTable];
+  unsigned* const Wb = reinterpret_cast<unsigned*>(smem + G::WORDS);
 
-  const ChainTable& CT = c_chains[D - 3];
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
 
@@ -274,6 +293,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int y0 = (tix % cfg.tiles[1]) * TY;
   tix /= cfg.tiles[1];
   const int z0 = (D == 4) ? tix * TZ : 0;
+  const int ldx = (int)mesh.ld[0], ldy = (int)mesh.ld[1], ldz = (D == 4) ? (int)mesh.ld[2] : 1;
   // time in int: local dims are below 2^16
   const int lt = (int)mesh.ld[D - 1];
   const int t0 = (int)blockIdx.y * cfg.tchunk;
@@ -281,57 +301,57 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int s_end = min(t1, lt - 1);  // last vertex slice this block reads
   // array coordinates of local (0,0,0,0): global for multicomponent arrays,
   // local for separate arrays
-  long long aoff[4];
+  int aoff[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) aoff[k] = (k < D) ? mesh.off[k] - fa.shift[k] : 0;
+  for (int k = 0; k < 4; ++k) aoff[k] = (k < D) ? (int)(mesh.off[k] - fa.shift[k]) : 0;
 
-  // per-thread vertex slots of a slice, fixed for the whole time march
-  int voff[VPT];    // element offset of component 0 in a raw slice buffer (-1: absent)
+  // per-thread vertex slots of a slice, fixed for the whole time march:
+  // element offset of component 0 in a slice buffer and a validity bit
+  int voff[VPT];
+  unsigned vvalid = 0;
 #pragma unroll
   for (int u = 0; u < VPT; ++u) {
     const int i = tid + u * kThreads;
-    voff[u] = -1;
-    if (i < VS) {
-      const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
-      const bool in = x0 + vx < mesh.ld[0] && y0 + vy < mesh.ld[1] && (D == 3 || z0 + vz < mesh.ld[2]);
-      if (in) voff[u] = bs.multi ? ((vz * VY + vy) * bs.vxbox + vx) * M : (vz * VY + vy) * bs.vxbox + vx;
-    }
+    const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
+    const bool in = i < VS && x0 + vx < ldx && y0 + vy < ldy && (D == 3 || z0 + vz < ldz);
+    voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
+    vvalid |= (in ? 1u : 0u) << u;
   }
-  const int comp_elems = (int)(bs.comp / sizeof(T));
   fill_band_table<T>(band_tbl, tid, kThreads);  // visible after the first barrier below
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
+    unsigned char* dst0 = smem + buf * G::BYTES;
     if constexpr (TMA) {
       if (tid == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bar[buf], bs.tx);
-        const int cx = (int)((x0 + aoff[0]) * (bs.multi ? M : 1));
-        const int cy = (int)(y0 + aoff[1]);
-        const CUtensorMap* maps[3] = {&map0, &map1, &map2};
-        for (int j = 0; j < (bs.multi ? 1 : M); ++j) {
-          unsigned char* dst = reinterpret_cast<unsigned char*>(raw[buf]) + j * bs.comp;
-          if constexpr (D == 4)
-            tma_load_4d(dst, maps[j], cx, cy, (int)(z0 + aoff[2]), (int)(s + aoff[3]), &bar[buf]);
-          else
-            tma_load_3d(dst, maps[j], cx, cy, (int)(s + aoff[2]), &bar[buf]);
+        mbar_expect_tx(&bar[buf], G::TX_BYTES);
+        const int cx = (x0 + aoff[0]) * (MULTI ? M : 1);
+        const int cy = y0 + aoff[1];
+        if constexpr (MULTI) {
+          if constexpr (D == 4) tma_load_4d(dst0, &map0, cx, cy, z0 + aoff[2], s + aoff[3], &bar[buf]);
+          else tma_load_3d(dst0, &map0, cx, cy, s + aoff[2], &bar[buf]);
+        } else {
+          const CUtensorMap* maps[3] = {&map0, &map1, &map2};
+#pragma unroll
+          for (int j = 0; j < M; ++j) {
+            if constexpr (D == 4)
+              tma_load_4d(dst0 + j * G::COMP, maps[j], cx, cy, z0 + aoff[2], s + aoff[3], &bar[buf]);
+            else
+              tma_load_3d(dst0 + j * G::COMP, maps[j], cx, cy, s + aoff[2], &bar[buf]);
+          }
         }
       }
     } else {
       // plain cooperative loads into the same layout (zero outside the array)
-      const int nper = bs.vxbox * VY * VZ;
-      for (int e = tid; e < nper * M; e += kThreads) {
-        int j, r;
-        if (bs.multi) {
-          j = e % M;
-          r = e / M;
-        } else {
-          j = e / nper;
-          r = e % nper;
-        }
-        const int vx = r % bs.vxbox;
-        const int vy = (r / bs.vxbox) % VY;
-        const int vz = r / (bs.vxbox * VY);
+      T* dst = reinterpret_cast<T*>(dst0);
+      constexpr int NPER = G::VXBOX * VY * VZ;
+      for (int e = tid; e < NPER * M; e += kThreads) {
+        const int j = MULTI ? e % M : e / NPER;
+        const int r = MULTI ? e / M : e % NPER;
+        const int vx = r % G::VXBOX;
+        const int vy = (r / G::VXBOX) % VY;
+        const int vz = r / (G::VXBOX * VY);
         const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : (long long)s, (long long)s};
         bool in = true;
         long long o = 0;
@@ -352,47 +372,29 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         T v = T(0);
         if (in) v = static_cast<const T*>(fa.comp[j])[o];
-        if (bs.multi) raw[buf][((vz * VY + vy) * bs.vxbox + vx) * M + j] = v;
-        else raw[buf][j * comp_elems + (vz * VY + vy) * bs.vxbox + vx] = v;
+        if (MULTI) dst[((vz * VY + vy) * G::VXBOX + vx) * M + j] = v;
+        else dst[j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX + vx] = v;
       }
     }
   };
+  // every thread waits for the slice's TMA phase itself (try_wait suspends
+  // in hardware); returns false when the bounded wait gave up
   auto wait = [&](int s, int buf) -> bool {
-    if constexpr (TMA) {
-      // one warp polls the barrier; the rest of the block waits at the
-      // block barrier without issuing instructions
-      if (warp == 0) {
-        const bool ok = mbar_wait(&bar[buf], (unsigned)(((s - t0) >> 1) & 1));
-        if (lane == 0) wait_failed = ok ? 0 : 1;
-      }
-      __syncthreads();
-      return wait_failed == 0;
-    } else {
-      __syncthreads();
-      return true;
-    }
+    if constexpr (TMA) return mbar_wait(&bar[buf], (unsigned)(((s - t0) >> 1) & 1));
+    else return true;
   };
-  // high 32-bit word of each element (the element itself for float)
-  constexpr int HW = sizeof(T) / 4;
-  auto words = [&](int buf, unsigned* dst) {
-    const unsigned* r = reinterpret_cast<const unsigned*>(raw[buf]) + (HW - 1);
+  auto words = [&](int buf, int slot) {
+    const unsigned* r = reinterpret_cast<const unsigned*>(smem + buf * G::BYTES) + (HW - 1);
+    unsigned* dst = Wb + slot * VSP;
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
-      const int i = tid + u * kThreads;
-      if (i < VS) {
-        unsigned w = kAbsent;
-        if (voff[u] >= 0) {
-          unsigned h[M];
+      unsigned h[M];
 #pragma unroll
-          for (int j = 0; j < M; ++j)
-            h[j] = r[HW * (bs.multi ? voff[u] + j : voff[u] + j * comp_elems)];
-          w = vertex_word_hi<T, M>(h, band_tbl);
-        }
-        dst[i] = w;
-      }
+      for (int j = 0; j < M; ++j) h[j] = r[HW * (MULTI ? voff[u] + j : voff[u] + j * G::COMP_ELEMS)];
+      const unsigned w = vertex_word_hi<T, M>(h, band_tbl);
+      dst[tid + u * kThreads] = ((vvalid >> u) & 1u) ? w : kAbsent;
     }
   };
-  auto W = [&](int s) -> unsigned* { return W0 + ((s - t0) % 3) * VS; };
 
   if constexpr (TMA) {
     if (tid == 0) {
@@ -406,15 +408,19 @@ __global__ void __launch_bounds__(kThreads, 2)
   } else {
     __syncthreads();
     issue(t0, 0);
+    __syncthreads();
   }
-  if (!wait(t0, 0)) {
-    // give the other copy in flight a bounded chance to land before leaving
-    if (TMA && t0 + 1 <= s_end && warp == 0) mbar_wait(&bar[1], 0);
-    if (tid == 0) atomicOr(err, 2u);
-    return;
+  int slot_a = 0;  // word slot of slice ct
+  {
+    const bool ok = wait(t0, 0);
+    if (ok) words(0, slot_a);
+    if (__syncthreads_or(!ok)) {
+      // give the other copy in flight a bounded chance to land before leaving
+      if (TMA && t0 + 1 <= s_end) mbar_wait(&bar[1], 0);
+      if (tid == 0) atomicOr(err, 2u);
+      return;
+    }
   }
-  words(0, W(t0));
-  __syncthreads();
   if (TMA && t0 + 2 <= s_end) issue(t0 + 2, 0);
 
   // corner validity per (lane, row) does not change along time
@@ -425,42 +431,48 @@ __global__ void __launch_bounds__(kThreads, 2)
   for (int q = 0; q < kRows; ++q) {
     const int cy = (D == 4) ? cyw : cyw + q;
     const int cz = (D == 4) ? czw + q : 0;
-    if (x0 + lane < mesh.ld[0] && y0 + cy < mesh.ld[1] && (D == 3 || z0 + cz < mesh.ld[2]))
-      row_valid |= 1u << q;
+    if (x0 + lane < ldx && y0 + cy < ldy && (D == 3 || z0 + cz < ldz)) row_valid |= 1u << q;
   }
 
   for (int ct = t0; ct < t1; ++ct) {
     const int s = ct + 1;
-    unsigned* B = W(s);
+    const int slot_b = slot_a == 2 ? 0 : slot_a + 1;  // word slot of slice s
+    unsigned* B = Wb + slot_b * VSP;
+    bool ok = true;
     if (s <= s_end) {
       const int buf = (s - t0) & 1;
-      if (!TMA) issue(s, buf);
-      if (!wait(s, buf)) {
-        if (TMA && s + 1 <= s_end && warp == 0) mbar_wait(&bar[buf ^ 1], (unsigned)(((s + 1 - t0) >> 1) & 1));
-        if (tid == 0) atomicOr(err, 2u);
-        return;
+      if (!TMA) {
+        issue(s, buf);
+        __syncthreads();
       }
-      words(buf, B);
+      ok = wait(s, buf);
+      if (ok) words(buf, slot_b);
     } else {
       for (int i = tid; i < VS; i += kThreads) B[i] = kAbsent;
     }
-    __syncthreads();
+    // the one block barrier of the step: words of slice s are visible, its
+    // raw buffer is free, and every warp has finished culling step ct - 1
+    if (__syncthreads_or(!ok)) {
+      if (TMA && s + 1 <= s_end) mbar_wait(&bar[((s - t0) & 1) ^ 1], (unsigned)(((s + 1 - t0) >> 1) & 1));
+      if (tid == 0) atomicOr(err, 2u);
+      return;
+    }
     if (TMA && s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
 
     // ---- hypercube cull: lanes along x, kRows corner rows per warp
-    const unsigned* A = W(ct);
+    const unsigned* A = Wb + slot_a * VSP;
     unsigned R[kRows + 1];
 #pragma unroll
     for (int q = 0; q <= kRows; ++q) {
-      unsigned r, e = kAbsent;
+      unsigned r, e;
       if constexpr (D == 4) {
         const int i0 = ((czw + q) * VY + cyw) * VX + lane, i1 = i0 + VX;
         r = A[i0] & A[i1] & B[i0] & B[i1];
-        if (lane == 31) e = A[i0 + 1] & A[i1 + 1] & B[i0 + 1] & B[i1 + 1];
+        e = (lane == 31) ? (A[i0 + 1] & A[i1 + 1] & B[i0 + 1] & B[i1 + 1]) : kAbsent;
       } else {
         const int i0 = (cyw + q) * VX + lane;
         r = A[i0] & B[i0];
-        if (lane == 31) e = A[i0 + 1] & B[i0 + 1];
+        e = (lane == 31) ? (A[i0 + 1] & B[i0 + 1]) : kAbsent;
       }
       const unsigned nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
       R[q] = r & (lane == 31 ? e : nb);
@@ -469,42 +481,30 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int q = 0; q < kRows; ++q) {
       const int cy = (D == 4) ? cyw : cyw + q;
       const int cz = (D == 4) ? czw + q : 0;
-      unsigned ball = __ballot_sync(0xFFFFFFFFu, ((row_valid >> q) & 1u) && !word_culled(R[q] & R[q + 1]));
-      while (ball) {
-        // one surviving hypercube at a time: lanes test its chains
-        const int cx = __ffs(ball) - 1;
-        ball &= ball - 1;
-        const long long l[4] = {x0 + cx, y0 + cy, (D == 4) ? z0 + cz : (long long)ct, (long long)ct};
-        int vmask = 0;  // axes along which the corner can step by +1
-#pragma unroll
-        for (int k = 0; k < D; ++k)
-          if (l[k] + 1 < mesh.ld[k]) vmask |= 1 << k;
-        unsigned long long chains = 0;
-        for (int base = 0; base < CT.n; base += 32) {
-          const int ch = base + lane;
-          bool ok = false;
-          if (ch < CT.n && (CT.mask[ch][M - 1] & ~vmask) == 0) {
-            unsigned wacc = A[((cz * VY) + cy) * VX + cx];
-#pragma unroll
-            for (int i = 0; i < M; ++i) {
-              const int mk = CT.mask[ch][i];
-              const int dx = mk & 1, dy = (mk >> 1) & 1, dz = (D == 4) ? (mk >> 2) & 1 : 0;
-              const int slot = ((cz + dz) * VY + (cy + dy)) * VX + (cx + dx);
-              wacc &= ((mk & TBIT) ? B : A)[slot];
-            }
-            ok = !word_culled(wacc);
-          }
-          chains |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, ok) << base;
-        }
-        if (chains && lane == 0) {
-          const unsigned idx = atomicAdd(cq.count, 1u);
+      const bool keep = ((row_valid >> q) & 1u) && !word_culled(R[q] & R[q + 1]);
+      const unsigned ball = __ballot_sync(0xFFFFFFFFu, keep);
+      if (ball) {
+        // surviving hypercubes are queued with every chain that fits in the
+        // mesh; the exact-test kernel applies the per-simplex word test
+        unsigned basei = 0;
+        if (lane == 0) basei = atomicAdd(cq.count, (unsigned)__popc(ball));
+        basei = __shfl_sync(0xFFFFFFFFu, basei, 0);
+        if (keep) {
+          const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
           if (idx < cq.cap) {
-            cq.corner[idx] = pack_corner(l[0], l[1], (D == 4) ? l[2] : 0, ct);
-            cq.chains[idx] = chains;
+            const int l0 = x0 + lane, l1 = y0 + cy, l2 = (D == 4) ? z0 + cz : ct;
+            int vmask = 0;  // axes along which the corner can step by +1
+            if (l0 + 1 < ldx) vmask |= 1;
+            if (l1 + 1 < ldy) vmask |= 2;
+            if (D == 4 && l2 + 1 < ldz) vmask |= 4;
+            if (ct + 1 < lt) vmask |= TBIT;
+            cq.corner[idx] = pack_corner(l0, l1, (D == 4) ? l2 : 0, ct);
+            cq.chains[idx] = c_chains_by_vmask[D - 3][vmask];
           }
         }
       }
     }
+    slot_a = slot_b;
   }
 }
 
@@ -521,6 +521,9 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
   constexpr int M = D - 1;
   constexpr int NV = 1 << D;
   __shared__ T cube[kRefineWarps][NV][M];
+  __shared__ unsigned band_tbl[kBandTable];
+  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  __syncthreads();
   const ChainTable& CT = c_chains[D - 3];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const unsigned n = min(*cq.count, cq.cap);
@@ -557,17 +560,35 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
       cube[wib][v][j] = in ? field_at<T>(fa, j, g, D, vid) : T(0);
     }
     __syncwarp();
+    // cull words of the hypercube's vertices (absent outside the mesh)
+    unsigned vw = kAbsent;
+    if (lane < NV) {
+      unsigned h[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) h[j] = hi_word<T>(cube[wib][lane][j]);
+      bool in = true;
+#pragma unroll
+      for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
+      vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
+    }
     for (int base = 0; base < CT.n; base += 32) {
       const int ch = base + lane;
       bool acc = false;
       double lam_out[4] = {0, 0, 0, 0};
       float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
       float sc_out = 0.f;
-      if (ch < CT.n && ((chains >> ch) & 1ull)) {
-        int mk[M + 1];
-        mk[0] = 0;
+      int mk[M + 1];
+      mk[0] = 0;
+      bool live = ch < CT.n && ((chains >> ch) & 1ull);
 #pragma unroll
-        for (int i = 0; i < M; ++i) mk[i + 1] = CT.mask[ch][i];
+      for (int i = 0; i < M; ++i) mk[i + 1] = live ? CT.mask[ch][i] : 0;
+      {
+        unsigned wacc = kAbsent;
+#pragma unroll
+        for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, mk[i]);
+        live = live && !word_culled(wacc);
+      }
+      if (live) {
         T vals[M + 1][M];
 #pragma unroll
         for (int i = 0; i <= M; ++i)
@@ -673,14 +694,17 @@ void upload_chain_tables() {
   build_chains(h[0], 3, 2);
   build_chains(h[1], 4, 3);
   cudaMemcpyToSymbol(c_chains, h, sizeof(h));
+  unsigned long long byv[2][16];
+  for (int t = 0; t < 2; ++t)
+    for (int vm = 0; vm < 16; ++vm) {
+      unsigned long long m = 0;
+      for (int c = 0; c < h[t].n; ++c)
+        if ((h[t].mask[c][t + 1] & ~vm) == 0) m |= 1ull << c;  // last vertex mask is index m-1 = t+1
+      byv[t][vm] = m;
+    }
+  cudaMemcpyToSymbol(c_chains_by_vmask, byv, sizeof(byv));
 }
 
-static int vxbox_for(int multi, int m, size_t es) {
-  // smallest box width >= 33 whose row is a multiple of 16 bytes
-  for (int v = 33; v <= kMaxVXBox; ++v)
-    if (((size_t)v * (multi ? m : 1) * es) % 16 == 0) return v;
-  return kMaxVXBox;
-}
 
 // cuTensorMapEncodeTiled is a driver API entry point; it is resolved through
 // the runtime so that the library carries no link-time libcuda dependency.
@@ -717,21 +741,13 @@ static bool encode_map(CUtensorMap* map, bool f64, const void* base, int rank, c
   return r == CUDA_SUCCESS;
 }
 
-template <typename T, int D>
+template <typename T, int D, bool MULTI>
 static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                             const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
                             int* used_tma) {
+  using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
-  constexpr int VY = Tile<D>::TY + 1, VZ = (D == 4) ? Tile<D>::TZ + 1 : 1;
   const size_t es = sizeof(T);
-  const int multi = (!fa.per_vertex && fa.estride[0] == M) ? 1 : 0;  // interleaved components
-  BoxShape bs;
-  bs.multi = multi;
-  bs.vxbox = vxbox_for(multi, M, es);
-  const size_t comp_bytes = (size_t)bs.vxbox * VY * VZ * es;
-  bs.comp = (unsigned)((comp_bytes + 127) & ~(size_t)127);
-  bs.tx = (unsigned)(comp_bytes * M);
-  bs.bytes = multi ? (unsigned)((comp_bytes * M + 127) & ~(size_t)127) : bs.comp * M;
 
   // TMA applies when every box starts on a 16-byte boundary and the array
   // strides are multiples of 16 bytes: inner coordinate = array x * (M or 1)
@@ -739,56 +755,64 @@ static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, cons
   memset(maps, 0, sizeof(maps));
   bool tma = allow_tma && !fa.per_vertex;
   const long long ax0 = mesh.off[0] - fa.shift[0];
-  const size_t inner_es = (multi ? M : 1) * es;
+  const size_t inner_es = (MULTI ? M : 1) * es;
   if (tma) {
     if (((size_t)ax0 * inner_es) % 16 != 0) tma = false;
     if (((size_t)fa.adims[0] * inner_es) % 16 != 0) tma = false;
-    for (int j = 0; j < (multi ? 1 : M); ++j)
+    for (int j = 0; j < (MULTI ? 1 : M); ++j)
       if (((uintptr_t)fa.comp[j]) % 16 != 0) tma = false;
     for (int k = 0; k < D; ++k)
-      if (fa.adims[k] * (k == 0 ? (multi ? M : 1) : 1) > 0x7FFFFFFFll) tma = false;
+      if (fa.adims[k] * (k == 0 ? (MULTI ? M : 1) : 1) > 0x7FFFFFFFll) tma = false;
   }
   if (tma) {
     uint64_t dims[4], strides[3];
     uint32_t box[4];
-    dims[0] = (uint64_t)fa.adims[0] * (multi ? M : 1);
-    box[0] = (uint32_t)(bs.vxbox * (multi ? M : 1));
+    dims[0] = (uint64_t)fa.adims[0] * (MULTI ? M : 1);
+    box[0] = (uint32_t)(G::VXBOX * (MULTI ? M : 1));
     uint64_t s = dims[0] * es;
     for (int k = 1; k < D; ++k) {
       dims[k] = (uint64_t)fa.adims[k];
       strides[k - 1] = s;
       s *= dims[k];
     }
-    box[1] = VY;
+    box[1] = G::VY;
     if (D == 4) {
-      box[2] = VZ;
+      box[2] = G::VZ;
       box[3] = 1;
     } else {
       box[2] = 1;
     }
-    for (int j = 0; j < (multi ? 1 : M) && tma; ++j)
+    for (int j = 0; j < (MULTI ? 1 : M) && tma; ++j)
       tma = encode_map(&maps[j], sizeof(T) == 8, fa.comp[j], D, dims, strides, box);
   }
   if (used_tma) *used_tma = tma ? 1 : 0;
-  const size_t words = 3 * sizeof(unsigned) * (size_t)(Tile<D>::TX + 1) * VY * VZ;
-  const size_t shm = 2 * (size_t)bs.bytes + words;
+  const size_t shm = G::SMEM;
   const long long lt = mesh.ld[D - 1];
   const unsigned nchunks = (unsigned)((lt + cfg.tchunk - 1) / cfg.tchunk);
   const unsigned ntiles = (unsigned)cfg.tiles[0] * cfg.tiles[1] * cfg.tiles[2];
   dim3 grid(ntiles, nchunks);
   cudaError_t e;
   if (tma) {
-    auto k = extract_regular_kernel<T, D, true>;
+    auto k = extract_regular_kernel<T, D, MULTI, true>;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e) return e;
-    k<<<grid, kThreads, shm, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, bs, err);
+    k<<<grid, kThreads, shm, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, err);
   } else {
-    auto k = extract_regular_kernel<T, D, false>;
+    auto k = extract_regular_kernel<T, D, MULTI, false>;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e) return e;
-    k<<<grid, kThreads, shm, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, bs, err);
+    k<<<grid, kThreads, shm, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, err);
   }
   return cudaGetLastError();
+}
+
+template <typename T, int D>
+static cudaError_t launch_td(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                             const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
+                             int* used_tma) {
+  const bool multi = !fa.per_vertex && fa.estride[0] == D - 1;  // interleaved components
+  return multi ? launch_t<T, D, true>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
+               : launch_t<T, D, false>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
 }
 
 void regular_tile(int d, int* tx, int* ty, int* tz) {
@@ -807,10 +831,10 @@ cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const Field
                                    const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
                                    cudaStream_t st, bool allow_tma, int* used_tma) {
   if (mesh.d == 4)
-    return f64 ? launch_t<double, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
-               : launch_t<float, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
-  return f64 ? launch_t<double, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
-             : launch_t<float, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
+    return f64 ? launch_td<double, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
+               : launch_td<float, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
+  return f64 ? launch_td<double, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
+             : launch_td<float, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
 }
 
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,

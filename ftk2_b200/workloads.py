@@ -45,6 +45,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--no-tma", action="store_true")
     ap.add_argument("--refined", action="store_true")
+    ap.add_argument("--tchunk", type=int, default=0, help="time steps per extraction block (0 = all)")
+    ap.add_argument("--no-graphs", action="store_true")
     args = ap.parse_args()
     import torch
     field, dims, m, q = make(args.case)
@@ -52,6 +54,10 @@ def main():
     with api.Context(0) as ctx:
         if args.no_tma:
             ctx.set_option(api.OPT_DISABLE_TMA, 1)
+        if args.tchunk:
+            ctx.set_option(api.OPT_TIME_CHUNK, args.tchunk)
+        if args.no_graphs:
+            ctx.set_option(api.OPT_USE_GRAPHS, 0)
         keep: list = []
         mesh = api.regular_mesh_desc(dims)
         fd = api.field_desc(field, api.LAYOUT_MULTICOMPONENT, m, keep=keep)
