@@ -101,6 +101,9 @@ SIGNATURES = {
     "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
     "ftk2b_ctx_last_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(C.c_uint64)]),
+    "ftk2b_cp_features_noalloc": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(FieldDesc), C.c_double,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                            C.c_void_p, C.POINTER(C.c_uint64)]),
 }
 
 _lib: Optional[C.CDLL] = None

@@ -176,6 +176,27 @@ ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out);
 ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* total_ms,
                                    uint64_t* kernels_launched);
 
+/* --- allocation-free extraction -------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory while they run (an in-situ step inside a simulation whose allocator
+ * owns the device, a serving loop held to a fixed memory budget, a host that
+ * records calls into a region where cudaMalloc is forbidden).  It runs the
+ * fused regular-mesh extraction on `stream` and writes the accepted simplices,
+ * unsorted, to caller-provided device memory: canonical keys (corner vertex id
+ * * n_types + chain rank) and 4 doubles of barycentrics per feature; `count`
+ * is a device word the call uses as its atomic counter, and *n_features
+ * receives the number found.  Field pointers must be device pointers.
+ * Scratch is a static device array of ~9.3 MiB that every GPU loading the
+ * library holds until exit; limits: capacity <= 262144 features and at most
+ * 262144 surviving hypercubes per call (FTK2B_INVALID_ARG /
+ * FTK2B_OVERFLOW_RETRY beyond them).  The first call on a device looks up the
+ * array's device address and uploads the kernels' constant tables; make that
+ * first call before any stream capture.  Calls share the array, so calls whose
+ * device work overlaps race.  The call synchronises `stream` before returning. */
+ftk2b_status ftk2b_cp_features_noalloc(const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                                       double sos_q, void* stream, uint64_t* keys, double* lambda,
+                                       uint32_t capacity, uint32_t* count, uint64_t* n_features);
+
 #ifdef __cplusplus
 }
 #endif
