@@ -53,7 +53,7 @@ class ClockSampler:
     """SM clocks and throttle reasons sampled through NVML every few
     milliseconds while the timed region runs (read-only queries)."""
 
-    def __init__(self, gpu: int, period_s: float = 0.005):
+    def __init__(self, gpu: int, period_s: float = 0.001):
         self.gpu = gpu
         self.period = period_s
         self.samples: list[tuple[float, int]] = []
