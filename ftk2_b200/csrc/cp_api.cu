@@ -187,6 +187,7 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
 void ftk2b_ctx::release_all() {
   // cached graphs point into these buffers
   graph_valid = false;
+  ext.valid = false;
   for (DevBuf* b : all_bufs()) b->release();
 }
 
@@ -196,6 +197,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
                             &simplices, &bary, &track, &edge_cnt, &edges, &parent, &counters,
                             &cls, &cand_corner, &cand_chains, &edge_slots};
   for (auto& b : extra) v.push_back(&b);
+  for (DevBuf* b : ext.bufs()) v.push_back(b);
   return v;
 }
 
@@ -351,6 +353,9 @@ ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int
     if (f->scalar_nd == 1) {
       fa.scalar_per_vertex = 1;
       sn = f->scalar_dims[0];
+      if (sn < n_vertices)
+        return fail(ctx, FTK2B_INVALID_ARG, "per-vertex scalar shorter than the vertex count (%llu < %llu)",
+                    (unsigned long long)sn, (unsigned long long)n_vertices);
     } else {
       if (f->scalar_nd != mesh_d) return fail(ctx, FTK2B_INVALID_ARG, "scalar needs nd == mesh dims");
       for (int k = 0; k < mesh_d; ++k)

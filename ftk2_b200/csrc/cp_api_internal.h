@@ -31,6 +31,23 @@ struct RegularGraphKey {
   int f64, want_edges, classify, allow_tma, key_bits, nch;
 };
 
+// Extruded meshes: the prepared base mesh (sorted cells, unique sorted
+// (cd-1)-faces with their coface cells), kept while the base cells' content
+// is unchanged, plus the work buffers of the extruded pipeline.
+struct ExtCache {
+  bool valid = false;
+  uint64_t hash = 0, ncell = 0, ns = 0;
+  int cd = 0;
+  unsigned nface = 0;
+  int fbits = 0;
+  DevBuf cells, fkeys, cof_start, cof;
+  DevBuf words, hi, lo, phase, hi_s, lo_s, phase_s, sort_k, sort_v, sort_k2, sort_v2, ekeys;
+  std::vector<DevBuf*> bufs() {
+    return {&cells, &fkeys, &cof_start, &cof, &words, &hi, &lo, &phase, &hi_s, &lo_s, &phase_s,
+            &sort_k, &sort_v, &sort_k2, &sort_v2, &ekeys};
+  }
+};
+
 struct LastRun {
   int kind = 0, m = 0;
   uint64_t n = 0, ne = 0, n_roots = 0, n_simplices = 0;
@@ -59,6 +76,7 @@ struct ftk2b_ctx {
   ftk2b::DevBuf key, lam, bary4, scalar, key_alt, perm0, perm1, hist, lam_s, bary4_s, scalar_s,
       simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains, edge_slots;
   std::vector<ftk2b::DevBuf> extra;
+  ftk2b::ExtCache ext;
   ftk2b::LastRun last;
   // CUDA graph of the last regular-mesh pipeline
   bool use_graphs = true;

@@ -114,7 +114,7 @@ __device__ __forceinline__ bool sos_inside2(const T v[3][2], double Q) {
 // of the three rows; exact integer arithmetic gives the reference's value for
 // any expansion of the same polynomial (and wraps identically on overflow).
 
-__device__ __noinline__ int sos_det3_levels(const i128 a[3], const i128 b[3], const i128 c[3]) {
+static __device__ __noinline__ int sos_det3_levels(const i128 a[3], const i128 b[3], const i128 c[3]) {
   i128 d;
   if ((d = b[0] * c[1] - b[1] * c[0])) return sgn(d);     // 1
   if ((d = -(b[0] * c[2] - b[2] * c[0]))) return sgn(d);  // 2

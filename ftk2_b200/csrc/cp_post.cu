@@ -14,6 +14,7 @@
 //      under the smaller one, so every component's root is its smallest
 //      canonical id = the reference's track_id (engine.hpp:46-74, 965-983).
 #include "cp_post.h"
+#include "cp_uf.cuh"
 
 namespace ftk2b {
 
@@ -412,37 +413,11 @@ __global__ void uf_init_kernel(unsigned* parent, const unsigned* n_ptr, unsigned
     parent[i] = i;
 }
 
-__device__ __forceinline__ unsigned uf_root(unsigned* parent, unsigned x) {
-  // follow parents to the root, halving the path on the way; parents only
-  // ever decrease, so the halving writes (atomicMin) never undo a hook
-  unsigned p = __ldcg(&parent[x]);
-  while (p != x) {
-    const unsigned gp = __ldcg(&parent[p]);
-    if (gp < p) atomicMin(&parent[x], gp);
-    x = p;
-    p = gp;
-  }
-  return x;
-}
-
 __global__ void uf_hook_kernel(unsigned* parent, const unsigned* __restrict__ edges,
                                const unsigned* ne_ptr, unsigned edge_cap, unsigned* err) {
   const unsigned ne = min(*ne_ptr, edge_cap);
-  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
-    unsigned a = edges[2 * (size_t)e], b = edges[2 * (size_t)e + 1];
-    // every retry follows a successful hook by another thread, and links only
-    // go to smaller indices, so this terminates; the bound is a safety net
-    int it = 0;
-    for (; it < (1 << 20); ++it) {
-      const unsigned ra = uf_root(parent, a), rb = uf_root(parent, b);
-      if (ra == rb) break;
-      const unsigned lo = min(ra, rb), hi = max(ra, rb);
-      if (atomicCAS(&parent[hi], hi, lo) == hi) break;
-      a = ra;
-      b = rb;
-    }
-    if (it == (1 << 20)) atomicOr(err, 1u);
-  }
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x)
+    uf_unite(parent, edges[2 * (size_t)e], edges[2 * (size_t)e + 1], err);
 }
 
 __global__ void uf_label_kernel(unsigned* parent, const unsigned* n_ptr, unsigned cap,
@@ -560,6 +535,33 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
   uf_hook_kernel<<<ge, 256, 0, st>>>(B.parent, B.edges, B.n_edges, B.edge_cap, B.err);
   uf_label_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap, B.track, B.n_roots);
   *launches += 6;  // edge count, scan, edge write, uf init, hook, label
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// launchers shared with the extruded-mesh pipeline
+
+cudaError_t launch_iota(unsigned* v, const unsigned* n_ptr, unsigned cap, cudaStream_t st) {
+  iota_kernel<<<grid_for(cap, 256, 4096), 256, 0, st>>>(v, n_ptr, cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan(unsigned* a, unsigned total, unsigned* total_out, const unsigned* n_ptr,
+                        cudaStream_t st) {
+  scan_inplace_kernel<<<1, 1024, 0, st>>>(a, total, total_out, n_ptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uf(unsigned* parent, const unsigned* n_ptr, unsigned cap, const unsigned* edges,
+                      const unsigned* ne_ptr, unsigned edge_cap, unsigned* err, cudaStream_t st) {
+  uf_init_kernel<<<grid_for(cap, 256, 4096), 256, 0, st>>>(parent, n_ptr, cap);
+  uf_hook_kernel<<<grid_for(edge_cap, 256, 4096), 256, 0, st>>>(parent, edges, ne_ptr, edge_cap, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uf_label(unsigned* parent, const unsigned* n_ptr, unsigned cap,
+                            unsigned long long* track, unsigned* n_roots, cudaStream_t st) {
+  uf_label_kernel<<<grid_for(cap, 256, 4096), 256, 0, st>>>(parent, n_ptr, cap, track, n_roots);
   return cudaGetLastError();
 }
 

@@ -43,6 +43,17 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
                                 int want_edges, cudaStream_t st, unsigned long long* launches);
 cudaError_t launch_classify_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa, int nch,
                                     const PostBuffers& B, cudaStream_t st);
+cudaError_t launch_iota(unsigned* v, const unsigned* n_ptr, unsigned cap, cudaStream_t st);
+// exclusive scan in place of min(total, *n_ptr) counters (n_ptr may be null);
+// the sum lands in *total_out when it is not null
+cudaError_t launch_scan(unsigned* a, unsigned total, unsigned* total_out, const unsigned* n_ptr,
+                        cudaStream_t st);
+// union-find: parent[i] = i, then the edges' endpoints united
+cudaError_t launch_uf(unsigned* parent, const unsigned* n_ptr, unsigned cap, const unsigned* edges,
+                      const unsigned* ne_ptr, unsigned edge_cap, unsigned* err, cudaStream_t st);
+// track[i] = root of i (the component's smallest index), roots counted
+cudaError_t launch_uf_label(unsigned* parent, const unsigned* n_ptr, unsigned cap,
+                            unsigned long long* track, unsigned* n_roots, cudaStream_t st);
 bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, unsigned* v1,
                 const unsigned* n_ptr, unsigned cap, int bits, unsigned* hist, int grid,
                 cudaStream_t st, unsigned long long* launches);

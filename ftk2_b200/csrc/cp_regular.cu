@@ -22,6 +22,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "cp_cull.cuh"
 #include "cp_device.cuh"
 #include "cp_internal.h"
 
@@ -31,105 +32,6 @@ __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=
 // chains whose vertices all stay inside the mesh, by the mask of axes along
 // which a corner may step: [0][vmask] for d = 3, [1][vmask] for d = 4
 __constant__ unsigned long long c_chains_by_vmask[2][16];
-
-// ---------------------------------------------------------------------------
-// Per-vertex cull word (32 bits), computed with integer operations on the
-// high 32 bits of each value (the whole value for float).
-//
-//   bits 0..2   component j strongly positive:  v_j >  kappa' * b,  b = max_k |v_k|
-//   bits 3..5   component j strongly negative:  v_j < -kappa' * b
-//   bit  6      tiny: b < 4e-13
-//   bits 7..31  magnitude-band mask {n-1, n, n+1}, n = (exponent(b) - E_LO) / B
-//
-// The AND of the words of a set S of vertices is "culled" when
-//   (a) a sign bit survives and the band mask is non-zero: then every vertex
-//       has component j of one strict sign with |v_ij| > kappa' * b_i, and
-//       the exponents of the b_i differ by at most 3B-1, so
-//       min_i |v_ij| > kappa' * 2^-(3B) * max_i b_i = kappa * M.  An accepted
-//       simplex needs lambda_i >= -1e-9, sum lambda = 1 and a residual
-//       sum_i lambda_i v_ij bounded by the backward error of partial-pivot
-//       elimination (|r| <= 72 gamma_9 M); with kappa = 2^-24 (double) and
-//       2^-12 (float) that is impossible, so no simplex inside S is accepted.
-//   (b) or the tiny bit survives: the first pivot of the solve is below 1e-12
-//       (zero_crossing.hpp:72), so the solve rejects.
-// Each predicate is evaluated on high words so that it can only err towards
-// "not strong" / "not tiny": a strictly larger high word of a non-negative
-// IEEE value implies a strictly larger value, and kappa' * b only shifts the
-// exponent field.  Infinite or NaN components give 0 (never culled).  Vertices
-// outside the mesh get ~0 (neutral under AND).
-template <typename T> struct CullParams;
-template <> struct CullParams<double> {
-  static constexpr int mant = 20;          // mantissa bits in the high word
-  static constexpr unsigned expmask = 0x7FF00000u;
-  static constexpr int bias = 1023;
-  static constexpr int kappa_exp = 12;     // kappa' = 2^-12
-  static constexpr int band = 4;           // exponents per band: kappa = 2^-24
-  static constexpr unsigned tiny_hi = 0x3D5C25C2u;  // high word of 4e-13 (rounded down)
-};
-template <> struct CullParams<float> {
-  static constexpr int mant = 23;
-  static constexpr unsigned expmask = 0x7F800000u;
-  static constexpr int bias = 127;
-  static constexpr int kappa_exp = 3;      // kappa' = 2^-3
-  static constexpr int band = 3;           // kappa = 2^-12
-  static constexpr unsigned tiny_hi = 0x2AE12E13u;  // 4e-13f (3.99999993e-13)
-};
-constexpr int kElo = -42;      // 2^-42 < 4e-13: smaller magnitudes are "tiny"
-constexpr int kBands = 25;
-constexpr unsigned kAbsent = ~0u;
-
-template <typename T> __device__ __forceinline__ unsigned hi_word(T v);
-template <> __device__ __forceinline__ unsigned hi_word<double>(double v) {
-  return (unsigned)__double2hiint(v);
-}
-template <> __device__ __forceinline__ unsigned hi_word<float>(float v) {
-  return __float_as_uint(v);
-}
-
-// Band masks by magnitude exponent: band_table[rel + 1] for rel = biased
-// exponent - bias - E_LO; 0 outside the banded window (and at index 0).
-constexpr int kBandTable = 128;
-
-template <typename T>
-__device__ __forceinline__ void fill_band_table(unsigned* tbl, int tid, int nthreads) {
-  using P = CullParams<T>;
-  for (int i = tid; i < kBandTable; i += nthreads) {
-    const int rel = i - 1;
-    unsigned w = 0;
-    if (rel >= 0 && rel < kBands * P::band) {
-      const int n = rel / P::band;
-      w = (((7u << n) >> 1) & ((1u << kBands) - 1u)) << 7;  // bits n-1, n, n+1
-    }
-    tbl[i] = w;
-  }
-}
-
-template <typename T, int M>
-__device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M], const unsigned* band_tbl) {
-  using P = CullParams<T>;
-  unsigned b = 0;
-#pragma unroll
-  for (int j = 0; j < M; ++j) b = max(b, h[j] & 0x7FFFFFFFu);
-  const unsigned kexp = (unsigned)P::kappa_exp << P::mant;
-  const unsigned thr = b > kexp ? b - kexp : 0u;  // high word of kappa' * b
-  unsigned w = 0;
-#pragma unroll
-  for (int j = 0; j < M; ++j) {
-    // positive and |v| > thr  <=>  (int)h > (int)thr  (thr >= 0)
-    // negative and |v| > thr  <=>  h > thr | sign bit   (unsigned)
-    w |= ((int)h[j] > (int)thr ? 1u : 0u) << j;
-    w |= (h[j] > (thr | 0x80000000u) ? 1u : 0u) << (3 + j);
-  }
-  w |= (b < P::tiny_hi ? 1u : 0u) << 6;
-  const int rel1 = (int)(b >> P::mant) - P::bias - kElo + 1;
-  w |= band_tbl[min((unsigned)rel1, (unsigned)(kBandTable - 1))];
-  // inf or nan somewhere: never culled
-  return b >= P::expmask ? 0u : w;
-}
-
-__device__ __forceinline__ bool word_culled(unsigned w) {
-  return (((w & 0x3Fu) != 0) && ((w >> 7) != 0)) || ((w & 0x40u) != 0);
-}
 
 // ---------------------------------------------------------------------------
 // field access

@@ -58,3 +58,17 @@ def test_simplex_count_matches_restatement():
     assert api.simplex_count(api.regular_mesh_desc([64, 64, 10]), 2) == res.n_tested
     # LUT part alone is 12 * 63 * 63 * 9 (mesh.hpp:270-302)
     assert res.n_tested > 12 * 63 * 63 * 9
+
+
+def test_extruded_simplex_count_matches_restatement():
+    # spatial cells at every layer, lateral prism pieces over every unique base
+    # face and the interior pieces (engine.hpp:573 counts the first two)
+    from oracle import bridge
+    import cases
+    for name in ("extruded_2d", "extruded_3d_s0"):
+        case = cases.GOLDEN_CASES[name]()
+        keep: list = []
+        mesh, fld = cases.oracle_inputs(case, keep)
+        res = bridge.run_restatement(mesh, fld)
+        desc = api.extruded_mesh_desc(case.coords.shape[0], case.cells, case.n_layers, keep)
+        assert api.simplex_count(desc, case.ncomp) == res.n_tested
