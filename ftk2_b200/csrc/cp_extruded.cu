@@ -774,7 +774,7 @@ cudaError_t enqueue_post(ftk2b_ctx* ctx, const ExtMeshDev& X, const ExtSink& sin
   unsigned long long* ekeys = (unsigned long long*)C.ekeys.p;
   ext_edges_kernel<M, 0><<<g, 256, 0, st>>>(X, Fs, ecnt, nullptr, ekeys, edge_cap, err);
   if ((e = launch_scan(ecnt, cap, n_edges, count, st))) return e;
-  ext_edges_kernel<M, 1><<<g, 256, 0, st>>>(X, Fs, ecnt, ecnt, ekeys, edge_cap, err);
+  ext_edges_kernel<M, 1><<<g, 256, 0, st>>>(X, Fs, nullptr, ecnt, ekeys, edge_cap, err);
   // (min, max) pairs sorted lexicographically; a pair spans exactly one top
   // cell, so there are no duplicates
   const int eb = 2 * 32;

@@ -1,0 +1,34 @@
+// Value access of the regular-mesh kernels (engine.hpp:999-1009 for separate
+// arrays indexed by global - offset, 1101-1124 for multicomponent arrays at
+// global coordinates, per-vertex arrays by vertex id).
+#pragma once
+
+#include "cp_internal.h"
+
+namespace ftk2b {
+
+template <typename T>
+__device__ __forceinline__ T field_at(const FieldAccess& fa, int j, const long long g[4], int d,
+                                      unsigned long long vid) {
+  const T* base = static_cast<const T*>(fa.comp[j]);
+  if (fa.per_vertex) return base[vid];
+  long long o = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < d) o += (g[k] - fa.shift[k]) * fa.estride[k];
+  return base[o];
+}
+
+template <typename T>
+__device__ __forceinline__ T scalar_at(const FieldAccess& fa, const long long g[4], int d,
+                                       unsigned long long vid) {
+  const T* base = static_cast<const T*>(fa.scalar);
+  if (fa.scalar_per_vertex) return base[vid];
+  long long o = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < d) o += g[k] * fa.sstride[k];
+  return base[o];
+}
+
+}  // namespace ftk2b

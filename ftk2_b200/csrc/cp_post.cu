@@ -14,6 +14,7 @@
 //      under the smaller one, so every component's root is its smallest
 //      canonical id = the reference's track_id (engine.hpp:46-74, 965-983).
 #include "cp_post.h"
+#include "cp_kuhn.cuh"
 #include "cp_uf.cuh"
 
 namespace ftk2b {
@@ -163,11 +164,6 @@ __global__ void gather_kernel(const unsigned* n_ptr, unsigned cap, const unsigne
 // ---------------------------------------------------------------------------
 // regular-mesh geometry helpers
 
-struct Decoded {
-  long long g[4];  // global coords of the corner
-  int mk[5];       // masks of the m+1 vertices (mk[0] = 0)
-};
-
 __device__ __forceinline__ void decode_key(const RegularMesh& mesh, int nch, unsigned long long key,
                                            Decoded& dc) {
   const ChainTable& CT = c_post_chains[mesh.d - 3];
@@ -198,52 +194,6 @@ __device__ __forceinline__ long long find_key(const unsigned long long* keys, un
     else hi = mid;
   }
   return -1;
-}
-
-// Cofaces (top cells) of the feature's simplex inside the local box, each as
-// corner + d+1 vertex masks.  A codimension-1 simplex of a Kuhn triangulation
-// has exactly two: if one axis a never steps, prepend (corner - e_a) or append
-// (full mask); otherwise split the one two-axis step in either order.
-__device__ int top_cells(const RegularMesh& mesh, const Decoded& dc, long long cc[2][4],
-                         int cm[2][5]) {
-  const int d = mesh.d, m = d - 1, full = (1 << d) - 1;
-  int nc = 0;
-  const int missing = full & ~dc.mk[m];
-  if (missing) {
-    const int a = __ffs(missing) - 1;
-    if (dc.g[a] - mesh.off[a] >= 1) {
-      for (int k = 0; k < 4; ++k) cc[nc][k] = dc.g[k];
-      cc[nc][a] -= 1;
-      cm[nc][0] = 0;
-      for (int j = 0; j <= m; ++j) cm[nc][j + 1] = dc.mk[j] | (1 << a);
-      ++nc;
-    }
-    if (dc.g[a] - mesh.off[a] + 1 < mesh.ld[a]) {
-      for (int k = 0; k < 4; ++k) cc[nc][k] = dc.g[k];
-      for (int j = 0; j <= m; ++j) cm[nc][j] = dc.mk[j];
-      cm[nc][m + 1] = full;
-      ++nc;
-    }
-  } else {
-    for (int j = 1; j <= m; ++j) {
-      const int step = dc.mk[j] & ~dc.mk[j - 1];
-      if (__popc(step) == 2) {
-        const int lo = step & -step, hi = step & ~lo;
-        const int ins[2] = {lo, hi};
-        for (int q = 0; q < 2; ++q) {
-          for (int k = 0; k < 4; ++k) cc[nc][k] = dc.g[k];
-          int w = 0;
-          for (int jj = 0; jj <= m; ++jj) {
-            if (jj == j) cm[nc][w++] = dc.mk[j - 1] | ins[q];
-            cm[nc][w++] = dc.mk[jj];
-          }
-          ++nc;
-        }
-        break;
-      }
-    }
-  }
-  return nc;
 }
 
 // Indices of the active faces of a top cell, ascending.

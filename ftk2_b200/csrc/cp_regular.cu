@@ -24,6 +24,7 @@
 
 #include "cp_cull.cuh"
 #include "cp_device.cuh"
+#include "cp_field.cuh"
 #include "cp_internal.h"
 
 namespace ftk2b {
@@ -32,33 +33,6 @@ __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=
 // chains whose vertices all stay inside the mesh, by the mask of axes along
 // which a corner may step: [0][vmask] for d = 3, [1][vmask] for d = 4
 __constant__ unsigned long long c_chains_by_vmask[2][16];
-
-// ---------------------------------------------------------------------------
-// field access
-
-template <typename T>
-__device__ __forceinline__ T field_at(const FieldAccess& fa, int j, const long long g[4], int d,
-                                      unsigned long long vid) {
-  const T* base = static_cast<const T*>(fa.comp[j]);
-  if (fa.per_vertex) return base[vid];
-  long long o = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (k < d) o += (g[k] - fa.shift[k]) * fa.estride[k];
-  return base[o];
-}
-
-template <typename T>
-__device__ __forceinline__ T scalar_at(const FieldAccess& fa, const long long g[4], int d,
-                                       unsigned long long vid) {
-  const T* base = static_cast<const T*>(fa.scalar);
-  if (fa.scalar_per_vertex) return base[vid];
-  long long o = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (k < d) o += g[k] * fa.sstride[k];
-  return base[o];
-}
 
 // ---------------------------------------------------------------------------
 // TMA / mbarrier primitives (inline PTX)

@@ -48,7 +48,7 @@ class OrcResult(C.Structure):
         ("lambda_", C.POINTER(C.c_double)), ("track_id", C.POINTER(C.c_uint64)),
         ("type", C.POINTER(C.c_uint32)), ("scalar", C.POINTER(C.c_float)),
         ("n_edges", C.c_uint64), ("edges", C.POINTER(C.c_uint32)),
-        ("n_tested", C.c_uint64),
+        ("n_tested", C.c_uint64), ("cp_class", C.POINTER(C.c_uint32)),
     ]
 
 
@@ -63,6 +63,7 @@ class CPResult:
     scalar: np.ndarray      # (n,) float32
     edges: np.ndarray       # (e, 2) uint32
     n_tested: int = 0
+    cp_class: np.ndarray | None = None  # (n,) uint32, restatement on regular meshes only
 
 
 _libs: dict[str, C.CDLL] = {}
@@ -81,6 +82,17 @@ def _load(path: str, prefix: str) -> C.CDLL:
         free.restype = None
         _libs[path] = lib
     return _libs[path]
+
+
+def classify_jacobian(J: np.ndarray) -> int:
+    """Class code of one spatial Jacobian (m x m, J[j][a] = d v_j / d x_a) by
+    the restatement's FP64 classifier."""
+    lib = _load(ORC_LIB, "cporacle")
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    fn = lib.cporacle_classify_jacobian
+    fn.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    fn.restype = C.c_uint32
+    return int(fn(J.shape[0], J.ctypes.data_as(C.POINTER(C.c_double))))
 
 
 def ref_available() -> bool:
@@ -178,6 +190,7 @@ def _run(path: str, prefix: str, mesh: OrcMesh, field: OrcField) -> CPResult:
             scalar=arr(res.scalar, n, np.float32),
             edges=arr(res.edges, 2 * e, np.uint32).reshape(e, 2),
             n_tested=int(res.n_tested),
+            cp_class=arr(res.cp_class, n, np.uint32) if res.cp_class else None,
         )
     finally:
         getattr(lib, prefix + "_free")(C.byref(res))

@@ -466,6 +466,106 @@ static int finish(feat_t* F, size_t n, int m, evec_t* E, uint64_t* parent, uint6
   return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Classification (no counterpart in the reference: type = 0 always,          */
+/* predicate.hpp:80).  J = spatial Jacobian of the linear interpolant on the  */
+/* feature's first coface top cell, in the field precision; invariants in     */
+/* FP64 on J scaled by 2^-e (e = exponent of max |J|), every operation        */
+/* rounded separately in the order below.  Codes: 1 degenerate, 2 source,     */
+/* 3 sink, 4 saddle, 5 spiral source, 6 spiral sink, 7 centre.                */
+
+enum { CL_DEGENERATE = 1, CL_SOURCE = 2, CL_SINK = 3, CL_SADDLE = 4, CL_SPIRAL_SOURCE = 5,
+       CL_SPIRAL_SINK = 6, CL_CENTER = 7 };
+
+static int sgnd(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+
+static uint32_t decide2(int sdet, int str, int sdisc) {
+  if (sdet == 0) return CL_DEGENERATE;
+  if (sdet < 0) return CL_SADDLE;
+  if (sdisc >= 0) return str > 0 ? CL_SOURCE : (str < 0 ? CL_SINK : CL_DEGENERATE);
+  return str > 0 ? CL_SPIRAL_SOURCE : (str < 0 ? CL_SPIRAL_SINK : CL_CENTER);
+}
+
+static uint32_t decide3(int sa2, int sa1, int sh, int sa0, int sdelta) {
+  if (sa0 == 0) return CL_DEGENERATE;
+  /* h = 0: (l + a2)(l^2 + a1) */
+  if (sh == 0) return sa1 < 0 ? CL_SADDLE : (sa1 > 0 ? CL_CENTER : CL_DEGENERATE);
+  if (sa2 == 0) return CL_SADDLE;
+  int c1 = sa2, c2 = sh * sa2, c3 = sa0;
+  int npos = (c1 < 0) + (c1 != c2) + (c2 != c3);
+  int cpx = sdelta < 0;
+  if (npos == 3) return cpx ? CL_SPIRAL_SOURCE : CL_SOURCE;
+  if (npos == 0) return cpx ? CL_SPIRAL_SINK : CL_SINK;
+  return CL_SADDLE;
+}
+
+/* J[j][a] = d v_j / d x_a as doubles holding values of the field precision */
+uint32_t cporacle_classify_jacobian(int m, const double* Jin) {
+  double mx = 0;
+  for (int i = 0; i < m * m; ++i) {
+    if (!isfinite(Jin[i])) return CL_DEGENERATE;
+    if (fabs(Jin[i]) > mx) mx = fabs(Jin[i]);
+  }
+  if (mx == 0) return CL_DEGENERATE;
+  int e;
+  frexp(mx, &e);
+  double J[3][3];
+  for (int j = 0; j < m; ++j)
+    for (int a = 0; a < m; ++a) J[j][a] = ldexp(Jin[j * m + a], -e);
+  if (m == 2) {
+    double ad = J[0][0] * J[1][1], bc = J[0][1] * J[1][0];
+    double det = ad - bc;
+    double tr = J[0][0] + J[1][1];
+    double disc = tr * tr - 4.0 * det;
+    return decide2(sgnd(det), sgnd(tr), sgnd(disc));
+  }
+  double p0 = J[1][1] * J[2][2], q0 = J[1][2] * J[2][1];
+  double p1 = J[0][0] * J[2][2], q1 = J[0][2] * J[2][0];
+  double p2 = J[0][0] * J[1][1], q2 = J[0][1] * J[1][0];
+  double m0 = p0 - q0, m1 = p1 - q1, m2 = p2 - q2;
+  double r1 = J[1][0] * J[2][2], u1 = J[1][2] * J[2][0];
+  double r2 = J[1][0] * J[2][1], u2 = J[1][1] * J[2][0];
+  double c1 = r1 - u1, c2 = r2 - u2;
+  double tr = (J[0][0] + J[1][1]) + J[2][2];
+  double a1 = (m0 + m1) + m2;
+  double det = (J[0][0] * m0 - J[0][1] * c1) + J[0][2] * c2;
+  double a2 = -tr, a0 = -det;
+  double h = a2 * a1 - a0;
+  double b = a2, c = a1, d = a0;
+  double t1 = ((18.0 * b) * c) * d;
+  double t2 = (((4.0 * b) * b) * b) * d;
+  double t3 = ((b * b) * c) * c;
+  double t4 = ((4.0 * c) * c) * c;
+  double t5 = (27.0 * d) * d;
+  double delta = (((t1 - t2) + t3) - t4) - t5;
+  return decide3(sgnd(a2), sgnd(a1), sgnd(h), sgnd(a0), sgnd(delta));
+}
+
+/* Class of a regular-mesh feature from its first coface top cell (corner
+ * cc, masks cm), or degenerate without one. */
+static uint32_t classify_regular_cell(const acc_t* acc, const orc_mesh* me, int d, int nc,
+                                      const uint64_t cc[4], const int cm[5]) {
+  int m = d - 1;
+  if (nc == 0) return CL_DEGENERATE;
+  double val[5][3];
+  for (int r = 0; r <= d; ++r) {
+    uint64_t g[4] = {0, 0, 0, 0};
+    for (int k = 0; k < d; ++k) g[k] = cc[k] + ((cm[r] >> k) & 1);
+    uint64_t vid = grid_id(me, g);
+    for (int j = 0; j < m; ++j) val[r][j] = field_value(acc, j, g, vid);
+  }
+  double J[9];
+  for (int r = 1; r <= d; ++r) {
+    int axis = __builtin_ctz(cm[r] ^ cm[r - 1]);
+    if (axis >= m) continue;
+    for (int j = 0; j < m; ++j) {
+      if (acc->f->dtype == ORC_F64) J[j * m + axis] = val[r][j] - val[r - 1][j];
+      else J[j * m + axis] = (double)((float)val[r][j] - (float)val[r - 1][j]);
+    }
+  }
+  return cporacle_classify_jacobian(m, J);
+}
+
 static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) {
   int d = me->ndims, M = f->ncomp;
   if (!((d == 3 && M == 2) || (d == 4 && M == 3))) return 2;
@@ -514,6 +614,12 @@ static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) 
   uint64_t* order = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
   for (size_t i = 0; i < n; ++i) order[i] = i;
   evec_t E = {0};
+  uint32_t* cls = (uint32_t*)malloc(sizeof(uint32_t) * (n + 1));
+  acc_t cacc;
+  memset(&cacc, 0, sizeof(cacc));
+  cacc.f = f;
+  cacc.nd_mesh = d;
+  for (int k = 0; k < 4; ++k) cacc.offset[k] = me->offset[k];
   int full = (1 << d) - 1;
   uint64_t stride[4] = {1, 1, 1, 1};
   for (int k = 1; k < d; ++k) stride[k] = stride[k - 1] * me->global_dims[k - 1];
@@ -570,6 +676,7 @@ static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) 
         }
       }
     }
+    cls[i] = classify_regular_cell(&cacc, me, d, nc, cell_c[0], cell_m[0]);
     for (int q = 0; q < nc; ++q) {
       uint64_t cell[5];
       for (int r = 0; r <= d; ++r) {
@@ -583,6 +690,7 @@ static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) 
   uint64_t* parent = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
   for (size_t i = 0; i < n; ++i) parent[i] = i;
   finish(F, n, M, &E, parent, tested, out);
+  out->cp_class = cls;
   free(parent);
   free(order);
   free(E.e);
@@ -912,6 +1020,7 @@ void cporacle_free(orc_result* r) {
   free(r->type);
   free(r->scalar);
   free(r->edges);
+  free(r->cp_class);
   memset(r, 0, sizeof(*r));
 }
 

@@ -73,6 +73,8 @@ typedef struct {
   uint64_t n_edges;
   uint32_t* edges;          /* 2*n_edges, sorted, unique, (lo, hi) */
   uint64_t n_tested;        /* m-simplices evaluated (restatement only) */
+  uint32_t* cp_class;       /* n classes (restatement only, regular meshes; else NULL):
+                               FTK2B_CLASS_* codes of include/ftk2b.h */
 } orc_result;
 
 /* reference engine build */
@@ -82,6 +84,8 @@ void ftk2ref_free(orc_result* r);
 /* own restatement */
 int cporacle_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);
 void cporacle_free(orc_result* r);
+/* FP64 classification of one spatial Jacobian (m x m, row = component) */
+uint32_t cporacle_classify_jacobian(int m, const double* J);
 
 #ifdef __cplusplus
 }
