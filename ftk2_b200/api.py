@@ -101,6 +101,13 @@ SIGNATURES = {
     "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
     "ftk2b_ctx_last_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(C.c_uint64)]),
+    "ftk2b_stream_open": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                    C.POINTER(CPParams), C.POINTER(C.c_void_p)]),
+    "ftk2b_stream_push": (C.c_int, [C.c_void_p, C.POINTER(FieldDesc), C.POINTER(C.c_uint64)]),
+    "ftk2b_stream_result": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_stream_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_double)]),
+    "ftk2b_stream_close": (None, [C.c_void_p]),
     "ftk2b_cp_features_noalloc": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(FieldDesc), C.c_double,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -337,6 +344,50 @@ class Context:
             return _result_from_c(out.contents)
         finally:
             self.lib.ftk2b_cp_result_free(out)
+
+
+class Stream:
+    """A time stream on a context (ftk2b_stream_*): push one timestep at a
+    time; result() equals Context.extract on all timesteps pushed so far."""
+
+    def __init__(self, ctx: Context, mesh: MeshDesc, template: FieldDesc, prm: Optional[CPParams] = None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        prm = prm or params()
+        h = C.c_void_p()
+        ctx._check(self.lib.ftk2b_stream_open(ctx.h, C.byref(mesh), C.byref(template), C.byref(prm),
+                                              C.byref(h)))
+        self.h = h
+
+    def push(self, step: FieldDesc) -> int:
+        n = C.c_uint64()
+        self.ctx._check(self.lib.ftk2b_stream_push(self.h, C.byref(step), C.byref(n)))
+        return int(n.value)
+
+    def result(self) -> CPResult:
+        out = C.POINTER(CPResultC)()
+        self.ctx._check(self.lib.ftk2b_stream_result(self.h, C.byref(out)))
+        try:
+            return _result_from_c(out.contents)
+        finally:
+            self.lib.ftk2b_cp_result_free(out)
+
+    def info(self):
+        """(timesteps pushed, features so far, device ms of the last push)."""
+        t, n, ms = C.c_uint64(), C.c_uint64(), C.c_double()
+        self.ctx._check(self.lib.ftk2b_stream_info(self.h, C.byref(t), C.byref(n), C.byref(ms)))
+        return int(t.value), int(n.value), float(ms.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ftk2b_stream_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def simplex_count(mesh: MeshDesc, m: int) -> int:

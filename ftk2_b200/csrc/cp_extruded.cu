@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "cp_api_internal.h"
+#include "cp_stream.h"
 #include "cp_cull.cuh"
 #include "cp_device.cuh"
 #include "cp_uf.cuh"
@@ -50,7 +51,10 @@ constexpr int kMaxOthers = 32;  // star partners of one centre: 8 coface cells x
 struct ExtMeshDev {
   int cd;                            // base cell dim = m = number of components
   unsigned ns;                       // spatial vertices: vertex id = s + t * ns
-  unsigned L;                        // time slabs; vertex layers 0..L
+  unsigned L;                        // time slabs; vertex layers t0..t0+L
+  unsigned t0;                       // global layer of the first local layer
+  unsigned tflip;                    // storage slot of local layer l = l xor tflip
+  int skip_first_spatial;            // 1: no spatial simplices at local layer 0
   unsigned ncell, nface;
   int fbits;                         // bits per base vertex id in a face key
   const unsigned* cells;             // [ncell][cd+1], ascending
@@ -208,13 +212,13 @@ __global__ void __launch_bounds__(256) ext_words_kernel(FieldAccess fa, unsigned
 
 template <typename T, int M>
 __device__ __forceinline__ bool ext_test(const FieldAccess& fa, const ExtractConfig& cfg,
-                                         const unsigned long long* vid, double lam_out[4],
+                                         const unsigned long long* sidx, double lam_out[4],
                                          float bary_out[4], float& sc_out) {
   T vals[M + 1][M];
 #pragma unroll
   for (int i = 0; i <= M; ++i)
 #pragma unroll
-    for (int j = 0; j < M; ++j) vals[i][j] = static_cast<const T*>(fa.comp[j])[vid[i]];
+    for (int j = 0; j < M; ++j) vals[i][j] = static_cast<const T*>(fa.comp[j])[sidx[i]];
   bool inside;
   if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
   else inside = sos_inside3<T>(vals, cfg.Q);
@@ -231,7 +235,7 @@ __device__ __forceinline__ bool ext_test(const FieldAccess& fa, const ExtractCon
     const T* s = static_cast<const T*>(fa.scalar);
     T sc = T(0);
 #pragma unroll
-    for (int i = 0; i <= M; ++i) sc = F::add(sc, F::mul(lam[i], s[vid[i]]));
+    for (int i = 0; i <= M; ++i) sc = F::add(sc, F::mul(lam[i], s[sidx[i]]));
     sc_out = (float)sc;
   }
   if (cfg.refined) {
@@ -243,22 +247,26 @@ __device__ __forceinline__ bool ext_test(const FieldAccess& fa, const ExtractCon
   return true;
 }
 
-// grid: x over the items of one layer, y = layer t.  Items of layer t:
+// grid: x over the items of one layer, y = local layer t.  Items of layer t:
 // [0, ncell) spatial cells, then (t < L only) [ncell, ncell + nface) base
 // faces (m lateral pieces each) and [ncell + nface, 2 ncell + nface) base
-// cells (m interior simplices each).
+// cells (m interior simplices each).  Values and words of local layer l sit
+// at storage layer l xor tflip; vertex ids use the global layer t0 + l.
 template <typename T, int M>
 __global__ void __launch_bounds__(kThreadsX) ext_extract_kernel(ExtMeshDev X, FieldAccess fa,
                                                                 const unsigned* __restrict__ words,
                                                                 ExtractConfig cfg, ExtSink sink, int vb) {
   const unsigned t = blockIdx.y;
   const unsigned nitems = (t < X.L) ? 2u * X.ncell + X.nface : X.ncell;
-  const unsigned long long bt = (unsigned long long)t * X.ns, bt1 = bt + X.ns;
+  const unsigned first = (X.skip_first_spatial && t == 0) ? X.ncell : 0u;
+  const unsigned long long bt = (unsigned long long)(X.t0 + t) * X.ns, bt1 = bt + X.ns;
+  const unsigned long long st = (unsigned long long)(t ^ X.tflip) * X.ns;
+  const unsigned long long st1 = (unsigned long long)((t + 1) ^ X.tflip) * X.ns;
   const int lane = threadIdx.x & 31;
   const unsigned fmask = (X.fbits >= 32) ? 0xFFFFFFFFu : ((1u << X.fbits) - 1u);
   for (unsigned base = blockIdx.x * kThreadsX; base < nitems; base += gridDim.x * kThreadsX) {
     const unsigned i = base + threadIdx.x;
-    const bool valid = i < nitems;
+    const bool valid = i < nitems && i >= first;
     int kind = 0;
     unsigned u[M + 1];
     unsigned wa[M + 1], wb[M + 1];
@@ -288,19 +296,20 @@ __global__ void __launch_bounds__(kThreadsX) ext_extract_kernel(ExtMeshDev X, Fi
 #pragma unroll
       for (int k = 0; k <= M; ++k)
         if (k < nu) {
-          wa[k] = words[bt + u[k]];
-          if (kind != 0) wb[k] = words[bt1 + u[k]];
+          wa[k] = words[st + u[k]];
+          if (kind != 0) wb[k] = words[st1 + u[k]];
         }
     }
 #pragma unroll
     for (int p = 0; p < M; ++p) {
       const bool live = valid && (kind != 0 || p == 0);
-      unsigned long long vid[M + 1];
+      unsigned long long vid[M + 1], sidx[M + 1];
       unsigned wacc = kAbsent;
       if (kind == 0) {
 #pragma unroll
         for (int k = 0; k <= M; ++k) {
           vid[k] = bt + u[k];
+          sidx[k] = st + u[k];
           wacc &= wa[k];
         }
       } else if (kind == 1) {
@@ -309,12 +318,14 @@ __global__ void __launch_bounds__(kThreadsX) ext_extract_kernel(ExtMeshDev X, Fi
 #pragma unroll
         for (int k = 0; k < M; ++k)
           if (k <= p) {
+            sidx[w] = st + u[k];
             vid[w++] = bt + u[k];
             wacc &= wa[k];
           }
 #pragma unroll
         for (int k = 0; k < M; ++k)
           if (k >= p) {
+            sidx[w] = st1 + u[k];
             vid[w++] = bt1 + u[k];
             wacc &= wb[k];
           }
@@ -324,6 +335,7 @@ __global__ void __launch_bounds__(kThreadsX) ext_extract_kernel(ExtMeshDev X, Fi
         for (int k = 0; k <= M; ++k) {
           const bool lo = k <= p;
           vid[k] = (lo ? bt : bt1) + u[k];
+          sidx[k] = (lo ? st : st1) + u[k];
           wacc &= lo ? wa[k] : wb[k];
         }
       }
@@ -331,7 +343,7 @@ __global__ void __launch_bounds__(kThreadsX) ext_extract_kernel(ExtMeshDev X, Fi
       double lam_out[4] = {0, 0, 0, 0};
       float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
       float sc_out = 0.f;
-      if (live && !word_culled(wacc)) acc = ext_test<T, M>(fa, cfg, vid, lam_out, bary_out, sc_out);
+      if (live && !word_culled(wacc)) acc = ext_test<T, M>(fa, cfg, sidx, lam_out, bary_out, sc_out);
       const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
       if (ball) {
         unsigned basei = 0;
@@ -431,11 +443,11 @@ __device__ __forceinline__ void for_each_coface(const ExtMeshDev& X, const unsig
   };
   if (n_at_t == M + 1) {
     // spatial simplex (a base cell at layer t): piece m of slab t, piece 0 of slab t-1
-    if (t < X.L) {
+    if (t < (unsigned long long)X.t0 + X.L) {
       piece(sp, t, M);
       visit(cell);
     }
-    if (t > 0) {
+    if (t > X.t0) {
       piece(sp, t - 1, 0);
       visit(cell);
     }
@@ -801,6 +813,16 @@ cudaError_t enqueue_post(ftk2b_ctx* ctx, const ExtMeshDev& X, const ExtSink& sin
 
 using namespace ftk2b;
 
+ftk2b_status stream_push_extruded(ftk2b_stream* s) {
+  s->ctx->err = "extruded streams are not implemented yet";
+  return FTK2B_UNSUPPORTED;
+}
+
+ftk2b_status stream_result_extruded(ftk2b_stream* s, ftk2b_cp_result**) {
+  s->ctx->err = "extruded streams are not implemented yet";
+  return FTK2B_UNSUPPORTED;
+}
+
 uint64_t extruded_simplex_count(const ftk2b_mesh_desc* mesh, int m) {
   const int cd = mesh->base_cell_dim;
   if ((cd != 2 && cd != 3) || m != cd || (mesh->n_base_cells && !mesh->base_cells)) return 0;
@@ -864,6 +886,9 @@ ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk
   X.fkeys = (const unsigned long long*)C.fkeys.p;
   X.cof_start = (const unsigned*)C.cof_start.p;
   X.cof = (const unsigned*)C.cof.p;
+  X.t0 = 0;
+  X.tflip = 0;
+  X.skip_first_spatial = 0;
   const int vb = bits_of(nv - 1);
   const uint64_t nsimp = C.ncell * (uint64_t)(L + 1) + (uint64_t)C.nface * L * M + C.ncell * (uint64_t)L * M;
 

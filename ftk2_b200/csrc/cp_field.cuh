@@ -15,7 +15,11 @@ __device__ __forceinline__ T field_at(const FieldAccess& fa, int j, const long l
   long long o = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k)
-    if (k < d) o += (g[k] - fa.shift[k]) * fa.estride[k];
+    if (k < d) {
+      long long a = g[k] - fa.shift[k];
+      if (k == d - 1) a ^= fa.tflip;
+      o += a * fa.estride[k];
+    }
   return base[o];
 }
 

@@ -28,6 +28,9 @@ struct FieldAccess {
   long long sstride[4];
   int scalar_per_vertex;
   int has_scalar;
+  // time-axis index of the component arrays = (g - shift) xor tflip: a
+  // stream's two-slot ring keeps timestep t in slot t & 1 (0 otherwise)
+  int tflip;
 };
 
 // Regular spacetime mesh: RegularSimplicialMesh(local, offset, global)
@@ -65,6 +68,7 @@ struct ExtractConfig {
   int refined;                 // 1: report FP32 + one FP64 refinement step
   int tchunk;                  // corner time steps per block
   int tiles[3];                // tiles along x, y, z (z = 1 for 2D)
+  int skip_first_spatial;      // 1: no purely spatial simplices at local time 0
 };
 
 // chain tables: masks of vertices 1..m of every m-simplex type of a

@@ -398,7 +398,7 @@ __global__ void expand_regular_kernel(RegularMesh mesh, int nch, const unsigned 
       for (int k = 0; k < mesh.d; ++k)
         vid += (unsigned long long)(dc.g[k] + ((dc.mk[v] >> k) & 1)) * mesh.gstride[k];
       simplices[(size_t)i * (m + 1) + v] = vid;
-      bary[(size_t)i * (m + 1) + v] = bary4[4 * (size_t)i + v];
+      if (bary) bary[(size_t)i * (m + 1) + v] = bary4[4 * (size_t)i + v];
     }
   }
 }
@@ -512,6 +512,26 @@ cudaError_t launch_uf(unsigned* parent, const unsigned* n_ptr, unsigned cap, con
 cudaError_t launch_uf_label(unsigned* parent, const unsigned* n_ptr, unsigned cap,
                             unsigned long long* track, unsigned* n_roots, cudaStream_t st) {
   uf_label_kernel<<<grid_for(cap, 256, 4096), 256, 0, st>>>(parent, n_ptr, cap, track, n_roots);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_window_edges_regular(const RegularMesh& mesh, int nch, const unsigned long long* skeys,
+                                        const unsigned* n_ptr, unsigned cap, unsigned* edge_cnt,
+                                        unsigned* edge_slots, unsigned* edges, unsigned* n_edges,
+                                        unsigned edge_cap, cudaStream_t st) {
+  const int g = grid_for(cap, 256, 4096);
+  edges_regular_warp_kernel<<<grid_for(cap, 8, 8192), 256, 0, st>>>(mesh, nch, skeys, n_ptr, cap, edge_cnt,
+                                                                   edge_slots);
+  scan_inplace_kernel<<<1, 1024, 0, st>>>(edge_cnt, cap, n_edges, n_ptr, nullptr);
+  edges_compact_kernel<<<g, 256, 0, st>>>(n_ptr, cap, edge_cnt, n_edges, edge_slots, edges, edge_cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_expand_regular(const RegularMesh& mesh, int nch, const unsigned long long* keys,
+                                  const unsigned* n_ptr, unsigned cap, const float* bary4,
+                                  unsigned long long* simplices, float* bary, cudaStream_t st) {
+  expand_regular_kernel<<<grid_for(cap, 256, 4096), 256, 0, st>>>(mesh, nch, keys, n_ptr, cap, bary4, simplices,
+                                                                  bary);
   return cudaGetLastError();
 }
 

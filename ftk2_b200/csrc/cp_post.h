@@ -54,6 +54,16 @@ cudaError_t launch_uf(unsigned* parent, const unsigned* n_ptr, unsigned cap, con
 // track[i] = root of i (the component's smallest index), roots counted
 cudaError_t launch_uf_label(unsigned* parent, const unsigned* n_ptr, unsigned cap,
                             unsigned long long* track, unsigned* n_roots, cudaStream_t st);
+// star edges of the top cells of `mesh` (a window of the full mesh) among the
+// sorted keys, as (centre, other) index pairs, sorted; count in *n_edges
+cudaError_t launch_window_edges_regular(const RegularMesh& mesh, int nch, const unsigned long long* skeys,
+                                        const unsigned* n_ptr, unsigned cap, unsigned* edge_cnt,
+                                        unsigned* edge_slots, unsigned* edges, unsigned* n_edges,
+                                        unsigned edge_cap, cudaStream_t st);
+// vertex ids (and, when bary is not null, float barycentrics) of keys
+cudaError_t launch_expand_regular(const RegularMesh& mesh, int nch, const unsigned long long* keys,
+                                  const unsigned* n_ptr, unsigned cap, const float* bary4,
+                                  unsigned long long* simplices, float* bary, cudaStream_t st);
 bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, unsigned* v1,
                 const unsigned* n_ptr, unsigned cap, int bits, unsigned* hist, int grid,
                 cudaStream_t st, unsigned long long* launches);

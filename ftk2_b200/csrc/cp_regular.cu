@@ -33,6 +33,8 @@ __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=
 // chains whose vertices all stay inside the mesh, by the mask of axes along
 // which a corner may step: [0][vmask] for d = 3, [1][vmask] for d = 4
 __constant__ unsigned long long c_chains_by_vmask[2][16];
+// chains whose last vertex steps along the time axis
+__constant__ unsigned long long c_time_chains[2];
 
 // ---------------------------------------------------------------------------
 // TMA / mbarrier primitives (inline PTX)
@@ -180,6 +182,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   int aoff[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) aoff[k] = (k < D) ? (int)(mesh.off[k] - fa.shift[k]) : 0;
+  // array time coordinate of vertex slice s: (s + aoff) xor tflip (a stream's
+  // two-slot ring stores timestep t in slot t & 1; tflip = 0 otherwise)
+  auto tcoord = [&](int s) { return (s + aoff[D - 1]) ^ fa.tflip; };
 
   // per-thread vertex slots of a slice, fixed for the whole time march:
   // element offset of component 0 in a slice buffer and a validity bit
@@ -205,16 +210,16 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int cx = (x0 + aoff[0]) * (MULTI ? M : 1);
         const int cy = y0 + aoff[1];
         if constexpr (MULTI) {
-          if constexpr (D == 4) tma_load_4d(dst0, &map0, cx, cy, z0 + aoff[2], s + aoff[3], &bar[buf]);
-          else tma_load_3d(dst0, &map0, cx, cy, s + aoff[2], &bar[buf]);
+          if constexpr (D == 4) tma_load_4d(dst0, &map0, cx, cy, z0 + aoff[2], tcoord(s), &bar[buf]);
+          else tma_load_3d(dst0, &map0, cx, cy, tcoord(s), &bar[buf]);
         } else {
           const CUtensorMap* maps[3] = {&map0, &map1, &map2};
 #pragma unroll
           for (int j = 0; j < M; ++j) {
             if constexpr (D == 4)
-              tma_load_4d(dst0 + j * G::COMP, maps[j], cx, cy, z0 + aoff[2], s + aoff[3], &bar[buf]);
+              tma_load_4d(dst0 + j * G::COMP, maps[j], cx, cy, z0 + aoff[2], tcoord(s), &bar[buf]);
             else
-              tma_load_3d(dst0 + j * G::COMP, maps[j], cx, cy, s + aoff[2], &bar[buf]);
+              tma_load_3d(dst0 + j * G::COMP, maps[j], cx, cy, tcoord(s), &bar[buf]);
           }
         }
       }
@@ -241,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         } else {
 #pragma unroll
           for (int k = 0; k < D; ++k) {
-            const long long a = l[k] + aoff[k];
+            const long long a = (k == D - 1) ? (long long)tcoord(s) : l[k] + aoff[k];
             in &= a >= 0 && a < fa.adims[k];
             o += a * fa.estride[k];
           }
@@ -375,7 +380,11 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (D == 4 && l2 + 1 < ldz) vmask |= 4;
             if (ct + 1 < lt) vmask |= TBIT;
             cq.corner[idx] = pack_corner(l0, l1, (D == 4) ? l2 : 0, ct);
-            cq.chains[idx] = c_chains_by_vmask[D - 3][vmask];
+            unsigned long long ch = c_chains_by_vmask[D - 3][vmask];
+            // a stream's window starts one slice before the new timestep: the
+            // purely spatial simplices of that slice were counted already
+            if (cfg.skip_first_spatial && ct == 0) ch &= c_time_chains[D - 3];
+            cq.chains[idx] = ch;
           }
         }
       }
@@ -579,6 +588,13 @@ void upload_chain_tables() {
       byv[t][vm] = m;
     }
   cudaMemcpyToSymbol(c_chains_by_vmask, byv, sizeof(byv));
+  unsigned long long tc[2] = {0, 0};
+  for (int t = 0; t < 2; ++t) {
+    const int tbit = 1 << (t + 2);  // time axis: bit d - 1
+    for (int c = 0; c < h[t].n; ++c)
+      if (h[t].mask[c][t + 1] & tbit) tc[t] |= 1ull << c;
+  }
+  cudaMemcpyToSymbol(c_time_chains, tc, sizeof(tc));
 }
 
 

@@ -1,0 +1,671 @@
+// Time streams over a fixed spatial mesh: timesteps are pushed one at a time
+// and only a two-timestep window of the field is kept on the device.
+//
+// Replaces the reference's streaming drivers (execute_stream and
+// execute_cuda_streaming_regular, engine.hpp:214-270, 601-819) with one-shot
+// semantics: after T pushes, ftk2b_stream_result returns exactly what
+// ftk2b_cp_extract (execute() + get_complex(), engine.hpp:96-99, 822-996)
+// returns for the T-timestep spacetime mesh.
+//
+// Push of timestep t (t >= 1), window = layers [t-1, t]:
+//   1. the step is copied into ring slot t & 1;
+//   2. the fused extraction runs on the window with the purely spatial
+//      simplices of layer t-1 skipped (the previous push found them), so the
+//      new features are exactly the simplices whose last layer is t;
+//   3. the window's features (new ones plus the spatial features of layer
+//      t-1) are sorted, and the star edges of every top cell of slab
+//      [t-1, t] are emitted -- every top cell belongs to exactly one slab, and
+//      its centre (smallest face in Simplex order) is decided inside it;
+//   4. the resident union-find over stream ids takes the new edges.
+// The result sorts the store (canonical ids = rank in Simplex order) and
+// labels every component with its smallest canonical id (engine.hpp:46-74).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "cp_post.h"
+#include "cp_stream.h"
+#include "cp_uf.cuh"
+
+using namespace ftk2b;
+
+namespace {
+
+enum { kSWin = 5, kSWinEdges = 6, kSPrev = 7 };
+
+ftk2b_status sfail(ftk2b_ctx* ctx, ftk2b_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return st;
+}
+
+#define S_TRY(ctx, call)                                                                        \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return sfail(ctx, e_ == cudaErrorMemoryAllocation ? FTK2B_OOM : FTK2B_CUDA_ERROR,          \
+                   "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+int bits_for(unsigned long long v) {
+  int b = 0;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b < 1 ? 1 : b;
+}
+
+int grid_of(unsigned long long n, int threads, int max_blocks) {
+  unsigned long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > (unsigned long long)max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+__global__ void set_u32_kernel(unsigned* p, unsigned v) { *p = v; }
+
+__global__ void window_build_kernel(const unsigned long long* __restrict__ key, const unsigned* __restrict__ prev,
+                                    unsigned n_prev, unsigned first_new, unsigned n_new,
+                                    unsigned long long* __restrict__ s_key, unsigned* __restrict__ s_id) {
+  const unsigned nS = n_prev + n_new;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += gridDim.x * blockDim.x) {
+    const unsigned id = i < n_prev ? prev[i] : first_new + (i - n_prev);
+    s_key[i] = key[id];
+    s_id[i] = id;
+  }
+}
+
+__global__ void uf_init_range_kernel(unsigned* parent, unsigned lo, unsigned n) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    parent[lo + i] = lo + i;
+}
+
+// window edges (indices into the sorted window) -> stream ids, united and
+// appended after the `base` edges already stored
+__global__ void append_edges_kernel(const unsigned* __restrict__ wedges, const unsigned* wn_ptr, unsigned wcap,
+                                    const unsigned* __restrict__ s_id, unsigned* parent, unsigned* __restrict__ out,
+                                    unsigned base, unsigned out_cap, unsigned* err) {
+  const unsigned wn = min(*wn_ptr, wcap);
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < wn; e += gridDim.x * blockDim.x) {
+    const unsigned a = s_id[wedges[2 * (size_t)e]], b = s_id[wedges[2 * (size_t)e + 1]];
+    uf_unite(parent, a, b, err);
+    if (base + e < out_cap) {
+      out[2 * (size_t)(base + e)] = a;
+      out[2 * (size_t)(base + e) + 1] = b;
+    }
+  }
+}
+
+// new features whose chain does not step in time are the spatial ones of
+// the newest layer
+__global__ void collect_spatial_kernel(const unsigned long long* __restrict__ key, unsigned first_new,
+                                       unsigned n_new, int nch, unsigned long long time_chains,
+                                       unsigned* __restrict__ prev, unsigned* prev_n) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+    const unsigned id = first_new + i;
+    const unsigned ch = (unsigned)(key[id] % (unsigned long long)nch);
+    if (!((time_chains >> ch) & 1ull)) prev[atomicAdd(prev_n, 1u)] = id;
+  }
+}
+
+__global__ void iota_u32_kernel(unsigned* v, unsigned n) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+__global__ void invert_kernel(const unsigned* __restrict__ perm, unsigned n, unsigned* __restrict__ inv) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) inv[perm[i]] = i;
+}
+
+// component minimum of the canonical ids, through the roots of the stream ids
+__global__ void comp_min_kernel(unsigned* parent, const unsigned* __restrict__ inv, unsigned n,
+                                unsigned* __restrict__ root, unsigned* cmin, unsigned* n_roots) {
+  for (unsigned id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    const unsigned r = uf_root(parent, id);
+    root[id] = r;
+    atomicMin(&cmin[r], inv[id]);
+    if (r == id) atomicAdd(n_roots, 1u);
+  }
+}
+
+__global__ void fill_u32_kernel(unsigned* v, unsigned n, unsigned x) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = x;
+}
+
+__global__ void canon_edges_kernel(const unsigned* __restrict__ edges, unsigned ne,
+                                   const unsigned* __restrict__ inv, unsigned long long* __restrict__ out) {
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const unsigned a = inv[edges[2 * (size_t)e]], b = inv[edges[2 * (size_t)e + 1]];
+    out[e] = ((unsigned long long)min(a, b) << 32) | max(a, b);
+  }
+}
+
+__global__ void unpack_edges_kernel(const unsigned long long* __restrict__ k, unsigned ne, unsigned* __restrict__ out) {
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    out[2 * (size_t)e] = (unsigned)(k[e] >> 32);
+    out[2 * (size_t)e + 1] = (unsigned)k[e];
+  }
+}
+
+// canonical-order copies of the per-feature records
+__global__ void gather_result_kernel(const unsigned* __restrict__ perm, unsigned n,
+                                     const unsigned* __restrict__ root, const unsigned* __restrict__ cmin,
+                                     const double* __restrict__ lam, const float* __restrict__ bary4,
+                                     const float* __restrict__ sc, const unsigned* __restrict__ cls,
+                                     double* __restrict__ lam_o, float* __restrict__ bary4_o,
+                                     float* __restrict__ sc_o, unsigned* __restrict__ cls_o,
+                                     unsigned long long* __restrict__ track) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned p = perm[i];
+    for (int k = 0; k < 4; ++k) {
+      lam_o[4 * (size_t)i + k] = lam[4 * (size_t)p + k];
+      bary4_o[4 * (size_t)i + k] = bary4[4 * (size_t)p + k];
+    }
+    sc_o[i] = sc[p];
+    cls_o[i] = cls[p];
+    track[i] = cmin[root[p]];
+  }
+}
+
+unsigned long long time_chain_mask(int d) {
+  // chains (canonical order) whose last vertex mask has the time bit
+  const int m = d - 1, full = (1 << d) - 1, tbit = 1 << (d - 1);
+  unsigned long long mask = 0;
+  int cur[5] = {0, 0, 0, 0, 0}, next[5] = {0, 0, 0, 0, 0}, depth = 1, cnt = 0;
+  while (depth > 0) {
+    const int prev = cur[depth - 1];
+    int nx = next[depth] + 1;
+    while (nx <= full && !(((nx & prev) == prev) && nx != prev)) ++nx;
+    if (nx > full) {
+      next[depth] = 0;
+      --depth;
+      continue;
+    }
+    next[depth] = nx;
+    cur[depth] = nx;
+    if (depth == m) {
+      if (nx & tbit) mask |= 1ull << cnt;
+      ++cnt;
+    } else {
+      ++depth;
+      next[depth] = 0;
+    }
+  }
+  return mask;
+}
+
+RegularMesh window_mesh(const ftk2b_stream* s, uint64_t t_start, uint64_t lt) {
+  RegularMesh rm;
+  memset(&rm, 0, sizeof(rm));
+  rm.d = s->d;
+  unsigned long long st = 1;
+  for (int k = 0; k < s->d; ++k) {
+    const bool tm = k == s->d - 1;
+    rm.ld[k] = tm ? (long long)lt : (long long)s->ld[k];
+    rm.off[k] = tm ? (long long)t_start : (long long)s->off[k];
+    rm.gd[k] = tm ? (1ll << 30) : (long long)s->gd[k];
+    rm.gstride[k] = st;
+    st *= (unsigned long long)rm.gd[k];
+  }
+  return rm;
+}
+
+FieldAccess window_field(const ftk2b_stream* s, uint64_t t_start) {
+  FieldAccess fa;
+  memset(&fa, 0, sizeof(fa));
+  const int d = s->d, M = s->m;
+  const bool multi = s->layout == FTK2B_LAYOUT_MULTICOMPONENT;
+  long long st = multi ? M : 1;
+  for (int k = 0; k < d; ++k) {
+    const bool tm = k == d - 1;
+    fa.adims[k] = tm ? 2 : (long long)s->adims[k];
+    fa.estride[k] = st;
+    st *= fa.adims[k];
+    fa.shift[k] = tm ? (long long)t_start : (multi ? 0 : (long long)s->off[k]);
+  }
+  for (int j = 0; j < M; ++j)
+    fa.comp[j] = multi ? (const void*)((const char*)s->ring[0].p + j * s->es) : s->ring[j].p;
+  fa.tflip = (int)(t_start & 1);
+  return fa;
+}
+
+ftk2b_status ensure_store(ftk2b_stream* s, unsigned want) {
+  ftk2b_ctx* ctx = s->ctx;
+  if (want <= s->cap) return FTK2B_OK;
+  unsigned nc = s->cap ? s->cap : 65536u;
+  while (nc < want) nc = nc * 2u > nc ? nc * 2u : 0xFFFFFFF0u;
+  cudaStream_t st = ctx->stream;
+  const size_t n = s->n;
+  if (s->kind == FTK2B_MESH_REGULAR) {
+    S_TRY(ctx, grow_keep(s->key, 8 * n, 8 * (size_t)nc, st));
+  } else {
+    S_TRY(ctx, grow_keep(s->hi, 8 * n, 8 * (size_t)nc, st));
+    S_TRY(ctx, grow_keep(s->lo, 8 * n, 8 * (size_t)nc, st));
+    S_TRY(ctx, grow_keep(s->phase, 4 * n, 4 * (size_t)nc, st));
+  }
+  S_TRY(ctx, grow_keep(s->lam, 32 * n, 32 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->bary4, 16 * n, 16 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->scalar, 4 * n, 4 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->cls, 4 * n, 4 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->parent, 4 * n, 4 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->prev_ids, 4 * (size_t)s->n_prev, 4 * (size_t)nc, st));
+  S_TRY(ctx, s->prev_ids2.ensure(4 * (size_t)nc));
+  s->cap = nc;
+  return FTK2B_OK;
+}
+
+ftk2b_status push_regular(ftk2b_stream* s) {
+  ftk2b_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  const int d = s->d, M = s->m;
+  const int nch = d == 3 ? 12 : 60;
+  const uint64_t T = s->T;
+  const uint64_t t_start = T ? T - 1 : 0, lt = T ? 2 : 1;
+  const RegularMesh rm = window_mesh(s, t_start, lt);
+  const FieldAccess fa = window_field(s, t_start);
+  ExtractConfig cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.Q = s->prm.sos_q;
+  cfg.refined = s->prm.precision == FTK2B_PRECISION_REFINED;
+  cfg.tchunk = (int)lt;
+  cfg.skip_first_spatial = T > 0;
+  int TX, TY, TZ;
+  regular_tile(d, &TX, &TY, &TZ);
+  cfg.tiles[0] = (int)((rm.ld[0] + TX - 1) / TX);
+  cfg.tiles[1] = (int)((rm.ld[1] + TY - 1) / TY);
+  cfg.tiles[2] = (d == 4) ? (int)((rm.ld[2] + TZ - 1) / TZ) : 1;
+  const int f64 = s->dtype == FTK2B_F64;
+
+  S_TRY(ctx, ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
+  unsigned* counters = (unsigned*)ctx->counters.p;
+  ftk2b_status rc = ensure_store(s, s->n + 1024);
+  if (rc) return rc;
+  unsigned ccap = ctx->cand_cap_hint ? ctx->cand_cap_hint : 65536u;
+  unsigned n_new = 0;
+  for (int attempt = 0;; ++attempt) {
+    if (attempt == 6) return sfail(ctx, FTK2B_OVERFLOW_RETRY, "stream buffers kept overflowing");
+    S_TRY(ctx, ctx->cand_corner.ensure(8 * (size_t)ccap));
+    S_TRY(ctx, ctx->cand_chains.ensure(8 * (size_t)ccap));
+    S_TRY(ctx, cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, st));
+    FeatureSink sink;
+    sink.key = (unsigned long long*)s->key.p + s->n;
+    sink.lam = (double*)s->lam.p + 4 * (size_t)s->n;
+    sink.bary4 = (float*)s->bary4.p + 4 * (size_t)s->n;
+    sink.scalar = (float*)s->scalar.p + s->n;
+    sink.count = counters + kCountFeatures;
+    sink.cap = s->cap - s->n;
+    CandidateQueue cq;
+    cq.corner = (unsigned long long*)ctx->cand_corner.p;
+    cq.chains = (unsigned long long*)ctx->cand_chains.p;
+    cq.count = counters + kCountCand;
+    cq.cap = ccap;
+    S_TRY(ctx, launch_extract_regular(f64, rm, fa, cfg, cq, counters + kCountErr, st, !ctx->disable_tma,
+                                      &ctx->last_used_tma));
+    S_TRY(ctx, launch_refine_regular(f64, rm, fa, cfg, cq, sink, ctx->num_sms, st));
+    ctx->launches += 2;
+    S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost,
+                               st));
+    S_TRY(ctx, cudaStreamSynchronize(st));
+    const unsigned* h = ctx->h_counters;
+    if (h[kCountErr] & 2u) return sfail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
+    if (h[kCountCand] > ccap) {
+      ccap = h[kCountCand] + h[kCountCand] / 4 + 1024;
+      ctx->cand_cap_hint = ccap;
+      continue;
+    }
+    if (h[kCountFeatures] > s->cap - s->n) {
+      rc = ensure_store(s, s->n + h[kCountFeatures] + h[kCountFeatures] / 4 + 1024);
+      if (rc) return rc;
+      continue;
+    }
+    n_new = h[kCountFeatures];
+    break;
+  }
+
+  // window: spatial features of layer t-1 plus the new ones, in key order
+  const unsigned first_new = s->n;
+  const unsigned nS = s->n_prev + n_new;
+  const unsigned wcap = nS ? nS : 1;
+  S_TRY(ctx, s->s_key.ensure(8 * (size_t)wcap));
+  S_TRY(ctx, s->s_key2.ensure(8 * (size_t)wcap));
+  S_TRY(ctx, s->s_id.ensure(4 * (size_t)wcap));
+  S_TRY(ctx, s->s_id2.ensure(4 * (size_t)wcap));
+  S_TRY(ctx, s->wedges.ensure(8 * 8 * (size_t)wcap));
+  S_TRY(ctx, ctx->edge_cnt.ensure(4 * (size_t)wcap));
+  S_TRY(ctx, ctx->edge_slots.ensure(4 * 8 * (size_t)wcap));
+  const int sgrid = ctx->sort_grid(wcap);
+  S_TRY(ctx, ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)sgrid));
+  const unsigned edge_room = s->n_edges + 8 * nS;
+  if (edge_room > s->edge_cap) {
+    unsigned nc = s->edge_cap ? s->edge_cap : 65536u;
+    while (nc < edge_room) nc *= 2;
+    S_TRY(ctx, grow_keep(s->edges, 8 * (size_t)s->n_edges, 8 * (size_t)nc, st));
+    s->edge_cap = nc;
+  }
+  const int g = grid_of(wcap, 256, 4096);
+  set_u32_kernel<<<1, 1, 0, st>>>(counters + kSWin, nS);
+  window_build_kernel<<<g, 256, 0, st>>>((const unsigned long long*)s->key.p, (const unsigned*)s->prev_ids.p,
+                                         s->n_prev, first_new, n_new, (unsigned long long*)s->s_key.p,
+                                         (unsigned*)s->s_id.p);
+  const unsigned long long nv_hi = (unsigned long long)rm.gstride[d - 1] * (T + 1);
+  const int key_bits = bits_for(nv_hi * (unsigned long long)nch);
+  const bool alt = radix_sort((unsigned long long*)s->s_key.p, (unsigned*)s->s_id.p,
+                              (unsigned long long*)s->s_key2.p, (unsigned*)s->s_id2.p, counters + kSWin, wcap,
+                              key_bits, (unsigned*)ctx->hist.p, sgrid, st, &ctx->launches);
+  const unsigned long long* skeys = (const unsigned long long*)(alt ? s->s_key2.p : s->s_key.p);
+  const unsigned* sids = (const unsigned*)(alt ? s->s_id2.p : s->s_id.p);
+  S_TRY(ctx, launch_window_edges_regular(rm, nch, skeys, counters + kSWin, wcap, (unsigned*)ctx->edge_cnt.p,
+                                         (unsigned*)ctx->edge_slots.p, (unsigned*)s->wedges.p,
+                                         counters + kSWinEdges, 8 * wcap, st));
+  if (n_new) uf_init_range_kernel<<<grid_of(n_new, 256, 4096), 256, 0, st>>>((unsigned*)s->parent.p, first_new, n_new);
+  append_edges_kernel<<<grid_of(8ull * wcap, 256, 4096), 256, 0, st>>>(
+      (const unsigned*)s->wedges.p, counters + kSWinEdges, 8 * wcap, sids, (unsigned*)s->parent.p,
+      (unsigned*)s->edges.p, s->n_edges, s->edge_cap, counters + kCountErr);
+  if (n_new)
+    collect_spatial_kernel<<<grid_of(n_new, 256, 4096), 256, 0, st>>>(
+        (const unsigned long long*)s->key.p, first_new, n_new, nch, time_chain_mask(d), (unsigned*)s->prev_ids2.p,
+        counters + kSPrev);
+  ctx->launches += 8;
+
+  // classification while the window's values are resident: the new features,
+  // and at the second push the first layer's (their coface lies in slab [0, 1])
+  if (s->prm.classify) {
+    S_TRY(ctx, s->tmp_simp.ensure(8 * (size_t)(M + 1) * (wcap > s->n_first ? wcap : s->n_first + 1)));
+    auto classify = [&](unsigned first, unsigned cnt, unsigned* count_slot) -> cudaError_t {
+      if (!cnt) return cudaSuccess;
+      set_u32_kernel<<<1, 1, 0, st>>>(count_slot, cnt);
+      cudaError_t e = launch_expand_regular(rm, nch, (const unsigned long long*)s->key.p + first, count_slot, cnt,
+                                            nullptr, (unsigned long long*)s->tmp_simp.p, nullptr, st);
+      if (e) return e;
+      PostBuffers B;
+      memset(&B, 0, sizeof(B));
+      B.cap = cnt;
+      B.count = count_slot;
+      B.simplices = (unsigned long long*)s->tmp_simp.p;
+      B.cls = (unsigned*)s->cls.p + first;
+      ctx->launches += 3;
+      return launch_classify_regular(f64, rm, fa, nch, B, st);
+    };
+    S_TRY(ctx, classify(first_new, n_new, counters + kCountRoots));
+    if (T == 1) S_TRY(ctx, classify(0, s->n_first, counters + kCountRoots));
+  }
+  S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
+  S_TRY(ctx, cudaStreamSynchronize(st));
+  const unsigned* h = ctx->h_counters;
+  if (h[kCountErr] & 1u) return sfail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
+  s->n_edges += h[kSWinEdges];
+  s->n_prev = h[kSPrev];
+  std::swap(s->prev_ids, s->prev_ids2);
+  s->n += n_new;
+  if (T == 0) s->n_first = n_new;
+  s->last_new = n_new;
+  return FTK2B_OK;
+}
+
+ftk2b_status result_regular(ftk2b_stream* s, ftk2b_cp_result** out) {
+  ftk2b_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  const int d = s->d, M = s->m, nch = d == 3 ? 12 : 60;
+  const unsigned n = s->n, ne = s->n_edges;
+  const unsigned nc = n ? n : 1, ec = ne ? ne : 1;
+  S_TRY(ctx, ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
+  unsigned* counters = (unsigned*)ctx->counters.p;
+  // canonical order of the whole store
+  S_TRY(ctx, s->s_key.ensure(8 * (size_t)(nc > ec ? nc : ec)));
+  S_TRY(ctx, s->s_key2.ensure(8 * (size_t)(nc > ec ? nc : ec)));
+  S_TRY(ctx, s->s_id.ensure(4 * (size_t)(nc > ec ? nc : ec)));
+  S_TRY(ctx, s->s_id2.ensure(4 * (size_t)(nc > ec ? nc : ec)));
+  S_TRY(ctx, ctx->perm0.ensure(4 * (size_t)nc));  // inverse permutation
+  S_TRY(ctx, ctx->perm1.ensure(4 * (size_t)nc));  // roots
+  S_TRY(ctx, ctx->parent.ensure(4 * (size_t)nc)); // component minimum
+  S_TRY(ctx, ctx->lam_s.ensure(32 * (size_t)nc));
+  S_TRY(ctx, ctx->bary4_s.ensure(16 * (size_t)nc));
+  S_TRY(ctx, ctx->scalar_s.ensure(4 * (size_t)nc));
+  S_TRY(ctx, ctx->cls.ensure(4 * (size_t)nc));
+  S_TRY(ctx, ctx->track.ensure(8 * (size_t)nc));
+  S_TRY(ctx, ctx->simplices.ensure(8 * (size_t)(M + 1) * nc));
+  S_TRY(ctx, ctx->bary.ensure(4 * (size_t)(M + 1) * nc));
+  S_TRY(ctx, ctx->edges.ensure(8 * (size_t)ec));
+  const int sgrid = ctx->sort_grid(nc > ec ? nc : ec);
+  S_TRY(ctx, ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)sgrid));
+  const int g = grid_of(nc > ec ? nc : ec, 256, 4096);
+  S_TRY(ctx, cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, st));
+  set_u32_kernel<<<1, 1, 0, st>>>(counters + kSWin, n);
+  set_u32_kernel<<<1, 1, 0, st>>>(counters + kSWinEdges, ne);
+  if (n) S_TRY(ctx, cudaMemcpyAsync(s->s_key.p, s->key.p, 8 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+  iota_u32_kernel<<<g, 256, 0, st>>>((unsigned*)s->s_id.p, n);
+  const RegularMesh full = window_mesh(s, 0, s->T);
+  const unsigned long long nv_hi = (unsigned long long)full.gstride[d - 1] * (s->T + 1);
+  const bool alt = radix_sort((unsigned long long*)s->s_key.p, (unsigned*)s->s_id.p, (unsigned long long*)s->s_key2.p,
+                              (unsigned*)s->s_id2.p, counters + kSWin, nc, bits_for(nv_hi * (unsigned long long)nch),
+                              (unsigned*)ctx->hist.p, sgrid, st, &ctx->launches);
+  const unsigned long long* skeys = (const unsigned long long*)(alt ? s->s_key2.p : s->s_key.p);
+  const unsigned* perm = (const unsigned*)(alt ? s->s_id2.p : s->s_id.p);
+  unsigned* inv = (unsigned*)ctx->perm0.p;
+  unsigned* root = (unsigned*)ctx->perm1.p;
+  unsigned* cmin = (unsigned*)ctx->parent.p;
+  invert_kernel<<<g, 256, 0, st>>>(perm, n, inv);
+  fill_u32_kernel<<<g, 256, 0, st>>>(cmin, n, 0xFFFFFFFFu);
+  comp_min_kernel<<<g, 256, 0, st>>>((unsigned*)s->parent.p, inv, n, root, cmin, counters + kCountRoots);
+  gather_result_kernel<<<g, 256, 0, st>>>(perm, n, root, cmin, (const double*)s->lam.p, (const float*)s->bary4.p,
+                                          (const float*)s->scalar.p, (const unsigned*)s->cls.p,
+                                          (double*)ctx->lam_s.p, (float*)ctx->bary4_s.p, (float*)ctx->scalar_s.p,
+                                          (unsigned*)ctx->cls.p, (unsigned long long*)ctx->track.p);
+  S_TRY(ctx, launch_expand_regular(full, nch, skeys, counters + kSWin, nc, (const float*)ctx->bary4_s.p,
+                                   (unsigned long long*)ctx->simplices.p, (float*)ctx->bary.p, st));
+  // edges in canonical ids, sorted (each pair spans one top cell: no duplicates)
+  unsigned long long* ek = (unsigned long long*)s->s_key.p;  // free again after the gathers
+  canon_edges_kernel<<<g, 256, 0, st>>>((const unsigned*)s->edges.p, ne, inv, ek);
+  const bool ealt = radix_sort(ek, (unsigned*)s->s_id.p, (unsigned long long*)s->s_key2.p, (unsigned*)s->s_id2.p,
+                               counters + kSWinEdges, ec, 2 * 32, (unsigned*)ctx->hist.p, sgrid, st, &ctx->launches);
+  unpack_edges_kernel<<<g, 256, 0, st>>>(ealt ? (const unsigned long long*)s->s_key2.p : ek, ne,
+                                         (unsigned*)ctx->edges.p);
+  ctx->launches += 7;
+  S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
+  S_TRY(ctx, cudaStreamSynchronize(st));
+  // hand the canonical buffers to the context's fetch
+  ctx->last.kind = FTK2B_MESH_REGULAR;
+  ctx->last.m = M;
+  ctx->last.n = n;
+  ctx->last.ne = s->prm.want_edges ? ne : 0;
+  ctx->last.n_roots = ctx->h_counters[kCountRoots];
+  ftk2b_mesh_desc md;
+  memset(&md, 0, sizeof(md));
+  md.kind = FTK2B_MESH_REGULAR;
+  md.ndims = d;
+  for (int k = 0; k < d - 1; ++k) md.local_dims[k] = s->ld[k];
+  md.local_dims[d - 1] = s->T;
+  ctx->last.n_simplices = ftk2b_mesh_simplex_count(&md, M);
+  ctx->last.device_ms = 0;
+  ctx->last.classify = s->prm.classify;
+  ctx->last.want_edges = s->prm.want_edges;
+  return ftk2b_cp_fetch(ctx, out);
+}
+
+}  // namespace
+
+namespace ftk2b {
+
+cudaError_t grow_keep(DevBuf& b, size_t used, size_t want, cudaStream_t st) {
+  if (b.p && b.bytes >= want) return cudaSuccess;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want < 256 ? 256 : want);
+  if (e) {
+    cudaGetLastError();
+    return e;
+  }
+  if (b.p && used) {
+    e = cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (e) {
+      cudaFree(p);
+      return e;
+    }
+  }
+  if (b.p) cudaFree(b.p);
+  b.p = p;
+  b.bytes = want < 256 ? 256 : want;
+  ++b.generation;
+  return cudaSuccess;
+}
+
+}  // namespace ftk2b
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" ftk2b_status ftk2b_stream_open(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* tmpl,
+                                          const ftk2b_cp_params* params, ftk2b_stream** out) {
+  if (!ctx || !out) return FTK2B_INVALID_ARG;
+  *out = nullptr;
+  if (!mesh || !tmpl) return sfail(ctx, FTK2B_INVALID_ARG, "null descriptor");
+  ftk2b_cp_params prm = params ? *params : ftk2b_cp_params_default();
+  if (!(prm.sos_q > 0)) return sfail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
+  if (tmpl->dtype != FTK2B_F32 && tmpl->dtype != FTK2B_F64)
+    return sfail(ctx, FTK2B_INVALID_ARG, "dtype must be FTK2B_F32 or FTK2B_F64");
+  if (tmpl->scalar) return sfail(ctx, FTK2B_UNSUPPORTED, "streams do not interpolate a scalar");
+  ftk2b_stream* s = new ftk2b_stream();
+  s->ctx = ctx;
+  s->kind = mesh->kind;
+  s->prm = prm;
+  s->dtype = tmpl->dtype;
+  s->layout = tmpl->layout;
+  s->ncomp = tmpl->ncomp;
+  s->location = tmpl->location;
+  s->es = tmpl->dtype == FTK2B_F64 ? 8 : 4;
+  if (mesh->kind == FTK2B_MESH_REGULAR) {
+    const int d = mesh->ndims;
+    if (d != 3 && d != 4) {
+      delete s;
+      return sfail(ctx, FTK2B_UNSUPPORTED, "regular streams need 3 or 4 dims including time");
+    }
+    s->d = d;
+    s->m = d - 1;
+    if (tmpl->ncomp != s->m) {
+      delete s;
+      return sfail(ctx, FTK2B_INVALID_ARG, "a %dD spacetime mesh needs %d components", d, d - 1);
+    }
+    if (tmpl->layout != FTK2B_LAYOUT_MULTICOMPONENT && tmpl->layout != FTK2B_LAYOUT_SEPARATE) {
+      delete s;
+      return sfail(ctx, FTK2B_UNSUPPORTED, "regular streams take multicomponent or separate arrays");
+    }
+    if (tmpl->nd != d - 1) {
+      delete s;
+      return sfail(ctx, FTK2B_INVALID_ARG, "a timestep has %d spatial dims", d - 1);
+    }
+    s->slice_elems = 1;
+    for (int k = 0; k < d - 1; ++k) {
+      s->ld[k] = mesh->local_dims[k];
+      s->off[k] = mesh->offset[k];
+      s->gd[k] = mesh->global_dims[k];
+      s->adims[k] = tmpl->dims[k];
+      const uint64_t need = tmpl->layout == FTK2B_LAYOUT_SEPARATE ? s->ld[k] : s->off[k] + s->ld[k];
+      if (s->ld[k] < 1 || s->off[k] + s->ld[k] > s->gd[k] || s->adims[k] < need || s->ld[k] >= 65536) {
+        delete s;
+        return sfail(ctx, FTK2B_INVALID_ARG, "inconsistent stream mesh / array dims along axis %d", k);
+      }
+      s->slice_elems *= s->adims[k];
+    }
+    if (tmpl->layout == FTK2B_LAYOUT_MULTICOMPONENT) s->slice_elems *= s->m;
+  } else if (mesh->kind == FTK2B_MESH_EXTRUDED) {
+    const int cd = mesh->base_cell_dim;
+    if ((cd != 2 && cd != 3) || tmpl->ncomp != cd || !mesh->base_cells || !mesh->n_base_cells) {
+      delete s;
+      return sfail(ctx, FTK2B_INVALID_ARG, "extruded streams need triangle or tet cells and ncomp = cell dim");
+    }
+    if (tmpl->layout == FTK2B_LAYOUT_MULTICOMPONENT) {
+      delete s;
+      return sfail(ctx, FTK2B_UNSUPPORTED, "extruded streams take per-vertex arrays");
+    }
+    s->d = cd + 1;
+    s->m = cd;
+    s->emesh = *mesh;
+    s->ecells.assign(mesh->base_cells, mesh->base_cells + mesh->n_base_cells * (cd + 1));
+    s->emesh.base_cells = s->ecells.data();
+    s->slice_elems = mesh->n_base_verts;
+  } else {
+    delete s;
+    return sfail(ctx, FTK2B_INVALID_ARG, "unknown mesh kind %d", mesh->kind);
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+    delete s;
+    return sfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  }
+  const int narr = s->layout == FTK2B_LAYOUT_MULTICOMPONENT ? 1 : s->m;
+  for (int j = 0; j < narr; ++j)
+    if (s->ring[j].ensure(2 * s->slice_elems * s->es) != cudaSuccess) {
+      for (auto& b : s->ring) b.release();
+      delete s;
+      return sfail(ctx, FTK2B_OOM, "stream ring allocation failed");
+    }
+  *out = s;
+  return FTK2B_OK;
+}
+
+extern "C" ftk2b_status ftk2b_stream_push(ftk2b_stream* s, const ftk2b_field_desc* step, uint64_t* n_new) {
+  if (!s) return FTK2B_INVALID_ARG;
+  ftk2b_ctx* ctx = s->ctx;
+  if (!step) return sfail(ctx, FTK2B_INVALID_ARG, "null timestep");
+  if (step->dtype != s->dtype || step->ncomp != s->ncomp || step->layout != s->layout)
+    return sfail(ctx, FTK2B_INVALID_ARG, "timestep dtype / ncomp / layout differ from the stream's");
+  if (s->kind == FTK2B_MESH_REGULAR) {
+    if (step->nd != s->d - 1) return sfail(ctx, FTK2B_INVALID_ARG, "a timestep has %d spatial dims", s->d - 1);
+    for (int k = 0; k < s->d - 1; ++k)
+      if (step->dims[k] != s->adims[k]) return sfail(ctx, FTK2B_INVALID_ARG, "timestep dims differ along axis %d", k);
+  } else {
+    if (step->dims[0] < s->emesh.n_base_verts)
+      return sfail(ctx, FTK2B_INVALID_ARG, "per-vertex timestep shorter than the base vertex count");
+  }
+  if (s->T + 2 >= (1ull << 30)) return sfail(ctx, FTK2B_UNSUPPORTED, "a stream holds fewer than 2^30 timesteps");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return sfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  cudaStream_t st = ctx->stream;
+  S_TRY(ctx, cudaEventRecord(ctx->ev0, st));
+  const int narr = s->layout == FTK2B_LAYOUT_MULTICOMPONENT ? 1 : s->m;
+  const size_t bytes = s->slice_elems * s->es;
+  const size_t slot = (size_t)(s->T & 1);
+  for (int j = 0; j < narr; ++j) {
+    if (!step->comp[j]) return sfail(ctx, FTK2B_INVALID_ARG, "component array %d is null", j);
+    S_TRY(ctx, cudaMemcpyAsync((char*)s->ring[j].p + slot * bytes, step->comp[j], bytes,
+                               step->location == FTK2B_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               st));
+  }
+  ftk2b_status rc = s->kind == FTK2B_MESH_REGULAR ? push_regular(s) : stream_push_extruded(s);
+  if (rc) return rc;
+  S_TRY(ctx, cudaEventRecord(ctx->ev1, st));
+  S_TRY(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) ms = 0.f;
+  cudaGetLastError();
+  s->last_ms = ms;
+  s->T += 1;
+  if (n_new) *n_new = s->last_new;
+  return FTK2B_OK;
+}
+
+extern "C" ftk2b_status ftk2b_stream_result(ftk2b_stream* s, ftk2b_cp_result** out) {
+  if (!s || !out) return FTK2B_INVALID_ARG;
+  *out = nullptr;
+  if (cudaSetDevice(s->ctx->device) != cudaSuccess) return sfail(s->ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  return s->kind == FTK2B_MESH_REGULAR ? result_regular(s, out) : stream_result_extruded(s, out);
+}
+
+extern "C" ftk2b_status ftk2b_stream_info(ftk2b_stream* s, uint64_t* timesteps, uint64_t* n_features,
+                                          double* last_push_ms) {
+  if (!s) return FTK2B_INVALID_ARG;
+  if (timesteps) *timesteps = s->T;
+  if (n_features) *n_features = s->n;
+  if (last_push_ms) *last_push_ms = s->last_ms;
+  return FTK2B_OK;
+}
+
+extern "C" void ftk2b_stream_close(ftk2b_stream* s) {
+  if (!s) return;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  for (DevBuf* b : {&s->ring[0], &s->ring[1], &s->ring[2], &s->key, &s->hi, &s->lo, &s->phase, &s->lam, &s->bary4,
+                    &s->scalar, &s->cls, &s->parent, &s->edges, &s->prev_ids, &s->prev_ids2, &s->s_key, &s->s_key2,
+                    &s->s_id, &s->s_id2, &s->s_hi, &s->s_lo, &s->s_phase, &s->wedges, &s->tmp_simp, &s->dummy})
+    b->release();
+  delete s;
+}

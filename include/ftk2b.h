@@ -176,6 +176,32 @@ ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out);
 ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* total_ms,
                                    uint64_t* kernels_launched);
 
+/* --- time streams ----------------------------------------------------------
+ * Replaces the reference's streaming drivers (SimplicialEngine::execute_stream
+ * and execute_cuda_streaming_regular, engine.hpp:214-270, 601-819) with
+ * one-shot semantics: after T pushes, ftk2b_stream_result returns exactly what
+ * ftk2b_cp_extract returns for the T-timestep spacetime mesh.  Only the two
+ * newest timesteps of the field, the features, their star edges and the
+ * union-find state stay on the device; each push extracts the simplices whose
+ * last layer is the new timestep and links them to the previous layer.
+ *
+ * mesh: REGULAR with ndims = spatial dims + 1 (the time entries are ignored)
+ *       or EXTRUDED (n_layers is ignored).
+ * tmpl: dtype, ncomp, layout, location and dims of ONE timestep
+ *       (nd = spatial dims; per-vertex arrays for extruded meshes); no scalar.
+ * A stream uses its context's stream and scratch buffers: do not interleave
+ * calls on one context from several threads. */
+typedef struct ftk2b_stream ftk2b_stream;
+ftk2b_status ftk2b_stream_open(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* tmpl,
+                               const ftk2b_cp_params* params, ftk2b_stream** out);
+/* Pushes the next timestep (same dtype / layout / dims as the template);
+ * *n_new receives the number of features whose last layer is this timestep. */
+ftk2b_status ftk2b_stream_push(ftk2b_stream* s, const ftk2b_field_desc* step, uint64_t* n_new);
+/* The complex of every timestep pushed so far (get_complex, engine.hpp:822-996). */
+ftk2b_status ftk2b_stream_result(ftk2b_stream* s, ftk2b_cp_result** out);
+ftk2b_status ftk2b_stream_info(ftk2b_stream* s, uint64_t* timesteps, uint64_t* n_features, double* last_push_ms);
+void ftk2b_stream_close(ftk2b_stream* s);
+
 /* --- allocation-free extraction -------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory while they run (an in-situ step inside a simulation whose allocator
