@@ -34,6 +34,7 @@
 
 #include "cp_api_internal.h"
 #include "cp_stream.h"
+#include "cp_stream_kernels.cuh"
 #include "cp_cull.cuh"
 #include "cp_device.cuh"
 #include "cp_uf.cuh"
@@ -563,7 +564,9 @@ __global__ void ext_unpack_edges_kernel(const unsigned long long* __restrict__ e
 // last layer-t vertex: for a lateral piece that is its own base face (the true
 // cofaces); for an interior simplex it is a face of its cell, and the pieces
 // of the neighbouring cell across that face join the component as well.
-__global__ void ext_coface_union_kernel(ExtMeshDev X, ExtFeatures Fs, unsigned* parent, unsigned* err) {
+// ids: union-find index of each feature (null: the feature index itself)
+__global__ void ext_coface_union_kernel(ExtMeshDev X, ExtFeatures Fs, const unsigned* __restrict__ ids,
+                                        unsigned* parent, unsigned* err) {
   constexpr int M = 3;
   const unsigned n = min(*Fs.n_ptr, Fs.cap);
   const unsigned long long ns = X.ns;
@@ -601,7 +604,8 @@ __global__ void ext_coface_union_kernel(ExtMeshDev X, ExtFeatures Fs, unsigned* 
       for (int k = jp; k <= M; ++k) cell[w++] = (t + 1) * ns + u[k];
       long long act[5];
       const int na = cell_features<M>(Fs, n, cell, act);
-      for (int a = 0; a < na; ++a) uf_unite(parent, i, (unsigned)act[a], err);
+      for (int a = 0; a < na; ++a)
+        uf_unite(parent, ids ? ids[i] : i, ids ? ids[act[a]] : (unsigned)act[a], err);
     }
   }
 }
@@ -663,11 +667,12 @@ ftk2b_status validate_mesh(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, int* fbi
 }
 
 // Builds (or reuses) the device copy of the base mesh.
-ftk2b_status prepare_base(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, int fbits, unsigned long long* nl) {
+ftk2b_status prepare_base(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, int fbits, unsigned long long* nl,
+                          const uint64_t* known_hash = nullptr) {
   ExtCache& C = ctx->ext;
   const int cd = mesh->base_cell_dim;
   const uint64_t nent64 = mesh->n_base_cells * (uint64_t)(cd + 1);
-  const uint64_t h = hash_cells(mesh->base_cells, nent64);
+  const uint64_t h = known_hash ? *known_hash : hash_cells(mesh->base_cells, nent64);
   if (C.valid && C.hash == h && C.ncell == mesh->n_base_cells && C.ns == mesh->n_base_verts && C.cd == cd)
     return FTK2B_OK;
   C.valid = false;
@@ -799,7 +804,7 @@ cudaError_t enqueue_post(ftk2b_ctx* ctx, const ExtMeshDev& X, const ExtSink& sin
   if ((e = launch_uf((unsigned*)ctx->parent.p, count, cap, (const unsigned*)ctx->edges.p, n_edges, edge_cap, err,
                      st)))
     return e;
-  if (M == 3) ext_coface_union_kernel<<<g, 256, 0, st>>>(X, Fs, (unsigned*)ctx->parent.p, err);
+  if (M == 3) ext_coface_union_kernel<<<g, 256, 0, st>>>(X, Fs, nullptr, (unsigned*)ctx->parent.p, err);
   if ((e = launch_uf_label((unsigned*)ctx->parent.p, count, cap, (unsigned long long*)ctx->track.p,
                            counters + kCountRoots, st)))
     return e;
@@ -813,14 +818,350 @@ cudaError_t enqueue_post(ftk2b_ctx* ctx, const ExtMeshDev& X, const ExtSink& sin
 
 using namespace ftk2b;
 
-ftk2b_status stream_push_extruded(ftk2b_stream* s) {
-  s->ctx->err = "extruded streams are not implemented yet";
-  return FTK2B_UNSUPPORTED;
+// ---------------------------------------------------------------------------
+// extruded time streams (the driver and its contract: cp_stream.cu)
+
+namespace ftk2b {
+namespace {
+
+enum { kSWin = 5, kSWinEdges = 6, kSPrev = 7 };
+constexpr int kStreamVb = 32;  // fixed id width of a stream's packed tuples
+
+__global__ void ext_window_build_kernel(const unsigned long long* __restrict__ lo, const unsigned* __restrict__ prev,
+                                        unsigned n_prev, unsigned first_new, unsigned n_new,
+                                        unsigned long long* __restrict__ k_out, unsigned* __restrict__ id_out) {
+  const unsigned nS = n_prev + n_new;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += gridDim.x * blockDim.x) {
+    const unsigned id = i < n_prev ? prev[i] : first_new + (i - n_prev);
+    k_out[i] = lo[id];
+    id_out[i] = id;
+  }
 }
 
-ftk2b_status stream_result_extruded(ftk2b_stream* s, ftk2b_cp_result**) {
-  s->ctx->err = "extruded streams are not implemented yet";
-  return FTK2B_UNSUPPORTED;
+__global__ void ext_gather_key_kernel(const unsigned long long* __restrict__ src, const unsigned* __restrict__ ids,
+                                      const unsigned* n_ptr, unsigned cap, unsigned long long* __restrict__ dst) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[ids[i]];
+}
+
+__global__ void ext_window_fill_kernel(const unsigned* __restrict__ ids, const unsigned* n_ptr, unsigned cap,
+                                       const unsigned long long* __restrict__ hi,
+                                       const unsigned long long* __restrict__ lo, const unsigned* __restrict__ phase,
+                                       unsigned long long* __restrict__ hi_s, unsigned long long* __restrict__ lo_s,
+                                       unsigned* __restrict__ phase_s) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned id = ids[i];
+    hi_s[i] = hi[id];
+    lo_s[i] = lo[id];
+    phase_s[i] = phase[id];
+  }
+}
+
+// window star edges (packed window indices) -> stream ids, united and stored
+__global__ void ext_append_edges_kernel(const unsigned long long* __restrict__ ek, const unsigned* n_ptr,
+                                        unsigned cap, const unsigned* __restrict__ ids, unsigned* parent,
+                                        unsigned* __restrict__ out, unsigned base, unsigned out_cap, unsigned* err) {
+  const unsigned n = min(*n_ptr, cap);
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const unsigned a = ids[(unsigned)(ek[e] >> 32)], b = ids[(unsigned)ek[e]];
+    uf_unite(parent, a, b, err);
+    if (base + e < out_cap) {
+      out[2 * (size_t)(base + e)] = a;
+      out[2 * (size_t)(base + e) + 1] = b;
+    }
+  }
+}
+
+template <int M>
+__global__ void ext_collect_spatial_kernel(const unsigned long long* __restrict__ hi,
+                                           const unsigned long long* __restrict__ lo, unsigned first_new,
+                                           unsigned n_new, unsigned long long ns, unsigned long long t,
+                                           unsigned* __restrict__ prev, unsigned* prev_n) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+    const unsigned id = first_new + i;
+    unsigned long long v[4];
+    unpack_tuple<M>(hi[id], lo[id], kStreamVb, v);
+    if (v[0] / ns == t && v[M] / ns == t) prev[atomicAdd(prev_n, 1u)] = id;
+  }
+}
+
+template <int M>
+__global__ void ext_stream_expand_kernel(const unsigned* __restrict__ perm, unsigned n,
+                                         const unsigned long long* __restrict__ hi,
+                                         const unsigned long long* __restrict__ lo, const float* __restrict__ bary4_s,
+                                         unsigned long long* __restrict__ simplices, float* __restrict__ bary) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned p = perm[i];
+    unsigned long long v[4];
+    unpack_tuple<M>(hi[p], lo[p], kStreamVb, v);
+    for (int k = 0; k <= M; ++k) {
+      simplices[(size_t)i * (M + 1) + k] = v[k];
+      bary[(size_t)i * (M + 1) + k] = bary4_s[4 * (size_t)i + k];
+    }
+  }
+}
+
+ExtMeshDev stream_mesh(ftk2b_ctx* ctx, const ftk2b_stream* s, unsigned t0, unsigned L) {
+  ExtCache& C = ctx->ext;
+  ExtMeshDev X;
+  X.cd = s->m;
+  X.ns = (unsigned)s->emesh.n_base_verts;
+  X.L = L;
+  X.t0 = t0;
+  X.tflip = t0 & 1u;
+  X.skip_first_spatial = 0;
+  X.ncell = (unsigned)C.ncell;
+  X.nface = C.nface;
+  X.fbits = C.fbits;
+  X.cells = (const unsigned*)C.cells.p;
+  X.fkeys = (const unsigned long long*)C.fkeys.p;
+  X.cof_start = (const unsigned*)C.cof_start.p;
+  X.cof = (const unsigned*)C.cof.p;
+  return X;
+}
+
+// sorts ids [0, n) (in k0/v0 order of the window or store) by (hi, lo);
+// returns the buffer holding the sorted ids
+unsigned* sort_by_tuple(ftk2b_ctx* ctx, ftk2b_stream* s, const unsigned* n_ptr, unsigned cap, int bits,
+                        unsigned long long* nl) {
+  cudaStream_t st = ctx->stream;
+  const int sgrid = ctx->sort_grid(cap);
+  unsigned* hist = (unsigned*)ctx->hist.p;
+  bool alt = radix_sort((unsigned long long*)s->s_key.p, (unsigned*)s->s_id.p, (unsigned long long*)s->s_key2.p,
+                        (unsigned*)s->s_id2.p, n_ptr, cap, bits, hist, sgrid, st, nl);
+  unsigned* ids = (unsigned*)(alt ? s->s_id2.p : s->s_id.p);
+  unsigned* ids_other = (unsigned*)(alt ? s->s_id.p : s->s_id2.p);
+  unsigned long long* kfree = (unsigned long long*)(alt ? s->s_key.p : s->s_key2.p);
+  unsigned long long* kother = (unsigned long long*)(alt ? s->s_key2.p : s->s_key.p);
+  ext_gather_key_kernel<<<grid_of(cap, 256, 4096), 256, 0, st>>>((const unsigned long long*)s->hi.p, ids, n_ptr, cap,
+                                                                 kfree);
+  alt = radix_sort(kfree, ids, kother, ids_other, n_ptr, cap, bits, hist, sgrid, st, nl);
+  *nl += 1;
+  return alt ? ids_other : ids;
+}
+
+template <typename T, int M>
+ftk2b_status push_extruded_t(ftk2b_stream* s) {
+  ftk2b_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  unsigned long long nl = 0;
+  int fbits = 0;
+  ftk2b_status rc = validate_mesh(ctx, &s->emesh, &fbits);
+  if (rc) return rc;
+  const uint64_t tnow = s->T;
+  const unsigned long long ns = s->emesh.n_base_verts;
+  if (ns * (tnow + 1) > 0xFFFFFFFFull) return ext_fail(ctx, FTK2B_UNSUPPORTED, "spacetime vertex ids exceed 32 bits");
+  rc = prepare_base(ctx, &s->emesh, fbits, &nl, &s->ebase_hash);
+  if (rc) return rc;
+  const unsigned t0 = tnow ? (unsigned)(tnow - 1) : 0u, L = tnow ? 1u : 0u;
+  ExtMeshDev X = stream_mesh(ctx, s, t0, L);
+  X.skip_first_spatial = tnow > 0;
+  FieldAccess fa;
+  memset(&fa, 0, sizeof(fa));
+  fa.per_vertex = 1;
+  for (int j = 0; j < M; ++j) fa.comp[j] = s->ring[j].p;
+  ExtractConfig cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.Q = s->prm.sos_q;
+  cfg.refined = s->prm.precision == FTK2B_PRECISION_REFINED;
+  const unsigned long long nv = ns * (L + 1);
+  ExtCache& C = ctx->ext;
+  EXT_TRY(C.words.ensure(sizeof(unsigned) * nv));
+  EXT_TRY(ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
+  unsigned* counters = (unsigned*)ctx->counters.p;
+  unsigned n_new = 0;
+  for (int attempt = 0;; ++attempt) {
+    if (attempt == 6) return ext_fail(ctx, FTK2B_OVERFLOW_RETRY, "stream buffers kept overflowing");
+    if (s->cap < s->n + 1024) {
+      rc = ensure_stream_store(s, s->n + 1024);
+      if (rc) return rc;
+    }
+    EXT_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, st));
+    ExtSink sink;
+    sink.hi = (unsigned long long*)s->hi.p + s->n;
+    sink.lo = (unsigned long long*)s->lo.p + s->n;
+    sink.phase = (unsigned*)s->phase.p + s->n;
+    sink.lam = (double*)s->lam.p + 4 * (size_t)s->n;
+    sink.bary4 = (float*)s->bary4.p + 4 * (size_t)s->n;
+    sink.scalar = (float*)s->scalar.p + s->n;
+    sink.count = counters + kCountFeatures;
+    sink.cap = s->cap - s->n;
+    EXT_TRY((enqueue_extract<T, M>(ctx, X, fa, cfg, sink, kStreamVb, nv, &nl)));
+    EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
+    EXT_TRY(cudaStreamSynchronize(st));
+    const unsigned got = ctx->h_counters[kCountFeatures];
+    if (got > s->cap - s->n) {
+      rc = ensure_stream_store(s, s->n + got + got / 4 + 1024);
+      if (rc) return rc;
+      continue;
+    }
+    n_new = got;
+    break;
+  }
+
+  // window: spatial features of layer t-1 plus the new ones, in Simplex order
+  const unsigned first_new = s->n;
+  const unsigned nS = s->n_prev + n_new;
+  const unsigned wcap = nS ? nS : 1;
+  const unsigned wecap = kMaxOthers * wcap;
+  EXT_TRY(s->s_key.ensure(8 * (size_t)wcap));
+  EXT_TRY(s->s_key2.ensure(8 * (size_t)wcap));
+  EXT_TRY(s->s_id.ensure(4 * (size_t)wcap));
+  EXT_TRY(s->s_id2.ensure(4 * (size_t)wcap));
+  EXT_TRY(s->s_hi.ensure(8 * (size_t)wcap));
+  EXT_TRY(s->s_lo.ensure(8 * (size_t)wcap));
+  EXT_TRY(s->s_phase.ensure(4 * (size_t)wcap));
+  EXT_TRY(s->wedges.ensure(8 * (size_t)wecap));
+  EXT_TRY(ctx->edge_cnt.ensure(4 * (size_t)wcap));
+  EXT_TRY(ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)ctx->sort_grid(wcap > wecap ? wcap : wecap)));
+  const unsigned edge_room = s->n_edges + wecap;
+  if (edge_room > s->edge_cap) {
+    unsigned nc = s->edge_cap ? s->edge_cap : 65536u;
+    while (nc < edge_room) nc *= 2;
+    EXT_TRY(grow_keep(s->edges, 8 * (size_t)s->n_edges, 8 * (size_t)nc, st));
+    s->edge_cap = nc;
+  }
+  const int g = grid_of(wcap, 256, 4096);
+  set_u32_kernel<<<1, 1, 0, st>>>(counters + kSWin, nS);
+  ext_window_build_kernel<<<g, 256, 0, st>>>((const unsigned long long*)s->lo.p, (const unsigned*)s->prev_ids.p,
+                                             s->n_prev, first_new, n_new, (unsigned long long*)s->s_key.p,
+                                             (unsigned*)s->s_id.p);
+  const int bits = kStreamVb + bits_of(ns * (tnow + 1));
+  const unsigned* ids = sort_by_tuple(ctx, s, counters + kSWin, wcap, bits, &nl);
+  ext_window_fill_kernel<<<g, 256, 0, st>>>(ids, counters + kSWin, wcap, (const unsigned long long*)s->hi.p,
+                                            (const unsigned long long*)s->lo.p, (const unsigned*)s->phase.p,
+                                            (unsigned long long*)s->s_hi.p, (unsigned long long*)s->s_lo.p,
+                                            (unsigned*)s->s_phase.p);
+  ExtFeatures Fs;
+  Fs.hi = (const unsigned long long*)s->s_hi.p;
+  Fs.lo = (const unsigned long long*)s->s_lo.p;
+  Fs.phase = (const unsigned*)s->s_phase.p;
+  Fs.n_ptr = counters + kSWin;
+  Fs.cap = wcap;
+  Fs.vb = kStreamVb;
+  unsigned* err = counters + kCountErr;
+  unsigned* ecnt = (unsigned*)ctx->edge_cnt.p;
+  unsigned long long* ek = (unsigned long long*)s->wedges.p;
+  ext_edges_kernel<M, 0><<<g, 256, 0, st>>>(X, Fs, ecnt, nullptr, ek, wecap, err);
+  EXT_TRY(launch_scan(ecnt, wcap, counters + kSWinEdges, counters + kSWin, st));
+  ext_edges_kernel<M, 1><<<g, 256, 0, st>>>(X, Fs, nullptr, ecnt, ek, wecap, err);
+  if (n_new) uf_init_range_kernel<<<grid_of(n_new, 256, 4096), 256, 0, st>>>((unsigned*)s->parent.p, first_new, n_new);
+  ext_append_edges_kernel<<<grid_of(wecap, 256, 4096), 256, 0, st>>>(ek, counters + kSWinEdges, wecap, ids,
+                                                                    (unsigned*)s->parent.p, (unsigned*)s->edges.p,
+                                                                    s->n_edges, s->edge_cap, err);
+  if (M == 3) ext_coface_union_kernel<<<g, 256, 0, st>>>(X, Fs, ids, (unsigned*)s->parent.p, err);
+  if (n_new)
+    ext_collect_spatial_kernel<M><<<grid_of(n_new, 256, 4096), 256, 0, st>>>(
+        (const unsigned long long*)s->hi.p, (const unsigned long long*)s->lo.p, first_new, n_new, ns, tnow,
+        (unsigned*)s->prev_ids2.p, counters + kSPrev);
+  nl += 9;
+  EXT_TRY(cudaGetLastError());
+  EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
+  EXT_TRY(cudaStreamSynchronize(st));
+  ctx->launches += nl;
+  const unsigned* h = ctx->h_counters;
+  if (h[kCountErr] & kErrCofaces) return ext_fail(ctx, FTK2B_UNSUPPORTED, "a base face has more than 8 coface cells");
+  if (h[kCountErr] & 1u) return ext_fail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
+  s->n_edges += h[kSWinEdges];
+  s->n_prev = h[kSPrev];
+  std::swap(s->prev_ids, s->prev_ids2);
+  s->n += n_new;
+  if (tnow == 0) s->n_first = n_new;
+  s->last_new = n_new;
+  return FTK2B_OK;
+}
+
+template <int M>
+ftk2b_status result_extruded_t(ftk2b_stream* s, ftk2b_cp_result** out) {
+  ftk2b_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  unsigned long long nl = 0;
+  const unsigned n = s->n, ne = s->n_edges;
+  const unsigned nc = n ? n : 1, ec = ne ? ne : 1, mc = nc > ec ? nc : ec;
+  EXT_TRY(ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
+  unsigned* counters = (unsigned*)ctx->counters.p;
+  EXT_TRY(s->s_key.ensure(8 * (size_t)mc));
+  EXT_TRY(s->s_key2.ensure(8 * (size_t)mc));
+  EXT_TRY(s->s_id.ensure(4 * (size_t)mc));
+  EXT_TRY(s->s_id2.ensure(4 * (size_t)mc));
+  EXT_TRY(ctx->perm0.ensure(4 * (size_t)nc));
+  EXT_TRY(ctx->perm1.ensure(4 * (size_t)nc));
+  EXT_TRY(ctx->parent.ensure(4 * (size_t)nc));
+  EXT_TRY(ctx->lam_s.ensure(32 * (size_t)nc));
+  EXT_TRY(ctx->bary4_s.ensure(16 * (size_t)nc));
+  EXT_TRY(ctx->scalar_s.ensure(4 * (size_t)nc));
+  EXT_TRY(ctx->cls.ensure(4 * (size_t)nc));
+  EXT_TRY(ctx->track.ensure(8 * (size_t)nc));
+  EXT_TRY(ctx->simplices.ensure(8 * (size_t)(M + 1) * nc));
+  EXT_TRY(ctx->bary.ensure(4 * (size_t)(M + 1) * nc));
+  EXT_TRY(ctx->edges.ensure(8 * (size_t)ec));
+  EXT_TRY(ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)ctx->sort_grid(mc)));
+  const int g = grid_of(mc, 256, 4096);
+  EXT_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, st));
+  set_u32_kernel<<<1, 1, 0, st>>>(counters + kSWin, n);
+  set_u32_kernel<<<1, 1, 0, st>>>(counters + kSWinEdges, ne);
+  if (n) EXT_TRY(cudaMemcpyAsync(s->s_key.p, s->lo.p, 8 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+  iota_u32_kernel<<<g, 256, 0, st>>>((unsigned*)s->s_id.p, n);
+  const unsigned long long ns = s->emesh.n_base_verts;
+  const unsigned* perm = sort_by_tuple(ctx, s, counters + kSWin, nc, kStreamVb + bits_of(ns * (s->T + 1)), &nl);
+  unsigned* inv = (unsigned*)ctx->perm0.p;
+  unsigned* root = (unsigned*)ctx->perm1.p;
+  unsigned* cmin = (unsigned*)ctx->parent.p;
+  invert_kernel<<<g, 256, 0, st>>>(perm, n, inv);
+  fill_u32_kernel<<<g, 256, 0, st>>>(cmin, n, 0xFFFFFFFFu);
+  comp_min_kernel<<<g, 256, 0, st>>>((unsigned*)s->parent.p, inv, n, root, cmin, counters + kCountRoots);
+  gather_result_kernel<<<g, 256, 0, st>>>(perm, n, root, cmin, (const double*)s->lam.p, (const float*)s->bary4.p,
+                                          (const float*)s->scalar.p, (const unsigned*)s->cls.p, (double*)ctx->lam_s.p,
+                                          (float*)ctx->bary4_s.p, (float*)ctx->scalar_s.p, (unsigned*)ctx->cls.p,
+                                          (unsigned long long*)ctx->track.p);
+  ext_stream_expand_kernel<M><<<g, 256, 0, st>>>(perm, n, (const unsigned long long*)s->hi.p,
+                                                 (const unsigned long long*)s->lo.p, (const float*)ctx->bary4_s.p,
+                                                 (unsigned long long*)ctx->simplices.p, (float*)ctx->bary.p);
+  // edges in canonical ids, sorted; the id buffers are free after the gathers
+  unsigned long long* ek = (unsigned long long*)(perm == (const unsigned*)s->s_id.p ? s->s_key2.p : s->s_key.p);
+  unsigned long long* ek2 = (unsigned long long*)(perm == (const unsigned*)s->s_id.p ? s->s_key.p : s->s_key2.p);
+  canon_edges_kernel<<<g, 256, 0, st>>>((const unsigned*)s->edges.p, ne, inv, ek);
+  const bool ealt = radix_sort(ek, (unsigned*)s->s_id.p, ek2, (unsigned*)s->s_id2.p, counters + kSWinEdges, ec, 64,
+                               (unsigned*)ctx->hist.p, ctx->sort_grid(mc), st, &nl);
+  unpack_edges_kernel<<<g, 256, 0, st>>>(ealt ? ek2 : ek, ne, (unsigned*)ctx->edges.p);
+  nl += 8;
+  EXT_TRY(cudaGetLastError());
+  EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
+  EXT_TRY(cudaStreamSynchronize(st));
+  ctx->launches += nl;
+  ctx->last.kind = FTK2B_MESH_EXTRUDED;
+  ctx->last.m = M;
+  ctx->last.n = n;
+  ctx->last.ne = s->prm.want_edges ? ne : 0;
+  ctx->last.n_roots = ctx->h_counters[kCountRoots];
+  ftk2b_mesh_desc md = s->emesh;
+  md.n_layers = s->T ? s->T - 1 : 0;
+  ctx->last.n_simplices = s->T ? extruded_simplex_count(&md, M) : 0;
+  ctx->last.device_ms = 0;
+  ctx->last.classify = 0;
+  ctx->last.want_edges = s->prm.want_edges;
+  return ftk2b_cp_fetch(ctx, out);
+}
+
+}  // namespace
+
+uint64_t hash_base_cells(const uint64_t* p, uint64_t n) { return hash_cells(p, n); }
+
+}  // namespace ftk2b
+
+ftk2b_status stream_push_extruded(ftk2b_stream* s) {
+  if (s->prm.classify) {
+    s->ctx->err = "classification of extruded meshes is not available";
+    return FTK2B_UNSUPPORTED;
+  }
+  const bool f64 = s->dtype == FTK2B_F64;
+  if (s->m == 3) return f64 ? push_extruded_t<double, 3>(s) : push_extruded_t<float, 3>(s);
+  return f64 ? push_extruded_t<double, 2>(s) : push_extruded_t<float, 2>(s);
+}
+
+ftk2b_status stream_result_extruded(ftk2b_stream* s, ftk2b_cp_result** out) {
+  return s->m == 3 ? result_extruded_t<3>(s, out) : result_extruded_t<2>(s, out);
 }
 
 uint64_t extruded_simplex_count(const ftk2b_mesh_desc* mesh, int m) {

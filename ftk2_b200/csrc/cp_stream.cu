@@ -25,6 +25,7 @@
 
 #include "cp_post.h"
 #include "cp_stream.h"
+#include "cp_stream_kernels.cuh"
 #include "cp_uf.cuh"
 
 using namespace ftk2b;
@@ -64,8 +65,6 @@ int grid_of(unsigned long long n, int threads, int max_blocks) {
   return (int)b;
 }
 
-__global__ void set_u32_kernel(unsigned* p, unsigned v) { *p = v; }
-
 __global__ void window_build_kernel(const unsigned long long* __restrict__ key, const unsigned* __restrict__ prev,
                                     unsigned n_prev, unsigned first_new, unsigned n_new,
                                     unsigned long long* __restrict__ s_key, unsigned* __restrict__ s_id) {
@@ -77,13 +76,6 @@ __global__ void window_build_kernel(const unsigned long long* __restrict__ key, 
   }
 }
 
-__global__ void uf_init_range_kernel(unsigned* parent, unsigned lo, unsigned n) {
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    parent[lo + i] = lo + i;
-}
-
-// window edges (indices into the sorted window) -> stream ids, united and
-// appended after the `base` edges already stored
 __global__ void append_edges_kernel(const unsigned* __restrict__ wedges, const unsigned* wn_ptr, unsigned wcap,
                                     const unsigned* __restrict__ s_id, unsigned* parent, unsigned* __restrict__ out,
                                     unsigned base, unsigned out_cap, unsigned* err) {
@@ -98,8 +90,6 @@ __global__ void append_edges_kernel(const unsigned* __restrict__ wedges, const u
   }
 }
 
-// new features whose chain does not step in time are the spatial ones of
-// the newest layer
 __global__ void collect_spatial_kernel(const unsigned long long* __restrict__ key, unsigned first_new,
                                        unsigned n_new, int nch, unsigned long long time_chains,
                                        unsigned* __restrict__ prev, unsigned* prev_n) {
@@ -107,64 +97,6 @@ __global__ void collect_spatial_kernel(const unsigned long long* __restrict__ ke
     const unsigned id = first_new + i;
     const unsigned ch = (unsigned)(key[id] % (unsigned long long)nch);
     if (!((time_chains >> ch) & 1ull)) prev[atomicAdd(prev_n, 1u)] = id;
-  }
-}
-
-__global__ void iota_u32_kernel(unsigned* v, unsigned n) {
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
-}
-
-__global__ void invert_kernel(const unsigned* __restrict__ perm, unsigned n, unsigned* __restrict__ inv) {
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) inv[perm[i]] = i;
-}
-
-// component minimum of the canonical ids, through the roots of the stream ids
-__global__ void comp_min_kernel(unsigned* parent, const unsigned* __restrict__ inv, unsigned n,
-                                unsigned* __restrict__ root, unsigned* cmin, unsigned* n_roots) {
-  for (unsigned id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
-    const unsigned r = uf_root(parent, id);
-    root[id] = r;
-    atomicMin(&cmin[r], inv[id]);
-    if (r == id) atomicAdd(n_roots, 1u);
-  }
-}
-
-__global__ void fill_u32_kernel(unsigned* v, unsigned n, unsigned x) {
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = x;
-}
-
-__global__ void canon_edges_kernel(const unsigned* __restrict__ edges, unsigned ne,
-                                   const unsigned* __restrict__ inv, unsigned long long* __restrict__ out) {
-  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
-    const unsigned a = inv[edges[2 * (size_t)e]], b = inv[edges[2 * (size_t)e + 1]];
-    out[e] = ((unsigned long long)min(a, b) << 32) | max(a, b);
-  }
-}
-
-__global__ void unpack_edges_kernel(const unsigned long long* __restrict__ k, unsigned ne, unsigned* __restrict__ out) {
-  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
-    out[2 * (size_t)e] = (unsigned)(k[e] >> 32);
-    out[2 * (size_t)e + 1] = (unsigned)k[e];
-  }
-}
-
-// canonical-order copies of the per-feature records
-__global__ void gather_result_kernel(const unsigned* __restrict__ perm, unsigned n,
-                                     const unsigned* __restrict__ root, const unsigned* __restrict__ cmin,
-                                     const double* __restrict__ lam, const float* __restrict__ bary4,
-                                     const float* __restrict__ sc, const unsigned* __restrict__ cls,
-                                     double* __restrict__ lam_o, float* __restrict__ bary4_o,
-                                     float* __restrict__ sc_o, unsigned* __restrict__ cls_o,
-                                     unsigned long long* __restrict__ track) {
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const unsigned p = perm[i];
-    for (int k = 0; k < 4; ++k) {
-      lam_o[4 * (size_t)i + k] = lam[4 * (size_t)p + k];
-      bary4_o[4 * (size_t)i + k] = bary4[4 * (size_t)p + k];
-    }
-    sc_o[i] = sc[p];
-    cls_o[i] = cls[p];
-    track[i] = cmin[root[p]];
   }
 }
 
@@ -230,31 +162,6 @@ FieldAccess window_field(const ftk2b_stream* s, uint64_t t_start) {
   return fa;
 }
 
-ftk2b_status ensure_store(ftk2b_stream* s, unsigned want) {
-  ftk2b_ctx* ctx = s->ctx;
-  if (want <= s->cap) return FTK2B_OK;
-  unsigned nc = s->cap ? s->cap : 65536u;
-  while (nc < want) nc = nc * 2u > nc ? nc * 2u : 0xFFFFFFF0u;
-  cudaStream_t st = ctx->stream;
-  const size_t n = s->n;
-  if (s->kind == FTK2B_MESH_REGULAR) {
-    S_TRY(ctx, grow_keep(s->key, 8 * n, 8 * (size_t)nc, st));
-  } else {
-    S_TRY(ctx, grow_keep(s->hi, 8 * n, 8 * (size_t)nc, st));
-    S_TRY(ctx, grow_keep(s->lo, 8 * n, 8 * (size_t)nc, st));
-    S_TRY(ctx, grow_keep(s->phase, 4 * n, 4 * (size_t)nc, st));
-  }
-  S_TRY(ctx, grow_keep(s->lam, 32 * n, 32 * (size_t)nc, st));
-  S_TRY(ctx, grow_keep(s->bary4, 16 * n, 16 * (size_t)nc, st));
-  S_TRY(ctx, grow_keep(s->scalar, 4 * n, 4 * (size_t)nc, st));
-  S_TRY(ctx, grow_keep(s->cls, 4 * n, 4 * (size_t)nc, st));
-  S_TRY(ctx, grow_keep(s->parent, 4 * n, 4 * (size_t)nc, st));
-  S_TRY(ctx, grow_keep(s->prev_ids, 4 * (size_t)s->n_prev, 4 * (size_t)nc, st));
-  S_TRY(ctx, s->prev_ids2.ensure(4 * (size_t)nc));
-  s->cap = nc;
-  return FTK2B_OK;
-}
-
 ftk2b_status push_regular(ftk2b_stream* s) {
   ftk2b_ctx* ctx = s->ctx;
   cudaStream_t st = ctx->stream;
@@ -279,7 +186,7 @@ ftk2b_status push_regular(ftk2b_stream* s) {
 
   S_TRY(ctx, ctx->counters.ensure(sizeof(unsigned) * kNumCounters));
   unsigned* counters = (unsigned*)ctx->counters.p;
-  ftk2b_status rc = ensure_store(s, s->n + 1024);
+  ftk2b_status rc = ensure_stream_store(s, s->n + 1024);
   if (rc) return rc;
   unsigned ccap = ctx->cand_cap_hint ? ctx->cand_cap_hint : 65536u;
   unsigned n_new = 0;
@@ -315,7 +222,7 @@ ftk2b_status push_regular(ftk2b_stream* s) {
       continue;
     }
     if (h[kCountFeatures] > s->cap - s->n) {
-      rc = ensure_store(s, s->n + h[kCountFeatures] + h[kCountFeatures] / 4 + 1024);
+      rc = ensure_stream_store(s, s->n + h[kCountFeatures] + h[kCountFeatures] / 4 + 1024);
       if (rc) return rc;
       continue;
     }
@@ -510,6 +417,31 @@ cudaError_t grow_keep(DevBuf& b, size_t used, size_t want, cudaStream_t st) {
   return cudaSuccess;
 }
 
+ftk2b_status ensure_stream_store(ftk2b_stream* s, unsigned want) {
+  ftk2b_ctx* ctx = s->ctx;
+  if (want <= s->cap) return FTK2B_OK;
+  unsigned nc = s->cap ? s->cap : 65536u;
+  while (nc < want) nc = nc * 2u > nc ? nc * 2u : 0xFFFFFFF0u;
+  cudaStream_t st = ctx->stream;
+  const size_t n = s->n;
+  if (s->kind == FTK2B_MESH_REGULAR) {
+    S_TRY(ctx, grow_keep(s->key, 8 * n, 8 * (size_t)nc, st));
+  } else {
+    S_TRY(ctx, grow_keep(s->hi, 8 * n, 8 * (size_t)nc, st));
+    S_TRY(ctx, grow_keep(s->lo, 8 * n, 8 * (size_t)nc, st));
+    S_TRY(ctx, grow_keep(s->phase, 4 * n, 4 * (size_t)nc, st));
+  }
+  S_TRY(ctx, grow_keep(s->lam, 32 * n, 32 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->bary4, 16 * n, 16 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->scalar, 4 * n, 4 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->cls, 4 * n, 4 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->parent, 4 * n, 4 * (size_t)nc, st));
+  S_TRY(ctx, grow_keep(s->prev_ids, 4 * (size_t)s->n_prev, 4 * (size_t)nc, st));
+  S_TRY(ctx, s->prev_ids2.ensure(4 * (size_t)nc));
+  s->cap = nc;
+  return FTK2B_OK;
+}
+
 }  // namespace ftk2b
 
 // ---------------------------------------------------------------------------
@@ -583,6 +515,7 @@ extern "C" ftk2b_status ftk2b_stream_open(ftk2b_ctx* ctx, const ftk2b_mesh_desc*
     s->emesh = *mesh;
     s->ecells.assign(mesh->base_cells, mesh->base_cells + mesh->n_base_cells * (cd + 1));
     s->emesh.base_cells = s->ecells.data();
+    s->ebase_hash = ftk2b::hash_base_cells(s->ecells.data(), (uint64_t)s->ecells.size());
     s->slice_elems = mesh->n_base_verts;
   } else {
     delete s;

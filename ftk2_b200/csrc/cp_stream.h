@@ -18,6 +18,7 @@ struct ftk2b_stream {
   // extruded: the base mesh (cells copied at open)
   ftk2b_mesh_desc emesh;
   std::vector<uint64_t> ecells;
+  uint64_t ebase_hash = 0;     // content hash of ecells (computed once)
 
   uint64_t T = 0;              // timesteps pushed
   size_t slice_elems = 0;      // elements of one timestep in one ring array
@@ -45,6 +46,10 @@ namespace ftk2b {
 
 // grow a device buffer keeping its first `used` bytes
 cudaError_t grow_keep(DevBuf& b, size_t used, size_t want, cudaStream_t st);
+// grows the feature store (and union-find / boundary lists) to hold `want`
+ftk2b_status ensure_stream_store(ftk2b_stream* s, unsigned want);
+// content hash of an extruded mesh's base cells (the prepared-mesh cache key)
+uint64_t hash_base_cells(const uint64_t* p, uint64_t n);
 
 }  // namespace ftk2b
 

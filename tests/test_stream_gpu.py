@@ -143,3 +143,64 @@ def test_stream_rejects_mismatched_step(ctx):
             st.push(api.field_desc(bad, cases.MULTI, 3, keep=keep))
         assert e.value.status == api.INVALID_ARG
         st.push(api.field_desc(steps_of(case, 0), case.layout, 3, keep=keep))
+
+
+# ---------------------------------------------------------------------------
+# extruded meshes (the serving stream of a triangulated plane extruded into tets)
+
+def ext_one_shot(ctx, case, nt):
+    keep: list = []
+    nv = case.coords.shape[0]
+    mesh = api.extruded_mesh_desc(nv, case.cells, nt - 1, keep)
+    fld = api.field_desc([np.ascontiguousarray(a[: nt * nv]) for a in case.arrays], case.layout, case.ncomp,
+                         keep=keep)
+    return ctx.extract(mesh, fld, api.params(case.sos_q))
+
+
+def ext_stream_case(ctx, case, check_every=False, device=False):
+    keep: list = []
+    nv = case.coords.shape[0]
+    nt = case.n_layers + 1
+    mesh = api.extruded_mesh_desc(nv, case.cells, case.n_layers, keep)
+    step = lambda t: [np.ascontiguousarray(a[t * nv:(t + 1) * nv]) for a in case.arrays]
+    tmpl = api.field_desc(step(0), case.layout, case.ncomp, keep=keep)
+    if device:
+        import torch
+    with api.Stream(ctx, mesh, tmpl, api.params(case.sos_q)) as st:
+        total = 0
+        for t in range(nt):
+            arrs = step(t)
+            if device:
+                arrs = [torch.from_numpy(a).cuda() for a in arrs]
+                keep.append(arrs)
+            total += st.push(api.field_desc(arrs, case.layout, case.ncomp, keep=keep))
+            if check_every or t == nt - 1:
+                r = st.result()
+                assert len(r.track_id) == total
+                assert_identical(r, ext_one_shot(ctx, case, t + 1))
+        return r
+
+
+def _ext_cases():
+    out = [cases.GOLDEN_CASES["extruded_3d_s0"](), cases.GOLDEN_CASES["extruded_2d"]()]
+    coords, tets = S.extruded_tet_mesh(24, 22, 9, seed=1)
+    vals = S.gaussian_sum_gradient_at(coords, 7, seed=201, n_blobs=24, sigma=(1.0, 3.0), drift=0.6,
+                                      dtype=np.float32)
+    out.append(cases.Case("ext3d_f32_7", "extruded", 3, cases.PER_VERTEX, [vals[0], vals[1], vals[2]],
+                          2.0 ** 20, coords=coords, cells=tets, n_layers=6))
+    return out
+
+
+@pytest.mark.parametrize("case", _ext_cases(), ids=lambda c: c.name)
+def test_extruded_stream_every_prefix(ctx, case):
+    ext_stream_case(ctx, case, check_every=True)
+
+
+def test_extruded_stream_matches_reference_fixture(ctx):
+    import os
+    case = cases.GOLDEN_CASES["extruded_3d_s4"]()
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "extruded_3d_s4.npz"))
+    r = ext_stream_case(ctx, case, device=True)
+    ref = bridge.CPResult(simplices=z["simplices"], bary=z["bary"], lam=z["lam"], track_id=z["track_id"],
+                          type=z["type"], scalar=z["scalar"], edges=z["edges"])
+    assert_identical(r, ref)
