@@ -83,6 +83,27 @@ class CPResultC(C.Structure):
     ]
 
 
+class RequestC(C.Structure):
+    _fields_ = [("kind", C.c_int), ("mesh", MeshDesc), ("field", FieldDesc), ("params", CPParams),
+                ("stream", C.c_uint64)]
+
+
+class RequestStatsC(C.Structure):
+    _fields_ = [("status", C.c_int), ("slot", C.c_int), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+                ("latency_ms", C.c_double), ("n_features", C.c_uint64), ("n_simplices", C.c_uint64)]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("rejected", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("max_ms", C.c_double), ("mean_ms", C.c_double), ("elapsed_s", C.c_double),
+                ("simplices", C.c_uint64), ("hbm_budget", C.c_uint64), ("hbm_reserved_peak", C.c_uint64),
+                ("max_in_flight", C.c_int)]
+
+
+REQ_EXTRACT, REQ_STREAM_PUSH = 0, 1
+
+
 # name -> (restype, argtypes); every symbol include/ftk2b.h declares
 SIGNATURES = {
     "ftk2b_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -108,6 +129,17 @@ SIGNATURES = {
     "ftk2b_stream_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_double)]),
     "ftk2b_stream_close": (None, [C.c_void_p]),
+    "ftk2b_server_create": (C.c_int, [C.c_int, C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_void_p)]),
+    "ftk2b_server_stream_open": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                           C.POINTER(CPParams), C.POINTER(C.c_uint64)]),
+    "ftk2b_server_submit": (C.c_int, [C.c_void_p, C.POINTER(RequestC), C.POINTER(C.c_uint64)]),
+    "ftk2b_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.POINTER(CPResultC)),
+                                    C.POINTER(RequestStatsC)]),
+    "ftk2b_server_stream_result": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_server_stream_close": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ftk2b_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStatsC)]),
+    "ftk2b_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "ftk2b_server_destroy": (None, [C.c_void_p]),
     "ftk2b_cp_features_noalloc": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(FieldDesc), C.c_double,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -382,6 +414,101 @@ class Stream:
         if getattr(self, "h", None):
             self.lib.ftk2b_stream_close(self.h)
             self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Server:
+    """Request loop over worker slots (ftk2b_server_*): extraction requests and
+    stream pushes are admitted in arrival order as workers and HBM budget
+    free up; their device work overlaps across slots.  Arrays referenced by a
+    request must stay alive until its wait() returns (pass `keep`)."""
+
+    def __init__(self, device: int = 0, n_slots: int = 4, hbm_budget: int = 0, queue_limit: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.ftk2b_server_create(int(device), int(n_slots), int(hbm_budget), int(queue_limit),
+                                          C.byref(h))
+        if st != OK:
+            raise Ftk2bError(st, "ftk2b_server_create failed")
+        self.h = h
+        self._keep: dict = {}
+
+    def _check(self, st: int):
+        if st != OK:
+            raise Ftk2bError(st, (self.lib.ftk2b_server_last_error(self.h) or b"").decode())
+
+    def open_stream(self, mesh: MeshDesc, template: FieldDesc, prm: Optional[CPParams] = None) -> int:
+        sid = C.c_uint64()
+        self._check(self.lib.ftk2b_server_stream_open(self.h, C.byref(mesh), C.byref(template),
+                                                      C.byref(prm or params()), C.byref(sid)))
+        return int(sid.value)
+
+    def _submit(self, req: RequestC, keep) -> int:
+        t = C.c_uint64()
+        self._check(self.lib.ftk2b_server_submit(self.h, C.byref(req), C.byref(t)))
+        self._keep[int(t.value)] = keep
+        return int(t.value)
+
+    def submit_extract(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None,
+                       keep=None) -> int:
+        r = RequestC()
+        r.kind = REQ_EXTRACT
+        r.mesh = mesh
+        r.field = field
+        r.params = prm or params()
+        return self._submit(r, keep)
+
+    def submit_push(self, stream_id: int, step: FieldDesc, keep=None) -> int:
+        r = RequestC()
+        r.kind = REQ_STREAM_PUSH
+        r.field = step
+        r.params = params()
+        r.stream = int(stream_id)
+        return self._submit(r, keep)
+
+    def wait(self, ticket: int, timeout: float = -1.0, want_result: bool = True):
+        """(CPResult or None, stats dict); raises on a failed request."""
+        out = C.POINTER(CPResultC)()
+        stc = RequestStatsC()
+        st = self.lib.ftk2b_server_wait(self.h, int(ticket), float(timeout),
+                                        C.byref(out) if want_result else None, C.byref(stc))
+        self._keep.pop(int(ticket), None)
+        self._check(st)
+        res = None
+        if want_result and out:
+            try:
+                res = _result_from_c(out.contents)
+            finally:
+                self.lib.ftk2b_cp_result_free(out)
+        stats = {k: getattr(stc, k) for k, _ in RequestStatsC._fields_}
+        return res, stats
+
+    def stream_result(self, stream_id: int) -> CPResult:
+        out = C.POINTER(CPResultC)()
+        self._check(self.lib.ftk2b_server_stream_result(self.h, int(stream_id), C.byref(out)))
+        try:
+            return _result_from_c(out.contents)
+        finally:
+            self.lib.ftk2b_cp_result_free(out)
+
+    def close_stream(self, stream_id: int):
+        self._check(self.lib.ftk2b_server_stream_close(self.h, int(stream_id)))
+
+    def stats(self) -> dict:
+        s = ServerStatsC()
+        self._check(self.lib.ftk2b_server_get_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStatsC._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ftk2b_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
 
     def __enter__(self):
         return self

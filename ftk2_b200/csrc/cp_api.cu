@@ -64,7 +64,8 @@ static ftk2b_status fail(ftk2b_ctx* ctx, ftk2b_status st, const char* fmt, ...) 
                   "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
-static std::once_flag g_tables_once;
+constexpr int kMaxDevices = 64;
+static std::once_flag g_tables_once[kMaxDevices];
 
 // ---------------------------------------------------------------------------
 // context
@@ -94,13 +95,17 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   ctx->num_sms = prop.multiProcessorCount;
-  std::call_once(g_tables_once, [] {
+  // constant tables live per device: upload them once for each device (a
+  // second upload while other contexts' kernels read them would be a race)
+  if (device < kMaxDevices) {
+    std::call_once(g_tables_once[device], [] {
+      upload_chain_tables();
+      upload_post_tables();
+    });
+  } else {
     upload_chain_tables();
     upload_post_tables();
-  });
-  // tables are per device: upload again for devices other than the first
-  upload_chain_tables();
-  upload_post_tables();
+  }
   if (cudaGetLastError() != cudaSuccess) {
     delete ctx;
     return FTK2B_CUDA_ERROR;

@@ -202,6 +202,62 @@ ftk2b_status ftk2b_stream_result(ftk2b_stream* s, ftk2b_cp_result** out);
 ftk2b_status ftk2b_stream_info(ftk2b_stream* s, uint64_t* timesteps, uint64_t* n_features, double* last_push_ms);
 void ftk2b_stream_close(ftk2b_stream* s);
 
+/* --- serving ----------------------------------------------------------------
+ * No counterpart in the reference (it has no request loop).  A server owns
+ * n_slots worker threads, each with its own context (device buffers and CUDA
+ * stream), so the device work of concurrent requests overlaps.  Requests are
+ * admitted in arrival order as soon as a worker is free and their estimated
+ * device memory fits the HBM budget (continuous batching: requests that
+ * arrive while others run start as slots and memory free up).  Pushes to one
+ * stream run in submission order, on the stream's own context, which keeps
+ * the stream's previous timestep and union-find state resident.
+ * Every pointer inside a request must stay valid until the request completes. */
+typedef struct ftk2b_server ftk2b_server;
+enum { FTK2B_REQ_EXTRACT = 0, FTK2B_REQ_STREAM_PUSH = 1 };
+typedef struct {
+  int kind;                 /* FTK2B_REQ_* */
+  ftk2b_mesh_desc mesh;     /* EXTRACT */
+  ftk2b_field_desc field;   /* EXTRACT: the field; STREAM_PUSH: one timestep */
+  ftk2b_cp_params params;   /* EXTRACT */
+  uint64_t stream;          /* STREAM_PUSH: id from ftk2b_server_stream_open */
+} ftk2b_request;
+typedef struct {
+  ftk2b_status status;
+  int slot;                 /* worker that ran it */
+  double queue_ms;          /* submit -> start */
+  double run_ms;            /* start -> done */
+  double latency_ms;        /* submit -> done */
+  uint64_t n_features;      /* EXTRACT: features; STREAM_PUSH: new features */
+  uint64_t n_simplices;     /* EXTRACT: m-simplices of the mesh */
+} ftk2b_request_stats;
+typedef struct {
+  uint64_t submitted, completed, failed, rejected;
+  double p50_ms, p99_ms, max_ms, mean_ms;  /* latency of completed requests */
+  double elapsed_s;                        /* first submit -> last completion */
+  uint64_t simplices;                      /* m-simplices of completed extractions */
+  uint64_t hbm_budget, hbm_reserved_peak;  /* bytes */
+  int max_in_flight;
+} ftk2b_server_stats;
+
+/* hbm_budget = 0: 90% of the device's free memory at creation.
+ * queue_limit = 0: unbounded; otherwise submit returns FTK2B_BUSY when full. */
+ftk2b_status ftk2b_server_create(int device, int n_slots, uint64_t hbm_budget, int queue_limit,
+                                 ftk2b_server** out);
+ftk2b_status ftk2b_server_stream_open(ftk2b_server* sv, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* tmpl,
+                                      const ftk2b_cp_params* params, uint64_t* stream_id);
+ftk2b_status ftk2b_server_submit(ftk2b_server* sv, const ftk2b_request* req, uint64_t* ticket);
+/* Blocks until the request is done (timeout_s < 0: no limit; FTK2B_TIMEOUT
+ * otherwise).  *out (may be null) receives an EXTRACT's result, owned by the
+ * caller (ftk2b_cp_result_free).  Returns the request's own status. */
+ftk2b_status ftk2b_server_wait(ftk2b_server* sv, uint64_t ticket, double timeout_s, ftk2b_cp_result** out,
+                               ftk2b_request_stats* stats);
+ftk2b_status ftk2b_server_stream_result(ftk2b_server* sv, uint64_t stream_id, ftk2b_cp_result** out);
+ftk2b_status ftk2b_server_stream_close(ftk2b_server* sv, uint64_t stream_id);
+ftk2b_status ftk2b_server_get_stats(ftk2b_server* sv, ftk2b_server_stats* out);
+/* text of the last failure of a server call or request */
+const char* ftk2b_server_last_error(ftk2b_server* sv);
+void ftk2b_server_destroy(ftk2b_server* sv);
+
 /* --- allocation-free extraction -------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory while they run (an in-situ step inside a simulation whose allocator

@@ -72,3 +72,15 @@ def test_extruded_simplex_count_matches_restatement():
         res = bridge.run_restatement(mesh, fld)
         desc = api.extruded_mesh_desc(case.coords.shape[0], case.cells, case.n_layers, keep)
         assert api.simplex_count(desc, case.ncomp) == res.n_tested
+
+
+def test_no_server_without_device():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(api.Ftk2bError) as e:
+        api.Server(0, n_slots=2)
+    assert e.value.status == api.NO_DEVICE
