@@ -151,6 +151,96 @@ def cpu_baseline_sample(field_np, steps_budget_s=20.0):
     return total_n / total_s, sample
 
 
+def _positions(simplices, lam, dims):
+    """Barycentric positions sum_i lambda_i p_i in grid units (x, y, z, t)."""
+    import numpy as np
+    ids = simplices.astype(np.int64)
+    coords = []
+    rest = ids
+    for n in dims:
+        coords.append(rest % n)
+        rest = rest // n
+    P = np.stack(coords, -1).astype(np.float64)  # (n, m+1, 4)
+    return (lam[:, :, None] * P).sum(1)
+
+
+def precision_c4(ctx, steps=5):
+    """Precision workload: 256^3 x 8 float32 Gaussian-sum gradient (64 blobs)
+    plus 1e-3 noise.  The refined-FP32 path (exact int64 SoS, float solve for
+    acceptance, reported positions from an FP32 solve plus one FP64 refinement
+    step) against the plain FP64 drop-in on the same field promoted to
+    float64, on the same GPU; positions compared on the simplices both accept."""
+    import numpy as np
+    import torch
+    from ftk2_b200 import api, generate
+    dims = [256, 256, 256, 8]
+    f32 = generate.c4_field()
+    torch.cuda.synchronize()
+    keep: list = []
+    mesh = api.regular_mesh_desc(dims)
+    nsimp = api.simplex_count(mesh, 3)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+    def timed(fd, prm):
+        for _ in range(3):
+            ctx.run(mesh, fd, prm)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        xs = []
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(steps):
+            ctx.run(mesh, fd, prm)
+            xs.append(ctx.last_timing()[0])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / steps, statistics.mean(xs), ctx.fetch()
+
+    fd32 = api.field_desc(f32, api.LAYOUT_MULTICOMPONENT, 3, keep=keep)
+    ms_r, x_r, res_r = timed(fd32, api.params(SOS_Q, precision=api.PRECISION_REFINED))
+    ms_e32, x_e32, res_e32 = timed(fd32, api.params(SOS_Q))
+    f64 = f32.double()
+    del keep[:]
+    del f32
+    fd64 = api.field_desc(f64, api.LAYOUT_MULTICOMPONENT, 3, keep=keep)
+    ms_64, x_64, res_64 = timed(fd64, api.params(SOS_Q))
+    del keep[:]
+    del f64
+    torch.cuda.empty_cache()
+
+    def rows(a):
+        return {tuple(r): i for i, r in enumerate(a.tolist())}
+
+    r64 = rows(res_64.simplices)
+    common = [(i, r64[tuple(r)]) for i, r in enumerate(res_r.simplices.tolist()) if tuple(r) in r64]
+    ia = np.array([c[0] for c in common], dtype=np.int64)
+    ib = np.array([c[1] for c in common], dtype=np.int64)
+    pos64 = _positions(res_64.simplices[ib], res_64.lam[ib], dims)
+    err_r = np.abs(_positions(res_r.simplices[ia], res_r.lam[ia], dims) - pos64).max(1)
+    err_e = np.abs(_positions(res_e32.simplices[ia], res_e32.lam[ia], dims) - pos64).max(1)
+    peak, _ = measured_peak()
+    alg32 = 3 * 4 * 256 ** 3 * 8
+    return {
+        "workload": "256^3 x 8 float32, 64 blobs + 1e-3 noise, Q=2^20",
+        "simplices": int(nsimp),
+        "refined_fp32": {"simplices_per_s": nsimp / (ms_r / 1e3), "ms_per_step": ms_r, "extract_ms": x_r,
+                         "features": int(len(res_r.track_id)),
+                         "hbm_frac_extract": alg32 / (x_r / 1e3) / 1e9 / peak},
+        "exact_fp32": {"simplices_per_s": nsimp / (ms_e32 / 1e3), "ms_per_step": ms_e32},
+        "plain_fp64": {"simplices_per_s": nsimp / (ms_64 / 1e3), "ms_per_step": ms_64, "extract_ms": x_64,
+                       "features": int(len(res_64.track_id))},
+        "speedup_refined_vs_fp64": ms_64 / ms_r,
+        "position_error_grid_units": {
+            "compared": int(len(ia)), "refined_max": float(err_r.max()) if len(ia) else None,
+            "refined_mean": float(err_r.mean()) if len(ia) else None,
+            "refined_frac_le_1e-9": float((err_r <= 1e-9).mean()) if len(ia) else None,
+            "fp32_unrefined_max": float(err_e.max()) if len(ia) else None,
+            "fp32_unrefined_mean": float(err_e.mean()) if len(ia) else None},
+        "sets": {"fp32_only": int(len(res_r.track_id) - len(ia)), "fp64_only": int(len(res_64.track_id) - len(ia)),
+                 "note": "acceptance follows the reference per precision: the float engine solves in float, "
+                         "the double engine in double (zero_crossing.hpp with T = float / double)"},
+    }
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -207,6 +297,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ftk2b", choices=["ftk2b", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="only the headline workload (no precision / serving measurements)")
+    ap.add_argument("--serve-seconds", type=float, default=5.0)
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -304,10 +397,19 @@ def main():
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1000.0},
             "roofline": roof, "clocks": clocks.summary(),
             "gpu_launches": int(launches1 - launches0)}
+    del pinned, host
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, sample = cpu_baseline_sample(host)
+        v, sample = cpu_baseline_sample(field.cpu().numpy())
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1,
                                 "kind": "reference", "sample": sample}
+    if not args.no_extra:
+        del field, fdev
+        keep.clear()
+        torch.cuda.empty_cache()
+        line["precision"] = precision_c4(ctx)
+        torch.cuda.empty_cache()
+        from ftk2_b200 import serving
+        line["serve"] = serving.run(duration_s=args.serve_seconds, device=local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -38,6 +38,7 @@ HOST, DEVICE = 0, 1
 PRECISION_EXACT, PRECISION_REFINED = 0, 1
 OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA, OPT_USE_GRAPHS = 1, 2, 3, 4
 INFO_LAST_TMA = 100
+OPT_BLOCKING_SYNC = 5
 CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
                "center"]
 
@@ -90,7 +91,8 @@ class RequestC(C.Structure):
 
 class RequestStatsC(C.Structure):
     _fields_ = [("status", C.c_int), ("slot", C.c_int), ("queue_ms", C.c_double), ("run_ms", C.c_double),
-                ("latency_ms", C.c_double), ("n_features", C.c_uint64), ("n_simplices", C.c_uint64)]
+                ("latency_ms", C.c_double), ("n_features", C.c_uint64), ("n_simplices", C.c_uint64),
+                ("phase_ms", C.c_double * 4)]
 
 
 class ServerStatsC(C.Structure):
@@ -120,6 +122,7 @@ SIGNATURES = {
     "ftk2b_cp_run": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                C.POINTER(CPParams), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_ctx_last_phases": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "ftk2b_ctx_last_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(C.c_uint64)]),
     "ftk2b_stream_open": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
@@ -133,6 +136,7 @@ SIGNATURES = {
     "ftk2b_server_stream_open": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                            C.POINTER(CPParams), C.POINTER(C.c_uint64)]),
     "ftk2b_server_submit": (C.c_int, [C.c_void_p, C.POINTER(RequestC), C.POINTER(C.c_uint64)]),
+    "ftk2b_server_warm": (C.c_int, [C.c_void_p, C.POINTER(RequestC)]),
     "ftk2b_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.POINTER(CPResultC)),
                                     C.POINTER(RequestStatsC)]),
     "ftk2b_server_stream_result": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.POINTER(CPResultC))]),
@@ -463,6 +467,15 @@ class Server:
         r.params = prm or params()
         return self._submit(r, keep)
 
+    def warm(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None):
+        """Runs one extraction on every slot (buffers and graphs sized for it)."""
+        r = RequestC()
+        r.kind = REQ_EXTRACT
+        r.mesh = mesh
+        r.field = field
+        r.params = prm or params()
+        self._check(self.lib.ftk2b_server_warm(self.h, C.byref(r)))
+
     def submit_push(self, stream_id: int, step: FieldDesc, keep=None) -> int:
         r = RequestC()
         r.kind = REQ_STREAM_PUSH
@@ -486,6 +499,7 @@ class Server:
             finally:
                 self.lib.ftk2b_cp_result_free(out)
         stats = {k: getattr(stc, k) for k, _ in RequestStatsC._fields_}
+        stats["phase_ms"] = list(stc.phase_ms)
         return res, stats
 
     def stream_result(self, stream_id: int) -> CPResult:

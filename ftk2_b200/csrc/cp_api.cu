@@ -24,11 +24,24 @@ namespace ftk2b {
 cudaError_t DevBuf::ensure(size_t want) {
   if (bytes >= want && p) return cudaSuccess;
   ++generation;
-  if (p) cudaFree(p);
+  // a buffer that has to grow gets half as much again, so that sizes creeping
+  // up call by call reallocate (and synchronise the device) only a few times
+  const bool regrow = p != nullptr;
+  if (p) {
+    if (st) cudaFreeAsync(p, st);
+    else cudaFree(p);
+  }
   p = nullptr;
   bytes = 0;
   size_t alloc = want < 256 ? 256 : want;
-  cudaError_t e = cudaMalloc(&p, alloc);
+  if (regrow) alloc += alloc / 2;
+  auto do_alloc = [&](size_t n) { return st ? cudaMallocAsync(&p, n, st) : cudaMalloc(&p, n); };
+  cudaError_t e = do_alloc(alloc);
+  if (e != cudaSuccess && regrow) {  // the headroom did not fit: exact size
+    cudaGetLastError();
+    alloc = want < 256 ? 256 : want;
+    e = do_alloc(alloc);
+  }
   if (e != cudaSuccess) {
     p = nullptr;
     cudaGetLastError();
@@ -39,7 +52,10 @@ cudaError_t DevBuf::ensure(size_t want) {
 }
 
 void DevBuf::release() {
-  if (p) cudaFree(p);
+  if (p) {
+    if (st) cudaFreeAsync(p, st);
+    else cudaFree(p);
+  }
   p = nullptr;
   bytes = 0;
 }
@@ -84,7 +100,8 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
   ctx->device = device;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
-      cudaEventCreate(&ctx->ev_x) != cudaSuccess || cudaEventCreate(&ctx->ev_r) != cudaSuccess) {
+      cudaEventCreate(&ctx->ev_x) != cudaSuccess || cudaEventCreate(&ctx->ev_r) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_sync, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess) {
     delete ctx;
     return FTK2B_CUDA_ERROR;
   }
@@ -92,6 +109,7 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
     delete ctx;
     return FTK2B_OOM;
   }
+  for (DevBuf* b : ctx->all_bufs()) b->st = ctx->stream;
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   ctx->num_sms = prop.multiProcessorCount;
@@ -114,6 +132,12 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
   return FTK2B_OK;
 }
 
+extern "C" ftk2b_status ftk2b_ctx_last_phases(ftk2b_ctx* ctx, double* phase_ms) {
+  if (!ctx || !phase_ms) return FTK2B_INVALID_ARG;
+  for (int i = 0; i < 4; ++i) phase_ms[i] = ctx->phase_ms[i];
+  return FTK2B_OK;
+}
+
 extern "C" ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* total_ms,
                                               uint64_t* kernels_launched) {
   if (!ctx) return FTK2B_INVALID_ARG;
@@ -128,13 +152,14 @@ extern "C" void ftk2b_ctx_destroy(ftk2b_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->release_all();
-  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
-  if (ctx->gexec2) cudaGraphExecDestroy(ctx->gexec2);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->drop_graphs();
   if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaEventDestroy(ctx->ev_x);
   cudaEventDestroy(ctx->ev_r);
+  cudaEventDestroy(ctx->ev_sync);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -170,7 +195,10 @@ extern "C" ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t
       return FTK2B_OK;
     case FTK2B_OPT_USE_GRAPHS:
       ctx->use_graphs = value != 0;
-      ctx->graph_valid = false;
+      ctx->drop_graphs();
+      return FTK2B_OK;
+    case FTK2B_OPT_BLOCKING_SYNC:
+      ctx->blocking_sync = value != 0;
       return FTK2B_OK;
     default:
       return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
@@ -185,13 +213,14 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_DISABLE_TMA: *value = ctx->disable_tma ? 1 : 0; return FTK2B_OK;
     case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
     case FTK2B_OPT_USE_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return FTK2B_OK;
+    case FTK2B_OPT_BLOCKING_SYNC: *value = ctx->blocking_sync ? 1 : 0; return FTK2B_OK;
     default: return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
 }
 
 void ftk2b_ctx::release_all() {
   // cached graphs point into these buffers
-  graph_valid = false;
+  drop_graphs();
   ext.valid = false;
   for (DevBuf* b : all_bufs()) b->release();
 }
@@ -475,6 +504,12 @@ static ftk2b_status build_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, R
 
 static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                 const ftk2b_field_desc* field, const ftk2b_cp_params* prm) {
+  using Clk = std::chrono::steady_clock;
+  auto msd = [](Clk::time_point a, Clk::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  const Clk::time_point p0 = Clk::now();
+  for (double& x : ctx->phase_ms) x = 0;
   RegularMesh rm;
   ftk2b_status st = build_regular(ctx, mesh, rm);
   if (st) return st;
@@ -556,6 +591,9 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       return cudaMemcpyAsync(ctx->h_counters, ctx->counters.p, sizeof(unsigned) * kNumCounters,
                              cudaMemcpyDeviceToHost, ctx->stream);
     };
+    const Clk::time_point p1 = Clk::now();
+    ctx->phase_ms[0] += msd(p0, p1);
+    Clk::time_point p2 = p1;
     if (ctx->use_graphs) {
       RegularGraphKey key;
       memset(&key, 0, sizeof(key));
@@ -572,10 +610,31 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       key.key_bits = key_bits;
       key.nch = nch;
       const unsigned long long gen = ctx->buffer_generation();
-      if (!(ctx->graph_valid && ctx->graph_gen == gen && memcmp(&key, &ctx->gkey, sizeof(key)) == 0)) {
-        ctx->graph_valid = false;
+      GraphEntry* ent = nullptr;
+      for (auto it = ctx->graphs.begin(); it != ctx->graphs.end();) {
+        if (it->gen != gen) {  // captured over buffers that have been reallocated since
+          if (it->g1) cudaGraphExecDestroy(it->g1);
+          if (it->g2) cudaGraphExecDestroy(it->g2);
+          it = ctx->graphs.erase(it);
+          continue;
+        }
+        if (memcmp(&it->key, &key, sizeof(key)) == 0) ent = &*it;
+        ++it;
+      }
+      if (!ent) {
+        if (ctx->graphs.size() >= kMaxGraphs) {
+          auto lru = ctx->graphs.begin();
+          for (auto it = ctx->graphs.begin(); it != ctx->graphs.end(); ++it)
+            if (it->last_use < lru->last_use) lru = it;
+          if (lru->g1) cudaGraphExecDestroy(lru->g1);
+          if (lru->g2) cudaGraphExecDestroy(lru->g2);
+          ctx->graphs.erase(lru);
+        }
+        GraphEntry e;
+        e.key = key;
+        e.gen = gen;
         unsigned long long nl = 0;
-        cudaGraphExec_t* slots[2] = {&ctx->gexec, &ctx->gexec2};
+        cudaGraphExec_t* slots[2] = {&e.g1, &e.g2};
         for (int part = 0; part < 2; ++part) {
           cudaGraph_t graph = nullptr;
           CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -583,27 +642,33 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
           cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
           if (ce || ee) {
             if (graph) cudaGraphDestroy(graph);
+            if (e.g1) cudaGraphExecDestroy(e.g1);
             cudaGetLastError();
             return fail(ctx, FTK2B_CUDA_ERROR, "graph capture failed: %s",
                         cudaGetErrorString(ce ? ce : ee));
           }
-          if (*slots[part]) cudaGraphExecDestroy(*slots[part]);
-          *slots[part] = nullptr;
           cudaError_t ie = cudaGraphInstantiate(slots[part], graph, 0);
           cudaGraphDestroy(graph);
-          if (ie) return fail(ctx, FTK2B_CUDA_ERROR, "graph instantiate failed: %s", cudaGetErrorString(ie));
+          if (ie) {
+            if (e.g1 && part == 1) cudaGraphExecDestroy(e.g1);
+            return fail(ctx, FTK2B_CUDA_ERROR, "graph instantiate failed: %s", cudaGetErrorString(ie));
+          }
         }
-        ctx->gkey = key;
-        ctx->graph_gen = gen;
-        ctx->graph_valid = true;
-        ctx->launches_per_run = nl;
+        e.launches = nl;
+        e.used_tma = ctx->last_used_tma;
+        ctx->graphs.push_back(e);
+        ent = &ctx->graphs.back();
       }
+      ent->last_use = ++ctx->graph_clock;
+      ctx->last_used_tma = ent->used_tma;
+      p2 = Clk::now();
+      ctx->phase_ms[1] += msd(p1, p2);
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-      CUDA_TRY(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
+      CUDA_TRY(ctx, cudaGraphLaunch(ent->g1, ctx->stream));
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
-      CUDA_TRY(ctx, cudaGraphLaunch(ctx->gexec2, ctx->stream));
+      CUDA_TRY(ctx, cudaGraphLaunch(ent->g2, ctx->stream));
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-      ctx->launches += ctx->launches_per_run;
+      ctx->launches += ent->launches;
     } else {
       unsigned long long nl = 0;
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
@@ -613,7 +678,8 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
       ctx->launches += nl;
     }
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, ctx->sync());
+    ctx->phase_ms[2] += msd(p2, Clk::now());
     unsigned h[kNumCounters];
     memcpy(h, ctx->h_counters, sizeof(h));
     float ms = 0.f, xms = 0.f;
@@ -676,6 +742,14 @@ extern "C" ftk2b_status ftk2b_cp_run(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh
 
 extern "C" ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out) {
   if (!ctx || !out) return FTK2B_INVALID_ARG;
+  const auto f0 = std::chrono::steady_clock::now();
+  struct PhaseTimer {
+    ftk2b_ctx* c;
+    std::chrono::steady_clock::time_point t;
+    ~PhaseTimer() {
+      c->phase_ms[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+    }
+  } phase_timer{ctx, f0};
   *out = nullptr;
   const uint64_t n = ctx->last.n, ne = ctx->last.ne;
   const int m = ctx->last.m;
@@ -715,7 +789,7 @@ extern "C" ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out) {
   if (!e && ctx->last.want_edges) e = d2h(r->track_id, ctx->track.p, sizeof(uint64_t) * n);
   if (!e && ctx->last.classify) e = d2h(r->cp_class, ctx->cls.p, sizeof(uint32_t) * n);
   if (!e) e = d2h(r->edges, ctx->edges.p, sizeof(uint32_t) * 2 * ne);
-  if (!e) e = cudaStreamSynchronize(s);
+  if (!e) e = ctx->sync();
   if (e) {
     ftk2b_cp_result_free(r);
     return fail(ctx, FTK2B_CUDA_ERROR, "result copy failed: %s", cudaGetErrorString(e));

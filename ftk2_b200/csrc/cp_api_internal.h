@@ -1,6 +1,7 @@
 // Context object and cross-file declarations of the C-ABI layer.
 #pragma once
 
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -10,11 +11,14 @@
 
 namespace ftk2b {
 
-// grow-only device allocation owned by a context
+// grow-only device allocation owned by a context.  With `st` set, memory is
+// allocated and freed in stream order on that stream (the only stream that
+// uses the buffer), so growing a buffer does not synchronise the device.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   unsigned long long generation = 0;  // bumped on every reallocation
+  cudaStream_t st = nullptr;
   cudaError_t ensure(size_t want);
   void release();
 };
@@ -48,6 +52,18 @@ struct ExtCache {
   }
 };
 
+// One cached pair of instantiated graphs of the regular-mesh pipeline.
+struct GraphEntry {
+  RegularGraphKey key;
+  unsigned long long gen = 0;      // buffer generation at capture
+  cudaGraphExec_t g1 = nullptr;    // counters reset + fused cull kernel
+  cudaGraphExec_t g2 = nullptr;    // exact tests + canonical order + trajectories
+  unsigned long long launches = 0;
+  unsigned long long last_use = 0;
+  int used_tma = 0;                // whether the captured cull kernel stages with TMA
+};
+constexpr size_t kMaxGraphs = 16;
+
 struct LastRun {
   int kind = 0, m = 0;
   uint64_t n = 0, ne = 0, n_roots = 0, n_simplices = 0;
@@ -80,13 +96,32 @@ struct ftk2b_ctx {
   ftk2b::LastRun last;
   // CUDA graph of the last regular-mesh pipeline
   bool use_graphs = true;
-  bool graph_valid = false;
-  ftk2b::RegularGraphKey gkey;
-  cudaGraphExec_t gexec = nullptr;   // counters reset + fused cull kernel
-  cudaGraphExec_t gexec2 = nullptr;  // exact tests + canonical order + trajectories
-  unsigned long long launches_per_run = 0;
+  // least-recently-used cache of the pipeline graphs of recent workloads
+  // (descriptor shapes and buffers), so that alternating requests replay
+  // instead of capturing again
+  std::vector<ftk2b::GraphEntry> graphs;
+  unsigned long long graph_clock = 0;
+  void drop_graphs() {
+    for (auto& g : graphs) {
+      if (g.g1) cudaGraphExecDestroy(g.g1);
+      if (g.g2) cudaGraphExecDestroy(g.g2);
+    }
+    graphs.clear();
+  }
   unsigned* h_counters = nullptr;  // pinned
-  unsigned long long graph_gen = 0;
+  // waits for the context's stream: spinning by default, or by blocking on an
+  // event (FTK2B_OPT_BLOCKING_SYNC), which frees the host core while waiting
+  // host time of the phases of the last call: [0] descriptors, staging and
+  // buffers, [1] CUDA-graph capture and instantiation, [2] launch to device
+  // completion, [3] result copy-back (ms)
+  double phase_ms[4] = {0, 0, 0, 0};
+  bool blocking_sync = false;
+  cudaEvent_t ev_sync = nullptr;
+  cudaError_t sync() {
+    if (!blocking_sync) return cudaStreamSynchronize(stream);
+    cudaError_t e = cudaEventRecord(ev_sync, stream);
+    return e ? e : cudaEventSynchronize(ev_sync);
+  }
   unsigned long long buffer_generation() {
     unsigned long long g = 0;
     for (ftk2b::DevBuf* b : all_bufs()) g += b->generation;

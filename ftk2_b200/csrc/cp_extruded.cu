@@ -718,7 +718,7 @@ ftk2b_status prepare_base(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, int fbits
     EXT_TRY(cudaGetLastError());
     EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters,
                             cudaMemcpyDeviceToHost, st));
-    EXT_TRY(cudaStreamSynchronize(st));
+    EXT_TRY(ctx->sync());
     if (ctx->h_counters[kCountErr] & kErrBadVertex)
       return ext_fail(ctx, FTK2B_INVALID_ARG, "a base cell lists a vertex id >= n_base_verts");
     nface = ctx->h_counters[kCountFaces];
@@ -989,7 +989,7 @@ ftk2b_status push_extruded_t(ftk2b_stream* s) {
     sink.cap = s->cap - s->n;
     EXT_TRY((enqueue_extract<T, M>(ctx, X, fa, cfg, sink, kStreamVb, nv, &nl)));
     EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
-    EXT_TRY(cudaStreamSynchronize(st));
+    EXT_TRY(ctx->sync());
     const unsigned got = ctx->h_counters[kCountFeatures];
     if (got > s->cap - s->n) {
       rc = ensure_stream_store(s, s->n + got + got / 4 + 1024);
@@ -1017,7 +1017,7 @@ ftk2b_status push_extruded_t(ftk2b_stream* s) {
   EXT_TRY(ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)ctx->sort_grid(wcap > wecap ? wcap : wecap)));
   const unsigned edge_room = s->n_edges + wecap;
   if (edge_room > s->edge_cap) {
-    unsigned nc = s->edge_cap ? s->edge_cap : 65536u;
+    unsigned nc = s->edge_cap ? s->edge_cap : 262144u;
     while (nc < edge_room) nc *= 2;
     EXT_TRY(grow_keep(s->edges, 8 * (size_t)s->n_edges, 8 * (size_t)nc, st));
     s->edge_cap = nc;
@@ -1058,7 +1058,7 @@ ftk2b_status push_extruded_t(ftk2b_stream* s) {
   nl += 9;
   EXT_TRY(cudaGetLastError());
   EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
-  EXT_TRY(cudaStreamSynchronize(st));
+  EXT_TRY(ctx->sync());
   ctx->launches += nl;
   const unsigned* h = ctx->h_counters;
   if (h[kCountErr] & kErrCofaces) return ext_fail(ctx, FTK2B_UNSUPPORTED, "a base face has more than 8 coface cells");
@@ -1128,16 +1128,17 @@ ftk2b_status result_extruded_t(ftk2b_stream* s, ftk2b_cp_result** out) {
   nl += 8;
   EXT_TRY(cudaGetLastError());
   EXT_TRY(cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
-  EXT_TRY(cudaStreamSynchronize(st));
+  EXT_TRY(ctx->sync());
   ctx->launches += nl;
   ctx->last.kind = FTK2B_MESH_EXTRUDED;
   ctx->last.m = M;
   ctx->last.n = n;
   ctx->last.ne = s->prm.want_edges ? ne : 0;
   ctx->last.n_roots = ctx->h_counters[kCountRoots];
-  ftk2b_mesh_desc md = s->emesh;
-  md.n_layers = s->T ? s->T - 1 : 0;
-  ctx->last.n_simplices = s->T ? extruded_simplex_count(&md, M) : 0;
+  // m-simplices of the T-timestep mesh, from the prepared base mesh's counts
+  const uint64_t L = s->T ? s->T - 1 : 0;
+  ctx->last.n_simplices =
+      s->T ? ctx->ext.ncell * (L + 1) + (uint64_t)ctx->ext.nface * L * M + ctx->ext.ncell * L * M : 0;
   ctx->last.device_ms = 0;
   ctx->last.classify = 0;
   ctx->last.want_edges = s->prm.want_edges;
@@ -1167,22 +1168,26 @@ ftk2b_status stream_result_extruded(ftk2b_stream* s, ftk2b_cp_result** out) {
 uint64_t extruded_simplex_count(const ftk2b_mesh_desc* mesh, int m) {
   const int cd = mesh->base_cell_dim;
   if ((cd != 2 && cd != 3) || m != cd || (mesh->n_base_cells && !mesh->base_cells)) return 0;
-  // unique (cd-1)-faces of the base, counted on the host
-  std::vector<std::vector<uint64_t>> faces;
-  faces.reserve(mesh->n_base_cells * (cd + 1));
+  // unique (cd-1)-faces of the base, counted on the host from packed keys
+  // (base vertex ids below 2^21 for tets, 2^32 for triangles; wider ids are
+  // not supported by the extruded path either)
+  const int fbits = bits_of(mesh->n_base_verts ? mesh->n_base_verts - 1 : 0);
+  if (fbits * cd > 64) return 0;
+  std::vector<uint64_t> keys;
+  keys.reserve(mesh->n_base_cells * (cd + 1));
   for (uint64_t c = 0; c < mesh->n_base_cells; ++c) {
     uint64_t v[4];
     for (int i = 0; i <= cd; ++i) v[i] = mesh->base_cells[c * (cd + 1) + i];
     std::sort(v, v + cd + 1);
     for (int r = 0; r <= cd; ++r) {
-      std::vector<uint64_t> f;
+      uint64_t k = 0;
       for (int i = 0; i <= cd; ++i)
-        if (i != r) f.push_back(v[i]);
-      faces.push_back(f);
+        if (i != r) k = (k << fbits) | v[i];
+      keys.push_back(k);
     }
   }
-  std::sort(faces.begin(), faces.end());
-  const uint64_t nface = (uint64_t)(std::unique(faces.begin(), faces.end()) - faces.begin());
+  std::sort(keys.begin(), keys.end());
+  const uint64_t nface = (uint64_t)(std::unique(keys.begin(), keys.end()) - keys.begin());
   const uint64_t L = mesh->n_layers;
   return mesh->n_base_cells * (L + 1) + nface * L * cd + mesh->n_base_cells * L * cd;
 }
@@ -1285,7 +1290,7 @@ ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk
     EXT_TRY(cudaMemcpyAsync(ctx->h_counters, ctx->counters.p, sizeof(unsigned) * kNumCounters,
                             cudaMemcpyDeviceToHost, s));
     EXT_TRY(cudaEventRecord(ctx->ev1, s));
-    EXT_TRY(cudaStreamSynchronize(s));
+    EXT_TRY(ctx->sync());
     ctx->launches += nl;
     nl = 0;
     unsigned h[kNumCounters];

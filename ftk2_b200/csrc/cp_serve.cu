@@ -42,6 +42,8 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 struct Req {
   uint64_t ticket = 0;
+  int pin = -1;       // worker that must run it (-1: any)
+  bool warm = false;  // warm-up request: kept out of the statistics
   ftk2b_request r;
   uint64_t est = 0;
   Clock::time_point t_submit, t_start, t_end;
@@ -50,6 +52,7 @@ struct Req {
   int slot = -1;
   ftk2b_cp_result* res = nullptr;
   uint64_t n_features = 0, n_simplices = 0;
+  double phase_ms[4] = {0, 0, 0, 0};
   std::string err;
 };
 
@@ -75,6 +78,7 @@ struct ftk2b_server {
   int device = 0;
   int n_slots = 0;
   uint64_t budget = 0, reserved = 0, reserved_peak = 0;
+  uint64_t reserved_pool = 0;  // bytes mapped into the allocation pool at creation
   int queue_limit = 0;
   int in_flight = 0, max_in_flight = 0;
   std::vector<ftk2b_ctx*> slot_ctx;
@@ -96,12 +100,14 @@ struct ftk2b_server {
 
 namespace {
 
-// First request of the queue that may start now (called with the lock held).
-Req* pick_locked(ftk2b_server* sv) {
+// First request of the queue that worker `slot` may start now (called with
+// the lock held).
+Req* pick_locked(ftk2b_server* sv, int slot) {
   std::set<uint64_t> blocked_streams;
   const Clock::time_point now = Clock::now();
   for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it) {
     Req* q = *it;
+    if (q->pin >= 0 && q->pin != slot) continue;
     if (q->r.kind == FTK2B_REQ_STREAM_PUSH) {
       auto s = sv->streams.find(q->r.stream);
       if (s == sv->streams.end()) {  // closed under it: fail it right away
@@ -129,6 +135,7 @@ void run_request(ftk2b_server* sv, Req* q, int slot) {
     ftk2b_ctx* ctx = sv->slot_ctx[slot];
     ftk2b_cp_result* res = nullptr;
     q->status = ftk2b_cp_extract(ctx, &q->r.mesh, &q->r.field, &q->r.params, &res);
+    ftk2b_ctx_last_phases(ctx, q->phase_ms);
     if (q->status == FTK2B_OK) {
       q->res = res;
       q->n_features = res->n_features;
@@ -165,7 +172,7 @@ void worker_main(ftk2b_server* sv, int slot) {
     Req* q = nullptr;
     {
       std::unique_lock<std::mutex> lk(sv->mu);
-      sv->cv_work.wait(lk, [&] { return sv->stop || (q = pick_locked(sv)) != nullptr; });
+      sv->cv_work.wait(lk, [&] { return sv->stop || (q = pick_locked(sv, slot)) != nullptr; });
       if (!q) return;
       q->started = true;
       q->slot = slot;
@@ -193,19 +200,36 @@ void worker_main(ftk2b_server* sv, int slot) {
         auto it = sv->streams.find(q->r.stream);
         if (it != sv->streams.end()) it->second.busy = false;
       }
-      if (q->status == FTK2B_OK) {
+      if (q->warm) {
+        // warm-up requests stay out of the statistics
+      } else if (q->status == FTK2B_OK) {
         sv->completed += 1;
         sv->latencies.push_back(ms_between(q->t_submit, q->t_end));
         sv->simplices += q->n_simplices;
+        sv->last_done = q->t_end;
       } else {
         sv->failed += 1;
         sv->err = q->err;
+        sv->last_done = q->t_end;
       }
-      sv->last_done = q->t_end;
     }
     sv->cv_done.notify_all();
     sv->cv_work.notify_all();
   }
+}
+
+uint64_t estimate_bytes(const ftk2b_request* req) {
+  uint64_t est;
+  if (req->kind == FTK2B_REQ_EXTRACT) {
+    est = kExtractOverhead + (req->field.location == FTK2B_HOST ? field_bytes(req->field) : 0);
+    if (req->mesh.kind == FTK2B_MESH_EXTRUDED) {
+      const uint64_t nv = req->mesh.n_base_verts * (req->mesh.n_layers + 1);
+      est += 4 * nv + 48 * req->mesh.n_base_cells * (uint64_t)(req->mesh.base_cell_dim + 1);
+    }
+  } else {
+    est = kPushOverhead + (req->field.location == FTK2B_HOST ? field_bytes(req->field) : 0);
+  }
+  return est;
 }
 
 ftk2b_status sv_fail(ftk2b_server* sv, ftk2b_status st, const std::string& msg) {
@@ -232,6 +256,7 @@ extern "C" ftk2b_status ftk2b_server_create(int device, int n_slots, uint64_t hb
       delete sv;
       return st;
     }
+    ftk2b_ctx_set_option(c, FTK2B_OPT_BLOCKING_SYNC, 1);
     sv->slot_ctx.push_back(c);
   }
   if (hbm_budget == 0) {
@@ -244,6 +269,26 @@ extern "C" ftk2b_status ftk2b_server_create(int device, int n_slots, uint64_t hb
     hbm_budget = (uint64_t)(0.9 * (double)fr);
   }
   sv->budget = hbm_budget;
+  // Growing a buffer maps new device memory into the stream-ordered pool,
+  // which holds up the work of every slot while it happens.  Keep freed pool
+  // memory mapped and map a reserve up front: min(budget / 2, n_slots GiB).
+  {
+    cudaSetDevice(device);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      const uint64_t reserve = std::min<uint64_t>(sv->budget / 2, (uint64_t)n_slots << 30);
+      void* p = nullptr;
+      cudaStream_t st = (cudaStream_t)ftk2b_ctx_stream(sv->slot_ctx[0]);
+      if (reserve && cudaMallocAsync(&p, reserve, st) == cudaSuccess) {
+        cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+      }
+      sv->reserved_pool = reserve;
+    }
+    cudaGetLastError();
+  }
   for (int i = 0; i < n_slots; ++i) sv->workers.emplace_back(worker_main, sv, i);
   *out = sv;
   return FTK2B_OK;
@@ -256,6 +301,7 @@ extern "C" ftk2b_status ftk2b_server_stream_open(ftk2b_server* sv, const ftk2b_m
   ftk2b_ctx* ctx = nullptr;
   ftk2b_status st = ftk2b_ctx_create(sv->device, &ctx);
   if (st != FTK2B_OK) return sv_fail(sv, st, "context creation failed");
+  ftk2b_ctx_set_option(ctx, FTK2B_OPT_BLOCKING_SYNC, 1);
   ftk2b_stream* s = nullptr;
   st = ftk2b_stream_open(ctx, mesh, tmpl, params, &s);
   if (st != FTK2B_OK) {
@@ -279,15 +325,7 @@ extern "C" ftk2b_status ftk2b_server_submit(ftk2b_server* sv, const ftk2b_reques
     return sv_fail(sv, FTK2B_INVALID_ARG, "unknown request kind");
   Req* q = new Req();
   q->r = *req;
-  if (req->kind == FTK2B_REQ_EXTRACT) {
-    q->est = kExtractOverhead + (req->field.location == FTK2B_HOST ? field_bytes(req->field) : 0);
-    if (req->mesh.kind == FTK2B_MESH_EXTRUDED) {
-      const uint64_t nv = req->mesh.n_base_verts * (req->mesh.n_layers + 1);
-      q->est += 4 * nv + 48 * req->mesh.n_base_cells * (uint64_t)(req->mesh.base_cell_dim + 1);
-    }
-  } else {
-    q->est = kPushOverhead + (req->field.location == FTK2B_HOST ? field_bytes(req->field) : 0);
-  }
+  q->est = estimate_bytes(req);
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     if (req->kind == FTK2B_REQ_STREAM_PUSH) {
@@ -321,6 +359,39 @@ extern "C" ftk2b_status ftk2b_server_submit(ftk2b_server* sv, const ftk2b_reques
   return FTK2B_OK;
 }
 
+extern "C" ftk2b_status ftk2b_server_warm(ftk2b_server* sv, const ftk2b_request* req) {
+  if (!sv || !req) return FTK2B_INVALID_ARG;
+  if (req->kind != FTK2B_REQ_EXTRACT) return sv_fail(sv, FTK2B_INVALID_ARG, "only extraction requests warm slots");
+  std::vector<Req*> mine;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (int w = 0; w < sv->n_slots; ++w) {
+      Req* q = new Req();
+      q->r = *req;
+      q->est = estimate_bytes(req);
+      q->pin = w;
+      q->warm = true;
+      q->ticket = sv->next_ticket++;
+      q->t_submit = Clock::now();
+      sv->queue.push_back(q);
+      mine.push_back(q);
+    }
+  }
+  sv->cv_work.notify_all();
+  ftk2b_status worst = FTK2B_OK;
+  std::unique_lock<std::mutex> lk(sv->mu);
+  for (Req* q : mine) {
+    sv->cv_done.wait(lk, [&] { return q->done; });
+    if (q->status != FTK2B_OK) {
+      worst = q->status;
+      sv->err = q->err;
+    }
+    if (q->res) ftk2b_cp_result_free(q->res);
+    delete q;
+  }
+  return worst;
+}
+
 extern "C" ftk2b_status ftk2b_server_wait(ftk2b_server* sv, uint64_t ticket, double timeout_s,
                                           ftk2b_cp_result** out, ftk2b_request_stats* stats) {
   if (!sv) return FTK2B_INVALID_ARG;
@@ -347,6 +418,7 @@ extern "C" ftk2b_status ftk2b_server_wait(ftk2b_server* sv, uint64_t ticket, dou
     stats->latency_ms = ms_between(q->t_submit, q->t_end);
     stats->n_features = q->n_features;
     stats->n_simplices = q->n_simplices;
+    for (int i = 0; i < 4; ++i) stats->phase_ms[i] = q->phase_ms[i];
   }
   const ftk2b_status st = q->status;
   if (st != FTK2B_OK) sv->err = q->err;

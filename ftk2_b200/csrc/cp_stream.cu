@@ -213,7 +213,7 @@ ftk2b_status push_regular(ftk2b_stream* s) {
     ctx->launches += 2;
     S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost,
                                st));
-    S_TRY(ctx, cudaStreamSynchronize(st));
+    S_TRY(ctx, ctx->sync());
     const unsigned* h = ctx->h_counters;
     if (h[kCountErr] & 2u) return sfail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountCand] > ccap) {
@@ -245,7 +245,7 @@ ftk2b_status push_regular(ftk2b_stream* s) {
   S_TRY(ctx, ctx->hist.ensure(sizeof(unsigned) * 256 * (size_t)sgrid));
   const unsigned edge_room = s->n_edges + 8 * nS;
   if (edge_room > s->edge_cap) {
-    unsigned nc = s->edge_cap ? s->edge_cap : 65536u;
+    unsigned nc = s->edge_cap ? s->edge_cap : 262144u;
     while (nc < edge_room) nc *= 2;
     S_TRY(ctx, grow_keep(s->edges, 8 * (size_t)s->n_edges, 8 * (size_t)nc, st));
     s->edge_cap = nc;
@@ -298,7 +298,7 @@ ftk2b_status push_regular(ftk2b_stream* s) {
     if (T == 1) S_TRY(ctx, classify(0, s->n_first, counters + kCountRoots));
   }
   S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
-  S_TRY(ctx, cudaStreamSynchronize(st));
+  S_TRY(ctx, ctx->sync());
   const unsigned* h = ctx->h_counters;
   if (h[kCountErr] & 1u) return sfail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
   s->n_edges += h[kSWinEdges];
@@ -370,7 +370,7 @@ ftk2b_status result_regular(ftk2b_stream* s, ftk2b_cp_result** out) {
                                          (unsigned*)ctx->edges.p);
   ctx->launches += 7;
   S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost, st));
-  S_TRY(ctx, cudaStreamSynchronize(st));
+  S_TRY(ctx, ctx->sync());
   // hand the canonical buffers to the context's fetch
   ctx->last.kind = FTK2B_MESH_REGULAR;
   ctx->last.m = M;
@@ -396,23 +396,26 @@ namespace ftk2b {
 
 cudaError_t grow_keep(DevBuf& b, size_t used, size_t want, cudaStream_t st) {
   if (b.p && b.bytes >= want) return cudaSuccess;
+  // stream-ordered: allocate, copy and free the old block after the work
+  // already queued on the stream, without synchronising the device
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, want < 256 ? 256 : want);
+  const size_t n = want < 256 ? 256 : want;
+  cudaError_t e = cudaMallocAsync(&p, n, st);
   if (e) {
     cudaGetLastError();
     return e;
   }
   if (b.p && used) {
     e = cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, st);
-    if (!e) e = cudaStreamSynchronize(st);
     if (e) {
-      cudaFree(p);
+      cudaFreeAsync(p, st);
       return e;
     }
   }
-  if (b.p) cudaFree(b.p);
+  if (b.p) cudaFreeAsync(b.p, st);
   b.p = p;
-  b.bytes = want < 256 ? 256 : want;
+  b.bytes = n;
+  b.st = st;
   ++b.generation;
   return cudaSuccess;
 }
@@ -420,7 +423,7 @@ cudaError_t grow_keep(DevBuf& b, size_t used, size_t want, cudaStream_t st) {
 ftk2b_status ensure_stream_store(ftk2b_stream* s, unsigned want) {
   ftk2b_ctx* ctx = s->ctx;
   if (want <= s->cap) return FTK2B_OK;
-  unsigned nc = s->cap ? s->cap : 65536u;
+  unsigned nc = s->cap ? s->cap : 262144u;
   while (nc < want) nc = nc * 2u > nc ? nc * 2u : 0xFFFFFFF0u;
   cudaStream_t st = ctx->stream;
   const size_t n = s->n;
@@ -525,6 +528,11 @@ extern "C" ftk2b_status ftk2b_stream_open(ftk2b_ctx* ctx, const ftk2b_mesh_desc*
     delete s;
     return sfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
   }
+  for (DevBuf* b : {&s->ring[0], &s->ring[1], &s->ring[2], &s->key, &s->hi, &s->lo, &s->phase, &s->lam,
+                    &s->bary4, &s->scalar, &s->cls, &s->parent, &s->edges, &s->prev_ids, &s->prev_ids2, &s->s_key,
+                    &s->s_key2, &s->s_id, &s->s_id2, &s->s_hi, &s->s_lo, &s->s_phase, &s->wedges, &s->tmp_simp,
+                    &s->dummy})
+    b->st = ctx->stream;
   const int narr = s->layout == FTK2B_LAYOUT_MULTICOMPONENT ? 1 : s->m;
   for (int j = 0; j < narr; ++j)
     if (s->ring[j].ensure(2 * s->slice_elems * s->es) != cudaSuccess) {
@@ -566,7 +574,7 @@ extern "C" ftk2b_status ftk2b_stream_push(ftk2b_stream* s, const ftk2b_field_des
   ftk2b_status rc = s->kind == FTK2B_MESH_REGULAR ? push_regular(s) : stream_push_extruded(s);
   if (rc) return rc;
   S_TRY(ctx, cudaEventRecord(ctx->ev1, st));
-  S_TRY(ctx, cudaEventSynchronize(ctx->ev1));
+  S_TRY(ctx, ctx->sync());
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) ms = 0.f;
   cudaGetLastError();

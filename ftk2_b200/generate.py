@@ -67,3 +67,27 @@ def c4_field(device: str = "cuda"):
     import torch
     return gaussian_field_device((256, 256, 256), 8, seed=4321, n_blobs=64, dtype=torch.float32,
                                  noise=1e-3, sigma=(16.0, 48.0), scale=256.0, device=device)
+
+
+def gaussian_at_device(points, nt: int, seed: int = 1234, n_blobs: int = 32, dtype=None, box=None,
+                       sigma=(4.0, 12.0), drift: float = 0.5, t0: int = 0, device: str = "cuda"):
+    """The drifting Gaussian-sum gradient at arbitrary points (nv, ndim), on the
+    device: one per-vertex array per component of length nt * nv (vertex id =
+    spatial id + t * nv), as ftk2_b200.synthetic.gaussian_sum_gradient_at
+    defines it; ``t0`` shifts the time of the first step."""
+    import torch
+    dtype = dtype or torch.float64
+    P = torch.as_tensor(np.asarray(points, dtype=np.float64), device=device)
+    nv, ndim = P.shape
+    if box is None:
+        box = (P.max(dim=0).values + 1.0).cpu().numpy()
+    blobs = gaussian_blobs(seed, n_blobs, box, sigma, drift)
+    out = torch.zeros((ndim, nt, nv), dtype=torch.float64, device=device)
+    for k in range(nt):
+        for b in range(n_blobs):
+            c = torch.as_tensor(blobs["centers"][b] + blobs["vel"][b] * (k + t0), device=device)
+            s2 = float(blobs["sigma"][b]) ** 2
+            d = P - c
+            e = float(blobs["amps"][b]) * torch.exp(-(d * d).sum(1) / (2.0 * s2))
+            out[:, k, :] -= (e[:, None] * d / s2).T
+    return out.reshape(ndim, nt * nv).to(dtype)

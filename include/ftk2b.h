@@ -143,7 +143,8 @@ enum {
   FTK2B_OPT_FEATURE_CAPACITY = 1, /* initial feature capacity; grows on overflow */
   FTK2B_OPT_TIME_CHUNK = 2,       /* time steps per extraction block (0 = all) */
   FTK2B_OPT_DISABLE_TMA = 3,      /* 1: stage slices with plain loads instead of TMA */
-  FTK2B_OPT_USE_GRAPHS = 4        /* 1 (default): replay the device pipeline as a CUDA graph */
+  FTK2B_OPT_USE_GRAPHS = 4,       /* 1 (default): replay the device pipeline as a CUDA graph */
+  FTK2B_OPT_BLOCKING_SYNC = 5     /* 1: wait for the device by blocking, not spinning (servers set it) */
 };
 ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
 /* Reads an option back, or FTK2B_INFO_LAST_TMA: 1 when the last regular-mesh
@@ -175,6 +176,11 @@ ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out);
  * number of kernels the context has launched so far. */
 ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* total_ms,
                                    uint64_t* kernels_launched);
+/* Host time (ms) of the phases of the last regular-mesh extraction on the
+ * context: [0] descriptors, staging copies and buffers, [1] CUDA-graph
+ * capture and instantiation, [2] launch to device completion, [3] result
+ * copy-back (ftk2b_cp_fetch). */
+ftk2b_status ftk2b_ctx_last_phases(ftk2b_ctx* ctx, double* phase_ms);
 
 /* --- time streams ----------------------------------------------------------
  * Replaces the reference's streaming drivers (SimplicialEngine::execute_stream
@@ -229,6 +235,7 @@ typedef struct {
   double latency_ms;        /* submit -> done */
   uint64_t n_features;      /* EXTRACT: features; STREAM_PUSH: new features */
   uint64_t n_simplices;     /* EXTRACT: m-simplices of the mesh */
+  double phase_ms[4];       /* EXTRACT on a regular mesh: ftk2b_ctx_last_phases */
 } ftk2b_request_stats;
 typedef struct {
   uint64_t submitted, completed, failed, rejected;
@@ -240,12 +247,21 @@ typedef struct {
 } ftk2b_server_stats;
 
 /* hbm_budget = 0: 90% of the device's free memory at creation.
- * queue_limit = 0: unbounded; otherwise submit returns FTK2B_BUSY when full. */
+ * queue_limit = 0: unbounded; otherwise submit returns FTK2B_BUSY when full.
+ * The server's contexts allocate in stream order from the device's default
+ * memory pool; creation sets that pool to keep freed memory mapped and maps
+ * min(hbm_budget / 2, n_slots GiB) up front, so that buffers growing during
+ * serving do not map new memory (which would hold up every slot). */
 ftk2b_status ftk2b_server_create(int device, int n_slots, uint64_t hbm_budget, int queue_limit,
                                  ftk2b_server** out);
 ftk2b_status ftk2b_server_stream_open(ftk2b_server* sv, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* tmpl,
                                       const ftk2b_cp_params* params, uint64_t* stream_id);
 ftk2b_status ftk2b_server_submit(ftk2b_server* sv, const ftk2b_request* req, uint64_t* ticket);
+/* Runs an extraction request once on every worker slot and waits: the slots'
+ * buffers and cached pipeline graphs then fit requests of that shape, so
+ * serving traffic does not pay for first-time set-up.  Not counted in the
+ * statistics. */
+ftk2b_status ftk2b_server_warm(ftk2b_server* sv, const ftk2b_request* req);
 /* Blocks until the request is done (timeout_s < 0: no limit; FTK2B_TIMEOUT
  * otherwise).  *out (may be null) receives an EXTRACT's result, owned by the
  * caller (ftk2b_cp_result_free).  Returns the request's own status. */

@@ -252,3 +252,13 @@ def test_refined_precision_same_set_smaller_error(ctx):
     err_ref = np.abs(a - b).max()
     err_f32 = np.abs(c - b).max()
     assert err_ref <= 1e-9 or err_ref < 1e-3 * err_f32, (err_ref, err_f32)
+
+
+def test_graph_cache_alternating_workloads(ctx):
+    # several workloads in turn on one context: each replays its own cached
+    # graphs and still gives its own exact result
+    cs = _medium_cases()[:3]
+    first = [gpu_run(ctx, c) for c in cs]
+    for _ in range(2):
+        for c, f in zip(cs, first):
+            assert_identical(gpu_run(ctx, c), f)

@@ -124,3 +124,17 @@ def test_queue_limit_rejects_with_busy():
             sv.wait(tk, timeout=120.0, want_result=False)
         st = sv.stats()
     assert busy >= 1 and st["rejected"] == busy and st["completed"] == len(tickets)
+
+
+def test_warm_runs_on_every_slot_and_stays_out_of_stats(ctx):
+    case = mixed_requests(seed=2)[1]
+    with api.Server(0, n_slots=3) as sv:
+        k: list = []
+        mesh, fld = cases.gpu_inputs(case, k)
+        sv.warm(mesh, fld, api.params(case.sos_q))
+        st = sv.stats()
+        assert st["completed"] == 0 and st["submitted"] == 0
+        t = sv.submit_extract(mesh, fld, api.params(case.sos_q), keep=k)
+        res, s = sv.wait(t)
+        assert s["phase_ms"][1] < 50.0  # replayed a cached graph, no capture of note
+    assert identical(res, alone(ctx, case))
