@@ -193,7 +193,10 @@ def precision_c4(ctx, steps=5):
             xs.append(ctx.last_timing()[0])
         ev1.record(stream)
         torch.cuda.synchronize()
+        modes.append(ctx.get_option(api.INFO_LAST_CULL_MODE))
         return ev0.elapsed_time(ev1) / steps, statistics.mean(xs), ctx.fetch()
+
+    modes: list = []  # cull mode the autotuner chose per timed form
 
     fd32 = api.field_desc(f32, api.LAYOUT_MULTICOMPONENT, 3, keep=keep)
     ms_r, x_r, res_r = timed(fd32, api.params(SOS_Q, precision=api.PRECISION_REFINED))
@@ -223,11 +226,11 @@ def precision_c4(ctx, steps=5):
         "workload": "256^3 x 8 float32, 64 blobs + 1e-3 noise, Q=2^20",
         "simplices": int(nsimp),
         "refined_fp32": {"simplices_per_s": nsimp / (ms_r / 1e3), "ms_per_step": ms_r, "extract_ms": x_r,
-                         "features": int(len(res_r.track_id)),
+                         "features": int(len(res_r.track_id)), "cull_mode": modes[0],
                          "hbm_frac_extract": alg32 / (x_r / 1e3) / 1e9 / peak},
         "exact_fp32": {"simplices_per_s": nsimp / (ms_e32 / 1e3), "ms_per_step": ms_e32},
         "plain_fp64": {"simplices_per_s": nsimp / (ms_64 / 1e3), "ms_per_step": ms_64, "extract_ms": x_64,
-                       "features": int(len(res_64.track_id))},
+                       "features": int(len(res_64.track_id)), "cull_mode": modes[2]},
         "speedup_refined_vs_fp64": ms_64 / ms_r,
         "position_error_grid_units": {
             "compared": int(len(ia)), "refined_max": float(err_r.max()) if len(ia) else None,
@@ -346,6 +349,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     _, _, launches1 = ctx.last_timing()
+    cull_mode = ctx.get_option(api.INFO_LAST_CULL_MODE)
     ms_total = ev0.elapsed_time(ev1)
     if pg:
         t = torch.tensor([ms_total], device="cuda")
@@ -385,7 +389,10 @@ def main():
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic_per_launch(),
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-            else "fallback 6650 GB/s", "kernel": "extract_regular_kernel<double,4>",
+            else "fallback 6650 GB/s",
+            "kernel": "extract_regular_kernel<double,4>" if cull_mode == 0
+            else "plane_stats_stream_kernel + tile_runs_kernel + run_cull_kernel <double,4>",
+            "cull_mode": cull_mode,
             "kernel_ms": xms, "algorithmic_bytes": alg_bytes}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -38,7 +38,9 @@ HOST, DEVICE = 0, 1
 PRECISION_EXACT, PRECISION_REFINED = 0, 1
 OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA, OPT_USE_GRAPHS = 1, 2, 3, 4
 INFO_LAST_TMA = 100
+INFO_LAST_CULL_MODE = 101
 OPT_BLOCKING_SYNC = 5
+OPT_CULL_MODE = 6
 CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
                "center"]
 

@@ -200,6 +200,10 @@ extern "C" ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_BLOCKING_SYNC:
       ctx->blocking_sync = value != 0;
       return FTK2B_OK;
+    case FTK2B_OPT_CULL_MODE:
+      if (value < 0 || value > 2) return fail(ctx, FTK2B_INVALID_ARG, "cull mode is 0, 1 or 2");
+      ctx->cull_mode = (int)value;
+      return FTK2B_OK;
     default:
       return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
@@ -212,8 +216,10 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_TIME_CHUNK: *value = ctx->tune_tchunk; return FTK2B_OK;
     case FTK2B_OPT_DISABLE_TMA: *value = ctx->disable_tma ? 1 : 0; return FTK2B_OK;
     case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
+    case FTK2B_INFO_LAST_CULL_MODE: *value = ctx->last_cull_mode; return FTK2B_OK;
     case FTK2B_OPT_USE_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return FTK2B_OK;
     case FTK2B_OPT_BLOCKING_SYNC: *value = ctx->blocking_sync ? 1 : 0; return FTK2B_OK;
+    case FTK2B_OPT_CULL_MODE: *value = ctx->cull_mode; return FTK2B_OK;
     default: return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
 }
@@ -229,7 +235,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   std::vector<DevBuf*> v = {&stage[0], &stage[1], &stage[2], &stage_scalar, &key, &lam, &bary4,
                             &scalar, &key_alt, &perm0, &perm1, &hist, &lam_s, &bary4_s, &scalar_s,
                             &simplices, &bary, &track, &edge_cnt, &edges, &parent, &counters,
-                            &cls, &cand_corner, &cand_chains, &edge_slots};
+                            &cls, &cand_corner, &cand_chains, &edge_slots, &tstats, &runs};
   for (auto& b : extra) v.push_back(&b);
   for (DevBuf* b : ext.bufs()) v.push_back(b);
   return v;
@@ -502,6 +508,75 @@ static ftk2b_status build_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, R
   return FTK2B_OK;
 }
 
+namespace ftk2b {
+
+cudaError_t setup_cull_scratch(ftk2b_ctx* ctx, const RegularMesh& rm, ExtractConfig& cfg) {
+  size_t sb = 0;
+  unsigned rc = 0;
+  tile_scratch_size(rm, &sb, &rc);
+  cudaError_t e = ctx->tstats.ensure(sb);
+  if (!e) e = ctx->runs.ensure(16 * (size_t)rc + 16);
+  if (e) return e;
+  cfg.tstats = (int*)ctx->tstats.p;
+  cfg.runs = (unsigned*)ctx->runs.p + 4;
+  cfg.n_runs = (unsigned*)ctx->runs.p;
+  cfg.runs_cap = rc;
+  return cudaSuccess;
+}
+
+cudaError_t resolve_cull_mode(ftk2b_ctx* ctx, const RegularMesh& rm, const FieldAccess& fa, int f64, bool multi,
+                              const std::function<cudaError_t(int)>& enqueue, int* mode) {
+  if (ctx->cull_mode != 2) {
+    *mode = ctx->cull_mode;
+    return cudaSuccess;
+  }
+  CullTune k;
+  memset(&k, 0, sizeof(k));
+  for (int i = 0; i < rm.d; ++i) {
+    k.ld[i] = rm.ld[i];
+    k.off[i] = rm.off[i];
+    k.adims[i] = fa.adims[i];
+    k.estride[i] = fa.estride[i];
+    k.shift[i] = fa.shift[i];
+  }
+  k.d = rm.d;
+  k.f64 = f64;
+  k.multi = multi ? 1 : 0;
+  k.tma = ctx->disable_tma ? 0 : 1;
+  auto same = [&](const CullTune& a) {
+    return memcmp(a.ld, k.ld, sizeof(k.ld)) == 0 && memcmp(a.off, k.off, sizeof(k.off)) == 0 &&
+           memcmp(a.adims, k.adims, sizeof(k.adims)) == 0 && memcmp(a.estride, k.estride, sizeof(k.estride)) == 0 &&
+           memcmp(a.shift, k.shift, sizeof(k.shift)) == 0 && a.d == k.d && a.f64 == k.f64 && a.multi == k.multi &&
+           a.tma == k.tma;
+  };
+  for (const CullTune& t : ctx->cull_tunes)
+    if (same(t)) {
+      *mode = t.mode;
+      return cudaSuccess;
+    }
+  cudaError_t e;
+  for (int m = 0; m < 2; ++m) {
+    float best = 0.f;
+    for (int rep = 0; rep < 4; ++rep) {
+      if ((e = cudaEventRecord(ctx->ev0, ctx->stream))) return e;
+      if ((e = enqueue(m))) return e;
+      if ((e = cudaEventRecord(ctx->ev_x, ctx->stream))) return e;
+      if ((e = ctx->sync())) return e;
+      float ms = 0.f;
+      if ((e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev_x))) return e;
+      if (rep == 1 || (rep > 1 && ms < best)) best = ms;  // rep 0 warms up
+    }
+    k.ms[m] = best;
+  }
+  k.mode = k.ms[1] < k.ms[0] ? 1 : 0;
+  if (ctx->cull_tunes.size() >= kMaxCullTunes) ctx->cull_tunes.erase(ctx->cull_tunes.begin());
+  ctx->cull_tunes.push_back(k);
+  *mode = k.mode;
+  return cudaSuccess;
+}
+
+}  // namespace ftk2b
+
 static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                 const ftk2b_field_desc* field, const ftk2b_cp_params* prm) {
   using Clk = std::chrono::steady_clock;
@@ -535,7 +610,9 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   memset(&cfg, 0, sizeof(cfg));
   cfg.Q = prm->sos_q;
   cfg.refined = prm->precision == FTK2B_PRECISION_REFINED;
+  cfg.cull_mode = ctx->cull_mode;  // 2 is resolved below, once the buffers exist
   cfg.tchunk = (int)rm.ld[d - 1];
+  if (cfg.cull_mode != 0) CUDA_TRY(ctx, setup_cull_scratch(ctx, rm, cfg));
   if (ctx->tune_tchunk > 0) cfg.tchunk = ctx->tune_tchunk;
   int TX, TY, TZ;
   regular_tile(d, &TX, &TY, &TZ);
@@ -573,10 +650,11 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e;
       if ((e = cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream))) return e;
+      int nk = 1;
       if ((e = launch_extract_regular(f64, rm, fa, cfg, cq, B.err, ctx->stream, !ctx->disable_tma,
-                                      &ctx->last_used_tma)))
+                                      &ctx->last_used_tma, &nk)))
         return e;
-      *nl += 1;
+      *nl += (unsigned long long)nk;
       return cudaSuccess;
     };
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
@@ -591,6 +669,25 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       return cudaMemcpyAsync(ctx->h_counters, ctx->counters.p, sizeof(unsigned) * kNumCounters,
                              cudaMemcpyDeviceToHost, ctx->stream);
     };
+    if (cfg.cull_mode == 2) {
+      int mode = 0;
+      CUDA_TRY(ctx, resolve_cull_mode(ctx, rm, fa, f64, field->layout == FTK2B_LAYOUT_MULTICOMPONENT,
+                                      [&](int md) -> cudaError_t {
+                                        ExtractConfig c = cfg;
+                                        c.cull_mode = md;
+                                        cudaError_t e = cudaMemsetAsync(ctx->counters.p, 0,
+                                                                        sizeof(unsigned) * kNumCounters, ctx->stream);
+                                        int nk = 1;
+                                        if (!e)
+                                          e = launch_extract_regular(f64, rm, fa, c, cq, B.err, ctx->stream,
+                                                                     !ctx->disable_tma, &ctx->last_used_tma, &nk);
+                                        ctx->launches += (unsigned long long)nk;
+                                        return e;
+                                      },
+                                      &mode));
+      cfg.cull_mode = mode;
+    }
+    ctx->last_cull_mode = cfg.cull_mode;
     const Clk::time_point p1 = Clk::now();
     ctx->phase_ms[0] += msd(p0, p1);
     Clk::time_point p2 = p1;

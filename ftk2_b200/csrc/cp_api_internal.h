@@ -2,6 +2,7 @@
 #pragma once
 
 #include <chrono>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -64,6 +65,18 @@ struct GraphEntry {
 };
 constexpr size_t kMaxGraphs = 16;
 
+// One workload shape decided by the cull-mode autotuner: the regular mesh
+// (local dims, offsets), the field's array shape and strides, dtype, layout
+// and whether TMA staging was allowed, with the extraction time measured for
+// each mode and the faster one.
+struct CullTune {
+  long long ld[4], off[4], adims[4], estride[4], shift[4];
+  int d, f64, multi, tma;
+  int mode;
+  float ms[2];
+};
+constexpr size_t kMaxCullTunes = 256;
+
 struct LastRun {
   int kind = 0, m = 0;
   uint64_t n = 0, ne = 0, n_roots = 0, n_simplices = 0;
@@ -86,11 +99,15 @@ struct ftk2b_ctx {
   unsigned cap_hint = 0;
   unsigned cand_cap_hint = 0;
   int tune_tchunk = 0;
+  int cull_mode = 2;  // FTK2B_OPT_CULL_MODE (2: chosen per workload shape)
+  int last_cull_mode = 0;  // the mode the last regular-mesh extraction ran
+  std::vector<ftk2b::CullTune> cull_tunes;
   bool disable_tma = false;
   int last_used_tma = 0;
   ftk2b::DevBuf stage[3], stage_scalar;
   ftk2b::DevBuf key, lam, bary4, scalar, key_alt, perm0, perm1, hist, lam_s, bary4_s, scalar_s,
       simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains, edge_slots;
+  ftk2b::DevBuf tstats, runs;  // cull mode 1 scratch (tile statistics, run list + count)
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::ExtCache ext;
   ftk2b::LastRun last;
@@ -147,6 +164,18 @@ ftk2b_status prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int mesh_d
                            const uint64_t* need_global_hi, const uint64_t* need_local_hi,
                            uint64_t n_vertices, FieldAccess& fa);
 ftk2b_status ensure_feature_buffers(ftk2b_ctx* ctx, unsigned cap, unsigned edge_cap, int m);
+
+// Sizes the tile-statistics scratch of cull mode 1 for this mesh and points
+// cfg at it.
+cudaError_t setup_cull_scratch(ftk2b_ctx* ctx, const RegularMesh& rm, ExtractConfig& cfg);
+
+// The cull mode of a regular-mesh extraction: modes 0 and 1 as the context
+// sets them; in mode 2 the mode decided for this workload shape, or, for a new
+// shape, the faster of 0 and 1 as timed with `enqueue(mode)` (counters reset
+// plus the extraction, on the context's stream): one warm-up pass, then the
+// best of three per mode.  Results never depend on the mode.
+cudaError_t resolve_cull_mode(ftk2b_ctx* ctx, const RegularMesh& rm, const FieldAccess& fa, int f64, bool multi,
+                              const std::function<cudaError_t(int)>& enqueue, int* mode);
 
 }  // namespace ftk2b
 

@@ -69,6 +69,13 @@ struct ExtractConfig {
   int tchunk;                  // corner time steps per block
   int tiles[3];                // tiles along x, y, z (z = 1 for 2D)
   int skip_first_spatial;      // 1: no purely spatial simplices at local time 0
+  int cull_mode;               // 0: per-vertex cull words only; 1: tile statistics first
+  // scratch of cull mode 1 (device): 8 ints per (slice, tile), and the runs
+  // of surviving tile-steps (4 words each: tile, first step, end step, pad)
+  int* tstats;
+  unsigned* runs;
+  unsigned* n_runs;
+  unsigned runs_cap;
 };
 
 // chain tables: masks of vertices 1..m of every m-simplex type of a
@@ -81,10 +88,13 @@ struct ChainTable {
 void upload_chain_tables();
 
 // Launches the fused extraction; uses TMA tensor-tile staging when allowed
-// and the array satisfies the 16-byte alignment rules (reported in used_tma).
+// and the array satisfies the 16-byte alignment rules (reported in used_tma);
+// *launches (optional) receives the number of kernels it launched.
 cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
                                    const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
-                                   cudaStream_t st, bool allow_tma, int* used_tma);
+                                   cudaStream_t st, bool allow_tma, int* used_tma, int* launches = nullptr);
+// Scratch of cull mode 1 for a mesh: tile-slice statistics and run list sizes.
+void tile_scratch_size(const RegularMesh& mesh, size_t* stats_bytes, unsigned* runs_cap);
 // Exact SoS + solve of the queued candidates, compacted into the sink.
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
                                   const ExtractConfig& cfg, const CandidateQueue& cq,

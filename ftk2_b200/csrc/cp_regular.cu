@@ -19,8 +19,11 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 #include "cp_cull.cuh"
 #include "cp_device.cuh"
@@ -393,6 +396,709 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Stage 1, tile-statistics form (cull mode 1), in three launches.
+//
+// 1. plane_stats_kernel: per (slice, z plane, y-tile, x-tile), the minimum
+//    and maximum of every component over the tile's TX + 1 by TY + 1 vertices
+//    of that plane, kept as order-preserving integer keys of the high 32-bit
+//    words; every vertex row is read once with coalesced loads.
+// 2. tile_runs_kernel: one thread per tile merges the TZ + 1 planes of its
+//    box per slice, decides every tile-step (the hypercubes between slices c
+//    and c+1) and lists the runs of consecutive steps that survive.  A step is dropped when
+//      * every magnitude is below 4e-13 (the first pivot of every solve is
+//        below 1e-12, zero_crossing.hpp:72), or
+//      * some component is strictly positive above kappa * M on every vertex,
+//        or strictly negative below -kappa * M (M = the step's largest
+//        magnitude; kappa = 2^-24 for double, 2^-12 for float): the argument
+//        of the per-vertex cull words applied to the whole tile-step.
+//    The bounds are conservative: minima of high words are lower bounds of
+//    positive values and maxima upper bounds of negative ones, M is rounded up.
+// 3. run_cull_kernel: persistent CTAs walk the runs; thread 0 streams each
+//    run's slices, in order and across run boundaries, through a ring of
+//    kNbuf TMA buffers, and the block computes the per-vertex words and the
+//    per-hypercube cull of every step of the run, as extract_regular_kernel
+//    does for a whole tile.
+constexpr int kNbuf = 4;
+
+template <typename T, int D, bool MULTI>
+struct Geo2 {
+  using G = Geo<T, D, MULTI>;
+  static constexpr int WORDS = kNbuf * G::BYTES;     // offset of the word slots
+  // word slots: one per raw buffer (the words of stream slice q in slot
+  // q % kNbuf) and one that stays all-absent (the missing next slice of a
+  // run's last corner slice)
+  static constexpr int SMEM = WORDS + (kNbuf + 1) * G::VSP * 4;
+};
+
+__device__ __forceinline__ int ord_key(unsigned h) {
+  // signed-integer order of IEEE sign-magnitude words
+  return (int)(h ^ ((unsigned)((int)h >> 31) >> 1));
+}
+
+constexpr int kStatsWarps = 8;
+
+// One warp per (chunk of XT x-tiles, y-tile, z plane, slice) of separate
+// component arrays: it streams the TY + 1 vertex rows of its y-tile (the next
+// tile's first row included) over the chunk's XT * TX + 1 vertices, lane l
+// loading vertex 32 g + l of every component (g: 32-vertex group), and writes
+// per x-tile the minimum and maximum order key of every component over the
+// tile's TX + 1 x-vertices and TY + 1 rows of this plane.  Group XT holds the
+// chunk's halo vertex (the next tile's first vertex), which belongs to the
+// last tile of the chunk as well.  The z planes of a tile are merged when the
+// tile-steps are decided, so no plane is read twice.
+template <typename T, int D, int XT>
+__global__ void __launch_bounds__(kStatsWarps * 32, 2)
+    plane_stats_kernel(RegularMesh mesh, FieldAccess fa, ExtractConfig cfg) {
+  constexpr int M = D - 1;
+  constexpr int TX = Tile<D>::TX, TY = Tile<D>::TY;
+  constexpr int NG = XT + 1;
+  static_assert(TX == 32, "a 32-vertex group is one x-tile");
+  const int lane = threadIdx.x & 31;
+  const int nxc = (cfg.tiles[0] + XT - 1) / XT;
+  const int ldz = (D == 4) ? (int)mesh.ld[2] : 1;
+  const int lt = (int)mesh.ld[D - 1];
+  long long task = (long long)blockIdx.x * kStatsWarps + (threadIdx.x >> 5);
+  const int xc = (int)(task % nxc);
+  task /= nxc;
+  const int yt = (int)(task % cfg.tiles[1]);
+  task /= cfg.tiles[1];
+  const int z = (int)(task % ldz);
+  const int s = (int)(task / ldz);
+  if (s >= lt) return;  // whole warp
+  const int xt0 = xc * XT;
+  const int x0 = xt0 * TX, y0 = yt * TY;
+  const int nvy = min(TY + 1, (int)mesh.ld[1] - y0);
+  const int nx = min(XT * TX + 1, (int)mesh.ld[0] - x0);  // chunk vertices, halo included
+  const long long at = ((long long)s + mesh.off[D - 1] - fa.shift[D - 1]) ^ fa.tflip;
+  long long obase = at * fa.estride[D - 1] + (x0 + mesh.off[0] - fa.shift[0]) * fa.estride[0];
+  if (D == 4) obase += (z + mesh.off[2] - fa.shift[2]) * fa.estride[2];
+  int kmn[NG][M], kmx[NG][M];
+#pragma unroll
+  for (int g = 0; g < NG; ++g)
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+      kmn[g][r] = 0x7FFFFFFF;
+      kmx[g][r] = (int)0x80000000;
+    }
+  for (int vy = 0; vy < nvy; ++vy) {
+    const long long orow = obase + (y0 + vy + mesh.off[1] - fa.shift[1]) * fa.estride[1];
+    T v[NG][M];
+#pragma unroll
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+      for (int r = 0; r < M; ++r) {
+        const int x = 32 * g + lane;
+        v[g][r] = (x < nx) ? __ldcs(static_cast<const T*>(fa.comp[r]) + orow + x * fa.estride[0]) : T(0);
+      }
+#pragma unroll
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+      for (int r = 0; r < M; ++r)
+        if (32 * g + lane < nx) {
+          const int key = ord_key(hi_word<T>(v[g][r]));
+          kmn[g][r] = min(kmn[g][r], key);
+          kmx[g][r] = max(kmx[g][r], key);
+        }
+  }
+  const size_t row_entry = (((size_t)s * ldz + z) * cfg.tiles[1] + yt) * cfg.tiles[0];
+#pragma unroll
+  for (int t = 0; t < XT; ++t) {
+    if (xt0 + t >= cfg.tiles[0]) break;  // whole warp
+    int rmn[M], rmx[M];
+#pragma unroll
+    for (int c = 0; c < M; ++c) {
+      rmn[c] = kmn[t][c];
+      rmx[c] = kmx[t][c];
+      if (lane == 0) {  // the halo vertex: lane 0 of group t + 1
+        rmn[c] = min(rmn[c], kmn[t + 1][c]);
+        rmx[c] = max(rmx[c], kmx[t + 1][c]);
+      }
+      rmn[c] = __reduce_min_sync(0xFFFFFFFFu, rmn[c]);
+      rmx[c] = __reduce_max_sync(0xFFFFFFFFu, rmx[c]);
+    }
+    if (lane == 0) {
+      int4 lo, hi;
+      lo.x = rmn[0];
+      lo.y = M > 1 ? rmn[M > 1 ? 1 : 0] : 0x7FFFFFFF;
+      lo.z = M > 2 ? rmn[M > 2 ? 2 : 0] : 0x7FFFFFFF;
+      lo.w = rmx[0];
+      hi.x = M > 1 ? rmx[M > 1 ? 1 : 0] : (int)0x80000000;
+      hi.y = M > 2 ? rmx[M > 2 ? 2 : 0] : (int)0x80000000;
+      hi.z = 0;
+      hi.w = 0;
+      int4* dst = reinterpret_cast<int4*>(cfg.tstats + 8 * (row_entry + xt0 + t));
+      dst[0] = lo;
+      dst[1] = hi;
+    }
+  }
+}
+
+// Per-thread asynchronous global -> shared copies (each thread later reads
+// back only what it copied itself, after cp.async.wait_group).
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_small(void* dst, const void* src) {
+  static_assert(N == 4 || N == 8, "cp.async.ca copies 4, 8 or 16 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "n"(N)
+               : "memory");
+}
+// high 32-bit word of element u of a 16-byte vector (little-endian)
+template <typename T>
+__device__ __forceinline__ unsigned vec_hi_word(const uint4& w, int u) {
+  if (sizeof(T) == 8) return u == 0 ? w.y : w.w;
+  return u == 0 ? w.x : u == 1 ? w.y : u == 2 ? w.z : w.w;
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The same statistics for interleaved components whose rows start on 16-byte
+// boundaries, streamed: persistent warps walk the tasks (warp w takes tasks
+// w, w + W, ... for W warps in the grid) as one continuous sequence of rows,
+// and every thread keeps S - 1 rows of its own 16-byte copies in flight
+// through a private S-stage ring in shared memory, across task boundaries.
+//   Lane l serves tile t = l / LPT of the chunk (LPT = 32 / XT lanes per
+//   tile) as its q = l % LPT-th part: its vector j covers tile elements
+//   LPT V j + V q .. + V - 1 (V elements per 16 bytes), so every copy
+//   instruction of the warp reads XT runs of LPT V consecutive elements.  The
+//   component of element e is e mod M = (a + V q) mod M with a = (LPT V j + u)
+//   mod M known at compile time: each lane keeps one accumulator per slot a
+//   and rotates them by V q when the task ends.  Lane q = LPT - 1 also copies
+//   the tile's halo vertex (the next tile's first).
+template <typename T, int D, int XT, int S>
+struct StatsStream {
+  static constexpr int M = D - 1;
+  static constexpr int V = 16 / (int)sizeof(T);
+  static constexpr int LPT = 32 / XT;
+  static constexpr int NV = 32 * M / (LPT * V);
+  static constexpr int THREADS = kStatsWarps * 32;
+  static constexpr int HALO = S * THREADS * NV;              // uint4 offset of the halo slots
+  static constexpr int SMEM = 16 * (HALO + S * kStatsWarps * XT);
+  static_assert(NV * LPT * V == 32 * M, "a tile row splits evenly over its lanes");
+};
+
+template <typename T, int D, int XT, int S>
+__global__ void __launch_bounds__(kStatsWarps * 32, 2)
+    plane_stats_stream_kernel(RegularMesh mesh, FieldAccess fa, ExtractConfig cfg, int ntasks) {
+  using SS = StatsStream<T, D, XT, S>;
+  constexpr int M = SS::M, V = SS::V, LPT = SS::LPT, NV = SS::NV;
+  constexpr int TX = Tile<D>::TX, TY = Tile<D>::TY;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint4* const ring = reinterpret_cast<uint4*>(smem);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t = lane / LPT, q = lane % LPT;
+  const int tb = 32 * M * t;  // the lane's tile, first element of the chunk row
+  const int nxc = (cfg.tiles[0] + XT - 1) / XT;
+  const int ldz = (D == 4) ? (int)mesh.ld[2] : 1;
+  const int nw = (int)gridDim.x * kStatsWarps;
+
+  struct Task {
+    int task, vy, nvy, ne, y0, xt0, yt, z, s;
+    const T* base;
+  };
+  auto decode = [&](int task, Task& g) {
+    g.task = task;
+    g.vy = 0;
+    if (task >= ntasks) return;
+    int r = task;
+    const int xc = r % nxc;
+    r /= nxc;
+    g.yt = r % cfg.tiles[1];
+    r /= cfg.tiles[1];
+    g.z = r % ldz;
+    g.s = r / ldz;
+    g.xt0 = xc * XT;
+    const int x0 = g.xt0 * TX;
+    g.y0 = g.yt * TY;
+    g.nvy = min(TY + 1, (int)mesh.ld[1] - g.y0);
+    g.ne = min(XT * TX + 1, (int)mesh.ld[0] - x0) * M;
+    const long long at = ((long long)g.s + mesh.off[D - 1] - fa.shift[D - 1]) ^ fa.tflip;
+    long long o = at * fa.estride[D - 1] + (x0 + mesh.off[0] - fa.shift[0]) * fa.estride[0] +
+                  (long long)(g.y0 + mesh.off[1] - fa.shift[1]) * fa.estride[1];
+    if (D == 4) o += (g.z + mesh.off[2] - fa.shift[2]) * fa.estride[2];
+    g.base = static_cast<const T*>(fa.comp[0]) + o;
+  };
+  auto vslot = [&](int stage, int j) { return ring + (stage * NV + j) * SS::THREADS + tid; };
+  auto hslot = [&](int stage) { return ring + SS::HALO + (stage * kStatsWarps + warp) * XT + t; };
+
+  Task gi, gc;  // the issuing and the consuming side of the row sequence
+  decode(blockIdx.x * kStatsWarps + warp, gi);
+  gc = gi;
+  auto issue = [&](int stage) {
+    if (gi.task < ntasks) {
+      const T* row = gi.base + (long long)gi.vy * fa.estride[1];
+#pragma unroll
+      for (int j = 0; j < NV; ++j) {
+        const int e = tb + LPT * V * j + V * q;
+        if (e + V <= gi.ne) {
+          cp_async_16(vslot(stage, j), row + e);
+        } else {
+#pragma unroll
+          for (int u = 0; u < V; ++u)
+            if (e + u < gi.ne) cp_async_small<sizeof(T)>(reinterpret_cast<T*>(vslot(stage, j)) + u, row + e + u);
+        }
+      }
+      if (q == LPT - 1) {
+#pragma unroll
+        for (int u = 0; u < M; ++u)
+          if (tb + 32 * M + u < gi.ne)
+            cp_async_small<sizeof(T)>(reinterpret_cast<T*>(hslot(stage)) + u, row + tb + 32 * M + u);
+      }
+      if (++gi.vy == gi.nvy) decode(gi.task + nw, gi);
+    }
+    cp_async_commit();  // empty groups keep the count uniform
+  };
+
+  int kmn[M], kmx[M], hmn[M], hmx[M];
+  auto reset = [&]() {
+#pragma unroll
+    for (int a = 0; a < M; ++a) {
+      kmn[a] = hmn[a] = 0x7FFFFFFF;
+      kmx[a] = hmx[a] = (int)0x80000000;
+    }
+  };
+  reset();
+#pragma unroll
+  for (int p = 0; p < S - 1; ++p) issue(p);
+  int stage = 0;
+  while (gc.task < ntasks) {
+    issue(stage == 0 ? S - 1 : stage - 1);  // the slot consumed one row ago
+    cp_async_wait<S - 1>();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      const uint4 w = *vslot(stage, j);
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const int a = (LPT * V * j + u) % M;
+        if (tb + LPT * V * j + V * q + u < gc.ne) {
+          const int key = ord_key(vec_hi_word<T>(w, u));
+          kmn[a] = min(kmn[a], key);
+          kmx[a] = max(kmx[a], key);
+        }
+      }
+    }
+    if (q == LPT - 1) {
+      const uint4 w = *hslot(stage);
+#pragma unroll
+      for (int u = 0; u < M; ++u)
+        if (tb + 32 * M + u < gc.ne) {
+          const int key = ord_key(vec_hi_word<T>(w, u));
+          hmn[u] = min(hmn[u], key);
+          hmx[u] = max(hmx[u], key);
+        }
+    }
+    stage = (stage + 1 == S) ? 0 : stage + 1;
+    if (++gc.vy < gc.nvy) continue;
+    // task complete: slot a holds component (a + V q) mod M
+    int rmn[M], rmx[M];
+    const int rot = (V * q) % M;
+#pragma unroll
+    for (int c = 0; c < M; ++c) {
+      rmn[c] = hmn[c];
+      rmx[c] = hmx[c];
+#pragma unroll
+      for (int a = 0; a < M; ++a)
+        if ((a + rot) % M == c) {
+          rmn[c] = min(rmn[c], kmn[a]);
+          rmx[c] = max(rmx[c], kmx[a]);
+        }
+#pragma unroll
+      for (int o = 1; o < LPT; o <<= 1) {
+        rmn[c] = min(rmn[c], __shfl_xor_sync(0xFFFFFFFFu, rmn[c], o));
+        rmx[c] = max(rmx[c], __shfl_xor_sync(0xFFFFFFFFu, rmx[c], o));
+      }
+    }
+    if (q == 0 && gc.xt0 + t < cfg.tiles[0]) {
+      int4 lo, hi;
+      lo.x = rmn[0];
+      lo.y = M > 1 ? rmn[M > 1 ? 1 : 0] : 0x7FFFFFFF;
+      lo.z = M > 2 ? rmn[M > 2 ? 2 : 0] : 0x7FFFFFFF;
+      lo.w = rmx[0];
+      hi.x = M > 1 ? rmx[M > 1 ? 1 : 0] : (int)0x80000000;
+      hi.y = M > 2 ? rmx[M > 2 ? 2 : 0] : (int)0x80000000;
+      hi.z = 0;
+      hi.w = 0;
+      const size_t entry = (((size_t)gc.s * ldz + gc.z) * cfg.tiles[1] + gc.yt) * cfg.tiles[0] + gc.xt0 + t;
+      int4* dst = reinterpret_cast<int4*>(cfg.tstats + 8 * entry);
+      dst[0] = lo;
+      dst[1] = hi;
+    }
+    reset();
+    decode(gc.task + nw, gc);
+  }
+  cp_async_wait<0>();
+}
+
+// largest high-word magnitude of a set of values, from the order keys of its
+// per-component extremes (|v| <= max(|min|, |max|)); a NaN or infinity, whose
+// key lies beyond every finite one, gives a magnitude >= the exponent mask
+__device__ __forceinline__ unsigned key_mag(int k) {
+  return k >= 0 ? (unsigned)k : (~(unsigned)k & 0x7FFFFFFFu);
+}
+
+// whether the tile-step between slices c and c+1 (c+1 absent for the last
+// corner slice) can hold no accepted simplex
+template <typename T, int M>
+__device__ __forceinline__ bool tile_step_culled(const int* st_c, const int* st_s) {
+  using P = CullParams<T>;
+  constexpr int kKappaTile = P::kappa_exp + 3 * P::band;  // kappa = 2^-kKappaTile
+  unsigned am = (unsigned)st_c[6];
+  int kmn[3] = {st_c[0], st_c[1], st_c[2]}, kmx[3] = {st_c[3], st_c[4], st_c[5]};
+  if (st_s) {
+    am = max(am, (unsigned)st_s[6]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      kmn[j] = min(kmn[j], st_s[j]);
+      kmx[j] = max(kmx[j], st_s[3 + j]);
+    }
+  }
+  if (am >= P::expmask) return false;  // an infinite or NaN value: never dropped
+  if (am < P::tiny_hi) return true;
+  const unsigned mup = am + 1u;  // upper bound of M in high-word space
+  const unsigned kexp = (unsigned)kKappaTile << P::mant;
+  if ((mup & P::expmask) <= kexp) return false;
+  const unsigned thr = mup - kexp;  // kappa * M_up, exact
+  const int kpos = (int)thr, kneg = ord_key(thr | 0x80000000u);
+  bool culled = false;
+#pragma unroll
+  for (int j = 0; j < M; ++j) culled |= (kmn[j] > kpos) || (kmx[j] < kneg);
+  return culled;
+}
+
+// The statistics of one tile over slice c: the plane entries of its z
+// planes z0 .. z0 + TZ (clipped to the mesh) merged, and the magnitude bound
+// in word 6.
+template <int D>
+__device__ __forceinline__ void tile_slice_stats(const RegularMesh& mesh, const ExtractConfig& cfg, int xt, int yt,
+                                                 int zt, int c, int out[8]) {
+  constexpr int TZ = Tile<D>::TZ;
+  const int ldz = (D == 4) ? (int)mesh.ld[2] : 1;
+  const int z0 = (D == 4) ? zt * TZ : 0;
+  const int nz = (D == 4) ? min(TZ + 1, ldz - z0) : 1;
+  int4 a[TZ + 1], b[TZ + 1];
+#pragma unroll
+  for (int k = 0; k <= TZ; ++k)
+    if (k < nz) {
+      const int4* e = reinterpret_cast<const int4*>(
+          cfg.tstats + 8 * ((((size_t)c * ldz + z0 + k) * cfg.tiles[1] + yt) * cfg.tiles[0] + xt));
+      a[k] = e[0];
+      b[k] = e[1];
+    }
+  int4 p = a[0], q = b[0];
+#pragma unroll
+  for (int k = 1; k <= TZ; ++k)
+    if (k < nz) {
+      p.x = min(p.x, a[k].x);
+      p.y = min(p.y, a[k].y);
+      p.z = min(p.z, a[k].z);
+      p.w = max(p.w, a[k].w);
+      q.x = max(q.x, b[k].x);
+      q.y = max(q.y, b[k].y);
+    }
+  out[0] = p.x;
+  out[1] = p.y;
+  out[2] = p.z;
+  out[3] = p.w;
+  out[4] = q.x;
+  out[5] = q.y;
+  unsigned am = 0;
+#pragma unroll
+  for (int j = 0; j < D - 1; ++j) am = max(am, max(key_mag(out[j]), key_mag(out[3 + j])));
+  out[6] = (int)am;
+  out[7] = 0;
+}
+
+template <typename T, int D>
+__global__ void tile_runs_kernel(RegularMesh mesh, ExtractConfig cfg) {
+  constexpr int M = D - 1;
+  const int ntiles = cfg.tiles[0] * cfg.tiles[1] * cfg.tiles[2];
+  const int lt = (int)mesh.ld[D - 1];
+  for (int tile = blockIdx.x * blockDim.x + threadIdx.x; tile < ntiles; tile += gridDim.x * blockDim.x) {
+    const int xt = tile % cfg.tiles[0], yt = (tile / cfg.tiles[0]) % cfg.tiles[1];
+    const int zt = tile / (cfg.tiles[0] * cfg.tiles[1]);
+    int sc[8], ss[8];
+    tile_slice_stats<D>(mesh, cfg, xt, yt, zt, 0, ss);
+    int start = -1;
+    for (int c = 0; c <= lt; ++c) {
+      bool keep = false;
+      if (c < lt) {
+#pragma unroll
+        for (int f = 0; f < 8; ++f) sc[f] = ss[f];
+        if (c + 1 < lt) tile_slice_stats<D>(mesh, cfg, xt, yt, zt, c + 1, ss);
+        keep = !tile_step_culled<T, M>(sc, c + 1 < lt ? ss : nullptr);
+      }
+      if (keep && start < 0) start = c;
+      if (!keep && start >= 0) {
+        const unsigned r = atomicAdd(cfg.n_runs, 1u);
+        if (r < cfg.runs_cap) {
+          uint4 run;
+          run.x = (unsigned)tile;
+          run.y = (unsigned)start;
+          run.z = (unsigned)c;
+          run.w = 0;
+          reinterpret_cast<uint4*>(cfg.runs)[r] = run;
+        }
+        start = -1;
+      }
+    }
+  }
+}
+
+template <typename T, int D, bool MULTI, bool TMA>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1)
+    run_cull_kernel(const __grid_constant__ CUtensorMap map0, const __grid_constant__ CUtensorMap map1,
+                    const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa, ExtractConfig cfg,
+                    CandidateQueue cq, unsigned* err) {
+  using G = Geo<T, D, MULTI>;
+  using G2 = Geo2<T, D, MULTI>;
+  constexpr int M = D - 1;
+  constexpr int TX = G::TX, TY = G::TY, TZ = G::TZ;
+  constexpr int VX = G::VX, VY = G::VY, VZ = G::VZ, VS = G::VS, VPT = G::VPT, VSP = G::VSP;
+  constexpr int TBIT = 1 << (D - 1);
+  constexpr int HW = sizeof(T) / 4;
+  static_assert(D == 3 ? kWarps * kRows == TY : kWarps == TY * (TZ / kRows),
+                "every corner row of the tile belongs to exactly one warp");
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned long long bar[kNbuf];
+  __shared__ unsigned band_tbl[kBandTable];
+  unsigned* const W0 = reinterpret_cast<unsigned*>(smem + G2::WORDS);
+  auto wslot = [&](int w) { return W0 + w * VSP; };
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int ldx = (int)mesh.ld[0], ldy = (int)mesh.ld[1], ldz = (D == 4) ? (int)mesh.ld[2] : 1;
+  const int lt = (int)mesh.ld[D - 1];
+  const int n_items = (int)min(*cfg.n_runs, cfg.runs_cap);
+  const uint4* runs = reinterpret_cast<const uint4*>(cfg.runs);
+  int aoff[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) aoff[k] = (k < D) ? (int)(mesh.off[k] - fa.shift[k]) : 0;
+  auto tcoord = [&](int s) { return (s + aoff[D - 1]) ^ fa.tflip; };
+  auto item_geom = [&](int item, int& x0, int& y0, int& z0, int& t0, int& t1, int& s_end) {
+    const uint4 run = runs[item];
+    int tix = (int)run.x;
+    x0 = (tix % cfg.tiles[0]) * TX;
+    tix /= cfg.tiles[0];
+    y0 = (tix % cfg.tiles[1]) * TY;
+    tix /= cfg.tiles[1];
+    z0 = (D == 4) ? tix * TZ : 0;
+    t0 = (int)run.y;
+    t1 = (int)run.z;
+    s_end = min(t1, lt - 1);
+  };
+  fill_band_table<T>(band_tbl, tid, kThreads);
+
+  // ---- producer (thread 0): the CTA's slice stream over its runs
+  int p_item = blockIdx.x, p_s = 0, p_send = -1, px0 = 0, py0 = 0, pz0 = 0;
+  int pq = 0;  // stream index of the next slice to issue
+  auto p_begin = [&]() {
+    if (p_item < n_items) {
+      int t0, t1;
+      item_geom(p_item, px0, py0, pz0, t0, t1, p_send);
+      p_s = t0;
+    }
+  };
+  auto issue_next = [&]() {
+    const int buf = pq % kNbuf;
+    unsigned char* dst0 = smem + buf * G::BYTES;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[buf], G::TX_BYTES);
+    const int cx = (px0 + aoff[0]) * (MULTI ? M : 1);
+    const int cy = py0 + aoff[1];
+    if constexpr (MULTI) {
+      if constexpr (D == 4) tma_load_4d(dst0, &map0, cx, cy, pz0 + aoff[2], tcoord(p_s), &bar[buf]);
+      else tma_load_3d(dst0, &map0, cx, cy, tcoord(p_s), &bar[buf]);
+    } else {
+      const CUtensorMap* maps[3] = {&map0, &map1, &map2};
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        if constexpr (D == 4)
+          tma_load_4d(dst0 + j * G::COMP, maps[j], cx, cy, pz0 + aoff[2], tcoord(p_s), &bar[buf]);
+        else
+          tma_load_3d(dst0 + j * G::COMP, maps[j], cx, cy, tcoord(p_s), &bar[buf]);
+      }
+    }
+    ++pq;
+    if (++p_s > p_send) {
+      p_item += gridDim.x;
+      p_begin();
+    }
+  };
+  auto produce_until = [&](int qmax) {
+    while (pq <= qmax && p_item < n_items) issue_next();
+  };
+
+  int x0 = 0, y0 = 0, z0 = 0, t0 = 0, t1 = 0, s_end = 0;
+  int voff[VPT];
+#pragma unroll
+  for (int u = 0; u < VPT; ++u) voff[u] = 0;
+  unsigned vvalid = 0, row_valid = 0;
+  const int cyw = (D == 4) ? warp % TY : warp * kRows;
+  const int czw = (D == 4) ? (warp / TY) * kRows : 0;
+  auto load_plain = [&](int s, int buf) {
+    T* dst = reinterpret_cast<T*>(smem + buf * G::BYTES);
+    constexpr int NPER = G::VXBOX * VY * VZ;
+    for (int e = tid; e < NPER * M; e += kThreads) {
+      const int j = MULTI ? e % M : e / NPER;
+      const int r = MULTI ? e / M : e % NPER;
+      const int vx = r % G::VXBOX;
+      const int vy = (r / G::VXBOX) % VY;
+      const int vz = r / (G::VXBOX * VY);
+      const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : (long long)s, (long long)s};
+      bool in = true;
+      long long o = 0;
+      if (fa.per_vertex) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          in &= l[k] < mesh.ld[k];
+          o += (l[k] + mesh.off[k]) * (long long)mesh.gstride[k];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          const long long a = (k == D - 1) ? (long long)tcoord(s) : l[k] + aoff[k];
+          in &= a >= 0 && a < fa.adims[k];
+          o += a * fa.estride[k];
+        }
+      }
+      T v = T(0);
+      if (in) v = static_cast<const T*>(fa.comp[j])[o];
+      if (MULTI) dst[((vz * VY + vy) * G::VXBOX + vx) * M + j] = v;
+      else dst[j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX + vx] = v;
+    }
+  };
+  int cq_idx = 0;  // stream index of slice t0 of the current run
+  auto arrive = [&](int s) -> bool {
+    const int q = cq_idx + (s - t0);
+    if constexpr (TMA) return mbar_wait(&bar[q % kNbuf], (unsigned)((q / kNbuf) & 1));
+    load_plain(s, q % kNbuf);
+    __syncthreads();
+    return true;
+  };
+  auto words = [&](int s, unsigned* dst) {
+    const unsigned* r =
+        reinterpret_cast<const unsigned*>(smem + ((cq_idx + (s - t0)) % kNbuf) * G::BYTES) + (HW - 1);
+#pragma unroll
+    for (int u = 0; u < VPT; ++u) {
+      unsigned h[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) h[j] = r[HW * (MULTI ? voff[u] + j : voff[u] + j * G::COMP_ELEMS)];
+      const unsigned w = vertex_word_hi<T, M>(h, band_tbl);
+      dst[tid + u * kThreads] = ((vvalid >> u) & 1u) ? w : kAbsent;
+    }
+  };
+
+  if (TMA && tid == 0)
+    for (int b = 0; b < kNbuf; ++b) mbar_init(&bar[b], 1);
+  if (TMA && tid == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  for (int i = tid; i < VSP; i += kThreads) wslot(kNbuf)[i] = kAbsent;
+  __syncthreads();
+  if (TMA && tid == 0) {
+    p_begin();
+    produce_until(kNbuf - 1);
+  }
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    item_geom(item, x0, y0, z0, t0, t1, s_end);
+    vvalid = 0;
+#pragma unroll
+    for (int u = 0; u < VPT; ++u) {
+      const int i = tid + u * kThreads;
+      const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
+      const bool in = i < VS && x0 + vx < ldx && y0 + vy < ldy && (D == 3 || z0 + vz < ldz);
+      voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
+      vvalid |= (in ? 1u : 0u) << u;
+    }
+    row_valid = 0;
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      const int cy = (D == 4) ? cyw : cyw + q;
+      const int cz = (D == 4) ? czw + q : 0;
+      if (x0 + lane < ldx && y0 + cy < ldy && (D == 3 || z0 + cz < ldz)) row_valid |= 1u << q;
+    }
+    for (int c = t0; c < t1; ++c) {
+      const int s = c + 1;
+      const bool has_s = s <= s_end;
+      bool ok = true;
+      // words of stream slice q live in slot q % kNbuf: the slots written
+      // here were last read two or more steps ago, before the previous
+      // step's barrier
+      const int q_c = cq_idx + (c - t0);
+      if (c == t0) {
+        ok = arrive(c);
+        if (ok) words(c, wslot(q_c % kNbuf));
+      }
+      if (ok && has_s) {
+        ok = arrive(s);
+        if (ok) words(s, wslot((q_c + 1) % kNbuf));
+      }
+      // the one barrier of the step: words of both slices visible, every
+      // read of the raw buffer that the next issued slice reuses done
+      if (__syncthreads_or(!ok)) {
+        if (TMA && tid == 0)
+          for (int q = cq_idx + (c - t0); q < pq; ++q) mbar_wait(&bar[q % kNbuf], (unsigned)((q / kNbuf) & 1));
+        if (tid == 0) atomicOr(err, 2u);
+        return;
+      }
+      if (TMA && tid == 0) produce_until(q_c + kNbuf - 1);
+      const unsigned* A = wslot(q_c % kNbuf);
+      const unsigned* B = has_s ? wslot((q_c + 1) % kNbuf) : wslot(kNbuf);
+      unsigned R[kRows + 1];
+#pragma unroll
+      for (int q = 0; q <= kRows; ++q) {
+        unsigned r, e;
+        if constexpr (D == 4) {
+          const int i0 = ((czw + q) * VY + cyw) * VX + lane, i1 = i0 + VX;
+          r = A[i0] & A[i1] & B[i0] & B[i1];
+          e = (lane == 31) ? (A[i0 + 1] & A[i1 + 1] & B[i0 + 1] & B[i1 + 1]) : kAbsent;
+        } else {
+          const int i0 = (cyw + q) * VX + lane;
+          r = A[i0] & B[i0];
+          e = (lane == 31) ? (A[i0 + 1] & B[i0 + 1]) : kAbsent;
+        }
+        const unsigned nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
+        R[q] = r & (lane == 31 ? e : nb);
+      }
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) {
+        const int cy = (D == 4) ? cyw : cyw + q;
+        const int cz = (D == 4) ? czw + q : 0;
+        const bool keep = ((row_valid >> q) & 1u) && !word_culled(R[q] & R[q + 1]);
+        const unsigned ball = __ballot_sync(0xFFFFFFFFu, keep);
+        if (ball) {
+          unsigned basei = 0;
+          if (lane == 0) basei = atomicAdd(cq.count, (unsigned)__popc(ball));
+          basei = __shfl_sync(0xFFFFFFFFu, basei, 0);
+          if (keep) {
+            const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
+            if (idx < cq.cap) {
+              const int l0 = x0 + lane, l1 = y0 + cy, l2 = (D == 4) ? z0 + cz : c;
+              int vmask = 0;
+              if (l0 + 1 < ldx) vmask |= 1;
+              if (l1 + 1 < ldy) vmask |= 2;
+              if (D == 4 && l2 + 1 < ldz) vmask |= 4;
+              if (c + 1 < lt) vmask |= TBIT;
+              unsigned long long ch = c_chains_by_vmask[D - 3][vmask];
+              if (cfg.skip_first_spatial && c == 0) ch &= c_time_chains[D - 3];
+              cq.corner[idx] = pack_corner(l0, l1, (D == 4) ? l2 : 0, c);
+              cq.chains[idx] = ch;
+            }
+          }
+        }
+      }
+    }
+    cq_idx += s_end - t0 + 1;
+  }
+}
+
 // Stage 2: exact SoS test and bit-exact solve of the queued chains.  One warp
 // per candidate hypercube: its 2^D vertices' values are gathered once into
 // shared memory, then each lane tests one chain; accepted simplices are
@@ -633,10 +1339,33 @@ static bool encode_map(CUtensorMap* map, bool f64, const void* base, int rank, c
   return r == CUDA_SUCCESS;
 }
 
+constexpr int kStatsStages = 4;
+
+template <typename T, int D, int XT>
+cudaError_t launch_stats_stream(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                                int ntasks, cudaStream_t st) {
+  using SS = StatsStream<T, D, XT, kStatsStages>;
+  auto k = plane_stats_stream_kernel<T, D, XT, kStatsStages>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SS::SMEM);
+  if (e) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, SS::THREADS, SS::SMEM) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const long long want = (long long)sms * per_sm;
+  const long long need = (ntasks + kStatsWarps - 1) / kStatsWarps;
+  k<<<(unsigned)std::max<long long>(1, std::min(want, need)), SS::THREADS, SS::SMEM, st>>>(mesh, fa, cfg, ntasks);
+  return cudaGetLastError();
+}
+
 template <typename T, int D, bool MULTI>
 static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                             const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
-                            int* used_tma) {
+                            int* used_tma, int* launches) {
   using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
   const size_t es = sizeof(T);
@@ -684,6 +1413,54 @@ static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, cons
   const unsigned ntiles = (unsigned)cfg.tiles[0] * cfg.tiles[1] * cfg.tiles[2];
   dim3 grid(ntiles, nchunks);
   cudaError_t e;
+  // cull mode 1: arrays the TMA kernels can stage, with the caller's scratch
+  const bool vec_ok = tma && cfg.tstats && cfg.runs && cfg.n_runs && cfg.runs_cap;
+  bool sep = false, stats_ok = false;
+  if (cfg.cull_mode == 1 && vec_ok) {
+    bool ilv = MULTI && fa.estride[0] == M;
+    for (int j = 1; j < M && ilv; ++j)
+      ilv = static_cast<const char*>(fa.comp[j]) == static_cast<const char*>(fa.comp[0]) + j * sizeof(T);
+    // interleaved rows are read with 16-byte vectors, which needs every row
+    // of a chunk to start on a 16-byte boundary (as the TMA boxes do)
+    bool vec = ilv && (reinterpret_cast<uintptr_t>(fa.comp[0]) % 16 == 0) &&
+               ((mesh.off[0] - fa.shift[0]) * M * (long long)sizeof(T)) % 16 == 0;
+    for (int k = 1; k < D && vec; ++k) vec = (fa.estride[k] * (long long)sizeof(T)) % 16 == 0;
+    sep = !ilv;
+    stats_ok = vec || sep;
+  }
+  if (cfg.cull_mode == 1 && vec_ok && stats_ok) {
+    // chunks of 8 x-tiles (256 vertices) for interleaved float rows, else 4
+    const int xt = (cfg.tiles[0] <= 4 || sep || sizeof(T) == 8) ? 4 : 8;
+    const long long ldz = (D == 4) ? mesh.ld[2] : 1;
+    const long long tasks = (long long)((cfg.tiles[0] + xt - 1) / xt) * cfg.tiles[1] * ldz * lt;
+    if (sep) {
+      const unsigned sblocks = (unsigned)((tasks + kStatsWarps - 1) / kStatsWarps);
+      plane_stats_kernel<T, D, 4><<<sblocks, kStatsWarps * 32, 0, st>>>(mesh, fa, cfg);
+    } else {
+      if (tasks >= 0x7FFFFFFF) return cudaErrorInvalidValue;
+      if (xt == 4) e = launch_stats_stream<T, D, 4>(mesh, fa, cfg, (int)tasks, st);
+      else e = launch_stats_stream<T, D, 8>(mesh, fa, cfg, (int)tasks, st);
+      if (e) return e;
+    }
+    if ((e = cudaMemsetAsync(cfg.n_runs, 0, sizeof(unsigned), st))) return e;
+    tile_runs_kernel<T, D><<<(unsigned)std::max<long long>(1, (ntiles + 255) / 256), 256, 0, st>>>(mesh, cfg);
+    const size_t shm2 = Geo2<T, D, MULTI>::SMEM;
+    auto k = run_cull_kernel<T, D, MULTI, true>;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm2);
+    if (e) return e;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, shm2) != cudaSuccess || per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    // persistent CTAs; each reads the device-side run count itself
+    k<<<(unsigned)(sms * per_sm), kThreads, shm2, st>>>(maps[0], maps[1], maps[2], mesh, fa, cfg, cq, err);
+    if (launches) *launches = 3;
+    return cudaGetLastError();
+  }
+  if (launches) *launches = 1;
   if (tma) {
     auto k = extract_regular_kernel<T, D, MULTI, true>;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -701,10 +1478,25 @@ static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, cons
 template <typename T, int D>
 static cudaError_t launch_td(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                              const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
-                             int* used_tma) {
+                             int* used_tma, int* launches) {
   const bool multi = !fa.per_vertex && fa.estride[0] == D - 1;  // interleaved components
-  return multi ? launch_t<T, D, true>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
-               : launch_t<T, D, false>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
+  return multi ? launch_t<T, D, true>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches)
+               : launch_t<T, D, false>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches);
+}
+
+void tile_scratch_size(const RegularMesh& mesh, size_t* stats_bytes, unsigned* runs_cap) {
+  int TX, TY, TZ;
+  regular_tile(mesh.d, &TX, &TY, &TZ);
+  const long long tiles = ((mesh.ld[0] + TX - 1) / TX) * ((mesh.ld[1] + TY - 1) / TY) *
+                          (mesh.d == 4 ? (mesh.ld[2] + TZ - 1) / TZ : 1);
+  const long long lt = mesh.ld[mesh.d - 1];
+  // one 32-byte entry per (slice, z plane, y-tile, x-tile)
+  const long long planes = (mesh.d == 4) ? mesh.ld[2] : 1;
+  const long long ptiles = ((mesh.ld[0] + TX - 1) / TX) * ((mesh.ld[1] + TY - 1) / TY);
+  *stats_bytes = (size_t)(32 * ptiles * planes * lt);
+  // runs of surviving steps are separated by dropped ones: at most
+  // ceil(lt / 2) per tile
+  *runs_cap = (unsigned)std::min<long long>(tiles * ((lt + 1) / 2), 0x7FFFFFFF);
 }
 
 void regular_tile(int d, int* tx, int* ty, int* tz) {
@@ -721,12 +1513,12 @@ void regular_tile(int d, int* tx, int* ty, int* tz) {
 
 cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
                                    const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
-                                   cudaStream_t st, bool allow_tma, int* used_tma) {
+                                   cudaStream_t st, bool allow_tma, int* used_tma, int* launches) {
   if (mesh.d == 4)
-    return f64 ? launch_td<double, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
-               : launch_td<float, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
-  return f64 ? launch_td<double, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma)
-             : launch_td<float, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma);
+    return f64 ? launch_td<double, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches)
+               : launch_td<float, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches);
+  return f64 ? launch_td<double, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches)
+             : launch_td<float, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches);
 }
 
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,

@@ -177,6 +177,8 @@ ftk2b_status push_regular(ftk2b_stream* s) {
   cfg.refined = s->prm.precision == FTK2B_PRECISION_REFINED;
   cfg.tchunk = (int)lt;
   cfg.skip_first_spatial = T > 0;
+  cfg.cull_mode = ctx->cull_mode;  // 2 is resolved below, once the buffers exist
+  if (cfg.cull_mode != 0) S_TRY(ctx, setup_cull_scratch(ctx, rm, cfg));
   int TX, TY, TZ;
   regular_tile(d, &TX, &TY, &TZ);
   cfg.tiles[0] = (int)((rm.ld[0] + TX - 1) / TX);
@@ -207,10 +209,30 @@ ftk2b_status push_regular(ftk2b_stream* s) {
     cq.chains = (unsigned long long*)ctx->cand_chains.p;
     cq.count = counters + kCountCand;
     cq.cap = ccap;
+    if (cfg.cull_mode == 2) {
+      int mode = 0;
+      S_TRY(ctx, resolve_cull_mode(ctx, rm, fa, f64, s->layout == FTK2B_LAYOUT_MULTICOMPONENT,
+                                   [&](int md) -> cudaError_t {
+                                     ExtractConfig c = cfg;
+                                     c.cull_mode = md;
+                                     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, st);
+                                     int n = 1;
+                                     if (!e)
+                                       e = launch_extract_regular(f64, rm, fa, c, cq, counters + kCountErr, st,
+                                                                  !ctx->disable_tma, &ctx->last_used_tma, &n);
+                                     ctx->launches += (unsigned long long)n;
+                                     return e;
+                                   },
+                                   &mode));
+      cfg.cull_mode = mode;
+      S_TRY(ctx, cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, st));
+    }
+    ctx->last_cull_mode = cfg.cull_mode;
+    int nk = 1;
     S_TRY(ctx, launch_extract_regular(f64, rm, fa, cfg, cq, counters + kCountErr, st, !ctx->disable_tma,
-                                      &ctx->last_used_tma));
+                                      &ctx->last_used_tma, &nk));
     S_TRY(ctx, launch_refine_regular(f64, rm, fa, cfg, cq, sink, ctx->num_sms, st));
-    ctx->launches += 2;
+    ctx->launches += 1 + nk;
     S_TRY(ctx, cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost,
                                st));
     S_TRY(ctx, ctx->sync());

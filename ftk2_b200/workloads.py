@@ -47,6 +47,8 @@ def main():
     ap.add_argument("--refined", action="store_true")
     ap.add_argument("--tchunk", type=int, default=0, help="time steps per extraction block (0 = all)")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--cull-mode", type=int, default=2,
+                    help="0: per-vertex cull words only; 1: tile statistics first; 2: the faster, timed once (default)")
     args = ap.parse_args()
     import torch
     field, dims, m, q = make(args.case)
@@ -58,6 +60,7 @@ def main():
             ctx.set_option(api.OPT_TIME_CHUNK, args.tchunk)
         if args.no_graphs:
             ctx.set_option(api.OPT_USE_GRAPHS, 0)
+        ctx.set_option(api.OPT_CULL_MODE, args.cull_mode)
         keep: list = []
         mesh = api.regular_mesh_desc(dims)
         fd = api.field_desc(field, api.LAYOUT_MULTICOMPONENT, m, keep=keep)
@@ -67,8 +70,8 @@ def main():
             n, ne = ctx.run(mesh, fd, prm)
             x, tot, _ = ctx.last_timing()
             print(f"step {i}: {n} features {ne} edges  extract {x:.3f} ms  pipeline {tot:.3f} ms  "
-                  f"host {1e3 * (time.perf_counter() - t):.3f} ms  tma={ctx.get_option(api.INFO_LAST_TMA)}",
-                  flush=True)
+                  f"host {1e3 * (time.perf_counter() - t):.3f} ms  tma={ctx.get_option(api.INFO_LAST_TMA)}  "
+                  f"cull_mode={ctx.get_option(api.INFO_LAST_CULL_MODE)}", flush=True)
 
 
 if __name__ == "__main__":

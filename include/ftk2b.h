@@ -144,12 +144,15 @@ enum {
   FTK2B_OPT_TIME_CHUNK = 2,       /* time steps per extraction block (0 = all) */
   FTK2B_OPT_DISABLE_TMA = 3,      /* 1: stage slices with plain loads instead of TMA */
   FTK2B_OPT_USE_GRAPHS = 4,       /* 1 (default): replay the device pipeline as a CUDA graph */
-  FTK2B_OPT_BLOCKING_SYNC = 5     /* 1: wait for the device by blocking, not spinning (servers set it) */
+  FTK2B_OPT_BLOCKING_SYNC = 5,    /* 1: wait for the device by blocking, not spinning (servers set it) */
+  FTK2B_OPT_CULL_MODE = 6         /* 0: per-vertex cull words only; 1: tile statistics first; 2 (default):
+                                     the faster of the two, timed once per workload shape by the context */
 };
 ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
 /* Reads an option back, or FTK2B_INFO_LAST_TMA: 1 when the last regular-mesh
- * extraction staged its slices with TMA tensor copies. */
-enum { FTK2B_INFO_LAST_TMA = 100 };
+ * extraction staged its slices with TMA tensor copies, or
+ * FTK2B_INFO_LAST_CULL_MODE: the cull mode (0 or 1) it ran. */
+enum { FTK2B_INFO_LAST_TMA = 100, FTK2B_INFO_LAST_CULL_MODE = 101 };
 ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t* value);
 
 /* m-simplices a mesh holds for codimension m (2 or 3): the unit of work. */

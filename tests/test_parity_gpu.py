@@ -262,3 +262,68 @@ def test_graph_cache_alternating_workloads(ctx):
     for _ in range(2):
         for c, f in zip(cs, first):
             assert_identical(gpu_run(ctx, c), f)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_cull_modes_agree_with_restatement(ctx, mode):
+    # mode 0: per-vertex cull words only; mode 1: tile statistics first;
+    # mode 2: the faster of the two per workload shape, timed once
+    ctx.set_option(api.OPT_CULL_MODE, mode)
+    try:
+        for case in _medium_cases()[:4]:
+            assert_identical(gpu_run(ctx, case), oracle_run(case))
+    finally:
+        ctx.set_option(api.OPT_CULL_MODE, 2)
+
+
+def test_tile_cull_edge_fields(ctx):
+    # whole tiles that the tile statistics drop (one-signed component, values
+    # below the pivot floor) next to tiles that they must keep
+    base = S.gaussian_sum_gradient((70, 44, 38), 4, seed=21, n_blobs=16)
+    shifted = base.copy()
+    shifted[..., 0] += 5.0                      # component 0 positive everywhere
+    tiny = base * 1e-14                          # every |v| below 4e-13
+    mixed = base.copy()
+    mixed[:, :, :, :30, :] *= 1e-14              # tiny on one side only
+    mixed[:, :, :, 50:, 1] -= 3.0                # one-signed on the other
+    for name, f, q in (("shifted", shifted, 2.0 ** 20), ("tiny", tiny, 2.0 ** 20),
+                       ("mixed", mixed, 2.0 ** 20), ("tiny_q", tiny, 1e15)):
+        case = cases.Case(name, "regular", 3, cases.MULTI, np.ascontiguousarray(f), q, [70, 44, 38, 4])
+        g, o = gpu_run(ctx, case), oracle_run(case)
+        assert_identical(g, o)
+        if name in ("shifted", "tiny"):
+            assert len(o.track_id) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_tile_cull_partial_rows(ctx, dtype):
+    # sub-meshes of aligned arrays (so the tile statistics stream 16-byte
+    # vectors) whose rows end inside a vector: the tail elements are copied
+    # one by one and nothing beyond the local mesh is read
+    g = S.gaussian_sum_gradient((40, 36, 32), 5, seed=17, n_blobs=24, dtype=dtype, noise=1e-3, sigma=(3, 8))
+    for dims, off in (([35, 30, 27, 4], [4, 2, 1, 1]), ([35, 33, 31, 5], [0, 3, 1, 0]),
+                      ([21, 36, 32, 5], [16, 0, 0, 0])):
+        case = cases.Case(f"part_{dims[0]}", "regular", 3, cases.MULTI, g, 2.0 ** 20, dims, off, [40, 36, 32, 5])
+        o = oracle_run(case)
+        for mode in (0, 1):
+            ctx.set_option(api.OPT_CULL_MODE, mode)
+            try:
+                r = gpu_run(ctx, case)
+            finally:
+                ctx.set_option(api.OPT_CULL_MODE, 2)
+            assert ctx.get_option(api.INFO_LAST_TMA) == 1
+            assert_identical(r, o)
+
+
+def test_cull_autotuner_keeps_its_choice(ctx):
+    # the first extraction of a shape times both modes; later ones of the
+    # same shape run the mode it chose, with identical results
+    case = _medium_cases()[2]
+    ctx.set_option(api.OPT_CULL_MODE, 2)
+    first = gpu_run(ctx, case)
+    mode = ctx.get_option(api.INFO_LAST_CULL_MODE)
+    assert mode in (0, 1)
+    for _ in range(2):
+        assert_identical(gpu_run(ctx, case), first)
+        assert ctx.get_option(api.INFO_LAST_CULL_MODE) == mode
+    assert_identical(first, oracle_run(case))
