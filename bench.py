@@ -293,6 +293,80 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def batched_c3(ctx, steps=5, check=True):
+    """Batched workload: 256 independent float32 fields (2D sides U[32,512],
+    3D sides U[16,96], nt U[2,8], 8-64 blobs), device-resident.  Plain = one
+    extraction call per field; batched = one ftk2b_cp_run_batch call for all
+    of them.  With check, every field's batched result is compared with its
+    plain result."""
+    import numpy as np
+    import torch
+    from ftk2_b200 import api, generate
+    t0 = time.perf_counter()
+    fields = generate.c3_batch()
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    keep: list = []
+    meshes = [api.regular_mesh_desc(d) for d, _, _ in fields]
+    fds = [api.field_desc(f, api.LAYOUT_MULTICOMPONENT, m, keep=keep) for _, m, f in fields]
+    prms = [api.params(SOS_Q) for _ in fields]
+    nsimp = sum(api.simplex_count(md, len(d) - 1) for md, (d, _, _) in zip(meshes, fields))
+    nbytes = sum(f.numel() * f.element_size() for _, _, f in fields)
+    n2 = sum(1 for d, _, _ in fields if len(d) == 3)
+
+    def plain_pass():
+        nf = 0
+        for md, fd, p in zip(meshes, fds, prms):
+            nf += ctx.run(md, fd, p)[0]
+        return nf
+
+    for _ in range(2):
+        plain_pass()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(steps):
+        nf_plain = plain_pass()
+    ms_plain = (time.perf_counter() - t) * 1e3 / steps
+    for _ in range(3):
+        ctx.run_batch(meshes, fds, prms)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    xs = []
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(steps):
+        nf_batch = ctx.run_batch(meshes, fds, prms)
+        xs.append(ctx.last_timing())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_batch_wall = (time.perf_counter() - t) * 1e3 / steps
+    ms_batch = ev0.elapsed_time(ev1) / steps
+    cull_ms = statistics.mean(x[0] for x in xs)
+    out = {
+        "workload": "256 fields: 2D sides U[32,512] / 3D sides U[16,96], nt U[2,8], 8-64 blobs, float32, Q=2^20",
+        "fields": len(fields), "fields_2d": n2, "fields_3d": len(fields) - n2, "simplices": int(nsimp),
+        "input_bytes": int(nbytes), "generate_s": gen_s, "features": int(nf_batch),
+        "plain": {"ms_per_pass": ms_plain, "simplices_per_s": nsimp / (ms_plain / 1e3), "calls": len(fields)},
+        "batched": {"ms_per_pass": ms_batch, "ms_per_pass_wall": ms_batch_wall,
+                    "simplices_per_s": nsimp / (ms_batch / 1e3), "cull_ms": cull_ms,
+                    "cull_hbm_gbs": nbytes / (cull_ms / 1e3) / 1e9},
+        "speedup_batched_vs_plain": ms_plain / ms_batch,
+    }
+    if check:
+        batch = ctx.fetch_batch()
+        same = 0
+        for md, fd, p, b in zip(meshes, fds, prms, batch):
+            r = ctx.extract(md, fd, p)
+            same += int(np.array_equal(r.simplices, b.simplices) and np.array_equal(r.track_id, b.track_id)
+                        and np.array_equal(r.edges, b.edges) and np.array_equal(r.lam, b.lam)
+                        and np.array_equal(r.bary, b.bary))
+        out["identical_to_plain"] = f"{same}/{len(batch)}"
+        out["features_plain"] = int(nf_plain)
+    del fds, keep, fields
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,6 +488,8 @@ def main():
         keep.clear()
         torch.cuda.empty_cache()
         line["precision"] = precision_c4(ctx)
+        torch.cuda.empty_cache()
+        line["batched"] = batched_c3(ctx)
         torch.cuda.empty_cache()
         from ftk2_b200 import serving
         line["serve"] = serving.run(duration_s=args.serve_seconds, device=local)

@@ -39,8 +39,10 @@ PRECISION_EXACT, PRECISION_REFINED = 0, 1
 OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA, OPT_USE_GRAPHS = 1, 2, 3, 4
 INFO_LAST_TMA = 100
 INFO_LAST_CULL_MODE = 101
+INFO_LAST_BATCH_TIME_CHUNK = 102
 OPT_BLOCKING_SYNC = 5
 OPT_CULL_MODE = 6
+OPT_BATCH_TIME_CHUNK = 7
 CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
                "center"]
 
@@ -146,6 +148,11 @@ SIGNATURES = {
     "ftk2b_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStatsC)]),
     "ftk2b_server_last_error": (C.c_char_p, [C.c_void_p]),
     "ftk2b_server_destroy": (None, [C.c_void_p]),
+    "ftk2b_cp_run_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                     C.POINTER(CPParams), C.POINTER(C.c_uint64)]),
+    "ftk2b_cp_fetch_batch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_cp_extract_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                         C.POINTER(CPParams), C.POINTER(C.POINTER(CPResultC))]),
     "ftk2b_cp_features_noalloc": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(FieldDesc), C.c_double,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -382,6 +389,48 @@ class Context:
             return _result_from_c(out.contents)
         finally:
             self.lib.ftk2b_cp_result_free(out)
+
+
+    # ---- batches (ftk2b_cp_*_batch): n fields of uneven sizes in one pass
+    @staticmethod
+    def _batch_arrays(meshes, fields, prms):
+        n = len(meshes)
+        if len(fields) != n or (prms is not None and len(prms) != n):
+            raise ValueError("meshes, fields and params must have the same length")
+        ma = (MeshDesc * n)(*meshes)
+        fa = (FieldDesc * n)(*fields)
+        pa = (CPParams * n)(*prms) if prms is not None else None
+        return n, ma, fa, pa
+
+    def run_batch(self, meshes, fields, prms=None) -> int:
+        """Device pipeline of a batch; results stay on the device until
+        fetch_batch().  Returns the number of features of the whole batch."""
+        n, ma, fa, pa = self._batch_arrays(meshes, fields, prms)
+        tot = C.c_uint64()
+        self._check(self.lib.ftk2b_cp_run_batch(self.h, n, ma, fa, pa, C.byref(tot)))
+        self._batch_n = n
+        return int(tot.value)
+
+    def fetch_batch(self) -> list:
+        n = getattr(self, "_batch_n", 0)
+        outs = (C.POINTER(CPResultC) * max(n, 1))()
+        self._check(self.lib.ftk2b_cp_fetch_batch(self.h, outs))
+        try:
+            return [_result_from_c(outs[i].contents) for i in range(n)]
+        finally:
+            for i in range(n):
+                self.lib.ftk2b_cp_result_free(outs[i])
+
+    def extract_batch(self, meshes, fields, prms=None) -> list:
+        """One result per field, each identical to extract() on that field."""
+        n, ma, fa, pa = self._batch_arrays(meshes, fields, prms)
+        outs = (C.POINTER(CPResultC) * n)()
+        self._check(self.lib.ftk2b_cp_extract_batch(self.h, n, ma, fa, pa, outs))
+        try:
+            return [_result_from_c(outs[i].contents) for i in range(n)]
+        finally:
+            for i in range(n):
+                self.lib.ftk2b_cp_result_free(outs[i])
 
 
 class Stream:

@@ -155,6 +155,8 @@ extern "C" void ftk2b_ctx_destroy(ftk2b_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   ctx->drop_graphs();
   if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+  if (ctx->batch.h_tab) cudaFreeHost(ctx->batch.h_tab);
+  if (ctx->batch.h_fbase) cudaFreeHost(ctx->batch.h_fbase);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaEventDestroy(ctx->ev_x);
@@ -204,6 +206,10 @@ extern "C" ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t
       if (value < 0 || value > 2) return fail(ctx, FTK2B_INVALID_ARG, "cull mode is 0, 1 or 2");
       ctx->cull_mode = (int)value;
       return FTK2B_OK;
+    case FTK2B_OPT_BATCH_TIME_CHUNK:
+      if (value < 0 || value > 65535) return fail(ctx, FTK2B_INVALID_ARG, "batch time chunk out of range");
+      ctx->batch.tchunk = (int)value;
+      return FTK2B_OK;
     default:
       return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
@@ -217,9 +223,11 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_DISABLE_TMA: *value = ctx->disable_tma ? 1 : 0; return FTK2B_OK;
     case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
     case FTK2B_INFO_LAST_CULL_MODE: *value = ctx->last_cull_mode; return FTK2B_OK;
+    case FTK2B_INFO_LAST_BATCH_TIME_CHUNK: *value = ctx->batch.last_tchunk; return FTK2B_OK;
     case FTK2B_OPT_USE_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return FTK2B_OK;
     case FTK2B_OPT_BLOCKING_SYNC: *value = ctx->blocking_sync ? 1 : 0; return FTK2B_OK;
     case FTK2B_OPT_CULL_MODE: *value = ctx->cull_mode; return FTK2B_OK;
+    case FTK2B_OPT_BATCH_TIME_CHUNK: *value = ctx->batch.tchunk; return FTK2B_OK;
     default: return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
 }
@@ -238,6 +246,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
                             &cls, &cand_corner, &cand_chains, &edge_slots, &tstats, &runs};
   for (auto& b : extra) v.push_back(&b);
   for (DevBuf* b : ext.bufs()) v.push_back(b);
+  for (DevBuf* b : batch.bufs()) v.push_back(b);
   return v;
 }
 
@@ -321,7 +330,7 @@ static uint64_t prod(const uint64_t* d, int n) {
 
 ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int mesh_d,
                            const uint64_t* need_global_hi, const uint64_t* need_local_hi,
-                           uint64_t n_vertices, FieldAccess& fa) {
+                           uint64_t n_vertices, FieldAccess& fa, StageArena* arena) {
   memset(&fa, 0, sizeof(fa));
   if (f->dtype != FTK2B_F32 && f->dtype != FTK2B_F64)
     return fail(ctx, FTK2B_INVALID_ARG, "dtype must be FTK2B_F32 or FTK2B_F64");
@@ -371,10 +380,21 @@ ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int
     if (!f->comp[j]) return fail(ctx, FTK2B_INVALID_ARG, "component array %d is null", j);
 
   // device pointers (staging copies for host input)
+  // arena: host arrays go to consecutive 256-byte aligned slots of the
+  // caller's staging buffer; with a null base only the bytes are counted
+  auto arena_slot = [&](size_t bytes) -> unsigned char* {
+    const size_t o = arena->off;
+    arena->off += (bytes + 255) & ~(size_t)255;
+    return arena->base ? arena->base + o : nullptr;
+  };
   const void* dev[3] = {nullptr, nullptr, nullptr};
   for (int j = 0; j < narr; ++j) {
     if (f->location == FTK2B_DEVICE) {
       dev[j] = f->comp[j];
+    } else if (arena) {
+      unsigned char* dst = arena_slot(nelem * es);
+      if (dst) CUDA_TRY(ctx, cudaMemcpyAsync(dst, f->comp[j], nelem * es, cudaMemcpyHostToDevice, ctx->stream));
+      dev[j] = dst;
     } else {
       CUDA_TRY(ctx, ctx->stage[j].ensure(nelem * es));
       CUDA_TRY(ctx, cudaMemcpyAsync(ctx->stage[j].p, f->comp[j], nelem * es, cudaMemcpyHostToDevice,
@@ -410,6 +430,10 @@ ftk2b_status ftk2b::prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int
     }
     if (f->location == FTK2B_DEVICE) {
       fa.scalar = f->scalar;
+    } else if (arena) {
+      unsigned char* dst = arena_slot(sn * es);
+      if (dst) CUDA_TRY(ctx, cudaMemcpyAsync(dst, f->scalar, sn * es, cudaMemcpyHostToDevice, ctx->stream));
+      fa.scalar = dst;
     } else {
       CUDA_TRY(ctx, ctx->stage_scalar.ensure(sn * es));
       CUDA_TRY(ctx, cudaMemcpyAsync(ctx->stage_scalar.p, f->scalar, sn * es, cudaMemcpyHostToDevice,
@@ -486,7 +510,7 @@ PostBuffers ftk2b_ctx::post_buffers(unsigned cap_, unsigned edge_cap_, int key_b
 // ---------------------------------------------------------------------------
 // regular meshes
 
-static ftk2b_status build_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, RegularMesh& rm) {
+ftk2b_status ftk2b::build_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, RegularMesh& rm) {
   memset(&rm, 0, sizeof(rm));
   const int d = mesh->ndims;
   if (d != 3 && d != 4) return fail(ctx, FTK2B_UNSUPPORTED, "regular meshes need 3 or 4 dims (got %d)", d);
@@ -586,7 +610,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   const Clk::time_point p0 = Clk::now();
   for (double& x : ctx->phase_ms) x = 0;
   RegularMesh rm;
-  ftk2b_status st = build_regular(ctx, mesh, rm);
+  ftk2b_status st = ftk2b::build_regular(ctx, mesh, rm);
   if (st) return st;
   const int d = rm.d, m = d - 1;
   if (field->ncomp != m)
@@ -638,7 +662,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     sink.scalar = B.scalar;
     sink.count = B.count;
     sink.cap = cap;
-    CandidateQueue cq;
+    CandidateQueue cq{};
     cq.corner = (unsigned long long*)ctx->cand_corner.p;
     cq.chains = (unsigned long long*)ctx->cand_chains.p;
     cq.count = (unsigned*)ctx->counters.p + kCountCand;

@@ -24,7 +24,15 @@ struct DevBuf {
   void release();
 };
 
-enum { kCountFeatures = 0, kCountEdges = 1, kCountRoots = 2, kCountErr = 3, kCountCand = 4, kNumCounters = 8 };
+enum {
+  kCountFeatures = 0,
+  kCountEdges = 1,
+  kCountRoots = 2,
+  kCountErr = 3,
+  kCountCand = 4,
+  kCountItems = 5,  // batches: next cull item
+  kNumCounters = 8
+};
 
 // Everything a regular-mesh run bakes into its kernel launches; a cached CUDA
 // graph is replayed only when the next run's key is byte-identical.
@@ -77,6 +85,44 @@ struct CullTune {
 };
 constexpr size_t kMaxCullTunes = 256;
 
+// Batched extraction state of a context: device tables of the last batch,
+// its per-field bookkeeping for the fetch, and its cached graph pair.
+struct BatchFieldInfo {
+  int m, want_edges;
+  uint64_t nsimp;
+};
+struct BatchGraphKey {
+  int nf;
+  unsigned n_items, cap, ccap, edge_cap;
+  int key_bits, f64, multi;
+  const void* h_fbase;
+};
+struct BatchCtx {
+  DevBuf fields, meshes, kb, fbase, cand_field, stage;
+  void* h_tab = nullptr;          // pinned staging of the tables
+  size_t h_tab_bytes = 0;
+  unsigned* h_fbase = nullptr;    // pinned: first feature of every field
+  size_t h_fbase_n = 0;
+  unsigned cap_hint = 0, ccap_hint = 0;
+  int tchunk = 0;                 // FTK2B_OPT_BATCH_TIME_CHUNK (0: tuned per batch shape)
+  int last_tchunk = 0;            // the time chunk the last batch ran (0xFFFF: whole range)
+  std::vector<std::pair<uint64_t, int>> tunes;  // batch shape hash -> time chunk
+  int nf = 0;
+  uint64_t n = 0, ne = 0;
+  double device_ms = 0;
+  std::vector<BatchFieldInfo> info;
+  std::vector<unsigned> fb;       // fbase of the last batch (nf + 1)
+  BatchGraphKey gkey;
+  unsigned long long ggen = 0, glaunches = 0;
+  cudaGraphExec_t g1 = nullptr, g2 = nullptr;
+  void drop_graph() {
+    if (g1) cudaGraphExecDestroy(g1);
+    if (g2) cudaGraphExecDestroy(g2);
+    g1 = g2 = nullptr;
+  }
+  std::vector<DevBuf*> bufs() { return {&fields, &meshes, &kb, &fbase, &cand_field, &stage}; }
+};
+
 struct LastRun {
   int kind = 0, m = 0;
   uint64_t n = 0, ne = 0, n_roots = 0, n_simplices = 0;
@@ -110,6 +156,7 @@ struct ftk2b_ctx {
   ftk2b::DevBuf tstats, runs;  // cull mode 1 scratch (tile statistics, run list + count)
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::ExtCache ext;
+  ftk2b::BatchCtx batch;
   ftk2b::LastRun last;
   // CUDA graph of the last regular-mesh pipeline
   bool use_graphs = true;
@@ -119,6 +166,7 @@ struct ftk2b_ctx {
   std::vector<ftk2b::GraphEntry> graphs;
   unsigned long long graph_clock = 0;
   void drop_graphs() {
+    batch.drop_graph();
     for (auto& g : graphs) {
       if (g.g1) cudaGraphExecDestroy(g.g1);
       if (g.g2) cudaGraphExecDestroy(g.g2);
@@ -160,9 +208,19 @@ struct ftk2b_ctx {
 
 namespace ftk2b {
 
+// Staging of host arrays into one device buffer: consecutive 256-byte
+// aligned slots from `off`; a null base only counts the bytes.
+struct StageArena {
+  unsigned char* base;
+  size_t off;
+};
+// Validates a field descriptor and fills fa (device pointers; host arrays are
+// copied to the context's staging buffers, or into the arena when given).
 ftk2b_status prepare_field(ftk2b_ctx* ctx, const ftk2b_field_desc* f, int mesh_d,
                            const uint64_t* need_global_hi, const uint64_t* need_local_hi,
-                           uint64_t n_vertices, FieldAccess& fa);
+                           uint64_t n_vertices, FieldAccess& fa, StageArena* arena = nullptr);
+// RegularSimplicialMesh(local, offset, global) of a descriptor, validated.
+ftk2b_status build_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, RegularMesh& rm);
 ftk2b_status ensure_feature_buffers(ftk2b_ctx* ctx, unsigned cap, unsigned edge_cap, int m);
 
 // Sizes the tile-statistics scratch of cull mode 1 for this mesh and points

@@ -61,6 +61,8 @@ struct CandidateQueue {
   unsigned long long* chains;  // bit c: chain c still needs the exact test
   unsigned* count;             // number queued (may exceed cap: overflow)
   unsigned cap;
+  unsigned* field;             // batches: field index of every candidate (null otherwise)
+  unsigned field_id;           // the index written by the current tile
 };
 
 struct ExtractConfig {

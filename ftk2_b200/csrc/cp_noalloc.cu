@@ -144,7 +144,7 @@ extern "C" ftk2b_status ftk2b_cp_features_noalloc(const ftk2b_mesh_desc* mesh,
 
   unsigned long long* sw = static_cast<unsigned long long*>(scratch);
   unsigned* counters = reinterpret_cast<unsigned*>(sw + kOffCounters);  // [0] candidates, [1] error
-  CandidateQueue cq;
+  CandidateQueue cq{};
   cq.corner = sw + kOffCorner;
   cq.chains = sw + kOffChains;
   cq.count = counters;

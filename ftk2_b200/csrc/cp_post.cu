@@ -13,6 +13,7 @@
 //   3. trajectories: lock-free union-find that always hooks the larger root
 //      under the smaller one, so every component's root is its smallest
 //      canonical id = the reference's track_id (engine.hpp:46-74, 965-983).
+#include "cp_batch.h"
 #include "cp_post.h"
 #include "cp_kuhn.cuh"
 #include "cp_uf.cuh"
@@ -233,7 +234,8 @@ constexpr int kEdgeSlots = 8;  // a codimension-1 simplex has 2 cofaces with <= 
 // Index of the face of top cell (cc, cm) without vertex r, or -1.
 __device__ __forceinline__ long long face_index(const RegularMesh& mesh, int nch,
                                                 const unsigned long long* keys, unsigned n,
-                                                const long long cc[4], const int cm[5], int r) {
+                                                const long long cc[4], const int cm[5], int r,
+                                                unsigned long long kbase = 0) {
   const int d = mesh.d;
   const int basem = (r == 0) ? cm[1] : 0;
   int rel[4];
@@ -244,13 +246,53 @@ __device__ __forceinline__ long long face_index(const RegularMesh& mesh, int nch
   }
   unsigned long long vid = 0;
   for (int k = 0; k < d; ++k) vid += (unsigned long long)(cc[k] + ((basem >> k) & 1)) * mesh.gstride[k];
-  return find_key(keys, n, vid * (unsigned long long)nch + (unsigned long long)chain_rank(d, rel));
+  return find_key(keys, n, kbase + vid * (unsigned long long)nch + (unsigned long long)chain_rank(d, rel));
 }
 
 // One warp per feature: lanes look up the faces of both cofaces in parallel;
 // when the feature is the smallest active face of a cell it writes the star
 // edges to its other active faces into padded slots (ascending), and its
-// edge count.
+// edge count.  Feature i has key kbase + local_key; keys of its mesh's faces
+// are searched in the same key space.
+__device__ __forceinline__ void edges_of_feature(const RegularMesh& mesh, int nch,
+                                                 const unsigned long long* __restrict__ keys, unsigned n, unsigned i,
+                                                 unsigned long long local_key, unsigned long long kbase, int lane,
+                                                 unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+  const int d = mesh.d;
+  Decoded dc;
+  decode_key(mesh, nch, local_key, dc);
+  long long cc[2][4];
+  int cm[2][5];
+  const int nc = top_cells(mesh, dc, cc, cm);
+  long long idx = -1;
+  const int q = lane / (d + 1), r = lane % (d + 1);
+  if (lane < nc * (d + 1)) idx = face_index(mesh, nch, keys, n, cc[q], cm[q], r, kbase);
+  const unsigned act = __ballot_sync(0xFFFFFFFFu, idx >= 0);
+  unsigned others[kEdgeSlots];
+  int no = 0;
+  for (int qq = 0; qq < nc; ++qq) {
+    const unsigned cellmask = ((1u << (d + 1)) - 1u) << (qq * (d + 1));
+    const unsigned a = act & cellmask;
+    const unsigned v = ((a >> lane) & 1u) ? (unsigned)idx : 0xFFFFFFFFu;
+    const unsigned mn = __reduce_min_sync(0xFFFFFFFFu, v);
+    if (__popc(a) < 2 || mn != i) continue;
+    for (unsigned bits = a; bits; bits &= bits - 1) {
+      const unsigned val = __shfl_sync(0xFFFFFFFFu, (unsigned)idx, __ffs(bits) - 1);
+      if (val != i && no < kEdgeSlots) others[no++] = val;
+    }
+  }
+  if (lane == 0) {
+    for (int a2 = 1; a2 < no; ++a2)
+      for (int b2 = a2; b2 > 0 && others[b2 - 1] > others[b2]; --b2) {
+        const unsigned t = others[b2];
+        others[b2] = others[b2 - 1];
+        others[b2 - 1] = t;
+      }
+    cnt[i] = no;
+    for (int k = 0; k < no; ++k) slots[(size_t)i * kEdgeSlots + k] = others[k];
+  }
+}
+
 __global__ void edges_regular_warp_kernel(RegularMesh mesh, int nch,
                                           const unsigned long long* __restrict__ keys,
                                           const unsigned* n_ptr, unsigned cap,
@@ -259,40 +301,32 @@ __global__ void edges_regular_warp_kernel(RegularMesh mesh, int nch,
   const int lane = threadIdx.x & 31;
   const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned nw = (gridDim.x * blockDim.x) >> 5;
-  const int d = mesh.d;
+  for (unsigned i = gw; i < n; i += nw) edges_of_feature(mesh, nch, keys, n, i, keys[i], 0ull, lane, cnt, slots);
+}
+
+// Field of a key of a batch: the last f with kb[f] <= key (kb ascending, nf entries).
+__device__ __forceinline__ unsigned batch_field_of(const unsigned long long* __restrict__ kb, int nf,
+                                                   unsigned long long key) {
+  unsigned lo = 0, hi = (unsigned)nf;
+  while (hi - lo > 1) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (kb[mid] <= key) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const unsigned long long* __restrict__ kb,
+                                        int nf, const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
+                                        unsigned cap, unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+  const unsigned n = min(*n_ptr, cap);
+  const int lane = threadIdx.x & 31;
+  const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
   for (unsigned i = gw; i < n; i += nw) {
-    Decoded dc;
-    decode_key(mesh, nch, keys[i], dc);
-    long long cc[2][4];
-    int cm[2][5];
-    const int nc = top_cells(mesh, dc, cc, cm);
-    long long idx = -1;
-    const int q = lane / (d + 1), r = lane % (d + 1);
-    if (lane < nc * (d + 1)) idx = face_index(mesh, nch, keys, n, cc[q], cm[q], r);
-    const unsigned act = __ballot_sync(0xFFFFFFFFu, idx >= 0);
-    unsigned others[kEdgeSlots];
-    int no = 0;
-    for (int qq = 0; qq < nc; ++qq) {
-      const unsigned cellmask = ((1u << (d + 1)) - 1u) << (qq * (d + 1));
-      const unsigned a = act & cellmask;
-      const unsigned v = ((a >> lane) & 1u) ? (unsigned)idx : 0xFFFFFFFFu;
-      const unsigned mn = __reduce_min_sync(0xFFFFFFFFu, v);
-      if (__popc(a) < 2 || mn != i) continue;
-      for (unsigned bits = a; bits; bits &= bits - 1) {
-        const unsigned val = __shfl_sync(0xFFFFFFFFu, (unsigned)idx, __ffs(bits) - 1);
-        if (val != i && no < kEdgeSlots) others[no++] = val;
-      }
-    }
-    if (lane == 0) {
-      for (int a2 = 1; a2 < no; ++a2)
-        for (int b2 = a2; b2 > 0 && others[b2 - 1] > others[b2]; --b2) {
-          const unsigned t = others[b2];
-          others[b2] = others[b2 - 1];
-          others[b2 - 1] = t;
-        }
-      cnt[i] = no;
-      for (int k = 0; k < no; ++k) slots[(size_t)i * kEdgeSlots + k] = others[k];
-    }
+    const unsigned long long key = keys[i];
+    const unsigned f = batch_field_of(kb, nf, key);
+    edges_of_feature(fm[f].mesh, fm[f].nch, keys, n, i, key - kb[f], kb[f], lane, cnt, slots);
   }
 }
 
@@ -383,23 +417,61 @@ __global__ void uf_label_kernel(unsigned* parent, const unsigned* n_ptr, unsigne
 // ---------------------------------------------------------------------------
 // output expansion: vertex ids and float barycentrics
 
+// Vertex ids (and float barycentrics) of feature i with local key key, into
+// rows of `stride` entries.
+__device__ __forceinline__ void expand_feature(const RegularMesh& mesh, int nch, unsigned long long key, unsigned i,
+                                               int stride, const float* __restrict__ bary4,
+                                               unsigned long long* __restrict__ simplices, float* __restrict__ bary) {
+  const int m = mesh.d - 1;
+  Decoded dc;
+  decode_key(mesh, nch, key, dc);
+  for (int v = 0; v <= m; ++v) {
+    unsigned long long vid = 0;
+    for (int k = 0; k < mesh.d; ++k)
+      vid += (unsigned long long)(dc.g[k] + ((dc.mk[v] >> k) & 1)) * mesh.gstride[k];
+    simplices[(size_t)i * stride + v] = vid;
+    if (bary) bary[(size_t)i * stride + v] = bary4[4 * (size_t)i + v];
+  }
+}
+
 __global__ void expand_regular_kernel(RegularMesh mesh, int nch, const unsigned long long* __restrict__ keys,
                                       const unsigned* n_ptr, unsigned cap,
                                       const float* __restrict__ bary4,
                                       unsigned long long* __restrict__ simplices,
                                       float* __restrict__ bary) {
   const unsigned n = min(*n_ptr, cap);
-  const int m = mesh.d - 1;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    expand_feature(mesh, nch, keys[i], i, mesh.d, bary4, simplices, bary);
+}
+
+// Batches: rows of 4 entries whatever the field's dimension.
+__global__ void expand_batch_kernel(const BatchMesh* __restrict__ fm, const unsigned long long* __restrict__ kb, int nf,
+                                    const unsigned long long* __restrict__ keys, const unsigned* n_ptr, unsigned cap,
+                                    const float* __restrict__ bary4, unsigned long long* __restrict__ simplices,
+                                    float* __restrict__ bary) {
+  const unsigned n = min(*n_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    Decoded dc;
-    decode_key(mesh, nch, keys[i], dc);
-    for (int v = 0; v <= m; ++v) {
-      unsigned long long vid = 0;
-      for (int k = 0; k < mesh.d; ++k)
-        vid += (unsigned long long)(dc.g[k] + ((dc.mk[v] >> k) & 1)) * mesh.gstride[k];
-      simplices[(size_t)i * (m + 1) + v] = vid;
-      if (bary) bary[(size_t)i * (m + 1) + v] = bary4[4 * (size_t)i + v];
+    const unsigned long long key = keys[i];
+    const unsigned f = batch_field_of(kb, nf, key);
+    expand_feature(fm[f].mesh, fm[f].nch, key - kb[f], i, 4, bary4, simplices, bary);
+  }
+}
+
+// fbase[f] = index of the first feature of field f in canonical order
+// (f = 0 .. nf; kb[nf] is the end of the key space)
+__global__ void batch_bounds_kernel(const unsigned long long* __restrict__ kb, int nf,
+                                    const unsigned long long* __restrict__ keys, const unsigned* n_ptr, unsigned cap,
+                                    unsigned* __restrict__ fbase) {
+  const unsigned n = min(*n_ptr, cap);
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f <= nf; f += gridDim.x * blockDim.x) {
+    const unsigned long long k = kb[f];
+    unsigned lo = 0, hi = n;
+    while (lo < hi) {
+      const unsigned mid = (lo + hi) >> 1;
+      if (keys[mid] < k) lo = mid + 1;
+      else hi = mid;
     }
+    fbase[f] = lo;
   }
 }
 
@@ -535,4 +607,28 @@ cudaError_t launch_expand_regular(const RegularMesh& mesh, int nch, const unsign
   return cudaGetLastError();
 }
 
+
+cudaError_t launch_post_batch(const BatchMesh* fm, const unsigned long long* kb, int nf, const PostBuffers& B,
+                              unsigned* fbase, cudaStream_t st, unsigned long long* launches) {
+  const unsigned cap = B.cap;
+  const int g = grid_for(cap, 256, 4096);
+  iota_kernel<<<g, 256, 0, st>>>(B.perm0, B.count, cap);
+  const bool alt = radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits, B.hist, B.sort_grid,
+                              st, launches);
+  const unsigned long long* skey = alt ? B.key_alt : B.key;
+  const unsigned* perm = alt ? B.perm1 : B.perm0;
+  gather_kernel<<<g, 256, 0, st>>>(B.count, cap, perm, B.lam, B.scalar, B.bary4, B.lam_sorted, B.scalar_sorted,
+                                   B.bary4_sorted);
+  expand_batch_kernel<<<g, 256, 0, st>>>(fm, kb, nf, skey, B.count, cap, B.bary4_sorted, B.simplices, B.bary);
+  batch_bounds_kernel<<<(nf + 256) / 256, 256, 0, st>>>(kb, nf, skey, B.count, cap, fbase);
+  edges_batch_warp_kernel<<<grid_for(cap, 8, 8192), 256, 0, st>>>(fm, kb, nf, skey, B.count, cap, B.edge_cnt,
+                                                                 B.edge_slots);
+  scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count, nullptr);
+  edges_compact_kernel<<<g, 256, 0, st>>>(B.count, cap, B.edge_cnt, B.n_edges, B.edge_slots, B.edges, B.edge_cap);
+  uf_init_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap);
+  uf_hook_kernel<<<grid_for(B.edge_cap, 256, 4096), 256, 0, st>>>(B.parent, B.edges, B.n_edges, B.edge_cap, B.err);
+  uf_label_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap, B.track, B.n_roots);
+  *launches += 11;  // iota, gather, expand, bounds, edges, scan, compact, uf init, hook, label (+ sort passes)
+  return cudaGetLastError();
+}
 }  // namespace ftk2b

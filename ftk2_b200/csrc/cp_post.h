@@ -64,6 +64,13 @@ cudaError_t launch_window_edges_regular(const RegularMesh& mesh, int nch, const 
 cudaError_t launch_expand_regular(const RegularMesh& mesh, int nch, const unsigned long long* keys,
                                   const unsigned* n_ptr, unsigned cap, const float* bary4,
                                   unsigned long long* simplices, float* bary, cudaStream_t st);
+struct BatchMesh;
+// Post-extraction stages of a batch: canonical order over the batch's key
+// space (kb[f] = first key of field f, ascending, kb[nf] = end), star edges
+// and trajectories (which never cross fields), vertex ids in rows of 4, and
+// fbase[f] = first feature of field f (f = 0 .. nf).
+cudaError_t launch_post_batch(const BatchMesh* fm, const unsigned long long* kb, int nf, const PostBuffers& B,
+                              unsigned* fbase, cudaStream_t st, unsigned long long* launches);
 bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, unsigned* v1,
                 const unsigned* n_ptr, unsigned cap, int bits, unsigned* hist, int grid,
                 cudaStream_t st, unsigned long long* launches);

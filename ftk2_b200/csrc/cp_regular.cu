@@ -25,6 +25,7 @@
 #include <mutex>
 #include <type_traits>
 
+#include "cp_batch.h"
 #include "cp_cull.cuh"
 #include "cp_device.cuh"
 #include "cp_field.cuh"
@@ -90,6 +91,35 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Per-thread asynchronous global -> shared copies (each thread later reads
+// back only what it copied itself, after cp.async.wait_group).
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_small(void* dst, const void* src) {
+  static_assert(N == 4 || N == 8, "cp.async.ca copies 4, 8 or 16 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "n"(N)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// element copy with zero fill: src_bytes = 0 writes zeros without reading
+template <int N>
+__device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, unsigned src_bytes) {
+  static_assert(N == 4 || N == 8, "element copies of 4 or 8 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "n"(N), "r"(src_bytes)
+               : "memory");
+}
+
 // ---------------------------------------------------------------------------
 
 template <int D> struct Tile;
@@ -144,12 +174,19 @@ __device__ __forceinline__ unsigned long long pack_corner(long long x, long long
 
 // Stage 1: stream the field through shared memory, cull hypercubes, queue
 // the survivors with the chains whose own vertices survive the cull.
+//
+// cull_tile marches one tile over the corner time steps of one chunk.  The
+// block's two slice buffers, word slots, mbarriers and band table are the
+// caller's; ph[b] counts the phases mbarrier b has completed before this call
+// (so that a persistent block can march many tiles) and is advanced past the
+// copies this call waits for.  Returns false when a bounded TMA wait gave up
+// (the error flag is set).
 template <typename T, int D, bool MULTI, bool TMA>
-__global__ void __launch_bounds__(kThreads, 2)
-    extract_regular_kernel(const __grid_constant__ CUtensorMap map0,
-                           const __grid_constant__ CUtensorMap map1,
-                           const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa,
-                           ExtractConfig cfg, CandidateQueue cq, unsigned* err) {
+__device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtensorMap* map1,
+                                          const CUtensorMap* map2, const RegularMesh& mesh, const FieldAccess& fa,
+                                          const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
+                                          int tile, int chunk, unsigned char* smem, unsigned long long* bar,
+                                          const unsigned* band_tbl, unsigned ph[2]) {
   using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
   constexpr int TX = G::TX, TY = G::TY, TZ = G::TZ;
@@ -158,17 +195,12 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr int HW = sizeof(T) / 4;   // the high 32-bit word of an element is its last
   static_assert(D == 3 ? kWarps * kRows == TY : kWarps == TY * (TZ / kRows),
                 "every corner row of the tile belongs to exactly one warp");
-
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ unsigned long long bar[2];
-  __shared__ unsigned band_tbl[kBandTable];
   unsigned* const Wb = reinterpret_cast<unsigned*>(smem + G::WORDS);
-
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
 
   // tile origin (local coordinates)
-  int tix = blockIdx.x;
+  int tix = tile;
   const int x0 = (tix % cfg.tiles[0]) * TX;
   tix /= cfg.tiles[0];
   const int y0 = (tix % cfg.tiles[1]) * TY;
@@ -177,7 +209,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int ldx = (int)mesh.ld[0], ldy = (int)mesh.ld[1], ldz = (D == 4) ? (int)mesh.ld[2] : 1;
   // time in int: local dims are below 2^16
   const int lt = (int)mesh.ld[D - 1];
-  const int t0 = (int)blockIdx.y * cfg.tchunk;
+  const int t0 = chunk * cfg.tchunk;
   const int t1 = min(t0 + cfg.tchunk, lt);
   const int s_end = min(t1, lt - 1);  // last vertex slice this block reads
   // array coordinates of local (0,0,0,0): global for multicomponent arrays,
@@ -201,7 +233,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
     vvalid |= (in ? 1u : 0u) << u;
   }
-  fill_band_table<T>(band_tbl, tid, kThreads);  // visible after the first barrier below
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
@@ -213,10 +244,10 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int cx = (x0 + aoff[0]) * (MULTI ? M : 1);
         const int cy = y0 + aoff[1];
         if constexpr (MULTI) {
-          if constexpr (D == 4) tma_load_4d(dst0, &map0, cx, cy, z0 + aoff[2], tcoord(s), &bar[buf]);
-          else tma_load_3d(dst0, &map0, cx, cy, tcoord(s), &bar[buf]);
+          if constexpr (D == 4) tma_load_4d(dst0, map0, cx, cy, z0 + aoff[2], tcoord(s), &bar[buf]);
+          else tma_load_3d(dst0, map0, cx, cy, tcoord(s), &bar[buf]);
         } else {
-          const CUtensorMap* maps[3] = {&map0, &map1, &map2};
+          const CUtensorMap* maps[3] = {map0, map1, map2};
 #pragma unroll
           for (int j = 0; j < M; ++j) {
             if constexpr (D == 4)
@@ -227,7 +258,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
       }
     } else {
-      // plain cooperative loads into the same layout (zero outside the array)
+      // per-thread asynchronous element copies into the same layout (zeros
+      // outside the array), one commit group per slice
       T* dst = reinterpret_cast<T*>(dst0);
       constexpr int NPER = G::VXBOX * VY * VZ;
       for (int e = tid; e < NPER * M; e += kThreads) {
@@ -254,18 +286,27 @@ __global__ void __launch_bounds__(kThreads, 2)
             o += a * fa.estride[k];
           }
         }
-        T v = T(0);
-        if (in) v = static_cast<const T*>(fa.comp[j])[o];
-        if (MULTI) dst[((vz * VY + vy) * G::VXBOX + vx) * M + j] = v;
-        else dst[j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX + vx] = v;
+        const T* src = static_cast<const T*>(fa.comp[j]) + (in ? o : 0);
+        T* d = MULTI ? &dst[((vz * VY + vy) * G::VXBOX + vx) * M + j]
+                     : &dst[j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX + vx];
+        cp_async_zfill<sizeof(T)>(d, src, in ? (unsigned)sizeof(T) : 0u);
       }
+      cp_async_commit();
     }
   };
   // every thread waits for the slice's TMA phase itself (try_wait suspends
   // in hardware); returns false when the bounded wait gave up
   auto wait = [&](int s, int buf) -> bool {
-    if constexpr (TMA) return mbar_wait(&bar[buf], (unsigned)(((s - t0) >> 1) & 1));
-    else return true;
+    if constexpr (TMA) {
+      return mbar_wait(&bar[buf], (ph[buf] + (unsigned)((s - t0) >> 1)) & 1u);
+    } else {
+      // slice s + 1 (when it exists) was issued after s: one group may stay
+      // in flight; then every thread's copies of slice s are visible
+      if (s + 1 <= s_end) cp_async_wait<1>();
+      else cp_async_wait<0>();
+      __syncthreads();
+      return true;
+    }
   };
   auto words = [&](int buf, int slot) {
     const unsigned* r = reinterpret_cast<const unsigned*>(smem + buf * G::BYTES) + (HW - 1);
@@ -280,32 +321,22 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
   };
 
-  if constexpr (TMA) {
-    if (tid == 0) {
-      mbar_init(&bar[0], 1);
-      mbar_init(&bar[1], 1);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    issue(t0, 0);
-    if (t0 + 1 <= s_end) issue(t0 + 1, 1);
-  } else {
-    __syncthreads();
-    issue(t0, 0);
-    __syncthreads();
-  }
+  // the previous tile of a persistent block is done with every buffer
+  __syncthreads();
+  issue(t0, 0);
+  if (t0 + 1 <= s_end) issue(t0 + 1, 1);
   int slot_a = 0;  // word slot of slice ct
   {
     const bool ok = wait(t0, 0);
     if (ok) words(0, slot_a);
     if (__syncthreads_or(!ok)) {
       // give the other copy in flight a bounded chance to land before leaving
-      if (TMA && t0 + 1 <= s_end) mbar_wait(&bar[1], 0);
+      if (TMA && t0 + 1 <= s_end) mbar_wait(&bar[1], ph[1] & 1u);
       if (tid == 0) atomicOr(err, 2u);
-      return;
+      return false;
     }
   }
-  if (TMA && t0 + 2 <= s_end) issue(t0 + 2, 0);
+  if (t0 + 2 <= s_end) issue(t0 + 2, 0);
 
   // corner validity per (lane, row) does not change along time
   const int cyw = (D == 4) ? warp % TY : warp * kRows;
@@ -325,10 +356,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     bool ok = true;
     if (s <= s_end) {
       const int buf = (s - t0) & 1;
-      if (!TMA) {
-        issue(s, buf);
-        __syncthreads();
-      }
       ok = wait(s, buf);
       if (ok) words(buf, slot_b);
     } else {
@@ -337,11 +364,12 @@ __global__ void __launch_bounds__(kThreads, 2)
     // the one block barrier of the step: words of slice s are visible, its
     // raw buffer is free, and every warp has finished culling step ct - 1
     if (__syncthreads_or(!ok)) {
-      if (TMA && s + 1 <= s_end) mbar_wait(&bar[((s - t0) & 1) ^ 1], (unsigned)(((s + 1 - t0) >> 1) & 1));
+      const int ob = ((s - t0) & 1) ^ 1;
+      if (TMA && s + 1 <= s_end) mbar_wait(&bar[ob], (ph[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
       if (tid == 0) atomicOr(err, 2u);
-      return;
+      return false;
     }
-    if (TMA && s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
+    if (s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
 
     // ---- hypercube cull: lanes along x, kRows corner rows per warp
     const unsigned* A = Wb + slot_a * VSP;
@@ -383,6 +411,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (D == 4 && l2 + 1 < ldz) vmask |= 4;
             if (ct + 1 < lt) vmask |= TBIT;
             cq.corner[idx] = pack_corner(l0, l1, (D == 4) ? l2 : 0, ct);
+            if (cq.field) cq.field[idx] = cq.field_id;
             unsigned long long ch = c_chains_by_vmask[D - 3][vmask];
             // a stream's window starts one slice before the new timestep: the
             // purely spatial simplices of that slice were counted already
@@ -394,6 +423,33 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     slot_a = slot_b;
   }
+  if constexpr (TMA) {
+    // slices t0 .. s_end alternate buffers 0, 1, 0, ...
+    const unsigned nsl = (unsigned)(s_end - t0 + 1);
+    ph[0] += (nsl + 1) >> 1;
+    ph[1] += nsl >> 1;
+  }
+  return true;
+}
+
+template <typename T, int D, bool MULTI, bool TMA>
+__global__ void __launch_bounds__(kThreads, 2)
+    extract_regular_kernel(const __grid_constant__ CUtensorMap map0,
+                           const __grid_constant__ CUtensorMap map1,
+                           const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa,
+                           ExtractConfig cfg, CandidateQueue cq, unsigned* err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned long long bar[2];
+  __shared__ unsigned band_tbl[kBandTable];
+  fill_band_table<T>(band_tbl, threadIdx.x, kThreads);  // visible after the tile's first barrier
+  if (TMA && threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  unsigned ph[2] = {0u, 0u};
+  cull_tile<T, D, MULTI, TMA>(&map0, &map1, &map2, mesh, fa, cfg, cq, err, (int)blockIdx.x, (int)blockIdx.y, smem,
+                              bar, band_tbl, ph);
 }
 
 // ---------------------------------------------------------------------------
@@ -534,32 +590,12 @@ __global__ void __launch_bounds__(kStatsWarps * 32, 2)
   }
 }
 
-// Per-thread asynchronous global -> shared copies (each thread later reads
-// back only what it copied itself, after cp.async.wait_group).
-__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_small(void* dst, const void* src) {
-  static_assert(N == 4 || N == 8, "cp.async.ca copies 4, 8 or 16 bytes");
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src), "n"(N)
-               : "memory");
-}
 // high 32-bit word of element u of a 16-byte vector (little-endian)
 template <typename T>
 __device__ __forceinline__ unsigned vec_hi_word(const uint4& w, int u) {
   if (sizeof(T) == 8) return u == 0 ? w.y : w.w;
   return u == 0 ? w.x : u == 1 ? w.y : u == 2 ? w.z : w.w;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // The same statistics for interleaved components whose rows start on 16-byte
 // boundaries, streamed: persistent warps walk the tasks (warp w takes tasks
 // w, w + W, ... for W warps in the grid) as one continuous sequence of rows,
@@ -1089,6 +1125,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1)
               unsigned long long ch = c_chains_by_vmask[D - 3][vmask];
               if (cfg.skip_first_spatial && c == 0) ch &= c_time_chains[D - 3];
               cq.corner[idx] = pack_corner(l0, l1, (D == 4) ? l2 : 0, c);
+              if (cq.field) cq.field[idx] = cq.field_id;
               cq.chains[idx] = ch;
             }
           }
@@ -1105,144 +1142,245 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1)
 // compacted by warp ballot.
 constexpr int kRefineWarps = 8;
 
+// One candidate hypercube (packed local corner pc, chains to test) of a
+// regular mesh, by one warp; cube is the warp's 2^D * M staging slots.
+// Accepted simplices get key key_base + corner vertex id * chains + rank.
+template <typename T, int D>
+__device__ __forceinline__ void refine_candidate(const RegularMesh& mesh, const FieldAccess& fa,
+                                                 const ExtractConfig& cfg, unsigned long long pc,
+                                                 unsigned long long chains, const FeatureSink& sink,
+                                                 unsigned long long key_base, T* cube, const unsigned* band_tbl,
+                                                 int lane) {
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;
+  const ChainTable& CT = c_chains[D - 3];
+  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+  long long g0[4];
+  unsigned long long vid0 = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    // D = 3: the time coordinate is the third axis
+    const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+    g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+    if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
+  }
+  // gather the hypercube's vertex values (only vertices inside the mesh)
+  for (int e = lane; e < NV * M; e += 32) {
+    const int v = e / M, j = e % M;
+    long long g[4];
+    unsigned long long vid = 0;
+    bool in = true;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
+      if (k < D) {
+        in &= g[k] - mesh.off[k] < mesh.ld[k];
+        vid += (unsigned long long)g[k] * mesh.gstride[k];
+      }
+    }
+    cube[v * M + j] = in ? field_at<T>(fa, j, g, D, vid) : T(0);
+  }
+  __syncwarp();
+  // cull words of the hypercube's vertices (absent outside the mesh)
+  unsigned vw = kAbsent;
+  if (lane < NV) {
+    unsigned h[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) h[j] = hi_word<T>(cube[lane * M + j]);
+    bool in = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
+    vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
+  }
+  for (int base = 0; base < CT.n; base += 32) {
+    const int ch = base + lane;
+    bool acc = false;
+    double lam_out[4] = {0, 0, 0, 0};
+    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+    float sc_out = 0.f;
+    int mk[M + 1];
+    mk[0] = 0;
+    bool live = ch < CT.n && ((chains >> ch) & 1ull);
+#pragma unroll
+    for (int i = 0; i < M; ++i) mk[i + 1] = live ? CT.mask[ch][i] : 0;
+    {
+      unsigned wacc = kAbsent;
+#pragma unroll
+      for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, mk[i]);
+      live = live && !word_culled(wacc);
+    }
+    if (live) {
+      T vals[M + 1][M];
+#pragma unroll
+      for (int i = 0; i <= M; ++i)
+#pragma unroll
+        for (int j = 0; j < M; ++j) vals[i][j] = cube[mk[i] * M + j];
+      bool inside;
+      if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
+      else inside = sos_inside3<T>(vals, cfg.Q);
+      if (inside) {
+        T lam[M + 1];
+        if (solve_exact<M, T>(vals, lam)) {
+          acc = true;
+#pragma unroll
+          for (int i = 0; i <= M; ++i) {
+            lam_out[i] = (double)lam[i];
+            bary_out[i] = (float)lam[i];
+          }
+          if (fa.has_scalar) {
+            using F = fp<T>;
+            T sc = T(0);
+#pragma unroll
+            for (int i = 0; i <= M; ++i) {
+              long long gv[4];
+              unsigned long long vid = 0;
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                gv[k] = (k < D) ? g0[k] + ((mk[i] >> k) & 1) : 0;
+                if (k < D) vid += (unsigned long long)gv[k] * mesh.gstride[k];
+              }
+              sc = F::add(sc, F::mul(lam[i], scalar_at<T>(fa, gv, D, vid)));
+            }
+            sc_out = (float)sc;
+          }
+          if (cfg.refined) {
+            double rr[M + 1];
+            if (solve_refined<M, T>(vals, rr))
+#pragma unroll
+              for (int i = 0; i <= M; ++i) lam_out[i] = rr[i];
+          }
+        }
+      }
+    }
+    const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
+    if (ball) {
+      unsigned int basei = 0;
+      const int leader = __ffs(ball) - 1;
+      if (lane == leader) basei = atomicAdd(sink.count, (unsigned)__popc(ball));
+      basei = __shfl_sync(0xFFFFFFFFu, basei, leader);
+      if (acc) {
+        const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
+        if (idx < sink.cap) {
+          sink.key[idx] = key_base + vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            sink.lam[4 * (size_t)idx + i] = lam_out[i];
+            sink.bary4[4 * (size_t)idx + i] = bary_out[i];
+          }
+          sink.scalar[idx] = sc_out;
+        }
+      }
+    }
+  }
+  __syncwarp();
+}
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kRefineWarps * 32, 2)
     refine_regular_kernel(RegularMesh mesh, FieldAccess fa, ExtractConfig cfg, CandidateQueue cq,
                           FeatureSink sink) {
   constexpr int M = D - 1;
   constexpr int NV = 1 << D;
-  __shared__ T cube[kRefineWarps][NV][M];
+  __shared__ T cube[kRefineWarps][NV * M];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   __syncthreads();
-  const ChainTable& CT = c_chains[D - 3];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned n = min(*cq.count, cq.cap);
+  const unsigned gw = blockIdx.x * kRefineWarps + wib;
+  const unsigned nw = gridDim.x * kRefineWarps;
+  for (unsigned c = gw; c < n; c += nw)
+    refine_candidate<T, D>(mesh, fa, cfg, cq.corner[c], cq.chains[c], sink, 0ull, cube[wib], band_tbl, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Batches: every field's tiles in one persistent launch, every candidate of
+// the batch in one exact-test launch.  Each item runs the single-field code
+// (cull_tile, refine_candidate) with its field's record, so a field's
+// candidates and features are those of its own extraction.
+
+template <typename T, bool MULTI>
+__global__ void __launch_bounds__(kThreads, 2)
+    batch_cull_kernel(const BatchField* __restrict__ fields, int nf, unsigned n_items, unsigned* item_next,
+                      CandidateQueue cq, unsigned* err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned long long bar[2];
+  __shared__ unsigned band_tbl[kBandTable];
+  __shared__ unsigned s_item, s_field;
+  fill_band_table<T>(band_tbl, threadIdx.x, kThreads);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  unsigned ph[2] = {0u, 0u};
+  for (;;) {
+    __syncthreads();  // s_item of the previous item has been read by every thread
+    if (threadIdx.x == 0) {
+      const unsigned it = atomicAdd(item_next, 1u);
+      unsigned f = 0;
+      if (it < n_items) {
+        // the last field whose first item is <= it
+        unsigned lo = 0, hi = (unsigned)nf;
+        while (hi - lo > 1) {
+          const unsigned mid = (lo + hi) >> 1;
+          if (fields[mid].item_base <= it) lo = mid;
+          else hi = mid;
+        }
+        f = lo;
+      }
+      s_item = it;
+      s_field = f;
+    }
+    __syncthreads();
+    const unsigned it = s_item;
+    if (it >= n_items) break;
+    const unsigned f = s_field;
+    const BatchField& F = fields[f];
+    const unsigned local = it - F.item_base;
+    const unsigned ntiles = (unsigned)F.cfg.tiles[0] * F.cfg.tiles[1] * F.cfg.tiles[2];
+    CandidateQueue q = cq;
+    q.field_id = f;
+    bool ok;
+    if (F.mesh.d == 4) {
+      ok = F.tma ? cull_tile<T, 4, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+                                                (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                ph)
+                 : cull_tile<T, 4, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                 ph);
+    } else {
+      ok = F.tma ? cull_tile<T, 3, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+                                                (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                ph)
+                 : cull_tile<T, 3, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                 ph);
+    }
+    if (!ok) break;  // the whole block saw the failed wait
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRefineWarps * 32, 2)
+    batch_refine_kernel(const BatchField* __restrict__ fields, CandidateQueue cq, FeatureSink sink) {
+  __shared__ T cube[kRefineWarps][16 * 3];
+  __shared__ unsigned band_tbl[kBandTable];
+  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const unsigned n = min(*cq.count, cq.cap);
   const unsigned gw = blockIdx.x * kRefineWarps + wib;
   const unsigned nw = gridDim.x * kRefineWarps;
   for (unsigned c = gw; c < n; c += nw) {
-    const unsigned long long pc = cq.corner[c];
-    const unsigned long long chains = cq.chains[c];
-    const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
-                            (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
-    long long g0[4];
-    unsigned long long vid0 = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      // D = 3: the time coordinate is the third axis
-      const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
-      g0[k] = (k < D) ? lk + mesh.off[k] : 0;
-      if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
-    }
-    // gather the hypercube's vertex values (only vertices inside the mesh)
-    for (int e = lane; e < NV * M; e += 32) {
-      const int v = e / M, j = e % M;
-      long long g[4];
-      unsigned long long vid = 0;
-      bool in = true;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
-        if (k < D) {
-          in &= g[k] - mesh.off[k] < mesh.ld[k];
-          vid += (unsigned long long)g[k] * mesh.gstride[k];
-        }
-      }
-      cube[wib][v][j] = in ? field_at<T>(fa, j, g, D, vid) : T(0);
-    }
-    __syncwarp();
-    // cull words of the hypercube's vertices (absent outside the mesh)
-    unsigned vw = kAbsent;
-    if (lane < NV) {
-      unsigned h[M];
-#pragma unroll
-      for (int j = 0; j < M; ++j) h[j] = hi_word<T>(cube[wib][lane][j]);
-      bool in = true;
-#pragma unroll
-      for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
-      vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
-    }
-    for (int base = 0; base < CT.n; base += 32) {
-      const int ch = base + lane;
-      bool acc = false;
-      double lam_out[4] = {0, 0, 0, 0};
-      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-      float sc_out = 0.f;
-      int mk[M + 1];
-      mk[0] = 0;
-      bool live = ch < CT.n && ((chains >> ch) & 1ull);
-#pragma unroll
-      for (int i = 0; i < M; ++i) mk[i + 1] = live ? CT.mask[ch][i] : 0;
-      {
-        unsigned wacc = kAbsent;
-#pragma unroll
-        for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, mk[i]);
-        live = live && !word_culled(wacc);
-      }
-      if (live) {
-        T vals[M + 1][M];
-#pragma unroll
-        for (int i = 0; i <= M; ++i)
-#pragma unroll
-          for (int j = 0; j < M; ++j) vals[i][j] = cube[wib][mk[i]][j];
-        bool inside;
-        if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
-        else inside = sos_inside3<T>(vals, cfg.Q);
-        if (inside) {
-          T lam[M + 1];
-          if (solve_exact<M, T>(vals, lam)) {
-            acc = true;
-#pragma unroll
-            for (int i = 0; i <= M; ++i) {
-              lam_out[i] = (double)lam[i];
-              bary_out[i] = (float)lam[i];
-            }
-            if (fa.has_scalar) {
-              using F = fp<T>;
-              T sc = T(0);
-#pragma unroll
-              for (int i = 0; i <= M; ++i) {
-                long long gv[4];
-                unsigned long long vid = 0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                  gv[k] = (k < D) ? g0[k] + ((mk[i] >> k) & 1) : 0;
-                  if (k < D) vid += (unsigned long long)gv[k] * mesh.gstride[k];
-                }
-                sc = F::add(sc, F::mul(lam[i], scalar_at<T>(fa, gv, D, vid)));
-              }
-              sc_out = (float)sc;
-            }
-            if (cfg.refined) {
-              double rr[M + 1];
-              if (solve_refined<M, T>(vals, rr))
-#pragma unroll
-                for (int i = 0; i <= M; ++i) lam_out[i] = rr[i];
-            }
-          }
-        }
-      }
-      const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
-      if (ball) {
-        unsigned int basei = 0;
-        const int leader = __ffs(ball) - 1;
-        if (lane == leader) basei = atomicAdd(sink.count, (unsigned)__popc(ball));
-        basei = __shfl_sync(0xFFFFFFFFu, basei, leader);
-        if (acc) {
-          const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
-          if (idx < sink.cap) {
-            sink.key[idx] = vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              sink.lam[4 * (size_t)idx + i] = lam_out[i];
-              sink.bary4[4 * (size_t)idx + i] = bary_out[i];
-            }
-            sink.scalar[idx] = sc_out;
-          }
-        }
-      }
-    }
-    __syncwarp();
+    const BatchField& F = fields[cq.field[c]];
+    if (F.mesh.d == 4)
+      refine_candidate<T, 4>(F.mesh, F.fa, F.cfg, cq.corner[c], cq.chains[c], sink, F.key_base, cube[wib], band_tbl,
+                             lane);
+    else
+      refine_candidate<T, 3>(F.mesh, F.fa, F.cfg, cq.corner[c], cq.chains[c], sink, F.key_base, cube[wib], band_tbl,
+                             lane);
   }
 }
 
@@ -1339,41 +1477,14 @@ static bool encode_map(CUtensorMap* map, bool f64, const void* base, int rank, c
   return r == CUDA_SUCCESS;
 }
 
-constexpr int kStatsStages = 4;
-
-template <typename T, int D, int XT>
-cudaError_t launch_stats_stream(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
-                                int ntasks, cudaStream_t st) {
-  using SS = StatsStream<T, D, XT, kStatsStages>;
-  auto k = plane_stats_stream_kernel<T, D, XT, kStatsStages>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SS::SMEM);
-  if (e) return e;
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, SS::THREADS, SS::SMEM) != cudaSuccess ||
-      per_sm < 1) {
-    cudaGetLastError();
-    per_sm = 1;
-  }
-  const long long want = (long long)sms * per_sm;
-  const long long need = (ntasks + kStatsWarps - 1) / kStatsWarps;
-  k<<<(unsigned)std::max<long long>(1, std::min(want, need)), SS::THREADS, SS::SMEM, st>>>(mesh, fa, cfg, ntasks);
-  return cudaGetLastError();
-}
-
+// TMA applies when every box starts on a 16-byte boundary and the array
+// strides are multiples of 16 bytes: inner coordinate = array x * (M or 1)
 template <typename T, int D, bool MULTI>
-static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
-                            const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
-                            int* used_tma, int* launches) {
+static bool build_tma_maps(const RegularMesh& mesh, const FieldAccess& fa, bool allow_tma, CUtensorMap maps[3]) {
   using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
   const size_t es = sizeof(T);
-
-  // TMA applies when every box starts on a 16-byte boundary and the array
-  // strides are multiples of 16 bytes: inner coordinate = array x * (M or 1)
-  CUtensorMap maps[3];
-  memset(maps, 0, sizeof(maps));
+  memset(maps, 0, 3 * sizeof(CUtensorMap));
   bool tma = allow_tma && !fa.per_vertex;
   const long long ax0 = mesh.off[0] - fa.shift[0];
   const size_t inner_es = (MULTI ? M : 1) * es;
@@ -1406,6 +1517,55 @@ static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, cons
     for (int j = 0; j < (MULTI ? 1 : M) && tma; ++j)
       tma = encode_map(&maps[j], sizeof(T) == 8, fa.comp[j], D, dims, strides, box);
   }
+  return tma;
+}
+
+bool regular_tma_maps(int f64, const RegularMesh& mesh, const FieldAccess& fa, bool allow, CUtensorMap maps[3]) {
+  const bool multi = !fa.per_vertex && fa.estride[0] == mesh.d - 1;
+  if (mesh.d == 4) {
+    if (f64) return multi ? build_tma_maps<double, 4, true>(mesh, fa, allow, maps)
+                          : build_tma_maps<double, 4, false>(mesh, fa, allow, maps);
+    return multi ? build_tma_maps<float, 4, true>(mesh, fa, allow, maps)
+                 : build_tma_maps<float, 4, false>(mesh, fa, allow, maps);
+  }
+  if (f64) return multi ? build_tma_maps<double, 3, true>(mesh, fa, allow, maps)
+                        : build_tma_maps<double, 3, false>(mesh, fa, allow, maps);
+  return multi ? build_tma_maps<float, 3, true>(mesh, fa, allow, maps)
+               : build_tma_maps<float, 3, false>(mesh, fa, allow, maps);
+}
+
+constexpr int kStatsStages = 4;
+
+template <typename T, int D, int XT>
+cudaError_t launch_stats_stream(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                                int ntasks, cudaStream_t st) {
+  using SS = StatsStream<T, D, XT, kStatsStages>;
+  auto k = plane_stats_stream_kernel<T, D, XT, kStatsStages>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SS::SMEM);
+  if (e) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, SS::THREADS, SS::SMEM) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const long long want = (long long)sms * per_sm;
+  const long long need = (ntasks + kStatsWarps - 1) / kStatsWarps;
+  k<<<(unsigned)std::max<long long>(1, std::min(want, need)), SS::THREADS, SS::SMEM, st>>>(mesh, fa, cfg, ntasks);
+  return cudaGetLastError();
+}
+
+template <typename T, int D, bool MULTI>
+static cudaError_t launch_t(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                            const CandidateQueue& cq, unsigned* err, cudaStream_t st, bool allow_tma,
+                            int* used_tma, int* launches) {
+  using G = Geo<T, D, MULTI>;
+  constexpr int M = D - 1;
+
+  CUtensorMap maps[3];
+  const bool tma = build_tma_maps<T, D, MULTI>(mesh, fa, allow_tma, maps);
   if (used_tma) *used_tma = tma ? 1 : 0;
   const size_t shm = G::SMEM;
   const long long lt = mesh.ld[D - 1];
@@ -1536,4 +1696,47 @@ cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldA
   return cudaGetLastError();
 }
 
+
+template <typename T, bool MULTI>
+static cudaError_t launch_batch_cull_t(const BatchField* fields, int nf, unsigned n_items, unsigned* item_next,
+                                       const CandidateQueue& cq, unsigned* err, cudaStream_t st) {
+  constexpr int shm = Geo<T, 4, MULTI>::SMEM > Geo<T, 3, MULTI>::SMEM ? Geo<T, 4, MULTI>::SMEM
+                                                                      : Geo<T, 3, MULTI>::SMEM;
+  auto k = batch_cull_kernel<T, MULTI>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  if (e) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, shm) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const long long want = (long long)sms * per_sm;
+  k<<<(unsigned)std::max<long long>(1, std::min<long long>(want, n_items)), kThreads, shm, st>>>(fields, nf, n_items,
+                                                                                             item_next, cq, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, int nf, unsigned n_items,
+                              unsigned* item_next, const CandidateQueue& cq, unsigned* err, cudaStream_t st) {
+  if (f64) return multi ? launch_batch_cull_t<double, true>(fields, nf, n_items, item_next, cq, err, st)
+                        : launch_batch_cull_t<double, false>(fields, nf, n_items, item_next, cq, err, st);
+  return multi ? launch_batch_cull_t<float, true>(fields, nf, n_items, item_next, cq, err, st)
+               : launch_batch_cull_t<float, false>(fields, nf, n_items, item_next, cq, err, st);
+}
+
+cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
+                                int num_sms, cudaStream_t st) {
+  const int grid = num_sms * 8;
+  if (f64) batch_refine_kernel<double><<<grid, kRefineWarps * 32, 0, st>>>(fields, cq, sink);
+  else batch_refine_kernel<float><<<grid, kRefineWarps * 32, 0, st>>>(fields, cq, sink);
+  return cudaGetLastError();
+}
+
+int batch_time_chunk(long long lt, int pick) {
+  // pick 0: the whole time range per item; otherwise that many steps
+  if (pick <= 0 || pick >= lt) return (int)std::max<long long>(1, lt);
+  return pick;
+}
 }  // namespace ftk2b

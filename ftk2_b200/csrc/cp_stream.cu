@@ -204,7 +204,7 @@ ftk2b_status push_regular(ftk2b_stream* s) {
     sink.scalar = (float*)s->scalar.p + s->n;
     sink.count = counters + kCountFeatures;
     sink.cap = s->cap - s->n;
-    CandidateQueue cq;
+    CandidateQueue cq{};
     cq.corner = (unsigned long long*)ctx->cand_corner.p;
     cq.chains = (unsigned long long*)ctx->cand_chains.p;
     cq.count = counters + kCountCand;

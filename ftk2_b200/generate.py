@@ -91,3 +91,68 @@ def gaussian_at_device(points, nt: int, seed: int = 1234, n_blobs: int = 32, dty
             e = float(blobs["amps"][b]) * torch.exp(-(d * d).sum(1) / (2.0 * s2))
             out[:, k, :] -= (e[:, None] * d / s2).T
     return out.reshape(ndim, nt * nv).to(dtype)
+
+
+def batch_specs(n: int = 256, seed: int = 2024, sides2=(32, 512), sides3=(16, 96), nt=(2, 8), blobs=(8, 64)):
+    """Seeded shapes of a batch of independent fields: each field is 2D or 3D
+    with probability 1/2, sides U[sides2] (2D) or U[sides3] (3D) per axis,
+    nt U[nt] timesteps and U[blobs] Gaussians; returns a list of
+    (spatial dims, nt, n_blobs, field seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        three = bool(rng.integers(0, 2))
+        lo, hi = sides3 if three else sides2
+        dims = tuple(int(v) for v in rng.integers(lo, hi + 1, size=3 if three else 2))
+        out.append((dims, int(rng.integers(nt[0], nt[1] + 1)), int(rng.integers(blobs[0], blobs[1] + 1)),
+                    int(seed * 1000 + i)))
+    return out
+
+
+def gaussian_field_fast(dims, nt: int, seed: int, n_blobs: int, dtype=None, sigma=(4.0, 12.0), drift: float = 0.5,
+                        device: str = "cuda", chunk: int = 16):
+    """The drifting Gaussian-sum gradient of gaussian_field_device with the
+    blobs evaluated ``chunk`` at a time (same blob parameters; the sum is
+    accumulated in another order, so values may differ in the last bits)."""
+    import torch
+    dtype = dtype or torch.float32
+    ndim = len(dims)
+    b = gaussian_blobs(seed, n_blobs, dims, sigma, drift)
+    shape = tuple(dims[::-1])
+    axes = []
+    for i in range(ndim):
+        view = [1] * (ndim + 1)
+        view[ndim - i] = dims[i]
+        axes.append(torch.arange(dims[i], dtype=torch.float64, device=device).view(view))
+    out = torch.empty((nt,) + shape + (ndim,), dtype=dtype, device=device)
+    cen = torch.as_tensor(b["centers"], device=device)
+    vel = torch.as_tensor(b["vel"], device=device)
+    amp = torch.as_tensor(b["amps"], device=device)
+    s2 = torch.as_tensor(b["sigma"], device=device) ** 2
+    bview = [-1] + [1] * ndim
+    for k in range(nt):
+        acc = torch.zeros(shape + (ndim,), dtype=torch.float64, device=device)
+        for c0 in range(0, n_blobs, chunk):
+            c1 = min(n_blobs, c0 + chunk)
+            c = cen[c0:c1] + vel[c0:c1] * k
+            d = [axes[i] - c[:, i].view(bview) for i in range(ndim)]
+            r2 = d[0] * d[0]
+            for i in range(1, ndim):
+                r2 = r2 + d[i] * d[i]
+            e = amp[c0:c1].view(bview) * torch.exp(-r2 / (2.0 * s2[c0:c1].view(bview))) / s2[c0:c1].view(bview)
+            for i in range(ndim):
+                acc[..., i] -= (e * d[i]).sum(0)
+        out[k] = acc.to(dtype)
+    return out
+
+
+def c3_batch(n: int = 256, seed: int = 2024, device: str = "cuda"):
+    """Batched workload: n independent float32 fields (2D sides U[32,512] or
+    3D sides U[16,96], nt U[2,8], 8-64 blobs each) as a list of
+    (mesh dims incl. time, ncomp, device tensor (nt, [nz,] ny, nx, ncomp))."""
+    import torch
+    out = []
+    for dims, nt, nb, fs in batch_specs(n, seed):
+        f = gaussian_field_fast(dims, nt, fs, nb, dtype=torch.float32, device=device)
+        out.append((list(dims) + [nt], len(dims), f))
+    return out

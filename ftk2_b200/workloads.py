@@ -9,6 +9,7 @@ c2_small  the same field definition on 128^3 x 4 (200 MB, larger than L2)
 c4        precision workload: 256^3 x 8 float32 with 1e-3 noise
 c4_small  the same on 256^3 x 2
 c1        2D analytic 64 x 64 x 10 float64, Q = 1e6
+c3        batch of 256 float32 fields (2D and 3D, uneven sizes), one batched call per step
 """
 from __future__ import annotations
 
@@ -39,6 +40,30 @@ def make(case: str):
     raise ValueError(case)
 
 
+def run_batch_case(args):
+    """c3: the 256-field batch, one ftk2b_cp_run_batch per step."""
+    import torch
+    fields = generate.c3_batch(n=args.nfields)
+    torch.cuda.synchronize()
+    with api.Context(0) as ctx:
+        if args.no_graphs:
+            ctx.set_option(api.OPT_USE_GRAPHS, 0)
+        if args.no_tma:
+            ctx.set_option(api.OPT_DISABLE_TMA, 1)
+        if args.tchunk:
+            ctx.set_option(api.OPT_BATCH_TIME_CHUNK, args.tchunk)
+        keep: list = []
+        meshes = [api.regular_mesh_desc(d) for d, _, _ in fields]
+        fds = [api.field_desc(f, api.LAYOUT_MULTICOMPONENT, m, keep=keep) for _, m, f in fields]
+        prms = [api.params(2.0 ** 20) for _ in fields]
+        for i in range(args.steps):
+            t = time.perf_counter()
+            n = ctx.run_batch(meshes, fds, prms)
+            x, tot, _ = ctx.last_timing()
+            print(f"step {i}: {n} features  cull {x:.3f} ms  pipeline {tot:.3f} ms  "
+                  f"host {1e3 * (time.perf_counter() - t):.3f} ms", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default="c2_small")
@@ -47,10 +72,13 @@ def main():
     ap.add_argument("--refined", action="store_true")
     ap.add_argument("--tchunk", type=int, default=0, help="time steps per extraction block (0 = all)")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--nfields", type=int, default=256, help="c3: fields in the batch")
     ap.add_argument("--cull-mode", type=int, default=2,
                     help="0: per-vertex cull words only; 1: tile statistics first; 2: the faster, timed once (default)")
     args = ap.parse_args()
     import torch
+    if args.case == "c3":
+        return run_batch_case(args)
     field, dims, m, q = make(args.case)
     torch.cuda.synchronize()
     with api.Context(0) as ctx:

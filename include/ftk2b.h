@@ -145,14 +145,18 @@ enum {
   FTK2B_OPT_DISABLE_TMA = 3,      /* 1: stage slices with plain loads instead of TMA */
   FTK2B_OPT_USE_GRAPHS = 4,       /* 1 (default): replay the device pipeline as a CUDA graph */
   FTK2B_OPT_BLOCKING_SYNC = 5,    /* 1: wait for the device by blocking, not spinning (servers set it) */
-  FTK2B_OPT_CULL_MODE = 6         /* 0: per-vertex cull words only; 1: tile statistics first; 2 (default):
+  FTK2B_OPT_CULL_MODE = 6,        /* 0: per-vertex cull words only; 1: tile statistics first; 2 (default):
                                      the faster of the two, timed once per workload shape by the context */
+  FTK2B_OPT_BATCH_TIME_CHUNK = 7  /* batches: corner time steps per cull item (0, default: chosen by the
+                                     context, timed once per batch shape) */
 };
 ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
 /* Reads an option back, or FTK2B_INFO_LAST_TMA: 1 when the last regular-mesh
  * extraction staged its slices with TMA tensor copies, or
- * FTK2B_INFO_LAST_CULL_MODE: the cull mode (0 or 1) it ran. */
-enum { FTK2B_INFO_LAST_TMA = 100, FTK2B_INFO_LAST_CULL_MODE = 101 };
+ * FTK2B_INFO_LAST_CULL_MODE: the cull mode (0 or 1) it ran, or
+ * FTK2B_INFO_LAST_BATCH_TIME_CHUNK: corner time steps per cull item of the
+ * last batch (65535: each field's whole time range). */
+enum { FTK2B_INFO_LAST_TMA = 100, FTK2B_INFO_LAST_CULL_MODE = 101, FTK2B_INFO_LAST_BATCH_TIME_CHUNK = 102 };
 ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t* value);
 
 /* m-simplices a mesh holds for codimension m (2 or 3): the unit of work. */
@@ -184,6 +188,27 @@ ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* t
  * capture and instantiation, [2] launch to device completion, [3] result
  * copy-back (ftk2b_cp_fetch). */
 ftk2b_status ftk2b_ctx_last_phases(ftk2b_ctx* ctx, double* phase_ms);
+
+/* --- batches ---------------------------------------------------------------
+ * No counterpart in the reference (one engine per field).  n independent
+ * regular-mesh fields of uneven sizes, 2D and 3D mixed, extracted together:
+ * one persistent cull launch walks every field's tiles, one launch runs the
+ * exact tests of every candidate, and one canonical-order / star-edge /
+ * union-find pipeline covers the whole batch, replayed as a CUDA graph for
+ * batches of the same shape.  Field i's result is identical to
+ * ftk2b_cp_extract on field i alone.
+ * All fields share one dtype and either the multicomponent or the separate /
+ * per-vertex layouts; params may be null (defaults) or hold n entries
+ * (classify is not supported in batches). */
+ftk2b_status ftk2b_cp_run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes,
+                                const ftk2b_field_desc* fields, const ftk2b_cp_params* params,
+                                uint64_t* n_features);
+/* Copies the last batch's results out: out[0 .. n-1], one result per field,
+ * each freed with ftk2b_cp_result_free. */
+ftk2b_status ftk2b_cp_fetch_batch(ftk2b_ctx* ctx, ftk2b_cp_result** out);
+ftk2b_status ftk2b_cp_extract_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes,
+                                    const ftk2b_field_desc* fields, const ftk2b_cp_params* params,
+                                    ftk2b_cp_result** out);
 
 /* --- time streams ----------------------------------------------------------
  * Replaces the reference's streaming drivers (SimplicialEngine::execute_stream
