@@ -488,6 +488,8 @@ def main():
         keep.clear()
         torch.cuda.empty_cache()
         line["precision"] = precision_c4(ctx)
+        # refined FP32 (c4) against the plain FP64 drop-in workload (c2, this line's value)
+        line["precision"]["refined_fp32_vs_plain_fp64_c2"] = line["precision"]["refined_fp32"]["simplices_per_s"] / value
         torch.cuda.empty_cache()
         line["batched"] = batched_c3(ctx)
         torch.cuda.empty_cache()

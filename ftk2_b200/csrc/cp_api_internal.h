@@ -98,7 +98,7 @@ struct BatchGraphKey {
   const void* h_fbase;
 };
 struct BatchCtx {
-  DevBuf fields, meshes, kb, fbase, cand_field, stage;
+  DevBuf fields, meshes, kb, fbase, cand_field, stage, item_base;
   void* h_tab = nullptr;          // pinned staging of the tables
   size_t h_tab_bytes = 0;
   unsigned* h_fbase = nullptr;    // pinned: first feature of every field
@@ -120,7 +120,7 @@ struct BatchCtx {
     if (g2) cudaGraphExecDestroy(g2);
     g1 = g2 = nullptr;
   }
-  std::vector<DevBuf*> bufs() { return {&fields, &meshes, &kb, &fbase, &cand_field, &stage}; }
+  std::vector<DevBuf*> bufs() { return {&fields, &meshes, &kb, &fbase, &cand_field, &stage, &item_base}; }
 };
 
 struct LastRun {

@@ -183,16 +183,23 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
   // tables to the device through pinned staging
   const size_t o_f = 0, o_m = align_up(sizeof(BatchField) * n, 256);
   const size_t o_k = o_m + align_up(sizeof(BatchMesh) * n, 256);
-  const size_t tab_bytes = o_k + sizeof(unsigned long long) * (n + 1);
+  const size_t o_i = o_k + align_up(sizeof(unsigned long long) * (n + 1), 256);
+  const size_t tab_bytes = o_i + sizeof(unsigned) * n;
   B_TRY(ctx, ensure_pinned(&bc.h_tab, &bc.h_tab_bytes, tab_bytes));
   unsigned char* ht = static_cast<unsigned char*>(bc.h_tab);
   B_TRY(ctx, bc.fields.ensure(sizeof(BatchField) * n));
   B_TRY(ctx, bc.meshes.ensure(sizeof(BatchMesh) * n));
   B_TRY(ctx, bc.kb.ensure(sizeof(unsigned long long) * (n + 1)));
   B_TRY(ctx, bc.fbase.ensure(sizeof(unsigned) * (n + 1)));
+  B_TRY(ctx, bc.item_base.ensure(sizeof(unsigned) * n));
   auto upload_fields = [&]() -> cudaError_t {
     memcpy(ht + o_f, hf.data(), sizeof(BatchField) * n);
-    return cudaMemcpyAsync(bc.fields.p, ht + o_f, sizeof(BatchField) * n, cudaMemcpyHostToDevice, ctx->stream);
+    unsigned* ib = reinterpret_cast<unsigned*>(ht + o_i);
+    for (uint32_t i = 0; i < n; ++i) ib[i] = hf[i].item_base;
+    cudaError_t e =
+        cudaMemcpyAsync(bc.fields.p, ht + o_f, sizeof(BatchField) * n, cudaMemcpyHostToDevice, ctx->stream);
+    if (!e) e = cudaMemcpyAsync(bc.item_base.p, ht + o_i, sizeof(unsigned) * n, cudaMemcpyHostToDevice, ctx->stream);
+    return e;
   };
   memcpy(ht + o_m, hm.data(), sizeof(BatchMesh) * n);
   memcpy(ht + o_k, hkb.data(), sizeof(unsigned long long) * (n + 1));
@@ -202,6 +209,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
   unsigned cap = bc.cap_hint ? bc.cap_hint : 65536u;
   unsigned ccap = bc.ccap_hint ? bc.ccap_hint : 65536u;
   const BatchField* dfields = static_cast<const BatchField*>(bc.fields.p);
+  const unsigned* ditems = static_cast<const unsigned*>(bc.item_base.p);
 
   // time chunk: as set, else the autotuner's choice for this batch shape,
   // timed once over the cull launch alone (results never depend on it)
@@ -232,7 +240,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
       for (int rep = 0; rep < 3; ++rep) {
         B_TRY(ctx, cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, ctx->stream));
         B_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-        B_TRY(ctx, launch_batch_cull(f64, multi, dfields, (int)n, (unsigned)it, counters + kCountItems, cq,
+        B_TRY(ctx, launch_batch_cull(f64, multi, dfields, ditems, (int)n, (unsigned)it, counters + kCountItems, cq,
                                      counters + kCountErr, ctx->stream));
         B_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
         B_TRY(ctx, ctx->sync());
@@ -289,8 +297,9 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     unsigned* const dfbase = static_cast<unsigned*>(bc.fbase.p);
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, ctx->stream);
-      if (!e) e = launch_batch_cull(f64, multi, dfields, (int)n, (unsigned)items, counters + kCountItems, cq, B.err,
-                                    ctx->stream);
+      if (!e)
+        e = launch_batch_cull(f64, multi, dfields, ditems, (int)n, (unsigned)items, counters + kCountItems, cq, B.err,
+                              ctx->stream);
       *nl += 1;
       return e;
     };

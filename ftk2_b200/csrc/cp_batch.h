@@ -31,9 +31,11 @@ struct BatchMesh {
 bool regular_tma_maps(int f64, const RegularMesh& mesh, const FieldAccess& fa, bool allow, CUtensorMap maps[3]);
 
 // One persistent launch culling every (field, tile, time chunk) item of the
-// batch; blocks take items from *item_next (zeroed by the caller).
-cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, int nf, unsigned n_items,
-                              unsigned* item_next, const CandidateQueue& cq, unsigned* err, cudaStream_t st);
+// batch; blocks take items from *item_next (zeroed by the caller);
+// item_base[f] = fields[f].item_base (ascending, nf entries).
+cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, const unsigned* item_base, int nf,
+                              unsigned n_items, unsigned* item_next, const CandidateQueue& cq, unsigned* err,
+                              cudaStream_t st);
 // Exact tests of every queued candidate of the batch (cq.field names its field).
 cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
                                 int num_sms, cudaStream_t st);

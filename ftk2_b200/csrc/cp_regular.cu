@@ -262,34 +262,60 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       // outside the array), one commit group per slice
       T* dst = reinterpret_cast<T*>(dst0);
       constexpr int NPER = G::VXBOX * VY * VZ;
-      for (int e = tid; e < NPER * M; e += kThreads) {
-        const int j = MULTI ? e % M : e / NPER;
-        const int r = MULTI ? e / M : e % NPER;
-        const int vx = r % G::VXBOX;
-        const int vy = (r / G::VXBOX) % VY;
-        const int vz = r / (G::VXBOX * VY);
-        const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : (long long)s, (long long)s};
-        bool in = true;
-        long long o = 0;
-        if (fa.per_vertex) {
+      if (!fa.per_vertex) {
+        // one box row per warp at a time: (vz, vy) rows of VXBOX * M
+        // interleaved elements, or (j, vz, vy) rows of VXBOX elements
+        constexpr int RW = MULTI ? G::VXBOX * M : G::VXBOX;
+        constexpr int NROWS = VY * VZ * (MULTI ? 1 : M);
+        const long long ax = (long long)x0 + aoff[0];  // array x of the box's first vertex
+        const long long at = (long long)tcoord(s);
+        for (int row = warp; row < NROWS; row += kWarps) {
+          const int j = MULTI ? 0 : row / (VY * VZ);
+          const int rr = MULTI ? row : row % (VY * VZ);
+          const int vy = rr % VY, vz = rr / VY;
+          const long long a1 = (long long)y0 + vy + aoff[1];
+          const long long a2 = (D == 4) ? (long long)z0 + vz + aoff[2] : at;
+          bool row_in = a1 >= 0 && a1 < fa.adims[1] && a2 >= 0 && a2 < fa.adims[2];
+          long long ob = a1 * fa.estride[1] + a2 * fa.estride[2];
+          if (D == 4) {
+            row_in = row_in && at >= 0 && at < fa.adims[3];
+            ob += at * fa.estride[3];
+          }
+          // elements of the row inside the array along x
+          const long long xin = fa.adims[0] - ax;
+          const long long xe = xin * (MULTI ? M : 1);
+          const int nin = !row_in || xin <= 0 ? 0 : (xe < RW ? (int)xe : RW);
+          const T* src = static_cast<const T*>(fa.comp[j]) + ob + ax * fa.estride[0];
+          T* d = MULTI ? dst + (vz * VY + vy) * RW : dst + j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX;
+          for (int q = lane; q < RW; q += 32) {
+            const bool in = q < nin && ax >= 0;
+            // separate arrays step by estride[0] along x; interleaved rows are contiguous
+            const long long so = MULTI ? q : (long long)q * fa.estride[0];
+            cp_async_zfill<sizeof(T)>(d + q, in ? src + so : static_cast<const T*>(fa.comp[j]),
+                                      in ? (unsigned)sizeof(T) : 0u);
+          }
+        }
+      } else {
+        for (int e = tid; e < NPER * M; e += kThreads) {
+          const int j = MULTI ? e % M : e / NPER;
+          const int r = MULTI ? e / M : e % NPER;
+          const int vx = r % G::VXBOX;
+          const int vy = (r / G::VXBOX) % VY;
+          const int vz = r / (G::VXBOX * VY);
+          const long long l[4] = {x0 + vx, y0 + vy, (D == 4) ? z0 + vz : (long long)s, (long long)s};
           // 1-D per-vertex arrays: index by vertex id, only inside the mesh
+          bool in = true;
+          long long o = 0;
 #pragma unroll
           for (int k = 0; k < D; ++k) {
             in &= l[k] < mesh.ld[k];
             o += (l[k] + mesh.off[k]) * (long long)mesh.gstride[k];
           }
-        } else {
-#pragma unroll
-          for (int k = 0; k < D; ++k) {
-            const long long a = (k == D - 1) ? (long long)tcoord(s) : l[k] + aoff[k];
-            in &= a >= 0 && a < fa.adims[k];
-            o += a * fa.estride[k];
-          }
+          const T* src = static_cast<const T*>(fa.comp[j]) + (in ? o : 0);
+          T* d = MULTI ? &dst[((vz * VY + vy) * G::VXBOX + vx) * M + j]
+                       : &dst[j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX + vx];
+          cp_async_zfill<sizeof(T)>(d, src, in ? (unsigned)sizeof(T) : 0u);
         }
-        const T* src = static_cast<const T*>(fa.comp[j]) + (in ? o : 0);
-        T* d = MULTI ? &dst[((vz * VY + vy) * G::VXBOX + vx) * M + j]
-                     : &dst[j * G::COMP_ELEMS + (vz * VY + vy) * G::VXBOX + vx];
-        cp_async_zfill<sizeof(T)>(d, src, in ? (unsigned)sizeof(T) : 0u);
       }
       cp_async_commit();
     }
@@ -1300,14 +1326,21 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 // (cull_tile, refine_candidate) with its field's record, so a field's
 // candidates and features are those of its own extraction.
 
+constexpr int kBatchSmemFields = 2048;  // item bases kept in shared memory up to this many fields
+
 template <typename T, bool MULTI>
 __global__ void __launch_bounds__(kThreads, 2)
-    batch_cull_kernel(const BatchField* __restrict__ fields, int nf, unsigned n_items, unsigned* item_next,
-                      CandidateQueue cq, unsigned* err) {
+    batch_cull_kernel(const BatchField* __restrict__ fields, const unsigned* __restrict__ item_base, int nf,
+                      unsigned n_items, unsigned* item_next, CandidateQueue cq, unsigned* err) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long bar[2];
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned s_item, s_field;
+  __shared__ unsigned s_ib[kBatchSmemFields];
+  const bool ib_smem = nf <= kBatchSmemFields;
+  if (ib_smem)
+    for (int i = threadIdx.x; i < nf; i += kThreads) s_ib[i] = item_base[i];
+  const unsigned* ib = ib_smem ? s_ib : item_base;
   fill_band_table<T>(band_tbl, threadIdx.x, kThreads);
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
@@ -1325,7 +1358,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         unsigned lo = 0, hi = (unsigned)nf;
         while (hi - lo > 1) {
           const unsigned mid = (lo + hi) >> 1;
-          if (fields[mid].item_base <= it) lo = mid;
+          if (ib[mid] <= it) lo = mid;
           else hi = mid;
         }
         f = lo;
@@ -1698,8 +1731,9 @@ cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldA
 
 
 template <typename T, bool MULTI>
-static cudaError_t launch_batch_cull_t(const BatchField* fields, int nf, unsigned n_items, unsigned* item_next,
-                                       const CandidateQueue& cq, unsigned* err, cudaStream_t st) {
+static cudaError_t launch_batch_cull_t(const BatchField* fields, const unsigned* item_base, int nf, unsigned n_items,
+                                       unsigned* item_next, const CandidateQueue& cq, unsigned* err,
+                                       cudaStream_t st) {
   constexpr int shm = Geo<T, 4, MULTI>::SMEM > Geo<T, 3, MULTI>::SMEM ? Geo<T, 4, MULTI>::SMEM
                                                                       : Geo<T, 3, MULTI>::SMEM;
   auto k = batch_cull_kernel<T, MULTI>;
@@ -1713,17 +1747,18 @@ static cudaError_t launch_batch_cull_t(const BatchField* fields, int nf, unsigne
     per_sm = 1;
   }
   const long long want = (long long)sms * per_sm;
-  k<<<(unsigned)std::max<long long>(1, std::min<long long>(want, n_items)), kThreads, shm, st>>>(fields, nf, n_items,
-                                                                                             item_next, cq, err);
+  k<<<(unsigned)std::max<long long>(1, std::min<long long>(want, n_items)), kThreads, shm, st>>>(
+      fields, item_base, nf, n_items, item_next, cq, err);
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, int nf, unsigned n_items,
-                              unsigned* item_next, const CandidateQueue& cq, unsigned* err, cudaStream_t st) {
-  if (f64) return multi ? launch_batch_cull_t<double, true>(fields, nf, n_items, item_next, cq, err, st)
-                        : launch_batch_cull_t<double, false>(fields, nf, n_items, item_next, cq, err, st);
-  return multi ? launch_batch_cull_t<float, true>(fields, nf, n_items, item_next, cq, err, st)
-               : launch_batch_cull_t<float, false>(fields, nf, n_items, item_next, cq, err, st);
+cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, const unsigned* item_base, int nf,
+                              unsigned n_items, unsigned* item_next, const CandidateQueue& cq, unsigned* err,
+                              cudaStream_t st) {
+  if (f64) return multi ? launch_batch_cull_t<double, true>(fields, item_base, nf, n_items, item_next, cq, err, st)
+                        : launch_batch_cull_t<double, false>(fields, item_base, nf, n_items, item_next, cq, err, st);
+  return multi ? launch_batch_cull_t<float, true>(fields, item_base, nf, n_items, item_next, cq, err, st)
+               : launch_batch_cull_t<float, false>(fields, item_base, nf, n_items, item_next, cq, err, st);
 }
 
 cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
