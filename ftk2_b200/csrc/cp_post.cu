@@ -16,6 +16,7 @@
 #include "cp_batch.h"
 #include "cp_post.h"
 #include "cp_kuhn.cuh"
+#include "cp_pdl.cuh"
 #include "cp_uf.cuh"
 
 namespace ftk2b {
@@ -31,6 +32,7 @@ constexpr int kRsThreads = 256;
 
 __global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
                                unsigned cap, int shift, unsigned* __restrict__ hist) {
+  pdl_enter();
   __shared__ unsigned h[256];
   const unsigned n = min(*n_ptr, cap);
   const unsigned G = gridDim.x, b = blockIdx.x;
@@ -47,6 +49,7 @@ __global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, cons
 // exclusive scan of `total` counters in place, one block of 1024 threads
 __global__ void scan_inplace_kernel(unsigned* __restrict__ a, unsigned total, unsigned* total_out,
                                     const unsigned* n_ptr, const unsigned* skip_small) {
+  pdl_enter();
   __shared__ unsigned part[1024];
   const unsigned t = threadIdx.x;
   (void)skip_small;
@@ -77,6 +80,7 @@ __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
                                   unsigned long long* __restrict__ kout, unsigned* __restrict__ vout,
                                   const unsigned* n_ptr, unsigned cap, int shift,
                                   const unsigned* __restrict__ hist) {
+  pdl_enter();
   __shared__ unsigned base[256];
   __shared__ unsigned wcnt[kRsThreads / 32][256];
   const unsigned n = min(*n_ptr, cap);
@@ -118,6 +122,7 @@ __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
 }
 
 __global__ void iota_kernel(unsigned* v, const unsigned* n_ptr, unsigned cap) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
@@ -134,9 +139,10 @@ bool radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, un
     const unsigned* vi = alt ? v1 : v0;
     unsigned long long* ko = alt ? k0 : k1;
     unsigned* vo = alt ? v0 : v1;
-    rs_hist_kernel<<<grid, kRsThreads, 0, st>>>(ki, n_ptr, cap, shift, hist);
-    scan_inplace_kernel<<<1, 1024, 0, st>>>(hist, 256u * grid, nullptr, nullptr, n_ptr);
-    rs_scatter_kernel<<<grid, kRsThreads, 0, st>>>(ki, vi, ko, vo, n_ptr, cap, shift, hist);
+    launch_pdl(rs_hist_kernel, grid, kRsThreads, 0, st, ki, n_ptr, cap, shift, hist);
+    launch_pdl(scan_inplace_kernel, 1, 1024, 0, st, hist, 256u * grid, (unsigned*)nullptr, (const unsigned*)nullptr,
+               n_ptr);
+    launch_pdl(rs_scatter_kernel, grid, kRsThreads, 0, st, ki, vi, ko, vo, n_ptr, cap, shift, (const unsigned*)hist);
     if (launches) *launches += 3;
     alt = !alt;
   }
@@ -150,6 +156,7 @@ __global__ void gather_kernel(const unsigned* n_ptr, unsigned cap, const unsigne
                               const double* __restrict__ lam_in, const float* __restrict__ sc_in,
                               const float* __restrict__ bary_in, double* __restrict__ lam_out,
                               float* __restrict__ sc_out, float* __restrict__ bary_out) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned p = perm[i];
@@ -297,6 +304,7 @@ __global__ void edges_regular_warp_kernel(RegularMesh mesh, int nch,
                                           const unsigned long long* __restrict__ keys,
                                           const unsigned* n_ptr, unsigned cap,
                                           unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   const int lane = threadIdx.x & 31;
   const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -335,6 +343,7 @@ __global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const 
 __global__ void edges_compact_kernel(const unsigned* n_ptr, unsigned cap, const unsigned* __restrict__ off,
                                      const unsigned* n_edges, const unsigned* __restrict__ slots,
                                      unsigned* __restrict__ edges, unsigned edge_cap) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   const unsigned ne = *n_edges;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -392,6 +401,7 @@ __global__ void edges_regular_kernel(RegularMesh mesh, int nch, const unsigned l
 // union-find
 
 __global__ void uf_init_kernel(unsigned* parent, const unsigned* n_ptr, unsigned cap) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     parent[i] = i;
@@ -399,6 +409,7 @@ __global__ void uf_init_kernel(unsigned* parent, const unsigned* n_ptr, unsigned
 
 __global__ void uf_hook_kernel(unsigned* parent, const unsigned* __restrict__ edges,
                                const unsigned* ne_ptr, unsigned edge_cap, unsigned* err) {
+  pdl_enter();
   const unsigned ne = min(*ne_ptr, edge_cap);
   for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x)
     uf_unite(parent, edges[2 * (size_t)e], edges[2 * (size_t)e + 1], err);
@@ -406,6 +417,7 @@ __global__ void uf_hook_kernel(unsigned* parent, const unsigned* __restrict__ ed
 
 __global__ void uf_label_kernel(unsigned* parent, const unsigned* n_ptr, unsigned cap,
                                 unsigned long long* __restrict__ track, unsigned* n_roots) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned x = uf_root(parent, i);
@@ -439,6 +451,7 @@ __global__ void expand_regular_kernel(RegularMesh mesh, int nch, const unsigned 
                                       const float* __restrict__ bary4,
                                       unsigned long long* __restrict__ simplices,
                                       float* __restrict__ bary) {
+  pdl_enter();
   const unsigned n = min(*n_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     expand_feature(mesh, nch, keys[i], i, mesh.d, bary4, simplices, bary);
@@ -531,31 +544,35 @@ cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuff
   const int gsort = B.sort_grid;
   const int g = grid_for(cap, 256, 4096);
   // keys in canonical order: multi-block stable LSD radix passes
-  iota_kernel<<<g, 256, 0, st>>>(B.perm0, B.count, cap);
+  // consecutive kernels overlap their launch with the predecessor's tail
+  // (programmatic dependent launch; each waits for its predecessor first)
+  launch_pdl(iota_kernel, g, 256, 0, st, B.perm0, (const unsigned*)B.count, cap);
   const bool alt = radix_sort(B.key, B.perm0, B.key_alt, B.perm1, B.count, cap, B.key_bits, B.hist,
                               gsort, st, launches);
   *launches += 3;  // iota, gather, expand
   const unsigned long long* skey = alt ? B.key_alt : B.key;
   const unsigned* perm = alt ? B.perm1 : B.perm0;
-  gather_kernel<<<g, 256, 0, st>>>(B.count, cap, perm, B.lam, B.scalar, B.bary4, B.lam_sorted,
-                                   B.scalar_sorted, B.bary4_sorted);
-  expand_regular_kernel<<<g, 256, 0, st>>>(mesh, nch, skey, B.count, cap, B.bary4_sorted,
-                                           B.simplices, B.bary);
+  launch_pdl(gather_kernel, g, 256, 0, st, (const unsigned*)B.count, cap, perm, (const double*)B.lam,
+             (const float*)B.scalar, (const float*)B.bary4, B.lam_sorted, B.scalar_sorted, B.bary4_sorted);
+  launch_pdl(expand_regular_kernel, g, 256, 0, st, mesh, nch, skey, (const unsigned*)B.count, cap,
+             (const float*)B.bary4_sorted, B.simplices, B.bary);
   if (!want_edges) return cudaGetLastError();
   // star edges, written in (centre, other) order: already sorted and unique
   {
     const int gw = grid_for(cap, 8, 8192);  // one warp per feature, 8 warps per block
-    edges_regular_warp_kernel<<<gw, 256, 0, st>>>(mesh, nch, skey, B.count, cap, B.edge_cnt,
-                                                  B.edge_slots);
+    launch_pdl(edges_regular_warp_kernel, gw, 256, 0, st, mesh, nch, skey, (const unsigned*)B.count, cap, B.edge_cnt,
+               B.edge_slots);
   }
-  scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count, nullptr);
-  edges_compact_kernel<<<g, 256, 0, st>>>(B.count, cap, B.edge_cnt, B.n_edges, B.edge_slots, B.edges,
-                                          B.edge_cap);
+  launch_pdl(scan_inplace_kernel, 1, 1024, 0, st, B.edge_cnt, cap, B.n_edges, (const unsigned*)B.count,
+             (const unsigned*)nullptr);
+  launch_pdl(edges_compact_kernel, g, 256, 0, st, (const unsigned*)B.count, cap, (const unsigned*)B.edge_cnt,
+             (const unsigned*)B.n_edges, (const unsigned*)B.edge_slots, B.edges, B.edge_cap);
   // trajectories
-  uf_init_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap);
+  launch_pdl(uf_init_kernel, g, 256, 0, st, B.parent, (const unsigned*)B.count, cap);
   const int ge = grid_for(B.edge_cap, 256, 4096);
-  uf_hook_kernel<<<ge, 256, 0, st>>>(B.parent, B.edges, B.n_edges, B.edge_cap, B.err);
-  uf_label_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap, B.track, B.n_roots);
+  launch_pdl(uf_hook_kernel, ge, 256, 0, st, B.parent, (const unsigned*)B.edges, (const unsigned*)B.n_edges,
+             B.edge_cap, B.err);
+  launch_pdl(uf_label_kernel, g, 256, 0, st, B.parent, (const unsigned*)B.count, cap, B.track, B.n_roots);
   *launches += 6;  // edge count, scan, edge write, uf init, hook, label
   return cudaGetLastError();
 }
