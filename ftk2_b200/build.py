@@ -81,5 +81,26 @@ def build_dropin_test(verbose: bool = False) -> str:
     return DROPIN_BIN
 
 
+TRACKER_SRC = os.path.join(ROOT, "tests", "cpp", "tracker_run.cpp")
+TRACKER_BIN = os.path.join(OUT_DIR, "tracker_run")
+
+
+def build_tracker_test(verbose: bool = False) -> str:
+    """C++ program driving include/ftk2b/feature_tracker.hpp from a YAML
+    configuration, as a reference caller drives ftk2::FeatureTracker."""
+    lib = build(verbose)
+    hdrs = [os.path.join(ROOT, "include", "ftk2b", h) for h in ("engine.hpp", "feature_tracker.hpp",
+                                                              "tracking_config.hpp")]
+    if os.path.exists(TRACKER_BIN) and os.path.getmtime(TRACKER_BIN) >= max(
+            [os.path.getmtime(TRACKER_SRC), os.path.getmtime(lib)] + [os.path.getmtime(h) for h in hdrs]):
+        return TRACKER_BIN
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), TRACKER_SRC, "-o", TRACKER_BIN,
+           "-L", OUT_DIR, "-lftk2b", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return TRACKER_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))

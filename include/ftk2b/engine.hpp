@@ -20,9 +20,12 @@
 // errors, engine.hpp:29-37); there is no CPU fallback.
 #pragma once
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -99,27 +102,94 @@ class ExtrudedSimplicialMesh : public Mesh {
  public:
   ExtrudedSimplicialMesh(std::shared_ptr<UnstructuredSimplicialMesh> base, uint64_t n_layers)
       : base_(std::move(base)), n_layers_(n_layers) {}
-  int get_total_dimension() const override { return base_->get_total_dimension() + 1; }
+  // Over a regular spatial mesh, as the reference's high-level caller builds
+  // its spacetime mesh (feature_tracker.cpp:520): the base cells are the
+  // spatial grid's Kuhn simplices (one per axis order, d! per cube, as
+  // RegularSimplicialMesh enumerates them) and the vertex id of spatial vertex
+  // s at timestep t is s + t * S with S = the base's grid_index_to_id(global
+  // dims), which is what ExtrudedSimplicialMesh's constructor takes as its
+  // spatial vertex count (mesh.hpp:544-560).
+  ExtrudedSimplicialMesh(std::shared_ptr<RegularSimplicialMesh> base, uint64_t n_layers)
+      : n_layers_(n_layers), regular_(std::move(base)) {
+    const std::vector<uint64_t>& g = regular_->get_global_dims();
+    const int d = (int)g.size();
+    if (d != 2 && d != 3) throw Error(FTK2B_UNSUPPORTED, "regular spatial meshes are 2D or 3D");
+    for (int k = 0; k < d; ++k)
+      if (regular_->get_offset()[k] != 0 || regular_->get_local_dims()[k] != g[k])
+        throw Error(FTK2B_UNSUPPORTED, "an extruded regular base must cover its global grid");
+    stride_ = 0;
+    uint64_t mul = 1;
+    for (int k = 0; k < d; ++k) {
+      stride_ += g[k] * mul;
+      mul *= g[k];
+    }
+    int perm[3] = {0, 1, 2};
+    std::vector<std::vector<int>> orders;
+    do {
+      orders.push_back(std::vector<int>(perm, perm + d));
+    } while (std::next_permutation(perm, perm + d));
+    const uint64_t nz = d == 3 ? g[2] : 1;
+    for (uint64_t z = 0; z + (d == 3 ? 1 : 0) < nz; ++z)
+      for (uint64_t y = 0; y + 1 < g[1]; ++y)
+        for (uint64_t x = 0; x + 1 < g[0]; ++x)
+          for (const auto& o : orders) {
+            uint64_t c[3] = {x, y, z};
+            cells_.push_back(c[0] + g[0] * (c[1] + g[1] * c[2]));
+            for (int i = 0; i < d; ++i) {
+              c[o[i]]++;
+              cells_.push_back(c[0] + g[0] * (c[1] + g[1] * c[2]));
+            }
+          }
+  }
+  int get_total_dimension() const override {
+    return (regular_ ? (int)regular_->get_global_dims().size() : base_->get_total_dimension()) + 1;
+  }
   uint64_t get_n_layers() const { return n_layers_; }
+  // regular base: its spatial grid and the per-timestep vertex id stride
+  const RegularSimplicialMesh* regular_base() const { return regular_.get(); }
+  uint64_t vertex_stride() const { return stride_; }
   ftk2b_mesh_desc desc() const override {
     ftk2b_mesh_desc d;
     std::memset(&d, 0, sizeof(d));
     d.kind = FTK2B_MESH_EXTRUDED;
+    d.n_layers = n_layers_;
+    if (regular_) {
+      const int sd = (int)regular_->get_global_dims().size();
+      d.ndims = sd + 1;
+      d.n_base_verts = stride_;
+      d.base_cells = cells_.data();
+      d.base_cell_dim = sd;
+      d.n_base_cells = cells_.size() / (sd + 1);
+      return d;
+    }
     d.ndims = base_->cell_dim() + 1;
     d.n_base_verts = base_->get_num_vertices();
     d.base_cells = base_->cells().data();
     d.base_cell_dim = base_->cell_dim();
     d.n_base_cells = base_->cells().size() / (base_->cell_dim() + 1);
-    d.n_layers = n_layers_;
     return d;
   }
 
  private:
   std::shared_ptr<UnstructuredSimplicialMesh> base_;
   uint64_t n_layers_;
+  std::shared_ptr<RegularSimplicialMesh> regular_;
+  uint64_t stride_ = 0;
+  std::vector<uint64_t> cells_;
 };
 
 // ---- predicate (the CP knobs of predicate.hpp:22-64)
+
+// An array value to record at every feature (predicate.hpp:34-40): type
+// "magnitude" or "scalar", component >= 0 for one component of a
+// multicomponent source, slot 0..15 of FeatureElement::attributes.
+struct AttributeSpec {
+  std::string name;
+  std::string source;
+  std::string type = "scalar";
+  int component = -1;
+  int slot = -1;
+};
 
 template <int M, typename T = double>
 struct CriticalPointPredicate {
@@ -129,6 +199,7 @@ struct CriticalPointPredicate {
   std::string var_names[M];
   std::string scalar_var_name;
   bool use_multicomponent = true;
+  std::vector<AttributeSpec> attributes;
   int precision = FTK2B_PRECISION_EXACT;  // new: refined-FP32 reporting
   bool classify = false;                  // new: Jacobian classification
 };
@@ -185,6 +256,11 @@ class SimplicialEngine {
 
   template <typename Array>
   void execute(const std::map<std::string, Array>& data, const std::vector<std::string>& = {}) {
+    const auto* ext = dynamic_cast<const ExtrudedSimplicialMesh*>(mesh_.get());
+    if (ext && ext->regular_base()) {
+      execute_extruded_regular(data, *ext);
+      return;
+    }
     ftk2b_mesh_desc md = mesh_->desc();
     ftk2b_field_desc fd;
     std::memset(&fd, 0, sizeof(fd));
@@ -225,6 +301,7 @@ class SimplicialEngine {
     ftk2b_status st = ftk2b_cp_extract(ctx_.get(), &md, &fd, &p, &r);
     if (st != FTK2B_OK) throw Error(st, ftk2b_last_error(ctx_.get()));
     result_.reset(r);
+    record_attributes(data);
   }
 
   template <typename Array>
@@ -236,6 +313,7 @@ class SimplicialEngine {
     FeatureComplex fc;
     const ftk2b_cp_result* r = result_.get();
     if (!r) return fc;
+    const bool with_attrs = attrs_.size() == 16 * (size_t)r->n_features;
     const int k = r->m + 1;
     fc.vertices.resize(r->n_features);
     fc.lambda.assign(r->lambda, r->lambda + r->n_features * k);
@@ -250,6 +328,8 @@ class SimplicialEngine {
       el.track_id = r->track_id[i];
       el.type = r->type[i];
       el.scalar = r->scalar[i];
+      if (with_attrs)
+        for (int a = 0; a < 16; ++a) el.attributes[a] = attrs_[16 * (size_t)i + a];
     }
     if (r->n_edges) {
       FeatureComplex::SimplexIndices e;
@@ -261,6 +341,167 @@ class SimplicialEngine {
   }
 
  private:
+  template <typename Array>
+  using elem_t = std::remove_cv_t<std::remove_pointer_t<decltype(std::declval<const Array&>().pdata())>>;
+
+  // ndarray's Fortran element access f(i0, i1, ...) with as many indices as
+  // given: offset = sum_k idx_k * prod_{j<k} dimf(j)
+  template <typename Array>
+  static double fetch(const Array& a, const uint64_t* idx, int n) {
+    uint64_t off = 0, mul = 1;
+    for (int k = 0; k < n; ++k) {
+      off += idx[k] * mul;
+      mul *= (k < (int)a.nd()) ? (uint64_t)a.dimf(k) : 1;
+    }
+    return (double)a.pdata()[off];
+  }
+
+  // Spacetime grid coordinates of a vertex (get_vertex_coordinates of the
+  // regular mesh, or of the extruded mesh over a regular base) and the
+  // offset that legacy arrays subtract (engine.hpp:999-1009, 1036-1038).
+  int vertex_coords(uint64_t vid, uint64_t* c, uint64_t* off) const {
+    const auto* ext = dynamic_cast<const ExtrudedSimplicialMesh*>(mesh_.get());
+    const RegularSimplicialMesh* reg = ext ? ext->regular_base() : dynamic_cast<const RegularSimplicialMesh*>(mesh_.get());
+    if (!reg) return 0;
+    const std::vector<uint64_t>& g = reg->get_global_dims();
+    int n = 0;
+    uint64_t v = vid;
+    if (ext) {
+      v = vid % ext->vertex_stride();
+      for (size_t k = 0; k < g.size(); ++k, ++n) {
+        c[n] = v % g[k];
+        v /= g[k];
+        off[n] = 0;
+      }
+      c[n] = vid / ext->vertex_stride();
+      off[n++] = 0;
+      return n;
+    }
+    for (size_t k = 0; k < g.size(); ++k, ++n) {
+      c[n] = v % g[k];
+      v /= g[k];
+      off[n] = reg->get_offset()[k];
+    }
+    return n;
+  }
+
+  // FeatureElement::attributes at each feature, interpolated with the float
+  // barycentrics the element stores, in the field precision T, as
+  // extract_simplex does for every accepted simplex (engine.hpp:1143-1199):
+  // one component of a multicomponent source, its magnitude, or the value of
+  // a plain (or per-vertex) array.  Runs on the host arrays, over the
+  // accepted features only.
+  template <typename Array>
+  void record_attributes(const std::map<std::string, Array>& data) {
+    attrs_.clear();
+    const ftk2b_cp_result* r = result_.get();
+    if (!r || pred_.attributes.empty()) return;
+    attrs_.assign(16 * (size_t)r->n_features, 0.f);
+    const int k = r->m + 1;
+    for (const AttributeSpec& spec : pred_.attributes) {
+      if (spec.slot < 0 || spec.slot >= 16) continue;
+      auto it = data.find(spec.source);
+      if (it == data.end()) continue;
+      const Array& a = it->second;
+      const bool multicomp = a.nd() >= 2 && a.dimf(0) >= 1 && a.dimf(0) <= 16;
+      for (uint64_t i = 0; i < r->n_features; ++i) {
+        T acc = 0;
+        for (int v = 0; v < k; ++v) {
+          const uint64_t vid = r->simplices[i * k + v];
+          uint64_t c[5], off[5], idx[6];
+          const int n = vertex_coords(vid, c, off);
+          T val = 0;
+          if (multicomp && spec.component >= 0) {
+            idx[0] = (uint64_t)spec.component;
+            for (int q = 0; q < n; ++q) idx[q + 1] = c[q];
+            val = (T)fetch(a, idx, n + 1);
+          } else if (multicomp && spec.type == "magnitude") {
+            T sq = 0;
+            for (uint64_t comp = 0; comp < (uint64_t)a.dimf(0); ++comp) {
+              idx[0] = comp;
+              for (int q = 0; q < n; ++q) idx[q + 1] = c[q];
+              const T cv = (T)fetch(a, idx, n + 1);
+              sq += cv * cv;
+            }
+            val = std::sqrt(sq);
+          } else if (a.nd() == 1) {
+            val = (T)a.pdata()[vid];
+          } else {
+            for (int q = 0; q < n; ++q) idx[q] = c[q] - off[q];
+            val = (T)fetch(a, idx, n);
+          }
+          acc += r->barycentric[i * k + v] * val;
+        }
+        attrs_[16 * (size_t)i + spec.slot] = (float)acc;
+      }
+    }
+  }
+
+  // The extruded mesh over a regular base: the reference reads the arrays at
+  // each vertex's grid coordinates (multicomponent f(j, x, y, [z,] t), legacy
+  // f(x, y, [z,] t)), so they are laid out here as per-vertex arrays indexed
+  // by the extruded vertex id s + t * S (the gap ids of each timestep, which no
+  // simplex uses, hold zeros).
+  template <typename Array>
+  void execute_extruded_regular(const std::map<std::string, Array>& data, const ExtrudedSimplicialMesh& ext) {
+    const std::vector<uint64_t>& g = ext.regular_base()->get_global_dims();
+    uint64_t nxy = 1;
+    for (uint64_t d : g) nxy *= d;
+    const uint64_t S = ext.vertex_stride(), nt = ext.get_n_layers() + 1;
+    std::vector<std::vector<T>> comps(m);
+    auto lay_out = [&](const Array& a, int j, int ncomp, std::vector<T>& dst) {
+      dst.assign(S * nt, T(0));
+      const uint64_t have = (uint64_t)a.nelem() / (uint64_t)ncomp;
+      for (uint64_t t = 0; t < nt; ++t)
+        for (uint64_t sv = 0; sv < nxy; ++sv) {
+          const uint64_t e = sv + nxy * t;
+          if (e < have) dst[sv + S * t] = (T)a.pdata()[(uint64_t)j + (uint64_t)ncomp * e];
+        }
+    };
+    if (pred_.use_multicomponent && !pred_.vector_var_name.empty()) {
+      const Array& a = data.at(pred_.vector_var_name);
+      for (int j = 0; j < m; ++j) lay_out(a, j, m, comps[j]);
+    } else {
+      for (int j = 0; j < m; ++j) {
+        const Array& a = data.at(pred_.var_names[j]);
+        if (a.nd() == 1) {
+          comps[j].assign(a.pdata(), a.pdata() + a.nelem());
+          comps[j].resize(std::max<size_t>(comps[j].size(), S * nt), T(0));
+        } else {
+          lay_out(a, 0, 1, comps[j]);
+        }
+      }
+    }
+    std::vector<T> scal;
+    ftk2b_mesh_desc md = ext.desc();
+    ftk2b_field_desc fd;
+    std::memset(&fd, 0, sizeof(fd));
+    fd.dtype = sizeof(T) == 8 ? FTK2B_F64 : FTK2B_F32;
+    fd.ncomp = m;
+    fd.location = FTK2B_HOST;
+    fd.layout = FTK2B_LAYOUT_PER_VERTEX;
+    fd.nd = 1;
+    fd.dims[0] = S * nt;
+    for (int j = 0; j < m; ++j) fd.comp[j] = comps[j].data();
+    if (!pred_.scalar_var_name.empty() && !pred_.use_multicomponent) {
+      const Array& sa = data.at(pred_.scalar_var_name);
+      if (sa.nd() == 1) scal.assign(sa.pdata(), sa.pdata() + sa.nelem());
+      else lay_out(sa, 0, 1, scal);
+      scal.resize(std::max<size_t>(scal.size(), S * nt), T(0));
+      fd.scalar = scal.data();
+      fd.scalar_nd = 1;
+      fd.scalar_dims[0] = S * nt;
+    }
+    ftk2b_cp_params p = ftk2b_cp_params_default();
+    p.sos_q = pred_.sos_q;
+    p.precision = pred_.precision;
+    ftk2b_cp_result* r = nullptr;
+    ftk2b_status st = ftk2b_cp_extract(ctx_.get(), &md, &fd, &p, &r);
+    if (st != FTK2B_OK) throw Error(st, ftk2b_last_error(ctx_.get()));
+    result_.reset(r);
+    record_attributes(data);
+  }
+
   struct CtxDel {
     void operator()(ftk2b_ctx* c) const { ftk2b_ctx_destroy(c); }
   };
@@ -271,6 +512,7 @@ class SimplicialEngine {
   PredicateType pred_;
   std::unique_ptr<ftk2b_ctx, CtxDel> ctx_;
   std::unique_ptr<ftk2b_cp_result, ResDel> result_;
+  std::vector<float> attrs_;  // 16 per feature when attributes were recorded
 };
 
 }  // namespace ftk2b

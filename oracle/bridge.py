@@ -204,3 +204,77 @@ def run_reference(mesh: OrcMesh, field: OrcField) -> CPResult:
 def run_restatement(mesh: OrcMesh, field: OrcField) -> CPResult:
     """Our exact C restatement of the same algorithm."""
     return _run(ORC_LIB, "cporacle", mesh, field)
+
+
+class OrcTracked(C.Structure):
+    _fields_ = [
+        ("dtype", C.c_int), ("m", C.c_int), ("dims", C.c_uint64 * 3), ("nt", C.c_uint64),
+        ("vec", C.c_void_p), ("n_attr", C.c_int),
+        ("attr_data", C.c_void_p * 16), ("attr_nd", C.c_int * 16), ("attr_dims", (C.c_uint64 * 6) * 16),
+        ("attr_magnitude", C.c_int * 16), ("attr_component", C.c_int * 16),
+    ]
+
+
+def run_reference_tracked(vec: np.ndarray, attrs=()):
+    """The reference high-level caller's critical-point flow: its engine on
+    ExtrudedSimplicialMesh(RegularSimplicialMesh(spatial dims), nt - 1) with
+    the multicomponent array ``vec`` (C-order shape (nt, [nz,] ny, nx, m), the
+    bytes of a Fortran [m, nx, ny, (nz,) nt] array) and attributes given as
+    (array, magnitude, component) with arrays in C order (reversed Fortran
+    shape).  Returns (CPResult, attributes (n, 16) float32)."""
+    lib = _load(REF_LIB, "ftk2ref")
+    if not hasattr(lib, "_tracked_bound"):
+        lib.ftk2ref_run_tracked.argtypes = [C.POINTER(OrcTracked), C.POINTER(OrcResult),
+                                            C.POINTER(C.POINTER(C.c_float))]
+        lib.ftk2ref_run_tracked.restype = C.c_int
+        lib.ftk2ref_free_attrs.argtypes = [C.POINTER(C.c_float)]
+        lib._tracked_bound = True
+    vec = np.ascontiguousarray(vec)
+    m = vec.shape[-1]
+    t = OrcTracked()
+    t.dtype = F64 if vec.dtype == np.float64 else F32
+    t.m = m
+    sp = vec.shape[1:-1][::-1]  # Fortran spatial dims
+    for i, d in enumerate(sp):
+        t.dims[i] = int(d)
+    t.nt = int(vec.shape[0])
+    t.vec = vec.ctypes.data
+    keep = [vec]
+    t.n_attr = len(attrs)
+    for a, (arr, mag, comp) in enumerate(attrs):
+        arr = np.ascontiguousarray(arr, dtype=vec.dtype)
+        keep.append(arr)
+        t.attr_data[a] = arr.ctypes.data
+        fd = arr.shape[::-1]
+        t.attr_nd[a] = len(fd)
+        for i, d in enumerate(fd):
+            t.attr_dims[a][i] = int(d)
+        t.attr_magnitude[a] = int(bool(mag))
+        t.attr_component[a] = int(comp)
+    res = OrcResult()
+    out = C.POINTER(C.c_float)()
+    rc = lib.ftk2ref_run_tracked(C.byref(t), C.byref(res), C.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"ftk2ref_run_tracked failed with status {rc}")
+    try:
+        n, k, e = int(res.n), int(res.m) + 1, int(res.n_edges)
+
+        def arr_(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        r = CPResult(
+            simplices=arr_(res.simplices, n * k, np.uint64).reshape(n, k),
+            bary=arr_(res.bary, n * k, np.float32).reshape(n, k),
+            lam=arr_(res.lambda_, n * k, np.float64).reshape(n, k),
+            track_id=arr_(res.track_id, n, np.uint64),
+            type=arr_(res.type, n, np.uint32),
+            scalar=arr_(res.scalar, n, np.float32),
+            edges=arr_(res.edges, 2 * e, np.uint32).reshape(e, 2),
+            n_tested=0, cp_class=None)
+        at = arr_(out, n * 16, np.float32).reshape(n, 16)
+        return r, at
+    finally:
+        lib.ftk2ref_free(C.byref(res))
+        lib.ftk2ref_free_attrs(out)

@@ -77,9 +77,31 @@ typedef struct {
                                FTK2B_CLASS_* codes of include/ftk2b.h */
 } orc_result;
 
+/* The high-level caller's critical-point flow (src/high_level/feature_tracker.cpp:
+ * 339-357 with the mesh of 480-520): ExtrudedSimplicialMesh over
+ * RegularSimplicialMesh(spatial dims) with nt - 1 layers, a multicomponent
+ * vector array [m, dims..., nt], and AttributeSpec entries recorded into
+ * FeatureElement::attributes (engine.hpp:1143-1199). */
+typedef struct {
+  int dtype;                   /* ORC_F32 / ORC_F64 */
+  int m;                       /* 2 or 3 */
+  uint64_t dims[3];            /* spatial dims */
+  uint64_t nt;
+  const void* vec;             /* [m, dims..., nt], Fortran order */
+  int n_attr;                  /* <= 16, slots 0 .. n_attr-1 */
+  const void* attr_data[16];
+  int attr_nd[16];
+  uint64_t attr_dims[16][6];   /* full Fortran shape of the source array */
+  int attr_magnitude[16];      /* 1: type "magnitude", else "scalar" */
+  int attr_component[16];      /* AttributeSpec::component (-1 = none) */
+} orc_tracked;
+
 /* reference engine build */
 int ftk2ref_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);
 void ftk2ref_free(orc_result* r);
+/* attrs receives n * 16 floats (malloc'd; release with ftk2ref_free_attrs) */
+int ftk2ref_run_tracked(const orc_tracked* in, orc_result* out, float** attrs);
+void ftk2ref_free_attrs(float* attrs);
 
 /* own restatement */
 int cporacle_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);

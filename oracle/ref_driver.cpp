@@ -145,6 +145,72 @@ int run(const orc_mesh* mesh, const orc_field* field, orc_result* out) {
   return 0;
 }
 
+
+// The high-level flow: the engine on the extruded regular spatial mesh, with
+// attributes; results flattened as run() does.
+template <typename T, int M>
+int run_tracked(const orc_tracked* in, orc_result* out, float** attrs) {
+  using namespace ftk2;
+  std::vector<uint64_t> sdims(in->dims, in->dims + M);
+  auto base = std::make_shared<RegularSimplicialMesh>(sdims);
+  std::shared_ptr<Mesh> mesh_ptr = std::make_shared<ExtrudedSimplicialMesh>(base, in->nt - 1);
+  CriticalPointPredicate<M, T> pred;
+  pred.use_multicomponent = true;
+  pred.vector_var_name = "vec";
+  std::map<std::string, ftk::ndarray<T>> data;
+  std::vector<uint64_t> vdims(in->dims, in->dims + M);
+  vdims.push_back(in->nt);
+  data["vec"] = make_array<T>(in->vec, M + 1, vdims.data(), (size_t)M);
+  for (int a = 0; a < in->n_attr; ++a) {
+    const std::string name = "attr" + std::to_string(a);
+    data[name] = make_array<T>(in->attr_data[a], in->attr_nd[a], in->attr_dims[a]);
+    AttributeSpec spec;
+    spec.name = name;
+    spec.source = name;
+    spec.type = in->attr_magnitude[a] ? "magnitude" : "scalar";
+    spec.component = in->attr_component[a];
+    spec.slot = a;
+    pred.attributes.push_back(spec);
+  }
+  SimplicialEngine<T, CriticalPointPredicate<M, T>> engine(mesh_ptr, pred);
+  std::streambuf* saved = std::cout.rdbuf();
+  std::ostringstream sink;
+  std::cout.rdbuf(sink.rdbuf());
+  engine.execute(data);
+  FeatureComplex complex = engine.get_complex();
+  std::cout.rdbuf(saved);
+  const uint64_t n = complex.vertices.size();
+  out->m = M;
+  out->n = n;
+  out->simplices = (uint64_t*)std::malloc(sizeof(uint64_t) * (n * (M + 1) + 1));
+  out->bary = (float*)std::malloc(sizeof(float) * (n * (M + 1) + 1));
+  out->lambda = (double*)std::malloc(sizeof(double) * (n * (M + 1) + 1));
+  out->track_id = (uint64_t*)std::malloc(sizeof(uint64_t) * (n + 1));
+  out->type = (uint32_t*)std::malloc(sizeof(uint32_t) * (n + 1));
+  out->scalar = (float*)std::malloc(sizeof(float) * (n + 1));
+  out->n_tested = 0;
+  *attrs = (float*)std::malloc(sizeof(float) * (n * 16 + 1));
+  for (uint64_t i = 0; i < n; ++i) {
+    const FeatureElement& el = complex.vertices[i];
+    for (int v = 0; v <= M; ++v) {
+      out->simplices[i * (M + 1) + v] = el.simplex.vertices[v];
+      out->bary[i * (M + 1) + v] = el.barycentric_coords[0][v];
+      out->lambda[i * (M + 1) + v] = NAN;
+    }
+    out->track_id[i] = el.track_id;
+    out->type[i] = el.type;
+    out->scalar[i] = el.scalar;
+    for (int a = 0; a < 16; ++a) (*attrs)[i * 16 + a] = el.attributes[a];
+  }
+  std::vector<uint32_t> edges;
+  for (const auto& conn : complex.connectivity)
+    if (conn.dimension == 1) edges = conn.indices;
+  out->n_edges = edges.size() / 2;
+  out->edges = (uint32_t*)std::malloc(sizeof(uint32_t) * (edges.size() + 2));
+  if (!edges.empty()) std::memcpy(out->edges, edges.data(), sizeof(uint32_t) * edges.size());
+  return 0;
+}
+
 }  // namespace
 
 extern "C" int ftk2ref_run(const orc_mesh* mesh, const orc_field* field, orc_result* out) {
@@ -170,3 +236,20 @@ extern "C" void ftk2ref_free(orc_result* r) {
   std::free(r->edges);
   std::memset(r, 0, sizeof(*r));
 }
+
+extern "C" int ftk2ref_run_tracked(const orc_tracked* in, orc_result* out, float** attrs) {
+  std::memset(out, 0, sizeof(*out));
+  *attrs = nullptr;
+  try {
+    if (in->m == 2) return in->dtype == ORC_F64 ? run_tracked<double, 2>(in, out, attrs)
+                                                : run_tracked<float, 2>(in, out, attrs);
+    if (in->m == 3) return in->dtype == ORC_F64 ? run_tracked<double, 3>(in, out, attrs)
+                                                : run_tracked<float, 3>(in, out, attrs);
+    return 2;
+  } catch (const std::exception& e) {
+    std::cerr << "ftk2ref_run_tracked: " << e.what() << std::endl;
+    return 1;
+  }
+}
+
+extern "C" void ftk2ref_free_attrs(float* attrs) { std::free(attrs); }
