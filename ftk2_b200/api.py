@@ -110,6 +110,14 @@ class ServerStatsC(C.Structure):
 REQ_EXTRACT, REQ_STREAM_PUSH = 0, 1
 
 
+ATTR_VALUE, ATTR_COMPONENT, ATTR_MAGNITUDE = 0, 1, 2
+
+
+class AttributeDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("component", C.c_int), ("slot", C.c_int), ("location", C.c_int),
+                ("data", C.c_void_p), ("nd", C.c_int), ("dims", C.c_uint64 * 6)]
+
+
 # name -> (restype, argtypes); every symbol include/ftk2b.h declares
 SIGNATURES = {
     "ftk2b_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -148,6 +156,8 @@ SIGNATURES = {
     "ftk2b_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStatsC)]),
     "ftk2b_server_last_error": (C.c_char_p, [C.c_void_p]),
     "ftk2b_server_destroy": (None, [C.c_void_p]),
+    "ftk2b_cp_attributes": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(C.c_uint64), C.c_uint32,
+                                      C.POINTER(AttributeDesc), C.c_void_p]),
     "ftk2b_cp_run_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                      C.POINTER(CPParams), C.POINTER(C.c_uint64)]),
     "ftk2b_cp_fetch_batch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
@@ -364,6 +374,7 @@ class Context:
         self._check(self.lib.ftk2b_cp_extract(self.h, C.byref(mesh), C.byref(field), C.byref(prm),
                                               C.byref(out)))
         try:
+            self._last_n = int(out.contents.n_features)
             return _result_from_c(out.contents)
         finally:
             self.lib.ftk2b_cp_result_free(out)
@@ -374,6 +385,7 @@ class Context:
         n, ne = C.c_uint64(), C.c_uint64()
         self._check(self.lib.ftk2b_cp_run(self.h, C.byref(mesh), C.byref(field), C.byref(prm),
                                           C.byref(n), C.byref(ne)))
+        self._last_n = int(n.value)
         return int(n.value), int(ne.value)
 
     def last_timing(self):
@@ -390,6 +402,36 @@ class Context:
         finally:
             self.lib.ftk2b_cp_result_free(out)
 
+
+    def attributes(self, mesh: MeshDesc, attrs, base_grid_dims=None) -> np.ndarray:
+        """Attributes at the features of the last run (ftk2b_cp_attributes).
+        attrs: list of (kind, array, component, slot); arrays in C order
+        (reversed Fortran shape), host numpy or device torch.  Returns
+        (n_features, 16) float32."""
+        n = self._last_n
+        keep = []
+        descs = (AttributeDesc * max(1, len(attrs)))()
+        for i, (kind, arr, comp, slot) in enumerate(attrs):
+            d = descs[i]
+            d.kind, d.component, d.slot = int(kind), int(comp), int(slot)
+            if hasattr(arr, "data_ptr"):
+                d.location, d.data = DEVICE, arr.data_ptr()
+                shape = tuple(arr.shape)
+            else:
+                arr = np.ascontiguousarray(arr)
+                d.location, d.data = HOST, arr.ctypes.data
+                shape = arr.shape
+            keep.append(arr)
+            d.nd = len(shape)
+            for q, v in enumerate(shape[::-1]):
+                d.dims[q] = int(v)
+        out = np.zeros((max(n, 1), 16), dtype=np.float32)
+        bg = None
+        if base_grid_dims is not None:
+            bg = (C.c_uint64 * 3)(*[int(x) for x in base_grid_dims] + [0] * (3 - len(base_grid_dims)))
+        self._check(self.lib.ftk2b_cp_attributes(self.h, C.byref(mesh), bg, len(attrs), descs,
+                                                 out.ctypes.data))
+        return out[:n]
 
     # ---- batches (ftk2b_cp_*_batch): n fields of uneven sizes in one pass
     @staticmethod

@@ -247,6 +247,9 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   for (auto& b : extra) v.push_back(&b);
   for (DevBuf* b : ext.bufs()) v.push_back(b);
   for (DevBuf* b : batch.bufs()) v.push_back(b);
+  v.push_back(&attr_out);
+  v.push_back(&attr_desc);
+  for (DevBuf& b : attr_stage) v.push_back(&b);
   return v;
 }
 
@@ -828,6 +831,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     }
     ctx->last.kind = FTK2B_MESH_REGULAR;
     ctx->last.m = m;
+    ctx->last.f64 = field->dtype == FTK2B_F64;
     ctx->last.n = h[kCountFeatures];
     ctx->last.ne = prm->want_edges ? h[kCountEdges] : 0;
     ctx->last.n_roots = h[kCountRoots];

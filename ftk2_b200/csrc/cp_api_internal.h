@@ -124,7 +124,7 @@ struct BatchCtx {
 };
 
 struct LastRun {
-  int kind = 0, m = 0;
+  int kind = 0, m = 0, f64 = 0;
   uint64_t n = 0, ne = 0, n_roots = 0, n_simplices = 0;
   double device_ms = 0;
   int classify = 0, want_edges = 1;
@@ -155,6 +155,7 @@ struct ftk2b_ctx {
       simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains, edge_slots;
   ftk2b::DevBuf tstats, runs;  // cull mode 1 scratch (tile statistics, run list + count)
   std::vector<ftk2b::DevBuf> extra;
+  ftk2b::DevBuf attr_out, attr_desc, attr_stage[16];  // ftk2b_cp_attributes
   ftk2b::ExtCache ext;
   ftk2b::BatchCtx batch;
   ftk2b::LastRun last;

@@ -1132,6 +1132,7 @@ ftk2b_status result_extruded_t(ftk2b_stream* s, ftk2b_cp_result** out) {
   ctx->launches += nl;
   ctx->last.kind = FTK2B_MESH_EXTRUDED;
   ctx->last.m = M;
+  ctx->last.f64 = s->dtype == FTK2B_F64;
   ctx->last.n = n;
   ctx->last.ne = s->prm.want_edges ? ne : 0;
   ctx->last.n_roots = ctx->h_counters[kCountRoots];
@@ -1314,6 +1315,7 @@ ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk
     }
     ctx->last.kind = FTK2B_MESH_EXTRUDED;
     ctx->last.m = M;
+    ctx->last.f64 = field->dtype == FTK2B_F64;
     ctx->last.n = h[kCountFeatures];
     ctx->last.ne = prm->want_edges ? h[kCountEdges] : 0;
     ctx->last.n_roots = h[kCountRoots];

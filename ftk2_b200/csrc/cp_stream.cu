@@ -396,6 +396,7 @@ ftk2b_status result_regular(ftk2b_stream* s, ftk2b_cp_result** out) {
   // hand the canonical buffers to the context's fetch
   ctx->last.kind = FTK2B_MESH_REGULAR;
   ctx->last.m = M;
+  ctx->last.f64 = s->dtype == FTK2B_F64;
   ctx->last.n = n;
   ctx->last.ne = s->prm.want_edges ? ne : 0;
   ctx->last.n_roots = ctx->h_counters[kCountRoots];

@@ -189,6 +189,34 @@ ftk2b_status ftk2b_ctx_last_timing(ftk2b_ctx* ctx, double* extract_ms, double* t
  * copy-back (ftk2b_cp_fetch). */
 ftk2b_status ftk2b_ctx_last_phases(ftk2b_ctx* ctx, double* phase_ms);
 
+/* --- attributes ------------------------------------------------------------
+ * The values the reference records into FeatureElement::attributes for each
+ * accepted simplex (AttributeSpec, predicate.hpp:34-40; engine.hpp:1143-1199),
+ * computed on the device for the features of the last ftk2b_cp_run /
+ * ftk2b_cp_extract on the context: sum over the feature's vertices of its
+ * float barycentric times the array's value there, in the field's precision.
+ *   COMPONENT: data is [ncomp, grid dims...]; value = component `component`
+ *   MAGNITUDE: data is [ncomp, grid dims...]; value = Euclidean norm
+ *   VALUE:     1-D data indexed by vertex id, else read at the vertex's grid
+ *              coordinates minus the regular mesh's offset
+ * (the reference picks COMPONENT / MAGNITUDE when the array's first dimension
+ * is 1..16 and component >= 0 / type "magnitude", VALUE otherwise).  data has
+ * the field's dtype; grid coordinates of extruded meshes need the spatial grid
+ * (base_grid_dims) of an extruded regular grid, else only 1-D VALUE arrays.
+ * out receives 16 floats per feature (slots not given stay 0). */
+enum { FTK2B_ATTR_VALUE = 0, FTK2B_ATTR_COMPONENT = 1, FTK2B_ATTR_MAGNITUDE = 2 };
+typedef struct {
+  int kind;           /* FTK2B_ATTR_* */
+  int component;      /* COMPONENT */
+  int slot;           /* 0..15 */
+  int location;       /* FTK2B_HOST or FTK2B_DEVICE */
+  const void* data;
+  int nd;
+  uint64_t dims[6];   /* Fortran order, first fastest */
+} ftk2b_attribute_desc;
+ftk2b_status ftk2b_cp_attributes(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const uint64_t* base_grid_dims,
+                                 uint32_t n_attrs, const ftk2b_attribute_desc* attrs, float* out);
+
 /* --- batches ---------------------------------------------------------------
  * No counterpart in the reference (one engine per field).  n independent
  * regular-mesh fields of uneven sizes, 2D and 3D mixed, extracted together:

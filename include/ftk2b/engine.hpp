@@ -344,97 +344,53 @@ class SimplicialEngine {
   template <typename Array>
   using elem_t = std::remove_cv_t<std::remove_pointer_t<decltype(std::declval<const Array&>().pdata())>>;
 
-  // ndarray's Fortran element access f(i0, i1, ...) with as many indices as
-  // given: offset = sum_k idx_k * prod_{j<k} dimf(j)
-  template <typename Array>
-  static double fetch(const Array& a, const uint64_t* idx, int n) {
-    uint64_t off = 0, mul = 1;
-    for (int k = 0; k < n; ++k) {
-      off += idx[k] * mul;
-      mul *= (k < (int)a.nd()) ? (uint64_t)a.dimf(k) : 1;
-    }
-    return (double)a.pdata()[off];
-  }
-
-  // Spacetime grid coordinates of a vertex (get_vertex_coordinates of the
-  // regular mesh, or of the extruded mesh over a regular base) and the
-  // offset that legacy arrays subtract (engine.hpp:999-1009, 1036-1038).
-  int vertex_coords(uint64_t vid, uint64_t* c, uint64_t* off) const {
-    const auto* ext = dynamic_cast<const ExtrudedSimplicialMesh*>(mesh_.get());
-    const RegularSimplicialMesh* reg = ext ? ext->regular_base() : dynamic_cast<const RegularSimplicialMesh*>(mesh_.get());
-    if (!reg) return 0;
-    const std::vector<uint64_t>& g = reg->get_global_dims();
-    int n = 0;
-    uint64_t v = vid;
-    if (ext) {
-      v = vid % ext->vertex_stride();
-      for (size_t k = 0; k < g.size(); ++k, ++n) {
-        c[n] = v % g[k];
-        v /= g[k];
-        off[n] = 0;
-      }
-      c[n] = vid / ext->vertex_stride();
-      off[n++] = 0;
-      return n;
-    }
-    for (size_t k = 0; k < g.size(); ++k, ++n) {
-      c[n] = v % g[k];
-      v /= g[k];
-      off[n] = reg->get_offset()[k];
-    }
-    return n;
-  }
-
-  // FeatureElement::attributes at each feature, interpolated with the float
-  // barycentrics the element stores, in the field precision T, as
-  // extract_simplex does for every accepted simplex (engine.hpp:1143-1199):
-  // one component of a multicomponent source, its magnitude, or the value of
-  // a plain (or per-vertex) array.  Runs on the host arrays, over the
-  // accepted features only.
+  // FeatureElement::attributes at each feature (engine.hpp:1143-1199),
+  // interpolated on the device by ftk2b_cp_attributes with the float
+  // barycentrics the elements store, in the field precision T.  The kind of
+  // each spec follows the reference: a source whose first dimension is 1..16
+  // is multicomponent, read as one component (component >= 0) or as its
+  // magnitude (type "magnitude"); anything else is read as a plain value.
   template <typename Array>
   void record_attributes(const std::map<std::string, Array>& data) {
     attrs_.clear();
     const ftk2b_cp_result* r = result_.get();
     if (!r || pred_.attributes.empty()) return;
-    attrs_.assign(16 * (size_t)r->n_features, 0.f);
-    const int k = r->m + 1;
+    std::vector<ftk2b_attribute_desc> descs;
+    std::vector<std::vector<T>> conv;
+    conv.reserve(pred_.attributes.size());
     for (const AttributeSpec& spec : pred_.attributes) {
       if (spec.slot < 0 || spec.slot >= 16) continue;
       auto it = data.find(spec.source);
       if (it == data.end()) continue;
       const Array& a = it->second;
+      if (a.nd() < 1 || a.nd() > 6) throw Error(FTK2B_UNSUPPORTED, "attribute arrays have 1 to 6 dimensions");
       const bool multicomp = a.nd() >= 2 && a.dimf(0) >= 1 && a.dimf(0) <= 16;
-      for (uint64_t i = 0; i < r->n_features; ++i) {
-        T acc = 0;
-        for (int v = 0; v < k; ++v) {
-          const uint64_t vid = r->simplices[i * k + v];
-          uint64_t c[5], off[5], idx[6];
-          const int n = vertex_coords(vid, c, off);
-          T val = 0;
-          if (multicomp && spec.component >= 0) {
-            idx[0] = (uint64_t)spec.component;
-            for (int q = 0; q < n; ++q) idx[q + 1] = c[q];
-            val = (T)fetch(a, idx, n + 1);
-          } else if (multicomp && spec.type == "magnitude") {
-            T sq = 0;
-            for (uint64_t comp = 0; comp < (uint64_t)a.dimf(0); ++comp) {
-              idx[0] = comp;
-              for (int q = 0; q < n; ++q) idx[q + 1] = c[q];
-              const T cv = (T)fetch(a, idx, n + 1);
-              sq += cv * cv;
-            }
-            val = std::sqrt(sq);
-          } else if (a.nd() == 1) {
-            val = (T)a.pdata()[vid];
-          } else {
-            for (int q = 0; q < n; ++q) idx[q] = c[q] - off[q];
-            val = (T)fetch(a, idx, n);
-          }
-          acc += r->barycentric[i * k + v] * val;
-        }
-        attrs_[16 * (size_t)i + spec.slot] = (float)acc;
+      ftk2b_attribute_desc d;
+      std::memset(&d, 0, sizeof(d));
+      d.kind = (multicomp && spec.component >= 0) ? FTK2B_ATTR_COMPONENT
+               : (multicomp && spec.type == "magnitude") ? FTK2B_ATTR_MAGNITUDE
+                                                         : FTK2B_ATTR_VALUE;
+      d.component = spec.component;
+      d.slot = spec.slot;
+      d.location = FTK2B_HOST;
+      d.nd = (int)a.nd();
+      for (int q = 0; q < d.nd; ++q) d.dims[q] = a.dimf(q);
+      if (std::is_same<elem_t<Array>, T>::value) {
+        d.data = a.pdata();
+      } else {
+        conv.emplace_back(a.pdata(), a.pdata() + a.nelem());
+        d.data = conv.back().data();
       }
+      descs.push_back(d);
     }
+    const auto* ext = dynamic_cast<const ExtrudedSimplicialMesh*>(mesh_.get());
+    const ftk2b_mesh_desc md = mesh_->desc();
+    std::vector<uint64_t> bg;
+    if (ext && ext->regular_base()) bg = ext->regular_base()->get_global_dims();
+    attrs_.assign(16 * (size_t)r->n_features, 0.f);
+    const ftk2b_status st = ftk2b_cp_attributes(ctx_.get(), &md, bg.empty() ? nullptr : bg.data(),
+                                                (uint32_t)descs.size(), descs.data(), attrs_.data());
+    if (st != FTK2B_OK) throw Error(st, ftk2b_last_error(ctx_.get()));
   }
 
   // The extruded mesh over a regular base: the reference reads the arrays at
