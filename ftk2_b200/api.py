@@ -107,6 +107,16 @@ class ServerStatsC(C.Structure):
                 ("max_in_flight", C.c_int)]
 
 
+class ContourResultC(C.Structure):
+    _fields_ = [
+        ("n_features", C.c_uint64), ("simplices", C.POINTER(C.c_uint64)), ("lambda_", C.POINTER(C.c_double)),
+        ("barycentric", C.POINTER(C.c_float)), ("track_id", C.POINTER(C.c_uint64)),
+        ("scalar", C.POINTER(C.c_float)), ("cell_dim", C.c_int), ("n_cells", C.c_uint64),
+        ("cells", C.POINTER(C.c_uint32)), ("n_tracks", C.c_uint64), ("n_simplices", C.c_uint64),
+        ("device_ms", C.c_double),
+    ]
+
+
 REQ_EXTRACT, REQ_STREAM_PUSH = 0, 1
 
 
@@ -131,6 +141,9 @@ SIGNATURES = {
     "ftk2b_cp_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                    C.POINTER(CPParams), C.POINTER(C.POINTER(CPResultC))]),
     "ftk2b_cp_result_free": (None, [C.POINTER(CPResultC)]),
+    "ftk2b_contour_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc), C.c_double,
+                                        C.c_double, C.POINTER(C.POINTER(ContourResultC))]),
+    "ftk2b_contour_result_free": (None, [C.POINTER(ContourResultC)]),
     "ftk2b_cp_run": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                C.POINTER(CPParams), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
@@ -321,6 +334,39 @@ def _result_from_c(r: CPResultC) -> CPResult:
         n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
 
 
+@dataclass
+class ContourResult:
+    """Flattened FeatureComplex of a level-set extraction (ContourPredicate):
+    features are mesh edges, cells the manifold cells of get_complex."""
+    simplices: np.ndarray      # (n, 2) uint64 edge vertex ids, simplex order
+    lam: np.ndarray            # (n, 2) float64 barycentrics in the field precision
+    bary: np.ndarray           # (n, 2) float32 as FeatureElement stores them
+    track_id: np.ndarray       # (n,) uint64
+    scalar: np.ndarray         # (n,) float32 (the threshold)
+    cells: np.ndarray          # (c, cell_dim + 1) uint32 feature indices
+    n_tracks: int = 0
+    n_simplices: int = 0
+    device_ms: float = 0.0
+
+
+def _contour_from_c(r: ContourResultC) -> ContourResult:
+    n, k, c = int(r.n_features), int(r.cell_dim) + 1, int(r.n_cells)
+
+    def arr(ptr, count, dt):
+        if count == 0:
+            return np.zeros(0, dtype=dt)
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+    return ContourResult(
+        simplices=arr(r.simplices, 2 * n, np.uint64).reshape(n, 2),
+        lam=arr(r.lambda_, 2 * n, np.float64).reshape(n, 2),
+        bary=arr(r.barycentric, 2 * n, np.float32).reshape(n, 2),
+        track_id=arr(r.track_id, n, np.uint64),
+        scalar=arr(r.scalar, n, np.float32),
+        cells=arr(r.cells, k * c, np.uint32).reshape(c, k),
+        n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
+
+
 class Context:
     """One ftk2b_ctx: a device, a CUDA stream and reusable device buffers."""
 
@@ -378,6 +424,21 @@ class Context:
             return _result_from_c(out.contents)
         finally:
             self.lib.ftk2b_cp_result_free(out)
+
+    def contour(self, mesh: MeshDesc, field, threshold: float = 0.0, sos_q: float = 1e6) -> ContourResult:
+        """Level sets (ContourPredicate<T>) on a regular mesh.  field: a
+        FieldDesc (ncomp 1, LAYOUT_SEPARATE), or the scalar array itself (numpy
+        or torch, C-order of reversed Fortran shape)."""
+        keep: list = []
+        if not isinstance(field, FieldDesc):
+            field = field_desc([field], LAYOUT_SEPARATE, 1, keep=keep)
+        out = C.POINTER(ContourResultC)()
+        self._check(self.lib.ftk2b_contour_extract(self.h, C.byref(mesh), C.byref(field), float(threshold),
+                                                   float(sos_q), C.byref(out)))
+        try:
+            return _contour_from_c(out.contents)
+        finally:
+            self.lib.ftk2b_contour_result_free(out)
 
     def run(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None):
         """Device pipeline only; results stay on the device until fetch()."""

@@ -250,6 +250,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   v.push_back(&attr_out);
   v.push_back(&attr_desc);
   for (DevBuf& b : attr_stage) v.push_back(&b);
+  for (DevBuf& b : contour) v.push_back(&b);
   return v;
 }
 

@@ -156,6 +156,7 @@ struct ftk2b_ctx {
   ftk2b::DevBuf tstats, runs;  // cull mode 1 scratch (tile statistics, run list + count)
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::DevBuf attr_out, attr_desc, attr_stage[16];  // ftk2b_cp_attributes
+  ftk2b::DevBuf contour[20];  // ftk2b_contour_extract scratch and outputs
   ftk2b::ExtCache ext;
   ftk2b::BatchCtx batch;
   ftk2b::LastRun last;

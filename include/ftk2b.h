@@ -351,6 +351,36 @@ ftk2b_status ftk2b_cp_features_noalloc(const ftk2b_mesh_desc* mesh, const ftk2b_
                                        double sos_q, void* stream, uint64_t* keys, double* lambda,
                                        uint32_t capacity, uint32_t* count, uint64_t* n_features);
 
+/* --- level sets (ContourPredicate<T>) -------------------------------------
+ * Replaces SimplicialEngine<T, ContourPredicate<T>>::execute + get_complex
+ * (engine.hpp:95-215, 822-996; predicate.hpp:135-183) on a regular mesh of
+ * 3 (2D+t) or 4 (3D+t) dims.  field: ncomp 1, layout SEPARATE, comp[0] the
+ * scalar array (nd == mesh dims, indexed by local coordinates; or nd 1,
+ * indexed by global vertex id).  Features are the mesh edges whose endpoints
+ * have different simulation-of-simplicity signs of value - threshold, in
+ * simplex order; cells are the manifold cells of get_complex (triangles on
+ * 2D+t, tets on 3D+t) as sorted rows of feature indices, sorted and unique;
+ * track ids are the components' smallest feature index.  Where the reference
+ * numbers nodes in the order its patching meets them (2D+t quads cut along
+ * the diagonal from their first node), this follows its sequential order. */
+typedef struct {
+  uint64_t n_features;
+  uint64_t* simplices;    /* 2 per feature: the edge's vertex ids, ascending */
+  double* lambda;         /* 2 per feature: the barycentrics in the field precision, widened */
+  float* barycentric;     /* 2 per feature, as FeatureElement::barycentric_coords[0] */
+  uint64_t* track_id;     /* n */
+  float* scalar;          /* n: the threshold as float */
+  int cell_dim;           /* 2 (triangles, 2D+t) or 3 (tets, 3D+t) */
+  uint64_t n_cells;
+  uint32_t* cells;        /* (cell_dim + 1) per cell */
+  uint64_t n_tracks;
+  uint64_t n_simplices;   /* edges of the mesh: the unit of work */
+  double device_ms;       /* device time of the pipeline */
+} ftk2b_contour_result;
+ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                                   double threshold, double sos_q, ftk2b_contour_result** out);
+void ftk2b_contour_result_free(ftk2b_contour_result* r);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,7 +2,8 @@
 
 Loads oracle/_ref/libftk2ref.so (the reference engine, built from the
 reference's own headers) and oracle/_build/libcporacle.so (our C restatement,
-cp_oracle.c).  Only tests/, the smoke check and bench.py's CPU-baseline leg
+cp_oracle.c); oracle/_ref/libftk2refcuda.so (the reference's own GPU engine)
+is loaded only to time the incumbent GPU path.  Only tests/, the smoke check and bench.py's CPU-baseline leg
 import this module; the product never does.
 """
 from __future__ import annotations
@@ -15,6 +16,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libftk2ref.so")
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libftk2refcuda.so")
+# the same engine with its worker pool sized 1: the level-set oracle
+REF1T_LIB = os.path.join(HERE, "_ref", "libftk2ref1t.so")
 ORC_LIB = os.path.join(HERE, "_build", "libcporacle.so")
 
 MESH_REGULAR, MESH_EXTRUDED = 0, 1
@@ -199,6 +203,105 @@ def _run(path: str, prefix: str, mesh: OrcMesh, field: OrcField) -> CPResult:
 def run_reference(mesh: OrcMesh, field: OrcField) -> CPResult:
     """The reference's own engine (execute + get_complex)."""
     return _run(REF_LIB, "ftk2ref", mesh, field)
+
+
+def _ref_cuda() -> C.CDLL:
+    lib = _load(REF_CUDA_LIB, "ftk2refcuda")
+    if not hasattr(lib, "_typed"):
+        lib.ftk2refcuda_run.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.POINTER(OrcResult),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.ftk2refcuda_time_kernel.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.c_int,
+                                                C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        lib.ftk2refcuda_time_kernel.restype = C.c_int
+        lib._typed = True
+    return lib
+
+
+def run_reference_cuda(mesh: OrcMesh, field: OrcField):
+    """The reference's own GPU engine: execute_cuda + get_complex on separate
+    component arrays of a regular mesh (engine.hpp:273-425).  Returns the
+    complex and the wall times of execute_cuda and get_complex in ms.  The
+    reference ends the process on a CUDA error, so callers run this in a
+    child process."""
+    lib = _ref_cuda()
+    res = OrcResult()
+    ex, cx = C.c_double(0), C.c_double(0)
+    rc = lib.ftk2refcuda_run(C.byref(mesh), C.byref(field), C.byref(res), C.byref(ex), C.byref(cx))
+    if rc != 0:
+        raise RuntimeError(f"ftk2refcuda_run failed with status {rc}")
+    try:
+        n, k, e = int(res.n), int(res.m) + 1, int(res.n_edges)
+
+        def arr(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        out = CPResult(
+            simplices=arr(res.simplices, n * k, np.uint64).reshape(n, k),
+            bary=arr(res.bary, n * k, np.float32).reshape(n, k),
+            lam=np.full((n, k), np.nan),
+            track_id=arr(res.track_id, n, np.uint64),
+            type=arr(res.type, n, np.uint32),
+            scalar=arr(res.scalar, n, np.float32),
+            edges=arr(res.edges, 2 * e, np.uint32).reshape(e, 2),
+        )
+    finally:
+        lib.ftk2refcuda_free(C.byref(res))
+    return out, ex.value, cx.value
+
+
+def time_reference_cuda_kernel(mesh: OrcMesh, field: OrcField, reps: int = 3):
+    """Mean CUDA-event time (ms) of the reference's extraction kernel
+    (cuda_engine.hpp:366-493) over `reps` launches, and its node count."""
+    lib = _ref_cuda()
+    ms, nn = C.c_double(0), C.c_int(0)
+    rc = lib.ftk2refcuda_time_kernel(C.byref(mesh), C.byref(field), int(reps), C.byref(ms), C.byref(nn))
+    if rc != 0:
+        raise RuntimeError(f"ftk2refcuda_time_kernel failed with status {rc}")
+    return ms.value, int(nn.value)
+
+
+class OrcConn(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n", C.c_uint64), ("idx", C.POINTER(C.c_uint32))]
+
+
+def run_reference_contour(mesh: OrcMesh, field: OrcField, threshold: float, one_thread: bool = True):
+    """The reference's own engine with ContourPredicate<T> on a regular mesh
+    (execute + get_complex): the features (mesh edges) and the manifold cells,
+    an (n, dim+1) array of feature indices.  By default the one-worker build:
+    with several workers the reference's patching races on its node map."""
+    lib = _load(REF1T_LIB if one_thread else REF_LIB, "ftk2ref")
+    fn = lib.ftk2ref_run_contour
+    fn.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.c_double, C.POINTER(OrcResult), C.POINTER(OrcConn)]
+    fn.restype = C.c_int
+    lib.ftk2ref_free_conn.argtypes = [C.POINTER(OrcConn)]
+    res, conn = OrcResult(), OrcConn()
+    rc = fn(C.byref(mesh), C.byref(field), float(threshold), C.byref(res), C.byref(conn))
+    if rc != 0:
+        raise RuntimeError(f"ftk2ref_run_contour failed with status {rc}")
+    try:
+        n, k = int(res.n), int(conn.dim) + 1
+
+        def arr(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        out = CPResult(
+            simplices=arr(res.simplices, 2 * n, np.uint64).reshape(n, 2),
+            bary=arr(res.bary, 2 * n, np.float32).reshape(n, 2),
+            lam=arr(res.lambda_, 2 * n, np.float64).reshape(n, 2),
+            track_id=arr(res.track_id, n, np.uint64),
+            type=arr(res.type, n, np.uint32),
+            scalar=arr(res.scalar, n, np.float32),
+            edges=np.zeros((0, 2), dtype=np.uint32),
+        )
+        cells = arr(conn.idx, int(conn.n) * k, np.uint32).reshape(-1, k)
+    finally:
+        lib.ftk2ref_free(C.byref(res))
+        lib.ftk2ref_free_conn(C.byref(conn))
+    return out, cells
 
 
 def run_restatement(mesh: OrcMesh, field: OrcField) -> CPResult:

@@ -103,6 +103,21 @@ void ftk2ref_free(orc_result* r);
 int ftk2ref_run_tracked(const orc_tracked* in, orc_result* out, float** attrs);
 void ftk2ref_free_attrs(float* attrs);
 
+/* Level sets (ContourPredicate<T>, predicate.hpp:135-183) on a regular mesh:
+ * field->comp[0] is the scalar array (layout SEPARATE, ncomp 1).  Features are
+ * mesh edges (m = 1); lambda holds the barycentrics the predicate used
+ * (solver output, or 0.5 where it falls back), widened.  conn receives the
+ * manifold cells of get_complex: triangles (dim 2) on 2D+t meshes, tets
+ * (dim 3) on 3D+t meshes, as sorted rows of feature indices. */
+typedef struct {
+  int dim;
+  uint64_t n;
+  uint32_t* idx;            /* (dim+1)*n */
+} orc_conn;
+int ftk2ref_run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, orc_result* out,
+                        orc_conn* conn);
+void ftk2ref_free_conn(orc_conn* c);
+
 /* own restatement */
 int cporacle_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);
 void cporacle_free(orc_result* r);

@@ -31,6 +31,17 @@
 
 #include "oracle_api.h"
 
+#ifdef FTK2REF_SINGLE_THREAD
+// One-worker build: the reference's parallel_for and get_num_threads
+// (parallel.hpp:14-67) size their pools by std::thread::hardware_concurrency(),
+// which answers 1 here, as on a one-core host, so every engine loop runs
+// sequentially.  Linked with -Bsymbolic-functions so the engine's calls bind
+// to this definition.  Used for the level-set path, whose multi-threaded
+// patching reads active_nodes_ without its lock while other workers insert
+// (engine.hpp:1229-1244) and numbers boundary nodes in thread-arrival order.
+unsigned int std::thread::hardware_concurrency() noexcept { return 1; }
+#endif
+
 namespace {
 
 template <typename T>
@@ -211,7 +222,102 @@ int run_tracked(const orc_tracked* in, orc_result* out, float** attrs) {
   return 0;
 }
 
+// Level sets: SimplicialEngine<T, ContourPredicate<T>> on a regular mesh
+// (the reference's tests/test_examples.cpp:225-256 set-up), features and the
+// manifold cells of get_complex flattened.
+template <typename T>
+int run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, orc_result* out, orc_conn* conn) {
+  using namespace ftk2;
+  std::vector<uint64_t> dims, off, glob;
+  for (int i = 0; i < mesh->ndims; ++i) {
+    dims.push_back(mesh->local_dims[i]);
+    off.push_back(mesh->offset[i]);
+    glob.push_back(mesh->global_dims[i]);
+  }
+  auto reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
+  ContourPredicate<T> pred;
+  pred.var_name = "S";
+  pred.threshold = (T)threshold;
+  pred.sos_q = field->sos_q;
+  std::map<std::string, ftk::ndarray<T>> data;
+  data["S"] = make_array<T>(field->comp[0], field->nd, field->dims);
+  SimplicialEngine<T, ContourPredicate<T>> engine(reg, pred);
+  std::streambuf* saved = std::cout.rdbuf();
+  std::ostringstream sink;
+  std::cout.rdbuf(sink.rdbuf());
+  engine.execute(data, {"S"});
+  FeatureComplex complex = engine.get_complex();
+  std::cout.rdbuf(saved);
+
+  const uint64_t n = complex.vertices.size();
+  const auto& a = data.at("S");
+  out->m = 1;
+  out->n = n;
+  out->simplices = (uint64_t*)std::malloc(sizeof(uint64_t) * (2 * n + 1));
+  out->bary = (float*)std::malloc(sizeof(float) * (2 * n + 1));
+  out->lambda = (double*)std::malloc(sizeof(double) * (2 * n + 1));
+  out->track_id = (uint64_t*)std::malloc(sizeof(uint64_t) * (n + 1));
+  out->type = (uint32_t*)std::malloc(sizeof(uint32_t) * (n + 1));
+  out->scalar = (float*)std::malloc(sizeof(float) * (n + 1));
+  out->n_tested = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const FeatureElement& el = complex.vertices[i];
+    T values[2][1];
+    for (int v = 0; v < 2; ++v) {
+      out->simplices[2 * i + v] = el.simplex.vertices[v];
+      out->bary[2 * i + v] = el.barycentric_coords[0][v];
+      T x;
+      if (a.nd() == 1) {
+        x = a[el.simplex.vertices[v]];
+      } else {
+        std::vector<double> c = reg->get_vertex_coordinates(el.simplex.vertices[v]);
+        for (size_t k = 0; k < c.size(); ++k) c[k] -= (double)off[k];
+        x = c.size() == 3 ? a.f(c[0], c[1], c[2]) : a.f(c[0], c[1], c[2], c[3]);
+      }
+      values[v][0] = x - pred.threshold;
+    }
+    // the barycentrics ContourPredicate::extract_it stores (predicate.hpp:149)
+    T lambda[2];
+    if (!ZeroCrossingSolver<1, T>::solve(values, lambda)) lambda[0] = lambda[1] = (T)0.5;
+    out->lambda[2 * i] = (double)lambda[0];
+    out->lambda[2 * i + 1] = (double)lambda[1];
+    out->track_id[i] = el.track_id;
+    out->type[i] = el.type;
+    out->scalar[i] = el.scalar;
+  }
+  out->n_edges = 0;
+  out->edges = (uint32_t*)std::malloc(sizeof(uint32_t) * 2);
+  conn->dim = mesh->ndims - 1;
+  conn->n = 0;
+  std::vector<uint32_t> cells;
+  for (const auto& c : complex.connectivity)
+    if (c.dimension == conn->dim) cells = c.indices;
+  conn->n = cells.size() / (conn->dim + 1);
+  conn->idx = (uint32_t*)std::malloc(sizeof(uint32_t) * (cells.size() + 1));
+  if (!cells.empty()) std::memcpy(conn->idx, cells.data(), sizeof(uint32_t) * cells.size());
+  return 0;
+}
+
 }  // namespace
+
+extern "C" int ftk2ref_run_contour(const orc_mesh* mesh, const orc_field* field, double threshold,
+                                   orc_result* out, orc_conn* conn) {
+  std::memset(out, 0, sizeof(*out));
+  std::memset(conn, 0, sizeof(*conn));
+  if (mesh->kind != ORC_MESH_REGULAR || (mesh->ndims != 3 && mesh->ndims != 4)) return 3;
+  try {
+    return field->dtype == ORC_F64 ? run_contour<double>(mesh, field, threshold, out, conn)
+                                   : run_contour<float>(mesh, field, threshold, out, conn);
+  } catch (const std::exception& e) {
+    std::cerr << "ftk2ref_run_contour: " << e.what() << std::endl;
+    return 1;
+  }
+}
+
+extern "C" void ftk2ref_free_conn(orc_conn* c) {
+  std::free(c->idx);
+  std::memset(c, 0, sizeof(*c));
+}
 
 extern "C" int ftk2ref_run(const orc_mesh* mesh, const orc_field* field, orc_result* out) {
   std::memset(out, 0, sizeof(*out));

@@ -18,12 +18,75 @@
 #include <vector>
 #include <initializer_list>
 
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
+
 namespace ftk {
+
+#ifdef __CUDACC__
+// Device copies for the reference's CUDA engine (engine.hpp:327-345), built
+// only into the incumbent-GPU timing driver: copy_to_device / to_device keep
+// one device copy of the buffer, get_devptr returns it, get_lattice().prod_
+// holds the Fortran strides in the reversed order the engine indexes them.
+enum { NDARRAY_DEVICE_CUDA = 1 };
+struct lattice_t {
+  std::vector<size_t> prod_;
+};
+#endif
 
 template <typename T>
 class ndarray {
 public:
   ndarray() = default;
+#ifdef __CUDACC__
+  ndarray(const ndarray& o) : dims_(o.dims_), buf_(o.buf_) {}
+  ndarray(ndarray&& o) noexcept : dims_(std::move(o.dims_)), buf_(std::move(o.buf_)), dev_(o.dev_) { o.dev_ = nullptr; }
+  ndarray& operator=(const ndarray& o) {
+    if (this != &o) {
+      dims_ = o.dims_;
+      buf_ = o.buf_;
+      release();
+    }
+    return *this;
+  }
+  ndarray& operator=(ndarray&& o) noexcept {
+    if (this != &o) {
+      release();
+      dims_ = std::move(o.dims_);
+      buf_ = std::move(o.buf_);
+      dev_ = o.dev_;
+      o.dev_ = nullptr;
+    }
+    return *this;
+  }
+  ~ndarray() { release(); }
+  void copy_to_device(int, int) {
+    release();
+    if (cudaMalloc(&dev_, sizeof(T) * (buf_.size() ? buf_.size() : 1)) != cudaSuccess) {
+      dev_ = nullptr;
+      return;
+    }
+    cudaMemcpy(dev_, buf_.data(), sizeof(T) * buf_.size(), cudaMemcpyHostToDevice);
+  }
+  void to_device(int a, int b) { copy_to_device(a, b); }
+  void* get_devptr() const { return dev_; }
+  lattice_t get_lattice() const {
+    lattice_t l;
+    const size_t n = dims_.size();
+    l.prod_.assign(n, 1);
+    for (size_t k = 0; k < n; ++k) {
+      size_t p = 1;
+      for (size_t j = 0; j + 1 + k < n; ++j) p *= dims_[j];
+      l.prod_[k] = p;
+    }
+    return l;
+  }
+  void release() {
+    if (dev_) cudaFree(dev_);
+    dev_ = nullptr;
+  }
+#endif
   explicit ndarray(const std::vector<size_t>& dims) { reshapef(dims); }
   ndarray(std::initializer_list<size_t> dims) { reshapef(std::vector<size_t>(dims)); }
 
@@ -70,6 +133,9 @@ private:
 
   std::vector<size_t> dims_;
   std::vector<T> buf_;
+#ifdef __CUDACC__
+  void* dev_ = nullptr;
+#endif
 };
 
 }  // namespace ftk

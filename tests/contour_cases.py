@@ -1,0 +1,97 @@
+"""Seeded inputs of the level-set (contour) parity cases.
+
+Each maker returns a dict: field (C-order, reversed Fortran shape of the local
+mesh), local_dims, offset, global_dims, threshold, q.  The moving sphere is
+the reference's own level-set example (tests/test_examples.cpp:225-256,
+66418 feature vertices); the others are seeded Gaussian sums, an integer field
+full of exact zeros (simulation-of-simplicity ties), a sub-box mesh with an
+offset, a single time layer and a field with no crossing at all.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def gaussian_potential(dims, nt, seed, n_blobs, dtype, sigma=(2.0, 6.0), drift=0.5):
+    """Sum of drifting Gaussians, shape (nt, [nz,] ny, nx)."""
+    rng = np.random.default_rng(seed)
+    d = len(dims)
+    centers = rng.uniform(0, 1, (n_blobs, d)) * np.array(dims, dtype=np.float64)
+    amps = rng.standard_normal(n_blobs)
+    sig = rng.uniform(sigma[0], sigma[1], n_blobs)
+    vel = rng.uniform(-drift, drift, (n_blobs, d))
+    axes = [np.arange(n, dtype=np.float64) for n in dims]
+    out = np.zeros((nt,) + tuple(dims[::-1]), dtype=np.float64)
+    for t in range(nt):
+        for b in range(n_blobs):
+            c = centers[b] + vel[b] * t
+            r2 = 0.0
+            for i in range(d):
+                shape = [1] * d
+                shape[d - 1 - i] = dims[i]
+                r2 = r2 + ((axes[i] - c[i]) ** 2).reshape(shape)
+            out[t] += amps[b] * np.exp(-r2 / (2.0 * sig[b] ** 2))
+    return out.astype(dtype)
+
+
+def moving_sphere():
+    """The reference's levelset_3d test field: |p - c(t)| - 8 on 32^3 x 10,
+    c(t) = (16 + 0.2 t, 16, 16), float, threshold 0."""
+    DW = DH = DD = 32
+    DT = 10
+    x = np.arange(DW, dtype=np.float32)
+    S = np.empty((DT, DD, DH, DW), dtype=np.float32)
+    for t in range(DT):
+        cx = np.float32(16.0) + np.float32(t) * np.float32(0.2)
+        c16 = np.float32(16.0)
+        dx = (x - cx).astype(np.float64)
+        dy = (x - c16).astype(np.float64)
+        dz = (x - c16).astype(np.float64)
+        s = dx[None, None, :] ** 2 + dy[None, :, None] ** 2
+        s = s + dz[:, None, None] ** 2
+        S[t] = np.sqrt(s).astype(np.float32) - np.float32(8.0)
+    return dict(field=S, local_dims=[DW, DH, DD, DT], offset=None, global_dims=None, threshold=0.0, q=1e6)
+
+
+def gauss_2d_f64():
+    f = gaussian_potential((40, 36), 6, seed=11, n_blobs=12, dtype=np.float64)
+    return dict(field=f, local_dims=[40, 36, 6], offset=None, global_dims=None, threshold=0.05, q=1e6)
+
+
+def gauss_3d_f32_offset():
+    """A 12x10x9x4 sub-box at offset (3,4,2,1) of a 20x18x16x5 mesh; the
+    array holds the sub-box's values."""
+    g = gaussian_potential((20, 18, 16), 5, seed=5, n_blobs=10, dtype=np.float32, sigma=(2.0, 5.0))
+    sub = np.ascontiguousarray(g[1:5, 2:11, 4:14, 3:15])
+    return dict(field=sub, local_dims=[12, 10, 9, 4], offset=[3, 4, 2, 1], global_dims=[20, 18, 16, 5],
+                threshold=-0.2, q=2.0 ** 20)
+
+
+def ties_2d():
+    """Integer values in {-1, 0, 1}: every zero is decided by vertex parity."""
+    rng = np.random.default_rng(3)
+    f = rng.integers(-1, 2, (4, 16, 16)).astype(np.float64)
+    return dict(field=f, local_dims=[16, 16, 4], offset=None, global_dims=None, threshold=0.0, q=1e6)
+
+
+def single_layer_3d():
+    f = gaussian_potential((10, 10, 10), 2, seed=8, n_blobs=6, dtype=np.float64)
+    return dict(field=f, local_dims=[10, 10, 10, 2], offset=None, global_dims=None, threshold=-0.01, q=1e6)
+
+
+def no_crossing():
+    f = np.full((3, 8, 8), 2.5, dtype=np.float64)
+    return dict(field=f, local_dims=[8, 8, 3], offset=None, global_dims=None, threshold=0.0, q=1e6)
+
+
+CASES = {
+    "moving_sphere": moving_sphere,
+    "gauss_2d_f64": gauss_2d_f64,
+    "gauss_3d_f32_offset": gauss_3d_f32_offset,
+    "ties_2d": ties_2d,
+    "single_layer_3d": single_layer_3d,
+    "no_crossing": no_crossing,
+}
+
+# the reference's own known answer (tests/test_examples.cpp:256)
+SPHERE_VERTICES = 66418

@@ -1,0 +1,67 @@
+"""Generate tests/golden/contour/*.npz by running the reference's own CPU
+engine with ContourPredicate<T> (oracle/_ref/libftk2ref.so, built from the
+reference headers by oracle/Makefile) on the seeded inputs of
+tests/contour_cases.py.
+
+Each fixture stores the sha256 of the input bytes and, per output array
+(simplices, bary, lam, track_id, scalar, cells), its sha256 and shape; the
+small cases also store the arrays themselves.
+
+Run here, where the reference tree exists:  python tests/golden/make_contour_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from oracle import bridge  # noqa: E402
+import contour_cases  # noqa: E402
+
+FULL_ARRAYS_BELOW = 20000  # features
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def run(case):
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+    fld = bridge.make_field([case["field"]], bridge.LAYOUT_SEPARATE, 1, sos_q=case["q"], keep=keep)
+    r, cells = bridge.run_reference_contour(mesh, fld, case["threshold"])
+    return {"simplices": r.simplices, "bary": r.bary, "lam": r.lam, "track_id": r.track_id,
+            "scalar": r.scalar, "cells": cells}
+
+
+def main(names=None):
+    out_dir = os.path.join(HERE, "contour")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, make in contour_cases.CASES.items():
+        if names and name not in names:
+            continue
+        case = make()
+        t = time.time()
+        res = run(case)
+        dt = time.time() - t
+        rec = {"input_sha256": np.array(digest(case["field"])), "reference_seconds": np.array(dt)}
+        for k, v in res.items():
+            rec[k + "_sha256"] = np.array(digest(v))
+            rec[k + "_shape"] = np.array(v.shape, dtype=np.int64)
+            if len(res["track_id"]) < FULL_ARRAYS_BELOW:
+                rec[k] = v
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **rec)
+        print(f"{name}: {len(res['track_id'])} features, {len(set(res['track_id'].tolist()))} tracks, "
+              f"{len(res['cells'])} cells, reference {dt:.1f}s")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -1,0 +1,81 @@
+"""The level-set restatement (oracle/contour_oracle.py) is pinned before the
+GPU path is checked against it.
+
+1. It reproduces the reference's own known answer: 66418 feature vertices on
+   the moving sphere (tests/test_examples.cpp:225-256).
+2. On every contour case it reproduces, bit for bit, the fixtures that the
+   reference's own engine produced (tests/golden/make_contour_golden.py):
+   simplices, float and widened barycentrics, track ids, scalars and the
+   manifold cells of get_complex.
+3. Where the reference build is present, it matches a live reference run.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import contour_cases
+from oracle import bridge
+from oracle import contour_oracle as co
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "contour")
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def restate(case):
+    return co.contour(case["field"], case["threshold"], case["local_dims"], case["offset"],
+                      case["global_dims"], case["q"])
+
+
+def check_against_fixture(name, res):
+    g = np.load(os.path.join(GOLD, f"{name}.npz"))
+    for k in ("simplices", "bary", "lam", "track_id", "scalar", "cells"):
+        a = res[k]
+        if k == "cells":
+            a = a.astype(np.uint32).reshape(-1, g["cells_shape"][1] if g["cells_shape"].size > 1 else 1) \
+                if a.size else a
+        assert tuple(a.shape) == tuple(g[k + "_shape"]) or a.size == 0 == int(np.prod(g[k + "_shape"])), k
+        if a.size:
+            assert digest(a) == str(g[k + "_sha256"]), (name, k)
+
+
+def test_sphere_known_answer():
+    res = restate(contour_cases.moving_sphere())
+    assert len(res["track_id"]) == contour_cases.SPHERE_VERTICES
+    assert res["cells"].shape[1] == 4  # 3D+t: tets
+
+
+@pytest.mark.parametrize("name", list(contour_cases.CASES))
+def test_restatement_matches_reference_fixtures(name):
+    case = contour_cases.CASES[name]()
+    g = np.load(os.path.join(GOLD, f"{name}.npz"))
+    assert digest(case["field"]) == str(g["input_sha256"]), "generator drift"
+    check_against_fixture(name, restate(case))
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name", ["gauss_2d_f64", "ties_2d", "gauss_3d_f32_offset"])
+def test_restatement_matches_live_reference(name):
+    case = contour_cases.CASES[name]()
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+    fld = bridge.make_field([case["field"]], bridge.LAYOUT_SEPARATE, 1, sos_q=case["q"], keep=keep)
+    ref, cells = bridge.run_reference_contour(mesh, fld, case["threshold"])
+    res = restate(case)
+    assert len(ref.track_id) > 0
+    assert np.array_equal(res["simplices"], ref.simplices)
+    assert np.array_equal(res["bary"].view(np.uint32), ref.bary.view(np.uint32))
+    assert np.array_equal(res["lam"].view(np.uint64), ref.lam.view(np.uint64))
+    assert np.array_equal(res["track_id"], ref.track_id)
+    assert np.array_equal(res["cells"], cells)
+
+
+def test_sos_sign_ties_follow_vertex_parity():
+    adj = np.array([0.0, 0.0, 4e-7, -4e-7, 6e-7, -6e-7])
+    gid = np.array([2, 3, 5, 6, 7, 8], dtype=np.uint64)
+    # 0 -> parity; |v|*1e6 + 0.5 below 1 -> parity; above -> its own sign
+    assert co.sos_positive(adj, gid, 1e6).tolist() == [True, False, False, True, True, False]

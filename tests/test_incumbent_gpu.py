@@ -1,0 +1,107 @@
+"""The reference's own GPU path beside ours on the 3D plain drop-in field
+definition (float64 Gaussian-sum gradient, 32 blobs, Q = 2^20) at 64^3 x 8.
+At 128^3 x 16 the reference's path (its extraction kernel launched four times
+plus one execute_cuda) did not finish within 850 s on a B200, so the
+comparison runs at 1/32 of that size with one timed kernel launch.
+
+The reference's execute_cuda (engine.hpp:273-425) and its extraction kernel
+(cuda_engine.hpp:366-493), built from its headers into
+oracle/_ref/libftk2refcuda.so, run in a child process because the reference
+ends the process on any CUDA error.  Its GPU path reads separate component
+arrays only (predicate.hpp:112), so the child splits the field by component.
+The test checks that the incumbent finds the same set of simplices as this
+implementation and records the timings of both when FTK2B_INCUMBENT_JSON names
+an output file.  It runs only when FTK2B_INCUMBENT=1 (it is a measurement
+of the reference, bounded by a 300 s limit on the child process)."""
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+import pytest
+
+from ftk2_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+DIMS = [64, 64, 64, 8]
+
+CHILD = r"""
+import json, sys, time
+DIMS = [64, 64, 64, 8]
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from oracle import bridge
+host = np.load(sys.argv[2], mmap_mode="r")
+comps = [np.ascontiguousarray(host[..., j]) for j in range(host.shape[-1])]
+keep = []
+mesh = bridge.make_regular_mesh(DIMS)
+field = bridge.make_field(comps, bridge.LAYOUT_SEPARATE, 3, sos_q=2.0 ** 20, keep=keep)
+kernel_ms, n_nodes = bridge.time_reference_cuda_kernel(mesh, field, reps=1)
+t = time.perf_counter()
+res, exec_ms, complex_ms = bridge.run_reference_cuda(mesh, field)
+wall_ms = (time.perf_counter() - t) * 1e3
+np.savez(sys.argv[3], simplices=res.simplices, track_id=res.track_id, edges=res.edges)
+json.dump({"kernel_ms": kernel_ms, "kernel_nodes": n_nodes, "execute_cuda_ms": exec_ms,
+           "get_complex_ms": complex_ms, "wall_ms": wall_ms}, open(sys.argv[4], "w"))
+"""
+
+
+def partition(simplices, track_id):
+    """Feature simplices grouped by track, as a set of frozensets of rows."""
+    groups: dict = {}
+    for row, t in zip(map(tuple, simplices.tolist()), track_id.tolist()):
+        groups.setdefault(t, set()).add(row)
+    return {frozenset(g) for g in groups.values()}
+
+
+@pytest.mark.skipif(os.environ.get("FTK2B_INCUMBENT") != "1", reason="measurement run only (FTK2B_INCUMBENT=1)")
+def test_incumbent_gpu_path_same_simplices(ctx, tmp_path):
+    torch = pytest.importorskip("torch")
+    from oracle import bridge
+    if not os.path.exists(bridge.REF_CUDA_LIB):
+        pytest.skip("reference GPU engine not built")
+    from ftk2_b200 import generate
+    dev = generate.gaussian_field_device(tuple(DIMS[:3]), DIMS[3], seed=1234, n_blobs=32, dtype=torch.float64)
+    host = dev.cpu().numpy()
+    np.save(tmp_path / "field.npy", host)
+    r = subprocess.run([sys.executable, "-c", CHILD, ROOT, str(tmp_path / "field.npy"),
+                        str(tmp_path / "ref.npz"), str(tmp_path / "ref.json")],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    ref = np.load(tmp_path / "ref.npz")
+    info = json.load(open(tmp_path / "ref.json"))
+
+    keep: list = []
+    mesh = api.regular_mesh_desc(DIMS)
+    prm = api.params(2.0 ** 20)
+    mine = ctx.extract(mesh, api.field_desc(dev, api.LAYOUT_MULTICOMPONENT, 3, keep=keep), prm)
+    dev_ms, e2e_ms = [], []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ctx.extract(mesh, api.field_desc(dev, api.LAYOUT_MULTICOMPONENT, 3, keep=keep), prm)
+        dev_ms.append((time.perf_counter() - t) * 1e3)
+        t = time.perf_counter()
+        ctx.extract(mesh, api.field_desc(host, api.LAYOUT_MULTICOMPONENT, 3, keep=keep), prm)
+        e2e_ms.append((time.perf_counter() - t) * 1e3)
+
+    ours = {tuple(x) for x in mine.simplices.tolist()}
+    theirs = {tuple(x) for x in ref["simplices"].tolist()}
+    info.update({
+        "workload": "3D Gaussian-sum gradient, 64^3 x 8 float64, 32 blobs, Q = 2^20",
+        "ours_features": len(ours), "incumbent_features": len(theirs),
+        "same_simplex_set": ours == theirs,
+        "same_tracks": partition(mine.simplices, mine.track_id) == partition(ref["simplices"], ref["track_id"]),
+        "ours_device_input_ms": min(dev_ms), "ours_host_input_ms": min(e2e_ms),
+    })
+    out = os.environ.get("FTK2B_INCUMBENT_JSON")
+    if out:
+        with open(out, "w") as fh:
+            json.dump(info, fh, indent=1)
+    print(json.dumps(info))
+    assert ours == theirs

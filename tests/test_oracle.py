@@ -136,3 +136,12 @@ def test_restatement_matches_live_reference(name, make):
     assert len(ref.track_id) > 0
     assert_same(res, {"simplices": ref.simplices, "track_id": ref.track_id, "edges": ref.edges,
                       "bary": ref.bary, "scalar": ref.scalar, "type": ref.type, "lam": ref.lam})
+
+
+@pytest.mark.skipif(not os.path.exists(bridge.REF_CUDA_LIB), reason="reference GPU build absent")
+def test_reference_gpu_build_loads():
+    """The reference's GPU engine, built only to time the incumbent GPU path,
+    loads without a device and exports its three entry points."""
+    lib = C.CDLL(bridge.REF_CUDA_LIB)
+    for name in ("ftk2refcuda_run", "ftk2refcuda_time_kernel", "ftk2refcuda_free"):
+        assert hasattr(lib, name)
