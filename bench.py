@@ -293,6 +293,34 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def contour_c2(ctx, steps=3):
+    """Level sets (ContourPredicate) of the 3D plain drop-in generator's scalar,
+    128^3 x 16 float64, threshold 0, Q = 2^20: device pipeline time per call
+    (CUDA events inside ftk2b_contour_extract) and mesh edges per second; the
+    result copy to the host is outside it and reported as wall time."""
+    import numpy as np
+    import torch
+    from ftk2_b200 import api, generate
+    dims, nt = (128, 128, 128), 16
+    pot = generate.gaussian_potential_device(dims, nt, seed=1234, n_blobs=32)
+    torch.cuda.synchronize()
+    mesh = api.regular_mesh_desc([*dims, nt])
+    r = ctx.contour(mesh, pot, 0.0, 2.0 ** 20)  # warm-up (buffers, first launches)
+    dev_ms, wall_ms = [], []
+    for _ in range(steps):
+        t = time.perf_counter()
+        r = ctx.contour(mesh, pot, 0.0, 2.0 ** 20)
+        wall_ms.append((time.perf_counter() - t) * 1e3)
+        dev_ms.append(r.device_ms)
+    ms = float(np.median(dev_ms))
+    nbytes = pot.numel() * 8
+    del pot
+    return {"workload": "level set of the 128^3 x 16 f64 Gaussian-sum potential (32 blobs), threshold 0",
+            "mesh_edges": int(r.n_simplices), "features": int(len(r.track_id)), "cells": int(len(r.cells)),
+            "tracks": int(r.n_tracks), "device_ms": ms, "edges_per_s": r.n_simplices / (ms * 1e-3),
+            "field_read_gbs": nbytes / (ms * 1e-3) / 1e9, "wall_ms_with_result_copy": float(np.median(wall_ms))}
+
+
 def batched_c3(ctx, steps=5, check=True):
     """Batched workload: 256 independent float32 fields (2D sides U[32,512],
     3D sides U[16,96], nt U[2,8], 8-64 blobs), device-resident.  Plain = one
@@ -495,6 +523,8 @@ def main():
         torch.cuda.empty_cache()
         from ftk2_b200 import serving
         line["serve"] = serving.run(duration_s=args.serve_seconds, device=local)
+        torch.cuda.empty_cache()
+        line["contour"] = contour_c2(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

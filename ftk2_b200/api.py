@@ -144,6 +144,8 @@ SIGNATURES = {
     "ftk2b_contour_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc), C.c_double,
                                         C.c_double, C.POINTER(C.POINTER(ContourResultC))]),
     "ftk2b_contour_result_free": (None, [C.POINTER(ContourResultC)]),
+    "ftk2b_fiber_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                      C.POINTER(C.c_double), C.c_double, C.POINTER(C.POINTER(CPResultC))]),
     "ftk2b_cp_run": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                C.POINTER(CPParams), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
@@ -439,6 +441,19 @@ class Context:
             return _contour_from_c(out.contents)
         finally:
             self.lib.ftk2b_contour_result_free(out)
+
+    def fiber(self, mesh: MeshDesc, field: FieldDesc, thresholds=(0.0, 0.0), sos_q: float = 1e6) -> CPResult:
+        """Fibers (FiberPredicate<T>) of two scalar fields on a regular 2D+t
+        mesh; field carries the two arrays as its two components."""
+        thr = (C.c_double * 2)(float(thresholds[0]), float(thresholds[1]))
+        out = C.POINTER(CPResultC)()
+        self._check(self.lib.ftk2b_fiber_extract(self.h, C.byref(mesh), C.byref(field), thr, float(sos_q),
+                                                 C.byref(out)))
+        try:
+            self._last_n = int(out.contents.n_features)
+            return _result_from_c(out.contents)
+        finally:
+            self.lib.ftk2b_cp_result_free(out)
 
     def run(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None):
         """Device pipeline only; results stay on the device until fetch()."""

@@ -102,5 +102,25 @@ def build_tracker_test(verbose: bool = False) -> str:
     return TRACKER_BIN
 
 
+CONTOUR_SRC = os.path.join(ROOT, "tests", "cpp", "contour_run.cpp")
+CONTOUR_BIN = os.path.join(OUT_DIR, "contour_run")
+
+
+def build_contour_test(verbose: bool = False) -> str:
+    """C++ program running level sets through include/ftk2b/engine.hpp's
+    SimplicialEngine<T, ContourPredicate<T>>."""
+    lib = build(verbose)
+    hdr = os.path.join(ROOT, "include", "ftk2b", "engine.hpp")
+    if os.path.exists(CONTOUR_BIN) and os.path.getmtime(CONTOUR_BIN) >= max(
+            os.path.getmtime(CONTOUR_SRC), os.path.getmtime(lib), os.path.getmtime(hdr)):
+        return CONTOUR_BIN
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), CONTOUR_SRC, "-o", CONTOUR_BIN,
+           "-L", OUT_DIR, "-lftk2b", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return CONTOUR_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))

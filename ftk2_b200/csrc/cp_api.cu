@@ -605,8 +605,11 @@ cudaError_t resolve_cull_mode(ftk2b_ctx* ctx, const RegularMesh& rm, const Field
 
 }  // namespace ftk2b
 
+// fiber_thr: null for CriticalPointPredicate; the two thresholds for
+// FiberPredicate (2D+t meshes)
 static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
-                                const ftk2b_field_desc* field, const ftk2b_cp_params* prm) {
+                                const ftk2b_field_desc* field, const ftk2b_cp_params* prm,
+                                const double* fiber_thr = nullptr) {
   using Clk = std::chrono::steady_clock;
   auto msd = [](Clk::time_point a, Clk::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
@@ -639,6 +642,13 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   cfg.Q = prm->sos_q;
   cfg.refined = prm->precision == FTK2B_PRECISION_REFINED;
   cfg.cull_mode = ctx->cull_mode;  // 2 is resolved below, once the buffers exist
+  if (fiber_thr) {
+    cfg.fiber = 1;
+    cfg.fthr[0] = fiber_thr[0];
+    cfg.fthr[1] = fiber_thr[1];
+    cfg.cull_mode = 0;
+    cfg.refined = 0;
+  }
   cfg.tchunk = (int)rm.ld[d - 1];
   if (cfg.cull_mode != 0) CUDA_TRY(ctx, setup_cull_scratch(ctx, rm, cfg));
   if (ctx->tune_tchunk > 0) cfg.tchunk = ctx->tune_tchunk;
@@ -652,6 +662,12 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   // on overflow; the context remembers the grown value
   unsigned cap = ctx->cap_hint ? ctx->cap_hint : 65536u;
   unsigned ccap = ctx->cand_cap_hint ? ctx->cand_cap_hint : 65536u;
+  if (fiber_thr) {  // every local vertex is a candidate corner
+    uint64_t nloc = 1;
+    for (int k = 0; k < d; ++k) nloc *= rm.ld[k];
+    if (nloc > 0xFFFFFFF0ull) return fail(ctx, FTK2B_UNSUPPORTED, "mesh too large for fiber extraction");
+    ccap = std::max<unsigned>(ccap, (unsigned)nloc);
+  }
   for (int attempt = 0; attempt < 4; ++attempt) {
     const unsigned edge_cap = cap * 2;
     st = ensure_feature_buffers(ctx, cap, edge_cap, m);
@@ -679,9 +695,12 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       cudaError_t e;
       if ((e = cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream))) return e;
       int nk = 1;
-      if ((e = launch_extract_regular(f64, rm, fa, cfg, cq, B.err, ctx->stream, !ctx->disable_tma,
-                                      &ctx->last_used_tma, &nk)))
+      if (cfg.fiber) {
+        if ((e = launch_fiber_candidates(rm, cq, ctx->num_sms, ctx->stream))) return e;
+      } else if ((e = launch_extract_regular(f64, rm, fa, cfg, cq, B.err, ctx->stream, !ctx->disable_tma,
+                                             &ctx->last_used_tma, &nk))) {
         return e;
+      }
       *nl += (unsigned long long)nk;
       return cudaSuccess;
     };
@@ -690,7 +709,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       if ((e = launch_refine_regular(f64, rm, fa, cfg, cq, sink, ctx->num_sms, ctx->stream))) return e;
       *nl += 1;
       if ((e = launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, nl))) return e;
-      if (prm->classify) {
+      if (prm->classify && !cfg.fiber) {
         if ((e = launch_classify_regular(f64, rm, fa, nch, B, ctx->stream))) return e;
         *nl += 1;
       }
@@ -838,7 +857,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     ctx->last.n_roots = h[kCountRoots];
     ctx->last.n_simplices = nsimp;
     ctx->last.device_ms = ms;
-    ctx->last.classify = prm->classify;
+    ctx->last.classify = prm->classify && !cfg.fiber;
     ctx->last.want_edges = prm->want_edges;
     return FTK2B_OK;
   }
@@ -926,6 +945,28 @@ extern "C" ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out) {
     for (uint64_t i = 0; i < n; ++i) r->track_id[i] = i;
   *out = r;
   return FTK2B_OK;
+}
+
+extern "C" ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
+                                            const ftk2b_field_desc* field, const double thresholds[2],
+                                            double sos_q, ftk2b_cp_result** out) {
+  if (!ctx) return FTK2B_INVALID_ARG;
+  if (!mesh || !field || !thresholds || !out) return fail(ctx, FTK2B_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (mesh->kind != FTK2B_MESH_REGULAR || mesh->ndims != 3)
+    return fail(ctx, FTK2B_UNSUPPORTED, "fiber extraction runs on regular 2D+t meshes (ndims 3)");
+  if (field->ncomp != 2) return fail(ctx, FTK2B_INVALID_ARG, "fibers read two scalar fields (ncomp 2)");
+  if (field->scalar) return fail(ctx, FTK2B_INVALID_ARG, "fibers interpolate no scalar");
+  if (!(sos_q > 0)) return fail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  ftk2b_cp_params prm = ftk2b_cp_params_default();
+  prm.sos_q = sos_q;
+  prm.precision = FTK2B_PRECISION_EXACT;
+  prm.classify = 0;
+  prm.want_edges = 1;
+  const ftk2b_status st = run_regular(ctx, mesh, field, &prm, thresholds);
+  if (st) return st;
+  return ftk2b_cp_fetch(ctx, out);
 }
 
 extern "C" ftk2b_status ftk2b_cp_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,

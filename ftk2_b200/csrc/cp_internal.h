@@ -72,6 +72,11 @@ struct ExtractConfig {
   int tiles[3];                // tiles along x, y, z (z = 1 for 2D)
   int skip_first_spatial;      // 1: no purely spatial simplices at local time 0
   int cull_mode;               // 0: per-vertex cull words only; 1: tile statistics first
+  // FiberPredicate<T> (predicate.hpp:341-362): every hypercube is a candidate
+  // (the cull words assume the solve must succeed), values are taken minus
+  // fthr[j], and a simplex whose solve fails is kept at the centroid
+  int fiber;
+  double fthr[2];
   // scratch of cull mode 1 (device): 8 ints per (slice, tile), and the runs
   // of surviving tile-steps (4 words each: tile, first step, end step, pad)
   int* tstats;
@@ -98,6 +103,10 @@ cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const Field
 // Scratch of cull mode 1 for a mesh: tile-slice statistics and run list sizes.
 void tile_scratch_size(const RegularMesh& mesh, size_t* stats_bytes, unsigned* runs_cap);
 // Exact SoS + solve of the queued candidates, compacted into the sink.
+// FiberPredicate: queue every local vertex as a corner with all its in-mesh
+// chains (no cull)
+cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueue& cq, int num_sms,
+                                    cudaStream_t st);
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
                                   const ExtractConfig& cfg, const CandidateQueue& cq,
                                   const FeatureSink& sink, int num_sms, cudaStream_t st);

@@ -1205,7 +1205,9 @@ __device__ __forceinline__ void refine_candidate(const RegularMesh& mesh, const 
         vid += (unsigned long long)g[k] * mesh.gstride[k];
       }
     }
-    cube[v * M + j] = in ? field_at<T>(fa, j, g, D, vid) : T(0);
+    T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
+    if (cfg.fiber) val = fp<T>::sub(val, (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
+    cube[v * M + j] = val;
   }
   __syncwarp();
   // cull words of the hypercube's vertices (absent outside the mesh)
@@ -1234,7 +1236,7 @@ __device__ __forceinline__ void refine_candidate(const RegularMesh& mesh, const 
       unsigned wacc = kAbsent;
 #pragma unroll
       for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, mk[i]);
-      live = live && !word_culled(wacc);
+      live = live && (cfg.fiber || !word_culled(wacc));
     }
     if (live) {
       T vals[M + 1][M];
@@ -1247,7 +1249,14 @@ __device__ __forceinline__ void refine_candidate(const RegularMesh& mesh, const 
       else inside = sos_inside3<T>(vals, cfg.Q);
       if (inside) {
         T lam[M + 1];
-        if (solve_exact<M, T>(vals, lam)) {
+        bool solved = solve_exact<M, T>(vals, lam);
+        if (!solved && cfg.fiber) {
+          // FiberPredicate keeps the simplex at the centroid: (T)1.0 / 3.0
+#pragma unroll
+          for (int i = 0; i <= M; ++i) lam[i] = (T)((double)(T)1.0 / 3.0);
+          solved = true;
+        }
+        if (solved) {
           acc = true;
 #pragma unroll
           for (int i = 0; i <= M; ++i) {
@@ -1712,6 +1721,41 @@ cudaError_t launch_extract_regular(int f64, const RegularMesh& mesh, const Field
                : launch_td<float, 4>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches);
   return f64 ? launch_td<double, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches)
              : launch_td<float, 3>(mesh, fa, cfg, cq, err, st, allow_tma, used_tma, launches);
+}
+
+// FiberPredicate candidates: every local vertex is a hypercube corner whose
+// chains inside the mesh all need the exact test (a chain is inside when its
+// last vertex, the union of its steps, is).
+__global__ void fiber_candidates_kernel(RegularMesh mesh, CandidateQueue cq) {
+  const int D = mesh.d;
+  const ChainTable& CT = c_chains[D - 3];
+  unsigned long long nv = 1;
+  for (int k = 0; k < D; ++k) nv *= (unsigned long long)mesh.ld[k];
+  const unsigned long long n = nv < cq.cap ? nv : cq.cap;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long r = i, l[4] = {0, 0, 0, 0};
+    unsigned inb = 0;
+    for (int k = 0; k < D; ++k) {
+      l[k] = r % (unsigned long long)mesh.ld[k];
+      r /= (unsigned long long)mesh.ld[k];
+      if (l[k] + 1 < (unsigned long long)mesh.ld[k]) inb |= 1u << k;
+    }
+    unsigned long long chains = 0;
+    for (int ch = 0; ch < CT.n; ++ch)
+      if ((CT.mask[ch][D - 2] & ~inb) == 0) chains |= 1ull << ch;
+    // corner layout of the candidate queue: x | y << 16 | z << 32 | t << 48
+    const unsigned long long t = l[D - 1];
+    cq.corner[i] = l[0] | (l[1] << 16) | (D == 4 ? l[2] << 32 : 0ull) | (t << 48);
+    cq.chains[i] = chains;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *cq.count = (unsigned)(nv < 0xFFFFFFFFull ? nv : 0xFFFFFFFFull);
+}
+
+cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueue& cq, int num_sms,
+                                    cudaStream_t st) {
+  fiber_candidates_kernel<<<num_sms * 8, 256, 0, st>>>(mesh, cq);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,

@@ -54,6 +54,33 @@ def gaussian_field_device(dims, nt: int, seed: int = 1234, n_blobs: int = 32, dt
     return out
 
 
+def gaussian_potential_device(dims, nt: int, seed: int = 1234, n_blobs: int = 32, sigma=(4.0, 12.0),
+                              drift: float = 0.5, device: str = "cuda"):
+    """The drifting Gaussian sum itself, sum_b A_b exp(-|p - c_b(t)|^2 / (2 s_b^2)),
+    float64, shape (nt, [nz,] ny, nx): the scalar whose gradient
+    gaussian_field_device returns (same blob draws), for level sets."""
+    import torch
+    ndim = len(dims)
+    blobs = gaussian_blobs(seed, n_blobs, dims, sigma, drift)
+    axes = [torch.arange(n, dtype=torch.float64, device=device) for n in dims]
+    shape = tuple(dims[::-1])
+    out = torch.empty((nt,) + shape, dtype=torch.float64, device=device)
+    for k in range(nt):
+        acc = torch.zeros(shape, dtype=torch.float64, device=device)
+        for b in range(n_blobs):
+            c = blobs["centers"][b] + blobs["vel"][b] * k
+            s2 = float(blobs["sigma"][b]) ** 2
+            r2 = None
+            for i in range(ndim):
+                view = [1] * ndim
+                view[ndim - 1 - i] = dims[i]
+                d = ((axes[i] - float(c[i])) ** 2).view(view)
+                r2 = d if r2 is None else r2 + d
+            acc += float(blobs["amps"][b]) * torch.exp(-r2 / (2.0 * s2))
+        out[k] = acc
+    return out
+
+
 def c2_field(device: str = "cuda"):
     """3D flow critical points, plain drop-in: 128^3 x 16, 32 blobs, float64."""
     import torch

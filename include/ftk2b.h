@@ -381,6 +381,19 @@ ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, 
                                    double threshold, double sos_q, ftk2b_contour_result** out);
 void ftk2b_contour_result_free(ftk2b_contour_result* r);
 
+/* --- fibers (FiberPredicate<T>) --------------------------------------------
+ * Replaces SimplicialEngine<T, FiberPredicate<T>>::execute + get_complex
+ * (predicate.hpp:341-362; form_general_manifold_patches engine.hpp:1341-1418)
+ * on a regular 2D+t mesh (ndims 3): features are the triangles where both
+ * fields minus their thresholds vanish (simulation of simplicity), kept at the
+ * centroid where the barycentric solve fails; edges join each top cell's
+ * features to its star centre.  field: ncomp 2 (SEPARATE, MULTICOMPONENT or
+ * PER_VERTEX layout as for critical points).  The result is a cp_result with
+ * m = 2, type 0 and scalar 0.  3D+t meshes (fiber surfaces) are
+ * FTK2B_UNSUPPORTED. */
+ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                                 const double thresholds[2], double sos_q, ftk2b_cp_result** out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,7 @@
 //   ftk2::UnstructuredSimplicialMesh(...)          ftk2b::UnstructuredSimplicialMesh (unstructured_mesh.hpp:16)
 //   ftk2::ExtrudedSimplicialMesh(base, layers)     ftk2b::ExtrudedSimplicialMesh  (mesh.hpp:544)
 //   ftk2::CriticalPointPredicate<M,T>              ftk2b::CriticalPointPredicate<M,T> (predicate.hpp:49-64)
+//   ftk2::ContourPredicate<T> (level sets)         ftk2b::ContourPredicate<T>     (predicate.hpp:135-183)
 //   ftk2::SimplicialEngine<T,Pred>(mesh, pred)     ftk2b::SimplicialEngine<T,Pred> (engine.hpp:84-85)
 //     .execute(data, vars) / .execute_cuda(...)      .execute / .execute_cuda      (engine.hpp:96-99, 273)
 //     .get_complex() -> FeatureComplex               .get_complex()                (engine.hpp:822-996)
@@ -469,6 +470,105 @@ class SimplicialEngine {
   std::unique_ptr<ftk2b_ctx, CtxDel> ctx_;
   std::unique_ptr<ftk2b_cp_result, ResDel> result_;
   std::vector<float> attrs_;  // 16 per feature when attributes were recorded
+};
+
+// ---- level sets (ContourPredicate<T>, predicate.hpp:135-183)
+
+template <typename T = double>
+struct ContourPredicate {
+  static constexpr int codimension = 1;
+  double sos_q = 1000000.0;
+  std::string var_name;
+  T threshold = (T)0.0;
+};
+
+// SimplicialEngine<T, ContourPredicate<T>> on a regular mesh: execute runs
+// ftk2b_contour_extract on the scalar array (the predicate's var_name, or the
+// first name passed); get_complex returns the edge features in simplex order
+// and the manifold cells (dimension 2 on 2D+t meshes, 3 on 3D+t meshes) as
+// the reference's get_complex lists them (engine.hpp:822-996).
+template <typename T>
+class SimplicialEngine<T, ContourPredicate<T>> {
+ public:
+  static constexpr int m = 1;
+
+  SimplicialEngine(std::shared_ptr<Mesh> mesh, ContourPredicate<T> pred = ContourPredicate<T>(), int device = 0)
+      : mesh_(std::move(mesh)), pred_(pred) {
+    ftk2b_ctx* c = nullptr;
+    ftk2b_status s = ftk2b_ctx_create(device, &c);
+    if (s != FTK2B_OK) throw Error(s, "ftk2b_ctx_create failed");
+    ctx_.reset(c);
+  }
+
+  template <typename Array>
+  void execute(const std::map<std::string, Array>& data, const std::vector<std::string>& vars = {}) {
+    const std::string& name = vars.empty() ? pred_.var_name : vars[0];
+    const Array& a = data.at(name);
+    ftk2b_mesh_desc md = mesh_->desc();
+    if (md.kind != FTK2B_MESH_REGULAR) throw Error(FTK2B_UNSUPPORTED, "level sets need a regular mesh");
+    using E = std::remove_cv_t<std::remove_pointer_t<decltype(a.pdata())>>;
+    std::vector<T> conv;
+    const void* p = a.pdata();
+    if (!std::is_same<E, T>::value) {
+      conv.assign(a.pdata(), a.pdata() + a.nelem());
+      p = conv.data();
+    }
+    ftk2b_field_desc fd;
+    std::memset(&fd, 0, sizeof(fd));
+    fd.dtype = sizeof(T) == 8 ? FTK2B_F64 : FTK2B_F32;
+    fd.ncomp = 1;
+    fd.layout = FTK2B_LAYOUT_SEPARATE;
+    fd.location = FTK2B_HOST;
+    fd.comp[0] = p;
+    fd.nd = (int)a.nd();
+    for (int i = 0; i < fd.nd && i < 4; ++i) fd.dims[i] = a.dimf(i);
+    ftk2b_contour_result* r = nullptr;
+    ftk2b_status st = ftk2b_contour_extract(ctx_.get(), &md, &fd, (double)pred_.threshold, pred_.sos_q, &r);
+    if (st != FTK2B_OK) throw Error(st, ftk2b_last_error(ctx_.get()));
+    result_.reset(r);
+  }
+
+  template <typename Array>
+  void execute_cuda(const std::map<std::string, Array>& data, const std::vector<std::string>& v = {}) {
+    execute(data, v);
+  }
+
+  FeatureComplex get_complex() const {
+    FeatureComplex fc;
+    const ftk2b_contour_result* r = result_.get();
+    if (!r) return fc;
+    fc.vertices.resize(r->n_features);
+    fc.lambda.assign(r->lambda, r->lambda + 2 * r->n_features);
+    for (uint64_t i = 0; i < r->n_features; ++i) {
+      FeatureElement& el = fc.vertices[i];
+      el.simplex.dimension = 1;
+      for (int v = 0; v < 2; ++v) {
+        el.simplex.vertices[v] = r->simplices[2 * i + v];
+        el.barycentric_coords[0][v] = r->barycentric[2 * i + v];
+      }
+      el.track_id = r->track_id[i];
+      el.scalar = r->scalar[i];
+    }
+    if (r->n_cells) {
+      FeatureComplex::SimplexIndices c;
+      c.dimension = r->cell_dim;
+      c.indices.assign(r->cells, r->cells + (size_t)(r->cell_dim + 1) * r->n_cells);
+      fc.connectivity.push_back(std::move(c));
+    }
+    return fc;
+  }
+
+ private:
+  struct CtxDel {
+    void operator()(ftk2b_ctx* c) const { ftk2b_ctx_destroy(c); }
+  };
+  struct ResDel {
+    void operator()(ftk2b_contour_result* r) const { ftk2b_contour_result_free(r); }
+  };
+  std::shared_ptr<Mesh> mesh_;
+  ContourPredicate<T> pred_;
+  std::unique_ptr<ftk2b_ctx, CtxDel> ctx_;
+  std::unique_ptr<ftk2b_contour_result, ResDel> result_;
 };
 
 }  // namespace ftk2b

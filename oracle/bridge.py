@@ -304,6 +304,39 @@ def run_reference_contour(mesh: OrcMesh, field: OrcField, threshold: float, one_
     return out, cells
 
 
+def run_reference_fiber(mesh: OrcMesh, field: OrcField, thresholds, one_thread: bool = False) -> CPResult:
+    """The reference's own engine with FiberPredicate<T> on a regular 2D+t
+    mesh: field.comp[0], comp[1] are the two scalar arrays."""
+    lib = _load(REF1T_LIB if one_thread else REF_LIB, "ftk2ref")
+    fn = lib.ftk2ref_run_fiber
+    fn.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.POINTER(C.c_double), C.POINTER(OrcResult)]
+    fn.restype = C.c_int
+    thr = (C.c_double * 2)(float(thresholds[0]), float(thresholds[1]))
+    res = OrcResult()
+    rc = fn(C.byref(mesh), C.byref(field), thr, C.byref(res))
+    if rc != 0:
+        raise RuntimeError(f"ftk2ref_run_fiber failed with status {rc}")
+    try:
+        n, e = int(res.n), int(res.n_edges)
+
+        def arr(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        return CPResult(
+            simplices=arr(res.simplices, 3 * n, np.uint64).reshape(n, 3),
+            bary=arr(res.bary, 3 * n, np.float32).reshape(n, 3),
+            lam=arr(res.lambda_, 3 * n, np.float64).reshape(n, 3),
+            track_id=arr(res.track_id, n, np.uint64),
+            type=arr(res.type, n, np.uint32),
+            scalar=arr(res.scalar, n, np.float32),
+            edges=arr(res.edges, 2 * e, np.uint32).reshape(e, 2),
+        )
+    finally:
+        lib.ftk2ref_free(C.byref(res))
+
+
 def run_restatement(mesh: OrcMesh, field: OrcField) -> CPResult:
     """Our exact C restatement of the same algorithm."""
     return _run(ORC_LIB, "cporacle", mesh, field)

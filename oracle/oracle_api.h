@@ -117,6 +117,10 @@ typedef struct {
 int ftk2ref_run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, orc_result* out,
                         orc_conn* conn);
 void ftk2ref_free_conn(orc_conn* c);
+/* Fibers (FiberPredicate<T>, predicate.hpp:341-362) of the two scalar arrays
+ * comp[0], comp[1] (layout SEPARATE) on a regular 2D+t mesh; thresholds[2].
+ * Flattened as ftk2ref_run, with the star edges of the trajectories. */
+int ftk2ref_run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thresholds, orc_result* out);
 
 /* own restatement */
 int cporacle_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);

@@ -298,7 +298,91 @@ int run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, 
   return 0;
 }
 
+// Fibers: SimplicialEngine<T, FiberPredicate<T>> on a regular mesh with the
+// two scalar fields F and G (the reference's tests/test_examples.cpp fiber
+// set-up), flattened as run() does.  lambda: the barycentrics the predicate
+// stores (solver output, or 1/3 where it falls back, predicate.hpp:354).
+template <typename T>
+int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, orc_result* out) {
+  using namespace ftk2;
+  std::vector<uint64_t> dims, off, glob;
+  for (int i = 0; i < mesh->ndims; ++i) {
+    dims.push_back(mesh->local_dims[i]);
+    off.push_back(mesh->offset[i]);
+    glob.push_back(mesh->global_dims[i]);
+  }
+  auto reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
+  FiberPredicate<T> pred;
+  pred.var_names[0] = "F";
+  pred.var_names[1] = "G";
+  pred.thresholds[0] = (T)thr[0];
+  pred.thresholds[1] = (T)thr[1];
+  pred.sos_q = field->sos_q;
+  std::map<std::string, ftk::ndarray<T>> data;
+  data["F"] = make_array<T>(field->comp[0], field->nd, field->dims);
+  data["G"] = make_array<T>(field->comp[1], field->nd, field->dims);
+  SimplicialEngine<T, FiberPredicate<T>> engine(reg, pred);
+  std::streambuf* saved = std::cout.rdbuf();
+  std::ostringstream sink;
+  std::cout.rdbuf(sink.rdbuf());
+  engine.execute(data, {"F", "G"});
+  FeatureComplex complex = engine.get_complex();
+  std::cout.rdbuf(saved);
+
+  const uint64_t n = complex.vertices.size();
+  out->m = 2;
+  out->n = n;
+  out->simplices = (uint64_t*)std::malloc(sizeof(uint64_t) * (3 * n + 1));
+  out->bary = (float*)std::malloc(sizeof(float) * (3 * n + 1));
+  out->lambda = (double*)std::malloc(sizeof(double) * (3 * n + 1));
+  out->track_id = (uint64_t*)std::malloc(sizeof(uint64_t) * (n + 1));
+  out->type = (uint32_t*)std::malloc(sizeof(uint32_t) * (n + 1));
+  out->scalar = (float*)std::malloc(sizeof(float) * (n + 1));
+  out->n_tested = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const FeatureElement& el = complex.vertices[i];
+    T values[3][2];
+    for (int v = 0; v < 3; ++v) {
+      out->simplices[3 * i + v] = el.simplex.vertices[v];
+      out->bary[3 * i + v] = el.barycentric_coords[0][v];
+      std::vector<double> c = reg->get_vertex_coordinates(el.simplex.vertices[v]);
+      for (size_t k = 0; k < c.size(); ++k) c[k] -= (double)off[k];
+      for (int j = 0; j < 2; ++j) {
+        const auto& a = data.at(j == 0 ? "F" : "G");
+        values[v][j] = (T)(a.f(c[0], c[1], c[2]) - pred.thresholds[j]);
+      }
+    }
+    T lambda[3];
+    if (!ZeroCrossingSolver<2, T>::solve(values, lambda))
+      for (int v = 0; v < 3; ++v) lambda[v] = (T)1.0 / 3.0;
+    for (int v = 0; v < 3; ++v) out->lambda[3 * i + v] = (double)lambda[v];
+    out->track_id[i] = el.track_id;
+    out->type[i] = el.type;
+    out->scalar[i] = el.scalar;
+  }
+  std::vector<uint32_t> edges;
+  for (const auto& conn : complex.connectivity)
+    if (conn.dimension == 1) edges = conn.indices;
+  out->n_edges = edges.size() / 2;
+  out->edges = (uint32_t*)std::malloc(sizeof(uint32_t) * (edges.size() + 2));
+  if (!edges.empty()) std::memcpy(out->edges, edges.data(), sizeof(uint32_t) * edges.size());
+  return 0;
+}
+
 }  // namespace
+
+extern "C" int ftk2ref_run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thresholds,
+                                 orc_result* out) {
+  std::memset(out, 0, sizeof(*out));
+  if (mesh->kind != ORC_MESH_REGULAR || mesh->ndims != 3 || field->layout != ORC_LAYOUT_SEPARATE) return 3;
+  try {
+    return field->dtype == ORC_F64 ? run_fiber<double>(mesh, field, thresholds, out)
+                                   : run_fiber<float>(mesh, field, thresholds, out);
+  } catch (const std::exception& e) {
+    std::cerr << "ftk2ref_run_fiber: " << e.what() << std::endl;
+    return 1;
+  }
+}
 
 extern "C" int ftk2ref_run_contour(const orc_mesh* mesh, const orc_field* field, double threshold,
                                    orc_result* out, orc_conn* conn) {

@@ -1,4 +1,4 @@
-"""Seeded inputs of the level-set (contour) parity cases.
+"""Seeded inputs of the level-set (contour) and fiber parity cases.
 
 Each maker returns a dict: field (C-order, reversed Fortran shape of the local
 mesh), local_dims, offset, global_dims, threshold, q.  The moving sphere is
@@ -95,3 +95,54 @@ CASES = {
 
 # the reference's own known answer (tests/test_examples.cpp:256)
 SPHERE_VERTICES = 66418
+
+
+# ---- fibers (FiberPredicate<T>): two scalar fields F, G on 2D+t meshes.
+# Makers return a dict: fields (F, G; C-order, reversed Fortran shape),
+# local_dims, offset, global_dims, thresholds, q.
+
+def fiber_gauss_f64():
+    f = gaussian_potential((40, 36), 6, seed=31, n_blobs=10, dtype=np.float64)
+    g = gaussian_potential((40, 36), 6, seed=32, n_blobs=10, dtype=np.float64)
+    return dict(fields=(f, g), local_dims=[40, 36, 6], offset=None, global_dims=None, thresholds=(0.05, -0.02),
+                q=1e6)
+
+
+def fiber_f32_offset():
+    """A 24x20x5 sub-box at offset (3, 4, 1) of a 30x28x7 mesh; the arrays
+    hold the sub-box's values."""
+    f = gaussian_potential((30, 28), 7, seed=33, n_blobs=8, dtype=np.float32)
+    g = gaussian_potential((30, 28), 7, seed=34, n_blobs=8, dtype=np.float32)
+    sub = tuple(np.ascontiguousarray(a[1:6, 4:24, 3:27]) for a in (f, g))
+    thr = tuple(float(np.median(a)) for a in sub)  # levels that cross inside the box
+    return dict(fields=sub, local_dims=[24, 20, 5], offset=[3, 4, 1], global_dims=[30, 28, 7],
+                thresholds=thr, q=2.0 ** 20)
+
+
+def fiber_ties():
+    """Integer values in {-1, 0, 1}: zeros decided by vertex parity, and
+    degenerate triangles where the solve fails and the centroid is kept."""
+    rng = np.random.default_rng(35)
+    f = rng.integers(-1, 2, (4, 14, 15)).astype(np.float64)
+    g = rng.integers(-1, 2, (4, 14, 15)).astype(np.float64)
+    return dict(fields=(f, g), local_dims=[15, 14, 4], offset=None, global_dims=None, thresholds=(0.0, 0.0),
+                q=1e6)
+
+
+def fiber_near_quantum():
+    """Values of a few 1/Q: many triangles whose quantised values are zero or
+    one unit, where the simulation of simplicity finds the origin inside but
+    the solve's pivot falls below 1e-12 and the centroid is kept."""
+    rng = np.random.default_rng(36)
+    f = rng.uniform(-3e-6, 3e-6, (4, 18, 20))
+    g = rng.uniform(-3e-6, 3e-6, (4, 18, 20))
+    return dict(fields=(f, g), local_dims=[20, 18, 4], offset=None, global_dims=None, thresholds=(0.0, 0.0),
+                q=1e6)
+
+
+FIBER_CASES = {
+    "fiber_gauss_f64": fiber_gauss_f64,
+    "fiber_f32_offset": fiber_f32_offset,
+    "fiber_ties": fiber_ties,
+    "fiber_near_quantum": fiber_near_quantum,
+}

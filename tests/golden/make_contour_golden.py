@@ -1,6 +1,7 @@
-"""Generate tests/golden/contour/*.npz by running the reference's own CPU
-engine with ContourPredicate<T> (oracle/_ref/libftk2ref.so, built from the
-reference headers by oracle/Makefile) on the seeded inputs of
+"""Generate tests/golden/contour/*.npz and tests/golden/fiber/*.npz by running
+the reference's own CPU engine with ContourPredicate<T> (one worker thread,
+oracle/_ref/libftk2ref1t.so) and FiberPredicate<T> (oracle/_ref/libftk2ref.so),
+built from the reference headers by oracle/Makefile, on the seeded inputs of
 tests/contour_cases.py.
 
 Each fixture stores the sha256 of the input bytes and, per output array
@@ -42,6 +43,33 @@ def run(case):
             "scalar": r.scalar, "cells": cells}
 
 
+def run_fiber(case):
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+    fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+    r = bridge.run_reference_fiber(mesh, fld, case["thresholds"])
+    return {"simplices": r.simplices, "bary": r.bary, "lam": r.lam, "track_id": r.track_id,
+            "scalar": r.scalar, "edges": r.edges}
+
+
+def main_fiber(names=None):
+    out_dir = os.path.join(HERE, "fiber")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, make in contour_cases.FIBER_CASES.items():
+        if names and name not in names:
+            continue
+        case = make()
+        t = time.time()
+        res = run_fiber(case)
+        dt = time.time() - t
+        rec = {"input_sha256": np.array(digest(np.concatenate([a.reshape(-1) for a in case["fields"]]))),
+               "reference_seconds": np.array(dt)}
+        rec.update(res)
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **rec)
+        print(f"{name}: {len(res['track_id'])} features, {len(set(res['track_id'].tolist()))} tracks, "
+              f"{len(res['edges'])} edges, reference {dt:.1f}s")
+
+
 def main(names=None):
     out_dir = os.path.join(HERE, "contour")
     os.makedirs(out_dir, exist_ok=True)
@@ -65,3 +93,4 @@ def main(names=None):
 
 if __name__ == "__main__":
     main(sys.argv[1:])
+    main_fiber(sys.argv[1:])

@@ -96,30 +96,6 @@ def test_contour_random_small_vs_restatement(ctx, seed, dims, dtype, thr):
     assert_same(as_dict(run_gpu(ctx, case)), want, str(seed))
 
 
-def potential_device(dims, nt, seed, n_blobs, sigma=(4.0, 12.0), drift=0.5):
-    """contour_cases.gaussian_potential evaluated with torch on the device
-    (same blob draws), float64, shape (nt, [nz,] ny, nx)."""
-    import torch
-    rng = np.random.default_rng(seed)
-    d = len(dims)
-    centers = rng.uniform(0, 1, (n_blobs, d)) * np.array(dims, dtype=np.float64)
-    amps = rng.standard_normal(n_blobs)
-    sig = rng.uniform(sigma[0], sigma[1], n_blobs)
-    vel = rng.uniform(-drift, drift, (n_blobs, d))
-    axes = [torch.arange(n, dtype=torch.float64, device="cuda") for n in dims]
-    out = torch.zeros((nt,) + tuple(dims[::-1]), dtype=torch.float64, device="cuda")
-    for t in range(nt):
-        for b in range(n_blobs):
-            c = centers[b] + vel[b] * t
-            r2 = 0.0
-            for i in range(d):
-                shape = [1] * d
-                shape[d - 1 - i] = dims[i]
-                r2 = r2 + ((axes[i] - float(c[i])) ** 2).reshape(shape)
-            out[t] += float(amps[b]) * torch.exp(-r2 / (2.0 * float(sig[b]) ** 2))
-    return out
-
-
 def test_contour_full_size_properties(ctx):
     """128^3 x 16 float64 Gaussian-sum potential (32 blobs, the 3D plain
     drop-in generator's scalar), threshold 0: features in strict simplex
@@ -129,7 +105,8 @@ def test_contour_full_size_properties(ctx):
     pytest.importorskip("torch")
     dims, nt = (128, 128, 128), 16
     q = 2.0 ** 20
-    dev = potential_device(dims, nt, seed=1234, n_blobs=32)
+    from ftk2_b200 import generate
+    dev = generate.gaussian_potential_device(dims, nt, seed=1234, n_blobs=32)
     mesh = api.regular_mesh_desc([*dims, nt])
     r = ctx.contour(mesh, dev, 0.0, q)
     f = dev.cpu().numpy()
@@ -162,3 +139,35 @@ def test_contour_full_size_properties(ctx):
     case = dict(field=win, local_dims=[18, 20, 24, 6], offset=None, global_dims=None, threshold=0.0, q=q)
     want = co.contour(win, 0.0, [18, 20, 24, 6], q=q)
     assert_same(as_dict(run_gpu(ctx, case)), want, "window")
+
+
+@pytest.mark.parametrize("name", ["gauss_2d_f64", "single_layer_3d", "ties_2d"])
+def test_contour_cpp_dropin_matches_restatement(tmp_path, name):
+    """SimplicialEngine<T, ContourPredicate<T>> of include/ftk2b/engine.hpp,
+    driven as the reference's own level-set test drives its engine."""
+    import subprocess
+    from ftk2_b200 import build as fb
+    case = contour_cases.CASES[name]()
+    exe = fb.build_contour_test()
+    f = case["field"]
+    path = tmp_path / "f.bin"
+    f.tofile(path)
+    dt = "f64" if f.dtype == np.float64 else "f32"
+    out = tmp_path / "out.txt"
+    r = subprocess.run([exe, str(path), dt, ",".join(str(x) for x in case["local_dims"]), repr(case["threshold"]),
+                        repr(case["q"]), str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    feats, cells = [], []
+    for line in open(out):
+        if line.startswith("F"):
+            vs, bs, tr, sc = line[1:].split("|")
+            feats.append(([int(x) for x in vs.split()], [int(x, 16) for x in bs.split()], int(tr), int(sc, 16)))
+        elif line.startswith("C"):
+            cells.append([int(x) for x in line.split()[2:]])
+    want = co.contour(f, case["threshold"], case["local_dims"], q=case["q"])
+    assert len(feats) == len(want["track_id"]) > 0
+    assert np.array_equal(np.array([v for v, _, _, _ in feats], dtype=np.uint64), want["simplices"])
+    assert np.array_equal(np.array([b for _, b, _, _ in feats], dtype=np.uint32), want["bary"].view(np.uint32))
+    assert np.array_equal(np.array([t for _, _, t, _ in feats], dtype=np.uint64), want["track_id"])
+    assert np.array_equal(np.array([s for _, _, _, s in feats], dtype=np.uint32), want["scalar"].view(np.uint32))
+    assert np.array_equal(np.array(cells, dtype=np.uint32).reshape(-1, want["cells"].shape[1]), want["cells"])

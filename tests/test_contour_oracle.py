@@ -79,3 +79,35 @@ def test_sos_sign_ties_follow_vertex_parity():
     gid = np.array([2, 3, 5, 6, 7, 8], dtype=np.uint64)
     # 0 -> parity; |v|*1e6 + 0.5 below 1 -> parity; above -> its own sign
     assert co.sos_positive(adj, gid, 1e6).tolist() == [True, False, False, True, True, False]
+
+
+FIBER_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber")
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_CASES))
+def test_fiber_reference_reproduces_fixtures_on_one_and_many_workers(name):
+    """The fiber fixtures are the reference engine's output; its result does
+    not depend on its worker count (star centres go by simplex code)."""
+    case = contour_cases.FIBER_CASES[name]()
+    g = np.load(os.path.join(FIBER_GOLD, f"{name}.npz"))
+    assert digest(np.concatenate([a.reshape(-1) for a in case["fields"]])) == str(g["input_sha256"])
+    for one in (False, True):
+        keep: list = []
+        mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+        fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+        r = bridge.run_reference_fiber(mesh, fld, case["thresholds"], one_thread=one)
+        assert len(r.track_id) > 0
+        assert np.array_equal(r.simplices, g["simplices"])
+        assert np.array_equal(r.bary.view(np.uint32), g["bary"].view(np.uint32))
+        assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
+        assert np.array_equal(r.track_id, g["track_id"])
+        assert np.array_equal(r.edges, g["edges"])
+
+
+def test_fiber_fixture_exercises_the_centroid_fallback():
+    """Near the quantum 1/Q the reference keeps simplices whose solve fails,
+    at 1/3 each (predicate.hpp:354); the fixture holds such features."""
+    g = np.load(os.path.join(FIBER_GOLD, "fiber_near_quantum.npz"))
+    third = np.float64(1.0) / 3.0
+    assert (g["lam"] == third).all(axis=1).sum() > 10

@@ -1,0 +1,73 @@
+"""Fibers on the GPU (ftk2b_fiber_extract) against the reference engine with
+FiberPredicate<T> (predicate.hpp:341-362): on 2D+t meshes the features, float
+and field-precision barycentrics (centroid where the solve fails), track ids
+and star edges are identical to the reference's fixtures
+(tests/golden/make_contour_golden.py) and, where the prebuilt reference
+library is present, to a live reference run."""
+import os
+
+import numpy as np
+import pytest
+
+import contour_cases
+from ftk2_b200 import api
+from oracle import bridge
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber")
+
+
+def run_gpu(ctx, case, fields=None):
+    keep: list = []
+    mesh = api.regular_mesh_desc(case["local_dims"], case["offset"], case["global_dims"])
+    fd = api.field_desc(list(case["fields"] if fields is None else fields), api.LAYOUT_SEPARATE, 2, keep=keep)
+    return ctx.fiber(mesh, fd, case["thresholds"], case["q"])
+
+
+def assert_same(r, want, name=""):
+    assert len(r.track_id) == len(want["track_id"]), name
+    assert np.array_equal(r.simplices, want["simplices"]), name
+    assert np.array_equal(r.bary.view(np.uint32), want["bary"].view(np.uint32)), name
+    assert np.array_equal(r.lam.view(np.uint64), want["lam"].view(np.uint64)), name
+    assert np.array_equal(r.track_id, want["track_id"]), name
+    assert np.array_equal(r.edges, want["edges"]), name
+    assert not r.type.any() and not r.scalar.any()
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_CASES))
+def test_fiber_matches_reference_fixture(ctx, name):
+    case = contour_cases.FIBER_CASES[name]()
+    g = np.load(os.path.join(GOLD, f"{name}.npz"))
+    r = run_gpu(ctx, case)
+    assert len(r.track_id) > 0
+    assert_same(r, {k: g[k] for k in ("simplices", "bary", "lam", "track_id", "edges")}, name)
+    assert r.n_tracks == len(set(r.track_id.tolist()))
+
+
+@pytest.mark.parametrize("seed,dims,thr", [(41, [19, 17, 5], (0.0, 0.0)), (42, [8, 9, 3], (0.02, -0.01))])
+def test_fiber_random_vs_live_reference(ctx, seed, dims, thr):
+    if not bridge.ref_available():
+        pytest.skip("reference build absent")
+    f = contour_cases.gaussian_potential(tuple(dims[:2]), dims[2], seed=seed, n_blobs=6, dtype=np.float64,
+                                         sigma=(1.5, 4.0))
+    g = contour_cases.gaussian_potential(tuple(dims[:2]), dims[2], seed=seed + 100, n_blobs=6, dtype=np.float64,
+                                         sigma=(1.5, 4.0))
+    case = dict(fields=(f, g), local_dims=dims, offset=None, global_dims=None, thresholds=thr, q=1e6)
+    keep: list = []
+    ref = bridge.run_reference_fiber(bridge.make_regular_mesh(dims),
+                                     bridge.make_field([f, g], bridge.LAYOUT_SEPARATE, 2, sos_q=1e6, keep=keep), thr)
+    assert_same(run_gpu(ctx, case), {"simplices": ref.simplices, "bary": ref.bary, "lam": ref.lam,
+                                     "track_id": ref.track_id, "edges": ref.edges}, str(seed))
+
+
+def test_fiber_device_input_and_3d_unsupported(ctx):
+    torch = pytest.importorskip("torch")
+    case = contour_cases.fiber_gauss_f64()
+    host = run_gpu(ctx, case)
+    dev = run_gpu(ctx, case, [torch.from_numpy(a).cuda() for a in case["fields"]])
+    assert np.array_equal(host.simplices, dev.simplices) and np.array_equal(host.edges, dev.edges)
+    a = np.zeros((3, 4, 5, 6))
+    keep: list = []
+    with pytest.raises(api.Ftk2bError):
+        ctx.fiber(api.regular_mesh_desc([6, 5, 4, 3]), api.field_desc([a, a], api.LAYOUT_SEPARATE, 2, keep=keep))
