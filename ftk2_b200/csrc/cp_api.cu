@@ -155,6 +155,10 @@ extern "C" void ftk2b_ctx_destroy(ftk2b_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   ctx->drop_graphs();
   if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->d2h_pin[i]) cudaFreeHost(ctx->d2h_pin[i]);
+    if (ctx->d2h_ev[i]) cudaEventDestroy(ctx->d2h_ev[i]);
+  }
   if (ctx->batch.h_tab) cudaFreeHost(ctx->batch.h_tab);
   if (ctx->batch.h_fbase) cudaFreeHost(ctx->batch.h_fbase);
   cudaEventDestroy(ctx->ev0);

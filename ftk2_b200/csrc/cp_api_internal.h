@@ -157,6 +157,9 @@ struct ftk2b_ctx {
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::DevBuf attr_out, attr_desc, attr_stage[16];  // ftk2b_cp_attributes
   ftk2b::DevBuf contour[20];  // ftk2b_contour_extract scratch and outputs
+  // two pinned host chunks for large result copies (allocated on first use)
+  void* d2h_pin[2] = {nullptr, nullptr};
+  cudaEvent_t d2h_ev[2] = {nullptr, nullptr};
   ftk2b::ExtCache ext;
   ftk2b::BatchCtx batch;
   ftk2b::LastRun last;

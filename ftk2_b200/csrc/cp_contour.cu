@@ -54,6 +54,8 @@ struct CtGeom {
   unsigned long long loff[16];  // local linear step to corner e
   unsigned long long goff[16];  // global id step to corner e
   unsigned long long aoff[16];  // array step to corner e
+  unsigned long long lstr[4];   // local linear strides
+  unsigned char perm[24][4];    // axis order of the p-th Kuhn simplex (CPU mesh order)
 };
 
 __device__ __forceinline__ void ct_coords(const CtGeom& g, unsigned long long i, unsigned long long* c) {
@@ -219,242 +221,256 @@ __global__ void ct_emit_kernel(CtGeom g, const T* __restrict__ a, T thr, const u
   }
 }
 
-// Axis order of the p-th Kuhn simplex as the CPU mesh decodes it
-// (mesh.hpp:407-409): successive swaps p[i] <-> p[i + j], j = p % (d - i).
-__device__ __forceinline__ void ct_perm(int p_idx, int d, int* ax) {
-  for (int i = 0; i < 4; ++i) ax[i] = i;
-  int t = p_idx;
-  for (int i = 0; i < d; ++i) {
-    const int j = t % (d - i);
-    const int x = ax[i];
-    ax[i] = ax[i + j];
-    ax[i + j] = x;
-    t /= d - i;
+// Mixed hypercubes (corner signs not all equal) are listed once, each as one
+// word: base vertex (local linear index) << 20 | upper-face axes << 16 |
+// corner signs (bit e: corner e positive).  An upper-face axis k is one where
+// the cube's corners with bit k set lie on the mesh's last layer (c_k = L_k - 2).
+constexpr int kCtBaseShift = 20;
+
+__global__ void ct_mixed_kernel(CtGeom g, const unsigned char* __restrict__ pos,
+                                unsigned long long* __restrict__ list, unsigned* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int ne = 1 << g.d;
+  for (unsigned long long q0 = blockIdx.x * (unsigned long long)blockDim.x; q0 < g.ncube;
+       q0 += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long q = q0 + threadIdx.x;
+    unsigned long long word = 0;
+    bool mixed = false;
+    if (q < g.ncube) {
+      unsigned long long base = 0, r = q;
+      unsigned upper = 0;
+      for (int k = 0; k < g.d; ++k) {
+        const unsigned long long n = g.L[k] - 1, c = r % n;
+        r /= n;
+        base += c * g.lstr[k];
+        if (c + 2 == g.L[k]) upper |= 1u << k;
+      }
+      unsigned sgn = 0;
+      for (int e = 0; e < ne; ++e) sgn |= (unsigned)pos[base + g.loff[e]] << e;
+      mixed = sgn != 0 && sgn != (1u << ne) - 1u;
+      word = (base << kCtBaseShift) | ((unsigned long long)upper << 16) | sgn;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, mixed);
+    unsigned wbase = 0;
+    if (lane == 0 && bal) wbase = atomicAdd(cnt, (unsigned)__popc(bal));
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    if (mixed) list[wbase + __popc(bal & ((1u << lane) - 1u))] = word;
   }
 }
 
-struct CtCube {
-  unsigned long long base;  // local linear index of the hypercube's base vertex
-  unsigned long long c[4];
-  unsigned sgn;             // bit e: corner e is positive
+// One Kuhn simplex of a listed cube, for the lane that owns it: path corners
+// (corner bit masks along the CPU mesh's permutation order) and signs.
+struct CtSimplex {
+  int pe[5];      // corner of path vertex i
+  unsigned ps;    // bit i: path vertex i positive
+  int npos;
 };
 
-__device__ __forceinline__ bool ct_load_cube(const CtGeom& g, unsigned long long q, const unsigned char* pos,
-                                             CtCube* cb) {
-  unsigned long long base = 0, r = q, ls = 1;
-  for (int k = 0; k < g.d; ++k) {
-    const unsigned long long n = g.L[k] - 1;
-    cb->c[k] = r % n;
-    r /= n;
-    base += cb->c[k] * ls;
-    ls *= g.L[k];
+__device__ __forceinline__ void ct_simplex(const CtGeom& g, unsigned sgn, int p_idx, CtSimplex* x) {
+  x->pe[0] = 0;
+  x->ps = sgn & 1u;
+  x->npos = (int)(sgn & 1u);
+  for (int i = 0; i < g.d; ++i) {
+    x->pe[i + 1] = x->pe[i] | (1 << g.perm[p_idx][i]);
+    const unsigned b = (sgn >> x->pe[i + 1]) & 1u;
+    x->ps |= b << (i + 1);
+    x->npos += (int)b;
   }
-  cb->base = base;
-  unsigned s = 0;
-  const int ne = 1 << g.d;
-  for (int e = 0; e < ne; ++e) s |= (unsigned)pos[base + g.loff[e]] << e;
-  cb->sgn = s;
-  return s != 0 && s != (1u << ne) - 1u;  // mixed signs: some edge crosses
 }
 
-// feature index of the crossing edge from corner lo to corner hi (lo a subset
-// of hi) of the cube
-__device__ __forceinline__ unsigned ct_node(const CtGeom& g, const CtCube& cb, const unsigned short* mask,
-                                            const unsigned* voff, int lo, int hi) {
-  const unsigned long long v = cb.base + g.loff[lo];
+// feature index of the crossing edge from path vertex a to path vertex b of
+// the cube at local vertex base
+__device__ __forceinline__ unsigned ct_node(const CtGeom& g, unsigned long long base, const CtSimplex& x,
+                                            const unsigned short* __restrict__ mask,
+                                            const unsigned* __restrict__ voff, int a, int b) {
+  const int lo = x.pe[min(a, b)], hi = x.pe[max(a, b)];
+  const unsigned long long v = base + g.loff[lo];
   const int dir = hi ^ lo;
-  return voff[v] + __popc((unsigned)mask[v] & ((1u << (dir - 1)) - 1u));
+  return __ldg(voff + v) + __popc((unsigned)__ldg(mask + v) & ((1u << (dir - 1)) - 1u));
 }
 
-// the edge from corner lo starts on an upper boundary face (its lower vertex
-// is no hypercube base): the reference's first pass does not visit it
-__device__ __forceinline__ bool ct_late(const CtGeom& g, const CtCube& cb, int lo) {
-  for (int k = 0; k < g.d; ++k)
-    if (cb.c[k] + ((lo >> k) & 1) == g.L[k] - 1) return true;
-  return false;
-}
-
-// The crossing edges of one Kuhn simplex in the order the reference's
-// marching functions meet them, as (lower, upper) path positions: a 1-vs-rest
-// split pairs the lone vertex with the others in order; otherwise every
-// positive vertex with every other vertex, positives outer (2D+t 2-2 split).
-// Returns the count (the pentatope 2-3 split is handled by its caller).
-__device__ __forceinline__ int ct_lone(int npos, int nvtx, const bool* ps) {
-  if (npos == 1) {
+// The crossing edges of a 1-vs-rest or 2D+t 2-2 split in the order the
+// reference's marching functions meet them, as path-vertex pairs: the lone
+// vertex with the others in order; positives outer, others inner.
+__device__ __forceinline__ int ct_crossings(const CtSimplex& x, int nvtx, int* ea, int* eb) {
+  int ne = 0;
+  if (x.npos == 1 || x.npos == nvtx - 1) {
+    const bool lone_pos = x.npos == 1;
+    int lone = 0;
     for (int i = 0; i < nvtx; ++i)
-      if (ps[i]) return i;
+      if ((((x.ps >> i) & 1u) != 0) == lone_pos) lone = i;
+    for (int o = 0; o < nvtx; ++o)
+      if (o != lone) {
+        ea[ne] = lone;
+        eb[ne] = o;
+        ++ne;
+      }
+  } else {
+    for (int a = 0; a < nvtx; ++a) {
+      if (!((x.ps >> a) & 1u)) continue;
+      for (int b = 0; b < nvtx; ++b) {
+        if ((x.ps >> b) & 1u) continue;
+        ea[ne] = a;
+        eb[ne] = b;
+        ++ne;
+      }
+    }
   }
-  for (int i = 0; i < nvtx; ++i)
-    if (!ps[i]) return i;
-  return 0;
+  return ne;
 }
 
-__global__ void ct_first_kernel(CtGeom g, const unsigned char* __restrict__ pos,
+// lanes of a warp: np lanes per listed cube (one per Kuhn simplex), 32 / np
+// cubes per warp
+struct CtLane {
+  int np, per, sub, p_idx;
+  bool active;
+};
+
+__device__ __forceinline__ CtLane ct_lane(int d) {
+  CtLane l;
+  const int lane = threadIdx.x & 31;
+  l.np = d == 3 ? 6 : 24;
+  l.per = 32 / l.np;
+  l.sub = lane / l.np;
+  l.p_idx = lane % l.np;
+  l.active = l.sub < l.per;
+  return l;
+}
+
+// (2D+t) where the reference's sequential patching first meets each node whose
+// edge starts on an upper boundary face: (cube base, permutation index,
+// position in the marching enumeration), minimised over every meeting
+__global__ void ct_first_kernel(CtGeom g, const unsigned long long* __restrict__ list, const unsigned* list_cnt,
                                 const unsigned short* __restrict__ mask, const unsigned* __restrict__ voff,
                                 unsigned long long* __restrict__ first) {
-  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < g.ncube;
-       q += (unsigned long long)gridDim.x * blockDim.x) {
-    CtCube cb;
-    if (!ct_load_cube(g, q, pos, &cb)) continue;
-    for (int p_idx = 0; p_idx < 6; ++p_idx) {
-      int ax[4];
-      ct_perm(p_idx, 3, ax);
-      int pe[4];
-      pe[0] = 0;
-      for (int i = 0; i < 3; ++i) pe[i + 1] = pe[i] | (1 << ax[i]);
-      bool ps[4];
-      int npos = 0;
-      for (int i = 0; i < 4; ++i) {
-        ps[i] = (cb.sgn >> pe[i]) & 1u;
-        npos += ps[i];
-      }
-      if (npos == 0 || npos == 4) continue;
-      int lo_i[4], hi_i[4], ne = 0;
-      if (npos == 1 || npos == 3) {
-        const int lone = ct_lone(npos, 4, ps);
-        for (int o = 0; o < 4; ++o) {
-          if (o == lone) continue;
-          lo_i[ne] = min(lone, o);
-          hi_i[ne] = max(lone, o);
-          ++ne;
-        }
-      } else {
-        for (int a = 0; a < 4; ++a) {
-          if (!ps[a]) continue;
-          for (int b = 0; b < 4; ++b) {
-            if (ps[b]) continue;
-            lo_i[ne] = min(a, b);
-            hi_i[ne] = max(a, b);
-            ++ne;
-          }
-        }
-      }
-      for (int k = 0; k < ne; ++k) {
-        const int lo = pe[lo_i[k]], hi = pe[hi_i[k]];
-        if (!ct_late(g, cb, lo)) continue;
-        const unsigned nd = ct_node(g, cb, mask, voff, lo, hi);
-        const unsigned long long key = ((cb.base * 6ull) + (unsigned long long)p_idx) * 4ull + (unsigned long long)k;
-        atomicMin(first + nd, key);
-      }
+  const CtLane ln = ct_lane(3);
+  const unsigned nl = *list_cnt;
+  const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long it = warp * ln.per + ln.sub; ln.active && it < nl; it += nwarps * ln.per) {
+    const unsigned long long w = list[it];
+    const unsigned long long base = w >> kCtBaseShift;
+    const unsigned upper = (unsigned)(w >> 16) & 0xFu, sgn = (unsigned)w & 0xFFFFu;
+    CtSimplex x;
+    ct_simplex(g, sgn, ln.p_idx, &x);
+    if (x.npos == 0 || x.npos == 4) continue;
+    int ea[4], eb[4];
+    const int ne = ct_crossings(x, 4, ea, eb);
+    for (int k = 0; k < ne; ++k) {
+      const int lo = x.pe[min(ea[k], eb[k])];
+      if (!(lo & (int)upper)) continue;  // the edge starts at a hypercube base
+      const unsigned nd = ct_node(g, base, x, mask, voff, ea[k], eb[k]);
+      const unsigned long long key = ((base * 6ull) + (unsigned long long)ln.p_idx) * 4ull + (unsigned long long)k;
+      atomicMin(first + nd, key);
     }
   }
 }
 
-template <int K>
-__device__ __forceinline__ void ct_sort_small(unsigned* v) {
-#pragma unroll
-  for (int i = 1; i < K; ++i)
-#pragma unroll
-    for (int j = i; j > 0; --j)
-      if (v[j - 1] > v[j]) {
-        const unsigned x = v[j - 1];
-        v[j - 1] = v[j];
-        v[j] = x;
-      }
+__device__ __forceinline__ void ct_sort4(unsigned* v, int k) {
+  for (int i = 1; i < k; ++i)
+    for (int j = i; j > 0 && v[j - 1] > v[j]; --j) {
+      const unsigned x = v[j - 1];
+      v[j - 1] = v[j];
+      v[j] = x;
+    }
 }
 
-template <int K>
-__device__ __forceinline__ void ct_put(const unsigned* cell, unsigned* cells, unsigned* cnt, unsigned cap,
-                                       unsigned* parent, unsigned* err) {
-  unsigned v[K];
-#pragma unroll
-  for (int i = 0; i < K; ++i) v[i] = cell[i];
-  ct_sort_small<K>(v);
-  const unsigned slot = atomicAdd(cnt, 1u);
-  if (slot < cap) {
-#pragma unroll
-    for (int i = 0; i < K; ++i) cells[(size_t)slot * K + i] = v[i];
-  }
-#pragma unroll
-  for (int i = 1; i < K; ++i) uf_unite(parent, v[0], v[i], err);
-}
-
-__global__ void ct_cells_kernel(CtGeom g, const unsigned char* __restrict__ pos,
+// Marching tetrahedra (2D+t) / pentatopes (3D+t) on the listed cubes, one
+// Kuhn simplex per lane: up to three cells each, slots reserved per warp;
+// the simplex's crossing nodes are joined in the union-find by a star from its
+// first node (the same components as joining every cell's nodes).
+__global__ void ct_cells_kernel(CtGeom g, const unsigned long long* __restrict__ list, const unsigned* list_cnt,
                                 const unsigned short* __restrict__ mask, const unsigned* __restrict__ voff,
-                                const unsigned long long* __restrict__ first, unsigned n, unsigned* __restrict__ cells,
-                                unsigned* cnt, unsigned cap, unsigned* parent, unsigned* err) {
+                                const unsigned long long* __restrict__ first, unsigned n,
+                                unsigned* __restrict__ cells, unsigned* cnt, unsigned cap, unsigned* parent,
+                                unsigned* err) {
   const int d = g.d;
-  const int np = d == 3 ? 6 : 24;
-  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < g.ncube;
-       q += (unsigned long long)gridDim.x * blockDim.x) {
-    CtCube cb;
-    if (!ct_load_cube(g, q, pos, &cb)) continue;
-    for (int p_idx = 0; p_idx < np; ++p_idx) {
-      int ax[4];
-      ct_perm(p_idx, d, ax);
-      int pe[5];
-      pe[0] = 0;
-      for (int i = 0; i < d; ++i) pe[i + 1] = pe[i] | (1 << ax[i]);
-      bool ps[5];
-      int npos = 0;
-      for (int i = 0; i <= d; ++i) {
-        ps[i] = (cb.sgn >> pe[i]) & 1u;
-        npos += ps[i];
-      }
-      if (npos == 0 || npos == d + 1) continue;
-      auto node = [&](int i, int j) {
-        const int a = min(i, j), b = max(i, j);
-        return ct_node(g, cb, mask, voff, pe[a], pe[b]);
-      };
-      if (npos == 1 || npos == d) {
-        const int lone = ct_lone(npos, d + 1, ps);
-        unsigned cell[4];
-        int k = 0;
-        for (int o = 0; o <= d; ++o)
-          if (o != lone) cell[k++] = node(lone, o);
-        if (d == 3) ct_put<3>(cell, cells, cnt, cap, parent, err);
-        else ct_put<4>(cell, cells, cnt, cap, parent, err);
-      } else if (d == 3) {
-        // 2-2 split: the quad of the four crossing edges, cut along the
-        // diagonal from its node the reference numbered first
-        unsigned nd[4];
-        unsigned long long key[4];
-        int k = 0;
-        for (int a = 0; a < 4; ++a) {
-          if (!ps[a]) continue;
-          for (int b = 0; b < 4; ++b) {
-            if (ps[b]) continue;
-            nd[k] = node(a, b);
-            const unsigned long long f = first[nd[k]];
-            key[k] = f == ~0ull ? (unsigned long long)nd[k] : (unsigned long long)n + f;
-            ++k;
+  const int kc = d;  // entries per cell
+  const CtLane ln = ct_lane(d);
+  const int lane = threadIdx.x & 31;
+  const unsigned nl = *list_cnt;
+  const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long it0 = warp * ln.per; it0 < nl; it0 += nwarps * ln.per) {
+    const unsigned long long it = it0 + ln.sub;
+    unsigned cell[3][4];
+    unsigned nodes[6];
+    int nn = 0, ncell = 0;
+    if (ln.active && it < nl) {
+      const unsigned long long w = list[it];
+      const unsigned long long base = w >> kCtBaseShift;
+      CtSimplex x;
+      ct_simplex(g, (unsigned)w & 0xFFFFu, ln.p_idx, &x);
+      if (x.npos != 0 && x.npos != d + 1) {
+        if (x.npos == 1 || x.npos == d || d == 3) {
+          int ea[6], eb[6];
+          const int ne = ct_crossings(x, d + 1, ea, eb);
+          for (int k = 0; k < ne; ++k) nodes[k] = ct_node(g, base, x, mask, voff, ea[k], eb[k]);
+          nn = ne;
+          if (ne == d) {  // 1-vs-rest: one cell
+            for (int k = 0; k < d; ++k) cell[0][k] = nodes[k];
+            ncell = 1;
+          } else {  // 2D+t 2-2 split: the quad cut along the diagonal from the
+                    // node the reference numbered first
+            unsigned nd[4];
+            unsigned long long key[4];
+            for (int k = 0; k < 4; ++k) {
+              nd[k] = nodes[k];
+              const unsigned long long f = first[nd[k]];
+              key[k] = f == ~0ull ? (unsigned long long)nd[k] : (unsigned long long)n + f;
+            }
+            for (int i = 1; i < 4; ++i)
+              for (int j = i; j > 0 && key[j - 1] > key[j]; --j) {
+                const unsigned long long kx = key[j - 1];
+                key[j - 1] = key[j];
+                key[j] = kx;
+                const unsigned nx = nd[j - 1];
+                nd[j - 1] = nd[j];
+                nd[j] = nx;
+              }
+            cell[0][0] = nd[0], cell[0][1] = nd[1], cell[0][2] = nd[2];
+            cell[1][0] = nd[0], cell[1][1] = nd[2], cell[1][2] = nd[3];
+            ncell = 2;
           }
-        }
-        for (int i = 1; i < 4; ++i)
-          for (int j = i; j > 0 && key[j - 1] > key[j]; --j) {
-            const unsigned long long kx = key[j - 1];
-            key[j - 1] = key[j];
-            key[j] = kx;
-            const unsigned nx = nd[j - 1];
-            nd[j - 1] = nd[j];
-            nd[j] = nx;
+        } else {  // pentatope 2-3 split
+          const bool two_pos = x.npos == 2;
+          int two[2], three[3], n2 = 0, n3 = 0;
+          for (int i = 0; i < 5; ++i) {
+            if ((((x.ps >> i) & 1u) != 0) == two_pos) two[n2++] = i;
+            else three[n3++] = i;
           }
-        const unsigned t1[3] = {nd[0], nd[1], nd[2]};
-        const unsigned t2[3] = {nd[0], nd[2], nd[3]};
-        ct_put<3>(t1, cells, cnt, cap, parent, err);
-        ct_put<3>(t2, cells, cnt, cap, parent, err);
-      } else {
-        // pentatope 2-3 split: T0 / T1 = crossing edges from the pair's first /
-        // second vertex to the triple, in order; three tets
-        const bool two_pos = npos == 2;
-        int two[2], three[3], n2 = 0, n3 = 0;
-        for (int i = 0; i < 5; ++i) {
-          if (ps[i] == two_pos) two[n2++] = i;
-          else three[n3++] = i;
+          unsigned T0[3], T1[3];
+          for (int t = 0; t < 3; ++t) {
+            T0[t] = ct_node(g, base, x, mask, voff, two[0], three[t]);
+            T1[t] = ct_node(g, base, x, mask, voff, two[1], three[t]);
+          }
+          cell[0][0] = T0[0], cell[0][1] = T0[1], cell[0][2] = T0[2], cell[0][3] = T1[2];
+          cell[1][0] = T0[0], cell[1][1] = T0[1], cell[1][2] = T1[1], cell[1][3] = T1[2];
+          cell[2][0] = T0[0], cell[2][1] = T1[0], cell[2][2] = T1[1], cell[2][3] = T1[2];
+          for (int t = 0; t < 3; ++t) nodes[t] = T0[t], nodes[3 + t] = T1[t];
+          nn = 6;
+          ncell = 3;
         }
-        unsigned T0[3], T1[3];
-        for (int t = 0; t < 3; ++t) {
-          T0[t] = node(two[0], three[t]);
-          T1[t] = node(two[1], three[t]);
-        }
-        const unsigned c0[4] = {T0[0], T0[1], T0[2], T1[2]};
-        const unsigned c1[4] = {T0[0], T0[1], T1[1], T1[2]};
-        const unsigned c2[4] = {T0[0], T1[0], T1[1], T1[2]};
-        ct_put<4>(c0, cells, cnt, cap, parent, err);
-        ct_put<4>(c1, cells, cnt, cap, parent, err);
-        ct_put<4>(c2, cells, cnt, cap, parent, err);
       }
     }
+    // slots for the warp's cells
+    unsigned incl = (unsigned)ncell;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned wtot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned wbase = 0;
+    if (lane == 31 && wtot) wbase = atomicAdd(cnt, wtot);
+    wbase = __shfl_sync(0xffffffffu, wbase, 31);
+    unsigned slot = wbase + incl - (unsigned)ncell;
+    for (int c = 0; c < ncell; ++c, ++slot) {
+      ct_sort4(cell[c], kc);
+      if (slot < cap)
+        for (int k = 0; k < kc; ++k) cells[(size_t)slot * kc + k] = cell[c][k];
+    }
+    for (int k = 1; k < nn; ++k) uf_unite(parent, nodes[0], nodes[k], err);
   }
 }
 
@@ -532,9 +548,58 @@ ftk2b_status cfail(ftk2b_ctx* ctx, ftk2b_status st, const char* fmt, ...) {
                    "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
+// Device -> pageable host memory through two pinned chunks: the device copy
+// of one chunk overlaps the host copy of the previous one (a pageable
+// cudaMemcpy of a large result runs at a few GB/s).
+cudaError_t ct_d2h(ftk2b_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  constexpr size_t kChunk = size_t(32) << 20;
+  if (!bytes) return cudaSuccess;
+  for (int i = 0; i < 2; ++i) {
+    if (!ctx->d2h_pin[i]) {
+      cudaError_t e = cudaHostAlloc(&ctx->d2h_pin[i], kChunk, cudaHostAllocDefault);
+      if (e) {
+        ctx->d2h_pin[i] = nullptr;
+        return e;
+      }
+    }
+    if (!ctx->d2h_ev[i]) {
+      cudaError_t e = cudaEventCreateWithFlags(&ctx->d2h_ev[i], cudaEventDisableTiming);
+      if (e) return e;
+    }
+  }
+  auto* out = static_cast<unsigned char*>(dst);
+  const auto* in = static_cast<const unsigned char*>(src);
+  size_t off = 0, prev_off = 0, prev_n = 0;
+  int cur = 0, prev = -1;
+  while (off < bytes || prev >= 0) {
+    size_t n = 0;
+    if (off < bytes) {
+      n = std::min(kChunk, bytes - off);
+      cudaError_t e = cudaMemcpyAsync(ctx->d2h_pin[cur], in + off, n, cudaMemcpyDeviceToHost, ctx->stream);
+      if (!e) e = cudaEventRecord(ctx->d2h_ev[cur], ctx->stream);
+      if (e) return e;
+    }
+    if (prev >= 0) {
+      cudaError_t e = cudaEventSynchronize(ctx->d2h_ev[prev]);
+      if (e) return e;
+      std::memcpy(out + prev_off, ctx->d2h_pin[prev], prev_n);
+    }
+    if (off < bytes) {
+      prev = cur;
+      prev_off = off;
+      prev_n = n;
+      off += n;
+      cur ^= 1;
+    } else {
+      prev = -1;
+    }
+  }
+  return cudaSuccess;
+}
+
 enum {
   kBufField = 0, kBufPos, kBufMask, kBufBlk, kBufVoff, kBufSimp, kBufLam, kBufBary, kBufFirst, kBufParent,
-  kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount
+  kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount, kBufList
 };
 
 template <typename T>
@@ -585,9 +650,16 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   auto* first = d == 3 ? static_cast<unsigned long long*>(B[kBufFirst].p) : nullptr;
   ct_emit_kernel<T><<<(unsigned)nblk, kCtThreads, 0, st>>>(g, a, thr, mask, blk, voff, simp, lam, bary);
   ctx->launches += 1;
+  // the mixed hypercubes, once: every later stage walks this list
+  C_TRY(B[kBufList].ensure(8 * (g.ncube ? g.ncube : 1)));
+  auto* list = static_cast<unsigned long long*>(B[kBufList].p);
+  unsigned* list_cnt = counts + 4;
+  ct_mixed_kernel<<<grid_of(g.ncube, 256, 64ull * sms), 256, 0, st>>>(g, pos, list, list_cnt);
+  ctx->launches += 1;
+  const unsigned wgrid = 16u * sms;  // 8 warps per block
   if (d == 3 && n) {
     ct_fill_u64_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(first, ~0ull, n);
-    ct_first_kernel<<<grid_of(g.ncube, 256, 64ull * sms), 256, 0, st>>>(g, pos, mask, voff, first);
+    ct_first_kernel<<<wgrid, 256, 0, st>>>(g, list, list_cnt, mask, voff, first);
     ctx->launches += 2;
   }
 
@@ -602,7 +674,7 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
     auto* cells = static_cast<unsigned*>(B[kBufCells].p);
     C_TRY(cudaMemsetAsync(counts + 1, 0, 12, st));
     if (n) ct_iota_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(parent, n);
-    ct_cells_kernel<<<grid_of(g.ncube, 256, 64ull * sms), 256, 0, st>>>(g, pos, mask, voff, first, n, cells,
+    ct_cells_kernel<<<wgrid, 256, 0, st>>>(g, list, list_cnt, mask, voff, first, n, cells,
                                                                         counts + 1, cap, parent, counts + 3);
     ctx->launches += 2;
     C_TRY(cudaMemcpyAsync(&ncell, counts + 1, 4, cudaMemcpyDeviceToHost, st));
@@ -669,14 +741,12 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   res->cells = static_cast<uint32_t*>(std::malloc(4ull * kc * ccap));
   if (!res->simplices || !res->lambda || !res->barycentric || !res->track_id || !res->scalar || !res->cells)
     return cfail(ctx, FTK2B_OOM, "host result allocation failed");
-  if (n) {
-    C_TRY(cudaMemcpyAsync(res->simplices, simp, 16ull * n, cudaMemcpyDeviceToHost, st));
-    C_TRY(cudaMemcpyAsync(res->lambda, lam, 16ull * n, cudaMemcpyDeviceToHost, st));
-    C_TRY(cudaMemcpyAsync(res->barycentric, bary, 8ull * n, cudaMemcpyDeviceToHost, st));
-    C_TRY(cudaMemcpyAsync(res->track_id, track, 8ull * n, cudaMemcpyDeviceToHost, st));
-  }
-  if (ncell) C_TRY(cudaMemcpyAsync(res->cells, cells_out, 4ull * kc * ncell, cudaMemcpyDeviceToHost, st));
   C_TRY(ctx->sync());
+  C_TRY(ct_d2h(ctx, res->simplices, simp, 16ull * n));
+  C_TRY(ct_d2h(ctx, res->lambda, lam, 16ull * n));
+  C_TRY(ct_d2h(ctx, res->barycentric, bary, 8ull * n));
+  C_TRY(ct_d2h(ctx, res->track_id, track, 8ull * n));
+  C_TRY(ct_d2h(ctx, res->cells, cells_out, 4ull * kc * ncell));
   if (hc[3] & 1u) return cfail(ctx, FTK2B_CUDA_ERROR, "union-find did not settle");
   if (hc[3] & 2u) return cfail(ctx, FTK2B_CUDA_ERROR, "duplicate manifold cell");
   const float sc = (float)thr;
@@ -742,6 +812,19 @@ extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_d
   for (int k = 0; k < d; ++k) {
     lstr[k] = ls;
     ls *= g.L[k];
+  }
+  for (int k = 0; k < d; ++k) g.lstr[k] = lstr[k];
+  // axis order of the p-th Kuhn simplex as the CPU mesh decodes it
+  // (mesh.hpp:407-409): successive swaps p[i] <-> p[i + j], j = p % (d - i)
+  const int np = d == 3 ? 6 : 24;
+  for (int p = 0; p < np; ++p) {
+    int ax[4] = {0, 1, 2, 3}, t = p;
+    for (int i = 0; i < d; ++i) {
+      const int j = t % (d - i);
+      std::swap(ax[i], ax[i + j]);
+      t /= d - i;
+    }
+    for (int i = 0; i < 4; ++i) g.perm[p][i] = (unsigned char)ax[i];
   }
   for (int e = 0; e < (1 << d); ++e)
     for (int k = 0; k < d; ++k)

@@ -10,6 +10,9 @@ c4        precision workload: 256^3 x 8 float32 with 1e-3 noise
 c4_small  the same on 256^3 x 2
 c1        2D analytic 64 x 64 x 10 float64, Q = 1e6
 c3        batch of 256 float32 fields (2D and 3D, uneven sizes), one batched call per step
+contour   level set (threshold 0, Q = 2^20) of the 128^3 x 16 float64 Gaussian-sum potential
+          whose gradient is c2
+contour_small  the same potential on 128^3 x 8 (134 MB, larger than L2)
 """
 from __future__ import annotations
 
@@ -64,6 +67,21 @@ def run_batch_case(args):
                   f"host {1e3 * (time.perf_counter() - t):.3f} ms", flush=True)
 
 
+def run_contour_case(args):
+    """contour: one ftk2b_contour_extract per step on the device-resident potential."""
+    import torch
+    dims, nt = (128, 128, 128), (16 if args.case == "contour" else 8)
+    pot = generate.gaussian_potential_device(dims, nt, seed=1234, n_blobs=32)
+    torch.cuda.synchronize()
+    mesh = api.regular_mesh_desc([*dims, nt])
+    with api.Context(0) as ctx:
+        for i in range(args.steps):
+            t = time.perf_counter()
+            r = ctx.contour(mesh, pot, 0.0, 2.0 ** 20)
+            print(f"step {i}: {len(r.track_id)} features {len(r.cells)} cells {r.n_tracks} tracks  "
+                  f"device {r.device_ms:.3f} ms  host {1e3 * (time.perf_counter() - t):.3f} ms", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default="c2_small")
@@ -79,6 +97,8 @@ def main():
     import torch
     if args.case == "c3":
         return run_batch_case(args)
+    if args.case in ("contour", "contour_small"):
+        return run_contour_case(args)
     field, dims, m, q = make(args.case)
     torch.cuda.synchronize()
     with api.Context(0) as ctx:
