@@ -21,8 +21,9 @@
 //              from their smallest-numbered node)
 //   ct_cells   marching tetrahedra / pentatopes over every Kuhn simplex of
 //              every hypercube: manifold cells, union-find hooks
-//   sort       cells into lexicographic order (two stable radix passes)
-//   ct_gather  sorted cells, duplicates flagged
+//   buckets    cells into lexicographic order: counted and scattered by
+//              their leading node, each bucket's few rows sorted, duplicates
+//              flagged
 //   label      track id = the component's smallest feature index
 #include <algorithm>
 #include <cstdarg>
@@ -482,45 +483,84 @@ __global__ void ct_fill_u64_kernel(unsigned long long* __restrict__ v, unsigned 
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = x;
 }
 
-// sort keys: pass 0 the last two entries (k-2, k-1) of each cell, pass 1 the
-// leading ones (entry 0 of a triangle, entries 0 and 1 of a tet), read through
-// the permutation of pass 0
-__global__ void ct_key_kernel(const unsigned* __restrict__ cells, const unsigned* cnt_ptr, unsigned cap, int k,
-                              unsigned long long n, int pass, const unsigned* __restrict__ perm_in,
-                              unsigned long long* __restrict__ key, unsigned* __restrict__ val) {
+// Lexicographic order of the cells.  Each row is sorted, so the rows fall
+// into buckets by their leading node: counts per leading node, a scan, a
+// scatter into the buckets, then a small sort of each bucket's rows (a few
+// rows: the cells at one crossing edge).
+__global__ void ct_bucket_count_kernel(const unsigned* __restrict__ cells, const unsigned* cnt_ptr, unsigned cap,
+                                       int k, unsigned* __restrict__ bcount) {
+  const unsigned m = min(*cnt_ptr, cap);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    atomicAdd(bcount + cells[(size_t)i * k], 1u);
+}
+
+__global__ void ct_bucket_scatter_kernel(const unsigned* __restrict__ cells, const unsigned* cnt_ptr,
+                                         unsigned cap, int k, const unsigned* __restrict__ boff,
+                                         unsigned* __restrict__ bcur, unsigned* __restrict__ out) {
   const unsigned m = min(*cnt_ptr, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const unsigned src = pass == 0 ? i : perm_in[i];
-    const unsigned* c = cells + (size_t)src * k;
-    if (pass == 0) key[i] = (unsigned long long)c[k - 2] * n + c[k - 1];
-    else key[i] = k == 3 ? (unsigned long long)c[0] : (unsigned long long)c[0] * n + c[1];
-    val[i] = src;
+    const unsigned* c = cells + (size_t)i * k;
+    const unsigned a = c[0];
+    const unsigned dst = boff[a] + atomicAdd(bcur + a, 1u);
+    for (int j = 0; j < k; ++j) out[(size_t)dst * k + j] = c[j];
   }
 }
 
-__global__ void ct_gather_kernel(const unsigned* __restrict__ cells, const unsigned* __restrict__ perm,
-                                 const unsigned* cnt_ptr, unsigned cap, int k, unsigned* __restrict__ out,
-                                 unsigned* err) {
-  const unsigned m = min(*cnt_ptr, cap);
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const unsigned* c = cells + (size_t)perm[i] * k;
-    bool same = i > 0;
-    const unsigned* p = i > 0 ? cells + (size_t)perm[i - 1] * k : c;
-    for (int j = 0; j < k; ++j) {
-      out[(size_t)i * k + j] = c[j];
-      same = same && p[j] == c[j];
+__device__ __forceinline__ bool ct_row_less(const unsigned* x, const unsigned* y, int k) {
+  for (int j = 1; j < k; ++j)
+    if (x[j] != y[j]) return x[j] < y[j];
+  return false;
+}
+
+// one thread per leading node: insertion sort of its bucket's rows by their
+// remaining entries; equal neighbours (duplicate cells) raise bit 1 of *err
+__global__ void ct_bucket_sort_kernel(unsigned* __restrict__ rows, const unsigned* __restrict__ boff, unsigned n,
+                                      int k, unsigned* err) {
+  for (unsigned a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const unsigned lo = boff[a], hi = boff[a + 1];
+    for (unsigned i = lo + 1; i < hi; ++i) {
+      unsigned cur[4];
+      for (int j = 0; j < k; ++j) cur[j] = rows[(size_t)i * k + j];
+      unsigned p = i;
+      while (p > lo && ct_row_less(cur, rows + (size_t)(p - 1) * k, k)) {
+        for (int j = 0; j < k; ++j) rows[(size_t)p * k + j] = rows[(size_t)(p - 1) * k + j];
+        --p;
+      }
+      for (int j = 0; j < k; ++j) rows[(size_t)p * k + j] = cur[j];
     }
-    if (same) atomicOr(err, 2u);
+    for (unsigned i = lo + 1; i < hi; ++i)
+      if (!ct_row_less(rows + (size_t)(i - 1) * k, rows + (size_t)i * k, k)) atomicOr(err, 2u);
   }
 }
 
-int bitlen(unsigned long long x) {
-  int b = 0;
-  while (x) {
-    ++b;
-    x >>= 1;
+// Exclusive scan of n counters in place (n up to 2^32 - 1): per-block scans
+// of 2048 entries with their totals, a scan of the totals, the block offsets
+// added back.
+constexpr int kScanPer = 8;  // entries per thread
+__global__ void ct_scan_blocks_kernel(unsigned* __restrict__ a, unsigned n, unsigned* __restrict__ tot) {
+  __shared__ unsigned btot;
+  const unsigned long long b0 = (unsigned long long)blockIdx.x * kCtThreads * kScanPer;
+  const unsigned long long t0 = b0 + (unsigned long long)threadIdx.x * kScanPer;
+  unsigned v[kScanPer], sum = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) {
+    v[j] = t0 + j < n ? a[t0 + j] : 0u;
+    sum += v[j];
   }
-  return b < 1 ? 1 : b;
+  unsigned run = ct_block_scan(sum, &btot);
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) {
+    if (t0 + j < n) a[t0 + j] = run;
+    run += v[j];
+  }
+  if (threadIdx.x == 0) tot[blockIdx.x] = btot;
+}
+
+__global__ void ct_scan_add_kernel(unsigned* __restrict__ a, unsigned n, const unsigned* __restrict__ tot) {
+  const unsigned long long b0 = (unsigned long long)blockIdx.x * kCtThreads * kScanPer;
+  const unsigned add = tot[blockIdx.x];
+  for (int j = threadIdx.x; j < kCtThreads * kScanPer; j += kCtThreads)
+    if (b0 + j < n) a[b0 + j] += add;
 }
 
 unsigned grid_of(unsigned long long work, int threads, unsigned long long max_blocks) {
@@ -685,41 +725,30 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   }
   auto* cells = static_cast<unsigned*>(B[kBufCells].p);
 
-  // lexicographic order of the cells: a stable pass on the trailing pair,
-  // then one on the leading entry (or pair)
+  // lexicographic order of the cells: buckets by leading node, then each
+  // bucket's rows sorted
   const unsigned ccap = ncell ? ncell : 1;
-  const int grid = ctx->sort_grid(ccap);
-  C_TRY(B[kBufKey0].ensure(8ull * ccap));
-  C_TRY(B[kBufKey1].ensure(8ull * ccap));
-  C_TRY(B[kBufVal0].ensure(4ull * ccap));
-  C_TRY(B[kBufVal1].ensure(4ull * ccap));
-  C_TRY(B[kBufHist].ensure(4ull * 256 * grid));
+  const unsigned nb = n + 1;  // bucket offsets, the last one the total
+  const unsigned sblocks = (unsigned)((nb + kCtThreads * kScanPer - 1) / (kCtThreads * kScanPer));
+  C_TRY(B[kBufKey0].ensure(4ull * nb));            // counts, then offsets
+  C_TRY(B[kBufKey1].ensure(4ull * nb));            // scatter cursors
+  C_TRY(B[kBufVal0].ensure(4ull * (sblocks + 1)));  // scan block totals
   C_TRY(B[kBufCellsOut].ensure(4ull * kc * ccap));
-  auto* k0 = static_cast<unsigned long long*>(B[kBufKey0].p);
-  auto* k1 = static_cast<unsigned long long*>(B[kBufKey1].p);
-  auto* v0 = static_cast<unsigned*>(B[kBufVal0].p);
-  auto* v1 = static_cast<unsigned*>(B[kBufVal1].p);
-  auto* hist = static_cast<unsigned*>(B[kBufHist].p);
+  auto* boff = static_cast<unsigned*>(B[kBufKey0].p);
+  auto* bcur = static_cast<unsigned*>(B[kBufKey1].p);
+  auto* btot = static_cast<unsigned*>(B[kBufVal0].p);
   auto* cells_out = static_cast<unsigned*>(B[kBufCellsOut].p);
-  const unsigned long long nn = n ? n : 1;
-  const int bits_pair = bitlen(nn * nn - 1);
-  const unsigned cg = grid_of(ccap, 256, 8ull * sms);
-  const unsigned* perm = nullptr;
+  const unsigned cg = grid_of(ccap, 256, 16ull * sms);
   if (ncell) {
-    ct_key_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, nn, 0, nullptr, k0, v0);
-    const bool alt0 = radix_sort(k0, v0, k1, v1, counts + 1, ccap, bits_pair, hist, grid, st, &ctx->launches);
-    const unsigned* perm0 = alt0 ? v1 : v0;
-    // pass 1 reads pass 0's permutation into the other value buffer's pair
-    unsigned long long* kk = alt0 ? k0 : k1;
-    unsigned* vv = alt0 ? v0 : v1;
-    unsigned long long* kk2 = alt0 ? k1 : k0;
-    unsigned* vv2 = alt0 ? v1 : v0;
-    ct_key_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, nn, 1, perm0, kk, vv);
-    const int bits1 = kc == 3 ? bitlen(nn - 1) : bits_pair;
-    const bool alt1 = radix_sort(kk, vv, kk2, vv2, counts + 1, ccap, bits1, hist, grid, st, &ctx->launches);
-    perm = alt1 ? vv2 : vv;
-    ct_gather_kernel<<<cg, 256, 0, st>>>(cells, perm, counts + 1, cap, kc, cells_out, counts + 3);
-    ctx->launches += 3;
+    C_TRY(cudaMemsetAsync(boff, 0, 4ull * nb, st));
+    C_TRY(cudaMemsetAsync(bcur, 0, 4ull * nb, st));
+    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, boff);
+    ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
+    ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, boff, bcur, cells_out);
+    ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(cells_out, boff, n, kc, counts + 3);
+    ctx->launches += 6;
   }
   if (n) {
     C_TRY(launch_uf_label(parent, counts + 0, n, track, counts + 2, st));

@@ -9,10 +9,15 @@ The reference's execute_cuda (engine.hpp:273-425) and its extraction kernel
 oracle/_ref/libftk2refcuda.so, run in a child process because the reference
 ends the process on any CUDA error.  Its GPU path reads separate component
 arrays only (predicate.hpp:112), so the child splits the field by component.
-The test checks that the incumbent finds the same set of simplices as this
-implementation and records the timings of both when FTK2B_INCUMBENT_JSON names
-an output file.  It runs only when FTK2B_INCUMBENT=1 (it is a measurement
-of the reference, bounded by a 300 s limit on the child process)."""
+The incumbent's feature set differs from its own CPU engine's (which this
+implementation reproduces bit for bit) in two documented ways, and the test
+checks that every difference is one of them: its kernel extracts only the
+simplices that start at a hypercube base, never the upper-boundary ones the CPU
+engine's patching adds (engine.hpp:1352-1367 against cuda_engine.hpp:396-404),
+and it keeps a simplex whose solve fails at the centroid where the CPU engine
+rejects it (predicate.hpp:115 against :74).  It records the timings of both
+when FTK2B_INCUMBENT_JSON names an output file.  It runs only when FTK2B_INCUMBENT=1 (it is a measurement
+of the reference, bounded by a 240 s limit on the child process)."""
 import json
 import os
 import subprocess
@@ -45,22 +50,14 @@ kernel_ms, n_nodes = bridge.time_reference_cuda_kernel(mesh, field, reps=1)
 t = time.perf_counter()
 res, exec_ms, complex_ms = bridge.run_reference_cuda(mesh, field)
 wall_ms = (time.perf_counter() - t) * 1e3
-np.savez(sys.argv[3], simplices=res.simplices, track_id=res.track_id, edges=res.edges)
+np.savez(sys.argv[3], simplices=res.simplices, bary=res.bary, track_id=res.track_id, edges=res.edges)
 json.dump({"kernel_ms": kernel_ms, "kernel_nodes": n_nodes, "execute_cuda_ms": exec_ms,
            "get_complex_ms": complex_ms, "wall_ms": wall_ms}, open(sys.argv[4], "w"))
 """
 
 
-def partition(simplices, track_id):
-    """Feature simplices grouped by track, as a set of frozensets of rows."""
-    groups: dict = {}
-    for row, t in zip(map(tuple, simplices.tolist()), track_id.tolist()):
-        groups.setdefault(t, set()).add(row)
-    return {frozenset(g) for g in groups.values()}
-
-
 @pytest.mark.skipif(os.environ.get("FTK2B_INCUMBENT") != "1", reason="measurement run only (FTK2B_INCUMBENT=1)")
-def test_incumbent_gpu_path_same_simplices(ctx, tmp_path):
+def test_incumbent_gpu_path_timed_and_differences_explained(ctx, tmp_path):
     torch = pytest.importorskip("torch")
     from oracle import bridge
     if not os.path.exists(bridge.REF_CUDA_LIB):
@@ -71,7 +68,7 @@ def test_incumbent_gpu_path_same_simplices(ctx, tmp_path):
     np.save(tmp_path / "field.npy", host)
     r = subprocess.run([sys.executable, "-c", CHILD, ROOT, str(tmp_path / "field.npy"),
                         str(tmp_path / "ref.npz"), str(tmp_path / "ref.json")],
-                       capture_output=True, text=True, timeout=300)
+                       capture_output=True, text=True, timeout=240)
     assert r.returncode == 0, r.stderr[-2000:]
     ref = np.load(tmp_path / "ref.npz")
     info = json.load(open(tmp_path / "ref.json"))
@@ -92,16 +89,31 @@ def test_incumbent_gpu_path_same_simplices(ctx, tmp_path):
 
     ours = {tuple(x) for x in mine.simplices.tolist()}
     theirs = {tuple(x) for x in ref["simplices"].tolist()}
+    only_ours, only_theirs = ours - theirs, theirs - ours
+
+    def on_upper_face(simplex):
+        v, c = int(simplex[0]), []
+        for n in DIMS:
+            c.append(v % n)
+            v //= n
+        return any(ci == n - 1 for ci, n in zip(c, DIMS))
+
+    bary = {tuple(s_): b for s_, b in zip(ref["simplices"].tolist(), ref["bary"].tolist())}
     info.update({
         "workload": "3D Gaussian-sum gradient, 64^3 x 8 float64, 32 blobs, Q = 2^20",
-        "ours_features": len(ours), "incumbent_features": len(theirs),
-        "same_simplex_set": ours == theirs,
-        "same_tracks": partition(mine.simplices, mine.track_id) == partition(ref["simplices"], ref["track_id"]),
+        "ours_features": len(ours), "incumbent_features": len(theirs), "common": len(ours & theirs),
+        "only_ours": len(only_ours), "only_ours_start_on_upper_face": sum(map(on_upper_face, only_ours)),
+        "only_incumbent": len(only_theirs),
+        "only_incumbent_at_centroid": sum(all(x == 0.25 for x in bary[t]) for t in only_theirs),
         "ours_device_input_ms": min(dev_ms), "ours_host_input_ms": min(e2e_ms),
+        "speedup_kernel_vs_ours_device_call": info["kernel_ms"] / min(dev_ms),
+        "speedup_execute_cuda_vs_ours_host_call": info["execute_cuda_ms"] / min(e2e_ms),
     })
     out = os.environ.get("FTK2B_INCUMBENT_JSON")
     if out:
         with open(out, "w") as fh:
             json.dump(info, fh, indent=1)
     print(json.dumps(info))
-    assert ours == theirs
+    assert info["common"] > 0
+    assert info["only_ours_start_on_upper_face"] == info["only_ours"]
+    assert info["only_incumbent_at_centroid"] == info["only_incumbent"]
