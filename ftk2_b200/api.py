@@ -117,6 +117,15 @@ class ContourResultC(C.Structure):
     ]
 
 
+class FiberSurfaceResultC(C.Structure):
+    _fields_ = [
+        ("n_features", C.c_uint64), ("simplices", C.POINTER(C.c_uint64)), ("lambda_", C.POINTER(C.c_double)),
+        ("barycentric", C.POINTER(C.c_float)), ("track_id", C.POINTER(C.c_uint64)),
+        ("scalar", C.POINTER(C.c_float)), ("n_cells", C.c_uint64), ("cells", C.POINTER(C.c_uint32)),
+        ("n_tracks", C.c_uint64), ("n_simplices", C.c_uint64), ("device_ms", C.c_double),
+    ]
+
+
 REQ_EXTRACT, REQ_STREAM_PUSH = 0, 1
 
 
@@ -146,6 +155,10 @@ SIGNATURES = {
     "ftk2b_contour_result_free": (None, [C.POINTER(ContourResultC)]),
     "ftk2b_fiber_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                       C.POINTER(C.c_double), C.c_double, C.POINTER(C.POINTER(CPResultC))]),
+    "ftk2b_fiber_surface_extract": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
+                                              C.POINTER(C.c_double), C.c_double,
+                                              C.POINTER(C.POINTER(FiberSurfaceResultC))]),
+    "ftk2b_fiber_surface_result_free": (None, [C.POINTER(FiberSurfaceResultC)]),
     "ftk2b_cp_run": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                C.POINTER(CPParams), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ftk2b_cp_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(CPResultC))]),
@@ -454,6 +467,35 @@ class Context:
             return _result_from_c(out.contents)
         finally:
             self.lib.ftk2b_cp_result_free(out)
+
+    def fiber_surface(self, mesh: MeshDesc, field: FieldDesc, thresholds=(0.0, 0.0),
+                      sos_q: float = 1e6) -> ContourResult:
+        """Fiber surfaces (FiberPredicate<T>) of two scalar fields on a regular
+        3D+t mesh: triangle features (simplices (n, 3)) and the star-fan
+        triangles of get_complex (cells (c, 3))."""
+        thr = (C.c_double * 2)(float(thresholds[0]), float(thresholds[1]))
+        out = C.POINTER(FiberSurfaceResultC)()
+        self._check(self.lib.ftk2b_fiber_surface_extract(self.h, C.byref(mesh), C.byref(field), thr,
+                                                         float(sos_q), C.byref(out)))
+        try:
+            r = out.contents
+            n, c = int(r.n_features), int(r.n_cells)
+
+            def arr(ptr, count, dt):
+                if count == 0:
+                    return np.zeros(0, dtype=dt)
+                return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+            return ContourResult(
+                simplices=arr(r.simplices, 3 * n, np.uint64).reshape(n, 3),
+                lam=arr(r.lambda_, 3 * n, np.float64).reshape(n, 3),
+                bary=arr(r.barycentric, 3 * n, np.float32).reshape(n, 3),
+                track_id=arr(r.track_id, n, np.uint64),
+                scalar=arr(r.scalar, n, np.float32),
+                cells=arr(r.cells, 3 * c, np.uint32).reshape(c, 3),
+                n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
+        finally:
+            self.lib.ftk2b_fiber_surface_result_free(out)
 
     def run(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None):
         """Device pipeline only; results stay on the device until fetch()."""

@@ -513,9 +513,11 @@ __device__ __forceinline__ bool ct_row_less(const unsigned* x, const unsigned* y
 }
 
 // one thread per leading node: insertion sort of its bucket's rows by their
-// remaining entries; equal neighbours (duplicate cells) raise bit 1 of *err
+// remaining entries.  Without uniq, equal neighbours (duplicate cells) raise
+// bit 1 of *err; with uniq, they are dropped (the unique rows stay at the
+// start of the bucket, their count in uniq[a]).
 __global__ void ct_bucket_sort_kernel(unsigned* __restrict__ rows, const unsigned* __restrict__ boff, unsigned n,
-                                      int k, unsigned* err) {
+                                      int k, unsigned* err, unsigned* __restrict__ uniq) {
   for (unsigned a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
     const unsigned lo = boff[a], hi = boff[a + 1];
     for (unsigned i = lo + 1; i < hi; ++i) {
@@ -528,8 +530,31 @@ __global__ void ct_bucket_sort_kernel(unsigned* __restrict__ rows, const unsigne
       }
       for (int j = 0; j < k; ++j) rows[(size_t)p * k + j] = cur[j];
     }
-    for (unsigned i = lo + 1; i < hi; ++i)
-      if (!ct_row_less(rows + (size_t)(i - 1) * k, rows + (size_t)i * k, k)) atomicOr(err, 2u);
+    if (!uniq) {
+      for (unsigned i = lo + 1; i < hi; ++i)
+        if (!ct_row_less(rows + (size_t)(i - 1) * k, rows + (size_t)i * k, k)) atomicOr(err, 2u);
+    } else {
+      unsigned w = lo;
+      for (unsigned i = lo; i < hi; ++i) {
+        if (i > lo && !ct_row_less(rows + (size_t)(w - 1) * k, rows + (size_t)i * k, k)) continue;
+        if (w != i)
+          for (int j = 0; j < k; ++j) rows[(size_t)w * k + j] = rows[(size_t)i * k + j];
+        ++w;
+      }
+      uniq[a] = w - lo;
+    }
+  }
+}
+
+// unique rows of every bucket to their place in the output (uoff: scanned
+// unique counts)
+__global__ void ct_bucket_compact_kernel(const unsigned* __restrict__ rows, const unsigned* __restrict__ boff,
+                                         const unsigned* __restrict__ uoff, unsigned n, int k,
+                                         unsigned* __restrict__ out) {
+  for (unsigned a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const unsigned lo = boff[a], cnt = uoff[a + 1] - uoff[a], dst = uoff[a];
+    for (unsigned i = 0; i < cnt; ++i)
+      for (int j = 0; j < k; ++j) out[(size_t)(dst + i) * k + j] = rows[(size_t)(lo + i) * k + j];
   }
 }
 
@@ -639,7 +664,8 @@ cudaError_t ct_d2h(ftk2b_ctx* ctx, void* dst, const void* src, size_t bytes) {
 
 enum {
   kBufField = 0, kBufPos, kBufMask, kBufBlk, kBufVoff, kBufSimp, kBufLam, kBufBary, kBufFirst, kBufParent,
-  kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount, kBufList
+  kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount, kBufList,
+  kBufField2
 };
 
 template <typename T>
@@ -747,7 +773,8 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
     C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
     ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
     ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, boff, bcur, cells_out);
-    ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(cells_out, boff, n, kc, counts + 3);
+    ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(cells_out, boff, n, kc, counts + 3,
+                                                                         nullptr);
     ctx->launches += 6;
   }
   if (n) {
@@ -787,7 +814,390 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   return FTK2B_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Fiber surfaces: FiberPredicate<T> on a regular 3D+t mesh (predicate.hpp:
+// 341-362; form_general_manifold_patches with k = 2, engine.hpp:1341-1418).
+// Features are the mesh triangles where both fields minus their thresholds
+// have the origin inside (simulation of simplicity, 2-D).  Every triangle of
+// the Freudenthal mesh is (c, c + a, c + b) for corner masks 0 < a < b, a a
+// subset of b (50 types in a 4-cube), so triangles in simplex order are
+// (c, a, b) in vertex order, then a, then b as binary numbers: ranks again
+// come from per-vertex masks and a scan.  The reference's node code
+// (v_min << 24 | a << 4 | b, mesh.hpp:736-749) orders triangles the same way,
+// so its star centres are the smallest ranks.
+
+struct FsTables {
+  unsigned char ta[50], tb[50];  // corner masks of the second and third vertex, by type
+  unsigned char idx[16][16];     // type of (a, b), 255 where (a, b) is no triangle
+};
+
+// per vertex and component: bit 2j positive (quantised >= 1), bit 2j+1
+// negative (<= -1); zero leaves both clear
+template <typename T>
+__global__ void fs_class_kernel(CtGeom g, const T* __restrict__ f0, const T* __restrict__ f1, T t0, T t1,
+                                double q, unsigned char* __restrict__ cls) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < g.nv;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long c[4];
+    ct_coords(g, i, c);
+    const unsigned long long gid = ct_gid(g, c), ai = ct_aidx(g, c);
+    unsigned char b = 0;
+    const T v[2] = {ct_adj(g, f0, ai, gid, t0), ct_adj(g, f1, ai, gid, t1)};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const double x = __dadd_rn(__dmul_rn((double)v[j], q), v[j] > T(0) ? 0.5 : -0.5);
+      if (x >= 1.0) b |= (unsigned char)(1u << (2 * j));
+      if (x <= -1.0) b |= (unsigned char)(2u << (2 * j));
+    }
+    cls[i] = b;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void fs_values(const CtGeom& g, const T* f0, const T* f1, T t0, T t1,
+                                          unsigned long long ai, unsigned long long gid, int a, int b, T v[3][2]) {
+  const unsigned long long ao[3] = {0ull, g.aoff[a], g.aoff[b]}, go[3] = {0ull, g.goff[a], g.goff[b]};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    v[i][0] = ct_adj(g, f0, ai + ao[i], gid + go[i], t0);
+    v[i][1] = ct_adj(g, f1, ai + ao[i], gid + go[i], t1);
+  }
+}
+
+// per vertex: bit t of the 50-bit mask = triangle type t from this vertex is
+// a feature.  One component of one strict sign at all three vertices keeps
+// the origin outside whatever the ties (exact pre-test); the rest go through
+// the exact 2-D test.
+template <typename T>
+__global__ void fs_mask_kernel(CtGeom g, FsTables tb, const T* __restrict__ f0, const T* __restrict__ f1, T t0,
+                               T t1, double q, const unsigned char* __restrict__ cls,
+                               unsigned long long* __restrict__ mask, unsigned* __restrict__ blk,
+                               unsigned long long* __restrict__ total64) {
+  __shared__ unsigned tot;
+  const unsigned long long i = blockIdx.x * (unsigned long long)kCtThreads + threadIdx.x;
+  unsigned long long m = 0;
+  if (i < g.nv) {
+    unsigned long long c[4];
+    ct_coords(g, i, c);
+    const unsigned inb = ct_inbounds(g, c);
+    const unsigned long long gid = ct_gid(g, c), ai = ct_aidx(g, c);
+    const unsigned c0 = cls[i];
+    for (int t = 0; t < 50; ++t) {
+      const int a = tb.ta[t], b = tb.tb[t];
+      if (b & ~inb) continue;
+      const unsigned all = c0 & cls[i + g.loff[a]] & cls[i + g.loff[b]];
+      if (all) continue;
+      T v[3][2];
+      fs_values(g, f0, f1, t0, t1, ai, gid, a, b, v);
+      if (sos_inside2<T>(v, q)) m |= 1ull << t;
+    }
+    mask[i] = m;
+  }
+  ct_block_scan((unsigned)__popcll(m), &tot);
+  if (threadIdx.x == 0) {
+    blk[blockIdx.x] = tot;
+    atomicAdd(total64, (unsigned long long)tot);
+  }
+}
+
+template <typename T>
+__global__ void fs_emit_kernel(CtGeom g, FsTables tb, const T* __restrict__ f0, const T* __restrict__ f1, T t0,
+                               T t1, const unsigned long long* __restrict__ mask,
+                               const unsigned* __restrict__ blk_off, unsigned* __restrict__ voff,
+                               unsigned long long* __restrict__ simp, double* __restrict__ lam,
+                               float* __restrict__ bary) {
+  __shared__ unsigned tot;
+  const unsigned long long i = blockIdx.x * (unsigned long long)kCtThreads + threadIdx.x;
+  const unsigned long long m = i < g.nv ? mask[i] : 0ull;
+  const unsigned base = blk_off[blockIdx.x] + ct_block_scan((unsigned)__popcll(m), &tot);
+  if (i >= g.nv) return;
+  voff[i] = base;
+  if (!m) return;
+  unsigned long long c[4];
+  ct_coords(g, i, c);
+  const unsigned long long gid = ct_gid(g, c), ai = ct_aidx(g, c);
+  unsigned r = base;
+  for (int t = 0; t < 50; ++t) {
+    if (!((m >> t) & 1ull)) continue;
+    const int a = tb.ta[t], b = tb.tb[t];
+    T v[3][2];
+    fs_values(g, f0, f1, t0, t1, ai, gid, a, b, v);
+    T l[3];
+    if (!solve_exact<2, T>(v, l))  // FiberPredicate keeps the centroid: (T)1.0 / 3.0
+      for (int k = 0; k < 3; ++k) l[k] = (T)((double)(T)1.0 / 3.0);
+    simp[3 * (size_t)r] = gid;
+    simp[3 * (size_t)r + 1] = gid + g.goff[a];
+    simp[3 * (size_t)r + 2] = gid + g.goff[b];
+    for (int k = 0; k < 3; ++k) {
+      lam[3 * (size_t)r + k] = (double)l[k];
+      bary[3 * (size_t)r + k] = (float)l[k];
+    }
+    ++r;
+  }
+}
+
+// hypercubes with a feature triangle at one of their lower corners (a
+// superset of the cubes whose pentatopes hold features)
+__global__ void fs_list_kernel(CtGeom g, const unsigned long long* __restrict__ mask,
+                               unsigned long long* __restrict__ list, unsigned* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  for (unsigned long long q0 = blockIdx.x * (unsigned long long)blockDim.x; q0 < g.ncube;
+       q0 += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long q = q0 + threadIdx.x;
+    bool any = false;
+    unsigned long long base = 0;
+    if (q < g.ncube) {
+      unsigned long long r = q;
+      for (int k = 0; k < g.d; ++k) {
+        const unsigned long long n = g.L[k] - 1, c = r % n;
+        r /= n;
+        base += c * g.lstr[k];
+      }
+      for (int e = 0; e < 15 && !any; ++e) any = mask[base + g.loff[e]] != 0ull;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, any);
+    unsigned wbase = 0;
+    if (lane == 0 && bal) wbase = atomicAdd(cnt, (unsigned)__popc(bal));
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    if (any) list[wbase + __popc(bal & ((1u << lane) - 1u))] = base;
+  }
+}
+
+// One pentatope per lane (24 per listed cube): its feature triangles in rank
+// order (the reference's code order), the star centre h_S = the first; per
+// tet face (path vertex i left out), the face's feature triangles in order,
+// h_T the first, and a triangle {h_S, h_T, n} for every later n, unless h_S is
+// h_T or n (engine.hpp:1388-1413).  Two passes: count, reserve per warp, write.
+__global__ void fs_cells_kernel(CtGeom g, FsTables tb, const unsigned long long* __restrict__ list,
+                                const unsigned* list_cnt, const unsigned long long* __restrict__ mask,
+                                const unsigned* __restrict__ voff, unsigned* __restrict__ cells, unsigned* cnt,
+                                unsigned cap, unsigned* parent, unsigned* err) {
+  const int lane = threadIdx.x & 31;
+  const unsigned nl = *list_cnt;
+  const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long it = warp; it < nl; it += nwarps) {
+    unsigned rank[10], vset[10];
+    int nn = 0;
+    if (lane < 24) {
+      const unsigned long long base = list[it];
+      int pe[5];
+      pe[0] = 0;
+      for (int i = 0; i < 4; ++i) pe[i + 1] = pe[i] | (1 << g.perm[lane][i]);
+      for (int i = 0; i < 3; ++i)
+        for (int j = i + 1; j < 4; ++j)
+          for (int k = j + 1; k < 5; ++k) {
+            const int lo = pe[i], t = tb.idx[pe[j] ^ lo][pe[k] ^ lo];
+            const unsigned long long v = base + g.loff[lo];
+            const unsigned long long mv = __ldg(mask + v);
+            if (!((mv >> t) & 1ull)) continue;
+            unsigned rk = __ldg(voff + v) + (unsigned)__popcll(mv & ((1ull << t) - 1ull));
+            unsigned vs = (1u << i) | (1u << j) | (1u << k);
+            int p = nn++;
+            while (p > 0 && rank[p - 1] > rk) {
+              rank[p] = rank[p - 1];
+              vset[p] = vset[p - 1];
+              --p;
+            }
+            rank[p] = rk;
+            vset[p] = vs;
+          }
+    }
+    // pass 1: count
+    unsigned mine = 0;
+    if (nn >= 2) {
+      const unsigned hs = rank[0];
+      for (int f = 0; f < 5; ++f) {
+        int seen = 0;
+        unsigned ht = 0;
+        for (int x = 0; x < nn; ++x) {
+          if (vset[x] & (1u << f)) continue;
+          if (seen++ == 0) {
+            ht = rank[x];
+            continue;
+          }
+          if (hs != ht && hs != rank[x]) ++mine;
+        }
+      }
+    }
+    unsigned incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned wtot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned wbase = 0;
+    if (lane == 31 && wtot) wbase = atomicAdd(cnt, wtot);
+    wbase = __shfl_sync(0xffffffffu, wbase, 31);
+    unsigned slot = wbase + incl - mine;
+    // pass 2: write and join
+    if (mine) {
+      const unsigned hs = rank[0];
+      for (int f = 0; f < 5; ++f) {
+        int seen = 0;
+        unsigned ht = 0;
+        for (int x = 0; x < nn; ++x) {
+          if (vset[x] & (1u << f)) continue;
+          if (seen++ == 0) {
+            ht = rank[x];
+            continue;
+          }
+          if (hs == ht || hs == rank[x]) continue;
+          unsigned tri[3] = {hs, ht, rank[x]};
+          ct_sort4(tri, 3);
+          if (slot < cap)
+            for (int k = 0; k < 3; ++k) cells[(size_t)slot * 3 + k] = tri[k];
+          ++slot;
+          uf_unite(parent, tri[0], tri[1], err);
+          uf_unite(parent, tri[0], tri[2], err);
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+ftk2b_status run_fiber_surface(ftk2b_ctx* ctx, const CtGeom& g, const FsTables& tb, const void* fa,
+                               const void* fb, T t0, T t1, double q, ftk2b_fiber_surface_result* res) {
+  cudaStream_t st = ctx->stream;
+  DevBuf* B = ctx->contour;
+  const unsigned long long nblk = (g.nv + kCtThreads - 1) / kCtThreads;
+  if (nblk >= 0xFFFFFFF0ull) return cfail(ctx, FTK2B_UNSUPPORTED, "mesh too large");
+  C_TRY(B[kBufPos].ensure(g.nv));
+  C_TRY(B[kBufHist].ensure(8 * g.nv));
+  C_TRY(B[kBufVoff].ensure(4 * g.nv));
+  C_TRY(B[kBufBlk].ensure(4 * (nblk + 1)));
+  C_TRY(B[kBufCount].ensure(64));
+  auto* cls = static_cast<unsigned char*>(B[kBufPos].p);
+  auto* mask = static_cast<unsigned long long*>(B[kBufHist].p);
+  auto* voff = static_cast<unsigned*>(B[kBufVoff].p);
+  auto* blk = static_cast<unsigned*>(B[kBufBlk].p);
+  auto* counts = static_cast<unsigned*>(B[kBufCount].p);  // [0] n, [1] cells, [2] roots, [3] err, [4] cubes
+  auto* total64 = reinterpret_cast<unsigned long long*>(counts + 8);
+  const T* a0 = static_cast<const T*>(fa);
+  const T* a1 = static_cast<const T*>(fb);
+  const unsigned sms = (unsigned)ctx->num_sms;
+  C_TRY(cudaMemsetAsync(counts, 0, 64, st));
+  C_TRY(cudaEventRecord(ctx->ev0, st));
+  fs_class_kernel<T><<<grid_of(g.nv, 256, 32ull * sms), 256, 0, st>>>(g, a0, a1, t0, t1, q, cls);
+  fs_mask_kernel<T><<<(unsigned)nblk, kCtThreads, 0, st>>>(g, tb, a0, a1, t0, t1, q, cls, mask, blk, total64);
+  C_TRY(launch_scan(blk, (unsigned)nblk, counts + 0, nullptr, st));  // counts[0]: feature count (labels)
+  ctx->launches += 3;
+  unsigned long long n64 = 0;
+  C_TRY(cudaMemcpyAsync(&n64, total64, 8, cudaMemcpyDeviceToHost, st));
+  C_TRY(ctx->sync());
+  if (n64 >= 0xFFFFFFF0ull) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^32 - 16 feature triangles");
+  const unsigned n = (unsigned)n64;
+  const size_t ncap = n ? n : 1;
+  C_TRY(B[kBufSimp].ensure(24 * ncap));
+  C_TRY(B[kBufLam].ensure(24 * ncap));
+  C_TRY(B[kBufBary].ensure(12 * ncap));
+  C_TRY(B[kBufParent].ensure(4 * ncap));
+  C_TRY(B[kBufTrack].ensure(8 * ncap));
+  auto* simp = static_cast<unsigned long long*>(B[kBufSimp].p);
+  auto* lam = static_cast<double*>(B[kBufLam].p);
+  auto* bary = static_cast<float*>(B[kBufBary].p);
+  auto* parent = static_cast<unsigned*>(B[kBufParent].p);
+  auto* track = static_cast<unsigned long long*>(B[kBufTrack].p);
+  fs_emit_kernel<T><<<(unsigned)nblk, kCtThreads, 0, st>>>(g, tb, a0, a1, t0, t1, mask, blk, voff, simp, lam, bary);
+  C_TRY(B[kBufList].ensure(8 * (g.ncube ? g.ncube : 1)));
+  auto* list = static_cast<unsigned long long*>(B[kBufList].p);
+  unsigned* list_cnt = counts + 4;
+  fs_list_kernel<<<grid_of(g.ncube, 256, 64ull * sms), 256, 0, st>>>(g, mask, list, list_cnt);
+  ctx->launches += 2;
+
+  unsigned cap = (unsigned)std::min<unsigned long long>(0x7FFFFFFFull, std::max<unsigned long long>(1024ull, 4ull * n));
+  unsigned ncell = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    C_TRY(B[kBufCells].ensure((size_t)12 * cap));
+    auto* cells = static_cast<unsigned*>(B[kBufCells].p);
+    C_TRY(cudaMemsetAsync(counts + 1, 0, 12, st));
+    if (n) ct_iota_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(parent, n);
+    fs_cells_kernel<<<16u * sms, 256, 0, st>>>(g, tb, list, list_cnt, mask, voff, cells, counts + 1, cap, parent,
+                                              counts + 3);
+    ctx->launches += 2;
+    C_TRY(cudaMemcpyAsync(&ncell, counts + 1, 4, cudaMemcpyDeviceToHost, st));
+    C_TRY(ctx->sync());
+    if (ncell <= cap) break;
+    if (ncell >= 0x7FFFFFFFu) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 manifold triangles");
+    cap = ncell;
+  }
+  auto* cells = static_cast<unsigned*>(B[kBufCells].p);
+
+  // sorted, unique triangles: buckets by leading node, each sorted and made
+  // unique, compacted
+  const unsigned ccap = ncell ? ncell : 1;
+  const unsigned nb = n + 1;
+  const unsigned sblocks = (unsigned)((nb + kCtThreads * kScanPer - 1) / (kCtThreads * kScanPer));
+  C_TRY(B[kBufKey0].ensure(4ull * nb));
+  C_TRY(B[kBufKey1].ensure(4ull * nb));
+  C_TRY(B[kBufVal0].ensure(4ull * (sblocks + 1)));
+  C_TRY(B[kBufVal1].ensure(4ull * nb));
+  C_TRY(B[kBufCellsOut].ensure(12ull * ccap));
+  C_TRY(B[kBufMask].ensure(12ull * ccap));
+  auto* boff = static_cast<unsigned*>(B[kBufKey0].p);
+  auto* bcur = static_cast<unsigned*>(B[kBufKey1].p);
+  auto* btot = static_cast<unsigned*>(B[kBufVal0].p);
+  auto* uoff = static_cast<unsigned*>(B[kBufVal1].p);
+  auto* rows = static_cast<unsigned*>(B[kBufCellsOut].p);
+  auto* cells_out = static_cast<unsigned*>(B[kBufMask].p);
+  const unsigned cg = grid_of(ccap, 256, 16ull * sms);
+  unsigned nuniq = 0;
+  if (ncell) {
+    C_TRY(cudaMemsetAsync(boff, 0, 4ull * nb, st));
+    C_TRY(cudaMemsetAsync(bcur, 0, 4ull * nb, st));
+    C_TRY(cudaMemsetAsync(uoff, 0, 4ull * nb, st));
+    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, 3, boff);
+    ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
+    ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, 3, boff, bcur, rows);
+    ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(rows, boff, n, 3, counts + 3, uoff);
+    ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(uoff, nb, btot);
+    C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
+    ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(uoff, nb, btot);
+    ct_bucket_compact_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(rows, boff, uoff, n, 3, cells_out);
+    ctx->launches += 10;
+    C_TRY(cudaMemcpyAsync(&nuniq, uoff + n, 4, cudaMemcpyDeviceToHost, st));
+  }
+  if (n) {
+    C_TRY(launch_uf_label(parent, counts + 0, n, track, counts + 2, st));
+    ctx->launches += 1;
+  }
+  C_TRY(cudaEventRecord(ctx->ev1, st));
+  unsigned hc[4] = {0, 0, 0, 0};
+  C_TRY(cudaMemcpyAsync(hc, counts, 16, cudaMemcpyDeviceToHost, st));
+  C_TRY(ctx->sync());
+  res->n_features = n;
+  res->n_cells = nuniq;
+  res->simplices = static_cast<uint64_t*>(std::malloc(24 * ncap));
+  res->lambda = static_cast<double*>(std::malloc(24 * ncap));
+  res->barycentric = static_cast<float*>(std::malloc(12 * ncap));
+  res->track_id = static_cast<uint64_t*>(std::malloc(8 * ncap));
+  res->scalar = static_cast<float*>(std::calloc(ncap, 4));
+  res->cells = static_cast<uint32_t*>(std::malloc(12ull * (nuniq ? nuniq : 1)));
+  if (!res->simplices || !res->lambda || !res->barycentric || !res->track_id || !res->scalar || !res->cells)
+    return cfail(ctx, FTK2B_OOM, "host result allocation failed");
+  C_TRY(ct_d2h(ctx, res->simplices, simp, 24ull * n));
+  C_TRY(ct_d2h(ctx, res->lambda, lam, 24ull * n));
+  C_TRY(ct_d2h(ctx, res->barycentric, bary, 12ull * n));
+  C_TRY(ct_d2h(ctx, res->track_id, track, 8ull * n));
+  C_TRY(ct_d2h(ctx, res->cells, cells_out, 12ull * nuniq));
+  if (hc[3] & 1u) return cfail(ctx, FTK2B_CUDA_ERROR, "union-find did not settle");
+  res->n_tracks = hc[2];
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  res->device_ms = ms;
+  return FTK2B_OK;
+}
+
 }  // namespace
+
+// Geometry of a regular mesh and its scalar array(s) for the level-set and
+// fiber-surface pipelines; *nelem receives the element count of one array.
+static ftk2b_status ct_geometry(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                                CtGeom& g, size_t* nelem_out);
 
 extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                               const ftk2b_field_desc* field, double threshold, double sos_q,
@@ -804,6 +1214,47 @@ extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_d
     return cfail(ctx, FTK2B_INVALID_ARG, "level sets read one scalar array (ncomp 1, layout SEPARATE)");
   if (!(sos_q > 0)) return cfail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
   CtGeom g;
+  size_t nelem = 1;
+  {
+    const ftk2b_status gs = ct_geometry(ctx, mesh, field, g, &nelem);
+    if (gs != FTK2B_OK) return gs;
+  }
+  const size_t es = field->dtype == FTK2B_F64 ? 8 : 4;
+  const unsigned long long nv = g.nv;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return cfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  const void* dev = field->comp[0];
+  if (field->location != FTK2B_DEVICE) {
+    C_TRY(ctx->contour[kBufField].ensure(nelem * es));
+    C_TRY(cudaMemcpyAsync(ctx->contour[kBufField].p, field->comp[0], nelem * es, cudaMemcpyHostToDevice,
+                          ctx->stream));
+    dev = ctx->contour[kBufField].p;
+  }
+  (void)nv;
+  auto* res = new (std::nothrow) ftk2b_contour_result;
+  if (!res) return cfail(ctx, FTK2B_OOM, "result allocation failed");
+  std::memset(res, 0, sizeof(*res));
+  unsigned long long edges = 0;
+  for (int e = 1; e < (1 << d); ++e) {
+    unsigned long long c = 1;
+    for (int k = 0; k < d; ++k) c *= ((e >> k) & 1) ? g.L[k] - 1 : g.L[k];
+    edges += c;
+  }
+  res->n_simplices = edges;
+  const ftk2b_status st =
+      field->dtype == FTK2B_F64
+          ? run_contour<double>(ctx, g, dev, (double)threshold, sos_q, res)
+          : run_contour<float>(ctx, g, dev, (float)threshold, sos_q, res);
+  if (st != FTK2B_OK) {
+    ftk2b_contour_result_free(res);
+    return st;
+  }
+  *out = res;
+  return FTK2B_OK;
+}
+
+static ftk2b_status ct_geometry(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                                CtGeom& g, size_t* nelem_out) {
+  const int d = mesh->ndims;
   std::memset(&g, 0, sizeof(g));
   g.d = d;
   unsigned long long nv = 1, ncube = 1, gstride = 1;
@@ -820,7 +1271,6 @@ extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_d
   }
   g.nv = nv;
   g.ncube = ncube;
-  const size_t es = field->dtype == FTK2B_F64 ? 8 : 4;
   size_t nelem = 1;
   if (field->nd == 1) {
     g.per_vertex = 1;
@@ -862,34 +1312,90 @@ extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_d
         g.goff[e] += g.gs[k];
         g.aoff[e] += g.as[k];
       }
-  if (cudaSetDevice(ctx->device) != cudaSuccess) return cfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
-  const void* dev = field->comp[0];
-  if (field->location != FTK2B_DEVICE) {
-    C_TRY(ctx->contour[kBufField].ensure(nelem * es));
-    C_TRY(cudaMemcpyAsync(ctx->contour[kBufField].p, field->comp[0], nelem * es, cudaMemcpyHostToDevice,
-                          ctx->stream));
-    dev = ctx->contour[kBufField].p;
+  *nelem_out = nelem;
+  return FTK2B_OK;
+}
+
+extern "C" ftk2b_status ftk2b_fiber_surface_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
+                                                    const ftk2b_field_desc* field, const double thresholds[2],
+                                                    double sos_q, ftk2b_fiber_surface_result** out) {
+  if (!ctx) return FTK2B_INVALID_ARG;
+  if (!mesh || !field || !thresholds || !out) return cfail(ctx, FTK2B_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (mesh->kind != FTK2B_MESH_REGULAR || mesh->ndims != 4)
+    return cfail(ctx, FTK2B_UNSUPPORTED, "fiber surfaces run on regular 3D+t meshes (ndims 4)");
+  if (field->dtype != FTK2B_F32 && field->dtype != FTK2B_F64)
+    return cfail(ctx, FTK2B_INVALID_ARG, "dtype must be FTK2B_F32 or FTK2B_F64");
+  if (field->ncomp != 2 || field->layout != FTK2B_LAYOUT_SEPARATE || !field->comp[0] || !field->comp[1])
+    return cfail(ctx, FTK2B_INVALID_ARG, "fiber surfaces read two scalar arrays (ncomp 2, layout SEPARATE)");
+  if (!(sos_q > 0)) return cfail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
+  CtGeom g;
+  size_t nelem = 1;
+  {
+    const ftk2b_status gs = ct_geometry(ctx, mesh, field, g, &nelem);
+    if (gs != FTK2B_OK) return gs;
   }
-  auto* res = new (std::nothrow) ftk2b_contour_result;
+  if (g.nv >= 0xFFFFFFF0ull) return cfail(ctx, FTK2B_UNSUPPORTED, "mesh too large for fiber surfaces");
+  // triangle types of a 4-cube: corner masks 0 < a < b with a a subset of b,
+  // in (a, b) order
+  FsTables tb;
+  std::memset(&tb, 255, sizeof(tb));
+  int nt = 0;
+  for (int a = 1; a < 16; ++a)
+    for (int b = a + 1; b < 16; ++b)
+      if ((a & b) == a) {
+        tb.ta[nt] = (unsigned char)a;
+        tb.tb[nt] = (unsigned char)b;
+        tb.idx[a][b] = (unsigned char)nt;
+        ++nt;
+      }
+  if (nt != 50) return cfail(ctx, FTK2B_CUDA_ERROR, "triangle table has %d types", nt);
+  const size_t es = field->dtype == FTK2B_F64 ? 8 : 4;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return cfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  const void* dev[2] = {field->comp[0], field->comp[1]};
+  if (field->location != FTK2B_DEVICE) {
+    const int slot[2] = {kBufField, kBufField2};
+    for (int j = 0; j < 2; ++j) {
+      C_TRY(ctx->contour[slot[j]].ensure(nelem * es));
+      C_TRY(cudaMemcpyAsync(ctx->contour[slot[j]].p, field->comp[j], nelem * es, cudaMemcpyHostToDevice,
+                            ctx->stream));
+      dev[j] = ctx->contour[slot[j]].p;
+    }
+  }
+  auto* res = new (std::nothrow) ftk2b_fiber_surface_result;
   if (!res) return cfail(ctx, FTK2B_OOM, "result allocation failed");
   std::memset(res, 0, sizeof(*res));
-  unsigned long long edges = 0;
-  for (int e = 1; e < (1 << d); ++e) {
+  // triangles of the mesh: for each type, the corners c with c + b inside
+  unsigned long long tris = 0;
+  for (int t = 0; t < 50; ++t) {
     unsigned long long c = 1;
-    for (int k = 0; k < d; ++k) c *= ((e >> k) & 1) ? g.L[k] - 1 : g.L[k];
-    edges += c;
+    for (int k = 0; k < 4; ++k) c *= ((tb.tb[t] >> k) & 1) ? g.L[k] - 1 : g.L[k];
+    tris += c;
   }
-  res->n_simplices = edges;
+  res->n_simplices = tris;
   const ftk2b_status st =
       field->dtype == FTK2B_F64
-          ? run_contour<double>(ctx, g, dev, (double)threshold, sos_q, res)
-          : run_contour<float>(ctx, g, dev, (float)threshold, sos_q, res);
+          ? run_fiber_surface<double>(ctx, g, tb, dev[0], dev[1], (double)thresholds[0], (double)thresholds[1],
+                                      sos_q, res)
+          : run_fiber_surface<float>(ctx, g, tb, dev[0], dev[1], (float)thresholds[0], (float)thresholds[1], sos_q,
+                                     res);
   if (st != FTK2B_OK) {
-    ftk2b_contour_result_free(res);
+    ftk2b_fiber_surface_result_free(res);
     return st;
   }
   *out = res;
   return FTK2B_OK;
+}
+
+extern "C" void ftk2b_fiber_surface_result_free(ftk2b_fiber_surface_result* r) {
+  if (!r) return;
+  std::free(r->simplices);
+  std::free(r->lambda);
+  std::free(r->barycentric);
+  std::free(r->track_id);
+  std::free(r->scalar);
+  std::free(r->cells);
+  delete r;
 }
 
 extern "C" void ftk2b_contour_result_free(ftk2b_contour_result* r) {

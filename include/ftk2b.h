@@ -389,10 +389,36 @@ void ftk2b_contour_result_free(ftk2b_contour_result* r);
  * centroid where the barycentric solve fails; edges join each top cell's
  * features to its star centre.  field: ncomp 2 (SEPARATE, MULTICOMPONENT or
  * PER_VERTEX layout as for critical points).  The result is a cp_result with
- * m = 2, type 0 and scalar 0.  3D+t meshes (fiber surfaces) are
- * FTK2B_UNSUPPORTED. */
+ * m = 2, type 0 and scalar 0.  3D+t meshes (fiber surfaces): use
+ * ftk2b_fiber_surface_extract. */
 ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
                                  const double thresholds[2], double sos_q, ftk2b_cp_result** out);
+
+/* Fiber surfaces: SimplicialEngine<T, FiberPredicate<T>>::execute +
+ * get_complex on a regular 3D+t mesh (ndims 4).  field: ncomp 2, layout
+ * SEPARATE (nd 4, indexed by local coordinates, or nd 1 by global vertex id).
+ * Features are the triangles of the 4-D mesh, in simplex order, with their
+ * barycentrics (centroid where the solve fails); cells are the star-fan
+ * triangles of form_general_manifold_patches (engine.hpp:1388-1413) as sorted,
+ * unique rows of feature indices; track ids are the components' smallest
+ * feature index. */
+typedef struct {
+  uint64_t n_features;
+  uint64_t* simplices;    /* 3 per feature: vertex ids, ascending */
+  double* lambda;         /* 3 per feature, the field precision widened */
+  float* barycentric;     /* 3 per feature, as FeatureElement stores them */
+  uint64_t* track_id;     /* n */
+  float* scalar;          /* n: 0 */
+  uint64_t n_cells;
+  uint32_t* cells;        /* 3 per cell */
+  uint64_t n_tracks;
+  uint64_t n_simplices;   /* triangles of the mesh: the unit of work */
+  double device_ms;
+} ftk2b_fiber_surface_result;
+ftk2b_status ftk2b_fiber_surface_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
+                                         const ftk2b_field_desc* field, const double thresholds[2], double sos_q,
+                                         ftk2b_fiber_surface_result** out);
+void ftk2b_fiber_surface_result_free(ftk2b_fiber_surface_result* r);
 
 #ifdef __cplusplus
 }

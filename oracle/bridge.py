@@ -337,6 +337,45 @@ def run_reference_fiber(mesh: OrcMesh, field: OrcField, thresholds, one_thread: 
         lib.ftk2ref_free(C.byref(res))
 
 
+def run_reference_fiber_surface(mesh: OrcMesh, field: OrcField, thresholds):
+    """The reference's own engine with FiberPredicate<T> on a regular 3D+t
+    mesh: the triangle features and the star-fan triangles of get_complex,
+    an (n, 3) array of feature indices."""
+    lib = _load(REF_LIB, "ftk2ref")
+    fn = lib.ftk2ref_run_fiber_surface
+    fn.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.POINTER(C.c_double), C.POINTER(OrcResult),
+                   C.POINTER(OrcConn)]
+    fn.restype = C.c_int
+    lib.ftk2ref_free_conn.argtypes = [C.POINTER(OrcConn)]
+    thr = (C.c_double * 2)(float(thresholds[0]), float(thresholds[1]))
+    res, conn = OrcResult(), OrcConn()
+    rc = fn(C.byref(mesh), C.byref(field), thr, C.byref(res), C.byref(conn))
+    if rc != 0:
+        raise RuntimeError(f"ftk2ref_run_fiber_surface failed with status {rc}")
+    try:
+        n = int(res.n)
+
+        def arr(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        out = CPResult(
+            simplices=arr(res.simplices, 3 * n, np.uint64).reshape(n, 3),
+            bary=arr(res.bary, 3 * n, np.float32).reshape(n, 3),
+            lam=arr(res.lambda_, 3 * n, np.float64).reshape(n, 3),
+            track_id=arr(res.track_id, n, np.uint64),
+            type=arr(res.type, n, np.uint32),
+            scalar=arr(res.scalar, n, np.float32),
+            edges=np.zeros((0, 2), dtype=np.uint32),
+        )
+        cells = arr(conn.idx, int(conn.n) * 3, np.uint32).reshape(-1, 3)
+    finally:
+        lib.ftk2ref_free(C.byref(res))
+        lib.ftk2ref_free_conn(C.byref(conn))
+    return out, cells
+
+
 def run_restatement(mesh: OrcMesh, field: OrcField) -> CPResult:
     """Our exact C restatement of the same algorithm."""
     return _run(ORC_LIB, "cporacle", mesh, field)

@@ -121,6 +121,10 @@ void ftk2ref_free_conn(orc_conn* c);
  * comp[0], comp[1] (layout SEPARATE) on a regular 2D+t mesh; thresholds[2].
  * Flattened as ftk2ref_run, with the star edges of the trajectories. */
 int ftk2ref_run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thresholds, orc_result* out);
+/* Fiber surfaces: the same on a regular 3D+t mesh (ndims 4); conn receives
+ * the star-fan triangles (dim 2) of get_complex. */
+int ftk2ref_run_fiber_surface(const orc_mesh* mesh, const orc_field* field, const double* thresholds,
+                              orc_result* out, orc_conn* conn);
 
 /* own restatement */
 int cporacle_run(const orc_mesh* mesh, const orc_field* field, orc_result* out);

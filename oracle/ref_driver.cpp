@@ -303,7 +303,8 @@ int run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, 
 // set-up), flattened as run() does.  lambda: the barycentrics the predicate
 // stores (solver output, or 1/3 where it falls back, predicate.hpp:354).
 template <typename T>
-int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, orc_result* out) {
+int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, orc_result* out,
+              orc_conn* conn = nullptr) {
   using namespace ftk2;
   std::vector<uint64_t> dims, off, glob;
   for (int i = 0; i < mesh->ndims; ++i) {
@@ -349,7 +350,8 @@ int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, o
       for (size_t k = 0; k < c.size(); ++k) c[k] -= (double)off[k];
       for (int j = 0; j < 2; ++j) {
         const auto& a = data.at(j == 0 ? "F" : "G");
-        values[v][j] = (T)(a.f(c[0], c[1], c[2]) - pred.thresholds[j]);
+        const T x = c.size() == 3 ? a.f(c[0], c[1], c[2]) : a.f(c[0], c[1], c[2], c[3]);
+        values[v][j] = (T)(x - pred.thresholds[j]);
       }
     }
     T lambda[3];
@@ -360,16 +362,40 @@ int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, o
     out->type[i] = el.type;
     out->scalar[i] = el.scalar;
   }
-  std::vector<uint32_t> edges;
-  for (const auto& conn : complex.connectivity)
-    if (conn.dimension == 1) edges = conn.indices;
+  std::vector<uint32_t> edges, tris;
+  for (const auto& cc : complex.connectivity) {
+    if (cc.dimension == 1) edges = cc.indices;
+    if (cc.dimension == 2) tris = cc.indices;
+  }
   out->n_edges = edges.size() / 2;
   out->edges = (uint32_t*)std::malloc(sizeof(uint32_t) * (edges.size() + 2));
   if (!edges.empty()) std::memcpy(out->edges, edges.data(), sizeof(uint32_t) * edges.size());
+  if (conn) {
+    conn->dim = 2;
+    conn->n = tris.size() / 3;
+    conn->idx = (uint32_t*)std::malloc(sizeof(uint32_t) * (tris.size() + 1));
+    if (!tris.empty()) std::memcpy(conn->idx, tris.data(), sizeof(uint32_t) * tris.size());
+  }
   return 0;
 }
 
 }  // namespace
+
+// Fiber surfaces: FiberPredicate<T> on a regular 3D+t mesh; conn receives the
+// star-fan triangles of get_complex (form_general_manifold_patches, k = 2).
+extern "C" int ftk2ref_run_fiber_surface(const orc_mesh* mesh, const orc_field* field, const double* thresholds,
+                                         orc_result* out, orc_conn* conn) {
+  std::memset(out, 0, sizeof(*out));
+  std::memset(conn, 0, sizeof(*conn));
+  if (mesh->kind != ORC_MESH_REGULAR || mesh->ndims != 4 || field->layout != ORC_LAYOUT_SEPARATE) return 3;
+  try {
+    return field->dtype == ORC_F64 ? run_fiber<double>(mesh, field, thresholds, out, conn)
+                                   : run_fiber<float>(mesh, field, thresholds, out, conn);
+  } catch (const std::exception& e) {
+    std::cerr << "ftk2ref_run_fiber_surface: " << e.what() << std::endl;
+    return 1;
+  }
+}
 
 extern "C" int ftk2ref_run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thresholds,
                                  orc_result* out) {

@@ -146,3 +146,38 @@ FIBER_CASES = {
     "fiber_ties": fiber_ties,
     "fiber_near_quantum": fiber_near_quantum,
 }
+
+
+# ---- fiber surfaces (FiberPredicate<T> on 3D+t meshes): two scalar fields.
+
+def fs_gauss_f64():
+    f = gaussian_potential((10, 9, 8), 4, seed=51, n_blobs=6, dtype=np.float64, sigma=(1.5, 4.0))
+    g = gaussian_potential((10, 9, 8), 4, seed=52, n_blobs=6, dtype=np.float64, sigma=(1.5, 4.0))
+    return dict(fields=(f, g), local_dims=[10, 9, 8, 4], offset=None, global_dims=None, thresholds=(0.0, 0.0),
+                q=1e6)
+
+
+def fs_f32_offset():
+    """A 11x10x9x3 sub-box at offset (2, 1, 3, 1) of a 14x12x13x5 mesh."""
+    f = gaussian_potential((14, 12, 13), 5, seed=53, n_blobs=7, dtype=np.float32, sigma=(1.5, 4.0))
+    g = gaussian_potential((14, 12, 13), 5, seed=54, n_blobs=7, dtype=np.float32, sigma=(1.5, 4.0))
+    sub = tuple(np.ascontiguousarray(a[1:4, 3:12, 1:11, 2:13]) for a in (f, g))
+    thr = tuple(float(np.median(a)) for a in sub)
+    return dict(fields=sub, local_dims=[11, 10, 9, 3], offset=[2, 1, 3, 1], global_dims=[14, 12, 13, 5],
+                thresholds=thr, q=2.0 ** 20)
+
+
+def fs_near_quantum():
+    """Values of a few 1/Q: the centroid fallback and many ties."""
+    rng = np.random.default_rng(55)
+    f = rng.uniform(-3e-6, 3e-6, (3, 6, 7, 8))
+    g = rng.uniform(-3e-6, 3e-6, (3, 6, 7, 8))
+    return dict(fields=(f, g), local_dims=[8, 7, 6, 3], offset=None, global_dims=None, thresholds=(0.0, 0.0),
+                q=1e6)
+
+
+FIBER_SURFACE_CASES = {
+    "fs_gauss_f64": fs_gauss_f64,
+    "fs_f32_offset": fs_f32_offset,
+    "fs_near_quantum": fs_near_quantum,
+}

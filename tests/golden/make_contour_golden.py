@@ -1,4 +1,5 @@
-"""Generate tests/golden/contour/*.npz and tests/golden/fiber/*.npz by running
+"""Generate tests/golden/contour/*.npz, tests/golden/fiber/*.npz and
+tests/golden/fiber_surface/*.npz by running
 the reference's own CPU engine with ContourPredicate<T> (one worker thread,
 oracle/_ref/libftk2ref1t.so) and FiberPredicate<T> (oracle/_ref/libftk2ref.so),
 built from the reference headers by oracle/Makefile, on the seeded inputs of
@@ -70,6 +71,27 @@ def main_fiber(names=None):
               f"{len(res['edges'])} edges, reference {dt:.1f}s")
 
 
+def main_fiber_surface(names=None):
+    out_dir = os.path.join(HERE, "fiber_surface")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, make in contour_cases.FIBER_SURFACE_CASES.items():
+        if names and name not in names:
+            continue
+        case = make()
+        keep: list = []
+        mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+        fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+        t = time.time()
+        r, cells = bridge.run_reference_fiber_surface(mesh, fld, case["thresholds"])
+        dt = time.time() - t
+        rec = {"input_sha256": np.array(digest(np.concatenate([a.reshape(-1) for a in case["fields"]]))),
+               "reference_seconds": np.array(dt), "simplices": r.simplices, "bary": r.bary, "lam": r.lam,
+               "track_id": r.track_id, "scalar": r.scalar, "cells": cells}
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **rec)
+        print(f"{name}: {len(r.track_id)} features, {len(set(r.track_id.tolist()))} tracks, "
+              f"{len(cells)} triangles, reference {dt:.1f}s")
+
+
 def main(names=None):
     out_dir = os.path.join(HERE, "contour")
     os.makedirs(out_dir, exist_ok=True)
@@ -94,3 +116,4 @@ def main(names=None):
 if __name__ == "__main__":
     main(sys.argv[1:])
     main_fiber(sys.argv[1:])
+    main_fiber_surface(sys.argv[1:])

@@ -111,3 +111,30 @@ def test_fiber_fixture_exercises_the_centroid_fallback():
     g = np.load(os.path.join(FIBER_GOLD, "fiber_near_quantum.npz"))
     third = np.float64(1.0) / 3.0
     assert (g["lam"] == third).all(axis=1).sum() > 10
+
+
+FS_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber_surface")
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_CASES))
+def test_fiber_surface_reference_reproduces_fixtures(name):
+    """Fiber surfaces (3D+t): the fixtures are the reference engine's output
+    (features, barycentrics, tracks, star-fan triangles)."""
+    case = contour_cases.FIBER_SURFACE_CASES[name]()
+    g = np.load(os.path.join(FS_GOLD, f"{name}.npz"))
+    assert digest(np.concatenate([a.reshape(-1) for a in case["fields"]])) == str(g["input_sha256"])
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+    fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+    r, cells = bridge.run_reference_fiber_surface(mesh, fld, case["thresholds"])
+    assert len(r.track_id) > 0 and len(cells) > 0
+    assert np.array_equal(r.simplices, g["simplices"])
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
+    assert np.array_equal(r.track_id, g["track_id"])
+    assert np.array_equal(cells, g["cells"])
+
+
+def test_fiber_surface_fixture_exercises_the_centroid_fallback():
+    g = np.load(os.path.join(FS_GOLD, "fs_near_quantum.npz"))
+    assert (g["lam"] == np.float64(1.0) / 3.0).all(axis=1).sum() > 10

@@ -61,7 +61,7 @@ def test_fiber_random_vs_live_reference(ctx, seed, dims, thr):
                                      "track_id": ref.track_id, "edges": ref.edges}, str(seed))
 
 
-def test_fiber_device_input_and_3d_unsupported(ctx):
+def test_fiber_device_input_and_3d_mesh_rejected(ctx):
     torch = pytest.importorskip("torch")
     case = contour_cases.fiber_gauss_f64()
     host = run_gpu(ctx, case)
@@ -71,3 +71,49 @@ def test_fiber_device_input_and_3d_unsupported(ctx):
     keep: list = []
     with pytest.raises(api.Ftk2bError):
         ctx.fiber(api.regular_mesh_desc([6, 5, 4, 3]), api.field_desc([a, a], api.LAYOUT_SEPARATE, 2, keep=keep))
+
+
+FS_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber_surface")
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_CASES))
+def test_fiber_surface_matches_reference_fixture(ctx, name):
+    """Fiber surfaces on 3D+t meshes (ftk2b_fiber_surface_extract): triangle
+    features, barycentrics (centroid where the solve fails), track ids and the
+    star-fan triangles of get_complex, bit for bit."""
+    case = contour_cases.FIBER_SURFACE_CASES[name]()
+    g = np.load(os.path.join(FS_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh = api.regular_mesh_desc(case["local_dims"], case["offset"], case["global_dims"])
+    fd = api.field_desc(list(case["fields"]), api.LAYOUT_SEPARATE, 2, keep=keep)
+    r = ctx.fiber_surface(mesh, fd, case["thresholds"], case["q"])
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    assert np.array_equal(r.simplices, g["simplices"])
+    assert np.array_equal(r.bary.view(np.uint32), g["bary"].view(np.uint32))
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
+    assert np.array_equal(r.track_id, g["track_id"])
+    assert np.array_equal(r.cells, g["cells"])
+    assert r.n_tracks == len(set(r.track_id.tolist()))
+    assert not r.scalar.any()
+
+
+def test_fiber_surface_vs_live_reference(ctx):
+    if not bridge.ref_available():
+        pytest.skip("reference build absent")
+    dims = [9, 8, 7, 3]
+    f = contour_cases.gaussian_potential(tuple(dims[:3]), dims[3], seed=61, n_blobs=5, dtype=np.float64,
+                                         sigma=(1.5, 3.5))
+    g = contour_cases.gaussian_potential(tuple(dims[:3]), dims[3], seed=62, n_blobs=5, dtype=np.float64,
+                                         sigma=(1.5, 3.5))
+    thr = (float(np.median(f)), float(np.median(g)))  # levels that cross inside the box
+    keep: list = []
+    ref, cells = bridge.run_reference_fiber_surface(
+        bridge.make_regular_mesh(dims), bridge.make_field([f, g], bridge.LAYOUT_SEPARATE, 2, sos_q=1e6, keep=keep),
+        thr)
+    r = ctx.fiber_surface(api.regular_mesh_desc(dims), api.field_desc([f, g], api.LAYOUT_SEPARATE, 2, keep=keep),
+                          thr, 1e6)
+    assert len(r.track_id) == len(ref.track_id) > 0
+    assert np.array_equal(r.simplices, ref.simplices)
+    assert np.array_equal(r.lam.view(np.uint64), ref.lam.view(np.uint64))
+    assert np.array_equal(r.track_id, ref.track_id)
+    assert np.array_equal(r.cells, cells)
