@@ -315,10 +315,64 @@ def contour_c2(ctx, steps=3):
     ms = float(np.median(dev_ms))
     nbytes = pot.numel() * 8
     del pot
-    return {"workload": "level set of the 128^3 x 16 f64 Gaussian-sum potential (32 blobs), threshold 0",
-            "mesh_edges": int(r.n_simplices), "features": int(len(r.track_id)), "cells": int(len(r.cells)),
-            "tracks": int(r.n_tracks), "device_ms": ms, "edges_per_s": r.n_simplices / (ms * 1e-3),
-            "field_read_gbs": nbytes / (ms * 1e-3) / 1e9, "wall_ms_with_result_copy": float(np.median(wall_ms))}
+    out = {"workload": "level set of the 128^3 x 16 f64 Gaussian-sum potential (32 blobs), threshold 0",
+           "mesh_edges": int(r.n_simplices), "features": int(len(r.track_id)), "cells": int(len(r.cells)),
+           "tracks": int(r.n_tracks), "device_ms": ms, "edges_per_s": r.n_simplices / (ms * 1e-3),
+           "field_read_gbs": nbytes / (ms * 1e-3) / 1e9, "wall_ms_with_result_copy": float(np.median(wall_ms))}
+    # the reference's level-set engine on the host cores, on a bounded sample:
+    # its own moving-sphere test field (32^3 x 10 float32)
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import contour_cases
+        from oracle import bridge
+        case = contour_cases.moving_sphere()
+        keep: list = []
+        rmesh = bridge.make_regular_mesh(case["local_dims"])
+        rfld = bridge.make_field([case["field"]], bridge.LAYOUT_SEPARATE, 1, sos_q=case["q"], keep=keep)
+        t = time.perf_counter()
+        ref, _ = bridge.run_reference_contour(rmesh, rfld, 0.0, one_thread=False)
+        secs = time.perf_counter() - t
+        dims = case["local_dims"]
+        edges = 0
+        for e in range(1, 16):
+            c = 1
+            for k in range(4):
+                c *= dims[k] - 1 if (e >> k) & 1 else dims[k]
+            edges += c
+        out["cpu_baseline"] = {"value": edges / secs, "unit": "edges/s", "cores": os.cpu_count() or 1,
+                               "kind": "reference", "features": int(len(ref.track_id)),
+                               "sample": f"the reference's moving-sphere level set, 32^3 x 10 float32 ({edges} edges), "
+                                         f"reference engine execute+get_complex, {secs:.1f} s"}
+    except Exception as e:  # the reference build travels prebuilt; report its absence
+        out["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    return out
+
+
+def fiber_surface_bench(ctx, steps=3):
+    """Fiber surfaces (FiberPredicate on 3D+t) of two Gaussian-sum potentials,
+    96^3 x 8 float64 (seeds 1234, 4321), thresholds at 0: device time per call
+    and mesh triangles per second."""
+    import numpy as np
+    import torch
+    from ftk2_b200 import api, generate
+    dims, nt = (96, 96, 96), 8
+    f = generate.gaussian_potential_device(dims, nt, seed=1234, n_blobs=32)
+    g = generate.gaussian_potential_device(dims, nt, seed=4321, n_blobs=32)
+    torch.cuda.synchronize()
+    keep: list = []
+    mesh = api.regular_mesh_desc([*dims, nt])
+    fd = api.field_desc([f, g], api.LAYOUT_SEPARATE, 2, keep=keep)
+    r = ctx.fiber_surface(mesh, fd, (0.0, 0.0), 2.0 ** 20)
+    dev_ms = []
+    for _ in range(steps):
+        r = ctx.fiber_surface(mesh, fd, (0.0, 0.0), 2.0 ** 20)
+        dev_ms.append(r.device_ms)
+    ms = float(np.median(dev_ms))
+    del f, g, fd
+    keep.clear()
+    return {"workload": "fiber surface of two 96^3 x 8 f64 Gaussian-sum potentials (32 blobs each), thresholds 0",
+            "mesh_triangles": int(r.n_simplices), "features": int(len(r.track_id)), "triangles": int(len(r.cells)),
+            "tracks": int(r.n_tracks), "device_ms": ms, "mesh_triangles_per_s": r.n_simplices / (ms * 1e-3)}
 
 
 def batched_c3(ctx, steps=5, check=True):
@@ -525,6 +579,8 @@ def main():
         line["serve"] = serving.run(duration_s=args.serve_seconds, device=local)
         torch.cuda.empty_cache()
         line["contour"] = contour_c2(ctx)
+        torch.cuda.empty_cache()
+        line["fiber_surface"] = fiber_surface_bench(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -10,6 +10,7 @@
 //   ftk2::ExtrudedSimplicialMesh(base, layers)     ftk2b::ExtrudedSimplicialMesh  (mesh.hpp:544)
 //   ftk2::CriticalPointPredicate<M,T>              ftk2b::CriticalPointPredicate<M,T> (predicate.hpp:49-64)
 //   ftk2::ContourPredicate<T> (level sets)         ftk2b::ContourPredicate<T>     (predicate.hpp:135-183)
+//   ftk2::FiberPredicate<T> (fibers)               ftk2b::FiberPredicate<T>       (predicate.hpp:341-362)
 //   ftk2::SimplicialEngine<T,Pred>(mesh, pred)     ftk2b::SimplicialEngine<T,Pred> (engine.hpp:84-85)
 //     .execute(data, vars) / .execute_cuda(...)      .execute / .execute_cuda      (engine.hpp:96-99, 273)
 //     .get_complex() -> FeatureComplex               .get_complex()                (engine.hpp:822-996)
@@ -569,6 +570,132 @@ class SimplicialEngine<T, ContourPredicate<T>> {
   ContourPredicate<T> pred_;
   std::unique_ptr<ftk2b_ctx, CtxDel> ctx_;
   std::unique_ptr<ftk2b_contour_result, ResDel> result_;
+};
+
+// ---- fibers (FiberPredicate<T>, predicate.hpp:341-362)
+
+template <typename T = double>
+struct FiberPredicate {
+  static constexpr int codimension = 2;
+  double sos_q = 1000000.0;
+  std::string var_names[2];
+  T thresholds[2] = {(T)0.0, (T)0.0};
+};
+
+// SimplicialEngine<T, FiberPredicate<T>> on a regular mesh: 2D+t meshes give
+// triangle features joined by star edges (ftk2b_fiber_extract), 3D+t meshes
+// triangle features of the 4-D mesh with the star-fan triangles of
+// get_complex (ftk2b_fiber_surface_extract).
+template <typename T>
+class SimplicialEngine<T, FiberPredicate<T>> {
+ public:
+  static constexpr int m = 2;
+
+  SimplicialEngine(std::shared_ptr<Mesh> mesh, FiberPredicate<T> pred = FiberPredicate<T>(), int device = 0)
+      : mesh_(std::move(mesh)), pred_(pred) {
+    ftk2b_ctx* c = nullptr;
+    ftk2b_status s = ftk2b_ctx_create(device, &c);
+    if (s != FTK2B_OK) throw Error(s, "ftk2b_ctx_create failed");
+    ctx_.reset(c);
+  }
+
+  template <typename Array>
+  void execute(const std::map<std::string, Array>& data, const std::vector<std::string>& vars = {}) {
+    const std::string n0 = vars.size() >= 2 ? vars[0] : pred_.var_names[0];
+    const std::string n1 = vars.size() >= 2 ? vars[1] : pred_.var_names[1];
+    const Array* a[2] = {&data.at(n0), &data.at(n1)};
+    ftk2b_mesh_desc md = mesh_->desc();
+    if (md.kind != FTK2B_MESH_REGULAR) throw Error(FTK2B_UNSUPPORTED, "fibers need a regular mesh");
+    using E = std::remove_cv_t<std::remove_pointer_t<decltype(a[0]->pdata())>>;
+    std::vector<T> conv[2];
+    ftk2b_field_desc fd;
+    std::memset(&fd, 0, sizeof(fd));
+    fd.dtype = sizeof(T) == 8 ? FTK2B_F64 : FTK2B_F32;
+    fd.ncomp = 2;
+    fd.layout = FTK2B_LAYOUT_SEPARATE;
+    fd.location = FTK2B_HOST;
+    for (int j = 0; j < 2; ++j) {
+      fd.comp[j] = a[j]->pdata();
+      if (!std::is_same<E, T>::value) {
+        conv[j].assign(a[j]->pdata(), a[j]->pdata() + a[j]->nelem());
+        fd.comp[j] = conv[j].data();
+      }
+    }
+    fd.nd = (int)a[0]->nd();
+    for (int i = 0; i < fd.nd && i < 4; ++i) fd.dims[i] = a[0]->dimf(i);
+    const double thr[2] = {(double)pred_.thresholds[0], (double)pred_.thresholds[1]};
+    cp_.reset();
+    fs_.reset();
+    ftk2b_status st;
+    if (md.ndims == 4) {
+      ftk2b_fiber_surface_result* r = nullptr;
+      st = ftk2b_fiber_surface_extract(ctx_.get(), &md, &fd, thr, pred_.sos_q, &r);
+      fs_.reset(r);
+    } else {
+      ftk2b_cp_result* r = nullptr;
+      st = ftk2b_fiber_extract(ctx_.get(), &md, &fd, thr, pred_.sos_q, &r);
+      cp_.reset(r);
+    }
+    if (st != FTK2B_OK) throw Error(st, ftk2b_last_error(ctx_.get()));
+  }
+
+  template <typename Array>
+  void execute_cuda(const std::map<std::string, Array>& data, const std::vector<std::string>& v = {}) {
+    execute(data, v);
+  }
+
+  FeatureComplex get_complex() const {
+    FeatureComplex fc;
+    uint64_t n = 0;
+    const uint64_t* simp = nullptr;
+    const double* lam = nullptr;
+    const float* bary = nullptr;
+    const uint64_t* track = nullptr;
+    if (cp_) n = cp_->n_features, simp = cp_->simplices, lam = cp_->lambda, bary = cp_->barycentric,
+             track = cp_->track_id;
+    if (fs_) n = fs_->n_features, simp = fs_->simplices, lam = fs_->lambda, bary = fs_->barycentric,
+             track = fs_->track_id;
+    fc.vertices.resize(n);
+    if (n) fc.lambda.assign(lam, lam + 3 * n);
+    for (uint64_t i = 0; i < n; ++i) {
+      FeatureElement& el = fc.vertices[i];
+      el.simplex.dimension = 2;
+      for (int v = 0; v < 3; ++v) {
+        el.simplex.vertices[v] = simp[3 * i + v];
+        el.barycentric_coords[0][v] = bary[3 * i + v];
+      }
+      el.track_id = track[i];
+    }
+    if (cp_ && cp_->n_edges) {
+      FeatureComplex::SimplexIndices e;
+      e.dimension = 1;
+      e.indices.assign(cp_->edges, cp_->edges + 2 * cp_->n_edges);
+      fc.connectivity.push_back(std::move(e));
+    }
+    if (fs_ && fs_->n_cells) {
+      FeatureComplex::SimplexIndices c;
+      c.dimension = 2;
+      c.indices.assign(fs_->cells, fs_->cells + 3 * fs_->n_cells);
+      fc.connectivity.push_back(std::move(c));
+    }
+    return fc;
+  }
+
+ private:
+  struct CtxDel {
+    void operator()(ftk2b_ctx* c) const { ftk2b_ctx_destroy(c); }
+  };
+  struct CpDel {
+    void operator()(ftk2b_cp_result* r) const { ftk2b_cp_result_free(r); }
+  };
+  struct FsDel {
+    void operator()(ftk2b_fiber_surface_result* r) const { ftk2b_fiber_surface_result_free(r); }
+  };
+  std::shared_ptr<Mesh> mesh_;
+  FiberPredicate<T> pred_;
+  std::unique_ptr<ftk2b_ctx, CtxDel> ctx_;
+  std::unique_ptr<ftk2b_cp_result, CpDel> cp_;
+  std::unique_ptr<ftk2b_fiber_surface_result, FsDel> fs_;
 };
 
 }  // namespace ftk2b

@@ -117,3 +117,40 @@ def test_fiber_surface_vs_live_reference(ctx):
     assert np.array_equal(r.lam.view(np.uint64), ref.lam.view(np.uint64))
     assert np.array_equal(r.track_id, ref.track_id)
     assert np.array_equal(r.cells, cells)
+
+
+@pytest.mark.parametrize("name,gold,conn", [("fiber_gauss_f64", "fiber", "edges"),
+                                            ("fs_gauss_f64", "fiber_surface", "cells")])
+def test_fiber_cpp_dropin_matches_reference_fixture(tmp_path, name, gold, conn):
+    """SimplicialEngine<T, FiberPredicate<T>> of include/ftk2b/engine.hpp on a
+    2D+t (star edges) and a 3D+t (star-fan triangles) mesh."""
+    import subprocess
+    from ftk2_b200 import build as fb
+    cases = dict(contour_cases.FIBER_CASES, **contour_cases.FIBER_SURFACE_CASES)
+    case = cases[name]()
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", gold, f"{name}.npz"))
+    exe = fb.build_contour_test()
+    paths = []
+    for j, a in enumerate(case["fields"]):
+        p = tmp_path / f"f{j}.bin"
+        a.tofile(p)
+        paths.append(str(p))
+    dt = "f64" if case["fields"][0].dtype == np.float64 else "f32"
+    out = tmp_path / "out.txt"
+    r = subprocess.run([exe, "fiber", *paths, dt, ",".join(str(x) for x in case["local_dims"]),
+                        repr(case["thresholds"][0]), repr(case["thresholds"][1]), repr(case["q"]), str(out)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    feats, rows = [], []
+    for line in open(out):
+        if line.startswith("F"):
+            vs, bs, tr = line[1:].split("|")
+            feats.append(([int(x) for x in vs.split()], [int(x, 16) for x in bs.split()], int(tr)))
+        elif line.startswith("C"):
+            rows.append([int(x) for x in line.split()[2:]])
+    assert len(feats) == len(g["track_id"]) > 0
+    assert np.array_equal(np.array([v for v, _, _ in feats], dtype=np.uint64), g["simplices"])
+    assert np.array_equal(np.array([b for _, b, _ in feats], dtype=np.uint32), g["bary"].view(np.uint32))
+    assert np.array_equal(np.array([t for _, _, t in feats], dtype=np.uint64), g["track_id"])
+    want = g[conn]
+    assert np.array_equal(np.array(rows, dtype=np.uint32).reshape(-1, want.shape[1]), want)
