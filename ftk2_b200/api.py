@@ -351,11 +351,12 @@ def _result_from_c(r: CPResultC) -> CPResult:
 
 @dataclass
 class ContourResult:
-    """Flattened FeatureComplex of a level-set extraction (ContourPredicate):
-    features are mesh edges, cells the manifold cells of get_complex."""
-    simplices: np.ndarray      # (n, 2) uint64 edge vertex ids, simplex order
-    lam: np.ndarray            # (n, 2) float64 barycentrics in the field precision
-    bary: np.ndarray           # (n, 2) float32 as FeatureElement stores them
+    """Flattened FeatureComplex of a level-set (ContourPredicate) or
+    fiber-surface (FiberPredicate on 3D+t) extraction: features are mesh
+    edges or triangles, cells the manifold cells of get_complex."""
+    simplices: np.ndarray      # (n, m+1) uint64 vertex ids, simplex order (m = 1 edges, 2 triangles)
+    lam: np.ndarray            # (n, m+1) float64 barycentrics in the field precision
+    bary: np.ndarray           # (n, m+1) float32 as FeatureElement stores them
     track_id: np.ndarray       # (n,) uint64
     scalar: np.ndarray         # (n,) float32 (the threshold)
     cells: np.ndarray          # (c, cell_dim + 1) uint32 feature indices
