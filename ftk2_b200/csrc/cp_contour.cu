@@ -25,9 +25,12 @@
 //              their leading node, each bucket's few rows sorted, duplicates
 //              flagged
 //   label      track id = the component's smallest feature index
+#include <sys/mman.h>
+
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -662,6 +665,18 @@ cudaError_t ct_d2h(ftk2b_ctx* ctx, void* dst, const void* src, size_t bytes) {
   return cudaSuccess;
 }
 
+// Host memory for large results (released with free()): 2 MB-aligned and
+// advised for huge pages, so the first touch while copying in faults once per
+// 2 MB instead of once per 4 KB (about half the copy time for a 1 GB result).
+void* ct_host_alloc(size_t bytes) {
+  constexpr size_t kHuge = size_t(2) << 20;
+  if (bytes < (size_t(64) << 20)) return std::malloc(bytes ? bytes : 1);
+  void* p = nullptr;
+  if (posix_memalign(&p, kHuge, (bytes + kHuge - 1) / kHuge * kHuge) != 0) return nullptr;
+  madvise(p, (bytes + kHuge - 1) / kHuge * kHuge, MADV_HUGEPAGE);
+  return p;
+}
+
 enum {
   kBufField = 0, kBufPos, kBufMask, kBufBlk, kBufVoff, kBufSimp, kBufLam, kBufBary, kBufFirst, kBufParent,
   kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount, kBufList,
@@ -789,12 +804,12 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   res->n_features = n;
   res->cell_dim = d - 1;
   res->n_cells = ncell;
-  res->simplices = static_cast<uint64_t*>(std::malloc(16 * ncap));
-  res->lambda = static_cast<double*>(std::malloc(16 * ncap));
-  res->barycentric = static_cast<float*>(std::malloc(8 * ncap));
-  res->track_id = static_cast<uint64_t*>(std::malloc(8 * ncap));
-  res->scalar = static_cast<float*>(std::malloc(4 * ncap));
-  res->cells = static_cast<uint32_t*>(std::malloc(4ull * kc * ccap));
+  res->simplices = static_cast<uint64_t*>(ct_host_alloc(16 * ncap));
+  res->lambda = static_cast<double*>(ct_host_alloc(16 * ncap));
+  res->barycentric = static_cast<float*>(ct_host_alloc(8 * ncap));
+  res->track_id = static_cast<uint64_t*>(ct_host_alloc(8 * ncap));
+  res->scalar = static_cast<float*>(ct_host_alloc(4 * ncap));
+  res->cells = static_cast<uint32_t*>(ct_host_alloc(4ull * kc * ccap));
   if (!res->simplices || !res->lambda || !res->barycentric || !res->track_id || !res->scalar || !res->cells)
     return cfail(ctx, FTK2B_OOM, "host result allocation failed");
   C_TRY(ctx->sync());
@@ -1171,12 +1186,12 @@ ftk2b_status run_fiber_surface(ftk2b_ctx* ctx, const CtGeom& g, const FsTables& 
   C_TRY(ctx->sync());
   res->n_features = n;
   res->n_cells = nuniq;
-  res->simplices = static_cast<uint64_t*>(std::malloc(24 * ncap));
-  res->lambda = static_cast<double*>(std::malloc(24 * ncap));
-  res->barycentric = static_cast<float*>(std::malloc(12 * ncap));
-  res->track_id = static_cast<uint64_t*>(std::malloc(8 * ncap));
+  res->simplices = static_cast<uint64_t*>(ct_host_alloc(24 * ncap));
+  res->lambda = static_cast<double*>(ct_host_alloc(24 * ncap));
+  res->barycentric = static_cast<float*>(ct_host_alloc(12 * ncap));
+  res->track_id = static_cast<uint64_t*>(ct_host_alloc(8 * ncap));
   res->scalar = static_cast<float*>(std::calloc(ncap, 4));
-  res->cells = static_cast<uint32_t*>(std::malloc(12ull * (nuniq ? nuniq : 1)));
+  res->cells = static_cast<uint32_t*>(ct_host_alloc(12ull * (nuniq ? nuniq : 1)));
   if (!res->simplices || !res->lambda || !res->barycentric || !res->track_id || !res->scalar || !res->cells)
     return cfail(ctx, FTK2B_OOM, "host result allocation failed");
   C_TRY(ct_d2h(ctx, res->simplices, simp, 24ull * n));
