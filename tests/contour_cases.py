@@ -74,6 +74,16 @@ def ties_2d():
     return dict(field=f, local_dims=[16, 16, 4], offset=None, global_dims=None, threshold=0.0, q=1e6)
 
 
+def ties_2d_offset():
+    """Integer values on a 14x12x4 sub-box at offset (3, 4, 1) of a 20x18x5
+    mesh: parity ties and quads cut at the sub-box's upper faces."""
+    rng = np.random.default_rng(4)
+    full = rng.integers(-1, 2, (5, 18, 20)).astype(np.float64)
+    sub = np.ascontiguousarray(full[1:5, 4:16, 3:17])
+    return dict(field=sub, local_dims=[14, 12, 4], offset=[3, 4, 1], global_dims=[20, 18, 5], threshold=0.0,
+                q=1e6)
+
+
 def single_layer_3d():
     f = gaussian_potential((10, 10, 10), 2, seed=8, n_blobs=6, dtype=np.float64)
     return dict(field=f, local_dims=[10, 10, 10, 2], offset=None, global_dims=None, threshold=-0.01, q=1e6)
@@ -89,6 +99,7 @@ CASES = {
     "gauss_2d_f64": gauss_2d_f64,
     "gauss_3d_f32_offset": gauss_3d_f32_offset,
     "ties_2d": ties_2d,
+    "ties_2d_offset": ties_2d_offset,
     "single_layer_3d": single_layer_3d,
     "no_crossing": no_crossing,
 }
