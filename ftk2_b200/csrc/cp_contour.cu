@@ -386,7 +386,8 @@ __device__ __forceinline__ void ct_sort4(unsigned* v, int k) {
 __global__ void ct_cells_kernel(CtGeom g, const unsigned long long* __restrict__ list, const unsigned* list_cnt,
                                 const unsigned short* __restrict__ mask, const unsigned* __restrict__ voff,
                                 const unsigned long long* __restrict__ first, unsigned n,
-                                unsigned* __restrict__ cells, unsigned* cnt, unsigned cap, unsigned* parent,
+                                unsigned* __restrict__ cells, unsigned long long* cnt, unsigned cap,
+                                unsigned* parent,
                                 unsigned* err) {
   const int d = g.d;
   const int kc = d;  // entries per cell
@@ -465,10 +466,10 @@ __global__ void ct_cells_kernel(CtGeom g, const unsigned long long* __restrict__
       if (lane >= o) incl += y;
     }
     const unsigned wtot = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned wbase = 0;
-    if (lane == 31 && wtot) wbase = atomicAdd(cnt, wtot);
+    unsigned long long wbase = 0;
+    if (lane == 31 && wtot) wbase = atomicAdd(cnt, (unsigned long long)wtot);
     wbase = __shfl_sync(0xffffffffu, wbase, 31);
-    unsigned slot = wbase + incl - (unsigned)ncell;
+    unsigned long long slot = wbase + incl - (unsigned)ncell;
     for (int c = 0; c < ncell; ++c, ++slot) {
       ct_sort4(cell[c], kc);
       if (slot < cap)
@@ -490,17 +491,15 @@ __global__ void ct_fill_u64_kernel(unsigned long long* __restrict__ v, unsigned 
 // into buckets by their leading node: counts per leading node, a scan, a
 // scatter into the buckets, then a small sort of each bucket's rows (a few
 // rows: the cells at one crossing edge).
-__global__ void ct_bucket_count_kernel(const unsigned* __restrict__ cells, const unsigned* cnt_ptr, unsigned cap,
-                                       int k, unsigned* __restrict__ bcount) {
-  const unsigned m = min(*cnt_ptr, cap);
+__global__ void ct_bucket_count_kernel(const unsigned* __restrict__ cells, unsigned m, int k,
+                                       unsigned* __restrict__ bcount) {
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
     atomicAdd(bcount + cells[(size_t)i * k], 1u);
 }
 
-__global__ void ct_bucket_scatter_kernel(const unsigned* __restrict__ cells, const unsigned* cnt_ptr,
-                                         unsigned cap, int k, const unsigned* __restrict__ boff,
-                                         unsigned* __restrict__ bcur, unsigned* __restrict__ out) {
-  const unsigned m = min(*cnt_ptr, cap);
+__global__ void ct_bucket_scatter_kernel(const unsigned* __restrict__ cells, unsigned m, int k,
+                                         const unsigned* __restrict__ boff, unsigned* __restrict__ bcur,
+                                         unsigned* __restrict__ out) {
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     const unsigned* c = cells + (size_t)i * k;
     const unsigned a = c[0];
@@ -701,6 +700,7 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   auto* blk = static_cast<unsigned*>(B[kBufBlk].p);
   auto* counts = static_cast<unsigned*>(B[kBufCount].p);  // [0] n, [1] cells, [2] roots, [3] err
   auto* total64 = reinterpret_cast<unsigned long long*>(counts + 8);
+  auto* cell64 = reinterpret_cast<unsigned long long*>(counts + 10);  // manifold cells (64-bit)
   const T* a = static_cast<const T*>(field);
   const unsigned sms = (unsigned)ctx->num_sms;
 
@@ -754,14 +754,17 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
     C_TRY(B[kBufCells].ensure((size_t)4 * kc * cap));
     auto* cells = static_cast<unsigned*>(B[kBufCells].p);
     C_TRY(cudaMemsetAsync(counts + 1, 0, 12, st));
+    C_TRY(cudaMemsetAsync(cell64, 0, 8, st));
     if (n) ct_iota_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(parent, n);
-    ct_cells_kernel<<<wgrid, 256, 0, st>>>(g, list, list_cnt, mask, voff, first, n, cells,
-                                                                        counts + 1, cap, parent, counts + 3);
+    ct_cells_kernel<<<wgrid, 256, 0, st>>>(g, list, list_cnt, mask, voff, first, n, cells, cell64, cap, parent,
+                                           counts + 3);
     ctx->launches += 2;
-    C_TRY(cudaMemcpyAsync(&ncell, counts + 1, 4, cudaMemcpyDeviceToHost, st));
+    unsigned long long nc64 = 0;
+    C_TRY(cudaMemcpyAsync(&nc64, cell64, 8, cudaMemcpyDeviceToHost, st));
     C_TRY(ctx->sync());
+    if (nc64 >= 0x7FFFFFFFull) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 - 1 manifold cells");
+    ncell = (unsigned)nc64;
     if (ncell <= cap) break;
-    if (ncell >= 0x7FFFFFFFu) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 manifold cells");
     cap = ncell;
   }
   auto* cells = static_cast<unsigned*>(B[kBufCells].p);
@@ -783,11 +786,11 @@ ftk2b_status run_contour(ftk2b_ctx* ctx, const CtGeom& g, const void* field, T t
   if (ncell) {
     C_TRY(cudaMemsetAsync(boff, 0, 4ull * nb, st));
     C_TRY(cudaMemsetAsync(bcur, 0, 4ull * nb, st));
-    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, boff);
+    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, ncell, kc, boff);
     ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
     C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
     ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
-    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, kc, boff, bcur, cells_out);
+    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, ncell, kc, boff, bcur, cells_out);
     ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(cells_out, boff, n, kc, counts + 3,
                                                                          nullptr);
     ctx->launches += 6;
@@ -985,8 +988,8 @@ __global__ void fs_list_kernel(CtGeom g, const unsigned long long* __restrict__ 
 // h_T or n (engine.hpp:1388-1413).  Two passes: count, reserve per warp, write.
 __global__ void fs_cells_kernel(CtGeom g, FsTables tb, const unsigned long long* __restrict__ list,
                                 const unsigned* list_cnt, const unsigned long long* __restrict__ mask,
-                                const unsigned* __restrict__ voff, unsigned* __restrict__ cells, unsigned* cnt,
-                                unsigned cap, unsigned* parent, unsigned* err) {
+                                const unsigned* __restrict__ voff, unsigned* __restrict__ cells,
+                                unsigned long long* cnt, unsigned cap, unsigned* parent, unsigned* err) {
   const int lane = threadIdx.x & 31;
   const unsigned nl = *list_cnt;
   const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
@@ -1042,10 +1045,10 @@ __global__ void fs_cells_kernel(CtGeom g, FsTables tb, const unsigned long long*
       if (lane >= o) incl += y;
     }
     const unsigned wtot = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned wbase = 0;
-    if (lane == 31 && wtot) wbase = atomicAdd(cnt, wtot);
+    unsigned long long wbase = 0;
+    if (lane == 31 && wtot) wbase = atomicAdd(cnt, (unsigned long long)wtot);
     wbase = __shfl_sync(0xffffffffu, wbase, 31);
-    unsigned slot = wbase + incl - mine;
+    unsigned long long slot = wbase + incl - mine;
     // pass 2: write and join
     if (mine) {
       const unsigned hs = rank[0];
@@ -1090,6 +1093,7 @@ ftk2b_status run_fiber_surface(ftk2b_ctx* ctx, const CtGeom& g, const FsTables& 
   auto* blk = static_cast<unsigned*>(B[kBufBlk].p);
   auto* counts = static_cast<unsigned*>(B[kBufCount].p);  // [0] n, [1] cells, [2] roots, [3] err, [4] cubes
   auto* total64 = reinterpret_cast<unsigned long long*>(counts + 8);
+  auto* cell64 = reinterpret_cast<unsigned long long*>(counts + 10);  // manifold cells (64-bit)
   const T* a0 = static_cast<const T*>(fa);
   const T* a1 = static_cast<const T*>(fb);
   const unsigned sms = (unsigned)ctx->num_sms;
@@ -1128,14 +1132,17 @@ ftk2b_status run_fiber_surface(ftk2b_ctx* ctx, const CtGeom& g, const FsTables& 
     C_TRY(B[kBufCells].ensure((size_t)12 * cap));
     auto* cells = static_cast<unsigned*>(B[kBufCells].p);
     C_TRY(cudaMemsetAsync(counts + 1, 0, 12, st));
+    C_TRY(cudaMemsetAsync(cell64, 0, 8, st));
     if (n) ct_iota_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(parent, n);
-    fs_cells_kernel<<<16u * sms, 256, 0, st>>>(g, tb, list, list_cnt, mask, voff, cells, counts + 1, cap, parent,
+    fs_cells_kernel<<<16u * sms, 256, 0, st>>>(g, tb, list, list_cnt, mask, voff, cells, cell64, cap, parent,
                                               counts + 3);
     ctx->launches += 2;
-    C_TRY(cudaMemcpyAsync(&ncell, counts + 1, 4, cudaMemcpyDeviceToHost, st));
+    unsigned long long nc64 = 0;
+    C_TRY(cudaMemcpyAsync(&nc64, cell64, 8, cudaMemcpyDeviceToHost, st));
     C_TRY(ctx->sync());
+    if (nc64 >= 0x7FFFFFFFull) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 - 1 manifold triangles");
+    ncell = (unsigned)nc64;
     if (ncell <= cap) break;
-    if (ncell >= 0x7FFFFFFFu) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 manifold triangles");
     cap = ncell;
   }
   auto* cells = static_cast<unsigned*>(B[kBufCells].p);
@@ -1163,11 +1170,11 @@ ftk2b_status run_fiber_surface(ftk2b_ctx* ctx, const CtGeom& g, const FsTables& 
     C_TRY(cudaMemsetAsync(boff, 0, 4ull * nb, st));
     C_TRY(cudaMemsetAsync(bcur, 0, 4ull * nb, st));
     C_TRY(cudaMemsetAsync(uoff, 0, 4ull * nb, st));
-    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, 3, boff);
+    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, ncell, 3, boff);
     ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
     C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
     ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
-    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, counts + 1, cap, 3, boff, bcur, rows);
+    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, ncell, 3, boff, bcur, rows);
     ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(rows, boff, n, 3, counts + 3, uoff);
     ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(uoff, nb, btot);
     C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
