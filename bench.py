@@ -565,7 +565,9 @@ def main():
         v, sample = cpu_baseline_sample(field.cpu().numpy())
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1,
                                 "kind": "reference", "sample": sample}
-    if not args.no_extra:
+    # the extra lines are one-GPU measurements (and their CPU baselines belong
+    # to rank 0 at N = 1): with several ranks only the replica line is timed
+    if not args.no_extra and world == 1:
         del field, fdev
         keep.clear()
         torch.cuda.empty_cache()
