@@ -679,7 +679,7 @@ void* ct_host_alloc(size_t bytes) {
 enum {
   kBufField = 0, kBufPos, kBufMask, kBufBlk, kBufVoff, kBufSimp, kBufLam, kBufBary, kBufFirst, kBufParent,
   kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount, kBufList,
-  kBufField2
+  kBufField2, kBufUpOff, kBufUpNbr, kBufBaseCells
 };
 
 template <typename T>
@@ -1214,6 +1214,490 @@ ftk2b_status run_fiber_surface(ftk2b_ctx* ctx, const CtGeom& g, const FsTables& 
   return FTK2B_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Level sets on ExtrudedSimplicialMesh(UnstructuredSimplicialMesh, L)
+// (mesh.hpp:542-599): vertex ids v = s + t * S (S base vertices, layers
+// t = 0 .. L), the field per vertex.  The mesh's edges from a lower vertex
+// a + tS, in id order, are its spatial edges to b + tS (base edges a < b),
+// its vertical edge to a + (t + 1)S and the prism diagonals to b + (t + 1)S
+// (the Kuhn split of a prism over a sorted base cell joins v_a at t to v_b at
+// t + 1 only for a < b), so ranks again come from a per-vertex mask over
+// 2 deg(a) + 1 candidates and a scan.  The reference's first pass visits the
+// spatial and vertical edges only (iterate_simplices(1)); the diagonals it
+// meets while marching over the cells, which it visits by layer, base cell
+// (in stored order, each sorted) and Kuhn index j (vertices v_0..v_j at t,
+// v_j..v_k at t + 1), one worker at a time.
+
+struct CeGeom {
+  int d;                       // spacetime dims: 3 (triangle base) or 4 (tet base)
+  unsigned long long S, L;     // base vertices, layers
+  unsigned long long nv;       // S * (L + 1)
+  unsigned long long ncell;    // base cells
+  const unsigned* up_off;      // CSR of base neighbours b > a: up_nbr[up_off[a] .. up_off[a + 1])
+  const unsigned* up_nbr;
+  const unsigned* cells;       // ncell * d sorted base vertex ids
+};
+
+__device__ __forceinline__ int ce_nbr_index(const CeGeom& g, unsigned a, unsigned b) {
+  const unsigned lo = g.up_off[a], hi = g.up_off[a + 1];
+  for (unsigned i = lo; i < hi; ++i)
+    if (g.up_nbr[i] == b) return (int)(i - lo);
+  return -1;
+}
+
+// mask bit of the edge (x, y), x < y, in x's candidate order
+__device__ __forceinline__ int ce_bit(const CeGeom& g, unsigned long long x, unsigned long long y) {
+  const unsigned long long t = x / g.S;
+  const unsigned a = (unsigned)(x - t * g.S);
+  const int deg = (int)(g.up_off[a + 1] - g.up_off[a]);
+  if (y < (t + 1) * g.S) return ce_nbr_index(g, a, (unsigned)(y - t * g.S));
+  if (y == x + g.S) return deg;
+  return deg + 1 + ce_nbr_index(g, a, (unsigned)(y - (t + 1) * g.S));
+}
+
+__device__ __forceinline__ unsigned ce_node(const CeGeom& g, const unsigned long long* __restrict__ mask,
+                                            const unsigned* __restrict__ voff, unsigned long long x,
+                                            unsigned long long y) {
+  const int bit = max(ce_bit(g, x, y), 0);  // every cell pair is a base edge, so the index exists
+  return voff[x] + (unsigned)__popcll(mask[x] & ((1ull << bit) - 1ull));
+}
+
+template <typename T>
+__global__ void ce_sign_kernel(CeGeom g, const T* __restrict__ a, T thr, double q, unsigned char* __restrict__ pos) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < g.nv;
+       v += (unsigned long long)gridDim.x * blockDim.x)
+    pos[v] = ct_positive(fp<T>::sub(__ldg(a + v), thr), v, q) ? 1 : 0;
+}
+
+__global__ void ce_mask_kernel(CeGeom g, const unsigned char* __restrict__ pos, unsigned long long* __restrict__ mask,
+                               unsigned* __restrict__ blk, unsigned long long* __restrict__ total64) {
+  __shared__ unsigned tot;
+  const unsigned long long v = blockIdx.x * (unsigned long long)kCtThreads + threadIdx.x;
+  unsigned long long m = 0;
+  if (v < g.nv) {
+    const unsigned long long t = v / g.S;
+    const unsigned a = (unsigned)(v - t * g.S);
+    const unsigned lo = g.up_off[a], hi = g.up_off[a + 1];
+    const int deg = (int)(hi - lo);
+    const unsigned char p = pos[v];
+    for (unsigned i = lo; i < hi; ++i)
+      if (pos[g.up_nbr[i] + t * g.S] != p) m |= 1ull << (i - lo);
+    if (t < g.L) {
+      if (pos[v + g.S] != p) m |= 1ull << deg;
+      for (unsigned i = lo; i < hi; ++i)
+        if (pos[g.up_nbr[i] + (t + 1) * g.S] != p) m |= 1ull << (deg + 1 + (int)(i - lo));
+    }
+    mask[v] = m;
+  }
+  ct_block_scan((unsigned)__popcll(m), &tot);
+  if (threadIdx.x == 0) {
+    blk[blockIdx.x] = tot;
+    atomicAdd(total64, (unsigned long long)tot);
+  }
+}
+
+template <typename T>
+__global__ void ce_emit_kernel(CeGeom g, const T* __restrict__ a, T thr, const unsigned long long* __restrict__ mask,
+                               const unsigned* __restrict__ blk_off, unsigned* __restrict__ voff,
+                               unsigned long long* __restrict__ simp, double* __restrict__ lam,
+                               float* __restrict__ bary) {
+  __shared__ unsigned tot;
+  const unsigned long long v = blockIdx.x * (unsigned long long)kCtThreads + threadIdx.x;
+  const unsigned long long m = v < g.nv ? mask[v] : 0ull;
+  const unsigned base = blk_off[blockIdx.x] + ct_block_scan((unsigned)__popcll(m), &tot);
+  if (v >= g.nv) return;
+  voff[v] = base;
+  if (!m) return;
+  const unsigned long long t = v / g.S;
+  const unsigned aa = (unsigned)(v - t * g.S);
+  const unsigned lo = g.up_off[aa];
+  const int deg = (int)(g.up_off[aa + 1] - lo);
+  const T a0 = fp<T>::sub(__ldg(a + v), thr);
+  unsigned r = base;
+  for (int bit = 0; bit < 2 * deg + 1; ++bit) {
+    if (!((m >> bit) & 1ull)) continue;
+    unsigned long long y;
+    if (bit < deg) y = g.up_nbr[lo + bit] + t * g.S;
+    else if (bit == deg) y = v + g.S;
+    else y = g.up_nbr[lo + bit - deg - 1] + (t + 1) * g.S;
+    const T a1 = fp<T>::sub(__ldg(a + y), thr);
+    T l0, l1;
+    ct_solve(a0, a1, &l0, &l1);
+    simp[2 * (size_t)r] = v;
+    simp[2 * (size_t)r + 1] = y;
+    lam[2 * (size_t)r] = (double)l0;
+    lam[2 * (size_t)r + 1] = (double)l1;
+    bary[2 * (size_t)r] = (float)l0;
+    bary[2 * (size_t)r + 1] = (float)l1;
+    ++r;
+  }
+}
+
+// vertices (global ids, ascending) and signs of spacetime cell q = (t, c, j)
+__device__ __forceinline__ void ce_cell(const CeGeom& g, const unsigned char* pos, unsigned long long q,
+                                        unsigned long long* vid, unsigned* ps, int* npos) {
+  const int d = g.d;
+  const unsigned long long j = q % d, tc = q / d, c = tc % g.ncell, t = tc / g.ncell;
+  const unsigned* cv = g.cells + c * d;
+  int k = 0;
+  for (int l = 0; l <= (int)j; ++l) vid[k++] = cv[l] + t * g.S;
+  for (int l = (int)j; l < d; ++l) vid[k++] = cv[l] + (t + 1) * g.S;
+  unsigned s = 0;
+  int np = 0;
+  for (int i = 0; i <= d; ++i) {
+    const unsigned b = pos[vid[i]];
+    s |= b << i;
+    np += (int)b;
+  }
+  *ps = s;
+  *npos = np;
+}
+
+__device__ __forceinline__ bool ce_late(const CeGeom& g, unsigned long long x, unsigned long long y) {
+  // a diagonal: its ends lie on consecutive layers and it is not vertical
+  return y >= (x / g.S + 1) * g.S && y != x + g.S;
+}
+
+// (2D+t) first meeting of every diagonal node: (cell order, marching position)
+__global__ void ce_first_kernel(CeGeom g, const unsigned char* __restrict__ pos,
+                                const unsigned long long* __restrict__ mask, const unsigned* __restrict__ voff,
+                                unsigned long long* __restrict__ first) {
+  const unsigned long long nsc = g.L * g.ncell * 3ull;
+  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < nsc;
+       q += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long vid[5];
+    unsigned ps;
+    int npos;
+    ce_cell(g, pos, q, vid, &ps, &npos);
+    if (npos == 0 || npos == 4) continue;
+    CtSimplex x;
+    x.ps = ps;
+    x.npos = npos;
+    int ea[4], eb[4];
+    const int ne = ct_crossings(x, 4, ea, eb);
+    for (int k = 0; k < ne; ++k) {
+      const unsigned long long lo = vid[min(ea[k], eb[k])], hi = vid[max(ea[k], eb[k])];
+      if (!ce_late(g, lo, hi)) continue;
+      atomicMin(first + ce_node(g, mask, voff, lo, hi), q * 4ull + (unsigned long long)k);
+    }
+  }
+}
+
+// marching on every spacetime cell, one per thread; slots reserved per warp
+__global__ void ce_cells_kernel(CeGeom g, const unsigned char* __restrict__ pos,
+                                const unsigned long long* __restrict__ mask, const unsigned* __restrict__ voff,
+                                const unsigned long long* __restrict__ first, unsigned n,
+                                unsigned* __restrict__ cells, unsigned long long* cnt, unsigned cap,
+                                unsigned* parent, unsigned* err) {
+  const int d = g.d, kc = d;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nsc = g.L * g.ncell * (unsigned long long)d;
+  for (unsigned long long q0 = blockIdx.x * (unsigned long long)blockDim.x; q0 < nsc;
+       q0 += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long q = q0 + threadIdx.x;
+    unsigned cell[3][4];
+    unsigned nodes[6];
+    int nn = 0, ncell = 0;
+    if (q < nsc) {
+      unsigned long long vid[5];
+      unsigned ps;
+      int npos;
+      ce_cell(g, pos, q, vid, &ps, &npos);
+      CtSimplex x;
+      x.ps = ps;
+      x.npos = npos;
+      auto node = [&](int i, int j) { return ce_node(g, mask, voff, vid[min(i, j)], vid[max(i, j)]); };
+      if (npos != 0 && npos != d + 1) {
+        if (npos == 1 || npos == d || d == 3) {
+          int ea[6], eb[6];
+          const int ne = ct_crossings(x, d + 1, ea, eb);
+          for (int k = 0; k < ne; ++k) nodes[k] = node(ea[k], eb[k]);
+          nn = ne;
+          if (ne == d) {
+            for (int k = 0; k < d; ++k) cell[0][k] = nodes[k];
+            ncell = 1;
+          } else {
+            unsigned nd[4];
+            unsigned long long key[4];
+            for (int k = 0; k < 4; ++k) {
+              nd[k] = nodes[k];
+              const unsigned long long f = first[nd[k]];
+              key[k] = f == ~0ull ? (unsigned long long)nd[k] : (unsigned long long)n + f;
+            }
+            for (int i = 1; i < 4; ++i)
+              for (int j = i; j > 0 && key[j - 1] > key[j]; --j) {
+                const unsigned long long kx = key[j - 1];
+                key[j - 1] = key[j];
+                key[j] = kx;
+                const unsigned nx = nd[j - 1];
+                nd[j - 1] = nd[j];
+                nd[j] = nx;
+              }
+            cell[0][0] = nd[0], cell[0][1] = nd[1], cell[0][2] = nd[2];
+            cell[1][0] = nd[0], cell[1][1] = nd[2], cell[1][2] = nd[3];
+            ncell = 2;
+          }
+        } else {
+          const bool two_pos = npos == 2;
+          int two[2], three[3], n2 = 0, n3 = 0;
+          for (int i = 0; i < 5; ++i) {
+            if ((((ps >> i) & 1u) != 0) == two_pos) two[n2++] = i;
+            else three[n3++] = i;
+          }
+          unsigned T0[3], T1[3];
+          for (int t = 0; t < 3; ++t) {
+            T0[t] = node(two[0], three[t]);
+            T1[t] = node(two[1], three[t]);
+          }
+          cell[0][0] = T0[0], cell[0][1] = T0[1], cell[0][2] = T0[2], cell[0][3] = T1[2];
+          cell[1][0] = T0[0], cell[1][1] = T0[1], cell[1][2] = T1[1], cell[1][3] = T1[2];
+          cell[2][0] = T0[0], cell[2][1] = T1[0], cell[2][2] = T1[1], cell[2][3] = T1[2];
+          for (int t = 0; t < 3; ++t) nodes[t] = T0[t], nodes[3 + t] = T1[t];
+          nn = 6;
+          ncell = 3;
+        }
+      }
+    }
+    unsigned incl = (unsigned)ncell;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned wtot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long wbase = 0;
+    if (lane == 31 && wtot) wbase = atomicAdd(cnt, (unsigned long long)wtot);
+    wbase = __shfl_sync(0xffffffffu, wbase, 31);
+    unsigned long long slot = wbase + incl - (unsigned)ncell;
+    for (int c = 0; c < ncell; ++c, ++slot) {
+      ct_sort4(cell[c], kc);
+      if (slot < cap)
+        for (int k = 0; k < kc; ++k) cells[(size_t)slot * kc + k] = cell[c][k];
+    }
+    for (int k = 1; k < nn; ++k) uf_unite(parent, nodes[0], nodes[k], err);
+  }
+}
+
+template <typename T>
+ftk2b_status run_contour_extruded(ftk2b_ctx* ctx, CeGeom g, const void* field, T thr, double q,
+                                  ftk2b_contour_result* res) {
+  cudaStream_t st = ctx->stream;
+  DevBuf* B = ctx->contour;
+  const int d = g.d, kc = d;
+  const unsigned long long nblk = (g.nv + kCtThreads - 1) / kCtThreads;
+  if (nblk >= 0xFFFFFFF0ull) return cfail(ctx, FTK2B_UNSUPPORTED, "mesh too large");
+  C_TRY(B[kBufPos].ensure(g.nv));
+  C_TRY(B[kBufHist].ensure(8 * g.nv));
+  C_TRY(B[kBufVoff].ensure(4 * g.nv));
+  C_TRY(B[kBufBlk].ensure(4 * (nblk + 1)));
+  C_TRY(B[kBufCount].ensure(64));
+  auto* pos = static_cast<unsigned char*>(B[kBufPos].p);
+  auto* mask = static_cast<unsigned long long*>(B[kBufHist].p);
+  auto* voff = static_cast<unsigned*>(B[kBufVoff].p);
+  auto* blk = static_cast<unsigned*>(B[kBufBlk].p);
+  auto* counts = static_cast<unsigned*>(B[kBufCount].p);  // [0] n, [2] roots, [3] err
+  auto* total64 = reinterpret_cast<unsigned long long*>(counts + 8);
+  auto* cell64 = reinterpret_cast<unsigned long long*>(counts + 10);
+  const T* a = static_cast<const T*>(field);
+  const unsigned sms = (unsigned)ctx->num_sms;
+  C_TRY(cudaMemsetAsync(counts, 0, 64, st));
+  C_TRY(cudaEventRecord(ctx->ev0, st));
+  ce_sign_kernel<T><<<grid_of(g.nv, 256, 32ull * sms), 256, 0, st>>>(g, a, thr, q, pos);
+  ce_mask_kernel<<<(unsigned)nblk, kCtThreads, 0, st>>>(g, pos, mask, blk, total64);
+  C_TRY(launch_scan(blk, (unsigned)nblk, counts + 0, nullptr, st));
+  ctx->launches += 3;
+  unsigned long long n64 = 0;
+  C_TRY(cudaMemcpyAsync(&n64, total64, 8, cudaMemcpyDeviceToHost, st));
+  C_TRY(ctx->sync());
+  if (n64 >= 0xFFFFFFF0ull) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^32 - 16 crossing edges");
+  const unsigned n = (unsigned)n64;
+  const size_t ncap = n ? n : 1;
+  C_TRY(B[kBufSimp].ensure(16 * ncap));
+  C_TRY(B[kBufLam].ensure(16 * ncap));
+  C_TRY(B[kBufBary].ensure(8 * ncap));
+  C_TRY(B[kBufParent].ensure(4 * ncap));
+  C_TRY(B[kBufTrack].ensure(8 * ncap));
+  C_TRY(B[kBufFirst].ensure(8 * ncap));
+  auto* simp = static_cast<unsigned long long*>(B[kBufSimp].p);
+  auto* lam = static_cast<double*>(B[kBufLam].p);
+  auto* bary = static_cast<float*>(B[kBufBary].p);
+  auto* parent = static_cast<unsigned*>(B[kBufParent].p);
+  auto* track = static_cast<unsigned long long*>(B[kBufTrack].p);
+  auto* first = static_cast<unsigned long long*>(B[kBufFirst].p);
+  ce_emit_kernel<T><<<(unsigned)nblk, kCtThreads, 0, st>>>(g, a, thr, mask, blk, voff, simp, lam, bary);
+  ctx->launches += 1;
+  const unsigned long long nsc = g.L * g.ncell * (unsigned long long)d;
+  if (n) ct_fill_u64_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(first, ~0ull, n);
+  if (d == 3 && n) {
+    ce_first_kernel<<<grid_of(nsc, 256, 64ull * sms), 256, 0, st>>>(g, pos, mask, voff, first);
+    ctx->launches += 2;
+  }
+  unsigned cap = (unsigned)std::min<unsigned long long>(
+      0x7FFFFFFFull, std::max<unsigned long long>(1024ull, (d == 4 ? 8ull : 4ull) * n));
+  unsigned ncell = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    C_TRY(B[kBufCells].ensure((size_t)4 * kc * cap));
+    auto* cells = static_cast<unsigned*>(B[kBufCells].p);
+    C_TRY(cudaMemsetAsync(counts + 1, 0, 12, st));
+    C_TRY(cudaMemsetAsync(cell64, 0, 8, st));
+    if (n) ct_iota_kernel<<<grid_of(n, 256, 8ull * sms), 256, 0, st>>>(parent, n);
+    ce_cells_kernel<<<grid_of(nsc, 256, 64ull * sms), 256, 0, st>>>(g, pos, mask, voff, first, n, cells, cell64,
+                                                                    cap, parent, counts + 3);
+    ctx->launches += 2;
+    unsigned long long nc64 = 0;
+    C_TRY(cudaMemcpyAsync(&nc64, cell64, 8, cudaMemcpyDeviceToHost, st));
+    C_TRY(ctx->sync());
+    if (nc64 >= 0x7FFFFFFFull) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 - 1 manifold cells");
+    ncell = (unsigned)nc64;
+    if (ncell <= cap) break;
+    cap = ncell;
+  }
+  auto* cells = static_cast<unsigned*>(B[kBufCells].p);
+  const unsigned ccap = ncell ? ncell : 1;
+  const unsigned nb = n + 1;
+  const unsigned sblocks = (unsigned)((nb + kCtThreads * kScanPer - 1) / (kCtThreads * kScanPer));
+  C_TRY(B[kBufKey0].ensure(4ull * nb));
+  C_TRY(B[kBufKey1].ensure(4ull * nb));
+  C_TRY(B[kBufVal0].ensure(4ull * (sblocks + 1)));
+  C_TRY(B[kBufCellsOut].ensure(4ull * kc * ccap));
+  auto* boff = static_cast<unsigned*>(B[kBufKey0].p);
+  auto* bcur = static_cast<unsigned*>(B[kBufKey1].p);
+  auto* btot = static_cast<unsigned*>(B[kBufVal0].p);
+  auto* cells_out = static_cast<unsigned*>(B[kBufCellsOut].p);
+  const unsigned cg = grid_of(ccap, 256, 16ull * sms);
+  if (ncell) {
+    C_TRY(cudaMemsetAsync(boff, 0, 4ull * nb, st));
+    C_TRY(cudaMemsetAsync(bcur, 0, 4ull * nb, st));
+    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, ncell, kc, boff);
+    ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
+    ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, ncell, kc, boff, bcur, cells_out);
+    ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(cells_out, boff, n, kc, counts + 3,
+                                                                         nullptr);
+    ctx->launches += 6;
+  }
+  if (n) {
+    C_TRY(launch_uf_label(parent, counts + 0, n, track, counts + 2, st));
+    ctx->launches += 1;
+  }
+  C_TRY(cudaEventRecord(ctx->ev1, st));
+  unsigned hc[4] = {0, 0, 0, 0};
+  C_TRY(cudaMemcpyAsync(hc, counts, 16, cudaMemcpyDeviceToHost, st));
+  C_TRY(ctx->sync());
+  res->n_features = n;
+  res->cell_dim = d - 1;
+  res->n_cells = ncell;
+  res->simplices = static_cast<uint64_t*>(ct_host_alloc(16 * ncap));
+  res->lambda = static_cast<double*>(ct_host_alloc(16 * ncap));
+  res->barycentric = static_cast<float*>(ct_host_alloc(8 * ncap));
+  res->track_id = static_cast<uint64_t*>(ct_host_alloc(8 * ncap));
+  res->scalar = static_cast<float*>(ct_host_alloc(4 * ncap));
+  res->cells = static_cast<uint32_t*>(ct_host_alloc(4ull * kc * ccap));
+  if (!res->simplices || !res->lambda || !res->barycentric || !res->track_id || !res->scalar || !res->cells)
+    return cfail(ctx, FTK2B_OOM, "host result allocation failed");
+  C_TRY(ct_d2h(ctx, res->simplices, simp, 16ull * n));
+  C_TRY(ct_d2h(ctx, res->lambda, lam, 16ull * n));
+  C_TRY(ct_d2h(ctx, res->barycentric, bary, 8ull * n));
+  C_TRY(ct_d2h(ctx, res->track_id, track, 8ull * n));
+  C_TRY(ct_d2h(ctx, res->cells, cells_out, 4ull * kc * ncell));
+  if (hc[3] & 1u) return cfail(ctx, FTK2B_CUDA_ERROR, "union-find did not settle");
+  if (hc[3] & 2u) return cfail(ctx, FTK2B_CUDA_ERROR, "duplicate manifold cell");
+  const float sc = (float)thr;
+  for (unsigned i = 0; i < n; ++i) res->scalar[i] = sc;
+  res->n_tracks = hc[2];
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  res->device_ms = ms;
+  return FTK2B_OK;
+}
+
+// Level sets on an extruded mesh: base cells sorted, the CSR of base edges by
+// lower vertex, the field (one value per vertex id) staged.
+ftk2b_status contour_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                              double threshold, double sos_q, ftk2b_contour_result** out) {
+  const int cd = mesh->base_cell_dim;
+  if (cd != 2 && cd != 3) return cfail(ctx, FTK2B_UNSUPPORTED, "extruded base cells are triangles or tets");
+  if (!mesh->base_cells || !mesh->n_base_cells || !mesh->n_base_verts || mesh->n_layers < 1)
+    return cfail(ctx, FTK2B_INVALID_ARG, "extruded mesh needs base cells, vertices and at least one layer");
+  const unsigned long long S = mesh->n_base_verts, L = mesh->n_layers, nv = S * (L + 1);
+  if (S >= 0xFFFFFFFFull || nv >= (1ull << 40)) return cfail(ctx, FTK2B_UNSUPPORTED, "mesh too large");
+  if (field->nd != 1 || field->dims[0] < nv)
+    return cfail(ctx, FTK2B_INVALID_ARG, "extruded meshes read a per-vertex array of at least %llu values", nv);
+  const int d = cd + 1;
+  const unsigned long long nc = mesh->n_base_cells;
+  std::vector<unsigned> cells(nc * d);
+  std::vector<unsigned long long> pairs;
+  pairs.reserve(nc * d * (d - 1) / 2);
+  for (unsigned long long c = 0; c < nc; ++c) {
+    unsigned v[4];
+    for (int k = 0; k < d; ++k) {
+      const uint64_t x = mesh->base_cells[c * d + k];
+      if (x >= S) return cfail(ctx, FTK2B_INVALID_ARG, "base cell %llu names vertex %llu of %llu", c,
+                               (unsigned long long)x, S);
+      v[k] = (unsigned)x;
+    }
+    std::sort(v, v + d);
+    for (int k = 0; k < d; ++k) cells[c * d + k] = v[k];
+    for (int i = 0; i < d; ++i)
+      for (int j = i + 1; j < d; ++j) pairs.push_back(((unsigned long long)v[i] << 32) | v[j]);
+  }
+  std::sort(pairs.begin(), pairs.end());
+  pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+  std::vector<unsigned> up_off(S + 1, 0), up_nbr(pairs.size());
+  for (unsigned long long p : pairs) ++up_off[(p >> 32) + 1];
+  for (unsigned long long a = 0; a < S; ++a) {
+    if (up_off[a + 1] > 31) return cfail(ctx, FTK2B_UNSUPPORTED, "base vertex with more than 31 higher neighbours");
+    up_off[a + 1] += up_off[a];
+  }
+  for (size_t i = 0; i < pairs.size(); ++i) up_nbr[i] = (unsigned)(pairs[i] & 0xFFFFFFFFu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return cfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  DevBuf* B = ctx->contour;
+  C_TRY(B[kBufUpOff].ensure(4 * up_off.size()));
+  C_TRY(B[kBufUpNbr].ensure(4 * (up_nbr.size() + 1)));
+  C_TRY(B[kBufBaseCells].ensure(4 * cells.size()));
+  C_TRY(cudaMemcpyAsync(B[kBufUpOff].p, up_off.data(), 4 * up_off.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (!up_nbr.empty())
+    C_TRY(cudaMemcpyAsync(B[kBufUpNbr].p, up_nbr.data(), 4 * up_nbr.size(), cudaMemcpyHostToDevice, ctx->stream));
+  C_TRY(cudaMemcpyAsync(B[kBufBaseCells].p, cells.data(), 4 * cells.size(), cudaMemcpyHostToDevice, ctx->stream));
+  const size_t es = field->dtype == FTK2B_F64 ? 8 : 4;
+  const void* dev = field->comp[0];
+  if (field->location != FTK2B_DEVICE) {
+    C_TRY(B[kBufField].ensure(nv * es));
+    C_TRY(cudaMemcpyAsync(B[kBufField].p, field->comp[0], nv * es, cudaMemcpyHostToDevice, ctx->stream));
+    dev = B[kBufField].p;
+  }
+  CeGeom g;
+  std::memset(&g, 0, sizeof(g));
+  g.d = d;
+  g.S = S;
+  g.L = L;
+  g.nv = nv;
+  g.ncell = nc;
+  g.up_off = static_cast<const unsigned*>(B[kBufUpOff].p);
+  g.up_nbr = static_cast<const unsigned*>(B[kBufUpNbr].p);
+  g.cells = static_cast<const unsigned*>(B[kBufBaseCells].p);
+  auto* res = new (std::nothrow) ftk2b_contour_result;
+  if (!res) return cfail(ctx, FTK2B_OOM, "result allocation failed");
+  std::memset(res, 0, sizeof(*res));
+  const unsigned long long E = pairs.size();
+  res->n_simplices = E * (L + 1) + S * L + E * L;  // spatial, vertical, diagonal edges
+  // the upload of the host vectors must finish before they go out of scope
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    ftk2b_contour_result_free(res);
+    return cfail(ctx, FTK2B_CUDA_ERROR, "mesh upload failed");
+  }
+  const ftk2b_status st = field->dtype == FTK2B_F64
+                              ? run_contour_extruded<double>(ctx, g, dev, (double)threshold, sos_q, res)
+                              : run_contour_extruded<float>(ctx, g, dev, (float)threshold, sos_q, res);
+  if (st != FTK2B_OK) {
+    ftk2b_contour_result_free(res);
+    return st;
+  }
+  *out = res;
+  return FTK2B_OK;
+}
+
 }  // namespace
 
 // Geometry of a regular mesh and its scalar array(s) for the level-set and
@@ -1227,14 +1711,16 @@ extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_d
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field || !out) return cfail(ctx, FTK2B_INVALID_ARG, "null argument");
   *out = nullptr;
-  if (mesh->kind != FTK2B_MESH_REGULAR) return cfail(ctx, FTK2B_UNSUPPORTED, "level sets need a regular mesh");
-  const int d = mesh->ndims;
-  if (d != 3 && d != 4) return cfail(ctx, FTK2B_UNSUPPORTED, "regular meshes have 3 or 4 dims (got %d)", d);
   if (field->dtype != FTK2B_F32 && field->dtype != FTK2B_F64)
     return cfail(ctx, FTK2B_INVALID_ARG, "dtype must be FTK2B_F32 or FTK2B_F64");
-  if (field->ncomp != 1 || field->layout != FTK2B_LAYOUT_SEPARATE || !field->comp[0])
+  if (field->ncomp != 1 || !field->comp[0] ||
+      (field->layout != FTK2B_LAYOUT_SEPARATE && field->layout != FTK2B_LAYOUT_PER_VERTEX))
     return cfail(ctx, FTK2B_INVALID_ARG, "level sets read one scalar array (ncomp 1, layout SEPARATE)");
   if (!(sos_q > 0)) return cfail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
+  if (mesh->kind == FTK2B_MESH_EXTRUDED) return contour_extruded(ctx, mesh, field, threshold, sos_q, out);
+  if (mesh->kind != FTK2B_MESH_REGULAR) return cfail(ctx, FTK2B_INVALID_ARG, "unknown mesh kind %d", mesh->kind);
+  const int d = mesh->ndims;
+  if (d != 3 && d != 4) return cfail(ctx, FTK2B_UNSUPPORTED, "regular meshes have 3 or 4 dims (got %d)", d);
   CtGeom g;
   size_t nelem = 1;
   {

@@ -354,9 +354,11 @@ ftk2b_status ftk2b_cp_features_noalloc(const ftk2b_mesh_desc* mesh, const ftk2b_
 /* --- level sets (ContourPredicate<T>) -------------------------------------
  * Replaces SimplicialEngine<T, ContourPredicate<T>>::execute + get_complex
  * (engine.hpp:95-215, 822-996; predicate.hpp:135-183) on a regular mesh of
- * 3 (2D+t) or 4 (3D+t) dims.  field: ncomp 1, layout SEPARATE, comp[0] the
- * scalar array (nd == mesh dims, indexed by local coordinates; or nd 1,
- * indexed by global vertex id).  Features are the mesh edges whose endpoints
+ * 3 (2D+t) or 4 (3D+t) dims, or on an extruded mesh over triangles or tets
+ * (ExtrudedSimplicialMesh, mesh.hpp:542-599).  field: ncomp 1, layout
+ * SEPARATE, comp[0] the scalar array (regular: nd == mesh dims, indexed by
+ * local coordinates, or nd 1 indexed by global vertex id; extruded: nd 1,
+ * one value per vertex id s + t * n_base_verts).  Features are the mesh edges whose endpoints
  * have different simulation-of-simplicity signs of value - threshold, in
  * simplex order; cells are the manifold cells of get_complex (triangles on
  * 2D+t, tets on 3D+t) as sorted rows of feature indices, sorted and unique;

@@ -229,19 +229,32 @@ template <typename T>
 int run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, orc_result* out, orc_conn* conn) {
   using namespace ftk2;
   std::vector<uint64_t> dims, off, glob;
-  for (int i = 0; i < mesh->ndims; ++i) {
-    dims.push_back(mesh->local_dims[i]);
-    off.push_back(mesh->offset[i]);
-    glob.push_back(mesh->global_dims[i]);
+  std::shared_ptr<Mesh> mesh_ptr;
+  std::shared_ptr<RegularSimplicialMesh> reg;
+  if (mesh->kind == ORC_MESH_REGULAR) {
+    for (int i = 0; i < mesh->ndims; ++i) {
+      dims.push_back(mesh->local_dims[i]);
+      off.push_back(mesh->offset[i]);
+      glob.push_back(mesh->global_dims[i]);
+    }
+    reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
+    mesh_ptr = reg;
+  } else {
+    // ExtrudedSimplicialMesh over an UnstructuredSimplicialMesh: the field is
+    // per vertex (a 1-D array indexed by vertex id, engine.hpp:1000)
+    std::vector<double> coords(mesh->base_coords, mesh->base_coords + 3 * mesh->n_base_verts);
+    size_t nc = (size_t)mesh->n_base_cells * (mesh->base_cell_dim + 1);
+    std::vector<uint64_t> cells(mesh->base_cells, mesh->base_cells + nc);
+    auto base = std::make_shared<UnstructuredSimplicialMesh>(mesh->base_cell_dim, mesh->base_cell_dim, coords, cells);
+    mesh_ptr = std::make_shared<ExtrudedSimplicialMesh>(base, mesh->n_layers);
   }
-  auto reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
   ContourPredicate<T> pred;
   pred.var_name = "S";
   pred.threshold = (T)threshold;
   pred.sos_q = field->sos_q;
   std::map<std::string, ftk::ndarray<T>> data;
   data["S"] = make_array<T>(field->comp[0], field->nd, field->dims);
-  SimplicialEngine<T, ContourPredicate<T>> engine(reg, pred);
+  SimplicialEngine<T, ContourPredicate<T>> engine(mesh_ptr, pred);
   std::streambuf* saved = std::cout.rdbuf();
   std::ostringstream sink;
   std::cout.rdbuf(sink.rdbuf());
@@ -267,7 +280,7 @@ int run_contour(const orc_mesh* mesh, const orc_field* field, double threshold, 
       out->simplices[2 * i + v] = el.simplex.vertices[v];
       out->bary[2 * i + v] = el.barycentric_coords[0][v];
       T x;
-      if (a.nd() == 1) {
+      if (a.nd() == 1 || !reg) {
         x = a[el.simplex.vertices[v]];
       } else {
         std::vector<double> c = reg->get_vertex_coordinates(el.simplex.vertices[v]);
@@ -414,7 +427,8 @@ extern "C" int ftk2ref_run_contour(const orc_mesh* mesh, const orc_field* field,
                                    orc_result* out, orc_conn* conn) {
   std::memset(out, 0, sizeof(*out));
   std::memset(conn, 0, sizeof(*conn));
-  if (mesh->kind != ORC_MESH_REGULAR || (mesh->ndims != 3 && mesh->ndims != 4)) return 3;
+  if (mesh->ndims != 3 && mesh->ndims != 4) return 3;
+  if (mesh->kind == ORC_MESH_EXTRUDED && field->nd != 1) return 3;
   try {
     return field->dtype == ORC_F64 ? run_contour<double>(mesh, field, threshold, out, conn)
                                    : run_contour<float>(mesh, field, threshold, out, conn);

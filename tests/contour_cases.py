@@ -192,3 +192,49 @@ FIBER_SURFACE_CASES = {
     "fs_f32_offset": fs_f32_offset,
     "fs_near_quantum": fs_near_quantum,
 }
+
+
+# ---- level sets on ExtrudedSimplicialMesh(UnstructuredSimplicialMesh, L):
+# makers return a dict: coords, cells (base), n_layers, field (one value per
+# vertex id s + t * S), threshold, q.
+
+def ext_tri_2d():
+    """A triangulated 8x8 grid (jittered), 5 layers: 2D+t."""
+    from ftk2_b200 import synthetic as S
+    coords, _ = S.extruded_tet_mesh(8, 8, 2, seed=1)
+    coords = coords[:64]
+    nx = 8
+    i, j = np.meshgrid(np.arange(7), np.arange(7), indexing="xy")
+    p = (i + nx * j).ravel()
+    tris = np.sort(np.concatenate([np.stack([p, p + 1, p + nx + 1], 1),
+                                   np.stack([p, p + nx + 1, p + nx], 1)]), 1).astype(np.uint64)
+    L = 5
+    t = np.arange(L + 1)[:, None]
+    f = (np.sin(coords[None, :, 0] / 1.7) + np.cos(coords[None, :, 1] / 2.3) + 0.15 * t - 0.4).reshape(-1)
+    return dict(coords=coords, cells=tris, n_layers=L, field=np.ascontiguousarray(f), threshold=0.0, q=1e6)
+
+
+def ext_tet_3d():
+    """A jittered 7x6x4 tet mesh, 3 layers: 3D+t."""
+    from ftk2_b200 import synthetic as S
+    coords, tets = S.extruded_tet_mesh(7, 6, 4, seed=2)
+    L = 3
+    t = np.arange(L + 1)[:, None]
+    f = (np.sin(coords[None, :, 0] / 1.3) * np.cos(coords[None, :, 1] / 1.9) + 0.2 * coords[None, :, 2] - 0.3
+         + 0.1 * t).reshape(-1)
+    return dict(coords=coords, cells=tets, n_layers=L, field=np.ascontiguousarray(f), threshold=0.0, q=1e6)
+
+
+def ext_tri_ties_f32():
+    """Integer values on the 2D+t grid, float32: parity ties everywhere."""
+    c = ext_tri_2d()
+    rng = np.random.default_rng(9)
+    c["field"] = rng.integers(-1, 2, c["field"].shape).astype(np.float32)
+    return c
+
+
+EXTRUDED_CASES = {
+    "ext_tri_2d": ext_tri_2d,
+    "ext_tet_3d": ext_tet_3d,
+    "ext_tri_ties_f32": ext_tri_ties_f32,
+}

@@ -1,5 +1,5 @@
 """Generate tests/golden/contour/*.npz, tests/golden/fiber/*.npz and
-tests/golden/fiber_surface/*.npz by running
+tests/golden/fiber_surface/*.npz and tests/golden/contour_extruded/*.npz by running
 the reference's own CPU engine with ContourPredicate<T> (one worker thread,
 oracle/_ref/libftk2ref1t.so) and FiberPredicate<T> (oracle/_ref/libftk2ref.so),
 built from the reference headers by oracle/Makefile, on the seeded inputs of
@@ -71,6 +71,27 @@ def main_fiber(names=None):
               f"{len(res['edges'])} edges, reference {dt:.1f}s")
 
 
+def main_extruded(names=None):
+    out_dir = os.path.join(HERE, "contour_extruded")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, make in contour_cases.EXTRUDED_CASES.items():
+        if names and name not in names:
+            continue
+        case = make()
+        keep: list = []
+        mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+        fld = bridge.make_field([case["field"]], bridge.LAYOUT_SEPARATE, 1, sos_q=case["q"], keep=keep)
+        t = time.time()
+        r, cells = bridge.run_reference_contour(mesh, fld, case["threshold"])
+        dt = time.time() - t
+        rec = {"input_sha256": np.array(digest(case["field"])), "reference_seconds": np.array(dt),
+               "simplices": r.simplices, "bary": r.bary, "lam": r.lam, "track_id": r.track_id,
+               "scalar": r.scalar, "cells": cells}
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **rec)
+        print(f"{name}: {len(r.track_id)} features, {len(set(r.track_id.tolist()))} tracks, "
+              f"{len(cells)} cells, reference {dt:.1f}s")
+
+
 def main_fiber_surface(names=None):
     out_dir = os.path.join(HERE, "fiber_surface")
     os.makedirs(out_dir, exist_ok=True)
@@ -117,3 +138,4 @@ if __name__ == "__main__":
     main(sys.argv[1:])
     main_fiber(sys.argv[1:])
     main_fiber_surface(sys.argv[1:])
+    main_extruded(sys.argv[1:])

@@ -171,3 +171,21 @@ def test_contour_cpp_dropin_matches_restatement(tmp_path, name):
     assert np.array_equal(np.array([t for _, _, t, _ in feats], dtype=np.uint64), want["track_id"])
     assert np.array_equal(np.array([s for _, _, _, s in feats], dtype=np.uint32), want["scalar"].view(np.uint32))
     assert np.array_equal(np.array(cells, dtype=np.uint32).reshape(-1, want["cells"].shape[1]), want["cells"])
+
+
+EXT_GOLD = os.path.join(os.path.dirname(__file__), "golden", "contour_extruded")
+
+
+@pytest.mark.parametrize("name", list(contour_cases.EXTRUDED_CASES))
+def test_contour_extruded_matches_reference_fixture(ctx, name):
+    """Level sets on ExtrudedSimplicialMesh(UnstructuredSimplicialMesh, L):
+    edge features (spatial, vertical, prism diagonals), barycentrics, tracks
+    and manifold cells identical to the reference engine's."""
+    case = contour_cases.EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(EXT_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh = api.extruded_mesh_desc(case["coords"].shape[0], case["cells"], case["n_layers"], keep)
+    r = ctx.contour(mesh, api.field_desc([case["field"]], api.LAYOUT_SEPARATE, 1, keep=keep), case["threshold"],
+                    case["q"])
+    assert_same(as_dict(r), {k: g[k] for k in ("simplices", "bary", "lam", "track_id", "scalar", "cells")}, name)
+    assert r.n_tracks == len(set(r.track_id.tolist()))

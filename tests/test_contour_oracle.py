@@ -138,3 +138,26 @@ def test_fiber_surface_reference_reproduces_fixtures(name):
 def test_fiber_surface_fixture_exercises_the_centroid_fallback():
     g = np.load(os.path.join(FS_GOLD, "fs_near_quantum.npz"))
     assert (g["lam"] == np.float64(1.0) / 3.0).all(axis=1).sum() > 10
+
+
+EXT_GOLD = os.path.join(os.path.dirname(__file__), "golden", "contour_extruded")
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name", list(contour_cases.EXTRUDED_CASES))
+def test_extruded_level_set_reference_reproduces_fixtures(name):
+    """Level sets on ExtrudedSimplicialMesh: the fixtures are the one-worker
+    reference engine's output (its patching numbers the prism diagonals in the
+    order it meets them)."""
+    case = contour_cases.EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(EXT_GOLD, f"{name}.npz"))
+    assert digest(case["field"]) == str(g["input_sha256"])
+    keep: list = []
+    mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+    fld = bridge.make_field([case["field"]], bridge.LAYOUT_SEPARATE, 1, sos_q=case["q"], keep=keep)
+    r, cells = bridge.run_reference_contour(mesh, fld, case["threshold"])
+    assert len(r.track_id) > 0
+    assert np.array_equal(r.simplices, g["simplices"])
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
+    assert np.array_equal(r.track_id, g["track_id"])
+    assert np.array_equal(cells, g["cells"])
