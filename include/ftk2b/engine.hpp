@@ -483,7 +483,8 @@ struct ContourPredicate {
   T threshold = (T)0.0;
 };
 
-// SimplicialEngine<T, ContourPredicate<T>> on a regular mesh: execute runs
+// SimplicialEngine<T, ContourPredicate<T>> on a regular mesh or an extruded
+// mesh over an unstructured base (one value per vertex id): execute runs
 // ftk2b_contour_extract on the scalar array (the predicate's var_name, or the
 // first name passed); get_complex returns the edge features in simplex order
 // and the manifold cells (dimension 2 on 2D+t meshes, 3 on 3D+t meshes) as
@@ -506,7 +507,13 @@ class SimplicialEngine<T, ContourPredicate<T>> {
     const std::string& name = vars.empty() ? pred_.var_name : vars[0];
     const Array& a = data.at(name);
     ftk2b_mesh_desc md = mesh_->desc();
-    if (md.kind != FTK2B_MESH_REGULAR) throw Error(FTK2B_UNSUPPORTED, "level sets need a regular mesh");
+    if (md.kind == FTK2B_MESH_EXTRUDED) {
+      // extruded meshes over unstructured bases, one value per vertex id; a
+      // regular base's vertex ids leave gaps that carry no vertex
+      const auto* ext = dynamic_cast<const ExtrudedSimplicialMesh*>(mesh_.get());
+      if (!ext || ext->regular_base())
+        throw Error(FTK2B_UNSUPPORTED, "level sets on extruded meshes need an unstructured base");
+    }
     using E = std::remove_cv_t<std::remove_pointer_t<decltype(a.pdata())>>;
     std::vector<T> conv;
     const void* p = a.pdata();
@@ -523,6 +530,10 @@ class SimplicialEngine<T, ContourPredicate<T>> {
     fd.comp[0] = p;
     fd.nd = (int)a.nd();
     for (int i = 0; i < fd.nd && i < 4; ++i) fd.dims[i] = a.dimf(i);
+    if (md.kind == FTK2B_MESH_EXTRUDED) {
+      fd.nd = 1;
+      fd.dims[0] = a.nelem();
+    }
     ftk2b_contour_result* r = nullptr;
     ftk2b_status st = ftk2b_contour_extract(ctx_.get(), &md, &fd, (double)pred_.threshold, pred_.sos_q, &r);
     if (st != FTK2B_OK) throw Error(st, ftk2b_last_error(ctx_.get()));
