@@ -1,6 +1,6 @@
 """Restatement of the reference's level-set path in numpy (TEST INFRASTRUCTURE
 ONLY: tests/ and the smoke check import it as a checker; the product never
-does).
+does).  contour() covers regular meshes, contour_extruded() extruded ones.
 
 SimplicialEngine<T, ContourPredicate<T>> on a RegularSimplicialMesh, execute()
 then get_complex():
@@ -281,3 +281,146 @@ _POP16 = np.array([bin(i).count("1") for i in range(1 << 16)], dtype=np.int64)
 def _popcount(a: np.ndarray) -> np.ndarray:
     """Set bits of direction masks (below 2^15)."""
     return _POP16[np.asarray(a, dtype=np.int64)]
+
+
+def contour_extruded(field: np.ndarray, cells, n_base_verts: int, n_layers: int, threshold: float,
+                     q: float = 1e6):
+    """Level sets on ExtrudedSimplicialMesh(UnstructuredSimplicialMesh, L)
+    (mesh.hpp:542-599): field holds one value per vertex id s + t * S.
+
+    The mesh's edges are the spatial edges of every layer, the vertical edges
+    and the prism diagonals (v_a at t, v_b at t + 1, a < b: the Kuhn split of a
+    prism over a sorted base cell); the reference's first pass visits the
+    spatial and vertical ones, its patching meets the diagonals while visiting
+    the cells by layer, base cell (stored order, each sorted) and Kuhn index j
+    (vertices v_0..v_j at t, v_j..v_k at t + 1).  Same output layout as
+    contour()."""
+    T = field.dtype.type
+    S, L = int(n_base_verts), int(n_layers)
+    nv = S * (L + 1)
+    cells = np.sort(np.asarray(cells, dtype=np.int64), axis=1)
+    d = cells.shape[1]  # spacetime dims (base cell has d vertices)
+    adj = (field[:nv] - T(threshold)).astype(T)
+    pos = sos_positive(adj, np.arange(nv, dtype=np.uint64), q)
+    pairs = np.unique(np.concatenate([cells[:, [i, j]] for i in range(d) for j in range(i + 1, d)]), axis=0)
+    cand = []
+    for t in range(L + 1):
+        cand.append(np.stack([pairs[:, 0] + t * S, pairs[:, 1] + t * S], 1))
+    for t in range(L):
+        s = np.arange(S, dtype=np.int64)
+        cand.append(np.stack([s + t * S, s + (t + 1) * S], 1))
+        cand.append(np.stack([pairs[:, 0] + t * S, pairs[:, 1] + (t + 1) * S], 1))
+    cand = np.concatenate(cand)
+    cand = cand[pos[cand[:, 0]] != pos[cand[:, 1]]]
+    order = np.lexsort((cand[:, 1], cand[:, 0]))
+    edges = cand[order]
+    n = len(edges)
+    key = edges[:, 0] * nv + edges[:, 1]
+
+    def node(x, y):
+        lo, hi = np.minimum(x, y), np.maximum(x, y)
+        return np.searchsorted(key, lo * nv + hi)
+
+    a0, a1 = adj[edges[:, 0]], adj[edges[:, 1]]
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        dd = (a0 - a1).astype(T)
+        l0 = (-a1 / dd).astype(T)
+        l1 = (T(1.0) - l0).astype(T)
+    eps = T(1e-9)
+    ok = (np.abs(dd) >= T(1e-12)) & (l0 >= -eps) & (l0 <= T(1.0) + eps)
+    l0 = np.where(ok, l0, T(0.5)).astype(T)
+    l1 = np.where(ok, l1, T(0.5)).astype(T)
+
+    # spacetime cells in the reference's visiting order
+    nc = len(cells)
+    verts = []
+    for t in range(L):
+        for j in range(d):
+            v = np.concatenate([cells[:, :j + 1] + t * S, cells[:, j:] + (t + 1) * S], axis=1)
+            verts.append((t, j, v))
+    vlist = np.zeros((L * nc * d, d + 1), dtype=np.int64)
+    for t, j, v in verts:
+        idx = (t * nc + np.arange(nc)) * d + j
+        vlist[idx] = v
+    ps = pos[vlist]
+    npos = ps.sum(axis=1)
+    qidx = np.arange(len(vlist), dtype=np.int64)
+
+    def late(x, y):
+        return (y >= (x // S + 1) * S) & (y != x + S)
+
+    order_key = np.arange(n, dtype=np.int64)
+    if d == 3 and n:
+        first = np.full(n, np.iinfo(np.int64).max, dtype=np.int64)
+        for lone in range(4):
+            for single_pos in (True, False):
+                s2 = (npos == (1 if single_pos else 3)) & (ps[:, lone] == single_pos)
+                for k_, o in enumerate(o for o in range(4) if o != lone):
+                    i, j = min(lone, o), max(lone, o)
+                    x, y = vlist[s2, i], vlist[s2, j]
+                    lt = late(x, y)
+                    np.minimum.at(first, node(x, y)[lt], (qidx[s2] * 4 + k_)[lt])
+        for A in itertools.combinations(range(4), 2):
+            B = [i for i in range(4) if i not in A]
+            s2 = (npos == 2) & ps[:, A[0]] & ps[:, A[1]]
+            for k_, (a, b) in enumerate((a, b) for a in A for b in B):
+                i, j = min(a, b), max(a, b)
+                x, y = vlist[s2, i], vlist[s2, j]
+                lt = late(x, y)
+                np.minimum.at(first, node(x, y)[lt], (qidx[s2] * 4 + k_)[lt])
+        met = first != np.iinfo(np.int64).max
+        order_key = np.where(met, n + first, order_key)
+
+    def nd(i, j, sel):
+        return node(vlist[sel, min(i, j)], vlist[sel, max(i, j)])
+
+    out = []
+    nvtx = d + 1
+    for single_pos in (True, False):
+        sel = npos == (1 if single_pos else d)
+        for lone in range(nvtx):
+            s2 = sel & (ps[:, lone] == single_pos)
+            if not s2.any():
+                continue
+            c = [nd(lone, o, s2) for o in range(nvtx) if o != lone]
+            out.append(np.sort(np.stack(c, axis=1), axis=1))
+    if d == 3:
+        for A in itertools.combinations(range(4), 2):
+            B = [i for i in range(4) if i not in A]
+            s2 = (npos == 2) & ps[:, A[0]] & ps[:, A[1]]
+            if not s2.any():
+                continue
+            q4 = np.stack([nd(a, b, s2) for a in A for b in B], axis=1)
+            q4 = np.take_along_axis(q4, np.argsort(order_key[q4], axis=1), axis=1)
+            out.append(np.sort(q4[:, [0, 1, 2]], axis=1))
+            out.append(np.sort(q4[:, [0, 2, 3]], axis=1))
+    else:
+        for two_pos in (True, False):
+            sel = npos == (2 if two_pos else 3)
+            for two in itertools.combinations(range(5), 2):
+                three = [i for i in range(5) if i not in two]
+                s2 = sel & (ps[:, two[0]] == two_pos) & (ps[:, two[1]] == two_pos)
+                if not s2.any():
+                    continue
+                T0 = [nd(two[0], t, s2) for t in three]
+                T1 = [nd(two[1], t, s2) for t in three]
+                for c in ((T0[0], T0[1], T0[2], T1[2]), (T0[0], T0[1], T1[1], T1[2]),
+                          (T0[0], T1[0], T1[1], T1[2])):
+                    out.append(np.sort(np.stack(c, axis=1), axis=1))
+    cells_out = np.unique(np.concatenate(out), axis=0).astype(np.uint32) if out else np.zeros((0, d), np.uint32)
+
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    k = cells_out.shape[1]
+    ua = np.repeat(cells_out[:, 0].astype(np.int64), k - 1)
+    ub = cells_out[:, 1:].reshape(-1).astype(np.int64)
+    g = coo_matrix((np.ones(ua.size, dtype=np.int8), (ua, ub)), shape=(n, n))
+    _, label = connected_components(g, directed=False)
+    root = np.full(label.max() + 1 if n else 0, n, dtype=np.int64)
+    np.minimum.at(root, label, np.arange(n, dtype=np.int64))
+    track = root[label].astype(np.uint64)
+    return {"simplices": edges.astype(np.uint64),
+            "lam": np.stack([l0.astype(np.float64), l1.astype(np.float64)], axis=1),
+            "bary": np.stack([l0.astype(np.float32), l1.astype(np.float32)], axis=1),
+            "track_id": track, "scalar": np.full(n, np.float32(T(threshold)), dtype=np.float32),
+            "cells": cells_out}

@@ -161,3 +161,15 @@ def test_extruded_level_set_reference_reproduces_fixtures(name):
     assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
     assert np.array_equal(r.track_id, g["track_id"])
     assert np.array_equal(cells, g["cells"])
+
+
+@pytest.mark.parametrize("name", list(contour_cases.EXTRUDED_CASES))
+def test_extruded_restatement_matches_reference_fixtures(name):
+    case = contour_cases.EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(EXT_GOLD, f"{name}.npz"))
+    res = co.contour_extruded(case["field"], case["cells"], case["coords"].shape[0], case["n_layers"],
+                              case["threshold"], case["q"])
+    for k in ("simplices", "track_id", "cells"):
+        assert np.array_equal(res[k], g[k]), (name, k)
+    assert np.array_equal(res["bary"].view(np.uint32), g["bary"].view(np.uint32))
+    assert np.array_equal(res["lam"].view(np.uint64), g["lam"].view(np.uint64))
