@@ -957,8 +957,8 @@ extern "C" ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_des
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field || !thresholds || !out) return fail(ctx, FTK2B_INVALID_ARG, "null argument");
   *out = nullptr;
-  if (mesh->kind != FTK2B_MESH_REGULAR || mesh->ndims != 3)
-    return fail(ctx, FTK2B_UNSUPPORTED, "fiber extraction runs on regular 2D+t meshes (ndims 3)");
+  if (mesh->ndims != 3 || (mesh->kind != FTK2B_MESH_REGULAR && mesh->kind != FTK2B_MESH_EXTRUDED))
+    return fail(ctx, FTK2B_UNSUPPORTED, "fibers run on 2D+t meshes (regular, or extruded over triangles)");
   if (field->ncomp != 2) return fail(ctx, FTK2B_INVALID_ARG, "fibers read two scalar fields (ncomp 2)");
   if (field->scalar) return fail(ctx, FTK2B_INVALID_ARG, "fibers interpolate no scalar");
   if (!(sos_q > 0)) return fail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
@@ -968,7 +968,8 @@ extern "C" ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_des
   prm.precision = FTK2B_PRECISION_EXACT;
   prm.classify = 0;
   prm.want_edges = 1;
-  const ftk2b_status st = run_regular(ctx, mesh, field, &prm, thresholds);
+  const ftk2b_status st = mesh->kind == FTK2B_MESH_REGULAR ? run_regular(ctx, mesh, field, &prm, thresholds)
+                                                          : run_extruded(ctx, mesh, field, &prm, thresholds);
   if (st) return st;
   return ftk2b_cp_fetch(ctx, out);
 }

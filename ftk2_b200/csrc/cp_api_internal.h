@@ -243,6 +243,8 @@ cudaError_t resolve_cull_mode(ftk2b_ctx* ctx, const RegularMesh& rm, const Field
 }  // namespace ftk2b
 
 // extruded meshes (cp_extruded.cu)
+// fiber_thr: null for CriticalPointPredicate; the two thresholds for
+// FiberPredicate (triangle bases)
 ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
-                          const ftk2b_cp_params* prm);
+                          const ftk2b_cp_params* prm, const double* fiber_thr = nullptr);
 uint64_t extruded_simplex_count(const ftk2b_mesh_desc* mesh, int m);

@@ -219,13 +219,21 @@ __device__ __forceinline__ bool ext_test(const FieldAccess& fa, const ExtractCon
 #pragma unroll
   for (int i = 0; i <= M; ++i)
 #pragma unroll
-    for (int j = 0; j < M; ++j) vals[i][j] = static_cast<const T*>(fa.comp[j])[sidx[i]];
+    for (int j = 0; j < M; ++j) {
+      vals[i][j] = static_cast<const T*>(fa.comp[j])[sidx[i]];
+      if (cfg.fiber) vals[i][j] = fp<T>::sub(vals[i][j], (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
+    }
   bool inside;
   if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
   else inside = sos_inside3<T>(vals, cfg.Q);
   if (!inside) return false;
   T lam[M + 1];
-  if (!solve_exact<M, T>(vals, lam)) return false;
+  if (!solve_exact<M, T>(vals, lam)) {
+    if (!cfg.fiber) return false;
+    // FiberPredicate keeps the simplex at the centroid: (T)1.0 / 3.0
+#pragma unroll
+    for (int i = 0; i <= M; ++i) lam[i] = (T)((double)(T)1.0 / 3.0);
+  }
 #pragma unroll
   for (int i = 0; i <= M; ++i) {
     lam_out[i] = (double)lam[i];
@@ -344,7 +352,9 @@ __global__ void __launch_bounds__(kThreadsX) ext_extract_kernel(ExtMeshDev X, Fi
       double lam_out[4] = {0, 0, 0, 0};
       float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
       float sc_out = 0.f;
-      if (live && !word_culled(wacc)) acc = ext_test<T, M>(fa, cfg, sidx, lam_out, bary_out, sc_out);
+      // the cull words assume an accepted simplex has a successful solve,
+      // which fibers do not require
+      if (live && (cfg.fiber || !word_culled(wacc))) acc = ext_test<T, M>(fa, cfg, sidx, lam_out, bary_out, sc_out);
       const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
       if (ball) {
         unsigned basei = 0;
@@ -1194,7 +1204,7 @@ uint64_t extruded_simplex_count(const ftk2b_mesh_desc* mesh, int m) {
 }
 
 ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
-                          const ftk2b_cp_params* prm) {
+                          const ftk2b_cp_params* prm, const double* fiber_thr) {
   int fbits = 0;
   ftk2b_status st = validate_mesh(ctx, mesh, &fbits);
   if (st) return st;
@@ -1243,6 +1253,12 @@ ftk2b_status run_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk
   memset(&cfg, 0, sizeof(cfg));
   cfg.Q = prm->sos_q;
   cfg.refined = prm->precision == FTK2B_PRECISION_REFINED;
+  if (fiber_thr) {  // FiberPredicate: every simplex tested, values minus thresholds
+    cfg.fiber = 1;
+    cfg.fthr[0] = fiber_thr[0];
+    cfg.fthr[1] = fiber_thr[1];
+    cfg.refined = 0;
+  }
   const int f64 = field->dtype == FTK2B_F64;
   EXT_TRY(C.words.ensure(sizeof(unsigned) * nv));
 

@@ -386,7 +386,8 @@ void ftk2b_contour_result_free(ftk2b_contour_result* r);
 /* --- fibers (FiberPredicate<T>) --------------------------------------------
  * Replaces SimplicialEngine<T, FiberPredicate<T>>::execute + get_complex
  * (predicate.hpp:341-362; form_general_manifold_patches engine.hpp:1341-1418)
- * on a regular 2D+t mesh (ndims 3): features are the triangles where both
+ * on a 2D+t mesh (ndims 3: regular, or extruded over triangles with
+ * per-vertex fields): features are the triangles where both
  * fields minus their thresholds vanish (simulation of simplicity), kept at the
  * centroid where the barycentric solve fails; edges join each top cell's
  * features to its star centre.  field: ncomp 2 (SEPARATE, MULTICOMPONENT or

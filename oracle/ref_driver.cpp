@@ -320,12 +320,23 @@ int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, o
               orc_conn* conn = nullptr) {
   using namespace ftk2;
   std::vector<uint64_t> dims, off, glob;
-  for (int i = 0; i < mesh->ndims; ++i) {
-    dims.push_back(mesh->local_dims[i]);
-    off.push_back(mesh->offset[i]);
-    glob.push_back(mesh->global_dims[i]);
+  std::shared_ptr<Mesh> mesh_ptr;
+  std::shared_ptr<RegularSimplicialMesh> reg;
+  if (mesh->kind == ORC_MESH_REGULAR) {
+    for (int i = 0; i < mesh->ndims; ++i) {
+      dims.push_back(mesh->local_dims[i]);
+      off.push_back(mesh->offset[i]);
+      glob.push_back(mesh->global_dims[i]);
+    }
+    reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
+    mesh_ptr = reg;
+  } else {
+    std::vector<double> coords(mesh->base_coords, mesh->base_coords + 3 * mesh->n_base_verts);
+    size_t nc = (size_t)mesh->n_base_cells * (mesh->base_cell_dim + 1);
+    std::vector<uint64_t> cells(mesh->base_cells, mesh->base_cells + nc);
+    auto base = std::make_shared<UnstructuredSimplicialMesh>(mesh->base_cell_dim, mesh->base_cell_dim, coords, cells);
+    mesh_ptr = std::make_shared<ExtrudedSimplicialMesh>(base, mesh->n_layers);
   }
-  auto reg = std::make_shared<RegularSimplicialMesh>(dims, off, glob);
   FiberPredicate<T> pred;
   pred.var_names[0] = "F";
   pred.var_names[1] = "G";
@@ -335,7 +346,7 @@ int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, o
   std::map<std::string, ftk::ndarray<T>> data;
   data["F"] = make_array<T>(field->comp[0], field->nd, field->dims);
   data["G"] = make_array<T>(field->comp[1], field->nd, field->dims);
-  SimplicialEngine<T, FiberPredicate<T>> engine(reg, pred);
+  SimplicialEngine<T, FiberPredicate<T>> engine(mesh_ptr, pred);
   std::streambuf* saved = std::cout.rdbuf();
   std::ostringstream sink;
   std::cout.rdbuf(sink.rdbuf());
@@ -359,11 +370,16 @@ int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, o
     for (int v = 0; v < 3; ++v) {
       out->simplices[3 * i + v] = el.simplex.vertices[v];
       out->bary[3 * i + v] = el.barycentric_coords[0][v];
-      std::vector<double> c = reg->get_vertex_coordinates(el.simplex.vertices[v]);
-      for (size_t k = 0; k < c.size(); ++k) c[k] -= (double)off[k];
       for (int j = 0; j < 2; ++j) {
         const auto& a = data.at(j == 0 ? "F" : "G");
-        const T x = c.size() == 3 ? a.f(c[0], c[1], c[2]) : a.f(c[0], c[1], c[2], c[3]);
+        T x;
+        if (!reg || a.nd() == 1) {
+          x = a[el.simplex.vertices[v]];
+        } else {
+          std::vector<double> c = reg->get_vertex_coordinates(el.simplex.vertices[v]);
+          for (size_t k = 0; k < c.size(); ++k) c[k] -= (double)off[k];
+          x = c.size() == 3 ? a.f(c[0], c[1], c[2]) : a.f(c[0], c[1], c[2], c[3]);
+        }
         values[v][j] = (T)(x - pred.thresholds[j]);
       }
     }
@@ -413,7 +429,8 @@ extern "C" int ftk2ref_run_fiber_surface(const orc_mesh* mesh, const orc_field* 
 extern "C" int ftk2ref_run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thresholds,
                                  orc_result* out) {
   std::memset(out, 0, sizeof(*out));
-  if (mesh->kind != ORC_MESH_REGULAR || mesh->ndims != 3 || field->layout != ORC_LAYOUT_SEPARATE) return 3;
+  if (mesh->ndims != 3 || field->layout != ORC_LAYOUT_SEPARATE) return 3;
+  if (mesh->kind == ORC_MESH_EXTRUDED && field->nd != 1) return 3;
   try {
     return field->dtype == ORC_F64 ? run_fiber<double>(mesh, field, thresholds, out)
                                    : run_fiber<float>(mesh, field, thresholds, out);

@@ -238,3 +238,29 @@ EXTRUDED_CASES = {
     "ext_tet_3d": ext_tet_3d,
     "ext_tri_ties_f32": ext_tri_ties_f32,
 }
+
+
+# ---- fibers on extruded 2D+t meshes (two per-vertex fields)
+
+def fiber_ext_tri():
+    c = ext_tri_2d()
+    coords, L = c["coords"], c["n_layers"]
+    t = np.arange(L + 1)[:, None]
+    f = (np.sin(coords[None, :, 0] / 1.7) + 0.1 * t - 0.2).reshape(-1)
+    g = (np.cos(coords[None, :, 1] / 2.1) - 0.15 * t + 0.1).reshape(-1)
+    return dict(coords=coords, cells=c["cells"], n_layers=L, fields=(np.ascontiguousarray(f), np.ascontiguousarray(g)),
+                thresholds=(0.0, 0.0), q=1e6)
+
+
+def fiber_ext_near_quantum():
+    c = ext_tri_2d()
+    rng = np.random.default_rng(12)
+    n = c["field"].size
+    return dict(coords=c["coords"], cells=c["cells"], n_layers=c["n_layers"],
+                fields=(rng.uniform(-3e-6, 3e-6, n), rng.uniform(-3e-6, 3e-6, n)), thresholds=(0.0, 0.0), q=1e6)
+
+
+FIBER_EXTRUDED_CASES = {
+    "fiber_ext_tri": fiber_ext_tri,
+    "fiber_ext_near_quantum": fiber_ext_near_quantum,
+}

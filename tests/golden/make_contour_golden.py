@@ -1,5 +1,6 @@
 """Generate tests/golden/contour/*.npz, tests/golden/fiber/*.npz and
-tests/golden/fiber_surface/*.npz and tests/golden/contour_extruded/*.npz by running
+tests/golden/fiber_surface/*.npz, tests/golden/contour_extruded/*.npz and
+tests/golden/fiber_extruded/*.npz by running
 the reference's own CPU engine with ContourPredicate<T> (one worker thread,
 oracle/_ref/libftk2ref1t.so) and FiberPredicate<T> (oracle/_ref/libftk2ref.so),
 built from the reference headers by oracle/Makefile, on the seeded inputs of
@@ -92,6 +93,27 @@ def main_extruded(names=None):
               f"{len(cells)} cells, reference {dt:.1f}s")
 
 
+def main_fiber_extruded(names=None):
+    out_dir = os.path.join(HERE, "fiber_extruded")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, make in contour_cases.FIBER_EXTRUDED_CASES.items():
+        if names and name not in names:
+            continue
+        case = make()
+        keep: list = []
+        mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+        fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+        t = time.time()
+        r = bridge.run_reference_fiber(mesh, fld, case["thresholds"])
+        dt = time.time() - t
+        rec = {"input_sha256": np.array(digest(np.concatenate([a.reshape(-1) for a in case["fields"]]))),
+               "reference_seconds": np.array(dt), "simplices": r.simplices, "bary": r.bary, "lam": r.lam,
+               "track_id": r.track_id, "scalar": r.scalar, "edges": r.edges}
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **rec)
+        print(f"{name}: {len(r.track_id)} features, {len(set(r.track_id.tolist()))} tracks, "
+              f"{len(r.edges)} edges, reference {dt:.1f}s")
+
+
 def main_fiber_surface(names=None):
     out_dir = os.path.join(HERE, "fiber_surface")
     os.makedirs(out_dir, exist_ok=True)
@@ -139,3 +161,4 @@ if __name__ == "__main__":
     main_fiber(sys.argv[1:])
     main_fiber_surface(sys.argv[1:])
     main_extruded(sys.argv[1:])
+    main_fiber_extruded(sys.argv[1:])

@@ -173,3 +173,22 @@ def test_extruded_restatement_matches_reference_fixtures(name):
         assert np.array_equal(res[k], g[k]), (name, k)
     assert np.array_equal(res["bary"].view(np.uint32), g["bary"].view(np.uint32))
     assert np.array_equal(res["lam"].view(np.uint64), g["lam"].view(np.uint64))
+
+
+FIBER_EXT_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber_extruded")
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_EXTRUDED_CASES))
+def test_extruded_fiber_reference_reproduces_fixtures(name):
+    case = contour_cases.FIBER_EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(FIBER_EXT_GOLD, f"{name}.npz"))
+    keep: list = []
+    r = bridge.run_reference_fiber(bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep),
+                                   bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"],
+                                                     keep=keep), case["thresholds"])
+    assert len(r.track_id) > 0
+    assert np.array_equal(r.simplices, g["simplices"])
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
+    assert np.array_equal(r.track_id, g["track_id"])
+    assert np.array_equal(r.edges, g["edges"])

@@ -154,3 +154,21 @@ def test_fiber_cpp_dropin_matches_reference_fixture(tmp_path, name, gold, conn):
     assert np.array_equal(np.array([t for _, _, t in feats], dtype=np.uint64), g["track_id"])
     want = g[conn]
     assert np.array_equal(np.array(rows, dtype=np.uint32).reshape(-1, want.shape[1]), want)
+
+
+FIBER_EXT_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber_extruded")
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_EXTRUDED_CASES))
+def test_fiber_extruded_matches_reference_fixture(ctx, name):
+    """Fibers on ExtrudedSimplicialMesh over triangles (the extruded pipeline's
+    fiber mode): features, barycentrics (centroid where the solve fails),
+    tracks and star edges identical to the reference engine's."""
+    case = contour_cases.FIBER_EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(FIBER_EXT_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh = api.extruded_mesh_desc(case["coords"].shape[0], case["cells"], case["n_layers"], keep)
+    fd = api.field_desc(list(case["fields"]), api.LAYOUT_PER_VERTEX, 2, keep=keep)
+    r = ctx.fiber(mesh, fd, case["thresholds"], case["q"])
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    assert_same(r, {k: g[k] for k in ("simplices", "bary", "lam", "track_id", "edges")}, name)
