@@ -808,14 +808,33 @@ class CriticalPointPredicate:
     classify: bool = False
 
 
-class SimplicialEngine:
-    """SimplicialEngine<T, CriticalPointPredicate<M,T>> (engine.hpp:79-996) on the GPU."""
+@dataclass
+class ContourPredicate:
+    """ContourPredicate<T> knobs (predicate.hpp:135-183): level sets of one
+    scalar field."""
+    var_name: str = ""
+    threshold: float = 0.0
+    sos_q: float = 1e6
 
-    def __init__(self, mesh, pred: CriticalPointPredicate, ctx: Optional[Context] = None):
+
+@dataclass
+class FiberPredicate:
+    """FiberPredicate<T> knobs (predicate.hpp:341-362): fibers of two scalar
+    fields (points of 2D+t meshes, surfaces of 3D+t meshes)."""
+    var_names: list = field(default_factory=lambda: ["", ""])
+    thresholds: tuple = (0.0, 0.0)
+    sos_q: float = 1e6
+
+
+class SimplicialEngine:
+    """SimplicialEngine<T, Predicate> (engine.hpp:79-996) on the GPU, for
+    CriticalPointPredicate, ContourPredicate and FiberPredicate."""
+
+    def __init__(self, mesh, pred, ctx: Optional[Context] = None):
         self.mesh = mesh
         self.pred = pred
         self.ctx = ctx or Context(0)
-        self._result: Optional[CPResult] = None
+        self._result = None
 
     def _field(self, data: dict, keep: list) -> FieldDesc:
         p = self.pred
@@ -829,13 +848,30 @@ class SimplicialEngine:
     def execute(self, data: dict, var_names=None):
         keep: list = []
         mesh = self.mesh.desc(keep)
+        p = self.pred
+        if isinstance(p, ContourPredicate):
+            name = var_names[0] if var_names else p.var_name
+            fld = field_desc([data[name]], LAYOUT_SEPARATE, 1, keep=keep)
+            self._result = self.ctx.contour(mesh, fld, p.threshold, p.sos_q)
+            return
+        if isinstance(p, FiberPredicate):
+            names = list(var_names[:2]) if var_names and len(var_names) >= 2 else list(p.var_names[:2])
+            layout = LAYOUT_PER_VERTEX if isinstance(self.mesh, ExtrudedSimplicialMesh) else LAYOUT_SEPARATE
+            fld = field_desc([data[n] for n in names], layout, 2, keep=keep)
+            if self.mesh.get_total_dimension() == 4:
+                self._result = self.ctx.fiber_surface(mesh, fld, p.thresholds, p.sos_q)
+            else:
+                self._result = self.ctx.fiber(mesh, fld, p.thresholds, p.sos_q)
+            return
         fld = self._field(data, keep)
-        prm = params(self.pred.sos_q, self.pred.precision, True, self.pred.classify)
+        prm = params(p.sos_q, p.precision, True, p.classify)
         self._result = self.ctx.extract(mesh, fld, prm)
 
     execute_cuda = execute
 
-    def get_complex(self) -> CPResult:
+    def get_complex(self):
+        """CPResult (critical points, 2D+t fibers) or ContourResult (level
+        sets, fiber surfaces)."""
         if self._result is None:
             raise RuntimeError("execute() has not run")
         return self._result
