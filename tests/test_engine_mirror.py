@@ -1,10 +1,17 @@
 """The Python mirror of the reference's engine (ftk2_b200.api.SimplicialEngine)
 routes each predicate to its C-ABI entry point with the reference's variable
-and threshold semantics (predicate.hpp:22-64, 135-183, 341-362).  Host logic
-only: a recording stand-in for the context takes the calls."""
-import numpy as np
+and threshold semantics (predicate.hpp:50-128, 136-181, 341-387).  On the CPU a
+recording stand-in for the context takes the calls; the gpu-marked tests run
+the mirror on the device against the reference's fixtures."""
+import os
 
+import numpy as np
+import pytest
+
+import contour_cases
 from ftk2_b200 import api
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 class Recorder:
@@ -65,3 +72,87 @@ def test_critical_point_predicate_still_extracts():
     api.SimplicialEngine(api.RegularSimplicialMesh([6, 5, 4]),
                          api.CriticalPointPredicate(2, vector_var_name="v"), ctx=rec).execute({"v": v})
     assert rec.calls[0][0] == "extract" and rec.calls[0][4] == api.LAYOUT_MULTICOMPONENT
+
+
+# On the GPU: the mirror's results are the reference engine's fixtures (and,
+# for the regular level sets, whose fixtures hold digests, the restatement).
+
+
+def _same(r, g, keys):
+    for k in keys:
+        a, b = getattr(r, k), g[k]
+        if k in ("bary", "scalar"):
+            a, b = a.view(np.uint32), b.view(np.uint32)
+        elif k == "lam":
+            a, b = a.view(np.uint64), b.view(np.uint64)
+        elif k == "cells":
+            a, b = a.astype(np.uint32), b.astype(np.uint32)
+        assert np.array_equal(a, b), k
+
+
+def _regular(case):
+    return api.RegularSimplicialMesh(case["local_dims"], case["offset"], case["global_dims"])
+
+
+def _extruded(case):
+    cells = case["cells"]
+    base = api.UnstructuredSimplicialMesh(3, cells.shape[1] - 1, case["coords"], cells)
+    return api.ExtrudedSimplicialMesh(base, case["n_layers"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["gauss_2d_f64", "moving_sphere"])
+def test_gpu_contour_predicate_regular(ctx, name):
+    from oracle import contour_oracle as co
+    case = contour_cases.CASES[name]()
+    e = api.SimplicialEngine(_regular(case), api.ContourPredicate("s", case["threshold"], case["q"]), ctx=ctx)
+    e.execute({"s": case["field"]})
+    r = e.get_complex()
+    want = co.contour(case["field"], case["threshold"], case["local_dims"], case["offset"],
+                      case["global_dims"], case["q"])
+    assert len(r.track_id) > 0
+    for k in ("simplices", "track_id", "cells"):
+        assert np.array_equal(getattr(r, k).astype(want[k].dtype), want[k]), k
+    assert np.array_equal(r.lam.view(np.uint64), want["lam"].view(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(contour_cases.EXTRUDED_CASES))
+def test_gpu_contour_predicate_extruded(ctx, name):
+    case = contour_cases.EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(GOLDEN, "contour_extruded", f"{name}.npz"))
+    e = api.SimplicialEngine(_extruded(case), api.ContourPredicate("s", case["threshold"], case["q"]), ctx=ctx)
+    e.execute({"s": case["field"]})
+    r = e.get_complex()
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    _same(r, g, ("simplices", "bary", "lam", "track_id", "cells"))
+
+
+@pytest.mark.gpu
+def test_gpu_fiber_predicate_regular_and_extruded(ctx):
+    case = contour_cases.FIBER_CASES["fiber_gauss_f64"]()
+    g = np.load(os.path.join(GOLDEN, "fiber", "fiber_gauss_f64.npz"))
+    e = api.SimplicialEngine(_regular(case), api.FiberPredicate(["f", "g"], case["thresholds"], case["q"]), ctx=ctx)
+    e.execute({"f": case["fields"][0], "g": case["fields"][1]})
+    r = e.get_complex()
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    _same(r, g, ("simplices", "bary", "lam", "track_id", "edges"))
+
+    case = contour_cases.FIBER_EXTRUDED_CASES["fiber_ext_tri"]()
+    g = np.load(os.path.join(GOLDEN, "fiber_extruded", "fiber_ext_tri.npz"))
+    e = api.SimplicialEngine(_extruded(case), api.FiberPredicate(["f", "g"], case["thresholds"], case["q"]), ctx=ctx)
+    e.execute({"f": case["fields"][0], "g": case["fields"][1]})
+    r = e.get_complex()
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    _same(r, g, ("simplices", "bary", "lam", "track_id", "edges"))
+
+
+@pytest.mark.gpu
+def test_gpu_fiber_predicate_surfaces(ctx):
+    case = contour_cases.FIBER_SURFACE_CASES["fs_gauss_f64"]()
+    g = np.load(os.path.join(GOLDEN, "fiber_surface", "fs_gauss_f64.npz"))
+    e = api.SimplicialEngine(_regular(case), api.FiberPredicate(["f", "g"], case["thresholds"], case["q"]), ctx=ctx)
+    e.execute({"f": case["fields"][0], "g": case["fields"][1]})
+    r = e.get_complex()
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    _same(r, g, ("simplices", "bary", "lam", "track_id", "cells"))
