@@ -353,7 +353,8 @@ def _result_from_c(r: CPResultC) -> CPResult:
 class ContourResult:
     """Flattened FeatureComplex of a level-set (ContourPredicate) or
     fiber-surface (FiberPredicate on 3D+t) extraction: features are mesh
-    edges or triangles, cells the manifold cells of get_complex."""
+    edges or triangles, cells the manifold cells of get_complex.  The arrays
+    are views of the library's result memory, freed with the last of them."""
     simplices: np.ndarray      # (n, m+1) uint64 vertex ids, simplex order (m = 1 edges, 2 triangles)
     lam: np.ndarray            # (n, m+1) float64 barycentrics in the field precision
     bary: np.ndarray           # (n, m+1) float32 as FeatureElement stores them
@@ -365,21 +366,53 @@ class ContourResult:
     device_ms: float = 0.0
 
 
-def _contour_from_c(r: ContourResultC) -> ContourResult:
+class _CResultOwner:
+    """Owns one result the library allocated (its host arrays are plain heap
+    or huge-page memory, independent of the context) and frees it with the
+    library's free function once the last numpy view of it is gone.  Level
+    sets return gigabytes; the views spare the host a second copy."""
+
+    __slots__ = ("_free", "_ptr")
+
+    def __init__(self, free, ptr):
+        self._free, self._ptr = free, ptr
+
+    def __del__(self):
+        if self._ptr is not None and self._ptr:
+            self._free(self._ptr)
+        self._ptr = None
+
+
+def _view(owner: _CResultOwner, ptr, count: int, dt) -> np.ndarray:
+    """A writable numpy view of count elements at ptr that keeps owner alive."""
+    if count == 0 or not ptr:
+        return np.zeros(0, dtype=dt)
+    buf = (C.c_uint8 * (count * np.dtype(dt).itemsize)).from_address(C.cast(ptr, C.c_void_p).value)
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dt)
+
+
+def _contour_from_c(r: ContourResultC, owner: _CResultOwner) -> ContourResult:
     n, k, c = int(r.n_features), int(r.cell_dim) + 1, int(r.n_cells)
-
-    def arr(ptr, count, dt):
-        if count == 0:
-            return np.zeros(0, dtype=dt)
-        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
-
     return ContourResult(
-        simplices=arr(r.simplices, 2 * n, np.uint64).reshape(n, 2),
-        lam=arr(r.lambda_, 2 * n, np.float64).reshape(n, 2),
-        bary=arr(r.barycentric, 2 * n, np.float32).reshape(n, 2),
-        track_id=arr(r.track_id, n, np.uint64),
-        scalar=arr(r.scalar, n, np.float32),
-        cells=arr(r.cells, k * c, np.uint32).reshape(c, k),
+        simplices=_view(owner, r.simplices, 2 * n, np.uint64).reshape(n, 2),
+        lam=_view(owner, r.lambda_, 2 * n, np.float64).reshape(n, 2),
+        bary=_view(owner, r.barycentric, 2 * n, np.float32).reshape(n, 2),
+        track_id=_view(owner, r.track_id, n, np.uint64),
+        scalar=_view(owner, r.scalar, n, np.float32),
+        cells=_view(owner, r.cells, k * c, np.uint32).reshape(c, k),
+        n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
+
+
+def _fiber_surface_from_c(r: FiberSurfaceResultC, owner: _CResultOwner) -> ContourResult:
+    n, c = int(r.n_features), int(r.n_cells)
+    return ContourResult(
+        simplices=_view(owner, r.simplices, 3 * n, np.uint64).reshape(n, 3),
+        lam=_view(owner, r.lambda_, 3 * n, np.float64).reshape(n, 3),
+        bary=_view(owner, r.barycentric, 3 * n, np.float32).reshape(n, 3),
+        track_id=_view(owner, r.track_id, n, np.uint64),
+        scalar=_view(owner, r.scalar, n, np.float32),
+        cells=_view(owner, r.cells, 3 * c, np.uint32).reshape(c, 3),
         n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
 
 
@@ -451,10 +484,7 @@ class Context:
         out = C.POINTER(ContourResultC)()
         self._check(self.lib.ftk2b_contour_extract(self.h, C.byref(mesh), C.byref(field), float(threshold),
                                                    float(sos_q), C.byref(out)))
-        try:
-            return _contour_from_c(out.contents)
-        finally:
-            self.lib.ftk2b_contour_result_free(out)
+        return _contour_from_c(out.contents, _CResultOwner(self.lib.ftk2b_contour_result_free, out))
 
     def fiber(self, mesh: MeshDesc, field: FieldDesc, thresholds=(0.0, 0.0), sos_q: float = 1e6) -> CPResult:
         """Fibers (FiberPredicate<T>) of two scalar fields on a regular 2D+t
@@ -478,25 +508,7 @@ class Context:
         out = C.POINTER(FiberSurfaceResultC)()
         self._check(self.lib.ftk2b_fiber_surface_extract(self.h, C.byref(mesh), C.byref(field), thr,
                                                          float(sos_q), C.byref(out)))
-        try:
-            r = out.contents
-            n, c = int(r.n_features), int(r.n_cells)
-
-            def arr(ptr, count, dt):
-                if count == 0:
-                    return np.zeros(0, dtype=dt)
-                return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
-
-            return ContourResult(
-                simplices=arr(r.simplices, 3 * n, np.uint64).reshape(n, 3),
-                lam=arr(r.lambda_, 3 * n, np.float64).reshape(n, 3),
-                bary=arr(r.barycentric, 3 * n, np.float32).reshape(n, 3),
-                track_id=arr(r.track_id, n, np.uint64),
-                scalar=arr(r.scalar, n, np.float32),
-                cells=arr(r.cells, 3 * c, np.uint32).reshape(c, 3),
-                n_tracks=int(r.n_tracks), n_simplices=int(r.n_simplices), device_ms=float(r.device_ms))
-        finally:
-            self.lib.ftk2b_fiber_surface_result_free(out)
+        return _fiber_surface_from_c(out.contents, _CResultOwner(self.lib.ftk2b_fiber_surface_result_free, out))
 
     def run(self, mesh: MeshDesc, field: FieldDesc, prm: Optional[CPParams] = None):
         """Device pipeline only; results stay on the device until fetch()."""

@@ -156,3 +156,42 @@ def test_gpu_fiber_predicate_surfaces(ctx):
     r = e.get_complex()
     assert len(r.track_id) == len(g["track_id"]) > 0
     _same(r, g, ("simplices", "bary", "lam", "track_id", "cells"))
+
+
+def test_level_set_results_are_views_freed_after_the_last_one():
+    """Level-set and fiber-surface results are numpy views of the library's
+    result memory; the result is freed once, after the last view goes."""
+    import ctypes as C
+    import gc
+    n, c = 5, 3
+    simp = (C.c_uint64 * (2 * n))(*range(10, 20))
+    lam = (C.c_double * (2 * n))(*[i / 8 for i in range(2 * n)])
+    bary = (C.c_float * (2 * n))(*[i / 4 for i in range(2 * n)])
+    track = (C.c_uint64 * n)(0, 0, 2, 2, 4)
+    scal = (C.c_float * n)(*([0.5] * n))
+    cells = (C.c_uint32 * (3 * c))(*range(9))
+    r = api.ContourResultC(n_features=n, cell_dim=2, n_cells=c, n_tracks=3, n_simplices=77, device_ms=1.5)
+    r.simplices, r.lambda_, r.barycentric = simp, lam, bary
+    r.track_id, r.scalar, r.cells = track, scal, cells
+    freed = []
+    out = C.pointer(r)
+    res = api._contour_from_c(out.contents, api._CResultOwner(lambda p: freed.append(p.contents.n_features), out))
+    assert res.simplices.shape == (n, 2) and res.simplices[4].tolist() == [18, 19]
+    assert res.lam[1].tolist() == [0.25, 0.375] and res.bary.dtype == np.float32
+    assert res.track_id.tolist() == [0, 0, 2, 2, 4] and res.cells.shape == (c, 3) and res.cells[2, 2] == 8
+    assert (res.n_tracks, res.n_simplices, res.device_ms) == (3, 77, 1.5)
+    keep = res.cells[1:]
+    del res
+    gc.collect()
+    assert freed == []
+    assert keep.tolist() == [[3, 4, 5], [6, 7, 8]]
+    del keep
+    gc.collect()
+    assert freed == [n]
+
+    # nothing to view: freed at once, empty arrays of the right shapes
+    e = api.ContourResultC(n_features=0, cell_dim=1, n_cells=0)
+    out = C.pointer(e)
+    res = api._contour_from_c(out.contents, api._CResultOwner(lambda p: freed.append("empty"), out))
+    gc.collect()
+    assert freed[-1] == "empty" and res.simplices.shape == (0, 2) and res.cells.shape == (0, 2)
