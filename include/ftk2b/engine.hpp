@@ -48,7 +48,11 @@ class Error : public std::runtime_error {
 class Mesh {
  public:
   virtual ~Mesh() = default;
+  virtual int get_spatial_dimension() const = 0;
   virtual int get_total_dimension() const = 0;
+  // grid or physical coordinates of a vertex, time last on extruded meshes
+  // (mesh.hpp:374-378, 714-720; unstructured_mesh.hpp:100-107)
+  virtual std::vector<double> get_vertex_coordinates(uint64_t vertex_id) const = 0;
   virtual ftk2b_mesh_desc desc() const = 0;
 };
 
@@ -60,7 +64,17 @@ class RegularSimplicialMesh : public Mesh {
     if (offset_.empty()) offset_.assign(dims_.size(), 0);
     if (global_dims_.empty()) global_dims_ = dims_;
   }
+  int get_spatial_dimension() const override { return (int)dims_.size(); }
   int get_total_dimension() const override { return (int)dims_.size(); }
+  // the global grid index of the id, one coordinate per axis
+  std::vector<double> get_vertex_coordinates(uint64_t id) const override {
+    std::vector<double> c(global_dims_.size());
+    for (size_t i = 0; i < global_dims_.size(); ++i) {
+      c[i] = (double)(id % global_dims_[i]);
+      id /= global_dims_[i];
+    }
+    return c;
+  }
   const std::vector<uint64_t>& get_local_dims() const { return dims_; }
   const std::vector<uint64_t>& get_offset() const { return offset_; }
   const std::vector<uint64_t>& get_global_dims() const { return global_dims_; }
@@ -86,8 +100,16 @@ class UnstructuredSimplicialMesh : public Mesh {
   UnstructuredSimplicialMesh(int spatial_dim, int cell_dim, const std::vector<double>& coords,
                              const std::vector<uint64_t>& cells)
       : spatial_dim_(spatial_dim), cell_dim_(cell_dim), coords_(coords), cells_(cells) {}
+  int get_spatial_dimension() const override { return spatial_dim_; }
   int get_total_dimension() const override { return cell_dim_; }
+  // the first spatial_dim of the vertex's three stored coordinates; empty
+  // past the last vertex
+  std::vector<double> get_vertex_coordinates(uint64_t id) const override {
+    if (id >= get_num_vertices()) return {};
+    return std::vector<double>(coords_.begin() + 3 * id, coords_.begin() + 3 * id + spatial_dim_);
+  }
   uint64_t get_num_vertices() const { return coords_.size() / 3; }
+  const std::vector<double>& coords() const { return coords_; }
   int cell_dim() const { return cell_dim_; }
   const std::vector<uint64_t>& cells() const { return cells_; }
   ftk2b_mesh_desc desc() const override {
@@ -143,8 +165,20 @@ class ExtrudedSimplicialMesh : public Mesh {
             }
           }
   }
+  int get_spatial_dimension() const override {
+    return regular_ ? regular_->get_spatial_dimension() : base_->get_spatial_dimension();
+  }
   int get_total_dimension() const override {
     return (regular_ ? (int)regular_->get_global_dims().size() : base_->get_total_dimension()) + 1;
+  }
+  // the base vertex's coordinates, then the layer (vertex id s + t * S)
+  std::vector<double> get_vertex_coordinates(uint64_t id) const override {
+    const uint64_t S = regular_ ? stride_ : base_->get_num_vertices();
+    if (S == 0) return {};
+    std::vector<double> c = regular_ ? regular_->get_vertex_coordinates(id % S)
+                                     : base_->get_vertex_coordinates(id % S);
+    c.push_back((double)(id / S));
+    return c;
   }
   uint64_t get_n_layers() const { return n_layers_; }
   // regular base: its spatial grid and the per-timestep vertex id stride

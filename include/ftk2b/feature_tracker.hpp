@@ -132,9 +132,15 @@ class FeatureTrackerImpl : public FeatureTracker {
     if (config_.input.type != InputType::Vector && config_.input.type != InputType::GradientVector)
       throw Error(FTK2B_UNSUPPORTED, "input type '" + TrackingConfig::input_type_to_string(config_.input.type) +
                                          "' does not feed critical points");
+    // The reference's unstructured route (read_vtu, feature_tracker.cpp:46-57)
+    // feeds the multicomponent gather physical vertex coordinates as array
+    // indices (engine.hpp:1107-1122 with mesh.hpp:714-720); the meshes it
+    // serves are loaded with ftk2b::read_vtu (vtk.hpp) and run through
+    // SimplicialEngine with per-vertex arrays instead.
     if (config_.mesh.type != MeshType::Regular)
       throw Error(FTK2B_UNSUPPORTED, "mesh type '" + TrackingConfig::mesh_type_to_string(config_.mesh.type) +
-                                         "' needs a VTU reader; use a regular mesh");
+                                         "' is not on the tracker's GPU route; load it with read_vtu and run "
+                                         "SimplicialEngine on ExtrudedSimplicialMesh");
     // regular spatial mesh: configured dims, or the first array's shape
     const detail::HostArray<T>& first = data.begin()->second;
     std::vector<uint64_t> dims = config_.mesh.dimensions;
