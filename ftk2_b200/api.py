@@ -775,6 +775,20 @@ class RegularSimplicialMesh:
     def get_total_dimension(self) -> int:
         return len(self.dims)
 
+    def get_spatial_dimension(self) -> int:
+        return len(self.dims)
+
+    def vertex_coordinates(self, ids: np.ndarray) -> np.ndarray:
+        """get_vertex_coordinates (mesh.hpp:374-378) of many ids: the global
+        grid index per axis, (..., nd) float64."""
+        ids = np.asarray(ids, dtype=np.uint64)
+        out = np.empty(ids.shape + (len(self.global_dims),), np.float64)
+        r = ids.copy()
+        for i, d in enumerate(self.global_dims):
+            out[..., i] = (r % np.uint64(d)).astype(np.float64)
+            r //= np.uint64(d)
+        return out
+
     def desc(self, keep: list) -> MeshDesc:
         return regular_mesh_desc(self.dims, self.offset, self.global_dims)
 
@@ -792,6 +806,14 @@ class UnstructuredSimplicialMesh:
     def get_total_dimension(self) -> int:
         return self.cell_dim
 
+    def get_spatial_dimension(self) -> int:
+        return self.spatial_dim
+
+    def vertex_coordinates(self, ids: np.ndarray) -> np.ndarray:
+        """get_vertex_coordinates (unstructured_mesh.hpp:100-107): the first
+        spatial_dim stored coordinates, (..., spatial_dim) float64."""
+        return self.coords[np.asarray(ids, dtype=np.int64)][..., :self.spatial_dim]
+
 
 class ExtrudedSimplicialMesh:
     """ExtrudedSimplicialMesh(base, n_layers) (mesh.hpp:542-562)."""
@@ -802,6 +824,17 @@ class ExtrudedSimplicialMesh:
 
     def get_total_dimension(self) -> int:
         return self.base.get_total_dimension() + 1
+
+    def get_spatial_dimension(self) -> int:
+        return self.base.get_spatial_dimension()
+
+    def vertex_coordinates(self, ids: np.ndarray) -> np.ndarray:
+        """get_vertex_coordinates (mesh.hpp:714-720): the base vertex's
+        coordinates, then the layer of vertex id s + t * n_base_vertices."""
+        ids = np.asarray(ids, dtype=np.uint64)
+        S = np.uint64(self.base.coords.shape[0])
+        base = self.base.vertex_coordinates((ids % S).astype(np.int64))
+        return np.concatenate([base, (ids // S).astype(np.float64)[..., None]], axis=-1)
 
     def desc(self, keep: list) -> MeshDesc:
         return extruded_mesh_desc(self.base.coords.shape[0], self.base.cells, self.n_layers, keep)

@@ -341,3 +341,68 @@ def test_read_vtu_round_trip_and_missing_file(vtk_run, tmp_path):
                                     'compressor="vtkZLibDataCompressor">\n</VTKFile>\n')
     r = subprocess.run([vtk_run, "read", str(tmp_path / "z.vtu")], capture_output=True, text=True)
     assert r.returncode == 2 and "compressed" in r.stderr
+
+
+# ---------------------------------------------------------------- Python writer
+
+def _py_result(feats, conn):
+    from types import SimpleNamespace
+    return SimpleNamespace(simplices=np.array([f[1] for f in feats], np.uint64),
+                           bary=np.array([f[2] for f in feats], np.float32),
+                           track_id=np.array([f[3] for f in feats], np.uint64),
+                           type=np.array([f[4] for f in feats], np.uint32),
+                           scalar=np.array([f[5] for f in feats], np.float32), connectivity=conn)
+
+
+def _py_mesh(mesh):
+    from ftk2_b200 import api
+    if mesh[0] == "regular":
+        return api.RegularSimplicialMesh(mesh[1])
+    _, sd, cd, coords, cells, nl = mesh
+    return api.ExtrudedSimplicialMesh(api.UnstructuredSimplicialMesh(sd, cd, coords, cells), nl)
+
+
+@pytest.mark.parametrize("name", ["regular_3d_t", "extruded_tri_2d", "extruded_tri_3d_coords"])
+def test_python_writer_is_byte_identical(vtk_run, tmp_path, name):
+    """ftk2_b200.vtk writes the same bytes as the C++ header for the same
+    complex, in every form the driver writes."""
+    from ftk2_b200 import vtk
+    mesh, feats, conn = CASES[name](np.random.default_rng(len(name)))
+    (tmp_path / "case.txt").write_text(case_text(mesh, feats, conn))
+    subprocess.run([vtk_run, "write", str(tmp_path / "case.txt"), str(tmp_path)], check=True)
+    r, m = _py_result(feats, conn), _py_mesh(mesh)
+    py = tmp_path / "py"
+    py.mkdir()
+    vtk.write_complex_to_vtp(r, m, str(py / "all_ascii.vtp"), -1, True)
+    vtk.write_complex_to_vtp(r, m, str(py / "all_raw.vtp"))
+    vtk.write_complex_to_vtp(r, m, str(py / "dim1_ascii.vtp"), 1, True)
+    vtk.write_complex_to_vtu(r, m, str(py / "all_ascii.vtu"), -1, True)
+    vtk.write_complex_to_vtu(r, m, str(py / "all_raw.vtu"))
+    vtk.write_complex_to_vtu(r, m, str(py / "dim0_raw.vtu"), 0)
+    vtk.write_complex_to_vtu(r, m, str(py / "dim3_ascii.vtu"), 3, True)
+    for f in sorted(os.listdir(py)):
+        assert (py / f).read_bytes() == (tmp_path / f).read_bytes(), f
+
+
+def test_python_writer_takes_extraction_results(tmp_path):
+    """CPResult star edges become lines; ContourResult cells become
+    triangles or tetrahedra."""
+    from ftk2_b200 import api, vtk
+    mesh = api.RegularSimplicialMesh([4, 4, 3])
+    cp = api.CPResult(simplices=np.array([[0, 1, 5], [1, 5, 21]], np.uint64), lam=np.zeros((2, 3)),
+                      bary=np.array([[0.5, 0.25, 0.25], [0.125, 0.5, 0.375]], np.float32),
+                      track_id=np.array([0, 0], np.uint64), type=np.zeros(2, np.uint32),
+                      cp_class=np.zeros(2, np.uint32), scalar=np.zeros(2, np.float32),
+                      edges=np.array([[0, 1]], np.uint32), n_tracks=1)
+    vtk.write_complex_to_vtp(cp, mesh, str(tmp_path / "cp.vtp"), use_ascii=True)
+    got, piece = parse_vtk(tmp_path / "cp.vtp")
+    assert got[("Lines", "connectivity")].tolist() == [0, 1] and piece["NumberOfLines"] == "1"
+    # vertex 21 = (1, 1, 1): point 2 = 0.125*(1,0,0) + 0.5*(1,1,0) + 0.375*(1,1,1)
+    assert got[("Points", "Points")].reshape(-1, 3)[1].tolist() == [1.0, 0.875, 0.375]
+    lv = api.ContourResult(simplices=np.array([[0, 1], [1, 2], [0, 4]], np.uint64), lam=np.zeros((3, 2)),
+                           bary=np.full((3, 2), 0.5, np.float32), track_id=np.zeros(3, np.uint64),
+                           scalar=np.full(3, 0.5, np.float32), cells=np.array([[0, 1, 2]], np.uint32))
+    vtk.write_complex_to_vtu(lv, mesh, str(tmp_path / "lv.vtu"))
+    got, _ = parse_vtk(tmp_path / "lv.vtu")
+    assert got[("Cells", "types")].tolist() == [5] and got[("Cells", "connectivity")].tolist() == [0, 1, 2]
+    assert got[("PointData", "Type")].tolist() == [0, 0, 0]
