@@ -11,7 +11,9 @@ spatial one, else 0).  Connectivity: CPResult star edges (dimension 1),
 ContourResult manifold cells (dimension = cell width - 1), or an explicit
 `connectivity` list of (dimension, flat indices) on the result.  ASCII when
 use_ascii is set or FTK_DEBUG is in the environment, else appended raw binary
-with UInt64 block headers.
+with UInt64 block headers.  read_vtu loads an unstructured base mesh as the
+reference's read_vtu does (utils/vtk.hpp:165-192), same result as the C++
+header's.
 """
 from __future__ import annotations
 
@@ -164,3 +166,112 @@ def write_complex_to_vtu(result, mesh, filename: str, target_dim: int = -1, use_
     w.array("UInt8", "types", 1, types, "        ")
     w.body.write("      </Cells>\n    </Piece>\n  </UnstructuredGrid>\n")
     w.save(filename, "UnstructuredGrid")
+
+
+# ---------------------------------------------------------------- reading
+
+_NP = {"Float32": "<f4", "Float64": "<f8", "Int8": "i1", "UInt8": "u1", "Int16": "<i2", "UInt16": "<u2",
+       "Int32": "<i4", "UInt32": "<u4", "Int64": "<i8", "UInt64": "<u8"}
+
+
+def _attrs(tag: str) -> dict:
+    import re
+    return dict(re.findall(r'(\w+)="([^"]*)"', tag))
+
+
+def _b64_stream(text: bytes, start: int, want: int) -> bytes:
+    """Decode base64 quanta from start until want bytes are out; '=' padding
+    may close a quantum mid-stream (a header encoded apart from its data)."""
+    import binascii
+    out, quantum, p = bytearray(), bytearray(), start
+    while len(out) < want and p < len(text):
+        c = text[p:p + 1]
+        p += 1
+        if c == b"<":
+            break
+        if c.isspace():
+            continue
+        quantum += c
+        if len(quantum) == 4:
+            out += binascii.a2b_base64(bytes(quantum))
+            quantum.clear()
+    return bytes(out)
+
+
+def read_vtu(filename: str):
+    """read_vtu (utils/vtk.hpp:165-192): points and the triangles and
+    tetrahedra of a single-piece, little-endian, uncompressed VTU file (ASCII,
+    inline base64, appended base64 or appended raw) as
+    UnstructuredSimplicialMesh(cell_dim, cell_dim, coords, cells); cell_dim is
+    that of the last triangle or tetrahedron.  None if the file cannot be
+    opened."""
+    import re
+    from . import api
+    try:
+        data = open(filename, "rb").read()
+    except OSError:
+        return None
+    m = re.search(rb"<VTKFile([^>]*)>", data)
+    root = _attrs(m.group(1).decode()) if m else {}
+    if root.get("type") != "UnstructuredGrid":
+        raise ValueError(f"not a VTK UnstructuredGrid file: {filename}")
+    if root.get("byte_order") == "BigEndian" or root.get("compressor"):
+        raise ValueError("big-endian or compressed VTU")
+    hb = 8 if root.get("header_type") == "UInt64" else 4
+    app_at, raw = None, False
+    am = re.search(rb"<AppendedData([^>]*)>", data)
+    if am:
+        raw = _attrs(am.group(1).decode()).get("encoding") == "raw"
+        app_at = data.index(b"_", am.end()) + 1
+    piece = _attrs(re.search(rb"<Piece([^>]*)>", data).group(1).decode())
+    n_pts, n_cells = int(piece["NumberOfPoints"]), int(piece["NumberOfCells"])
+
+    def array(section: bytes, name):
+        s = data.index(b"<" + section, 0)
+        e = data.index(b"</" + section + b">", s)
+        for dm in re.finditer(rb"<DataArray([^>]*?)(/?)>", data[s:e]):
+            a = _attrs(dm.group(1).decode())
+            if name is None or a.get("Name") == name:
+                return a, s + dm.end()
+        raise ValueError(f"VTU lacks DataArray {name}")
+
+    def values(a: dict, body: int, count: int) -> np.ndarray:
+        dt = np.dtype(_NP[a["type"]])
+        fmt = a.get("format", "ascii")
+        if fmt == "ascii":
+            txt = data[body:data.index(b"</DataArray>", body)].split()[:count]
+            return np.array([float(t) for t in txt], np.float64).astype(dt)
+        need = hb + count * dt.itemsize
+        if fmt == "binary":
+            b = _b64_stream(data, body, need)
+        else:
+            off = app_at + int(a["offset"])
+            b = data[off:off + need] if raw else _b64_stream(data, off, need)
+        if len(b) < need:
+            raise ValueError("truncated DataArray in VTU")
+        return np.frombuffer(b[hb:need], dt)
+
+    pa, pb = array(b"Points", None)
+    nc = int(pa.get("NumberOfComponents", "1") or 1)
+    xyz = values(pa, pb, n_pts * nc).astype(np.float64).reshape(n_pts, nc)
+    coords = np.zeros((n_pts, 3), np.float64)
+    coords[:, :min(3, nc)] = xyz[:, :3]
+    offs = values(*array(b"Cells", "offsets"), n_cells).astype(np.int64)
+    types = values(*array(b"Cells", "types"), n_cells).astype(np.int64)
+    conn = values(*array(b"Cells", "connectivity"), int(offs[-1]) if n_cells else 0).astype(np.uint64)
+    cells, cell_dim = [], 0
+    for i in range(n_cells):
+        if types[i] == 5:
+            cell_dim = 2
+        elif types[i] == 10:
+            cell_dim = 3
+        else:
+            continue
+        cells.append(conn[(offs[i - 1] if i else 0):offs[i]])
+    flat = np.concatenate(cells) if cells else np.zeros(0, np.uint64)
+    if all(len(c) == cell_dim + 1 for c in cells):
+        return api.UnstructuredSimplicialMesh(cell_dim, cell_dim, coords, flat)
+    # triangles and tetrahedra mixed: the flat id list, as the reference keeps it
+    mesh = api.UnstructuredSimplicialMesh.__new__(api.UnstructuredSimplicialMesh)
+    mesh.spatial_dim, mesh.cell_dim, mesh.coords, mesh.cells = cell_dim, cell_dim, coords, flat
+    return mesh

@@ -305,6 +305,8 @@ def run_read(vtk_run, path):
                                               ("base64", "UInt32", True), ("raw", "UInt32", False),
                                               ("raw", "UInt64", False)])
 def test_read_vtu_encodings(vtk_run, tmp_path, enc, header, joint):
+    """The C++ reader and the Python one (ftk2_b200.vtk.read_vtu)."""
+    from ftk2_b200 import vtk
     rng = np.random.default_rng(11)
     pts = rng.normal(size=(7, 3))
     # triangles kept; a line and a quad skipped, as VTK's cell types other
@@ -316,11 +318,16 @@ def test_read_vtu_encodings(vtk_run, tmp_path, enc, header, joint):
     assert (sd, cd) == (2, 2)
     assert np.array_equal(coords, pts)
     assert got.tolist() == [0, 1, 2, 1, 2, 3, 4, 5, 6]
+    m = vtk.read_vtu(str(p))
+    assert (m.spatial_dim, m.cell_dim) == (2, 2) and np.array_equal(m.coords, pts)
+    assert m.cells.reshape(-1).tolist() == got.tolist() and m.cells.shape == (3, 3)
 
     tets = [(10, [0, 1, 2, 3]), (10, [1, 2, 3, 4])]
     p.write_bytes(make_vtu(pts, tets, enc, header, joint))
     sd, cd, coords, got = run_read(vtk_run, p)
     assert (sd, cd) == (3, 3) and got.tolist() == [0, 1, 2, 3, 1, 2, 3, 4]
+    m = vtk.read_vtu(str(p))
+    assert m.cell_dim == 3 and m.cells.tolist() == [[0, 1, 2, 3], [1, 2, 3, 4]] and np.array_equal(m.coords, pts)
 
 
 def test_read_vtu_round_trip_and_missing_file(vtk_run, tmp_path):
@@ -337,6 +344,11 @@ def test_read_vtu_round_trip_and_missing_file(vtk_run, tmp_path):
         assert got.tolist() == ids and cd == (3 if last == 10 else 2)
     r = subprocess.run([vtk_run, "read", str(tmp_path / "absent.vtu")], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip() == "none"
+    from ftk2_b200 import vtk
+    assert vtk.read_vtu(str(tmp_path / "absent.vtu")) is None
+    m = vtk.read_vtu(str(tmp_path / "all_raw.vtu"))  # mixed triangles and tetrahedra: flat ids
+    assert np.array_equal(m.coords, xyz.astype(np.float64))
+    assert m.cells.tolist() == expected_cells(conn, {2, 3})[0]
     (tmp_path / "z.vtu").write_text('<?xml version="1.0"?>\n<VTKFile type="UnstructuredGrid" '
                                     'compressor="vtkZLibDataCompressor">\n</VTKFile>\n')
     r = subprocess.run([vtk_run, "read", str(tmp_path / "z.vtu")], capture_output=True, text=True)
