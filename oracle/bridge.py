@@ -42,6 +42,7 @@ class OrcField(C.Structure):
         ("comp", C.c_void_p * 4), ("nd", C.c_int), ("dims", C.c_uint64 * 4),
         ("scalar", C.c_void_p), ("scalar_nd", C.c_int), ("scalar_dims", C.c_uint64 * 4),
         ("sos_q", C.c_double), ("n_threads", C.c_int),
+        ("fiber", C.c_int), ("fiber_thr", C.c_double * 2),
     ]
 
 
@@ -134,10 +135,11 @@ def make_extruded_mesh(coords: np.ndarray, cells: np.ndarray, n_layers: int, kee
 
 
 def make_field(arrays, layout: int, ncomp: int, scalar=None, sos_q: float = 1e6,
-               n_threads: int = 0, keep: list | None = None) -> OrcField:
+               n_threads: int = 0, keep: list | None = None, fiber_thr=None) -> OrcField:
     """arrays: MULTI -> one numpy array whose memory is [M, dims...] Fortran
     (C-order shape (..reversed dims.., M)); SEPARATE / PER_VERTEX -> list of M
-    arrays (C-order shape reversed dims)."""
+    arrays (C-order shape reversed dims).  fiber_thr = (a, b): the
+    restatement runs FiberPredicate<T> with those thresholds (ncomp 2)."""
     keep = keep if keep is not None else []
     f = OrcField()
     first = arrays if layout == LAYOUT_MULTI else arrays[0]
@@ -168,6 +170,9 @@ def make_field(arrays, layout: int, ncomp: int, scalar=None, sos_q: float = 1e6,
             f.scalar_dims[i] = int(d)
     f.sos_q = float(sos_q)
     f.n_threads = int(n_threads)
+    if fiber_thr is not None:
+        f.fiber = 1
+        f.fiber_thr[0], f.fiber_thr[1] = float(fiber_thr[0]), float(fiber_thr[1])
     return f
 
 

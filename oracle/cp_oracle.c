@@ -235,12 +235,20 @@ static int evaluate(const acc_t* a, int M, const uint64_t vid[4], uint64_t g[4][
   double vals[4][3];
   for (int i = 0; i <= M; ++i)
     for (int j = 0; j < M; ++j) vals[i][j] = field_value(a, j, g[i], vid[i]);
+  if (f->fiber) /* FiberPredicate::extract_it: adj = values - thresholds in T */
+    for (int i = 0; i <= M; ++i)
+      for (int j = 0; j < M && j < 2; ++j)
+        vals[i][j] = f->dtype == ORC_F64 ? vals[i][j] - f->fiber_thr[j]
+                                         : (double)((float)vals[i][j] - (float)f->fiber_thr[j]);
   if (!sos_inside(M, vals, vid, f->sos_q)) return 0;
   int ok;
   if (f->dtype == ORC_F64) {
     double lam[4];
     ok = solve_f64(M, vals, lam);
-    if (!ok) return 0;
+    if (!ok && f->fiber) /* the centroid, (T)1.0 / 3.0 (predicate.hpp:354) */
+      for (int i = 0; i <= M; ++i) lam[i] = 1.0 / 3.0;
+    else if (!ok)
+      return 0;
     for (int i = 0; i <= M; ++i) out->lam[i] = lam[i];
     double s = 0;
     if (f->scalar && f->layout != ORC_LAYOUT_MULTI)
@@ -251,7 +259,10 @@ static int evaluate(const acc_t* a, int M, const uint64_t vid[4], uint64_t g[4][
     for (int i = 0; i <= M; ++i)
       for (int j = 0; j < M; ++j) fv[i][j] = (float)vals[i][j];
     ok = solve_f32(M, fv, lam);
-    if (!ok) return 0;
+    if (!ok && f->fiber)
+      for (int i = 0; i <= M; ++i) lam[i] = (float)(1.0 / 3.0);
+    else if (!ok)
+      return 0;
     for (int i = 0; i <= M; ++i) out->lam[i] = lam[i];
     float s = 0;
     if (f->scalar && f->layout != ORC_LAYOUT_MULTI)

@@ -59,6 +59,11 @@ typedef struct {
   uint64_t scalar_dims[4];
   double sos_q;             /* Predicate::sos_q (predicate.hpp:25) */
   int n_threads;            /* restatement only: worker threads (0 = all cores) */
+  /* restatement only: FiberPredicate<T> (predicate.hpp:341-362) instead of
+   * CriticalPointPredicate<2,T>: values less fiber_thr in the field precision,
+   * the centroid where the solve fails */
+  int fiber;
+  double fiber_thr[2];
 } orc_field;
 
 typedef struct {

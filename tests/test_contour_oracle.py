@@ -192,3 +192,38 @@ def test_extruded_fiber_reference_reproduces_fixtures(name):
     assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
     assert np.array_equal(r.track_id, g["track_id"])
     assert np.array_equal(r.edges, g["edges"])
+
+
+def _same_fiber(r, g, name):
+    assert len(r.track_id) == len(g["track_id"]) > 0, name
+    assert np.array_equal(r.simplices, g["simplices"]), name
+    assert np.array_equal(r.bary.view(np.uint32), g["bary"].view(np.uint32)), name
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64)), name
+    assert np.array_equal(r.track_id, g["track_id"]), name
+    assert np.array_equal(r.edges, g["edges"]), name
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_CASES))
+def test_fiber_restatement_matches_reference_fixtures(name):
+    """The C restatement's fiber mode (oracle/cp_oracle.c: values less the
+    thresholds in the field precision, centroid where the solve fails,
+    predicate.hpp:341-362) reproduces the reference engine's fiber fixtures on
+    regular 2D+t meshes, offsets and near-quantum ties included."""
+    case = contour_cases.FIBER_CASES[name]()
+    g = np.load(os.path.join(FIBER_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+    fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep,
+                            fiber_thr=case["thresholds"])
+    _same_fiber(bridge.run_restatement(mesh, fld), g, name)
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_EXTRUDED_CASES))
+def test_extruded_fiber_restatement_matches_reference_fixtures(name):
+    case = contour_cases.FIBER_EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(FIBER_EXT_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+    fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_PER_VERTEX, 2, sos_q=case["q"], keep=keep,
+                            fiber_thr=case["thresholds"])
+    _same_fiber(bridge.run_restatement(mesh, fld), g, name)
