@@ -119,6 +119,15 @@ def fiber_gauss_f64():
                 q=1e6)
 
 
+def fiber_seeded(dims=(160, 144), nt=12, dtype=np.float32):
+    """Two seeded 24-blob potentials at their medians: hundreds of fiber
+    points, most of them where the f32 solve fails (centroid fallback)."""
+    f = gaussian_potential(dims, nt, seed=41, n_blobs=24, dtype=dtype)
+    g = gaussian_potential(dims, nt, seed=42, n_blobs=24, dtype=dtype)
+    return dict(fields=(f, g), local_dims=[dims[0], dims[1], nt], offset=None, global_dims=None,
+                thresholds=(float(np.median(f)), float(np.median(g))), q=2.0 ** 20)
+
+
 def fiber_f32_offset():
     """A 24x20x5 sub-box at offset (3, 4, 1) of a 30x28x7 mesh; the arrays
     hold the sub-box's values."""

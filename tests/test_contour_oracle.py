@@ -227,3 +227,18 @@ def test_extruded_fiber_restatement_matches_reference_fixtures(name):
     fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_PER_VERTEX, 2, sos_q=case["q"], keep=keep,
                             fiber_thr=case["thresholds"])
     _same_fiber(bridge.run_restatement(mesh, fld), g, name)
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+def test_fiber_restatement_matches_live_reference_seeded():
+    """A larger seeded fiber case (96x80x10 f32, ~500 features, centroid
+    fallbacks among them): restatement == live reference engine."""
+    case = contour_cases.fiber_seeded((96, 80), 10)
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"])
+    ref = bridge.run_reference_fiber(mesh, bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2,
+                                                             sos_q=case["q"], keep=keep), case["thresholds"])
+    fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep,
+                            fiber_thr=case["thresholds"])
+    _same_fiber(bridge.run_restatement(mesh, fld),
+                {k: getattr(ref, k) for k in ("simplices", "bary", "lam", "track_id", "edges")}, "fiber_seeded")
