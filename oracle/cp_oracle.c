@@ -579,7 +579,8 @@ static uint32_t classify_regular_cell(const acc_t* acc, const orc_mesh* me, int 
 
 static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) {
   int d = me->ndims, M = f->ncomp;
-  if (!((d == 3 && M == 2) || (d == 4 && M == 3))) return 2;
+  const int surfaces = f->fiber && d == 4 && M == 2; /* fiber surfaces: triangles of the 3D+t mesh */
+  if (!((d == 3 && M == 2) || (d == 4 && M == 3) || surfaces)) return 2;
   chains_t ch;
   build_chains(&ch, d, M);
 
@@ -617,6 +618,20 @@ static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) 
   if (all.n) qsort(all.a, all.n, sizeof(feat_t), cmp_feat);
   size_t n = all.n;
   feat_t* F = all.a;
+
+  if (surfaces) {
+    /* the features only: the tracks and star-fan triangles of fiber surfaces
+     * come from form_general_manifold_patches (engine.hpp:1342-1417), which
+     * is not restated here; each track id is the feature's own index */
+    evec_t none = {0};
+    uint64_t* self = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+    for (size_t i = 0; i < n; ++i) self[i] = i;
+    finish(F, n, M, &none, self, tested, out);
+    out->cp_class = NULL;
+    free(self);
+    free(F);
+    return 0;
+  }
 
   /* star edges: every top cell with >= 2 active faces is a coface of each of
    * them, so visiting the cofaces of each feature covers engine.hpp:161-180.

@@ -128,6 +128,15 @@ def fiber_seeded(dims=(160, 144), nt=12, dtype=np.float32):
                 thresholds=(float(np.median(f)), float(np.median(g))), q=2.0 ** 20)
 
 
+def fiber_surface_seeded(dims=(32, 28, 24), nt=5, dtype=np.float32):
+    """Two seeded potentials on a 3D+t mesh at their medians: thousands of
+    fiber-surface triangles across many blocks of the device pipeline."""
+    f = gaussian_potential(dims, nt, seed=61, n_blobs=16, dtype=dtype, sigma=(2.0, 5.0))
+    g = gaussian_potential(dims, nt, seed=62, n_blobs=16, dtype=dtype, sigma=(2.0, 5.0))
+    return dict(fields=(f, g), local_dims=list(dims) + [nt], offset=None, global_dims=None,
+                thresholds=(float(np.median(f)), float(np.median(g))), q=2.0 ** 20)
+
+
 def fiber_f32_offset():
     """A 24x20x5 sub-box at offset (3, 4, 1) of a 30x28x7 mesh; the arrays
     hold the sub-box's values."""

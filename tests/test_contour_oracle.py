@@ -242,3 +242,21 @@ def test_fiber_restatement_matches_live_reference_seeded():
                             fiber_thr=case["thresholds"])
     _same_fiber(bridge.run_restatement(mesh, fld),
                 {k: getattr(ref, k) for k in ("simplices", "bary", "lam", "track_id", "edges")}, "fiber_seeded")
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_CASES))
+def test_fiber_surface_restatement_features_match_reference_fixtures(name):
+    """Fiber surfaces on 3D+t meshes: the restatement's triangle features (the
+    50 triangle types of the 4-D Kuhn cube, the 2-D origin test, the solve
+    with its centroid fallback) equal the reference's bit for bit; tracks and
+    star-fan triangles are pinned by the fixtures alone."""
+    case = contour_cases.FIBER_SURFACE_CASES[name]()
+    g = np.load(os.path.join(FS_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"], case["offset"], case["global_dims"])
+    r = bridge.run_restatement(mesh, bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2,
+                                                       sos_q=case["q"], keep=keep, fiber_thr=case["thresholds"]))
+    assert len(r.track_id) == len(g["track_id"]) > 0
+    assert np.array_equal(r.simplices, g["simplices"])
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
+    assert np.array_equal(r.bary.view(np.uint32), g["bary"].view(np.uint32))

@@ -172,20 +172,3 @@ def test_fiber_extruded_matches_reference_fixture(ctx, name):
     r = ctx.fiber(mesh, fd, case["thresholds"], case["q"])
     assert len(r.track_id) == len(g["track_id"]) > 0
     assert_same(r, {k: g[k] for k in ("simplices", "bary", "lam", "track_id", "edges")}, name)
-
-
-@pytest.mark.parametrize("dtype", [np.float32, np.float64])
-def test_fiber_matches_restatement_seeded(ctx, dtype):
-    """160x144x12 seeded fibers against the C restatement's fiber mode (itself
-    pinned to the reference's fixtures and live runs): features, both
-    barycentric precisions, tracks and star edges."""
-    case = contour_cases.fiber_seeded(dtype=dtype)
-    keep: list = []
-    want = bridge.run_restatement(
-        bridge.make_regular_mesh(case["local_dims"]),
-        bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep,
-                          fiber_thr=case["thresholds"]))
-    r = run_gpu(ctx, case)
-    assert len(want.track_id) > 100
-    assert_same(r, {"simplices": want.simplices, "bary": want.bary, "lam": want.lam, "track_id": want.track_id,
-                    "edges": want.edges}, str(dtype))
