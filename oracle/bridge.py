@@ -54,6 +54,7 @@ class OrcResult(C.Structure):
         ("type", C.POINTER(C.c_uint32)), ("scalar", C.POINTER(C.c_float)),
         ("n_edges", C.c_uint64), ("edges", C.POINTER(C.c_uint32)),
         ("n_tested", C.c_uint64), ("cp_class", C.POINTER(C.c_uint32)),
+        ("cell_dim", C.c_int), ("n_cells", C.c_uint64), ("cells", C.POINTER(C.c_uint32)),
     ]
 
 
@@ -69,6 +70,7 @@ class CPResult:
     edges: np.ndarray       # (e, 2) uint32
     n_tested: int = 0
     cp_class: np.ndarray | None = None  # (n,) uint32, restatement on regular meshes only
+    cells: np.ndarray | None = None     # (c, 3) uint32 star-fan triangles, restated fiber surfaces only
 
 
 _libs: dict[str, C.CDLL] = {}
@@ -200,6 +202,8 @@ def _run(path: str, prefix: str, mesh: OrcMesh, field: OrcField) -> CPResult:
             edges=arr(res.edges, 2 * e, np.uint32).reshape(e, 2),
             n_tested=int(res.n_tested),
             cp_class=arr(res.cp_class, n, np.uint32) if res.cp_class else None,
+            cells=arr(res.cells, int(res.n_cells) * (int(res.cell_dim) + 1), np.uint32).reshape(
+                int(res.n_cells), int(res.cell_dim) + 1) if res.cells else None,
         )
     finally:
         getattr(lib, prefix + "_free")(C.byref(res))

@@ -577,6 +577,114 @@ static uint32_t classify_regular_cell(const acc_t* acc, const orc_mesh* me, int 
   return cporacle_classify_jacobian(m, J);
 }
 
+typedef struct { uint32_t v[3]; } tri_t;
+
+static int cmp_tri(const void* x, const void* y) {
+  const uint32_t *a = ((const tri_t*)x)->v, *b = ((const tri_t*)y)->v;
+  for (int i = 0; i < 3; ++i)
+    if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+  return 0;
+}
+
+/* Fiber surfaces (triangle features of a 3D+t mesh): form_general_manifold_
+ * patches with k = 2 (engine.hpp:1342-1417) on every pentatope of the local
+ * mesh.  Its active triangles in feature order (the order of their
+ * encode_simplex_id codes), h_S the first; on each tet face holding two or
+ * more, h_T the first there and a triangle (h_S, h_T, n) for every later n
+ * whenever h_S differs from both.  get_complex keeps the sorted unique
+ * triangles and unites their features; a track id is the component's
+ * smallest feature index. */
+static void fiber_surface_cells(const orc_mesh* me, const feat_t* F, size_t n, uint64_t tested,
+                                orc_result* out) {
+  chains_t pc;
+  build_chains(&pc, 4, 4);
+  tri_t* T = NULL;
+  size_t nt = 0, cap = 0;
+  uint64_t n_corners = 1;
+  for (int k = 0; k < 4; ++k) n_corners *= me->local_dims[k];
+  for (uint64_t ci = 0; ci < n_corners && n; ++ci) {
+    uint64_t c[4], t = ci;
+    int inside = 1;
+    for (int k = 0; k < 4; ++k) {
+      c[k] = t % me->local_dims[k];
+      t /= me->local_dims[k];
+      if (c[k] + 1 >= me->local_dims[k]) inside = 0;
+    }
+    if (!inside) continue;
+    for (int ty = 0; ty < pc.n; ++ty) {
+      uint64_t cell[5];
+      for (int r = 0; r <= 4; ++r) {
+        uint64_t g[4];
+        for (int k = 0; k < 4; ++k) g[k] = c[k] + me->offset[k] + ((pc.mask[ty][r] >> k) & 1);
+        cell[r] = grid_id(me, g);
+      }
+      /* the 10 triangle faces (ids ascending, as the cell's are) */
+      int64_t node[10];
+      int nn = 0;
+      uint64_t nv[10][3];
+      for (int a = 0; a < 5; ++a)
+        for (int b = a + 1; b < 5; ++b)
+          for (int e = b + 1; e < 5; ++e) {
+            uint64_t key[3] = {cell[a], cell[b], cell[e]};
+            int64_t idx = find_feat(F, n, key, 2);
+            if (idx >= 0) {
+              node[nn] = idx;
+              nv[nn][0] = key[0]; nv[nn][1] = key[1]; nv[nn][2] = key[2];
+              nn++;
+            }
+          }
+      if (nn < 2) continue;
+      /* feature order */
+      for (int i = 1; i < nn; ++i)
+        for (int j = i; j > 0 && node[j] < node[j - 1]; --j) {
+          int64_t tn = node[j]; node[j] = node[j - 1]; node[j - 1] = tn;
+          for (int q = 0; q < 3; ++q) { uint64_t tv = nv[j][q]; nv[j][q] = nv[j - 1][q]; nv[j - 1][q] = tv; }
+        }
+      const int64_t hS = node[0];
+      for (int x = 0; x < 5; ++x) { /* the tet face without cell vertex x */
+        int64_t onf[10];
+        int no = 0;
+        for (int i = 0; i < nn; ++i)
+          if (nv[i][0] != cell[x] && nv[i][1] != cell[x] && nv[i][2] != cell[x]) onf[no++] = node[i];
+        if (no < 2) continue;
+        const int64_t hT = onf[0];
+        for (int j = 1; j < no; ++j) {
+          if (hS == hT || hS == onf[j]) continue;
+          uint32_t v[3] = {(uint32_t)hS, (uint32_t)hT, (uint32_t)onf[j]};
+          for (int i = 1; i < 3; ++i)
+            for (int q = i; q > 0 && v[q] < v[q - 1]; --q) { uint32_t tv = v[q]; v[q] = v[q - 1]; v[q - 1] = tv; }
+          if (nt == cap) {
+            cap = cap ? 2 * cap : 1024;
+            T = (tri_t*)realloc(T, cap * sizeof(tri_t));
+          }
+          T[nt].v[0] = v[0]; T[nt].v[1] = v[1]; T[nt].v[2] = v[2];
+          nt++;
+        }
+      }
+    }
+  }
+  if (nt) qsort(T, nt, sizeof(tri_t), cmp_tri);
+  size_t nu = 0;
+  for (size_t i = 0; i < nt; ++i)
+    if (nu == 0 || cmp_tri(&T[nu - 1], &T[i]) != 0) T[nu++] = T[i];
+  uint64_t* parent = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+  for (size_t i = 0; i < n; ++i) parent[i] = i;
+  for (size_t i = 0; i < nu; ++i) {
+    uf_unite(parent, T[i].v[0], T[i].v[1]);
+    uf_unite(parent, T[i].v[1], T[i].v[2]);
+  }
+  evec_t none = {0};
+  finish((feat_t*)F, n, 2, &none, parent, tested, out);
+  out->cp_class = NULL;
+  out->cell_dim = 2;
+  out->n_cells = nu;
+  out->cells = (uint32_t*)malloc(sizeof(uint32_t) * (3 * nu + 3));
+  for (size_t i = 0; i < nu; ++i)
+    for (int q = 0; q < 3; ++q) out->cells[3 * i + q] = T[i].v[q];
+  free(T);
+  free(parent);
+}
+
 static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) {
   int d = me->ndims, M = f->ncomp;
   const int surfaces = f->fiber && d == 4 && M == 2; /* fiber surfaces: triangles of the 3D+t mesh */
@@ -620,15 +728,7 @@ static int run_regular(const orc_mesh* me, const orc_field* f, orc_result* out) 
   feat_t* F = all.a;
 
   if (surfaces) {
-    /* the features only: the tracks and star-fan triangles of fiber surfaces
-     * come from form_general_manifold_patches (engine.hpp:1342-1417), which
-     * is not restated here; each track id is the feature's own index */
-    evec_t none = {0};
-    uint64_t* self = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
-    for (size_t i = 0; i < n; ++i) self[i] = i;
-    finish(F, n, M, &none, self, tested, out);
-    out->cp_class = NULL;
-    free(self);
+    fiber_surface_cells(me, F, n, tested, out);
     free(F);
     return 0;
   }
@@ -1047,6 +1147,7 @@ void cporacle_free(orc_result* r) {
   free(r->scalar);
   free(r->edges);
   free(r->cp_class);
+  free(r->cells);
   memset(r, 0, sizeof(*r));
 }
 

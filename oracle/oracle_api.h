@@ -80,6 +80,9 @@ typedef struct {
   uint64_t n_tested;        /* m-simplices evaluated (restatement only) */
   uint32_t* cp_class;       /* n classes (restatement only, regular meshes; else NULL):
                                FTK2B_CLASS_* codes of include/ftk2b.h */
+  int cell_dim;             /* restatement of fiber surfaces only: the star-fan */
+  uint64_t n_cells;         /* triangles of get_complex, (cell_dim + 1) sorted  */
+  uint32_t* cells;          /* feature indices each, rows in lexicographic order */
 } orc_result;
 
 /* The high-level caller's critical-point flow (src/high_level/feature_tracker.cpp:

@@ -245,11 +245,12 @@ def test_fiber_restatement_matches_live_reference_seeded():
 
 
 @pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_CASES))
-def test_fiber_surface_restatement_features_match_reference_fixtures(name):
+def test_fiber_surface_restatement_matches_reference_fixtures(name):
     """Fiber surfaces on 3D+t meshes: the restatement's triangle features (the
     50 triangle types of the 4-D Kuhn cube, the 2-D origin test, the solve
-    with its centroid fallback) equal the reference's bit for bit; tracks and
-    star-fan triangles are pinned by the fixtures alone."""
+    with its centroid fallback), its star-fan triangles
+    (form_general_manifold_patches with k = 2) and its tracks equal the
+    reference's bit for bit."""
     case = contour_cases.FIBER_SURFACE_CASES[name]()
     g = np.load(os.path.join(FS_GOLD, f"{name}.npz"))
     keep: list = []
@@ -260,3 +261,22 @@ def test_fiber_surface_restatement_features_match_reference_fixtures(name):
     assert np.array_equal(r.simplices, g["simplices"])
     assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64))
     assert np.array_equal(r.bary.view(np.uint32), g["bary"].view(np.uint32))
+    assert np.array_equal(r.cells, g["cells"])
+    assert np.array_equal(r.track_id, g["track_id"])
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+def test_fiber_surface_restatement_matches_live_reference_seeded():
+    case = contour_cases.fiber_surface_seeded((16, 14, 12), 4)
+    keep: list = []
+    mesh = bridge.make_regular_mesh(case["local_dims"])
+    ref, cells = bridge.run_reference_fiber_surface(
+        mesh, bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep),
+        case["thresholds"])
+    r = bridge.run_restatement(mesh, bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2,
+                                                       sos_q=case["q"], keep=keep, fiber_thr=case["thresholds"]))
+    assert len(r.track_id) > 100 and len(cells) > 0
+    assert np.array_equal(r.simplices, ref.simplices)
+    assert np.array_equal(r.lam.view(np.uint64), ref.lam.view(np.uint64))
+    assert np.array_equal(r.track_id, ref.track_id)
+    assert np.array_equal(r.cells, cells)

@@ -2,10 +2,10 @@
 on the device against the C restatement's fiber mode (oracle/cp_oracle.c),
 which reproduces the reference's fixtures and live runs
 (tests/test_contour_oracle.py).  Fibers: features, both barycentric
-precisions, tracks and star edges.  Fiber surfaces: features and barycentrics
-against the restatement; tracks and star-fan triangles through properties
-that hold at any size (track ids are component minima, every triangle joins
-features of one track, no triangle repeats)."""
+precisions, tracks and star edges.  Fiber surfaces: features, barycentrics,
+star-fan triangles and tracks, plus properties that hold at any size (track
+ids are component minima, every triangle joins features of one track, no
+triangle repeats)."""
 import numpy as np
 import pytest
 
@@ -65,3 +65,5 @@ def test_fiber_surface_seeded_32x28x24x5(ctx, dtype):
     assert len(c) > 0 and c.max() < n
     assert (t[c[:, 0]] == t[c[:, 1]]).all() and (t[c[:, 1]] == t[c[:, 2]]).all()
     assert len(np.unique(np.sort(c, axis=1), axis=0)) == len(c)
+    assert np.array_equal(r.cells.astype(np.uint32), want.cells)
+    assert np.array_equal(r.track_id, want.track_id)
