@@ -30,6 +30,13 @@
  *  - extruded meshes: spatial, prism and interior m-simplices, pentatope star
  *    edges by node-id order, and the coface unions of
  *    ExtrudedSimplicialMesh::cofaces (mesh.hpp:601-712) for 4D meshes         engine.hpp:896-963
+ *  - fiber mode (orc_field.fiber): FiberPredicate<T>, the values less the two
+ *    thresholds in precision T, the centroid (T)1.0/3.0 where the solve
+ *    fails, scalar 0                                                          predicate.hpp:341-362
+ *  - fiber surfaces (fiber mode on a 3D+t mesh): triangle features over the
+ *    50 triangle types of the 4-D Kuhn cube, star-fan triangles of
+ *    form_general_manifold_patches with k = 2 on every pentatope, tracks as
+ *    their components                                                         engine.hpp:1342-1417
  *
  * Compile without FMA contraction (-ffp-contract=off) so the solve rounds
  * exactly like the reference built for x86-64.
