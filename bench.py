@@ -14,7 +14,8 @@ A step = one full extraction (execute + get_complex equivalent) of the field.
 The field (805 MB) is larger than L2 (126 MB), so no flush is needed.
 
 --impl reference times the reference's own CPU engine (oracle/_ref, built from
-the reference's headers) on bounded sub-boxes of the same field.
+the reference's headers) on 32^3 x 2-vertex sub-boxes of the same field, one
+per step, and reports the exact C restatement's all-core rate beside it.
 With --gpus N > 1 every rank runs an independent replica on its own field
 (weak scaling); there is no data-path collective.
 """
@@ -39,7 +40,44 @@ SOS_Q = 2.0 ** 20
 CONFIG = {"workload": "3D flow critical points, plain drop-in: 128^3 x 16 float64 3-component "
                       "Gaussian-sum gradient (32 blobs), 4D Kuhn tets, SoS Q=2^20",
           "grid": [128, 128, 128, 16], "ncomp": 3, "field_dtype": "float64", "sos_q": SOS_Q,
+          "units": "tets = every 3-face of the 4D Kuhn top cells, upper-boundary faces included "
+                   "(the set the reference's phase 1 + phase 2 test): 1,860,189,828 at 128^3 x 16",
           "l2": "inputs larger than L2 (805 MB field vs 126 MB L2)"}
+# the reference's CPU engine runs on spatial sub-boxes of this size, one time
+# step of hypercubes each (a 32^3 x 2-vertex RegularSimplicialMesh sub-box)
+REF_SUB = (32, 32, 32, 2)
+
+
+def kuhn_chains(d: int, m: int):
+    """Vertex masks 1..m of every m-simplex type of the Kuhn d-cube (strictly
+    growing chains of corner masks), mesh.hpp:123-237."""
+    full = (1 << d) - 1
+    out = []
+
+    def rec(prev, depth, acc):
+        for nx in range(prev + 1, full + 1):
+            if (nx & prev) == prev and nx != prev:
+                if depth == m:
+                    out.append(acc + [nx])
+                else:
+                    rec(nx, depth + 1, acc + [nx])
+
+    rec(0, 1, [])
+    return out
+
+
+def kuhn_simplex_count(dims, m: int) -> int:
+    """m-simplices of the Kuhn triangulation of a regular grid of ``dims``
+    vertices, upper-boundary faces included: one per (corner vertex, chain)
+    whose top mask stays inside the grid.  Pure Python, so the reference arm
+    loads none of this repository's libraries."""
+    total = 0
+    for ch in kuhn_chains(len(dims), m):
+        c = 1
+        for k, n in enumerate(dims):
+            c *= n - 1 if (ch[-1] >> k) & 1 else n
+        total += c
+    return total
 
 
 def dist_env():
@@ -127,28 +165,71 @@ def traffic_per_launch():
         return None
 
 
-def cpu_baseline_sample(field_np, steps_budget_s=20.0):
-    """The reference's CPU engine on sub-boxes of the same field, run until
-    ~steps_budget_s seconds have been spent; returns (simplices/s, sample)."""
+def ref_sub_box(rng, corner=DIMS, nt=NT):
+    """A random REF_SUB sub-box (offset) inside a grid of ``corner`` x nt."""
+    return [int(rng.integers(0, corner[i] - REF_SUB[i] + 1)) for i in range(3)] + \
+        [int(rng.integers(0, nt - REF_SUB[3] + 1))]
+
+
+def run_reference_sub_box(lo, seed=1234):
+    """The reference's CPU engine (oracle/_ref) on one REF_SUB sub-box of the
+    headline field at offset ``lo``; the sub-box's values are generated on the
+    host from the same blob draws and handed to the engine as a mesh of its
+    own (multicomponent arrays are read at global coordinates, so an offset
+    mesh would need the whole field).  Returns (simplices, seconds)."""
     from oracle import bridge
+    from ftk2_b200 import synthetic
+    f = synthetic.gaussian_sum_gradient(REF_SUB[:3], REF_SUB[3], seed=seed, n_blobs=32, box=DIMS,
+                                        origin=lo[:3], t0=lo[3])
+    keep: list = []
+    mesh = bridge.make_regular_mesh(list(REF_SUB))
+    fld = bridge.make_field(f, bridge.LAYOUT_MULTI, 3, sos_q=SOS_Q, keep=keep)
+    t = time.perf_counter()
+    bridge.run_reference(mesh, fld)
+    return kuhn_simplex_count(REF_SUB, 3), time.perf_counter() - t
+
+
+def cpu_baseline_sample(budget_s=20.0):
+    """The reference's CPU engine on REF_SUB sub-boxes of the headline field
+    until ~budget_s seconds have been spent; returns (simplices/s, sample)."""
     import numpy as np
-    sub = (14, 14, 14, 4)
-    total_s, total_n, boxes = 0.0, 0, 0
     rng = np.random.default_rng(0)
-    while total_s < steps_budget_s and boxes < 64:
-        lo = [int(rng.integers(0, DIMS[i] - sub[i])) for i in range(3)] + [int(rng.integers(0, NT - sub[3]))]
-        keep: list = []
-        mesh = bridge.make_regular_mesh(list(sub), lo, list(DIMS) + [NT])
-        fld = bridge.make_field(field_np, bridge.LAYOUT_MULTI, 3, sos_q=SOS_Q, keep=keep)
-        t = time.perf_counter()
-        bridge.run_reference(mesh, fld)
-        total_s += time.perf_counter() - t
-        from ftk2_b200 import api
-        total_n += api.simplex_count(api.regular_mesh_desc(list(sub), lo, list(DIMS) + [NT]), 3)
+    total_s, total_n, boxes = 0.0, 0, 0
+    while total_s < budget_s and boxes < 16:
+        n, t = run_reference_sub_box(ref_sub_box(rng))
+        total_s += t
+        total_n += n
         boxes += 1
-    sample = (f"{boxes} sub-boxes of {sub[0]}x{sub[1]}x{sub[2]}x{sub[3]} vertices of the same "
-              f"field, reference engine (oracle/_ref) execute+get_complex, {total_s:.1f} s")
+    sample = (f"{boxes} sub-boxes of {REF_SUB[0]}x{REF_SUB[1]}x{REF_SUB[2]}x{REF_SUB[3]} vertices "
+              f"(one time step of 31^3 hypercubes) of the same field, reference engine (oracle/_ref) "
+              f"execute+get_complex, {total_s:.1f} s")
     return total_n / total_s, sample
+
+
+def restatement_rate(budget_s=10.0):
+    """The exact multithreaded C restatement (oracle/cp_oracle.c, every host
+    core) on 64^3 x 4 sub-boxes of the headline field: simplices/s."""
+    import numpy as np
+    from oracle import bridge
+    from ftk2_b200 import synthetic
+    sub = (64, 64, 64, 4)
+    rng = np.random.default_rng(2)
+    total_s, total_n, boxes = 0.0, 0, 0
+    while total_s < budget_s and boxes < 8:
+        lo = [int(rng.integers(0, DIMS[i] - sub[i] + 1)) for i in range(3)] + [int(rng.integers(0, NT - sub[3] + 1))]
+        f = synthetic.gaussian_sum_gradient(sub[:3], sub[3], seed=1234, n_blobs=32, box=DIMS,
+                                            origin=lo[:3], t0=lo[3])
+        keep: list = []
+        mesh = bridge.make_regular_mesh(list(sub))
+        fld = bridge.make_field(f, bridge.LAYOUT_MULTI, 3, sos_q=SOS_Q, keep=keep)
+        t = time.perf_counter()
+        bridge.run_restatement(mesh, fld)
+        total_s += time.perf_counter() - t
+        total_n += kuhn_simplex_count(sub, 3)
+        boxes += 1
+    return {"value": total_n / total_s, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"{boxes} sub-boxes of {sub[0]}x{sub[1]}x{sub[2]}x{sub[3]} vertices, the exact C "
+                      f"restatement on every host core, {total_s:.1f} s"}
 
 
 def _positions(simplices, lam, dims):
@@ -245,50 +326,38 @@ def precision_c4(ctx, steps=5):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU engine (oracle/_ref, built from its headers,
+    execute + get_complex) on REF_SUB sub-boxes of the headline field, one
+    sub-box per step, with the std::thread workers it starts itself.  Loads
+    none of this repository's CUDA code: simplex counts are pure Python."""
     if rank != 0:
         return 0
     from oracle import bridge
     import numpy as np
-    from ftk2_b200 import synthetic
     if not bridge.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference engine build oracle/_ref missing"}))
         return 0
-    # the reference's CPU engine on the same field definition; sub-boxes are
-    # drawn from a 40^3 x 16 corner of the field, generated on the host
-    corner = (40, 40, 40)
-    field = synthetic.gaussian_sum_gradient(corner, NT, seed=1234, n_blobs=32, box=DIMS)
-    sub = (12, 12, 12, 4)
     rng = np.random.default_rng(1)
-    from ftk2_b200 import api
-
-    def one():
-        lo = [int(rng.integers(0, corner[i] - sub[i])) for i in range(3)] + [int(rng.integers(0, NT - sub[3]))]
-        keep: list = []
-        mesh = bridge.make_regular_mesh(list(sub), lo, list(corner) + [NT])
-        fld = bridge.make_field(field, bridge.LAYOUT_MULTI, 3, sos_q=SOS_Q, keep=keep)
-        n = api.simplex_count(api.regular_mesh_desc(list(sub), lo, list(corner) + [NT]), 3)
-        t = time.perf_counter()
-        bridge.run_reference(mesh, fld)
-        return n, time.perf_counter() - t
-
     for _ in range(args.warmup):
-        one()
+        run_reference_sub_box(ref_sub_box(rng))
     tot_n, tot_t = 0, 0.0
     for _ in range(args.steps):
-        n, t = one()
+        n, t = run_reference_sub_box(ref_sub_box(rng))
         tot_n += n
         tot_t += t
     value = tot_n / tot_t
     cores = os.cpu_count() or 1
+    sample = (f"one {REF_SUB[0]}x{REF_SUB[1]}x{REF_SUB[2]}x{REF_SUB[3]}-vertex sub-box (31^3 hypercubes, "
+              f"one time step) of the workload field per step through the reference engine "
+              f"(std::thread parallel_for; phase 1 serial)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": dict(CONFIG, reference_sample=f"{sub[0]}x{sub[1]}x{sub[2]}x{sub[3]} sub-box per step"),
+            "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"one {sub[0]}x{sub[1]}x{sub[2]}x{sub[3]}-vertex sub-box of the "
-                                       f"workload field per step through the reference engine "
-                                       f"(std::thread parallel_for; phase 1 serial)"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "restatement": restatement_rate()}
     print(json.dumps(line))
     return 0
 
@@ -554,15 +623,15 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(CONFIG, parallelism=f"replicas{world}", features=int(nf), edges=int(ne),
-                           simplices=int(nsimp)),
+            "config": dict(CONFIG, parallelism=f"replicas{world}"),
+            "result": {"features": int(nf), "edges": int(ne), "simplices": int(nsimp)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host.nbytes),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1000.0},
             "roofline": roof, "clocks": clocks.summary(),
             "gpu_launches": int(launches1 - launches0)}
     del pinned, host
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, sample = cpu_baseline_sample(field.cpu().numpy())
+        v, sample = cpu_baseline_sample()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1,
                                 "kind": "reference", "sample": sample}
     # the extra lines are one-GPU measurements (and their CPU baselines belong

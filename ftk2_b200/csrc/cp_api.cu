@@ -83,6 +83,23 @@ static ftk2b_status fail(ftk2b_ctx* ctx, ftk2b_status st, const char* fmt, ...) 
 constexpr int kMaxDevices = 64;
 static std::once_flag g_tables_once[kMaxDevices];
 
+namespace ftk2b {
+// constant tables live per device: upload them once for each device, for
+// contexts and the allocation-free entry point alike
+bool ensure_device_tables(int device) {
+  if (device >= 0 && device < kMaxDevices) {
+    std::call_once(g_tables_once[device], [] {
+      upload_chain_tables();
+      upload_post_tables();
+    });
+  } else {
+    upload_chain_tables();
+    upload_post_tables();
+  }
+  return cudaGetLastError() == cudaSuccess;
+}
+}  // namespace ftk2b
+
 // ---------------------------------------------------------------------------
 // context
 
@@ -113,18 +130,7 @@ extern "C" ftk2b_status ftk2b_ctx_create(int device, ftk2b_ctx** out) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   ctx->num_sms = prop.multiProcessorCount;
-  // constant tables live per device: upload them once for each device (a
-  // second upload while other contexts' kernels read them would be a race)
-  if (device < kMaxDevices) {
-    std::call_once(g_tables_once[device], [] {
-      upload_chain_tables();
-      upload_post_tables();
-    });
-  } else {
-    upload_chain_tables();
-    upload_post_tables();
-  }
-  if (cudaGetLastError() != cudaSuccess) {
+  if (!ensure_device_tables(device)) {
     delete ctx;
     return FTK2B_CUDA_ERROR;
   }

@@ -93,6 +93,11 @@ struct ChainTable {
 };
 
 void upload_chain_tables();
+// Uploads the chain and post-processing constant tables to the current
+// device once per device for the life of the process (a second upload while
+// kernels of another caller read them would be a race).  Returns false when a
+// CUDA call failed.
+bool ensure_device_tables(int device);
 
 // Launches the fused extraction; uses TMA tensor-tile staging when allowed
 // and the array satisfies the 16-byte alignment rules (reported in used_tma);

@@ -1,20 +1,23 @@
 // Allocation-free variant of the regular-mesh feature extraction.
 //
-// Who needs it: callers that are not allowed to allocate device memory while
-// they run -- for instance an in-situ analysis step inside a simulation whose
-// memory manager owns the whole device, a serving loop that works inside a
-// fixed memory budget and cannot afford cudaMalloc's implicit device
-// synchronisation, or host frameworks that record the call into a captured
-// region where allocation is forbidden.  They get one entry point that uses
-// no cudaMalloc/cudaFree (and no allocating library routine): its scratch is
-// the file-scope array below, which every GPU that loads this library keeps
-// until the process exits.
+// Who needs it: callers that may not allocate device memory while they run.
+// An in-situ analysis step inside a simulation whose memory manager already
+// owns the whole device cannot get memory from cudaMalloc without evicting
+// the simulation's own pool; a serving loop held to a fixed memory budget
+// cannot afford cudaMalloc's implicit device synchronisation in the middle of
+// its latency budget.  They get one entry point that uses no cudaMalloc or
+// cudaFree (and no allocating library routine): its scratch is the file-scope
+// array below, which every GPU that loads this library keeps until the
+// process exits.  Inputs and outputs stay the caller's.
 //
 // Limits: at most kMaxCandidates surviving hypercubes and kMaxFeatures
-// accepted simplices per call (scratch: ~9.3 MiB per device).  Every call
-// shares the array; the entry point clears the counters it needs at the start
-// of each call, and calls whose device work overlaps (on different streams or
-// host threads at the same time) race on the shared array.
+// accepted simplices per call (scratch: ~9.3 MiB per device).  More surviving
+// hypercubes than the scratch holds returns FTK2B_UNSUPPORTED: the same call
+// can never succeed, so the caller splits the box into sub-boxes
+// (RegularSimplicialMesh offsets).  Every call shares the array; the entry
+// point clears the counters it needs at the start of each call, and calls
+// whose device work overlaps (on different streams or host threads at the
+// same time) race on the shared array.
 #include <cstring>
 #include <mutex>
 
@@ -52,8 +55,7 @@ static ftk2b_status noalloc_setup(int dev, void** ptr) {
       cudaGetLastError();
       return FTK2B_CUDA_ERROR;
     }
-    upload_chain_tables();
-    if (cudaGetLastError() != cudaSuccess) return FTK2B_CUDA_ERROR;
+    if (!ensure_device_tables(dev)) return FTK2B_CUDA_ERROR;
     g_scratch_ptr[dev] = p;
     g_setup_done[dev] = true;
   }
@@ -182,7 +184,9 @@ extern "C" ftk2b_status ftk2b_cp_features_noalloc(const ftk2b_mesh_desc* mesh,
   }
   *n_features = nf;
   if (h[1]) return FTK2B_TIMEOUT;                      // a bounded TMA wait gave up
-  if (h[0] > kMaxCandidates) return FTK2B_OVERFLOW_RETRY;  // more survivors than the scratch holds
+  // more survivors than the static scratch holds: no retry of this call can
+  // succeed, the box has to be split
+  if (h[0] > kMaxCandidates) return FTK2B_UNSUPPORTED;
   if (nf > capacity) return FTK2B_OVERFLOW_RETRY;     // caller's output too small
   return FTK2B_OK;
 }

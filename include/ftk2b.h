@@ -331,22 +331,25 @@ const char* ftk2b_server_last_error(ftk2b_server* sv);
 void ftk2b_server_destroy(ftk2b_server* sv);
 
 /* --- allocation-free extraction -------------------------------------------
- * No counterpart in the reference.  For callers that must not allocate device
- * memory while they run (an in-situ step inside a simulation whose allocator
- * owns the device, a serving loop held to a fixed memory budget, a host that
- * records calls into a region where cudaMalloc is forbidden).  It runs the
- * fused regular-mesh extraction on `stream` and writes the accepted simplices,
- * unsorted, to caller-provided device memory: canonical keys (corner vertex id
- * * n_types + chain rank) and 4 doubles of barycentrics per feature; `count`
- * is a device word the call uses as its atomic counter, and *n_features
- * receives the number found.  Field pointers must be device pointers.
- * Scratch is a static device array of ~9.3 MiB that every GPU loading the
- * library holds until exit; limits: capacity <= 262144 features and at most
- * 262144 surviving hypercubes per call (FTK2B_INVALID_ARG /
- * FTK2B_OVERFLOW_RETRY beyond them).  The first call on a device looks up the
- * array's device address and uploads the kernels' constant tables; make that
- * first call before any stream capture.  Calls share the array, so calls whose
- * device work overlaps race.  The call synchronises `stream` before returning. */
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory while they run: an in-situ step inside a simulation whose memory
+ * manager owns the whole device, or a serving loop held to a fixed memory
+ * budget that cannot absorb cudaMalloc's implicit synchronisation.  It runs
+ * the fused regular-mesh extraction on `stream` and writes the accepted
+ * simplices, unsorted, to caller-provided device memory: canonical keys
+ * (corner vertex id * n_types + chain rank) and 4 doubles of barycentrics per
+ * feature; `count` is a device word the call uses as its atomic counter, and
+ * *n_features receives the number found.  Field pointers must be device
+ * pointers.  Scratch is a static device array of ~9.3 MiB that every GPU
+ * loading the library holds until exit.  Limits: capacity <= 262144 features
+ * (FTK2B_INVALID_ARG beyond it); more features than `capacity` returns
+ * FTK2B_OVERFLOW_RETRY with the count found (retry with a larger output);
+ * more than 262144 surviving hypercubes returns FTK2B_UNSUPPORTED (no retry
+ * can succeed: split the box into sub-boxes).  The first call on a device
+ * looks up the array's device address and uploads the kernels' constant
+ * tables; make that first call before any stream capture.  Calls share the
+ * array, so calls whose device work overlaps race.  The call waits for
+ * `stream` before returning. */
 ftk2b_status ftk2b_cp_features_noalloc(const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
                                        double sos_q, void* stream, uint64_t* keys, double* lambda,
                                        uint32_t capacity, uint32_t* count, uint64_t* n_features);
