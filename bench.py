@@ -518,6 +518,36 @@ def batched_c3(ctx, steps=5, check=True):
     return out
 
 
+def north_star_summary(line):
+    """The targets of the workload set in one short object, printed last on
+    the line: HBM roofline fractions of the plain FP64 drop-in (128^3 x 16)
+    and of the 256^3 x 8 float32 workload (extraction kernels alone and whole
+    step), the refined-FP32 form against the plain FP64 drop-in on the same
+    field, its position error, the batch and serving figures."""
+    peak = line["roofline"]["peak"]
+    p = line.get("precision", {})
+    b = line.get("batched", {})
+    sv = line.get("serve", {})
+    alg32 = 3 * 4 * 256 ** 3 * 8
+    r32 = p.get("refined_fp32", {})
+    out = {
+        "peak_gbs": peak,
+        "c2_extract_frac": line["roofline"]["frac"],
+        "c2_step_frac": line["roofline"]["algorithmic_bytes"] / (line["ms_per_step"] / 1e3) / 1e9 / peak,
+        "c4_extract_frac": r32.get("hbm_frac_extract"),
+        "c4_step_frac": alg32 / (r32["ms_per_step"] / 1e3) / 1e9 / peak if r32 else None,
+        "c4_refined_vs_fp64_same_field": p.get("speedup_refined_vs_fp64"),
+        "c4_refined_max_pos_err": p.get("position_error_grid_units", {}).get("refined_max"),
+        "c4_sets_differ": (p.get("sets", {}).get("fp32_only"), p.get("sets", {}).get("fp64_only")),
+        "c3_cull_frac": b.get("batched", {}).get("cull_hbm_gbs", 0.0) / peak if b else None,
+        "c3_batched_vs_plain": b.get("speedup_batched_vs_plain"),
+        "c3_identical": b.get("identical_to_plain"),
+        "serve_p50_p99_ms": (sv.get("p50_ms"), sv.get("p99_ms")),
+        "serve_req_s": sv.get("throughput_req_s"),
+    }
+    return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in out.items()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -652,6 +682,7 @@ def main():
         line["contour"] = contour_c2(ctx)
         torch.cuda.empty_cache()
         line["fiber_surface"] = fiber_surface_bench(ctx)
+        line["north_star"] = north_star_summary(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -40,6 +40,7 @@ OPT_FEATURE_CAPACITY, OPT_TIME_CHUNK, OPT_DISABLE_TMA, OPT_USE_GRAPHS = 1, 2, 3,
 INFO_LAST_TMA = 100
 INFO_LAST_CULL_MODE = 101
 INFO_LAST_BATCH_TIME_CHUNK = 102
+INFO_LAST_CANDIDATES = 103
 OPT_BLOCKING_SYNC = 5
 OPT_CULL_MODE = 6
 OPT_BATCH_TIME_CHUNK = 7

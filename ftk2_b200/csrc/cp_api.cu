@@ -233,6 +233,7 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_DISABLE_TMA: *value = ctx->disable_tma ? 1 : 0; return FTK2B_OK;
     case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
     case FTK2B_INFO_LAST_CULL_MODE: *value = ctx->last_cull_mode; return FTK2B_OK;
+    case FTK2B_INFO_LAST_CANDIDATES: *value = (int64_t)ctx->last_candidates; return FTK2B_OK;
     case FTK2B_INFO_LAST_BATCH_TIME_CHUNK: *value = ctx->batch.last_tchunk; return FTK2B_OK;
     case FTK2B_OPT_USE_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return FTK2B_OK;
     case FTK2B_OPT_BLOCKING_SYNC: *value = ctx->blocking_sync ? 1 : 0; return FTK2B_OK;
@@ -494,6 +495,7 @@ PostBuffers ftk2b_ctx::post_buffers(unsigned cap_, unsigned edge_cap_, int key_b
   B.edge_cap = edge_cap_;
   B.key_bits = key_bits;
   B.sort_grid = sort_grid(cap_);
+  B.num_sms = num_sms;
   B.key = (unsigned long long*)key.p;
   B.lam = (double*)lam.p;
   B.bary4 = (float*)bary4.p;
@@ -668,9 +670,10 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   cfg.tiles[1] = (int)((rm.ld[1] + TY - 1) / TY);
   cfg.tiles[2] = (d == 4) ? (int)((rm.ld[2] + TZ - 1) / TZ) : 1;
 
-  // feature capacity: starts small (sorting cost scales with it) and grows
-  // on overflow; the context remembers the grown value
-  unsigned cap = ctx->cap_hint ? ctx->cap_hint : 65536u;
+  // feature capacity: starts small (sorting cost scales with it; up to
+  // kSmallPostCap the short post-extraction chain runs) and grows on
+  // overflow; the context remembers the grown value
+  unsigned cap = ctx->cap_hint ? ctx->cap_hint : kSmallPostCap;
   unsigned ccap = ctx->cand_cap_hint ? ctx->cand_cap_hint : 65536u;
   if (fiber_thr) {  // every local vertex is a candidate corner
     uint64_t nloc = 1;
@@ -841,6 +844,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     if (cudaEventElapsedTime(&xms, ctx->ev0, ctx->ev_x) != cudaSuccess) xms = 0.f;
     cudaGetLastError();  // a failed timing query must not linger in the error slot
     ctx->last_extract_ms = xms;
+    ctx->last_candidates = h[kCountCand];
     if (h[kCountErr] & 2u) return fail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return fail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
     if (h[kCountCand] > ccap) {

@@ -538,9 +538,201 @@ static int grid_for(unsigned cap, int threads, int max_blocks) {
   return (int)b;
 }
 
+// ---------------------------------------------------------------------------
+// Post-extraction for small feature counts (capacity <= kSmallPostCap): the
+// outputs of the general chain above in three launches.
+//   1. rank sort: every block holds all n keys in shared memory; the canonical
+//      position of a key is the number of keys below it (the keys of one
+//      extraction are distinct).  The block writes, at that position, its
+//      keys' sorted key, lambdas, float barycentrics, scalar and vertex ids.
+//   2. star edges: one warp per feature (edges_of_feature) with the sorted
+//      keys in shared memory.
+//   3. one block: exclusive scan of the edge counts, edge compaction, the
+//      union-find over the edges in shared memory, track ids and root count.
+
+constexpr int kRankThreads = 1024;
+constexpr int kRankMaxR = 8;  // keys per lane of a rank-sort block
+
+template <int R>
+__device__ __forceinline__ void rank_keys(const unsigned long long* sk, unsigned n, unsigned base, int lane,
+                                          int warp, unsigned (*part)[kRankMaxR][32]) {
+  unsigned long long mine[R];
+  unsigned cnt[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const unsigned i = base + lane + 32u * r;
+    mine[r] = i < n ? sk[i] : ~0ull;
+    cnt[r] = 0;
+  }
+  // warp w counts the keys of its segment below each of the lane's keys
+  const unsigned seg = (n + 31) / 32;
+  const unsigned j0 = min(n, warp * seg), j1 = min(n, j0 + seg);
+  for (unsigned j = j0; j < j1; ++j) {
+    const unsigned long long kj = sk[j];
+#pragma unroll
+    for (int r = 0; r < R; ++r) cnt[r] += kj < mine[r] ? 1u : 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) part[warp][r][lane] = cnt[r];
+}
+
+__global__ void __launch_bounds__(kRankThreads, 1)
+    small_rank_sort_kernel(RegularMesh mesh, int nch, PostBuffers B) {
+  pdl_enter();
+  extern __shared__ unsigned long long sk[];  // the n unsorted keys
+  __shared__ unsigned part[32][kRankMaxR][32];
+  const unsigned n = min(*B.count, B.cap);
+  const unsigned G = gridDim.x;
+  const unsigned R = (n + 32u * G - 1) / (32u * G);  // keys per lane
+  const unsigned base = blockIdx.x * 32u * R;
+  if (n == 0 || base >= n) return;
+  if (R > kRankMaxR) {  // the host sizes the grid so that this cannot happen
+    if (threadIdx.x == 0) atomicOr(B.err, 4u);
+    return;
+  }
+  for (unsigned i = threadIdx.x; i < n; i += kRankThreads) sk[i] = B.key[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (R == 1) rank_keys<1>(sk, n, base, lane, warp, part);
+  else if (R == 2) rank_keys<2>(sk, n, base, lane, warp, part);
+  else if (R <= 4) rank_keys<4>(sk, n, base, lane, warp, part);
+  else rank_keys<8>(sk, n, base, lane, warp, part);
+  __syncthreads();
+  if (threadIdx.x >= 32u * R) return;
+  const int r = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const unsigned i = base + l + 32u * r;
+  if (i >= n) return;
+  unsigned pos = 0;
+#pragma unroll 8
+  for (int w = 0; w < 32; ++w) pos += part[w][r][l];
+  const unsigned long long key = sk[i];
+  B.key_alt[pos] = key;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    B.lam_sorted[4 * (size_t)pos + k] = B.lam[4 * (size_t)i + k];
+    B.bary4_sorted[4 * (size_t)pos + k] = B.bary4[4 * (size_t)i + k];
+  }
+  B.scalar_sorted[pos] = B.scalar[i];
+  expand_feature(mesh, nch, key, pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
+}
+
+__global__ void __launch_bounds__(kRankThreads, 1)
+    small_edges_kernel(RegularMesh mesh, int nch, PostBuffers B) {
+  pdl_enter();
+  extern __shared__ unsigned long long sk[];  // the n sorted keys
+  const unsigned n = min(*B.count, B.cap);
+  for (unsigned i = threadIdx.x; i < n; i += kRankThreads) sk[i] = B.key_alt[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned gw = (blockIdx.x * kRankThreads + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * kRankThreads) >> 5;
+  for (unsigned i = gw; i < n; i += nw) edges_of_feature(mesh, nch, sk, n, i, sk[i], 0ull, lane, B.edge_cnt, B.edge_slots);
+}
+
+// union-find in shared memory: the global version's links (larger root under
+// the smaller one) with shared-memory atomics
+__device__ __forceinline__ unsigned uf_root_shared(unsigned* parent, unsigned x) {
+  volatile unsigned* vp = parent;
+  unsigned p = vp[x];
+  while (p != x) {
+    const unsigned gp = vp[p];
+    if (gp < p) atomicMin(&parent[x], gp);
+    x = p;
+    p = gp;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void uf_unite_shared(unsigned* parent, unsigned a, unsigned b, unsigned* err) {
+  for (int it = 0; it < (1 << 20); ++it) {
+    const unsigned ra = uf_root_shared(parent, a), rb = uf_root_shared(parent, b);
+    if (ra == rb) return;
+    const unsigned lo = min(ra, rb), hi = max(ra, rb);
+    if (atomicCAS(&parent[hi], hi, lo) == hi) return;
+    a = ra;
+    b = rb;
+  }
+  atomicOr(err, 1u);
+}
+
+__global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
+  pdl_enter();
+  extern __shared__ unsigned sp[];  // union-find parents of the n features
+  __shared__ unsigned part[1024];
+  __shared__ unsigned s_roots;
+  const unsigned n = min(*B.count, B.cap);
+  const unsigned t = threadIdx.x;
+  // exclusive scan of the per-feature edge counts, in place
+  const unsigned seg = (n + 1023) / 1024;
+  const unsigned s0 = min(t * seg, n), s1 = min(s0 + seg, n);
+  unsigned sum = 0;
+  for (unsigned i = s0; i < s1; ++i) sum += B.edge_cnt[i];
+  part[t] = sum;
+  for (unsigned i = t; i < n; i += 1024) sp[i] = i;
+  if (t == 0) s_roots = 0;
+  __syncthreads();
+  for (unsigned off = 1; off < 1024; off <<= 1) {
+    const unsigned v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  const unsigned total = part[1023];
+  unsigned run = part[t] - sum;
+  // each thread writes its features' edges at their offsets and unites them
+  for (unsigned i = s0; i < s1; ++i) {
+    const unsigned c = B.edge_cnt[i];
+    B.edge_cnt[i] = run;
+    for (unsigned k = 0; k < c; ++k) {
+      const unsigned other = B.edge_slots[(size_t)i * kEdgeSlots + k];
+      if (run + k < B.edge_cap) {
+        B.edges[2 * (size_t)(run + k)] = i;
+        B.edges[2 * (size_t)(run + k) + 1] = other;
+      }
+      uf_unite_shared(sp, i, other, B.err);
+    }
+    run += c;
+  }
+  if (t == 1023) *B.n_edges = total;
+  __syncthreads();
+  unsigned roots = 0;
+  for (unsigned i = t; i < n; i += 1024) {
+    const unsigned x = uf_root_shared(sp, i);
+    B.track[i] = x;
+    roots += x == i ? 1u : 0u;
+  }
+  atomicAdd(&s_roots, roots);
+  __syncthreads();
+  if (t == 0) *B.n_roots = s_roots;
+}
+
+static cudaError_t launch_post_small(const RegularMesh& mesh, int nch, const PostBuffers& B, int want_edges,
+                                     cudaStream_t st, unsigned long long* launches) {
+  const unsigned cap = B.cap;
+  const size_t key_smem = sizeof(unsigned long long) * (size_t)(cap ? cap : 1);
+  int g1 = B.num_sms > 0 ? B.num_sms : 148;
+  const int need = (int)((cap + 32u * kRankMaxR - 1) / (32u * kRankMaxR));
+  if (g1 < need) g1 = need;
+  cudaError_t e = cudaFuncSetAttribute(small_rank_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)key_smem);
+  if (!e) e = launch_pdl(small_rank_sort_kernel, g1, kRankThreads, key_smem, st, mesh, nch, B);
+  if (e) return e;
+  *launches += 1;
+  if (!want_edges) return cudaGetLastError();
+  e = cudaFuncSetAttribute(small_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
+  if (!e) e = launch_pdl(small_edges_kernel, B.num_sms > 0 ? B.num_sms : 148, kRankThreads, key_smem, st, mesh, nch, B);
+  if (e) return e;
+  const size_t uf_smem = sizeof(unsigned) * (size_t)(cap ? cap : 1);
+  e = cudaFuncSetAttribute(small_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uf_smem);
+  if (!e) e = launch_pdl(small_finish_kernel, 1, 1024, uf_smem, st, B);
+  *launches += 2;
+  return e ? e : cudaGetLastError();
+}
+
 cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuffers& B,
                                 int want_edges, cudaStream_t st, unsigned long long* launches) {
   const unsigned cap = B.cap;
+  if (cap <= kSmallPostCap) return launch_post_small(mesh, nch, B, want_edges, st, launches);
   const int gsort = B.sort_grid;
   const int g = grid_for(cap, 256, 4096);
   // keys in canonical order: multi-block stable LSD radix passes

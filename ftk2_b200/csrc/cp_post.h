@@ -5,8 +5,13 @@
 
 namespace ftk2b {
 
+// Feature capacities up to this run the short post-extraction chain (rank
+// sort, star edges, one-block union-find); larger ones the radix-sort chain.
+constexpr unsigned kSmallPostCap = 16384;
+
 struct PostBuffers {
   unsigned cap;                     // feature capacity
+  int num_sms;
   unsigned edge_cap;
   int key_bits;                     // significant bits of the canonical keys
   int sort_grid;

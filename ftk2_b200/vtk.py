@@ -10,13 +10,16 @@ point arrays Scalar (Float32), TrackID (Int32), Type (Int32) and Time
 spatial one, else 0).  Connectivity: CPResult star edges (dimension 1),
 ContourResult manifold cells (dimension = cell width - 1), or an explicit
 `connectivity` list of (dimension, flat indices) on the result.  ASCII when
-use_ascii is set or FTK_DEBUG is in the environment, else appended raw binary
-with UInt64 block headers.  read_vtu loads an unstructured base mesh as the
+use_ascii is set or FTK_DEBUG is in the environment, else appended data in
+base64 with UInt64 block headers and no compression, as the reference sets up
+VTK's writer (utils/vtk.hpp:102-108, 150-156): per array the base64 of its
+length header, then the base64 of its bytes, each padded on its own.  read_vtu loads an unstructured base mesh as the
 reference's read_vtu does (utils/vtk.hpp:165-192), same result as the C++
 header's.
 """
 from __future__ import annotations
 
+import base64
 import io
 import os
 from typing import List, Tuple
@@ -74,7 +77,7 @@ class _Writer:
         if not self.ascii:
             w(f' format="appended" offset="{len(self.appended)}"/>\n')
             raw = np.ascontiguousarray(a).tobytes()
-            self.appended += np.array([len(raw)], "<u8").tobytes() + raw
+            self.appended += base64.b64encode(np.array([len(raw)], "<u8").tobytes()) + base64.b64encode(raw)
             return
         w(' format="ascii">\n')
         vals = ["%.9g" % float(v) for v in a] if vtype == "Float32" else [str(int(v)) for v in a]
@@ -90,7 +93,7 @@ class _Writer:
                      f'header_type="UInt64">\n').encode())
             f.write(self.body.getvalue().encode())
             if not self.ascii:
-                f.write(b'  <AppendedData encoding="raw">\n   _' + bytes(self.appended) + b"\n  </AppendedData>\n")
+                f.write(b'  <AppendedData encoding="base64">\n   _' + bytes(self.appended) + b"\n  </AppendedData>\n")
             f.write(b"</VTKFile>\n")
 
 

@@ -119,7 +119,8 @@ def main():
             x, tot, _ = ctx.last_timing()
             print(f"step {i}: {n} features {ne} edges  extract {x:.3f} ms  pipeline {tot:.3f} ms  "
                   f"host {1e3 * (time.perf_counter() - t):.3f} ms  tma={ctx.get_option(api.INFO_LAST_TMA)}  "
-                  f"cull_mode={ctx.get_option(api.INFO_LAST_CULL_MODE)}", flush=True)
+                  f"cull_mode={ctx.get_option(api.INFO_LAST_CULL_MODE)}  "
+                  f"candidates={ctx.get_option(api.INFO_LAST_CANDIDATES)}", flush=True)
 
 
 if __name__ == "__main__":

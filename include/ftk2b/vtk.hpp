@@ -15,10 +15,13 @@
 // VTK_VERTEX / LINE / TRIANGLE / TETRA cells, or one VTK_VERTEX per feature
 // for target_dim 0.  A target_dim other than -1 keeps that dimension only.
 //
-// Encoding: ASCII when use_ascii is set or FTK_DEBUG is in the environment
-// (as the reference), else appended raw binary with UInt64 block headers
-// (the reference's VTK writer appends base64 text; raw is the same data
-// model, 25% smaller and needs no encoder).  read_vtu reads single-piece
+// Encoding: ASCII when use_ascii is set or FTK_DEBUG is in the environment,
+// else appended data encoded as base64 with UInt64 block headers and no
+// compression, as the reference configures VTK's writer (SetDataModeToAppended,
+// SetEncodeAppendedData(1), SetCompressorTypeToNone; utils/vtk.hpp:102-108,
+// 150-156): per array, the base64 of its 8-byte length header followed by the
+// base64 of its bytes, each padded on its own, offsets counted in characters
+// of the encoded text after the '_' marker.  read_vtu reads single-piece
 // little-endian files in ASCII, inline base64, appended base64 and appended
 // raw form, uncompressed, as utils/vtk.hpp:165-192 does through VTK: points,
 // and the triangles and tetrahedra among the cells (other cells skipped),
@@ -88,10 +91,8 @@ class Writer {
     if (!ascii_) {
       body << " format=\"appended\" offset=\"" << appended_.size() << "\"/>\n";
       const uint64_t nb = a.size() * sizeof(E);
-      const char* h = reinterpret_cast<const char*>(&nb);
-      appended_.insert(appended_.end(), h, h + 8);
-      const char* d = reinterpret_cast<const char*>(a.data());
-      appended_.insert(appended_.end(), d, d + nb);
+      b64(reinterpret_cast<const uint8_t*>(&nb), 8);
+      b64(reinterpret_cast<const uint8_t*>(a.data()), nb);
       return;
     }
     body << " format=\"ascii\">\n";
@@ -111,7 +112,7 @@ class Writer {
       << "\" version=\"1.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\">\n";
     f << body.str();
     if (!ascii_) {
-      f << "  <AppendedData encoding=\"raw\">\n   _";
+      f << "  <AppendedData encoding=\"base64\">\n   _";
       f.write(appended_.data(), (std::streamsize)appended_.size());
       f << "\n  </AppendedData>\n";
     }
@@ -120,6 +121,18 @@ class Writer {
   }
 
  private:
+  // appends the base64 text of n bytes, padded with '=' to whole quanta
+  void b64(const uint8_t* d, uint64_t n) {
+    static const char* A = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
+    for (uint64_t i = 0; i < n; i += 3) {
+      const uint32_t b0 = d[i], b1 = i + 1 < n ? d[i + 1] : 0, b2 = i + 2 < n ? d[i + 2] : 0;
+      const uint32_t w = b0 << 16 | b1 << 8 | b2;
+      appended_.push_back(A[(w >> 18) & 63]);
+      appended_.push_back(A[(w >> 12) & 63]);
+      appended_.push_back(i + 1 < n ? A[(w >> 6) & 63] : '=');
+      appended_.push_back(i + 2 < n ? A[w & 63] : '=');
+    }
+  }
   static void fmt(char* b, float v) { std::snprintf(b, 32, "%.9g", (double)v); }
   static void fmt(char* b, int32_t v) { std::snprintf(b, 32, "%d", v); }
   static void fmt(char* b, int64_t v) { std::snprintf(b, 32, "%lld", (long long)v); }

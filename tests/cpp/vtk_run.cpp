@@ -90,11 +90,11 @@ int main(int argc, char** argv) {
       const FeatureComplex c = read_complex(in);
       const std::string d = argv[3];
       write_complex_to_vtp(c, *mesh, d + "/all_ascii.vtp", -1, true);
-      write_complex_to_vtp(c, *mesh, d + "/all_raw.vtp");
+      write_complex_to_vtp(c, *mesh, d + "/all_bin.vtp");
       write_complex_to_vtp(c, *mesh, d + "/dim1_ascii.vtp", 1, true);
       write_complex_to_vtu(c, *mesh, d + "/all_ascii.vtu", -1, true);
-      write_complex_to_vtu(c, *mesh, d + "/all_raw.vtu");
-      write_complex_to_vtu(c, *mesh, d + "/dim0_raw.vtu", 0);
+      write_complex_to_vtu(c, *mesh, d + "/all_bin.vtu");
+      write_complex_to_vtu(c, *mesh, d + "/dim0_bin.vtu", 0);
       write_complex_to_vtu(c, *mesh, d + "/dim3_ascii.vtu", 3, true);
       return 0;
     }

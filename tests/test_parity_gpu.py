@@ -327,3 +327,31 @@ def test_cull_autotuner_keeps_its_choice(ctx):
         assert_identical(gpu_run(ctx, case), first)
         assert ctx.get_option(api.INFO_LAST_CULL_MODE) == mode
     assert_identical(first, oracle_run(case))
+
+
+def test_short_and_radix_post_chains_agree(ctx):
+    # feature capacities up to 16384 run the short post-extraction chain (rank
+    # sort, star edges, one-block union-find), larger ones the radix-sort chain
+    for case in _medium_cases()[:3] + [cases.c1_analytic_2d()]:
+        short = gpu_run(ctx, case)
+        ctx.set_option(api.OPT_FEATURE_CAPACITY, 20000)
+        try:
+            radix = gpu_run(ctx, case)
+        finally:
+            ctx.set_option(api.OPT_FEATURE_CAPACITY, 0)
+        assert_identical(short, radix)
+        assert_identical(short, oracle_run(case))
+
+
+def test_many_features_grow_past_the_short_chain():
+    # a noise field with more features than the short chain holds: the first
+    # attempt overflows its capacity and the retry runs the radix-sort chain
+    rng = np.random.default_rng(3)
+    g = np.ascontiguousarray(rng.standard_normal((3, 18, 20, 24, 3)).astype(np.float32))
+    case = cases.Case("noise", "regular", 3, cases.MULTI, g, 2.0 ** 20, [24, 20, 18, 3])
+    with api.Context(0) as c:
+        r = gpu_run(c, case)
+        assert c.get_option(api.OPT_FEATURE_CAPACITY) > 16384
+    assert len(r.track_id) > 16384
+    assert_identical(r, oracle_run(case))
+

@@ -151,10 +151,11 @@ def expected_points(mesh, feats):
 
 def parse_vtk(path):
     """{(section, name): array} and the Piece attributes of an ASCII or
-    appended-raw VTK XML file."""
+    appended-base64 VTK XML file (each array's length header and its bytes
+    encoded apart, as VTK's writer does without compression)."""
     data = open(path, "rb").read()
-    head, sep, tail = data.partition(b'<AppendedData encoding="raw">')
-    app = tail[tail.index(b"_") + 1:] if sep else None
+    head, sep, tail = data.partition(b'<AppendedData encoding="base64">')
+    app = tail[tail.index(b"_") + 1:tail.index(b"\n  </AppendedData>")] if sep else None
     text = head.decode()
     piece = dict(re.findall(r'(\w+)="([^"]*)"', re.search(r"<Piece ([^>]*)>", text).group(1)))
     out, section = {}, None
@@ -170,8 +171,10 @@ def parse_vtk(path):
             a = np.array(body.split(), dtype=np.float64).astype(dt) if body.split() else np.zeros(0, dt)
         else:
             off = int(at["offset"])
-            nb = int(np.frombuffer(app[off:off + 8], "<u8")[0])
-            a = np.frombuffer(app[off + 8:off + 8 + nb], dt)
+            nb = int(np.frombuffer(base64.b64decode(app[off:off + 12]), "<u8")[0])
+            text = app[off + 12:off + 12 + 4 * ((nb + 2) // 3)]
+            assert all(c in b"ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/=" for c in text)
+            a = np.frombuffer(base64.b64decode(text), dt)
         out[(section, at["Name"])] = a
     return out, piece
 
@@ -211,7 +214,7 @@ def test_writers_match_reference_content(vtk_run, tmp_path, name):
     mesh, feats, conn = CASES[name](np.random.default_rng(len(name)))
     (tmp_path / "case.txt").write_text(case_text(mesh, feats, conn))
     subprocess.run([vtk_run, "write", str(tmp_path / "case.txt"), str(tmp_path)], check=True)
-    for f in ("all_ascii.vtp", "all_raw.vtp"):
+    for f in ("all_ascii.vtp", "all_bin.vtp"):
         got, piece = parse_vtk(tmp_path / f)
         check_points(got, mesh, feats)
         for sec, dim in (("Verts", 0), ("Lines", 1), ("Polys", 2)):
@@ -223,7 +226,7 @@ def test_writers_match_reference_content(vtk_run, tmp_path, name):
     got, _ = parse_vtk(tmp_path / "dim1_ascii.vtp")
     assert got[("Lines", "connectivity")].tolist() == expected_cells(conn, {1})[0]
     assert got[("Verts", "connectivity")].size == 0 and got[("Polys", "connectivity")].size == 0
-    for f, kept in (("all_ascii.vtu", {0, 1, 2, 3}), ("all_raw.vtu", {0, 1, 2, 3}), ("dim3_ascii.vtu", {3})):
+    for f, kept in (("all_ascii.vtu", {0, 1, 2, 3}), ("all_bin.vtu", {0, 1, 2, 3}), ("dim3_ascii.vtu", {3})):
         got, piece = parse_vtk(tmp_path / f)
         check_points(got, mesh, feats)
         ids, offs, types = expected_cells(conn, kept)
@@ -231,7 +234,7 @@ def test_writers_match_reference_content(vtk_run, tmp_path, name):
         assert got[("Cells", "offsets")].tolist() == offs, f
         assert got[("Cells", "types")].tolist() == types, f
         assert int(piece["NumberOfCells"]) == len(types)
-    got, piece = parse_vtk(tmp_path / "dim0_raw.vtu")
+    got, piece = parse_vtk(tmp_path / "dim0_bin.vtu")
     n = len(feats)
     assert got[("Cells", "connectivity")].tolist() == list(range(n))
     assert got[("Cells", "types")].tolist() == [1] * n and got[("Cells", "offsets")].tolist() == list(range(1, n + 1))
@@ -242,8 +245,8 @@ def test_ftk_debug_forces_ascii(vtk_run, tmp_path):
     (tmp_path / "case.txt").write_text(case_text(mesh, feats, conn))
     subprocess.run([vtk_run, "write", str(tmp_path / "case.txt"), str(tmp_path)], check=True,
                    env=dict(os.environ, FTK_DEBUG="1"))
-    assert b"AppendedData" not in (tmp_path / "all_raw.vtu").read_bytes()
-    got, _ = parse_vtk(tmp_path / "all_raw.vtu")
+    assert b"AppendedData" not in (tmp_path / "all_bin.vtu").read_bytes()
+    got, _ = parse_vtk(tmp_path / "all_bin.vtu")
     check_points(got, mesh, feats)
 
 
@@ -335,7 +338,7 @@ def test_read_vtu_round_trip_and_missing_file(vtk_run, tmp_path):
     (tmp_path / "case.txt").write_text(case_text(mesh, feats, conn))
     subprocess.run([vtk_run, "write", str(tmp_path / "case.txt"), str(tmp_path)], check=True)
     xyz, _ = expected_points(mesh, feats)
-    for f in ("all_raw.vtu", "dim3_ascii.vtu"):
+    for f in ("all_bin.vtu", "dim3_ascii.vtu"):
         sd, cd, coords, got = run_read(vtk_run, tmp_path / f)
         assert np.array_equal(coords, xyz.astype(np.float64))
         ids, _, types = expected_cells(conn, {3} if "dim3" in f else {2, 3})
@@ -346,7 +349,7 @@ def test_read_vtu_round_trip_and_missing_file(vtk_run, tmp_path):
     assert r.returncode == 0 and r.stdout.strip() == "none"
     from ftk2_b200 import vtk
     assert vtk.read_vtu(str(tmp_path / "absent.vtu")) is None
-    m = vtk.read_vtu(str(tmp_path / "all_raw.vtu"))  # mixed triangles and tetrahedra: flat ids
+    m = vtk.read_vtu(str(tmp_path / "all_bin.vtu"))  # mixed triangles and tetrahedra: flat ids
     assert np.array_equal(m.coords, xyz.astype(np.float64))
     assert m.cells.tolist() == expected_cells(conn, {2, 3})[0]
     (tmp_path / "z.vtu").write_text('<?xml version="1.0"?>\n<VTKFile type="UnstructuredGrid" '
@@ -386,11 +389,11 @@ def test_python_writer_is_byte_identical(vtk_run, tmp_path, name):
     py = tmp_path / "py"
     py.mkdir()
     vtk.write_complex_to_vtp(r, m, str(py / "all_ascii.vtp"), -1, True)
-    vtk.write_complex_to_vtp(r, m, str(py / "all_raw.vtp"))
+    vtk.write_complex_to_vtp(r, m, str(py / "all_bin.vtp"))
     vtk.write_complex_to_vtp(r, m, str(py / "dim1_ascii.vtp"), 1, True)
     vtk.write_complex_to_vtu(r, m, str(py / "all_ascii.vtu"), -1, True)
-    vtk.write_complex_to_vtu(r, m, str(py / "all_raw.vtu"))
-    vtk.write_complex_to_vtu(r, m, str(py / "dim0_raw.vtu"), 0)
+    vtk.write_complex_to_vtu(r, m, str(py / "all_bin.vtu"))
+    vtk.write_complex_to_vtu(r, m, str(py / "dim0_bin.vtu"), 0)
     vtk.write_complex_to_vtu(r, m, str(py / "dim3_ascii.vtu"), 3, True)
     for f in sorted(os.listdir(py)):
         assert (py / f).read_bytes() == (tmp_path / f).read_bytes(), f
