@@ -73,6 +73,15 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return false;
 }
 
+// Untiled bulk copy global -> shared (both addresses and the size multiples
+// of 16 bytes), completing on the mbarrier's transaction count.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
                                             unsigned long long* bar) {
   asm volatile(
@@ -159,7 +168,15 @@ struct Geo {
   static constexpr int VXBOX = vxbox_of(MULTI, M, (int)sizeof(T));
   static constexpr int COMP_RAW = VXBOX * VY * VZ * (int)sizeof(T);  // bytes of one component box
   static constexpr int COMP = round128(COMP_RAW);
-  static constexpr int BYTES = MULTI ? round128(COMP_RAW * M) : COMP * M;  // one slice buffer
+  static constexpr int BOX_BYTES = MULTI ? round128(COMP_RAW * M) : COMP * M;
+  // bulk row staging (arrays a TMA tensor map cannot describe): box row r of
+  // a slice goes to bytes [r * ROWB, (r + 1) * ROWB) of the buffer, its data
+  // starting at the row's source address mod 16 (rows component-major for
+  // separate arrays)
+  static constexpr int ROWS = VY * VZ * (MULTI ? 1 : M);
+  static constexpr int ROWB = ((VX * (MULTI ? M : 1) * (int)sizeof(T) + 15) & ~15) + 32;
+  static constexpr int BULK_BYTES = round128(ROWS * ROWB);
+  static constexpr int BYTES = BOX_BYTES > BULK_BYTES ? BOX_BYTES : BULK_BYTES;  // one slice buffer
   static constexpr int TX_BYTES = COMP_RAW * M;                          // bytes TMA delivers
   static constexpr int COMP_ELEMS = COMP / (int)sizeof(T);
   static constexpr int WORDS = 2 * BYTES;                                // offset of the word slots
@@ -221,18 +238,38 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // two-slot ring stores timestep t in slot t & 1; tflip = 0 otherwise)
   auto tcoord = [&](int s) { return (s + aoff[D - 1]) ^ fa.tflip; };
 
+  // bulk row copies stage arrays that TMA cannot describe (rows not 16-byte
+  // multiples, misaligned offsets); per-vertex arrays keep element copies
+  const bool bulk = !TMA && !fa.per_vertex;
+  const bool mbar = TMA || bulk;
+
   // per-thread vertex slots of a slice, fixed for the whole time march:
-  // element offset of component 0 in a slice buffer and a validity bit
+  // element offset of component 0 in a slice buffer (bulk staging: byte
+  // offset from the row's slot, and the row's source offset mod 16 without
+  // the time term, 4 bits per slot) and a validity bit
   int voff[VPT];
-  unsigned vvalid = 0;
+  unsigned vvalid = 0, vshift = 0;
 #pragma unroll
   for (int u = 0; u < VPT; ++u) {
     const int i = tid + u * kThreads;
     const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
     const bool in = i < VS && x0 + vx < ldx && y0 + vy < ldy && (D == 3 || z0 + vz < ldz);
-    voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
+    if (bulk) {
+      voff[u] = in ? (vz * VY + vy) * G::ROWB + vx * (MULTI ? M : 1) * (int)sizeof(T) : 0;
+      long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
+      if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
+      vshift |= (unsigned)((e * (long long)sizeof(T)) & 15) << (4 * u);
+    } else {
+      voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
+    }
     vvalid |= (in ? 1u : 0u) << u;
   }
+  // source address mod 16 of each array, and the time axis' element stride
+  unsigned pbase = 0;
+#pragma unroll
+  for (int j = 0; j < (MULTI ? 1 : M); ++j)
+    pbase |= (unsigned)(reinterpret_cast<uintptr_t>(fa.comp[j]) & 15) << (4 * j);
+  const long long tstride = fa.estride[D - 1];
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
@@ -255,6 +292,49 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
             else
               tma_load_3d(dst0 + j * G::COMP, maps[j], cx, cy, tcoord(s), &bar[buf]);
           }
+        }
+      }
+    } else if (bulk) {
+      // warp 0: one bulk copy per box row holding vertices of the local
+      // mesh, from the 16-byte block of its first element to the block of
+      // its last (an aligned 16-byte block never crosses a page, so the
+      // bytes read around the row lie in pages the row occupies); the rows'
+      // byte total goes to the mbarrier before any copy is issued
+      if (warp == 0) {
+        const long long at = (long long)tcoord(s);
+        const int nvx = min(VX, ldx - x0);
+        const int rbytes = nvx * (MULTI ? M : 1) * (int)sizeof(T);
+        auto row_src = [&](int r, uintptr_t& lo, unsigned& n) {
+          const int rr = MULTI ? r : r % (VY * VZ);
+          const int j = MULTI ? 0 : r / (VY * VZ);
+          const int vy = rr % VY, vz = rr / VY;
+          n = 0;
+          lo = 0;
+          if (y0 + vy >= ldy || (D == 4 && z0 + vz >= ldz)) return;
+          long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
+          if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
+          e += at * tstride;
+          const uintptr_t src = reinterpret_cast<uintptr_t>(fa.comp[j]) + (uintptr_t)(e * (long long)sizeof(T));
+          lo = src & ~(uintptr_t)15;
+          n = (unsigned)(((src + (uintptr_t)rbytes + 15) & ~(uintptr_t)15) - lo);
+        };
+        unsigned total = 0;
+        for (int r = lane; r < G::ROWS; r += 32) {
+          uintptr_t lo;
+          unsigned n;
+          row_src(r, lo, n);
+          total += n;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xFFFFFFFFu, total, o);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (lane == 0) mbar_expect_tx(&bar[buf], total);
+        __syncwarp();
+        for (int r = lane; r < G::ROWS; r += 32) {
+          uintptr_t lo;
+          unsigned n;
+          row_src(r, lo, n);
+          if (n) bulk_load(dst0 + r * G::ROWB, reinterpret_cast<const void*>(lo), n, &bar[buf]);
         }
       }
     } else {
@@ -323,7 +403,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // every thread waits for the slice's TMA phase itself (try_wait suspends
   // in hardware); returns false when the bounded wait gave up
   auto wait = [&](int s, int buf) -> bool {
-    if constexpr (TMA) {
+    if (mbar) {
       return mbar_wait(&bar[buf], (ph[buf] + (unsigned)((s - t0) >> 1)) & 1u);
     } else {
       // slice s + 1 (when it exists) was issued after s: one group may stay
@@ -334,9 +414,27 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       return true;
     }
   };
-  auto words = [&](int buf, int slot) {
+  auto words = [&](int buf, int slot, int s) {
     const unsigned* r = reinterpret_cast<const unsigned*>(smem + buf * G::BYTES) + (HW - 1);
     unsigned* dst = Wb + slot * VSP;
+    if (bulk) {
+      const unsigned char* rb = smem + buf * G::BYTES + 4 * (HW - 1);
+      const unsigned ts = (unsigned)(((long long)tcoord(s) * tstride * (long long)sizeof(T)) & 15);
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) {
+        unsigned h[M];
+        const unsigned su = (vshift >> (4 * u)) + ts;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          const unsigned sh = (su + (pbase >> (4 * (MULTI ? 0 : j)))) & 15u;
+          const int o = voff[u] + (MULTI ? j * (int)sizeof(T) : j * VY * VZ * G::ROWB) + (int)sh;
+          h[j] = *reinterpret_cast<const unsigned*>(rb + o);
+        }
+        const unsigned w = vertex_word_hi<T, M>(h, band_tbl);
+        dst[tid + u * kThreads] = ((vvalid >> u) & 1u) ? w : kAbsent;
+      }
+      return;
+    }
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
       unsigned h[M];
@@ -354,10 +452,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   int slot_a = 0;  // word slot of slice ct
   {
     const bool ok = wait(t0, 0);
-    if (ok) words(0, slot_a);
+    if (ok) words(0, slot_a, t0);
     if (__syncthreads_or(!ok)) {
       // give the other copy in flight a bounded chance to land before leaving
-      if (TMA && t0 + 1 <= s_end) mbar_wait(&bar[1], ph[1] & 1u);
+      if (mbar && t0 + 1 <= s_end) mbar_wait(&bar[1], ph[1] & 1u);
       if (tid == 0) atomicOr(err, 2u);
       return false;
     }
@@ -383,7 +481,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     if (s <= s_end) {
       const int buf = (s - t0) & 1;
       ok = wait(s, buf);
-      if (ok) words(buf, slot_b);
+      if (ok) words(buf, slot_b, s);
     } else {
       for (int i = tid; i < VS; i += kThreads) B[i] = kAbsent;
     }
@@ -391,7 +489,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     // raw buffer is free, and every warp has finished culling step ct - 1
     if (__syncthreads_or(!ok)) {
       const int ob = ((s - t0) & 1) ^ 1;
-      if (TMA && s + 1 <= s_end) mbar_wait(&bar[ob], (ph[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
+      if (mbar && s + 1 <= s_end) mbar_wait(&bar[ob], (ph[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
       if (tid == 0) atomicOr(err, 2u);
       return false;
     }
@@ -449,7 +547,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     }
     slot_a = slot_b;
   }
-  if constexpr (TMA) {
+  if (mbar) {
     // slices t0 .. s_end alternate buffers 0, 1, 0, ...
     const unsigned nsl = (unsigned)(s_end - t0 + 1);
     ph[0] += (nsl + 1) >> 1;
@@ -468,7 +566,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   __shared__ unsigned long long bar[2];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, kThreads);  // visible after the tile's first barrier
-  if (TMA && threadIdx.x == 0) {
+  // TMA tensor copies and bulk row copies complete on these mbarriers
+  if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
