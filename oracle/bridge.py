@@ -346,11 +346,14 @@ def run_reference_fiber(mesh: OrcMesh, field: OrcField, thresholds, one_thread: 
         lib.ftk2ref_free(C.byref(res))
 
 
-def run_reference_fiber_surface(mesh: OrcMesh, field: OrcField, thresholds):
+def run_reference_fiber_surface(mesh: OrcMesh, field: OrcField, thresholds, one_thread: bool = False):
     """The reference's own engine with FiberPredicate<T> on a regular 3D+t
-    mesh: the triangle features and the star-fan triangles of get_complex,
-    an (n, 3) array of feature indices."""
-    lib = _load(REF_LIB, "ftk2ref")
+    mesh or an extruded mesh over tets: the triangle features and the
+    star-fan triangles of get_complex, an (n, 3) array of feature indices.
+    one_thread: the engine built to run its loops on one worker (on extruded
+    meshes the triangles found while patching are numbered in the order the
+    workers meet them, which only one worker makes deterministic)."""
+    lib = _load(REF1T_LIB if one_thread else REF_LIB, "ftk2ref")
     fn = lib.ftk2ref_run_fiber_surface
     fn.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcField), C.POINTER(C.c_double), C.POINTER(OrcResult),
                    C.POINTER(OrcConn)]

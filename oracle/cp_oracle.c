@@ -37,6 +37,10 @@
  *    50 triangle types of the 4-D Kuhn cube, star-fan triangles of
  *    form_general_manifold_patches with k = 2 on every pentatope, tracks as
  *    their components                                                         engine.hpp:1342-1417
+ *  - fiber surfaces on extruded tet meshes: phase-1 triangles (spatial, and
+ *    the Kuhn pieces over base edges) then the triangles inside the prisms
+ *    over base triangles, numbered as sequential patching meets them          mesh.hpp:568-599,
+ *                                                                             engine.hpp:101-212
  *
  * Compile without FMA contraction (-ffp-contract=off) so the solve rounds
  * exactly like the reference built for x86-64.
@@ -934,12 +938,242 @@ static void ext_emit_face_faces(const feat_t* F, size_t n, const uint64_t* cell,
   }
 }
 
+/* Fiber surfaces on an extruded tet mesh: FiberPredicate<T> on
+ * ExtrudedSimplicialMesh(UnstructuredSimplicialMesh(tets), L), a 4-D
+ * spacetime mesh whose features are triangles (engine.hpp:101-212, 1342-1417;
+ * mesh.hpp:568-599).
+ *  - phase 1 iterates the spatial triangles of every layer (the base mesh's
+ *    unique triangles, sorted) and the two Kuhn pieces of every base edge
+ *    between consecutive layers; its accepted triangles get node ids in
+ *    Simplex order;
+ *  - phase 2 visits the pentatopes in the reference's iteration order (layer,
+ *    base tet in stored order, prism piece j) and their 10 triangles in
+ *    find_m_subsimplices order (engine.hpp:1645-1652); a triangle no earlier
+ *    visit found is tested and, if accepted, takes the next node id.  Those
+ *    are the triangles interior to the prisms over base triangles.  This is
+ *    the order of the reference run with one worker; with several workers
+ *    the reference numbers them in thread-arrival order;
+ *  - per pentatope: its active triangles sorted by node id, h_S the first; on
+ *    each tet face the face's active triangles in the same order, h_T the
+ *    first, and {h_S, h_T, n} for every later n unless h_S is h_T or n;
+ *  - get_complex: canonical ids = Simplex order, the triangles sorted and
+ *    unique, their features united (the 4-D coface unions see no pentatope
+ *    among a triangle's cofaces), track id = the component's smallest index.
+ */
+typedef struct {
+  uint64_t v[3];
+  int64_t id; /* node id, or -1: tested and rejected */
+  int used;
+} tslot_t;
+
+typedef struct {
+  tslot_t* s;
+  size_t cap, n;
+} thash_t;
+
+static uint64_t thash_key(const uint64_t* v) {
+  uint64_t h = v[0] * 0x9E3779B97F4A7C15ull;
+  h ^= v[1] + 0x7F4A7C159E3779B9ull + (h << 6) + (h >> 2);
+  h ^= v[2] + 0x94D049BB133111EBull + (h << 6) + (h >> 2);
+  return h;
+}
+
+static tslot_t* thash_find(thash_t* H, const uint64_t* v, int insert) {
+  if (insert && 2 * (H->n + 1) > H->cap) {
+    thash_t G = {0};
+    G.cap = H->cap ? 2 * H->cap : 1024;
+    G.s = (tslot_t*)calloc(G.cap, sizeof(tslot_t));
+    for (size_t i = 0; i < H->cap; ++i)
+      if (H->s[i].used) {
+        size_t j = thash_key(H->s[i].v) & (G.cap - 1);
+        while (G.s[j].used) j = (j + 1) & (G.cap - 1);
+        G.s[j] = H->s[i];
+        G.n++;
+      }
+    free(H->s);
+    *H = G;
+  }
+  if (!H->cap) return NULL;
+  size_t j = thash_key(v) & (H->cap - 1);
+  while (H->s[j].used) {
+    if (H->s[j].v[0] == v[0] && H->s[j].v[1] == v[1] && H->s[j].v[2] == v[2]) return &H->s[j];
+    j = (j + 1) & (H->cap - 1);
+  }
+  if (!insert) return NULL;
+  H->s[j].used = 1;
+  H->s[j].v[0] = v[0]; H->s[j].v[1] = v[1]; H->s[j].v[2] = v[2];
+  H->s[j].id = -1;
+  H->n++;
+  return &H->s[j];
+}
+
+static int run_extruded_fiber_surface(const ext_t* X, const acc_t* acc, orc_result* out) {
+  const uint64_t ns = X->nv, L = X->L;
+  /* unique base edges, sorted (unstructured_mesh.hpp:44-53) */
+  face_t* E1 = (face_t*)malloc(sizeof(face_t) * (3 * X->nface + 1));
+  size_t n1 = 0;
+  for (size_t i = 0; i < X->nface; ++i) {
+    const uint64_t* w = X->faces[i].v;
+    uint64_t e[3][2] = {{w[0], w[1]}, {w[0], w[2]}, {w[1], w[2]}};
+    for (int q = 0; q < 3; ++q) { E1[n1].v[0] = e[q][0]; E1[n1].v[1] = e[q][1]; n1++; }
+  }
+  qsort(E1, n1, sizeof(face_t), cmp_face2);
+  size_t nu1 = 0;
+  for (size_t i = 0; i < n1; ++i)
+    if (nu1 == 0 || cmp_tuple(E1[nu1 - 1].v, E1[i].v, 1) != 0) E1[nu1++] = E1[i];
+
+  /* phase 1 */
+  fvec_t P = {0};
+  uint64_t tested = 0;
+  uint64_t g[4][4] = {{0}};
+  for (uint64_t t = 0; t <= L; ++t)
+    for (size_t i = 0; i < X->nface; ++i) {
+      uint64_t vid[4] = {X->faces[i].v[0] + t * ns, X->faces[i].v[1] + t * ns, X->faces[i].v[2] + t * ns, 0};
+      feat_t fe;
+      tested++;
+      if (evaluate(acc, 2, vid, g, &fe)) fvec_push(&P, &fe);
+    }
+  for (uint64_t t = 0; t < L; ++t)
+    for (size_t i = 0; i < nu1; ++i) {
+      const uint64_t a = E1[i].v[0], b = E1[i].v[1];
+      uint64_t pieces[2][4] = {{a + t * ns, a + (t + 1) * ns, b + (t + 1) * ns, 0},
+                               {a + t * ns, b + t * ns, b + (t + 1) * ns, 0}};
+      for (int j = 0; j < 2; ++j) {
+        feat_t fe;
+        tested++;
+        if (evaluate(acc, 2, pieces[j], g, &fe)) fvec_push(&P, &fe);
+      }
+    }
+  g_m = 2;
+  if (P.n) qsort(P.a, P.n, sizeof(feat_t), cmp_feat);
+
+  /* node table: phase-1 nodes first, in Simplex order */
+  thash_t H = {0};
+  fvec_t all = {0};  /* every node, by node id */
+  for (size_t i = 0; i < P.n; ++i) {
+    tslot_t* sl = thash_find(&H, P.a[i].v, 1);
+    sl->id = (int64_t)all.n;
+    fvec_push(&all, &P.a[i]);
+  }
+  free(P.a);
+
+  /* phase 2: pentatopes in the reference's order */
+  typedef struct { uint32_t v[3]; } ntri_t;  /* star-fan triangles in node ids */
+  ntri_t* T = NULL;
+  size_t nt = 0, tcap = 0;
+  for (uint64_t t = 0; t < L; ++t)
+    for (uint64_t c = 0; c < X->ncell; ++c) {
+      const uint64_t* w = &X->cells[c * 4];
+      for (int j = 0; j <= 3; ++j) {
+        uint64_t cell[5];
+        int k = 0;
+        for (int l = 0; l <= j; ++l) cell[k++] = w[l] + t * ns;
+        for (int l = j; l <= 3; ++l) cell[k++] = w[l] + (t + 1) * ns;
+        int64_t node[10];
+        int vs[10];  /* cell positions of the triangle's vertices, as a bit set */
+        int nn = 0;
+        for (int p0 = 0; p0 < 5; ++p0)
+          for (int p1 = p0 + 1; p1 < 5; ++p1)
+            for (int p2 = p1 + 1; p2 < 5; ++p2) {
+              uint64_t key[3] = {cell[p0], cell[p1], cell[p2]};
+              tslot_t* sl = thash_find(&H, key, 0);
+              if (!sl) {
+                sl = thash_find(&H, key, 1);
+                uint64_t vid[4] = {key[0], key[1], key[2], 0};
+                feat_t fe;
+                tested++;
+                if (evaluate(acc, 2, vid, g, &fe)) {
+                  sl->id = (int64_t)all.n;
+                  fe.phase = 1;
+                  fvec_push(&all, &fe);
+                }
+              }
+              if (sl->id >= 0) {
+                node[nn] = sl->id;
+                vs[nn] = (1 << p0) | (1 << p1) | (1 << p2);
+                nn++;
+              }
+            }
+        if (nn < 2) continue;
+        for (int i = 1; i < nn; ++i)
+          for (int q = i; q > 0 && node[q] < node[q - 1]; --q) {
+            int64_t tn = node[q]; node[q] = node[q - 1]; node[q - 1] = tn;
+            int tv = vs[q]; vs[q] = vs[q - 1]; vs[q - 1] = tv;
+          }
+        const int64_t hS = node[0];
+        for (int x = 0; x < 5; ++x) { /* the tet face without cell vertex x */
+          int seen = 0;
+          int64_t hT = -1;
+          for (int i = 0; i < nn; ++i) {
+            if (vs[i] & (1 << x)) continue;
+            if (seen++ == 0) { hT = node[i]; continue; }
+            if (hS == hT || hS == node[i]) continue;
+            if (nt == tcap) {
+              tcap = tcap ? 2 * tcap : 1024;
+              T = (ntri_t*)realloc(T, tcap * sizeof(ntri_t));
+            }
+            T[nt].v[0] = (uint32_t)hS; T[nt].v[1] = (uint32_t)hT; T[nt].v[2] = (uint32_t)node[i];
+            nt++;
+          }
+        }
+      }
+    }
+  free(H.s);
+
+  /* get_complex: canonical order, triangles re-indexed, sorted, unique */
+  const size_t n = all.n;
+  uint64_t* canon = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));  /* node id -> canonical index */
+  {
+    feat_t* F = (feat_t*)malloc(sizeof(feat_t) * (n + 1));
+    /* v[3] carries the node id through the sort (the first three entries
+     * never tie: every node is a distinct triangle) */
+    for (size_t i = 0; i < n; ++i) { F[i] = all.a[i]; F[i].scalar = 0.0f; F[i].v[3] = i; }
+    if (n) qsort(F, n, sizeof(feat_t), cmp_feat);
+    for (size_t i = 0; i < n; ++i) { canon[F[i].v[3]] = i; F[i].v[3] = 0; }
+    free(all.a);
+    all.a = F;
+  }
+  tri_t* C = (tri_t*)malloc(sizeof(tri_t) * (nt + 1));
+  for (size_t i = 0; i < nt; ++i) {
+    uint32_t v[3] = {(uint32_t)canon[T[i].v[0]], (uint32_t)canon[T[i].v[1]], (uint32_t)canon[T[i].v[2]]};
+    for (int a = 1; a < 3; ++a)
+      for (int q = a; q > 0 && v[q] < v[q - 1]; --q) { uint32_t tv = v[q]; v[q] = v[q - 1]; v[q - 1] = tv; }
+    C[i].v[0] = v[0]; C[i].v[1] = v[1]; C[i].v[2] = v[2];
+  }
+  free(T);
+  free(canon);
+  if (nt) qsort(C, nt, sizeof(tri_t), cmp_tri);
+  size_t nu = 0;
+  for (size_t i = 0; i < nt; ++i)
+    if (nu == 0 || cmp_tri(&C[nu - 1], &C[i]) != 0) C[nu++] = C[i];
+  uint64_t* parent = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+  for (size_t i = 0; i < n; ++i) parent[i] = i;
+  for (size_t i = 0; i < nu; ++i) {
+    uf_unite(parent, C[i].v[0], C[i].v[1]);
+    uf_unite(parent, C[i].v[1], C[i].v[2]);
+  }
+  evec_t none = {0};
+  finish(all.a, n, 2, &none, parent, tested, out);
+  out->cp_class = NULL;
+  out->cell_dim = 2;
+  out->n_cells = nu;
+  out->cells = (uint32_t*)malloc(sizeof(uint32_t) * (3 * nu + 3));
+  for (size_t i = 0; i < nu; ++i)
+    for (int q = 0; q < 3; ++q) out->cells[3 * i + q] = C[i].v[q];
+  free(C);
+  free(parent);
+  free(all.a);
+  free(E1);
+  return 0;
+}
+
 static int run_extruded(const orc_mesh* me, const orc_field* f, orc_result* out) {
   ext_t X;
   memset(&X, 0, sizeof(X));
   X.cd = me->base_cell_dim;
   int M = f->ncomp;
-  if (X.cd != M || (M != 2 && M != 3)) return 2;
+  const int surfaces = f->fiber && X.cd == 3 && M == 2; /* fiber surfaces over tets */
+  if (!surfaces && (X.cd != M || (M != 2 && M != 3))) return 2;
   X.ncell = me->n_base_cells;
   X.L = me->n_layers;
   /* n_spatial_verts = max vertex id + 1 over the base's vertices (mesh.hpp:556-561);
@@ -996,6 +1230,18 @@ static int run_extruded(const orc_mesh* me, const orc_field* f, orc_result* out)
     }
   }
   free(fill);
+
+  if (surfaces) {
+    acc_t acc;
+    memset(&acc, 0, sizeof(acc));
+    acc.f = f;
+    int rc = run_extruded_fiber_surface(&X, &acc, out);
+    free(X.cells);
+    free(X.faces);
+    free(X.cof_start);
+    free(X.cof);
+    return rc;
+  }
 
   /* evaluate every m-simplex of the extruded mesh */
   int nt = nthreads_of(f);

@@ -410,13 +410,15 @@ int run_fiber(const orc_mesh* mesh, const orc_field* field, const double* thr, o
 
 }  // namespace
 
-// Fiber surfaces: FiberPredicate<T> on a regular 3D+t mesh; conn receives the
-// star-fan triangles of get_complex (form_general_manifold_patches, k = 2).
+// Fiber surfaces: FiberPredicate<T> on a regular 3D+t mesh, or on an extruded
+// mesh over tets (per-vertex arrays); conn receives the star-fan triangles of
+// get_complex (form_general_manifold_patches, k = 2).
 extern "C" int ftk2ref_run_fiber_surface(const orc_mesh* mesh, const orc_field* field, const double* thresholds,
                                          orc_result* out, orc_conn* conn) {
   std::memset(out, 0, sizeof(*out));
   std::memset(conn, 0, sizeof(*conn));
-  if (mesh->kind != ORC_MESH_REGULAR || mesh->ndims != 4 || field->layout != ORC_LAYOUT_SEPARATE) return 3;
+  if (mesh->ndims != 4 || field->layout != ORC_LAYOUT_SEPARATE) return 3;
+  if (mesh->kind == ORC_MESH_EXTRUDED && (mesh->base_cell_dim != 3 || field->nd != 1)) return 3;
   try {
     return field->dtype == ORC_F64 ? run_fiber<double>(mesh, field, thresholds, out, conn)
                                    : run_fiber<float>(mesh, field, thresholds, out, conn);

@@ -282,3 +282,48 @@ FIBER_EXTRUDED_CASES = {
     "fiber_ext_tri": fiber_ext_tri,
     "fiber_ext_near_quantum": fiber_ext_near_quantum,
 }
+
+
+# ---- fiber surfaces on extruded 3D+t meshes (ExtrudedSimplicialMesh over
+# tets, two per-vertex fields); the reference numbers the triangles it finds
+# while patching in the order its workers meet them, so fixtures come from
+# its one-worker build
+
+def _ext_tet_fields(nx, ny, nz, L, seed, dtype=np.float64, n_blobs=6):
+    from ftk2_b200 import synthetic as S
+    coords, tets = S.extruded_tet_mesh(nx, ny, nz, seed=seed)
+    f = S.gaussian_sum_gradient_at(coords, L + 1, seed=seed, n_blobs=n_blobs, sigma=(1.0, 2.5), drift=0.4)
+    return coords, tets, (np.ascontiguousarray(f[0].astype(dtype)), np.ascontiguousarray(f[1].astype(dtype)))
+
+
+def fs_ext_gauss_f64():
+    coords, tets, fields = _ext_tet_fields(7, 6, 5, 4, 2)
+    return dict(coords=coords, cells=tets, n_layers=4, fields=fields, thresholds=(0.0, 0.0), q=2.0 ** 20)
+
+
+def fs_ext_f32_thresholds():
+    coords, tets, fields = _ext_tet_fields(6, 6, 6, 3, 3, np.float32)
+    return dict(coords=coords, cells=tets, n_layers=3, fields=fields, thresholds=(0.01, -0.02), q=2.0 ** 20)
+
+
+def fs_ext_near_quantum():
+    """Values of a few 1/Q: ties in the origin test and failed solves (the
+    centroid fallback)."""
+    from ftk2_b200 import synthetic as S
+    coords, tets = S.extruded_tet_mesh(5, 5, 4, seed=4)
+    rng = np.random.default_rng(14)
+    n = coords.shape[0] * 4
+    return dict(coords=coords, cells=tets, n_layers=3,
+                fields=(rng.uniform(-3e-6, 3e-6, n), rng.uniform(-3e-6, 3e-6, n)), thresholds=(0.0, 0.0), q=1e6)
+
+
+def fs_ext_seeded(nx=14, ny=12, nz=8, L=5, dtype=np.float32):
+    coords, tets, fields = _ext_tet_fields(nx, ny, nz, L, 7, dtype, n_blobs=12)
+    return dict(coords=coords, cells=tets, n_layers=L, fields=fields, thresholds=(0.0, 0.0), q=2.0 ** 20)
+
+
+FIBER_SURFACE_EXTRUDED_CASES = {
+    "fs_ext_gauss_f64": fs_ext_gauss_f64,
+    "fs_ext_f32_thresholds": fs_ext_f32_thresholds,
+    "fs_ext_near_quantum": fs_ext_near_quantum,
+}

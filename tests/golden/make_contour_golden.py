@@ -1,6 +1,8 @@
 """Generate tests/golden/contour/*.npz, tests/golden/fiber/*.npz and
 tests/golden/fiber_surface/*.npz, tests/golden/contour_extruded/*.npz and
-tests/golden/fiber_extruded/*.npz by running
+tests/golden/fiber_extruded/*.npz and tests/golden/fiber_surface_extruded/*.npz
+(the one-worker engine, whose numbering of the triangles found while patching
+is deterministic) by running
 the reference's own CPU engine with ContourPredicate<T> (one worker thread,
 oracle/_ref/libftk2ref1t.so) and FiberPredicate<T> (oracle/_ref/libftk2ref.so),
 built from the reference headers by oracle/Makefile, on the seeded inputs of
@@ -135,6 +137,27 @@ def main_fiber_surface(names=None):
               f"{len(cells)} triangles, reference {dt:.1f}s")
 
 
+def main_fiber_surface_extruded(names=None):
+    out_dir = os.path.join(HERE, "fiber_surface_extruded")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, make in contour_cases.FIBER_SURFACE_EXTRUDED_CASES.items():
+        if names and name not in names:
+            continue
+        case = make()
+        keep: list = []
+        mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+        fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+        t = time.time()
+        r, cells = bridge.run_reference_fiber_surface(mesh, fld, case["thresholds"], one_thread=True)
+        dt = time.time() - t
+        rec = {"input_sha256": np.array(digest(np.concatenate([a.reshape(-1) for a in case["fields"]]))),
+               "reference_seconds": np.array(dt), "simplices": r.simplices, "bary": r.bary, "lam": r.lam,
+               "track_id": r.track_id, "scalar": r.scalar, "cells": cells}
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **rec)
+        print(f"{name}: {len(r.track_id)} features, {len(set(r.track_id.tolist()))} tracks, "
+              f"{len(cells)} triangles, reference {dt:.1f}s")
+
+
 def main(names=None):
     out_dir = os.path.join(HERE, "contour")
     os.makedirs(out_dir, exist_ok=True)
@@ -162,3 +185,4 @@ if __name__ == "__main__":
     main_fiber_surface(sys.argv[1:])
     main_extruded(sys.argv[1:])
     main_fiber_extruded(sys.argv[1:])
+    main_fiber_surface_extruded(sys.argv[1:])

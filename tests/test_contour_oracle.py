@@ -280,3 +280,59 @@ def test_fiber_surface_restatement_matches_live_reference_seeded():
     assert np.array_equal(r.lam.view(np.uint64), ref.lam.view(np.uint64))
     assert np.array_equal(r.track_id, ref.track_id)
     assert np.array_equal(r.cells, cells)
+
+
+FS_EXT_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber_surface_extruded")
+
+
+def _fs_ext_inputs(case, keep, fiber=True):
+    mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+    fld = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep,
+                            fiber_thr=case["thresholds"] if fiber else None)
+    return mesh, fld
+
+
+def _same_surface(r, cells, g, name):
+    assert len(r.track_id) == len(g["track_id"]) > 0, name
+    assert np.array_equal(r.simplices, g["simplices"]), name
+    assert np.array_equal(r.lam.view(np.uint64), g["lam"].view(np.uint64)), name
+    assert np.array_equal(r.bary.view(np.uint32), g["bary"].view(np.uint32)), name
+    assert np.array_equal(r.track_id, g["track_id"]), name
+    assert np.array_equal(cells, g["cells"]), name
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_EXTRUDED_CASES))
+def test_extruded_fiber_surface_reference_reproduces_fixtures(name):
+    case = contour_cases.FIBER_SURFACE_EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(FS_EXT_GOLD, f"{name}.npz"))
+    keep: list = []
+    mesh, fld = _fs_ext_inputs(case, keep, fiber=False)
+    r, cells = bridge.run_reference_fiber_surface(mesh, fld, case["thresholds"], one_thread=True)
+    _same_surface(r, cells, g, name)
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_EXTRUDED_CASES))
+def test_extruded_fiber_surface_restatement_matches_reference_fixtures(name):
+    """Fiber surfaces on ExtrudedSimplicialMesh over tets: the restatement's
+    phase-1 triangles, the prism-interior triangles numbered in the order
+    sequential patching meets them, its star-fan triangles and tracks equal
+    the reference's one-worker run bit for bit (centroid fallbacks and ties
+    included)."""
+    case = contour_cases.FIBER_SURFACE_EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(FS_EXT_GOLD, f"{name}.npz"))
+    keep: list = []
+    r = bridge.run_restatement(*_fs_ext_inputs(case, keep))
+    _same_surface(r, r.cells, g, name)
+
+
+@pytest.mark.skipif(not bridge.ref_available(), reason="reference build absent")
+def test_extruded_fiber_surface_restatement_matches_live_reference_seeded():
+    case = contour_cases.fs_ext_seeded()
+    keep: list = []
+    mesh, raw = _fs_ext_inputs(case, keep, fiber=False)
+    ref, cells = bridge.run_reference_fiber_surface(mesh, raw, case["thresholds"], one_thread=True)
+    r = bridge.run_restatement(*_fs_ext_inputs(case, keep))
+    assert len(r.track_id) > 500
+    _same_surface(r, r.cells, {"simplices": ref.simplices, "lam": ref.lam, "bary": ref.bary,
+                               "track_id": ref.track_id, "cells": cells}, "fs_ext_seeded")
