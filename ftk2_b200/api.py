@@ -503,8 +503,9 @@ class Context:
     def fiber_surface(self, mesh: MeshDesc, field: FieldDesc, thresholds=(0.0, 0.0),
                       sos_q: float = 1e6) -> ContourResult:
         """Fiber surfaces (FiberPredicate<T>) of two scalar fields on a regular
-        3D+t mesh: triangle features (simplices (n, 3)) and the star-fan
-        triangles of get_complex (cells (c, 3))."""
+        3D+t mesh or an extruded mesh over tets (per-vertex arrays): triangle
+        features (simplices (n, 3)) and the star-fan triangles of get_complex
+        (cells (c, 3))."""
         thr = (C.c_double * 2)(float(thresholds[0]), float(thresholds[1]))
         out = C.POINTER(FiberSurfaceResultC)()
         self._check(self.lib.ftk2b_fiber_surface_extract(self.h, C.byref(mesh), C.byref(field), thr,

@@ -157,7 +157,8 @@ struct ftk2b_ctx {
   ftk2b::DevBuf tstats, runs;  // cull mode 1 scratch (tile statistics, run list + count)
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::DevBuf attr_out, attr_desc, attr_stage[16];  // ftk2b_cp_attributes
-  ftk2b::DevBuf contour[28];  // level-set and fiber-surface scratch and outputs
+  ftk2b::DevBuf contour[40];  // level-set and fiber-surface scratch and outputs
+  unsigned fe_cap = 0;        // extruded fiber surfaces: accepted-triangle capacity (grows)
   // two pinned host chunks for large result copies (allocated on first use)
   void* d2h_pin[2] = {nullptr, nullptr};
   cudaEvent_t d2h_ev[2] = {nullptr, nullptr};

@@ -28,6 +28,8 @@
 #include <sys/mman.h>
 
 #include <algorithm>
+#include <array>
+#include <vector>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -679,7 +681,10 @@ void* ct_host_alloc(size_t bytes) {
 enum {
   kBufField = 0, kBufPos, kBufMask, kBufBlk, kBufVoff, kBufSimp, kBufLam, kBufBary, kBufFirst, kBufParent,
   kBufCells, kBufKey0, kBufKey1, kBufVal0, kBufVal1, kBufHist, kBufCellsOut, kBufTrack, kBufCount, kBufList,
-  kBufField2, kBufUpOff, kBufUpNbr, kBufBaseCells
+  kBufField2, kBufUpOff, kBufUpNbr, kBufBaseCells,
+  // fiber surfaces on extruded meshes
+  kBufFeTris, kBufFeEdges, kBufFeSimp, kBufFeLam, kBufFeBary, kBufFePhase, kBufFeDisc, kBufFeFlag, kBufFeHi,
+  kBufFeLo, kBufCount_
 };
 
 template <typename T>
@@ -1698,6 +1703,589 @@ ftk2b_status contour_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const
   return FTK2B_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Fiber surfaces on ExtrudedSimplicialMesh(UnstructuredSimplicialMesh(tets), L)
+// (FiberPredicate<T>, predicate.hpp:341-362; the mesh, mesh.hpp:542-712;
+// form_general_manifold_patches with k = 2, engine.hpp:1342-1417).  Vertex ids
+// s + t S, two fields per vertex.  The triangles of the 4-D mesh are
+//   spatial   every base triangle at every layer t = 0 .. L
+//   lateral   the two Kuhn pieces over every base edge a < b between layers
+//             t and t + 1: {a@t, a@t+1, b@t+1}, {a@t, b@t, b@t+1}
+//   interior  the two triangles inside the prism over every base triangle
+//             a < b < c: {a@t, b@t+1, c@t+1}, {a@t, b@t, c@t+1}
+// The reference's phase 1 iterates the spatial and lateral ones (node ids in
+// simplex order); the interior ones it finds while patching, numbered in the
+// order it meets them: pentatopes by layer, base tet (stored order) and prism
+// piece j, each pentatope's triangles in find_m_subsimplices order
+// (engine.hpp:1645-1652) -- the order of its run on one worker.  Pipeline:
+//   fe_test   one thread per candidate triangle: the 2-D origin test and the
+//             solve with its centroid fallback, accepted ones compacted
+//   sort      two stable radix sorts (third vertex, then the first two) give
+//             the canonical order
+//   fe_disc   one thread per pentatope: the first meeting position of every
+//             accepted interior triangle (atomic minimum)
+//   fe_fan    one thread per pentatope: its active triangles by node order,
+//             the star-fan triangles {h_S, h_T, n}, union-find hooks
+//   buckets   the fan triangles sorted and made unique; track ids
+
+struct FeGeom {
+  unsigned long long S, L, nv;      // base vertices, layers, S (L + 1)
+  unsigned long long ntet, ntri, nedge;
+  const unsigned* tets;              // 4 per base tet, ascending, stored order
+  const unsigned* tris;              // unique base triangles, simplex order
+  const unsigned* edges;             // unique base edges, simplex order
+};
+
+// candidate c: its vertex ids (ascending) and 1 when it lies inside a prism
+__device__ __forceinline__ int fe_candidate(const FeGeom& g, unsigned long long c, unsigned long long v[3]) {
+  const unsigned long long nsp = (g.L + 1) * g.ntri, nlat = 2 * g.L * g.nedge;
+  if (c < nsp) {
+    const unsigned long long t = c / g.ntri, i = c - t * g.ntri;
+    for (int k = 0; k < 3; ++k) v[k] = g.tris[3 * i + k] + t * g.S;
+    return 0;
+  }
+  c -= nsp;
+  if (c < nlat) {
+    const unsigned long long j = c & 1, q = c >> 1, t = q / g.nedge, e = q - t * g.nedge;
+    const unsigned long long a = g.edges[2 * e], b = g.edges[2 * e + 1];
+    v[0] = a + t * g.S;
+    v[1] = j == 0 ? a + (t + 1) * g.S : b + t * g.S;
+    v[2] = b + (t + 1) * g.S;
+    return 0;
+  }
+  c -= nlat;
+  const unsigned long long k = c & 1, q = c >> 1, t = q / g.ntri, i = q - t * g.ntri;
+  const unsigned long long a = g.tris[3 * i], b = g.tris[3 * i + 1], cc = g.tris[3 * i + 2];
+  v[0] = a + t * g.S;
+  v[1] = b + (k == 0 ? t + 1 : t) * g.S;
+  v[2] = cc + (t + 1) * g.S;
+  return 1;
+}
+
+template <typename T>
+__global__ void fe_test_kernel(FeGeom g, const T* __restrict__ f0, const T* __restrict__ f1, T t0, T t1, double q,
+                               unsigned long long ncand, unsigned long long* __restrict__ simp,
+                               double* __restrict__ lam, float* __restrict__ bary, unsigned* __restrict__ phase,
+                               unsigned* cnt, unsigned cap) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < ncand; base += stride) {
+    const unsigned long long c = base + threadIdx.x;
+    bool acc = false;
+    unsigned long long v[3] = {0, 0, 0};
+    int ph = 0;
+    T l[3];
+    if (c < ncand) {
+      ph = fe_candidate(g, c, v);
+      T val[3][2];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        val[k][0] = fp<T>::sub(__ldg(f0 + v[k]), t0);  // values[i][j] - thresholds[j]
+        val[k][1] = fp<T>::sub(__ldg(f1 + v[k]), t1);
+      }
+      if (sos_inside2<T>(val, q)) {
+        acc = true;
+        if (!solve_exact<2, T>(val, l))  // FiberPredicate keeps the centroid: (T)1.0 / 3.0
+          for (int k = 0; k < 3; ++k) l[k] = (T)((double)(T)1.0 / 3.0);
+      }
+    }
+    const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
+    if (!ball) continue;
+    unsigned b0 = 0;
+    if (lane == 0) b0 = atomicAdd(cnt, (unsigned)__popc(ball));
+    b0 = __shfl_sync(0xFFFFFFFFu, b0, 0);
+    if (!acc) continue;
+    const unsigned r = b0 + __popc(ball & ((1u << lane) - 1u));
+    if (r >= cap) continue;
+    for (int k = 0; k < 3; ++k) {
+      simp[3 * (size_t)r + k] = v[k];
+      lam[3 * (size_t)r + k] = (double)l[k];
+      bary[3 * (size_t)r + k] = (float)l[k];
+    }
+    phase[r] = (unsigned)ph;
+  }
+}
+
+__global__ void fe_set_kernel(unsigned* p, unsigned v) { *p = v; }
+
+__global__ void fe_key_lo_kernel(const unsigned long long* __restrict__ simp, unsigned n,
+                                 unsigned long long* __restrict__ key, unsigned* __restrict__ val) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    key[i] = simp[3 * (size_t)i + 2];
+    val[i] = i;
+  }
+}
+
+// keys of the first two vertices in the order of perm (the sort by the
+// third vertex), written over that sort's keys
+__global__ void fe_key_hi_kernel(const unsigned long long* __restrict__ simp, const unsigned* __restrict__ perm,
+                                 unsigned n, unsigned long long* __restrict__ key) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned p = perm[i];
+    key[i] = (simp[3 * (size_t)p] << 32) | simp[3 * (size_t)p + 1];
+  }
+}
+
+// canonical order: features gathered by perm, lookup keys, vertex flags,
+// first-meeting positions reset, union-find parents
+__global__ void fe_gather_kernel(const unsigned* __restrict__ perm, unsigned n,
+                                 const unsigned long long* __restrict__ simp_u, const double* __restrict__ lam_u,
+                                 const float* __restrict__ bary_u, const unsigned* __restrict__ phase_u,
+                                 unsigned long long* __restrict__ simp, double* __restrict__ lam,
+                                 float* __restrict__ bary, unsigned* __restrict__ phase,
+                                 unsigned long long* __restrict__ hi, unsigned* __restrict__ lo,
+                                 unsigned char* __restrict__ vflag, unsigned long long* __restrict__ disc,
+                                 unsigned* __restrict__ parent) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned p = perm[i];
+    unsigned long long v[3];
+    for (int k = 0; k < 3; ++k) {
+      v[k] = simp_u[3 * (size_t)p + k];
+      simp[3 * (size_t)i + k] = v[k];
+      lam[3 * (size_t)i + k] = lam_u[3 * (size_t)p + k];
+      bary[3 * (size_t)i + k] = bary_u[3 * (size_t)p + k];
+      vflag[v[k]] = 1;
+    }
+    phase[i] = phase_u[p];
+    hi[i] = (v[0] << 32) | v[1];
+    lo[i] = (unsigned)v[2];
+    disc[i] = ~0ull;
+    parent[i] = i;
+  }
+}
+
+__device__ __forceinline__ long long fe_find(const unsigned long long* __restrict__ hi,
+                                             const unsigned* __restrict__ lo, unsigned n, unsigned long long h,
+                                             unsigned l) {
+  unsigned a = 0, b = n;
+  while (a < b) {
+    const unsigned mid = (a + b) >> 1;
+    const unsigned long long hm = hi[mid];
+    const unsigned lm = lo[mid];
+    if (hm == h && lm == l) return mid;
+    if (hm < h || (hm == h && lm < l)) a = mid + 1;
+    else b = mid;
+  }
+  return -1;
+}
+
+// Pentatope p of the reference's iteration order: layer t, base tet c, prism
+// piece j; its vertex ids (ascending), the spatial id and layer of each.
+__device__ __forceinline__ void fe_pentatope(const FeGeom& g, unsigned long long p, unsigned long long cell[5],
+                                             unsigned sp[5], int lay[5]) {
+  const unsigned long long t = p / (4 * g.ntet), r = p - t * 4 * g.ntet, c = r >> 2;
+  const int j = (int)(r & 3);
+  const unsigned* w = g.tets + 4 * c;
+  int k = 0;
+  for (int l = 0; l <= j; ++l, ++k) {
+    sp[k] = w[l];
+    lay[k] = 0;
+    cell[k] = w[l] + t * g.S;
+  }
+  for (int l = j; l <= 3; ++l, ++k) {
+    sp[k] = w[l];
+    lay[k] = 1;
+    cell[k] = w[l] + (t + 1) * g.S;
+  }
+}
+
+__global__ void fe_disc_kernel(FeGeom g, unsigned long long npent, const unsigned char* __restrict__ vflag,
+                               const unsigned long long* __restrict__ hi, const unsigned* __restrict__ lo,
+                               unsigned n, unsigned long long* __restrict__ disc) {
+  for (unsigned long long p = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; p < npent;
+       p += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long cell[5];
+    unsigned sp[5];
+    int lay[5];
+    fe_pentatope(g, p, cell, sp, lay);
+    int nf = 0;
+    for (int k = 0; k < 5; ++k) nf += vflag[cell[k]];
+    if (nf < 3) continue;
+    int pos = 0;
+    for (int a = 0; a < 5; ++a)
+      for (int b = a + 1; b < 5; ++b)
+        for (int c = b + 1; c < 5; ++c, ++pos) {
+          // inside a prism: three distinct base vertices over both layers
+          if (sp[a] == sp[b] || sp[b] == sp[c] || lay[a] == lay[c]) continue;
+          const long long idx = fe_find(hi, lo, n, (cell[a] << 32) | cell[b], (unsigned)cell[c]);
+          if (idx >= 0) atomicMin(&disc[idx], p * 16 + (unsigned long long)pos);
+        }
+  }
+}
+
+__global__ void fe_fan_kernel(FeGeom g, unsigned long long npent, const unsigned char* __restrict__ vflag,
+                              const unsigned long long* __restrict__ hi, const unsigned* __restrict__ lo, unsigned n,
+                              const unsigned* __restrict__ phase, const unsigned long long* __restrict__ disc,
+                              unsigned* __restrict__ cells, unsigned long long* cnt, unsigned cap,
+                              unsigned* parent, unsigned* err) {
+  for (unsigned long long p = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; p < npent;
+       p += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long cell[5];
+    unsigned sp[5];
+    int lay[5];
+    fe_pentatope(g, p, cell, sp, lay);
+    int nf = 0;
+    for (int k = 0; k < 5; ++k) nf += vflag[cell[k]];
+    if (nf < 3) continue;
+    unsigned node[10], vs[10];
+    unsigned long long ord[10];
+    int nn = 0;
+    for (int a = 0; a < 5; ++a)
+      for (int b = a + 1; b < 5; ++b)
+        for (int c = b + 1; c < 5; ++c) {
+          const long long idx = fe_find(hi, lo, n, (cell[a] << 32) | cell[b], (unsigned)cell[c]);
+          if (idx < 0) continue;
+          // node order: phase-1 triangles in simplex order, then the others
+          // by the position at which patching first met them
+          const unsigned long long o = phase[idx] ? ((1ull << 63) | disc[idx]) : (unsigned long long)idx;
+          int w = nn++;
+          while (w > 0 && ord[w - 1] > o) {
+            ord[w] = ord[w - 1];
+            node[w] = node[w - 1];
+            vs[w] = vs[w - 1];
+            --w;
+          }
+          ord[w] = o;
+          node[w] = (unsigned)idx;
+          vs[w] = (1u << a) | (1u << b) | (1u << c);
+        }
+    if (nn < 2) continue;
+    const unsigned hs = node[0];
+    unsigned mine = 0;
+    for (int f = 0; f < 5; ++f) {
+      int seen = 0;
+      unsigned ht = 0;
+      for (int x = 0; x < nn; ++x) {
+        if (vs[x] & (1u << f)) continue;
+        if (seen++ == 0) {
+          ht = node[x];
+          continue;
+        }
+        if (hs != ht && hs != node[x]) ++mine;
+      }
+    }
+    if (!mine) continue;
+    unsigned long long slot = atomicAdd(cnt, (unsigned long long)mine);
+    for (int f = 0; f < 5; ++f) {
+      int seen = 0;
+      unsigned ht = 0;
+      for (int x = 0; x < nn; ++x) {
+        if (vs[x] & (1u << f)) continue;
+        if (seen++ == 0) {
+          ht = node[x];
+          continue;
+        }
+        if (hs == ht || hs == node[x]) continue;
+        unsigned tri[3] = {hs, ht, node[x]};
+        ct_sort4(tri, 3);
+        if (slot < cap)
+          for (int k = 0; k < 3; ++k) cells[(size_t)slot * 3 + k] = tri[k];
+        ++slot;
+        uf_unite(parent, tri[0], tri[1], err);
+        uf_unite(parent, tri[0], tri[2], err);
+      }
+    }
+  }
+}
+
+template <typename T>
+ftk2b_status run_fiber_surface_extruded(ftk2b_ctx* ctx, const FeGeom& g, const void* fa, const void* fb, T t0, T t1,
+                                        double q, ftk2b_fiber_surface_result* res) {
+  cudaStream_t st = ctx->stream;
+  DevBuf* B = ctx->contour;
+  const unsigned sms = (unsigned)ctx->num_sms;
+  const unsigned long long ncand = (g.L + 1) * g.ntri + 2 * g.L * g.nedge + 2 * g.L * g.ntri;
+  const unsigned long long npent = 4 * g.L * g.ntet;
+  C_TRY(B[kBufCount].ensure(64));
+  auto* counts = static_cast<unsigned*>(B[kBufCount].p);  // [0] n, [1] accepted, [2] roots, [3] err
+  auto* cell64 = reinterpret_cast<unsigned long long*>(counts + 10);
+  const T* a0 = static_cast<const T*>(fa);
+  const T* a1 = static_cast<const T*>(fb);
+  C_TRY(cudaMemsetAsync(counts, 0, 64, st));
+  C_TRY(cudaEventRecord(ctx->ev0, st));
+  // 1. every candidate triangle, accepted ones compacted (capacity grows once)
+  unsigned cap = ctx->fe_cap ? ctx->fe_cap : (1u << 18);
+  unsigned n = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    C_TRY(B[kBufSimp].ensure(24ull * cap));
+    C_TRY(B[kBufLam].ensure(24ull * cap));
+    C_TRY(B[kBufBary].ensure(12ull * cap));
+    C_TRY(B[kBufVoff].ensure(4ull * cap));
+    C_TRY(cudaMemsetAsync(counts + 1, 0, 4, st));
+    fe_test_kernel<T><<<grid_of(ncand, 256, 64ull * sms), 256, 0, st>>>(
+        g, a0, a1, t0, t1, q, ncand, static_cast<unsigned long long*>(B[kBufSimp].p),
+        static_cast<double*>(B[kBufLam].p), static_cast<float*>(B[kBufBary].p), static_cast<unsigned*>(B[kBufVoff].p),
+        counts + 1, cap);
+    ctx->launches += 1;
+    C_TRY(cudaMemcpyAsync(ctx->h_counters, counts + 1, 4, cudaMemcpyDeviceToHost, st));
+    C_TRY(ctx->sync());
+    n = ctx->h_counters[0];
+    if (n <= cap) break;
+    if (n >= 0x7FFFFFF0u) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 feature triangles");
+    cap = n + n / 8 + 1024;
+    ctx->fe_cap = cap;
+  }
+  const size_t ncap = n ? n : 1;
+  auto* simp_u = static_cast<unsigned long long*>(B[kBufSimp].p);
+  // 2. canonical order
+  C_TRY(B[kBufKey0].ensure(8 * ncap));
+  C_TRY(B[kBufKey1].ensure(8 * ncap));
+  C_TRY(B[kBufVal0].ensure(4 * ncap));
+  C_TRY(B[kBufVal1].ensure(4 * ncap));
+  const int sgrid = ctx->sort_grid((unsigned)ncap);
+  C_TRY(B[kBufHist].ensure(4ull * 256 * sgrid));
+  auto* k0 = static_cast<unsigned long long*>(B[kBufKey0].p);
+  auto* k1 = static_cast<unsigned long long*>(B[kBufKey1].p);
+  auto* v0 = static_cast<unsigned*>(B[kBufVal0].p);
+  auto* v1 = static_cast<unsigned*>(B[kBufVal1].p);
+  auto* hist = static_cast<unsigned*>(B[kBufHist].p);
+  int vb = 1;
+  while (vb < 64 && (g.nv >> vb) != 0) ++vb;
+  fe_set_kernel<<<1, 1, 0, st>>>(counts + 0, n);
+  fe_key_lo_kernel<<<grid_of(ncap, 256, 16ull * sms), 256, 0, st>>>(simp_u, n, k0, v0);
+  unsigned long long nl = 0;
+  const bool alt1 = radix_sort(k0, v0, k1, v1, counts + 0, (unsigned)ncap, vb, hist, sgrid, st, &nl);
+  unsigned long long* kr = alt1 ? k1 : k0;
+  unsigned* vr = alt1 ? v1 : v0;
+  fe_key_hi_kernel<<<grid_of(ncap, 256, 16ull * sms), 256, 0, st>>>(simp_u, vr, n, kr);
+  const bool alt2 = radix_sort(kr, vr, alt1 ? k0 : k1, alt1 ? v0 : v1, counts + 0, (unsigned)ncap, 32 + vb, hist,
+                               sgrid, st, &nl);
+  const unsigned* perm = alt2 ? (alt1 ? v0 : v1) : vr;
+  ctx->launches += nl + 3;
+  C_TRY(B[kBufFeSimp].ensure(24 * ncap));
+  C_TRY(B[kBufFeLam].ensure(24 * ncap));
+  C_TRY(B[kBufFeBary].ensure(12 * ncap));
+  C_TRY(B[kBufFePhase].ensure(4 * ncap));
+  C_TRY(B[kBufFeDisc].ensure(8 * ncap));
+  C_TRY(B[kBufFeHi].ensure(8 * ncap));
+  C_TRY(B[kBufFeLo].ensure(4 * ncap));
+  C_TRY(B[kBufFeFlag].ensure(g.nv));
+  C_TRY(B[kBufParent].ensure(4 * ncap));
+  C_TRY(B[kBufTrack].ensure(8 * ncap));
+  auto* simp = static_cast<unsigned long long*>(B[kBufFeSimp].p);
+  auto* lam = static_cast<double*>(B[kBufFeLam].p);
+  auto* bary = static_cast<float*>(B[kBufFeBary].p);
+  auto* phase = static_cast<unsigned*>(B[kBufFePhase].p);
+  auto* disc = static_cast<unsigned long long*>(B[kBufFeDisc].p);
+  auto* hi = static_cast<unsigned long long*>(B[kBufFeHi].p);
+  auto* lo = static_cast<unsigned*>(B[kBufFeLo].p);
+  auto* vflag = static_cast<unsigned char*>(B[kBufFeFlag].p);
+  auto* parent = static_cast<unsigned*>(B[kBufParent].p);
+  auto* track = static_cast<unsigned long long*>(B[kBufTrack].p);
+  C_TRY(cudaMemsetAsync(vflag, 0, g.nv, st));
+  fe_gather_kernel<<<grid_of(ncap, 256, 16ull * sms), 256, 0, st>>>(
+      perm, n, simp_u, static_cast<const double*>(B[kBufLam].p), static_cast<const float*>(B[kBufBary].p),
+      static_cast<const unsigned*>(B[kBufVoff].p), simp, lam, bary, phase, hi, lo, vflag, disc, parent);
+  // 3. first meeting positions of the interior triangles
+  fe_disc_kernel<<<grid_of(npent, 256, 64ull * sms), 256, 0, st>>>(g, npent, vflag, hi, lo, n, disc);
+  ctx->launches += 2;
+  // 4. star-fan triangles
+  unsigned ccap = (unsigned)std::min<unsigned long long>(0x7FFFFFFFull, std::max<unsigned long long>(1024ull, 4ull * n));
+  unsigned ncell = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    C_TRY(B[kBufCells].ensure((size_t)12 * ccap));
+    C_TRY(cudaMemsetAsync(cell64, 0, 8, st));
+    if (attempt) ct_iota_kernel<<<grid_of(ncap, 256, 8ull * sms), 256, 0, st>>>(parent, n);
+    fe_fan_kernel<<<grid_of(npent, 256, 64ull * sms), 256, 0, st>>>(g, npent, vflag, hi, lo, n, phase, disc,
+                                                                    static_cast<unsigned*>(B[kBufCells].p), cell64,
+                                                                    ccap, parent, counts + 3);
+    ctx->launches += 1;
+    unsigned long long nc64 = 0;
+    C_TRY(cudaMemcpyAsync(&nc64, cell64, 8, cudaMemcpyDeviceToHost, st));
+    C_TRY(ctx->sync());
+    if (nc64 >= 0x7FFFFFFFull) return cfail(ctx, FTK2B_UNSUPPORTED, "more than 2^31 - 1 manifold triangles");
+    ncell = (unsigned)nc64;
+    if (ncell <= ccap) break;
+    ccap = ncell;
+  }
+  auto* cells = static_cast<unsigned*>(B[kBufCells].p);
+  // 5. sorted, unique triangles: buckets by leading node
+  const unsigned nb = n + 1;
+  const unsigned sblocks = (unsigned)((nb + kCtThreads * kScanPer - 1) / (kCtThreads * kScanPer));
+  const unsigned cc = ncell ? ncell : 1;
+  C_TRY(B[kBufKey0].ensure(4ull * nb));
+  C_TRY(B[kBufKey1].ensure(4ull * nb));
+  C_TRY(B[kBufVal0].ensure(4ull * (sblocks + 1)));
+  C_TRY(B[kBufVal1].ensure(4ull * nb));
+  C_TRY(B[kBufCellsOut].ensure(12ull * cc));
+  C_TRY(B[kBufMask].ensure(12ull * cc));
+  auto* boff = static_cast<unsigned*>(B[kBufKey0].p);
+  auto* bcur = static_cast<unsigned*>(B[kBufKey1].p);
+  auto* btot = static_cast<unsigned*>(B[kBufVal0].p);
+  auto* uoff = static_cast<unsigned*>(B[kBufVal1].p);
+  auto* rows = static_cast<unsigned*>(B[kBufCellsOut].p);
+  auto* cells_out = static_cast<unsigned*>(B[kBufMask].p);
+  const unsigned cg = grid_of(cc, 256, 16ull * sms);
+  unsigned nuniq = 0;
+  if (ncell) {
+    C_TRY(cudaMemsetAsync(boff, 0, 4ull * nb, st));
+    C_TRY(cudaMemsetAsync(bcur, 0, 4ull * nb, st));
+    C_TRY(cudaMemsetAsync(uoff, 0, 4ull * nb, st));
+    ct_bucket_count_kernel<<<cg, 256, 0, st>>>(cells, ncell, 3, boff);
+    ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
+    ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(boff, nb, btot);
+    ct_bucket_scatter_kernel<<<cg, 256, 0, st>>>(cells, ncell, 3, boff, bcur, rows);
+    ct_bucket_sort_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(rows, boff, n, 3, counts + 3, uoff);
+    ct_scan_blocks_kernel<<<sblocks, kCtThreads, 0, st>>>(uoff, nb, btot);
+    C_TRY(launch_scan(btot, sblocks, nullptr, nullptr, st));
+    ct_scan_add_kernel<<<sblocks, kCtThreads, 0, st>>>(uoff, nb, btot);
+    ct_bucket_compact_kernel<<<grid_of(n, 128, 32ull * sms), 128, 0, st>>>(rows, boff, uoff, n, 3, cells_out);
+    ctx->launches += 10;
+    C_TRY(cudaMemcpyAsync(&nuniq, uoff + n, 4, cudaMemcpyDeviceToHost, st));
+  }
+  if (n) {
+    C_TRY(launch_uf_label(parent, counts + 0, n, track, counts + 2, st));
+    ctx->launches += 1;
+  }
+  C_TRY(cudaEventRecord(ctx->ev1, st));
+  unsigned hc[4] = {0, 0, 0, 0};
+  C_TRY(cudaMemcpyAsync(hc, counts, 16, cudaMemcpyDeviceToHost, st));
+  C_TRY(ctx->sync());
+  res->n_features = n;
+  res->n_cells = nuniq;
+  res->simplices = static_cast<uint64_t*>(ct_host_alloc(24 * ncap));
+  res->lambda = static_cast<double*>(ct_host_alloc(24 * ncap));
+  res->barycentric = static_cast<float*>(ct_host_alloc(12 * ncap));
+  res->track_id = static_cast<uint64_t*>(ct_host_alloc(8 * ncap));
+  res->scalar = static_cast<float*>(std::calloc(ncap, 4));
+  res->cells = static_cast<uint32_t*>(ct_host_alloc(12ull * (nuniq ? nuniq : 1)));
+  if (!res->simplices || !res->lambda || !res->barycentric || !res->track_id || !res->scalar || !res->cells)
+    return cfail(ctx, FTK2B_OOM, "host result allocation failed");
+  C_TRY(ct_d2h(ctx, res->simplices, simp, 24ull * n));
+  C_TRY(ct_d2h(ctx, res->lambda, lam, 24ull * n));
+  C_TRY(ct_d2h(ctx, res->barycentric, bary, 12ull * n));
+  C_TRY(ct_d2h(ctx, res->track_id, track, 8ull * n));
+  C_TRY(ct_d2h(ctx, res->cells, cells_out, 12ull * nuniq));
+  if (hc[3] & 1u) return cfail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
+  res->n_tracks = hc[2];
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  res->device_ms = ms;
+  return FTK2B_OK;
+}
+
+// Fiber surfaces on an extruded mesh over tets: base tets sorted, the unique
+// base triangles and edges in simplex order, both fields (one value per
+// vertex id) staged.
+ftk2b_status fiber_surface_extruded(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, const ftk2b_field_desc* field,
+                                    const double thr[2], double sos_q, ftk2b_fiber_surface_result** out) {
+  if (mesh->base_cell_dim != 3 || mesh->ndims != 4)
+    return cfail(ctx, FTK2B_UNSUPPORTED, "fiber surfaces on extruded meshes need tet base cells (ndims 4)");
+  if (!mesh->base_cells || !mesh->n_base_cells || !mesh->n_base_verts || mesh->n_layers < 1)
+    return cfail(ctx, FTK2B_INVALID_ARG, "extruded mesh needs base cells, vertices and at least one layer");
+  const unsigned long long S = mesh->n_base_verts, L = mesh->n_layers, nv = S * (L + 1);
+  if (S >= 0xFFFFFFFFull || nv >= 0xFFFFFFFFull) return cfail(ctx, FTK2B_UNSUPPORTED, "mesh too large");
+  if ((field->layout != FTK2B_LAYOUT_SEPARATE && field->layout != FTK2B_LAYOUT_PER_VERTEX) || field->nd != 1 ||
+      field->dims[0] < nv)
+    return cfail(ctx, FTK2B_INVALID_ARG, "extruded meshes read two per-vertex arrays of at least %llu values", nv);
+  const unsigned long long nc = mesh->n_base_cells;
+  std::vector<unsigned> tets(nc * 4);
+  std::vector<unsigned long long> tri_keys, edge_keys;
+  tri_keys.reserve(nc * 4);
+  edge_keys.reserve(nc * 6);
+  for (unsigned long long c = 0; c < nc; ++c) {
+    unsigned v[4];
+    for (int k = 0; k < 4; ++k) {
+      const uint64_t x = mesh->base_cells[c * 4 + k];
+      if (x >= S) return cfail(ctx, FTK2B_INVALID_ARG, "base cell %llu names vertex %llu of %llu", c,
+                               (unsigned long long)x, S);
+      v[k] = (unsigned)x;
+    }
+    std::sort(v, v + 4);
+    for (int k = 0; k < 4; ++k) tets[c * 4 + k] = v[k];
+    for (int r = 0; r < 4; ++r) {
+      unsigned w[3];
+      int k = 0;
+      for (int i = 0; i < 4; ++i)
+        if (i != r) w[k++] = v[i];
+      // 21 bits per id when they fit, else the rows are sorted as triples
+      tri_keys.push_back(((unsigned long long)w[0] << 42) | ((unsigned long long)w[1] << 21) | w[2]);
+    }
+    for (int i = 0; i < 4; ++i)
+      for (int j = i + 1; j < 4; ++j) edge_keys.push_back(((unsigned long long)v[i] << 32) | v[j]);
+  }
+  std::vector<unsigned> tris;
+  if (S < (1ull << 21)) {
+    std::sort(tri_keys.begin(), tri_keys.end());
+    tri_keys.erase(std::unique(tri_keys.begin(), tri_keys.end()), tri_keys.end());
+    tris.resize(3 * tri_keys.size());
+    for (size_t i = 0; i < tri_keys.size(); ++i) {
+      tris[3 * i] = (unsigned)(tri_keys[i] >> 42);
+      tris[3 * i + 1] = (unsigned)((tri_keys[i] >> 21) & 0x1FFFFF);
+      tris[3 * i + 2] = (unsigned)(tri_keys[i] & 0x1FFFFF);
+    }
+  } else {
+    std::vector<std::array<unsigned, 3>> t3;
+    t3.reserve(nc * 4);
+    for (unsigned long long c = 0; c < nc; ++c)
+      for (int r = 0; r < 4; ++r) {
+        std::array<unsigned, 3> w;
+        int k = 0;
+        for (int i = 0; i < 4; ++i)
+          if (i != r) w[k++] = tets[c * 4 + i];
+        t3.push_back(w);
+      }
+    std::sort(t3.begin(), t3.end());
+    t3.erase(std::unique(t3.begin(), t3.end()), t3.end());
+    tris.resize(3 * t3.size());
+    for (size_t i = 0; i < t3.size(); ++i)
+      for (int k = 0; k < 3; ++k) tris[3 * i + k] = t3[i][k];
+  }
+  std::sort(edge_keys.begin(), edge_keys.end());
+  edge_keys.erase(std::unique(edge_keys.begin(), edge_keys.end()), edge_keys.end());
+  std::vector<unsigned> edges(2 * edge_keys.size());
+  for (size_t i = 0; i < edge_keys.size(); ++i) {
+    edges[2 * i] = (unsigned)(edge_keys[i] >> 32);
+    edges[2 * i + 1] = (unsigned)(edge_keys[i] & 0xFFFFFFFFu);
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return cfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  DevBuf* B = ctx->contour;
+  C_TRY(B[kBufBaseCells].ensure(4 * tets.size()));
+  C_TRY(B[kBufFeTris].ensure(4 * tris.size()));
+  C_TRY(B[kBufFeEdges].ensure(4 * edges.size()));
+  C_TRY(cudaMemcpyAsync(B[kBufBaseCells].p, tets.data(), 4 * tets.size(), cudaMemcpyHostToDevice, ctx->stream));
+  C_TRY(cudaMemcpyAsync(B[kBufFeTris].p, tris.data(), 4 * tris.size(), cudaMemcpyHostToDevice, ctx->stream));
+  C_TRY(cudaMemcpyAsync(B[kBufFeEdges].p, edges.data(), 4 * edges.size(), cudaMemcpyHostToDevice, ctx->stream));
+  const size_t es = field->dtype == FTK2B_F64 ? 8 : 4;
+  const void* dev[2] = {field->comp[0], field->comp[1]};
+  if (field->location != FTK2B_DEVICE) {
+    const int slot[2] = {kBufField, kBufField2};
+    for (int j = 0; j < 2; ++j) {
+      C_TRY(B[slot[j]].ensure(nv * es));
+      C_TRY(cudaMemcpyAsync(B[slot[j]].p, field->comp[j], nv * es, cudaMemcpyHostToDevice, ctx->stream));
+      dev[j] = B[slot[j]].p;
+    }
+  }
+  // the upload of the host vectors must finish before they go out of scope
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return cfail(ctx, FTK2B_CUDA_ERROR, "mesh upload failed");
+  FeGeom g;
+  std::memset(&g, 0, sizeof(g));
+  g.S = S;
+  g.L = L;
+  g.nv = nv;
+  g.ntet = nc;
+  g.ntri = tris.size() / 3;
+  g.nedge = edges.size() / 2;
+  g.tets = static_cast<const unsigned*>(B[kBufBaseCells].p);
+  g.tris = static_cast<const unsigned*>(B[kBufFeTris].p);
+  g.edges = static_cast<const unsigned*>(B[kBufFeEdges].p);
+  auto* res = new (std::nothrow) ftk2b_fiber_surface_result;
+  if (!res) return cfail(ctx, FTK2B_OOM, "result allocation failed");
+  std::memset(res, 0, sizeof(*res));
+  res->n_simplices = (L + 1) * g.ntri + 2 * L * g.nedge + 2 * L * g.ntri;
+  const ftk2b_status st =
+      field->dtype == FTK2B_F64
+          ? run_fiber_surface_extruded<double>(ctx, g, dev[0], dev[1], thr[0], thr[1], sos_q, res)
+          : run_fiber_surface_extruded<float>(ctx, g, dev[0], dev[1], (float)thr[0], (float)thr[1], sos_q, res);
+  if (st != FTK2B_OK) {
+    ftk2b_fiber_surface_result_free(res);
+    return st;
+  }
+  *out = res;
+  return FTK2B_OK;
+}
+
 }  // namespace
 
 // Geometry of a regular mesh and its scalar array(s) for the level-set and
@@ -1830,13 +2418,18 @@ extern "C" ftk2b_status ftk2b_fiber_surface_extract(ftk2b_ctx* ctx, const ftk2b_
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field || !thresholds || !out) return cfail(ctx, FTK2B_INVALID_ARG, "null argument");
   *out = nullptr;
-  if (mesh->kind != FTK2B_MESH_REGULAR || mesh->ndims != 4)
-    return cfail(ctx, FTK2B_UNSUPPORTED, "fiber surfaces run on regular 3D+t meshes (ndims 4)");
   if (field->dtype != FTK2B_F32 && field->dtype != FTK2B_F64)
     return cfail(ctx, FTK2B_INVALID_ARG, "dtype must be FTK2B_F32 or FTK2B_F64");
+  if (!(sos_q > 0)) return cfail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
+  if (mesh->kind == FTK2B_MESH_EXTRUDED) {
+    if (field->ncomp != 2 || !field->comp[0] || !field->comp[1])
+      return cfail(ctx, FTK2B_INVALID_ARG, "fiber surfaces read two scalar arrays (ncomp 2)");
+    return fiber_surface_extruded(ctx, mesh, field, thresholds, sos_q, out);
+  }
+  if (mesh->kind != FTK2B_MESH_REGULAR || mesh->ndims != 4)
+    return cfail(ctx, FTK2B_UNSUPPORTED, "fiber surfaces run on 3D+t meshes (ndims 4)");
   if (field->ncomp != 2 || field->layout != FTK2B_LAYOUT_SEPARATE || !field->comp[0] || !field->comp[1])
     return cfail(ctx, FTK2B_INVALID_ARG, "fiber surfaces read two scalar arrays (ncomp 2, layout SEPARATE)");
-  if (!(sos_q > 0)) return cfail(ctx, FTK2B_INVALID_ARG, "sos_q must be positive");
   CtGeom g;
   size_t nelem = 1;
   {

@@ -404,8 +404,13 @@ ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, co
                                  const double thresholds[2], double sos_q, ftk2b_cp_result** out);
 
 /* Fiber surfaces: SimplicialEngine<T, FiberPredicate<T>>::execute +
- * get_complex on a regular 3D+t mesh (ndims 4).  field: ncomp 2, layout
- * SEPARATE (nd 4, indexed by local coordinates, or nd 1 by global vertex id).
+ * get_complex on a regular 3D+t mesh (ndims 4), or on an ExtrudedSimplicialMesh
+ * over tets (base_cell_dim 3; mesh.hpp:542-712).  field: ncomp 2, layout
+ * SEPARATE (regular: nd 4, indexed by local coordinates, or nd 1 by global
+ * vertex id; extruded: nd 1 per vertex id, or PER_VERTEX).  On extruded meshes
+ * the triangles inside the prisms over base triangles are ordered as the
+ * reference's patching meets them when it runs on one worker (with several
+ * workers it numbers them in thread-arrival order).
  * Features are the triangles of the 4-D mesh, in simplex order, with their
  * barycentrics (centroid where the solve fails); cells are the star-fan
  * triangles of form_general_manifold_patches (engine.hpp:1388-1413) as sorted,

@@ -627,10 +627,11 @@ struct FiberPredicate {
   T thresholds[2] = {(T)0.0, (T)0.0};
 };
 
-// SimplicialEngine<T, FiberPredicate<T>> on a regular mesh: 2D+t meshes give
-// triangle features joined by star edges (ftk2b_fiber_extract), 3D+t meshes
-// triangle features of the 4-D mesh with the star-fan triangles of
-// get_complex (ftk2b_fiber_surface_extract).
+// SimplicialEngine<T, FiberPredicate<T>> on a regular mesh or an
+// ExtrudedSimplicialMesh (per-vertex arrays): 2D+t meshes give triangle
+// features joined by star edges (ftk2b_fiber_extract), 3D+t meshes triangle
+// features of the 4-D mesh with the star-fan triangles of get_complex
+// (ftk2b_fiber_surface_extract).
 template <typename T>
 class SimplicialEngine<T, FiberPredicate<T>> {
  public:
@@ -650,7 +651,6 @@ class SimplicialEngine<T, FiberPredicate<T>> {
     const std::string n1 = vars.size() >= 2 ? vars[1] : pred_.var_names[1];
     const Array* a[2] = {&data.at(n0), &data.at(n1)};
     ftk2b_mesh_desc md = mesh_->desc();
-    if (md.kind != FTK2B_MESH_REGULAR) throw Error(FTK2B_UNSUPPORTED, "fibers need a regular mesh");
     using E = std::remove_cv_t<std::remove_pointer_t<decltype(a[0]->pdata())>>;
     std::vector<T> conv[2];
     ftk2b_field_desc fd;

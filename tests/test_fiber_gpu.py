@@ -172,3 +172,80 @@ def test_fiber_extruded_matches_reference_fixture(ctx, name):
     r = ctx.fiber(mesh, fd, case["thresholds"], case["q"])
     assert len(r.track_id) == len(g["track_id"]) > 0
     assert_same(r, {k: g[k] for k in ("simplices", "bary", "lam", "track_id", "edges")}, name)
+
+
+# ---------------------------------------------------------------------------
+# fiber surfaces on ExtrudedSimplicialMesh over tets (the reference numbers the
+# triangles inside its prisms as its one-worker patching meets them)
+
+FS_EXT_GOLD = os.path.join(os.path.dirname(__file__), "golden", "fiber_surface_extruded")
+
+
+def run_fs_ext(ctx, case, device=False, layout=api.LAYOUT_SEPARATE):
+    keep: list = []
+    nv = case["coords"].shape[0]
+    mesh = api.extruded_mesh_desc(nv, case["cells"], case["n_layers"], keep)
+    arrays = list(case["fields"])
+    if device:
+        import torch
+        arrays = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in arrays]
+        keep.append(arrays)
+    fd = api.field_desc(arrays, layout, 2, keep=keep)
+    return ctx.fiber_surface(mesh, fd, case["thresholds"], case["q"])
+
+
+def assert_same_surface(r, want, cells, name=""):
+    assert len(r.track_id) == len(want["track_id"]) > 0, name
+    assert np.array_equal(r.simplices, want["simplices"]), name
+    assert np.array_equal(r.bary.view(np.uint32), want["bary"].view(np.uint32)), name
+    assert np.array_equal(r.lam.view(np.uint64), want["lam"].view(np.uint64)), name
+    assert np.array_equal(r.track_id, want["track_id"]), name
+    assert np.array_equal(r.cells, cells), name
+    assert r.n_tracks == len(set(r.track_id.tolist()))
+    assert not r.scalar.any()
+
+
+@pytest.mark.parametrize("name", list(contour_cases.FIBER_SURFACE_EXTRUDED_CASES))
+def test_extruded_fiber_surface_matches_reference_fixture(ctx, name):
+    """Features (spatial, over base edges, inside prisms), barycentrics with
+    the centroid fallback, star-fan triangles and tracks equal the reference's
+    one-worker run bit for bit."""
+    case = contour_cases.FIBER_SURFACE_EXTRUDED_CASES[name]()
+    g = np.load(os.path.join(FS_EXT_GOLD, f"{name}.npz"))
+    assert_same_surface(run_fs_ext(ctx, case), g, g["cells"], name)
+
+
+def test_extruded_fiber_surface_device_input_and_per_vertex_layout(ctx):
+    case = contour_cases.FIBER_SURFACE_EXTRUDED_CASES["fs_ext_gauss_f64"]()
+    a = run_fs_ext(ctx, case)
+    for r in (run_fs_ext(ctx, case, device=True), run_fs_ext(ctx, case, layout=api.LAYOUT_PER_VERTEX)):
+        assert_same_surface(r, {"simplices": a.simplices, "bary": a.bary, "lam": a.lam, "track_id": a.track_id},
+                            a.cells)
+
+
+def test_extruded_fiber_surface_vs_live_reference_and_restatement(ctx):
+    case = contour_cases.fs_ext_seeded()
+    r = run_fs_ext(ctx, case)
+    keep: list = []
+    mesh = bridge.make_extruded_mesh(case["coords"], case["cells"], case["n_layers"], keep)
+    o = bridge.run_restatement(mesh, bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2,
+                                                       sos_q=case["q"], keep=keep, fiber_thr=case["thresholds"]))
+    assert len(r.track_id) > 500
+    assert_same_surface(r, {"simplices": o.simplices, "bary": o.bary, "lam": o.lam, "track_id": o.track_id},
+                        o.cells, "restatement")
+    if bridge.ref_available():
+        raw = bridge.make_field(list(case["fields"]), bridge.LAYOUT_SEPARATE, 2, sos_q=case["q"], keep=keep)
+        ref, cells = bridge.run_reference_fiber_surface(mesh, raw, case["thresholds"], one_thread=True)
+        assert_same_surface(r, {"simplices": ref.simplices, "bary": ref.bary, "lam": ref.lam,
+                                "track_id": ref.track_id}, cells, "reference")
+
+
+def test_extruded_fiber_surface_python_mirror(ctx):
+    case = contour_cases.FIBER_SURFACE_EXTRUDED_CASES["fs_ext_f32_thresholds"]()
+    g = np.load(os.path.join(FS_EXT_GOLD, "fs_ext_f32_thresholds.npz"))
+    base = api.UnstructuredSimplicialMesh(3, 3, case["coords"], case["cells"])
+    mesh = api.ExtrudedSimplicialMesh(base, case["n_layers"])
+    pred = api.FiberPredicate(var_names=["F", "G"], thresholds=case["thresholds"], sos_q=case["q"])
+    eng = api.SimplicialEngine(mesh, pred, ctx)
+    eng.execute({"F": case["fields"][0], "G": case["fields"][1]})
+    assert_same_surface(eng.get_complex(), g, g["cells"])
