@@ -44,6 +44,7 @@ INFO_LAST_CANDIDATES = 103
 OPT_BLOCKING_SYNC = 5
 OPT_CULL_MODE = 6
 OPT_BATCH_TIME_CHUNK = 7
+OPT_TEST_STALL_POLLS = 8
 CLASS_NAMES = ["none", "degenerate", "source", "sink", "saddle", "spiral_source", "spiral_sink",
                "center"]
 

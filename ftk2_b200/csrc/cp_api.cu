@@ -216,6 +216,10 @@ extern "C" ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t
       if (value < 0 || value > 2) return fail(ctx, FTK2B_INVALID_ARG, "cull mode is 0, 1 or 2");
       ctx->cull_mode = (int)value;
       return FTK2B_OK;
+    case FTK2B_OPT_TEST_STALL_POLLS:
+      if (value < 0 || value > (1 << 22)) return fail(ctx, FTK2B_INVALID_ARG, "stall polls out of range");
+      ctx->stall_polls = (int)value;
+      return FTK2B_OK;
     case FTK2B_OPT_BATCH_TIME_CHUNK:
       if (value < 0 || value > 65535) return fail(ctx, FTK2B_INVALID_ARG, "batch time chunk out of range");
       ctx->batch.tchunk = (int)value;
@@ -239,6 +243,7 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_OPT_BLOCKING_SYNC: *value = ctx->blocking_sync ? 1 : 0; return FTK2B_OK;
     case FTK2B_OPT_CULL_MODE: *value = ctx->cull_mode; return FTK2B_OK;
     case FTK2B_OPT_BATCH_TIME_CHUNK: *value = ctx->batch.tchunk; return FTK2B_OK;
+    case FTK2B_OPT_TEST_STALL_POLLS: *value = ctx->stall_polls; return FTK2B_OK;
     default: return fail(ctx, FTK2B_INVALID_ARG, "unknown option %d", option);
   }
 }
@@ -654,6 +659,10 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
   cfg.Q = prm->sos_q;
   cfg.refined = prm->precision == FTK2B_PRECISION_REFINED;
   cfg.cull_mode = ctx->cull_mode;  // 2 is resolved below, once the buffers exist
+  if (ctx->stall_polls > 0) {  // the failure-path check runs in the fused cull
+    cfg.stall_polls = ctx->stall_polls;
+    cfg.cull_mode = 0;
+  }
   if (fiber_thr) {
     cfg.fiber = 1;
     cfg.fthr[0] = fiber_thr[0];

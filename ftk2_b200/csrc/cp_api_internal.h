@@ -148,6 +148,7 @@ struct ftk2b_ctx {
   int cull_mode = 2;  // FTK2B_OPT_CULL_MODE (2: chosen per workload shape)
   int last_cull_mode = 0;  // the mode the last regular-mesh extraction ran
   unsigned long long last_candidates = 0;  // hypercubes the last regular-mesh cull kept
+  int stall_polls = 0;                     // FTK2B_OPT_TEST_STALL_POLLS
   std::vector<ftk2b::CullTune> cull_tunes;
   bool disable_tma = false;
   int last_used_tma = 0;

@@ -72,6 +72,10 @@ struct ExtractConfig {
   int tiles[3];                // tiles along x, y, z (z = 1 for 2D)
   int skip_first_spatial;      // 1: no purely spatial simplices at local time 0
   int cull_mode;               // 0: per-vertex cull words only; 1: tile statistics first
+  // > 0: failure-path check of the fused cull: after its first slice every
+  // block waits, at most this many polls, on an mbarrier nothing completes,
+  // and leaves through the timeout path (the call reports FTK2B_TIMEOUT)
+  int stall_polls;
   // FiberPredicate<T> (predicate.hpp:341-362): every hypercube is a candidate
   // (the cull words assume the solve must succeed), values are taken minus
   // fthr[j], and a simplex whose solve fails is kept at the centroid

@@ -57,10 +57,12 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
                : "memory");
 }
 
-// Bounded wait for the phase of the given parity; false if it never completed.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// Bounded wait for the phase of the given parity (at most `limit` polls);
+// false if it never completed.
+constexpr int kWaitPolls = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit = kWaitPolls) {
   const unsigned a = smem_addr(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
+  for (int it = 0; it < limit; ++it) {
     unsigned ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -451,7 +453,11 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   if (t0 + 1 <= s_end) issue(t0 + 1, 1);
   int slot_a = 0;  // word slot of slice ct
   {
-    const bool ok = wait(t0, 0);
+    bool ok = wait(t0, 0);
+    // failure-path check (host option): after the first slice has landed,
+    // wait on bar[2], which nothing ever completes, with the caller's short
+    // poll bound; the block then leaves through the bounded-wait error path
+    if (ok && mbar && cfg.stall_polls > 0) ok = mbar_wait(&bar[2], 0u, cfg.stall_polls);
     if (ok) words(0, slot_a, t0);
     if (__syncthreads_or(!ok)) {
       // give the other copy in flight a bounded chance to land before leaving
@@ -563,13 +569,15 @@ __global__ void __launch_bounds__(kThreads, 2)
                            const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa,
                            ExtractConfig cfg, CandidateQueue cq, unsigned* err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ unsigned long long bar[2];
+  __shared__ unsigned long long bar[3];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, kThreads);  // visible after the tile's first barrier
-  // TMA tensor copies and bulk row copies complete on these mbarriers
+  // TMA tensor copies and bulk row copies complete on bar[0..1]; bar[2] only
+  // serves the failure-path check and never completes
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   unsigned ph[2] = {0u, 0u};
@@ -1441,7 +1449,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     batch_cull_kernel(const BatchField* __restrict__ fields, const unsigned* __restrict__ item_base, int nf,
                       unsigned n_items, unsigned* item_next, CandidateQueue cq, unsigned* err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ unsigned long long bar[2];
+  __shared__ unsigned long long bar[3];
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned s_item, s_field;
   __shared__ unsigned s_ib[kBatchSmemFields];
@@ -1453,6 +1461,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   unsigned ph[2] = {0u, 0u};

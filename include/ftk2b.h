@@ -147,6 +147,9 @@ enum {
   FTK2B_OPT_BLOCKING_SYNC = 5,    /* 1: wait for the device by blocking, not spinning (servers set it) */
   FTK2B_OPT_CULL_MODE = 6,        /* 0: per-vertex cull words only; 1: tile statistics first; 2 (default):
                                      the faster of the two, timed once per workload shape by the context */
+  FTK2B_OPT_TEST_STALL_POLLS = 8, /* > 0: failure-path check -- the regular-mesh cull blocks wait, at most
+                                     this many polls, on an mbarrier nothing completes, so the call returns
+                                     FTK2B_TIMEOUT with every copy landed; 0 (default): off */
   FTK2B_OPT_BATCH_TIME_CHUNK = 7  /* batches: corner time steps per cull item (0, default: chosen by the
                                      context, timed once per batch shape) */
 };

@@ -355,3 +355,22 @@ def test_many_features_grow_past_the_short_chain():
     assert len(r.track_id) > 16384
     assert_identical(r, oracle_run(case))
 
+
+@pytest.mark.parametrize("staging", ["tma", "bulk"])
+def test_bounded_wait_runs_out_and_context_recovers(staging):
+    """Failure path without a fault: with the stall option every cull block,
+    once its first slice has landed, waits a few polls on an mbarrier that
+    nothing completes, leaves through the bounded-wait path (the other copy in
+    flight waited for) and the call reports FTK2B_TIMEOUT; the same context
+    then gives the restatement's result."""
+    case = _medium_cases()[0]
+    with api.Context(0) as c:
+        c.set_option(api.OPT_DISABLE_TMA, 1 if staging == "bulk" else 0)
+        c.set_option(api.OPT_TEST_STALL_POLLS, 64)
+        with pytest.raises(api.Ftk2bError) as e:
+            gpu_run(c, case)
+        assert e.value.status == api.TIMEOUT
+        c.set_option(api.OPT_TEST_STALL_POLLS, 0)
+        assert_identical(gpu_run(c, case), oracle_run(case))
+        assert c.get_option(api.INFO_LAST_TMA) == (1 if staging == "tma" else 0)
+
