@@ -62,8 +62,9 @@ def test_merge_of_slabs_equals_whole_mesh(name, n):
     run = orc_extract(field, m, q)
     whole = run(api.regular_mesh_desc(dims))
     assert len(whole.track_id) > 0
-    parts = [run(sharded.slab_mesh(dims, t0, t1)) for t0, t1 in sharded.slab_bounds(dims[-1], n)]
-    same(sharded.merge(parts), whole)
+    bounds = sharded.slab_bounds(dims[-1], n)
+    parts = [run(sharded.slab_mesh(dims, t0, t1)) for t0, t1 in bounds]
+    same(sharded.merge(parts, bounds, dims), whole)
 
 
 def _free_port():
