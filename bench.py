@@ -544,8 +544,78 @@ def north_star_summary(line):
         "c3_identical": b.get("identical_to_plain"),
         "serve_p50_p99_ms": (sv.get("p50_ms"), sv.get("p99_ms")),
         "serve_req_s": sv.get("throughput_req_s"),
+        "serve_capacity_req_s": line.get("serve_sweep", {}).get("capacity_req_s"),
     }
     return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in out.items()}
+
+
+def run_sharded(args, rank, world, local):
+    """The headline field split into time slabs, one per rank (each rank
+    generates and holds only its slab, as separate component arrays indexed
+    from the slab's offset), each slab extracted on its GPU and the exchange
+    of ftk2_b200.sharded run over NCCL; a step = the slab extractions plus the
+    exchange, timed on the device, max over ranks.  value = simplices of the
+    whole mesh per second (strong scaling)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from ftk2_b200 import api, generate, sharded
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        import socket
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+        sk.close()
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    dims = list(DIMS) + [NT]
+    bounds = sharded.slab_bounds(NT, world)
+    ctx = api.Context(local)
+    keep: list = []
+    fd = mesh = None
+    if rank < len(bounds):
+        t0, t1 = bounds[rank]
+        f = generate.gaussian_field_device(DIMS, t1 - t0 + 1, seed=1234, n_blobs=32, dtype=torch.float64, t0=t0)
+        comps = [f[..., j].contiguous() for j in range(3)]
+        del f
+        fd = api.field_desc(comps, api.LAYOUT_SEPARATE, 3, keep=keep)
+        mesh = sharded.slab_mesh(dims, t0, t1)
+    prm = api.params(SOS_Q)
+
+    def extractor(m, a, b):
+        return ctx.extract(mesh, fd, prm)
+
+    for _ in range(max(args.warmup, 3)):
+        sharded.extract_sharded(dims, None, 3, extractor=extractor)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        shard = sharded.extract_sharded(dims, None, 3, extractor=extractor)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t) * 1e3 / args.steps
+    tt = torch.tensor([ms], dtype=torch.float64, device="cuda" if world > 1 else "cpu")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    ms = float(tt.item())
+    nsimp = kuhn_simplex_count(dims, 3)
+    nfeat = torch.tensor([len(shard.track_id)], dtype=torch.int64, device="cuda" if world > 1 else "cpu")
+    if world > 1:
+        dist.all_reduce(nfeat)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": nsimp / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+                          "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": dict(CONFIG, parallelism=f"time-slabs{world}"),
+                          "result": {"features": int(nfeat.item()), "simplices": nsimp},
+                          "timing": "host wall clock around the slab extractions and the exchange, max over ranks"}),
+              flush=True)
+    ctx.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
 
 
 def main():
@@ -558,10 +628,15 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="only the headline workload (no precision / serving measurements)")
     ap.add_argument("--serve-seconds", type=float, default=5.0)
+    ap.add_argument("--shard", action="store_true",
+                    help="split the headline field into time slabs across the ranks (strong scaling) "
+                         "instead of one replica per rank")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.shard:
+        return run_sharded(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -678,6 +753,9 @@ def main():
         torch.cuda.empty_cache()
         from ftk2_b200 import serving
         line["serve"] = serving.run(duration_s=args.serve_seconds, device=local)
+        line["serve"].pop("slowest", None)
+        torch.cuda.empty_cache()
+        line["serve_sweep"] = serving.sweep(device=local)
         torch.cuda.empty_cache()
         line["contour"] = contour_c2(ctx)
         torch.cuda.empty_cache()

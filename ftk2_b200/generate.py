@@ -15,8 +15,9 @@ from .synthetic import gaussian_blobs
 
 def gaussian_field_device(dims, nt: int, seed: int = 1234, n_blobs: int = 32, dtype=None,
                           noise: float = 0.0, noise_seed: int | None = None, sigma=(4.0, 12.0),
-                          drift: float = 0.5, scale: float = 1.0, device: str = "cuda"):
+                          drift: float = 0.5, scale: float = 1.0, device: str = "cuda", t0: int = 0):
     """Analytic gradient of a drifting Gaussian sum, shape (nt, [nz,] ny, nx, ndim),
+    timesteps t0 .. t0 + nt - 1 (t0 > 0 only without noise),
     multiplied by ``scale`` (e.g. the box side for gradients per box length),
     plus ``noise`` * N(0,1)."""
     import torch
@@ -33,7 +34,7 @@ def gaussian_field_device(dims, nt: int, seed: int = 1234, n_blobs: int = 32, dt
     for k in range(nt):
         acc = torch.zeros(shape + (ndim,), dtype=torch.float64, device=device)
         for b in range(n_blobs):
-            c = blobs["centers"][b] + blobs["vel"][b] * k
+            c = blobs["centers"][b] + blobs["vel"][b] * (k + t0)
             s2 = float(blobs["sigma"][b]) ** 2
             d = []
             for i in range(ndim):

@@ -172,6 +172,30 @@ def run(duration_s: float = 5.0, rate: float = 200.0, p_push: float = 0.2, n_slo
     return out
 
 
+def sweep(rates=(200, 500, 1000, 2000, 4000, 8000), duration_s: float = 1.5, n_slots: int = 4,
+          one_slot_rates=(1000, 4000), seed: int = 5, device: int = 0):
+    """Offered-rate sweep: throughput and p50 / p99 latency per Poisson rate
+    (the same request mix and pools), until the server saturates; plus the
+    same load on one worker slot at some rates, which shows what admitting
+    requests into free slots while others run buys over a single queue."""
+    pools = make_pools(seed)
+    rows = []
+
+    def row(rate, slots):
+        r = run(duration_s=duration_s, rate=rate, n_slots=slots, seed=seed, pools=pools, device=device,
+                warm_pushes=2)
+        return {"offered_req_s": rate, "slots": slots, "served_req_s": round(r["throughput_req_s"], 1),
+                "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "failed": r["failed"],
+                "max_in_flight": r["max_in_flight"]}
+
+    for rate in rates:
+        rows.append(row(rate, n_slots))
+    for rate in one_slot_rates:
+        rows.append(row(rate, 1))
+    best = max((x for x in rows if x["slots"] == n_slots), key=lambda x: x["served_req_s"])
+    return {"duration_s_per_rate": duration_s, "rows": rows, "capacity_req_s": best["served_req_s"]}
+
+
 if __name__ == "__main__":
     import json
     import sys
