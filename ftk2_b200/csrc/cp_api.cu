@@ -259,7 +259,8 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   std::vector<DevBuf*> v = {&stage[0], &stage[1], &stage[2], &stage_scalar, &key, &lam, &bary4,
                             &scalar, &key_alt, &perm0, &perm1, &hist, &lam_s, &bary4_s, &scalar_s,
                             &simplices, &bary, &track, &edge_cnt, &edges, &parent, &counters,
-                            &cls, &cand_corner, &cand_chains, &edge_slots, &tstats, &runs};
+                            &cls, &cand_corner, &cand_chains, &edge_slots, &tstats, &runs, &refine_vals,
+                            &refine_pairs};
   for (auto& b : extra) v.push_back(&b);
   for (DevBuf* b : ext.bufs()) v.push_back(b);
   for (DevBuf* b : batch.bufs()) v.push_back(b);
@@ -690,12 +691,19 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     if (nloc > 0xFFFFFFF0ull) return fail(ctx, FTK2B_UNSUPPORTED, "mesh too large for fiber extraction");
     ccap = std::max<unsigned>(ccap, (unsigned)nloc);
   }
+  // simplices listed for the exact test: a few per surviving hypercube (every
+  // chain in fiber mode); grows on overflow
+  const unsigned long long pc0 = fiber_thr ? (unsigned long long)ccap * nch : (unsigned long long)ccap * 8;
+  unsigned pcap = ctx->pair_cap_hint ? ctx->pair_cap_hint : (unsigned)std::min<unsigned long long>(pc0, 0xFFFFFFF0ull);
+  if (fiber_thr) pcap = (unsigned)std::max<unsigned long long>(pcap, std::min<unsigned long long>(pc0, 0xFFFFFFF0ull));
   for (int attempt = 0; attempt < 4; ++attempt) {
     const unsigned edge_cap = cap * 2;
     st = ensure_feature_buffers(ctx, cap, edge_cap, m);
     if (st) return st;
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
+    CUDA_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * (1u << d) * m * (field->dtype == FTK2B_F64 ? 8 : 4)));
+    CUDA_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)pcap));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -709,6 +717,11 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cq.chains = (unsigned long long*)ctx->cand_chains.p;
     cq.count = (unsigned*)ctx->counters.p + kCountCand;
     cq.cap = ccap;
+    RefineStage rs;
+    rs.vals = ctx->refine_vals.p;
+    rs.pairs = (unsigned long long*)ctx->refine_pairs.p;
+    rs.count = (unsigned*)ctx->counters.p + kCountPairs;
+    rs.cap = pcap;
     const int f64 = field->dtype == FTK2B_F64;
     // the device pipeline in two parts so that the fused cull kernel can be
     // timed on its own: [counters reset, cull] and [exact tests, canonical
@@ -728,8 +741,8 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     };
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e;
-      if ((e = launch_refine_regular(f64, rm, fa, cfg, cq, sink, ctx->num_sms, ctx->stream))) return e;
-      *nl += 1;
+      if ((e = launch_refine_staged(f64, rm, fa, cfg, cq, rs, sink, ctx->num_sms, ctx->stream))) return e;
+      *nl += 2;
       if ((e = launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, nl))) return e;
       if (prm->classify && !cfg.fiber) {
         if ((e = launch_classify_regular(f64, rm, fa, nch, B, ctx->stream))) return e;
@@ -768,6 +781,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       key.cfg = cfg;
       key.cap = cap;
       key.ccap = ccap;
+      key.pcap = pcap;
       key.edge_cap = edge_cap;
       key.f64 = f64;
       key.want_edges = prm->want_edges;
@@ -861,6 +875,13 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       if (want > 0xFFFFFFF0ull) return fail(ctx, FTK2B_OVERFLOW_RETRY, "candidate count exceeds 2^32");
       ccap = (unsigned)want;
       ctx->cand_cap_hint = ccap;
+      continue;
+    }
+    if (h[kCountPairs] > pcap) {
+      const uint64_t want = (uint64_t)h[kCountPairs] + h[kCountPairs] / 4 + 1024;
+      if (want > 0xFFFFFFF0ull) return fail(ctx, FTK2B_OVERFLOW_RETRY, "listed simplex count exceeds 2^32");
+      pcap = (unsigned)want;
+      ctx->pair_cap_hint = pcap;
       continue;
     }
     if (h[kCountFeatures] > cap || h[kCountEdges] > edge_cap) {

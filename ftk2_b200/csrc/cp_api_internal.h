@@ -31,6 +31,7 @@ enum {
   kCountErr = 3,
   kCountCand = 4,
   kCountItems = 5,  // batches: next cull item
+  kCountPairs = 6,  // simplices listed for the exact test
   kNumCounters = 8
 };
 
@@ -40,7 +41,7 @@ struct RegularGraphKey {
   RegularMesh rm;
   FieldAccess fa;
   ExtractConfig cfg;
-  unsigned cap, ccap, edge_cap;
+  unsigned cap, ccap, edge_cap, pcap;
   int f64, want_edges, classify, allow_tma, key_bits, nch;
 };
 
@@ -144,6 +145,7 @@ struct ftk2b_ctx {
   std::string err;
   unsigned cap_hint = 0;
   unsigned cand_cap_hint = 0;
+  unsigned pair_cap_hint = 0;
   int tune_tchunk = 0;
   int cull_mode = 2;  // FTK2B_OPT_CULL_MODE (2: chosen per workload shape)
   int last_cull_mode = 0;  // the mode the last regular-mesh extraction ran
@@ -154,7 +156,8 @@ struct ftk2b_ctx {
   int last_used_tma = 0;
   ftk2b::DevBuf stage[3], stage_scalar;
   ftk2b::DevBuf key, lam, bary4, scalar, key_alt, perm0, perm1, hist, lam_s, bary4_s, scalar_s,
-      simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains, edge_slots;
+      simplices, bary, track, edge_cnt, edges, parent, counters, cls, cand_corner, cand_chains, edge_slots,
+      refine_vals, refine_pairs;
   ftk2b::DevBuf tstats, runs;  // cull mode 1 scratch (tile statistics, run list + count)
   std::vector<ftk2b::DevBuf> extra;
   ftk2b::DevBuf attr_out, attr_desc, attr_stage[16];  // ftk2b_cp_attributes

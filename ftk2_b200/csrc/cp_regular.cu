@@ -1437,6 +1437,203 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 }
 
 // ---------------------------------------------------------------------------
+// Exact test in two launches (the single-field path):
+//   refine_gather_kernel  one warp per candidate hypercube: its 2^D vertices'
+//                         values into a staging block (global memory, read
+//                         back from L2), their cull words, and the chains
+//                         whose words survive listed as (candidate, chain)
+//   refine_pairs_kernel   one thread per listed simplex: the exact SoS test,
+//                         the solve, and the warp-ballot compaction of the
+//                         accepted simplices
+// The gather is latency-bound and light, so it runs at high occupancy; the
+// integer SoS and the solve then keep every lane busy instead of the few
+// chains of a hypercube that survive its word test.
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(RegularMesh mesh, FieldAccess fa,
+                                                                          ExtractConfig cfg, CandidateQueue cq,
+                                                                          RefineStage rs) {
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;
+  __shared__ T cube[kRefineWarps][NV * M];
+  __shared__ unsigned band_tbl[kBandTable];
+  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const ChainTable& CT = c_chains[D - 3];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned n = min(*cq.count, cq.cap);
+  const unsigned gw = blockIdx.x * kRefineWarps + wib;
+  const unsigned nw = gridDim.x * kRefineWarps;
+  T* const my = cube[wib];
+  for (unsigned c = gw; c < n; c += nw) {
+    const unsigned long long pc = cq.corner[c], chains = cq.chains[c];
+    const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                            (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+    long long g0[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+      g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+    }
+    T* out = static_cast<T*>(rs.vals) + (size_t)c * (NV * M);
+    for (int e = lane; e < NV * M; e += 32) {
+      const int v = e / M, j = e % M;
+      long long g[4];
+      unsigned long long vid = 0;
+      bool in = true;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
+        if (k < D) {
+          in &= g[k] - mesh.off[k] < mesh.ld[k];
+          vid += (unsigned long long)g[k] * mesh.gstride[k];
+        }
+      }
+      T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
+      if (cfg.fiber) val = fp<T>::sub(val, (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
+      my[e] = val;
+      out[e] = val;
+    }
+    __syncwarp();
+    unsigned vw = kAbsent;
+    if (lane < NV) {
+      unsigned h[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) h[j] = hi_word<T>(my[lane * M + j]);
+      bool in = true;
+#pragma unroll
+      for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
+      vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
+    }
+    for (int base = 0; base < CT.n; base += 32) {
+      const int ch = base + lane;
+      bool live = ch < CT.n && ((chains >> ch) & 1ull);
+      unsigned wacc = kAbsent;
+#pragma unroll
+      for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, live ? (i ? CT.mask[ch][i - 1] : 0) : 0);
+      live = live && (cfg.fiber || !word_culled(wacc));
+      const unsigned ball = __ballot_sync(0xFFFFFFFFu, live);
+      if (!ball) continue;
+      unsigned b0 = 0;
+      if (lane == 0) b0 = atomicAdd(rs.count, (unsigned)__popc(ball));
+      b0 = __shfl_sync(0xFFFFFFFFu, b0, 0);
+      if (live) {
+        const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
+        if (idx < rs.cap) rs.pairs[idx] = ((unsigned long long)c << 6) | (unsigned long long)ch;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
+                                                                            ExtractConfig cfg, CandidateQueue cq,
+                                                                            RefineStage rs, FeatureSink sink) {
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;
+  const ChainTable& CT = c_chains[D - 3];
+  const int lane = threadIdx.x & 31;
+  const unsigned np = min(*rs.count, rs.cap);
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x; base < np; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool acc = false;
+    double lam_out[4] = {0, 0, 0, 0};
+    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+    float sc_out = 0.f;
+    unsigned long long key = 0;
+    if (i < np) {
+      const unsigned long long p = rs.pairs[i];
+      const unsigned c = (unsigned)(p >> 6);
+      const int ch = (int)(p & 63);
+      int mk[M + 1];
+      mk[0] = 0;
+#pragma unroll
+      for (int k = 0; k < M; ++k) mk[k + 1] = CT.mask[ch][k];
+      const T* src = static_cast<const T*>(rs.vals) + (size_t)c * (NV * M);
+      T vals[M + 1][M];
+#pragma unroll
+      for (int k = 0; k <= M; ++k)
+#pragma unroll
+        for (int j = 0; j < M; ++j) vals[k][j] = src[mk[k] * M + j];
+      bool inside;
+      if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
+      else inside = sos_inside3<T>(vals, cfg.Q);
+      if (inside) {
+        T lam[M + 1];
+        bool solved = solve_exact<M, T>(vals, lam);
+        if (!solved && cfg.fiber) {
+          // FiberPredicate keeps the simplex at the centroid: (T)1.0 / 3.0
+#pragma unroll
+          for (int k = 0; k <= M; ++k) lam[k] = (T)((double)(T)1.0 / 3.0);
+          solved = true;
+        }
+        if (solved) {
+          acc = true;
+          const unsigned long long pc = cq.corner[c];
+          const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                                  (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+          long long g0[4];
+          unsigned long long vid0 = 0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+            g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+            if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
+          }
+          key = vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
+#pragma unroll
+          for (int k = 0; k <= M; ++k) {
+            lam_out[k] = (double)lam[k];
+            bary_out[k] = (float)lam[k];
+          }
+          if (fa.has_scalar) {
+            using F = fp<T>;
+            T sc = T(0);
+#pragma unroll
+            for (int k = 0; k <= M; ++k) {
+              long long gv[4];
+              unsigned long long vid = 0;
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                gv[q] = (q < D) ? g0[q] + ((mk[k] >> q) & 1) : 0;
+                if (q < D) vid += (unsigned long long)gv[q] * mesh.gstride[q];
+              }
+              sc = F::add(sc, F::mul(lam[k], scalar_at<T>(fa, gv, D, vid)));
+            }
+            sc_out = (float)sc;
+          }
+          if (cfg.refined) {
+            double rr[M + 1];
+            if (solve_refined<M, T>(vals, rr))
+#pragma unroll
+              for (int k = 0; k <= M; ++k) lam_out[k] = rr[k];
+          }
+        }
+      }
+    }
+    const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
+    if (!ball) continue;
+    unsigned b0 = 0;
+    const int leader = __ffs(ball) - 1;
+    if (lane == leader) b0 = atomicAdd(sink.count, (unsigned)__popc(ball));
+    b0 = __shfl_sync(0xFFFFFFFFu, b0, leader);
+    if (!acc) continue;
+    const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
+    if (idx < sink.cap) {
+      sink.key[idx] = key;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        sink.lam[4 * (size_t)idx + k] = lam_out[k];
+        sink.bary4[4 * (size_t)idx + k] = bary_out[k];
+      }
+      sink.scalar[idx] = sc_out;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Batches: every field's tiles in one persistent launch, every candidate of
 // the batch in one exact-test launch.  Each item runs the single-field code
 // (cull_tile, refine_candidate) with its field's record, so a field's
@@ -1863,6 +2060,31 @@ __global__ void fiber_candidates_kernel(RegularMesh mesh, CandidateQueue cq) {
 cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueue& cq, int num_sms,
                                     cudaStream_t st) {
   fiber_candidates_kernel<<<num_sms * 8, 256, 0, st>>>(mesh, cq);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refine_staged(int f64, const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                                 const CandidateQueue& cq, const RefineStage& rs, const FeatureSink& sink, int num_sms,
+                                 cudaStream_t st) {
+  const int thr = kRefineWarps * 32;
+  const int g1 = num_sms * 16, g2 = num_sms * 8;
+  if (mesh.d == 4) {
+    if (f64) {
+      refine_gather_kernel<double, 4><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
+      refine_pairs_kernel<double, 4><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+    } else {
+      refine_gather_kernel<float, 4><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
+      refine_pairs_kernel<float, 4><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+    }
+  } else {
+    if (f64) {
+      refine_gather_kernel<double, 3><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
+      refine_pairs_kernel<double, 3><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+    } else {
+      refine_gather_kernel<float, 3><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
+      refine_pairs_kernel<float, 3><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+    }
+  }
   return cudaGetLastError();
 }
 
