@@ -84,19 +84,23 @@ __device__ __forceinline__ void fill_band_table(unsigned* tbl, int tid, int nthr
 template <typename T, int M>
 __device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M], const unsigned* band_tbl) {
   using P = CullParams<T>;
-  unsigned b = 0;
-#pragma unroll
-  for (int j = 0; j < M; ++j) b = max(b, h[j] & 0x7FFFFFFFu);
-  const unsigned kexp = (unsigned)P::kappa_exp << P::mant;
-  const unsigned thr = b > kexp ? b - kexp : 0u;  // high word of kappa' * b
-  unsigned w = 0;
+  unsigned a[M], b = 0;
 #pragma unroll
   for (int j = 0; j < M; ++j) {
-    // positive and |v| > thr  <=>  (int)h > (int)thr  (thr >= 0)
-    // negative and |v| > thr  <=>  h > thr | sign bit   (unsigned)
-    w |= ((int)h[j] > (int)thr ? 1u : 0u) << j;
-    w |= (h[j] > (thr | 0x80000000u) ? 1u : 0u) << (3 + j);
+    a[j] = h[j] & 0x7FFFFFFFu;
+    b = max(b, a[j]);
   }
+  const unsigned kexp = (unsigned)P::kappa_exp << P::mant;
+  const unsigned thr = max(b, kexp) - kexp;  // high word of kappa' * b (0 below kappa')
+  // component j strong: |v_j| > thr; the sign bit then picks bit j
+  // (positive) or bit 3 + j (negative)
+  unsigned strong = 0, neg = 0;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    strong |= (a[j] > thr ? 1u : 0u) << j;
+    neg |= (h[j] >> 31) << j;
+  }
+  unsigned w = (strong & ~neg) | ((strong & neg) << 3);
   w |= (b < P::tiny_hi ? 1u : 0u) << 6;
   const int rel1 = (int)(b >> P::mant) - P::bias - kElo + 1;
   w |= band_tbl[min((unsigned)rel1, (unsigned)(kBandTable - 1))];

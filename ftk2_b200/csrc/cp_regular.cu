@@ -182,7 +182,7 @@ struct Geo {
   static constexpr int TX_BYTES = COMP_RAW * M;                          // bytes TMA delivers
   static constexpr int COMP_ELEMS = COMP / (int)sizeof(T);
   static constexpr int WORDS = 2 * BYTES;                                // offset of the word slots
-  static constexpr int SMEM = WORDS + 3 * VSP * 4;
+  static constexpr int SMEM = WORDS + 2 * VSP * 4;
 };
 
 __device__ __forceinline__ unsigned long long pack_corner(long long x, long long y, long long z,
@@ -416,9 +416,9 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       return true;
     }
   };
-  auto words = [&](int buf, int slot, int s) {
+  // cull words of slice s into w[] (the thread's slots; absent outside the mesh)
+  auto words = [&](int buf, int s, unsigned (&w)[VPT]) {
     const unsigned* r = reinterpret_cast<const unsigned*>(smem + buf * G::BYTES) + (HW - 1);
-    unsigned* dst = Wb + slot * VSP;
     if (bulk) {
       const unsigned char* rb = smem + buf * G::BYTES + 4 * (HW - 1);
       const unsigned ts = (unsigned)(((long long)tcoord(s) * tstride * (long long)sizeof(T)) & 15);
@@ -432,8 +432,8 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
           const int o = voff[u] + (MULTI ? j * (int)sizeof(T) : j * VY * VZ * G::ROWB) + (int)sh;
           h[j] = *reinterpret_cast<const unsigned*>(rb + o);
         }
-        const unsigned w = vertex_word_hi<T, M>(h, band_tbl);
-        dst[tid + u * kThreads] = ((vvalid >> u) & 1u) ? w : kAbsent;
+        const unsigned x = vertex_word_hi<T, M>(h, band_tbl);
+        w[u] = ((vvalid >> u) & 1u) ? x : kAbsent;
       }
       return;
     }
@@ -442,23 +442,26 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       unsigned h[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) h[j] = r[HW * (MULTI ? voff[u] + j : voff[u] + j * G::COMP_ELEMS)];
-      const unsigned w = vertex_word_hi<T, M>(h, band_tbl);
-      dst[tid + u * kThreads] = ((vvalid >> u) & 1u) ? w : kAbsent;
+      const unsigned x = vertex_word_hi<T, M>(h, band_tbl);
+      w[u] = ((vvalid >> u) & 1u) ? x : kAbsent;
     }
   };
+  // Each thread keeps its slots' words of the previous slice in registers
+  // and stores, per time step, the AND of the two slices' words: a
+  // hypercube's 2^D vertices then take 2^(D-1) shared-memory words.
+  unsigned prev[VPT];
 
   // the previous tile of a persistent block is done with every buffer
   __syncthreads();
   issue(t0, 0);
   if (t0 + 1 <= s_end) issue(t0 + 1, 1);
-  int slot_a = 0;  // word slot of slice ct
   {
     bool ok = wait(t0, 0);
     // failure-path check (host option): after the first slice has landed,
     // wait on bar[2], which nothing ever completes, with the caller's short
     // poll bound; the block then leaves through the bounded-wait error path
     if (ok && mbar && cfg.stall_polls > 0) ok = mbar_wait(&bar[2], 0u, cfg.stall_polls);
-    if (ok) words(0, slot_a, t0);
+    if (ok) words(0, t0, prev);
     if (__syncthreads_or(!ok)) {
       // give the other copy in flight a bounded chance to land before leaving
       if (mbar && t0 + 1 <= s_end) mbar_wait(&bar[1], ph[1] & 1u);
@@ -481,18 +484,27 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
 
   for (int ct = t0; ct < t1; ++ct) {
     const int s = ct + 1;
-    const int slot_b = slot_a == 2 ? 0 : slot_a + 1;  // word slot of slice s
-    unsigned* B = Wb + slot_b * VSP;
+    // time-pair words of step ct (slices ct and s; slots alternate by step)
+    unsigned* const A = Wb + ((ct - t0) & 1) * VSP;
     bool ok = true;
     if (s <= s_end) {
       const int buf = (s - t0) & 1;
       ok = wait(s, buf);
-      if (ok) words(buf, slot_b, s);
-    } else {
-      for (int i = tid; i < VS; i += kThreads) B[i] = kAbsent;
+      if (ok) {
+        unsigned cur[VPT];
+        words(buf, s, cur);
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) {
+          A[tid + u * kThreads] = prev[u] & cur[u];
+          prev[u] = cur[u];
+        }
+      }
+    } else {  // no slice after the last one: the step's words are slice ct's
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) A[tid + u * kThreads] = prev[u];
     }
-    // the one block barrier of the step: words of slice s are visible, its
-    // raw buffer is free, and every warp has finished culling step ct - 1
+    // the one block barrier of the step: words of step ct are visible, slice
+    // s's raw buffer is free, and every warp has finished culling step ct - 1
     if (__syncthreads_or(!ok)) {
       const int ob = ((s - t0) & 1) ^ 1;
       if (mbar && s + 1 <= s_end) mbar_wait(&bar[ob], (ph[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
@@ -502,19 +514,18 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     if (s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
 
     // ---- hypercube cull: lanes along x, kRows corner rows per warp
-    const unsigned* A = Wb + slot_a * VSP;
     unsigned R[kRows + 1];
 #pragma unroll
     for (int q = 0; q <= kRows; ++q) {
       unsigned r, e;
       if constexpr (D == 4) {
         const int i0 = ((czw + q) * VY + cyw) * VX + lane, i1 = i0 + VX;
-        r = A[i0] & A[i1] & B[i0] & B[i1];
-        e = (lane == 31) ? (A[i0 + 1] & A[i1 + 1] & B[i0 + 1] & B[i1 + 1]) : kAbsent;
+        r = A[i0] & A[i1];
+        e = (lane == 31) ? (A[i0 + 1] & A[i1 + 1]) : kAbsent;
       } else {
         const int i0 = (cyw + q) * VX + lane;
-        r = A[i0] & B[i0];
-        e = (lane == 31) ? (A[i0 + 1] & B[i0 + 1]) : kAbsent;
+        r = A[i0];
+        e = (lane == 31) ? A[i0 + 1] : kAbsent;
       }
       const unsigned nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
       R[q] = r & (lane == 31 ? e : nb);
@@ -551,7 +562,6 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
         }
       }
     }
-    slot_a = slot_b;
   }
   if (mbar) {
     // slices t0 .. s_end alternate buffers 0, 1, 0, ...
