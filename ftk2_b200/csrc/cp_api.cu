@@ -702,7 +702,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     if (st) return st;
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
-    CUDA_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * (1u << d) * m * (field->dtype == FTK2B_F64 ? 8 : 4)));
+    CUDA_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * 48 * (field->dtype == FTK2B_F64 ? 8 : 4)));
     CUDA_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)pcap));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;

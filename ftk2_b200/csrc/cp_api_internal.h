@@ -94,7 +94,7 @@ struct BatchFieldInfo {
 };
 struct BatchGraphKey {
   int nf;
-  unsigned n_items, cap, ccap, edge_cap;
+  unsigned n_items, cap, ccap, edge_cap, pcap;
   int key_bits, f64, multi;
   const void* h_fbase;
 };
@@ -104,7 +104,7 @@ struct BatchCtx {
   size_t h_tab_bytes = 0;
   unsigned* h_fbase = nullptr;    // pinned: first feature of every field
   size_t h_fbase_n = 0;
-  unsigned cap_hint = 0, ccap_hint = 0;
+  unsigned cap_hint = 0, ccap_hint = 0, pcap_hint = 0;
   int tchunk = 0;                 // FTK2B_OPT_BATCH_TIME_CHUNK (0: tuned per batch shape)
   int last_tchunk = 0;            // the time chunk the last batch ran (0xFFFF: whole range)
   std::vector<std::pair<uint64_t, int>> tunes;  // batch shape hash -> time chunk

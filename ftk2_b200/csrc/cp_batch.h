@@ -39,6 +39,10 @@ cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, cons
 // Exact tests of every queued candidate of the batch (cq.field names its field).
 cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
                                 int num_sms, cudaStream_t st);
+// The same in two launches: a gather of every candidate's vertex values and
+// surviving chains, then one thread per listed simplex.
+cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const CandidateQueue& cq,
+                                       const RefineStage& rs, const FeatureSink& sink, int num_sms, cudaStream_t st);
 // Time chunk of a field of a batch: corner time steps per cull item.
 int batch_time_chunk(long long lt, int pick);
 

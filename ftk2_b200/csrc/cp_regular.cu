@@ -1459,80 +1459,184 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 // integer SoS and the solve then keep every lane busy instead of the few
 // chains of a hypercube that survive its word test.
 
+// One candidate by one warp: its vertex values into `out` (stride NVMAX * M
+// values per candidate) and the warp's shared cube, its vertex words, and its
+// surviving chains listed as (candidate << 6 | chain).
+template <typename T, int D>
+__device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const FieldAccess& fa,
+                                                 const ExtractConfig& cfg, unsigned c, unsigned long long pc,
+                                                 unsigned long long chains, T* out, T* my, const unsigned* band_tbl,
+                                                 const RefineStage& rs, int lane) {
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;
+  const ChainTable& CT = c_chains[D - 3];
+  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+  long long g0[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+    g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+  }
+  for (int e = lane; e < NV * M; e += 32) {
+    const int v = e / M, j = e % M;
+    long long g[4];
+    unsigned long long vid = 0;
+    bool in = true;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
+      if (k < D) {
+        in &= g[k] - mesh.off[k] < mesh.ld[k];
+        vid += (unsigned long long)g[k] * mesh.gstride[k];
+      }
+    }
+    T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
+    if (cfg.fiber) val = fp<T>::sub(val, (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
+    my[e] = val;
+    out[e] = val;
+  }
+  __syncwarp();
+  unsigned vw = kAbsent;
+  if (lane < NV) {
+    unsigned h[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) h[j] = hi_word<T>(my[lane * M + j]);
+    bool in = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
+    vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
+  }
+  for (int base = 0; base < CT.n; base += 32) {
+    const int ch = base + lane;
+    bool live = ch < CT.n && ((chains >> ch) & 1ull);
+    unsigned wacc = kAbsent;
+#pragma unroll
+    for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, live ? (i ? CT.mask[ch][i - 1] : 0) : 0);
+    live = live && (cfg.fiber || !word_culled(wacc));
+    const unsigned ball = __ballot_sync(0xFFFFFFFFu, live);
+    if (!ball) continue;
+    unsigned b0 = 0;
+    if (lane == 0) b0 = atomicAdd(rs.count, (unsigned)__popc(ball));
+    b0 = __shfl_sync(0xFFFFFFFFu, b0, 0);
+    if (live) {
+      const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
+      if (idx < rs.cap) rs.pairs[idx] = ((unsigned long long)c << 6) | (unsigned long long)ch;
+    }
+  }
+  __syncwarp();
+}
+
+constexpr int kStageVals = 48;  // 2^D * M values per candidate, D <= 4
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(RegularMesh mesh, FieldAccess fa,
                                                                           ExtractConfig cfg, CandidateQueue cq,
                                                                           RefineStage rs) {
-  constexpr int M = D - 1;
-  constexpr int NV = 1 << D;
-  __shared__ T cube[kRefineWarps][NV * M];
+  __shared__ T cube[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   __syncthreads();
-  const ChainTable& CT = c_chains[D - 3];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const unsigned n = min(*cq.count, cq.cap);
   const unsigned gw = blockIdx.x * kRefineWarps + wib;
   const unsigned nw = gridDim.x * kRefineWarps;
-  T* const my = cube[wib];
-  for (unsigned c = gw; c < n; c += nw) {
-    const unsigned long long pc = cq.corner[c], chains = cq.chains[c];
-    const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
-                            (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
-    long long g0[4];
+  for (unsigned c = gw; c < n; c += nw)
+    gather_candidate<T, D>(mesh, fa, cfg, c, cq.corner[c], cq.chains[c],
+                           static_cast<T*>(rs.vals) + (size_t)c * kStageVals, cube[wib], band_tbl, rs, lane);
+}
+
+// One listed simplex (candidate c, chain ch) by one thread: the exact test
+// and, when accepted, its canonical key and reported values.
+template <typename T, int D>
+__device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                                          unsigned long long pc, int ch, const T* src, unsigned long long key_base,
+                                          unsigned long long& key, double lam_out[4], float bary_out[4],
+                                          float& sc_out) {
+  constexpr int M = D - 1;
+  const ChainTable& CT = c_chains[D - 3];
+  int mk[M + 1];
+  mk[0] = 0;
+#pragma unroll
+  for (int k = 0; k < M; ++k) mk[k + 1] = CT.mask[ch][k];
+  T vals[M + 1][M];
+#pragma unroll
+  for (int k = 0; k <= M; ++k)
+#pragma unroll
+    for (int j = 0; j < M; ++j) vals[k][j] = src[mk[k] * M + j];
+  bool inside;
+  if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
+  else inside = sos_inside3<T>(vals, cfg.Q);
+  if (!inside) return false;
+  T lam[M + 1];
+  bool solved = solve_exact<M, T>(vals, lam);
+  if (!solved && cfg.fiber) {
+    // FiberPredicate keeps the simplex at the centroid: (T)1.0 / 3.0
+#pragma unroll
+    for (int k = 0; k <= M; ++k) lam[k] = (T)((double)(T)1.0 / 3.0);
+    solved = true;
+  }
+  if (!solved) return false;
+  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+  long long g0[4];
+  unsigned long long vid0 = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+    g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+    if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
+  }
+  key = key_base + vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
+#pragma unroll
+  for (int k = 0; k <= M; ++k) {
+    lam_out[k] = (double)lam[k];
+    bary_out[k] = (float)lam[k];
+  }
+  if (fa.has_scalar) {
+    using F = fp<T>;
+    T sc = T(0);
+#pragma unroll
+    for (int k = 0; k <= M; ++k) {
+      long long gv[4];
+      unsigned long long vid = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        gv[q] = (q < D) ? g0[q] + ((mk[k] >> q) & 1) : 0;
+        if (q < D) vid += (unsigned long long)gv[q] * mesh.gstride[q];
+      }
+      sc = F::add(sc, F::mul(lam[k], scalar_at<T>(fa, gv, D, vid)));
+    }
+    sc_out = (float)sc;
+  }
+  if (cfg.refined) {
+    double rr[M + 1];
+    if (solve_refined<M, T>(vals, rr))
+#pragma unroll
+      for (int k = 0; k <= M; ++k) lam_out[k] = rr[k];
+  }
+  return true;
+}
+
+// warp-ballot compaction of the accepted simplices of one pass into the sink
+__device__ __forceinline__ void sink_write(const FeatureSink& sink, bool acc, unsigned long long key,
+                                           const double lam_out[4], const float bary_out[4], float sc_out, int lane) {
+  const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
+  if (!ball) return;
+  unsigned b0 = 0;
+  const int leader = __ffs(ball) - 1;
+  if (lane == leader) b0 = atomicAdd(sink.count, (unsigned)__popc(ball));
+  b0 = __shfl_sync(0xFFFFFFFFu, b0, leader);
+  if (!acc) return;
+  const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
+  if (idx < sink.cap) {
+    sink.key[idx] = key;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
-      g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+      sink.lam[4 * (size_t)idx + k] = lam_out[k];
+      sink.bary4[4 * (size_t)idx + k] = bary_out[k];
     }
-    T* out = static_cast<T*>(rs.vals) + (size_t)c * (NV * M);
-    for (int e = lane; e < NV * M; e += 32) {
-      const int v = e / M, j = e % M;
-      long long g[4];
-      unsigned long long vid = 0;
-      bool in = true;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
-        if (k < D) {
-          in &= g[k] - mesh.off[k] < mesh.ld[k];
-          vid += (unsigned long long)g[k] * mesh.gstride[k];
-        }
-      }
-      T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
-      if (cfg.fiber) val = fp<T>::sub(val, (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
-      my[e] = val;
-      out[e] = val;
-    }
-    __syncwarp();
-    unsigned vw = kAbsent;
-    if (lane < NV) {
-      unsigned h[M];
-#pragma unroll
-      for (int j = 0; j < M; ++j) h[j] = hi_word<T>(my[lane * M + j]);
-      bool in = true;
-#pragma unroll
-      for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
-      vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
-    }
-    for (int base = 0; base < CT.n; base += 32) {
-      const int ch = base + lane;
-      bool live = ch < CT.n && ((chains >> ch) & 1ull);
-      unsigned wacc = kAbsent;
-#pragma unroll
-      for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, live ? (i ? CT.mask[ch][i - 1] : 0) : 0);
-      live = live && (cfg.fiber || !word_culled(wacc));
-      const unsigned ball = __ballot_sync(0xFFFFFFFFu, live);
-      if (!ball) continue;
-      unsigned b0 = 0;
-      if (lane == 0) b0 = atomicAdd(rs.count, (unsigned)__popc(ball));
-      b0 = __shfl_sync(0xFFFFFFFFu, b0, 0);
-      if (live) {
-        const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
-        if (idx < rs.cap) rs.pairs[idx] = ((unsigned long long)c << 6) | (unsigned long long)ch;
-      }
-    }
-    __syncwarp();
+    sink.scalar[idx] = sc_out;
   }
 }
 
@@ -1540,9 +1644,6 @@ template <typename T, int D>
 __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
                                                                             ExtractConfig cfg, CandidateQueue cq,
                                                                             RefineStage rs, FeatureSink sink) {
-  constexpr int M = D - 1;
-  constexpr int NV = 1 << D;
-  const ChainTable& CT = c_chains[D - 3];
   const int lane = threadIdx.x & 31;
   const unsigned np = min(*rs.count, rs.cap);
   const unsigned stride = gridDim.x * blockDim.x;
@@ -1556,90 +1657,63 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(Regu
     if (i < np) {
       const unsigned long long p = rs.pairs[i];
       const unsigned c = (unsigned)(p >> 6);
-      const int ch = (int)(p & 63);
-      int mk[M + 1];
-      mk[0] = 0;
-#pragma unroll
-      for (int k = 0; k < M; ++k) mk[k + 1] = CT.mask[ch][k];
-      const T* src = static_cast<const T*>(rs.vals) + (size_t)c * (NV * M);
-      T vals[M + 1][M];
-#pragma unroll
-      for (int k = 0; k <= M; ++k)
-#pragma unroll
-        for (int j = 0; j < M; ++j) vals[k][j] = src[mk[k] * M + j];
-      bool inside;
-      if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
-      else inside = sos_inside3<T>(vals, cfg.Q);
-      if (inside) {
-        T lam[M + 1];
-        bool solved = solve_exact<M, T>(vals, lam);
-        if (!solved && cfg.fiber) {
-          // FiberPredicate keeps the simplex at the centroid: (T)1.0 / 3.0
-#pragma unroll
-          for (int k = 0; k <= M; ++k) lam[k] = (T)((double)(T)1.0 / 3.0);
-          solved = true;
-        }
-        if (solved) {
-          acc = true;
-          const unsigned long long pc = cq.corner[c];
-          const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
-                                  (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
-          long long g0[4];
-          unsigned long long vid0 = 0;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
-            g0[k] = (k < D) ? lk + mesh.off[k] : 0;
-            if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
-          }
-          key = vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
-#pragma unroll
-          for (int k = 0; k <= M; ++k) {
-            lam_out[k] = (double)lam[k];
-            bary_out[k] = (float)lam[k];
-          }
-          if (fa.has_scalar) {
-            using F = fp<T>;
-            T sc = T(0);
-#pragma unroll
-            for (int k = 0; k <= M; ++k) {
-              long long gv[4];
-              unsigned long long vid = 0;
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                gv[q] = (q < D) ? g0[q] + ((mk[k] >> q) & 1) : 0;
-                if (q < D) vid += (unsigned long long)gv[q] * mesh.gstride[q];
-              }
-              sc = F::add(sc, F::mul(lam[k], scalar_at<T>(fa, gv, D, vid)));
-            }
-            sc_out = (float)sc;
-          }
-          if (cfg.refined) {
-            double rr[M + 1];
-            if (solve_refined<M, T>(vals, rr))
-#pragma unroll
-              for (int k = 0; k <= M; ++k) lam_out[k] = rr[k];
-          }
-        }
-      }
+      acc = test_pair<T, D>(mesh, fa, cfg, cq.corner[c], (int)(p & 63),
+                            static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, 0ull, key, lam_out, bary_out,
+                            sc_out);
     }
-    const unsigned ball = __ballot_sync(0xFFFFFFFFu, acc);
-    if (!ball) continue;
-    unsigned b0 = 0;
-    const int leader = __ffs(ball) - 1;
-    if (lane == leader) b0 = atomicAdd(sink.count, (unsigned)__popc(ball));
-    b0 = __shfl_sync(0xFFFFFFFFu, b0, leader);
-    if (!acc) continue;
-    const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
-    if (idx < sink.cap) {
-      sink.key[idx] = key;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        sink.lam[4 * (size_t)idx + k] = lam_out[k];
-        sink.bary4[4 * (size_t)idx + k] = bary_out[k];
-      }
-      sink.scalar[idx] = sc_out;
+    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
+  }
+}
+
+// the same two launches over a batch: each candidate reads its field's record
+template <typename T>
+__global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const BatchField* __restrict__ fields,
+                                                                         CandidateQueue cq, RefineStage rs) {
+  __shared__ T cube[kRefineWarps][kStageVals];
+  __shared__ unsigned band_tbl[kBandTable];
+  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned n = min(*cq.count, cq.cap);
+  const unsigned gw = blockIdx.x * kRefineWarps + wib;
+  const unsigned nw = gridDim.x * kRefineWarps;
+  for (unsigned c = gw; c < n; c += nw) {
+    const BatchField& F = fields[cq.field[c]];
+    T* out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals;
+    if (F.mesh.d == 4)
+      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, cube[wib], band_tbl, rs, lane);
+    else
+      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, cube[wib], band_tbl, rs, lane);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRefineWarps * 32, 2) batch_pairs_kernel(const BatchField* __restrict__ fields,
+                                                                           CandidateQueue cq, RefineStage rs,
+                                                                           FeatureSink sink) {
+  const int lane = threadIdx.x & 31;
+  const unsigned np = min(*rs.count, rs.cap);
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x; base < np; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool acc = false;
+    double lam_out[4] = {0, 0, 0, 0};
+    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+    float sc_out = 0.f;
+    unsigned long long key = 0;
+    if (i < np) {
+      const unsigned long long p = rs.pairs[i];
+      const unsigned c = (unsigned)(p >> 6);
+      const BatchField& F = fields[cq.field[c]];
+      const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
+      if (F.mesh.d == 4)
+        acc = test_pair<T, 4>(F.mesh, F.fa, F.cfg, cq.corner[c], (int)(p & 63), src, F.key_base, key, lam_out,
+                              bary_out, sc_out);
+      else
+        acc = test_pair<T, 3>(F.mesh, F.fa, F.cfg, cq.corner[c], (int)(p & 63), src, F.key_base, key, lam_out,
+                              bary_out, sc_out);
     }
+    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
   }
 }
 
@@ -2143,6 +2217,19 @@ cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, cons
                         : launch_batch_cull_t<double, false>(fields, item_base, nf, n_items, item_next, cq, err, st);
   return multi ? launch_batch_cull_t<float, true>(fields, item_base, nf, n_items, item_next, cq, err, st)
                : launch_batch_cull_t<float, false>(fields, item_base, nf, n_items, item_next, cq, err, st);
+}
+
+cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const CandidateQueue& cq,
+                                       const RefineStage& rs, const FeatureSink& sink, int num_sms, cudaStream_t st) {
+  const int thr = kRefineWarps * 32;
+  if (f64) {
+    batch_gather_kernel<double><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
+    batch_pairs_kernel<double><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+  } else {
+    batch_gather_kernel<float><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
+    batch_pairs_kernel<float><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
