@@ -546,7 +546,7 @@ def north_star_summary(line):
         "serve_req_s": sv.get("throughput_req_s"),
         "serve_capacity_req_s": line.get("serve_sweep", {}).get("capacity_req_s"),
     }
-    return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in out.items()}
+    return {k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in out.items()}
 
 
 def run_sharded(args, rank, world, local):
