@@ -41,6 +41,7 @@ INFO_LAST_TMA = 100
 INFO_LAST_CULL_MODE = 101
 INFO_LAST_BATCH_TIME_CHUNK = 102
 INFO_LAST_CANDIDATES = 103
+INFO_LAST_TESTED = 104
 OPT_BLOCKING_SYNC = 5
 OPT_CULL_MODE = 6
 OPT_BATCH_TIME_CHUNK = 7

@@ -238,6 +238,7 @@ extern "C" ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t
     case FTK2B_INFO_LAST_TMA: *value = ctx->last_used_tma; return FTK2B_OK;
     case FTK2B_INFO_LAST_CULL_MODE: *value = ctx->last_cull_mode; return FTK2B_OK;
     case FTK2B_INFO_LAST_CANDIDATES: *value = (int64_t)ctx->last_candidates; return FTK2B_OK;
+    case FTK2B_INFO_LAST_TESTED: *value = (int64_t)ctx->last_tested; return FTK2B_OK;
     case FTK2B_INFO_LAST_BATCH_TIME_CHUNK: *value = ctx->batch.last_tchunk; return FTK2B_OK;
     case FTK2B_OPT_USE_GRAPHS: *value = ctx->use_graphs ? 1 : 0; return FTK2B_OK;
     case FTK2B_OPT_BLOCKING_SYNC: *value = ctx->blocking_sync ? 1 : 0; return FTK2B_OK;
@@ -691,11 +692,6 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     if (nloc > 0xFFFFFFF0ull) return fail(ctx, FTK2B_UNSUPPORTED, "mesh too large for fiber extraction");
     ccap = std::max<unsigned>(ccap, (unsigned)nloc);
   }
-  // simplices listed for the exact test: a few per surviving hypercube (every
-  // chain in fiber mode); grows on overflow
-  const unsigned long long pc0 = fiber_thr ? (unsigned long long)ccap * nch : (unsigned long long)ccap * 8;
-  unsigned pcap = ctx->pair_cap_hint ? ctx->pair_cap_hint : (unsigned)std::min<unsigned long long>(pc0, 0xFFFFFFF0ull);
-  if (fiber_thr) pcap = (unsigned)std::max<unsigned long long>(pcap, std::min<unsigned long long>(pc0, 0xFFFFFFF0ull));
   for (int attempt = 0; attempt < 4; ++attempt) {
     const unsigned edge_cap = cap * 2;
     st = ensure_feature_buffers(ctx, cap, edge_cap, m);
@@ -703,7 +699,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * 48 * (field->dtype == FTK2B_F64 ? 8 : 4)));
-    CUDA_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)pcap));
+    CUDA_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)ccap));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -719,9 +715,8 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cq.cap = ccap;
     RefineStage rs;
     rs.vals = ctx->refine_vals.p;
-    rs.pairs = (unsigned long long*)ctx->refine_pairs.p;
+    rs.live = (unsigned long long*)ctx->refine_pairs.p;
     rs.count = (unsigned*)ctx->counters.p + kCountPairs;
-    rs.cap = pcap;
     const int f64 = field->dtype == FTK2B_F64;
     // the device pipeline in two parts so that the fused cull kernel can be
     // timed on its own: [counters reset, cull] and [exact tests, canonical
@@ -781,7 +776,6 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       key.cfg = cfg;
       key.cap = cap;
       key.ccap = ccap;
-      key.pcap = pcap;
       key.edge_cap = edge_cap;
       key.f64 = f64;
       key.want_edges = prm->want_edges;
@@ -868,6 +862,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cudaGetLastError();  // a failed timing query must not linger in the error slot
     ctx->last_extract_ms = xms;
     ctx->last_candidates = h[kCountCand];
+    ctx->last_tested = h[kCountPairs];
     if (h[kCountErr] & 2u) return fail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return fail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
     if (h[kCountCand] > ccap) {
@@ -875,13 +870,6 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       if (want > 0xFFFFFFF0ull) return fail(ctx, FTK2B_OVERFLOW_RETRY, "candidate count exceeds 2^32");
       ccap = (unsigned)want;
       ctx->cand_cap_hint = ccap;
-      continue;
-    }
-    if (h[kCountPairs] > pcap) {
-      const uint64_t want = (uint64_t)h[kCountPairs] + h[kCountPairs] / 4 + 1024;
-      if (want > 0xFFFFFFF0ull) return fail(ctx, FTK2B_OVERFLOW_RETRY, "listed simplex count exceeds 2^32");
-      pcap = (unsigned)want;
-      ctx->pair_cap_hint = pcap;
       continue;
     }
     if (h[kCountFeatures] > cap || h[kCountEdges] > edge_cap) {

@@ -31,7 +31,7 @@ enum {
   kCountErr = 3,
   kCountCand = 4,
   kCountItems = 5,  // batches: next cull item
-  kCountPairs = 6,  // simplices listed for the exact test
+  kCountPairs = 6,  // simplices the exact test ran on
   kNumCounters = 8
 };
 
@@ -41,7 +41,7 @@ struct RegularGraphKey {
   RegularMesh rm;
   FieldAccess fa;
   ExtractConfig cfg;
-  unsigned cap, ccap, edge_cap, pcap;
+  unsigned cap, ccap, edge_cap;
   int f64, want_edges, classify, allow_tma, key_bits, nch;
 };
 
@@ -94,7 +94,7 @@ struct BatchFieldInfo {
 };
 struct BatchGraphKey {
   int nf;
-  unsigned n_items, cap, ccap, edge_cap, pcap;
+  unsigned n_items, cap, ccap, edge_cap;
   int key_bits, f64, multi;
   const void* h_fbase;
 };
@@ -104,7 +104,7 @@ struct BatchCtx {
   size_t h_tab_bytes = 0;
   unsigned* h_fbase = nullptr;    // pinned: first feature of every field
   size_t h_fbase_n = 0;
-  unsigned cap_hint = 0, ccap_hint = 0, pcap_hint = 0;
+  unsigned cap_hint = 0, ccap_hint = 0;
   int tchunk = 0;                 // FTK2B_OPT_BATCH_TIME_CHUNK (0: tuned per batch shape)
   int last_tchunk = 0;            // the time chunk the last batch ran (0xFFFF: whole range)
   std::vector<std::pair<uint64_t, int>> tunes;  // batch shape hash -> time chunk
@@ -145,11 +145,11 @@ struct ftk2b_ctx {
   std::string err;
   unsigned cap_hint = 0;
   unsigned cand_cap_hint = 0;
-  unsigned pair_cap_hint = 0;
   int tune_tchunk = 0;
   int cull_mode = 2;  // FTK2B_OPT_CULL_MODE (2: chosen per workload shape)
   int last_cull_mode = 0;  // the mode the last regular-mesh extraction ran
   unsigned long long last_candidates = 0;  // hypercubes the last regular-mesh cull kept
+  unsigned long long last_tested = 0;      // simplices the last exact test ran on
   int stall_polls = 0;                     // FTK2B_OPT_TEST_STALL_POLLS
   std::vector<ftk2b::CullTune> cull_tunes;
   bool disable_tma = false;

@@ -208,7 +208,6 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
                              ctx->stream));
   unsigned cap = bc.cap_hint ? bc.cap_hint : 65536u;
   unsigned ccap = bc.ccap_hint ? bc.ccap_hint : 65536u;
-  unsigned pcap = bc.pcap_hint ? bc.pcap_hint : 8u * 65536u;  // listed simplices of the exact test
   const BatchField* dfields = static_cast<const BatchField*>(bc.fields.p);
   const unsigned* ditems = static_cast<const unsigned*>(bc.item_base.p);
 
@@ -281,7 +280,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     B_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     B_TRY(ctx, bc.cand_field.ensure(sizeof(unsigned) * (size_t)ccap));
     B_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * 48 * (f64 ? 8 : 4)));
-    B_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)pcap));
+    B_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)ccap));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -300,9 +299,8 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     unsigned* const dfbase = static_cast<unsigned*>(bc.fbase.p);
     RefineStage rs;
     rs.vals = ctx->refine_vals.p;
-    rs.pairs = static_cast<unsigned long long*>(ctx->refine_pairs.p);
+    rs.live = static_cast<unsigned long long*>(ctx->refine_pairs.p);
     rs.count = counters + kCountPairs;
-    rs.cap = pcap;
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, ctx->stream);
       if (!e)
@@ -329,7 +327,6 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
       key.n_items = (unsigned)items;
       key.cap = cap;
       key.ccap = ccap;
-      key.pcap = pcap;
       key.edge_cap = edge_cap;
       key.key_bits = key_bits;
       key.f64 = f64;
@@ -392,13 +389,6 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
       if (want > 0xFFFFFFF0ull) return bfail(ctx, FTK2B_OVERFLOW_RETRY, "candidate count exceeds 2^32");
       ccap = (unsigned)want;
       bc.ccap_hint = ccap;
-      continue;
-    }
-    if (h[kCountPairs] > pcap) {
-      const uint64_t want = (uint64_t)h[kCountPairs] + h[kCountPairs] / 4 + 1024;
-      if (want > 0xFFFFFFF0ull) return bfail(ctx, FTK2B_OVERFLOW_RETRY, "listed simplex count exceeds 2^32");
-      pcap = (unsigned)want;
-      bc.pcap_hint = pcap;
       continue;
     }
     if (h[kCountFeatures] > cap || h[kCountEdges] > edge_cap) {

@@ -32,8 +32,9 @@ namespace ftk2b {
 // Each predicate is evaluated on high words so that it can only err towards
 // "not strong" / "not tiny": a strictly larger high word of a non-negative
 // IEEE value implies a strictly larger value, and kappa' * b only shifts the
-// exponent field.  Infinite or NaN components give 0 (never culled).  Vertices
-// outside the mesh get ~0 (neutral under AND).
+// exponent field.  Infinite or NaN components give a word without band and
+// tiny bits (never culled).  Vertices outside the mesh get ~0 (neutral under
+// AND).
 template <typename T> struct CullParams;
 template <> struct CullParams<double> {
   static constexpr int mant = 20;          // mantissa bits in the high word
@@ -103,9 +104,11 @@ __device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M], const un
   unsigned w = (strong & ~neg) | ((strong & neg) << 3);
   w |= (b < P::tiny_hi ? 1u : 0u) << 6;
   const int rel1 = (int)(b >> P::mant) - P::bias - kElo + 1;
+  // inf or nan somewhere: the exponent lies past the banded window, so the
+  // word gets no band bit (and no tiny bit) and no set of vertices holding
+  // it is ever culled
   w |= band_tbl[min((unsigned)rel1, (unsigned)(kBandTable - 1))];
-  // inf or nan somewhere: never culled
-  return b >= P::expmask ? 0u : w;
+  return w;
 }
 
 __device__ __forceinline__ bool word_culled(unsigned w) {

@@ -117,13 +117,12 @@ void tile_scratch_size(const RegularMesh& mesh, size_t* stats_bytes, unsigned* r
 cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueue& cq, int num_sms,
                                     cudaStream_t st);
 // The exact test in two launches (gather of each candidate's vertex values
-// and its surviving chains, then one thread per listed simplex): staging of
-// 2^D * M values per candidate and the (candidate << 6 | chain) list.
+// and the mask of its surviving chains, then one thread per surviving
+// simplex): staging of 2^D * M values and one chain mask per candidate.
 struct RefineStage {
   void* vals;
-  unsigned long long* pairs;
-  unsigned* count;   // simplices listed (may exceed cap: overflow)
-  unsigned cap;
+  unsigned long long* live;
+  unsigned* count;   // simplices tested (reported after the run)
 };
 cudaError_t launch_refine_staged(int f64, const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                                  const CandidateQueue& cq, const RefineStage& rs, const FeatureSink& sink, int num_sms,

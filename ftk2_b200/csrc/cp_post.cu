@@ -657,43 +657,64 @@ __device__ __forceinline__ void uf_unite_shared(unsigned* parent, unsigned a, un
 
 __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
   pdl_enter();
-  extern __shared__ unsigned sp[];  // union-find parents of the n features
+  extern __shared__ unsigned sh[];  // edge offsets of the n features (n + 1), then their union-find parents
   __shared__ unsigned part[1024];
   __shared__ unsigned s_roots;
+  constexpr int kPer = (int)(kSmallPostCap / 1024);  // features per thread, at most
   const unsigned n = min(*B.count, B.cap);
+  unsigned* const off = sh;
+  unsigned* const sp = sh + n + 1;
   const unsigned t = threadIdx.x;
-  // exclusive scan of the per-feature edge counts, in place
+  // exclusive scan of the per-feature edge counts: each thread's contiguous
+  // segment, its counts loaded first (independent loads)
   const unsigned seg = (n + 1023) / 1024;
-  const unsigned s0 = min(t * seg, n), s1 = min(s0 + seg, n);
+  const unsigned s0 = min(t * seg, n);
+  unsigned c[kPer];
   unsigned sum = 0;
-  for (unsigned i = s0; i < s1; ++i) sum += B.edge_cnt[i];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    c[k] = (k < (int)seg && s0 + k < n) ? B.edge_cnt[s0 + k] : 0u;
+    sum += c[k];
+  }
   part[t] = sum;
   for (unsigned i = t; i < n; i += 1024) sp[i] = i;
   if (t == 0) s_roots = 0;
   __syncthreads();
-  for (unsigned off = 1; off < 1024; off <<= 1) {
-    const unsigned v = t >= off ? part[t - off] : 0;
+  for (unsigned o = 1; o < 1024; o <<= 1) {
+    const unsigned v = t >= o ? part[t - o] : 0;
     __syncthreads();
     part[t] += v;
     __syncthreads();
   }
   const unsigned total = part[1023];
   unsigned run = part[t] - sum;
-  // each thread writes its features' edges at their offsets and unites them
-  for (unsigned i = s0; i < s1; ++i) {
-    const unsigned c = B.edge_cnt[i];
-    B.edge_cnt[i] = run;
-    for (unsigned k = 0; k < c; ++k) {
-      const unsigned other = B.edge_slots[(size_t)i * kEdgeSlots + k];
-      if (run + k < B.edge_cap) {
-        B.edges[2 * (size_t)(run + k)] = i;
-        B.edges[2 * (size_t)(run + k) + 1] = other;
-      }
-      uf_unite_shared(sp, i, other, B.err);
-    }
-    run += c;
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    if (k < (int)seg && s0 + k < n) off[s0 + k] = run;
+    run += c[k];
   }
-  if (t == 1023) *B.n_edges = total;
+  if (t == 0) {
+    off[n] = total;
+    *B.n_edges = total;
+  }
+  __syncthreads();
+  // every edge by its own thread: the feature whose offset range holds it
+  // (binary search in shared memory), its slot, the output pair, the hook
+#pragma unroll 4
+  for (unsigned e = t; e < total; e += 1024) {
+    unsigned lo = 0, hi = n;  // the last i with off[i] <= e
+    while (hi - lo > 1) {
+      const unsigned mid = (lo + hi) >> 1;
+      if (off[mid] <= e) lo = mid;
+      else hi = mid;
+    }
+    const unsigned other = B.edge_slots[(size_t)lo * kEdgeSlots + (e - off[lo])];
+    if (e < B.edge_cap) {
+      B.edges[2 * (size_t)e] = lo;
+      B.edges[2 * (size_t)e + 1] = other;
+    }
+    uf_unite_shared(sp, lo, other, B.err);
+  }
   __syncthreads();
   unsigned roots = 0;
   for (unsigned i = t; i < n; i += 1024) {
@@ -722,7 +743,7 @@ static cudaError_t launch_post_small(const RegularMesh& mesh, int nch, const Pos
   e = cudaFuncSetAttribute(small_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
   if (!e) e = launch_pdl(small_edges_kernel, B.num_sms > 0 ? B.num_sms : 148, kRankThreads, key_smem, st, mesh, nch, B);
   if (e) return e;
-  const size_t uf_smem = sizeof(unsigned) * (size_t)(cap ? cap : 1);
+  const size_t uf_smem = sizeof(unsigned) * (2 * (size_t)cap + 1);
   e = cudaFuncSetAttribute(small_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uf_smem);
   if (!e) e = launch_pdl(small_finish_kernel, 1, 1024, uf_smem, st, B);
   *launches += 2;

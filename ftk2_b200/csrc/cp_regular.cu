@@ -248,9 +248,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // per-thread vertex slots of a slice, fixed for the whole time march:
   // element offset of component 0 in a slice buffer (bulk staging: byte
   // offset from the row's slot, and the row's source offset mod 16 without
-  // the time term, 4 bits per slot) and a validity bit
+  // the time term, 4 bits per slot) and an absence mask
   int voff[VPT];
-  unsigned vvalid = 0, vshift = 0;
+  unsigned vshift = 0;
+  unsigned vinv[VPT];  // ~0 for slots outside the mesh (absent under AND), else 0
 #pragma unroll
   for (int u = 0; u < VPT; ++u) {
     const int i = tid + u * kThreads;
@@ -264,7 +265,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     } else {
       voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
     }
-    vvalid |= (in ? 1u : 0u) << u;
+    vinv[u] = in ? 0u : kAbsent;
   }
   // source address mod 16 of each array, and the time axis' element stride
   unsigned pbase = 0;
@@ -433,7 +434,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
           h[j] = *reinterpret_cast<const unsigned*>(rb + o);
         }
         const unsigned x = vertex_word_hi<T, M>(h, band_tbl);
-        w[u] = ((vvalid >> u) & 1u) ? x : kAbsent;
+        w[u] = x | vinv[u];
       }
       return;
     }
@@ -443,7 +444,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
 #pragma unroll
       for (int j = 0; j < M; ++j) h[j] = r[HW * (MULTI ? voff[u] + j : voff[u] + j * G::COMP_ELEMS)];
       const unsigned x = vertex_word_hi<T, M>(h, band_tbl);
-      w[u] = ((vvalid >> u) & 1u) ? x : kAbsent;
+      w[u] = x | vinv[u];
     }
   };
   // Each thread keeps its slots' words of the previous slice in registers
@@ -1450,18 +1451,21 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 // Exact test in two launches (the single-field path):
 //   refine_gather_kernel  one warp per candidate hypercube: its 2^D vertices'
 //                         values into a staging block (global memory, read
-//                         back from L2), their cull words, and the chains
-//                         whose words survive listed as (candidate, chain)
-//   refine_pairs_kernel   one thread per listed simplex: the exact SoS test,
-//                         the solve, and the warp-ballot compaction of the
-//                         accepted simplices
+//                         back from L2), their cull words, and the mask of
+//                         the chains whose words survive
+//   refine_pairs_kernel   each block takes 64 candidates, lays their masks'
+//                         set bits out by a prefix count in shared memory, and
+//                         gives one thread to every (candidate, chain): the
+//                         exact SoS test, the solve, and the warp-ballot
+//                         compaction of the accepted simplices
+// No global counter is taken per candidate: the only atomics are the sink's.
 // The gather is latency-bound and light, so it runs at high occupancy; the
 // integer SoS and the solve then keep every lane busy instead of the few
 // chains of a hypercube that survive its word test.
 
-// One candidate by one warp: its vertex values into `out` (stride NVMAX * M
-// values per candidate) and the warp's shared cube, its vertex words, and its
-// surviving chains listed as (candidate << 6 | chain).
+// One candidate by one warp: its vertex values into `out` (kStageVals values
+// per candidate) and the warp's shared cube, its vertex words, and the mask
+// of its surviving chains into rs.live[c].
 template <typename T, int D>
 __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const FieldAccess& fa,
                                                  const ExtractConfig& cfg, unsigned c, unsigned long long pc,
@@ -1507,6 +1511,7 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
     vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
   }
+  unsigned long long mask = 0;
   for (int base = 0; base < CT.n; base += 32) {
     const int ch = base + lane;
     bool live = ch < CT.n && ((chains >> ch) & 1ull);
@@ -1514,16 +1519,9 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
 #pragma unroll
     for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, live ? (i ? CT.mask[ch][i - 1] : 0) : 0);
     live = live && (cfg.fiber || !word_culled(wacc));
-    const unsigned ball = __ballot_sync(0xFFFFFFFFu, live);
-    if (!ball) continue;
-    unsigned b0 = 0;
-    if (lane == 0) b0 = atomicAdd(rs.count, (unsigned)__popc(ball));
-    b0 = __shfl_sync(0xFFFFFFFFu, b0, 0);
-    if (live) {
-      const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
-      if (idx < rs.cap) rs.pairs[idx] = ((unsigned long long)c << 6) | (unsigned long long)ch;
-    }
+    mask |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, live) << base;
   }
+  if (lane == 0) rs.live[c] = mask;
   __syncwarp();
 }
 
@@ -1640,28 +1638,79 @@ __device__ __forceinline__ void sink_write(const FeatureSink& sink, bool acc, un
   }
 }
 
+constexpr int kPairCands = 64;  // candidates a block of the exact-test launch takes at a time
+
+// The block's next kPairCands candidates from `first`: masks and the prefix
+// counts of their set bits in shared memory; returns the number of simplices.
+__device__ __forceinline__ unsigned pairs_layout(const RefineStage& rs, unsigned first, unsigned n,
+                                                 unsigned long long* msk, unsigned* off) {
+  const int t = threadIdx.x;
+  if (t < kPairCands) {
+    const unsigned c = first + t;
+    msk[t] = c < n ? rs.live[c] : 0ull;
+  }
+  __syncthreads();
+  if (t < 32) {
+    // two candidates per lane, a warp-wide inclusive scan of their counts
+    const unsigned a = __popcll(msk[2 * t]), b = __popcll(msk[2 * t + 1]);
+    unsigned incl = a + b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (t >= o) incl += y;
+    }
+    off[2 * t] = incl - a - b;
+    off[2 * t + 1] = incl - b;
+    if (t == 31) off[kPairCands] = incl;
+  }
+  __syncthreads();
+  return off[kPairCands];
+}
+
+// simplex p of the block's layout: its candidate slot k and chain
+__device__ __forceinline__ void pairs_locate(unsigned p, const unsigned long long* msk, const unsigned* off, int& k,
+                                             int& ch) {
+  int lo = 0, hi = kPairCands;  // the last k with off[k] <= p
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= p) lo = mid;
+    else hi = mid;
+  }
+  k = lo;
+  const unsigned r = p - off[k];
+  const unsigned long long m = msk[k];
+  const unsigned lo32 = (unsigned)m, nlo = __popc(lo32);
+  ch = r < nlo ? (int)__fns(lo32, 0, (int)r + 1) : 32 + (int)__fns((unsigned)(m >> 32), 0, (int)(r - nlo) + 1);
+}
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
                                                                             ExtractConfig cfg, CandidateQueue cq,
                                                                             RefineStage rs, FeatureSink sink) {
+  __shared__ unsigned long long msk[kPairCands];
+  __shared__ unsigned off[kPairCands + 1];
   const int lane = threadIdx.x & 31;
-  const unsigned np = min(*rs.count, rs.cap);
-  const unsigned stride = gridDim.x * blockDim.x;
-  for (unsigned base = blockIdx.x * blockDim.x; base < np; base += stride) {
-    const unsigned i = base + threadIdx.x;
-    bool acc = false;
-    double lam_out[4] = {0, 0, 0, 0};
-    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-    float sc_out = 0.f;
-    unsigned long long key = 0;
-    if (i < np) {
-      const unsigned long long p = rs.pairs[i];
-      const unsigned c = (unsigned)(p >> 6);
-      acc = test_pair<T, D>(mesh, fa, cfg, cq.corner[c], (int)(p & 63),
-                            static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, 0ull, key, lam_out, bary_out,
-                            sc_out);
+  const unsigned n = min(*cq.count, cq.cap);
+  for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
+    const unsigned P = pairs_layout(rs, first, n, msk, off);
+    if (threadIdx.x == 0) atomicAdd(rs.count, P);
+    for (unsigned base = 0; base < P; base += blockDim.x) {
+      const unsigned p = base + threadIdx.x;
+      bool acc = false;
+      double lam_out[4] = {0, 0, 0, 0};
+      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+      float sc_out = 0.f;
+      unsigned long long key = 0;
+      if (p < P) {
+        int k, ch;
+        pairs_locate(p, msk, off, k, ch);
+        const unsigned c = first + k;
+        acc = test_pair<T, D>(mesh, fa, cfg, cq.corner[c], ch, static_cast<const T*>(rs.vals) + (size_t)c * kStageVals,
+                              0ull, key, lam_out, bary_out, sc_out);
+      }
+      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
-    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
+    __syncthreads();  // the layout is rebuilt for the next candidates
   }
 }
 
@@ -1691,29 +1740,36 @@ template <typename T>
 __global__ void __launch_bounds__(kRefineWarps * 32, 2) batch_pairs_kernel(const BatchField* __restrict__ fields,
                                                                            CandidateQueue cq, RefineStage rs,
                                                                            FeatureSink sink) {
+  __shared__ unsigned long long msk[kPairCands];
+  __shared__ unsigned off[kPairCands + 1];
   const int lane = threadIdx.x & 31;
-  const unsigned np = min(*rs.count, rs.cap);
-  const unsigned stride = gridDim.x * blockDim.x;
-  for (unsigned base = blockIdx.x * blockDim.x; base < np; base += stride) {
-    const unsigned i = base + threadIdx.x;
-    bool acc = false;
-    double lam_out[4] = {0, 0, 0, 0};
-    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-    float sc_out = 0.f;
-    unsigned long long key = 0;
-    if (i < np) {
-      const unsigned long long p = rs.pairs[i];
-      const unsigned c = (unsigned)(p >> 6);
-      const BatchField& F = fields[cq.field[c]];
-      const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
-      if (F.mesh.d == 4)
-        acc = test_pair<T, 4>(F.mesh, F.fa, F.cfg, cq.corner[c], (int)(p & 63), src, F.key_base, key, lam_out,
-                              bary_out, sc_out);
-      else
-        acc = test_pair<T, 3>(F.mesh, F.fa, F.cfg, cq.corner[c], (int)(p & 63), src, F.key_base, key, lam_out,
-                              bary_out, sc_out);
+  const unsigned n = min(*cq.count, cq.cap);
+  for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
+    const unsigned P = pairs_layout(rs, first, n, msk, off);
+    if (threadIdx.x == 0) atomicAdd(rs.count, P);
+    for (unsigned base = 0; base < P; base += blockDim.x) {
+      const unsigned p = base + threadIdx.x;
+      bool acc = false;
+      double lam_out[4] = {0, 0, 0, 0};
+      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+      float sc_out = 0.f;
+      unsigned long long key = 0;
+      if (p < P) {
+        int k, ch;
+        pairs_locate(p, msk, off, k, ch);
+        const unsigned c = first + k;
+        const BatchField& F = fields[cq.field[c]];
+        const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
+        if (F.mesh.d == 4)
+          acc = test_pair<T, 4>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, F.key_base, key, lam_out, bary_out,
+                                sc_out);
+        else
+          acc = test_pair<T, 3>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, F.key_base, key, lam_out, bary_out,
+                                sc_out);
+      }
+      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
-    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
+    __syncthreads();
   }
 }
 
@@ -2151,7 +2207,7 @@ cudaError_t launch_refine_staged(int f64, const RegularMesh& mesh, const FieldAc
                                  const CandidateQueue& cq, const RefineStage& rs, const FeatureSink& sink, int num_sms,
                                  cudaStream_t st) {
   const int thr = kRefineWarps * 32;
-  const int g1 = num_sms * 16, g2 = num_sms * 8;
+  const int g1 = num_sms * 16, g2 = num_sms * 4;
   if (mesh.d == 4) {
     if (f64) {
       refine_gather_kernel<double, 4><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
@@ -2224,10 +2280,10 @@ cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const 
   const int thr = kRefineWarps * 32;
   if (f64) {
     batch_gather_kernel<double><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
-    batch_pairs_kernel<double><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<double><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
   } else {
     batch_gather_kernel<float><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
-    batch_pairs_kernel<float><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<float><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
   }
   return cudaGetLastError();
 }

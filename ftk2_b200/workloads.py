@@ -120,7 +120,8 @@ def main():
             print(f"step {i}: {n} features {ne} edges  extract {x:.3f} ms  pipeline {tot:.3f} ms  "
                   f"host {1e3 * (time.perf_counter() - t):.3f} ms  tma={ctx.get_option(api.INFO_LAST_TMA)}  "
                   f"cull_mode={ctx.get_option(api.INFO_LAST_CULL_MODE)}  "
-                  f"candidates={ctx.get_option(api.INFO_LAST_CANDIDATES)}", flush=True)
+                  f"candidates={ctx.get_option(api.INFO_LAST_CANDIDATES)}  "
+                  f"tested={ctx.get_option(api.INFO_LAST_TESTED)}", flush=True)
 
 
 if __name__ == "__main__":
