@@ -30,6 +30,7 @@
 #include "cp_device.cuh"
 #include "cp_field.cuh"
 #include "cp_internal.h"
+#include "cp_pdl.cuh"
 
 namespace ftk2b {
 
@@ -1534,6 +1535,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
   __shared__ T cube[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  pdl_enter();
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const unsigned n = min(*cq.count, cq.cap);
@@ -1689,6 +1691,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(Regu
                                                                             RefineStage rs, FeatureSink sink) {
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const unsigned n = min(*cq.count, cq.cap);
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
@@ -2208,24 +2211,27 @@ cudaError_t launch_refine_staged(int f64, const RegularMesh& mesh, const FieldAc
                                  cudaStream_t st) {
   const int thr = kRefineWarps * 32;
   const int g1 = num_sms * 16, g2 = num_sms * 4;
+  // programmatic dependent launches: each kernel waits for its predecessor
+  // at its start (pdl_enter), so its launch overlaps the predecessor's tail
+  cudaError_t e;
   if (mesh.d == 4) {
     if (f64) {
-      refine_gather_kernel<double, 4><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
-      refine_pairs_kernel<double, 4><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+      e = launch_pdl(refine_gather_kernel<double, 4>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
+      if (!e) e = launch_pdl(refine_pairs_kernel<double, 4>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
     } else {
-      refine_gather_kernel<float, 4><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
-      refine_pairs_kernel<float, 4><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+      e = launch_pdl(refine_gather_kernel<float, 4>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
+      if (!e) e = launch_pdl(refine_pairs_kernel<float, 4>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
     }
   } else {
     if (f64) {
-      refine_gather_kernel<double, 3><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
-      refine_pairs_kernel<double, 3><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+      e = launch_pdl(refine_gather_kernel<double, 3>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
+      if (!e) e = launch_pdl(refine_pairs_kernel<double, 3>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
     } else {
-      refine_gather_kernel<float, 3><<<g1, thr, 0, st>>>(mesh, fa, cfg, cq, rs);
-      refine_pairs_kernel<float, 3><<<g2, thr, 0, st>>>(mesh, fa, cfg, cq, rs, sink);
+      e = launch_pdl(refine_gather_kernel<float, 3>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
+      if (!e) e = launch_pdl(refine_pairs_kernel<float, 3>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
     }
   }
-  return cudaGetLastError();
+  return e ? e : cudaGetLastError();
 }
 
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
