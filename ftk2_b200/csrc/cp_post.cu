@@ -699,7 +699,7 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
   }
   __syncthreads();
   // every edge by its own thread: the feature whose offset range holds it
-  // (binary search in shared memory), its slot, the output pair, the hook
+  // (binary search in shared memory), its slot, the output pair
 #pragma unroll 4
   for (unsigned e = t; e < total; e += 1024) {
     unsigned lo = 0, hi = n;  // the last i with off[i] <= e
@@ -713,7 +713,17 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
       B.edges[2 * (size_t)e] = lo;
       B.edges[2 * (size_t)e + 1] = other;
     }
-    uf_unite_shared(sp, lo, other, B.err);
+  }
+  __syncthreads();
+  // hooks: each thread a contiguous run of edges (edges sorted by centre lie
+  // mostly within one track, runs of different threads mostly in different
+  // tracks, so few threads contend for the same root)
+  {
+    const unsigned ne = min(total, B.edge_cap);
+    const unsigned eseg = (ne + 1023) / 1024;
+    const unsigned e0 = min(t * eseg, ne), e1 = min(e0 + eseg, ne);
+    for (unsigned e = e0; e < e1; ++e)
+      uf_unite_shared(sp, B.edges[2 * (size_t)e], B.edges[2 * (size_t)e + 1], B.err);
   }
   __syncthreads();
   unsigned roots = 0;
