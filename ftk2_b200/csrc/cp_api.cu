@@ -698,8 +698,8 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     if (st) return st;
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
-    CUDA_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * 48 * (field->dtype == FTK2B_F64 ? 8 : 4)));
-    CUDA_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)ccap));
+    CUDA_TRY(ctx, ctx->refine_vals.ensure(refine_stage_bytes(ccap, field->dtype == FTK2B_F64)));
+    CUDA_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap)));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -714,9 +714,9 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cq.count = (unsigned*)ctx->counters.p + kCountCand;
     cq.cap = ccap;
     RefineStage rs;
-    rs.vals = ctx->refine_vals.p;
-    rs.live = (unsigned long long*)ctx->refine_pairs.p;
+    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64);
     rs.count = (unsigned*)ctx->counters.p + kCountPairs;
+    rs.big_count = (unsigned*)ctx->counters.p + kCountBig;
     const int f64 = field->dtype == FTK2B_F64;
     // the device pipeline in two parts so that the fused cull kernel can be
     // timed on its own: [counters reset, cull] and [exact tests, canonical
@@ -737,7 +737,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e;
       if ((e = launch_refine_staged(f64, rm, fa, cfg, cq, rs, sink, ctx->num_sms, ctx->stream))) return e;
-      *nl += 2;
+      *nl += 3;
       if ((e = launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, nl))) return e;
       if (prm->classify && !cfg.fiber) {
         if ((e = launch_classify_regular(f64, rm, fa, nch, B, ctx->stream))) return e;

@@ -32,6 +32,7 @@ enum {
   kCountCand = 4,
   kCountItems = 5,  // batches: next cull item
   kCountPairs = 6,  // simplices the exact test ran on
+  kCountBig = 7,    // candidates listed for the 128-bit inside test
   kNumCounters = 8
 };
 

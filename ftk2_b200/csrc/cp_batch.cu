@@ -279,8 +279,8 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     B_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     B_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     B_TRY(ctx, bc.cand_field.ensure(sizeof(unsigned) * (size_t)ccap));
-    B_TRY(ctx, ctx->refine_vals.ensure((size_t)ccap * 48 * (f64 ? 8 : 4)));
-    B_TRY(ctx, ctx->refine_pairs.ensure(sizeof(unsigned long long) * (size_t)ccap));
+    B_TRY(ctx, ctx->refine_vals.ensure(refine_stage_bytes(ccap, f64)));
+    B_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap)));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -298,9 +298,9 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     unsigned* const counters = static_cast<unsigned*>(ctx->counters.p);
     unsigned* const dfbase = static_cast<unsigned*>(bc.fbase.p);
     RefineStage rs;
-    rs.vals = ctx->refine_vals.p;
-    rs.live = static_cast<unsigned long long*>(ctx->refine_pairs.p);
+    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, f64);
     rs.count = counters + kCountPairs;
+    rs.big_count = counters + kCountBig;
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, ctx->stream);
       if (!e)
@@ -311,7 +311,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     };
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = launch_batch_refine_staged(f64, dfields, cq, rs, sink, ctx->num_sms, ctx->stream);
-      *nl += 2;
+      *nl += 3;
       if (!e) e = launch_post_batch(dmeshes, dkb, (int)n, B, dfbase, ctx->stream, nl);
       if (!e)
         e = cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost,

@@ -200,6 +200,77 @@ __device__ bool sos_inside3(const T v[4][3], double Q) {
 }
 
 // ---------------------------------------------------------------------------
+// The same inside tests from values quantised once per hypercube vertex: a
+// value enters as q when the fast path above would take it (|q| < 2^31 for
+// M = 2, 2^20 for M = 3, no overflow of the 64-bit conversion), else as
+// kQBig, and a simplex holding a kQBig value is tested by the functions above
+// from its field values.  Same signs, so the same decision.
+
+constexpr int kQBig = -2147483647 - 1;
+
+template <int M>
+__device__ __forceinline__ int quant_small(double v, double Q) {
+  bool b;
+  const long long q = quant64(v, Q, b);
+  const long long lim = M == 3 ? (1ll << 20) : (1ll << 31);
+  return (b || q >= lim || q <= -lim) ? kQBig : (int)q;
+}
+
+__device__ __forceinline__ bool sos_inside2_q(const int q[3][2]) {
+  const int tie[3] = {1, 1, -1};
+  int s[3];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const int a = e, b = (e + 1) % 3;
+    const long long d = (long long)q[a][0] * q[b][1] - (long long)q[a][1] * q[b][0];
+    s[e] = d ? sgn(d) : tie[e];
+  }
+  return s[0] == s[1] && s[1] == s[2];
+}
+
+// det3 of rows with |entries| < 2^20: the 2x2 minors from 32-bit products
+// (< 2^41), the whole sum below 2^63
+__device__ __forceinline__ long long det3_q32(const int a[3], const int b[3], const int c[3]) {
+  const long long m0 = (long long)b[1] * c[2] - (long long)b[2] * c[1];
+  const long long m1 = (long long)b[0] * c[2] - (long long)b[2] * c[0];
+  const long long m2 = (long long)b[0] * c[1] - (long long)b[1] * c[0];
+  return a[0] * m0 - a[1] * m1 + a[2] * m2;
+}
+
+// sos_det3_levels for entries below 2^20 in magnitude: every level is a
+// 2x2 minor (< 2^41) or a single entry, exact in 64 bits
+static __device__ __noinline__ int sos_det3_levels_q(const int a[3], const int b[3], const int c[3]) {
+  long long d;
+  auto m2 = [](int x0, int x1, int y0, int y1) { return (long long)x0 * y1 - (long long)x1 * y0; };
+  if ((d = m2(b[0], b[1], c[0], c[1]))) return sgn(d);    // 1
+  if ((d = -m2(b[0], b[2], c[0], c[2]))) return sgn(d);   // 2
+  if ((d = m2(b[1], b[2], c[1], c[2]))) return sgn(d);    // 3
+  if ((d = -m2(a[0], a[1], c[0], c[1]))) return sgn(d);   // 4
+  if ((d = c[0])) return sgn(d);                          // 5
+  if ((d = -(long long)c[1])) return sgn(d);              // 6
+  if ((d = m2(a[0], a[2], c[0], c[2]))) return sgn(d);    // 7
+  if ((d = c[2])) return sgn(d);                          // 8
+  if ((d = -m2(a[1], a[2], c[1], c[2]))) return sgn(d);   // 9
+  if ((d = m2(a[0], a[1], b[0], b[1]))) return sgn(d);    // 10
+  if ((d = -(long long)b[0])) return sgn(d);              // 11
+  if ((d = b[1])) return sgn(d);                          // 12
+  if ((d = a[0])) return sgn(d);                          // 13
+  return 1;                                               // 14
+}
+
+__device__ __forceinline__ bool sos_inside3_q(const int q[4][3]) {
+  int s[4];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    int r0, r1, r2;
+    face_rows(f, r0, r1, r2);
+    const long long d = det3_q32(q[r0], q[r1], q[r2]);
+    s[f] = d ? sgn(d) : sos_det3_levels_q(q[r0], q[r1], q[r2]);
+  }
+  return s[0] == s[1] && s[1] == s[2] && s[2] == s[3];
+}
+
+// ---------------------------------------------------------------------------
 // ZeroCrossingSolver<K,T>::solve, operation for operation
 
 template <int K, typename T>

@@ -10,7 +10,9 @@ namespace ftk2b {
 template <typename T>
 __device__ __forceinline__ T field_at(const FieldAccess& fa, int j, const long long g[4], int d,
                                       unsigned long long vid) {
-  const T* base = static_cast<const T*>(fa.comp[j]);
+  // a select instead of an index into the parameter array: an index that
+  // differs across lanes would copy the array to local memory
+  const T* base = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
   if (fa.per_vertex) return base[vid];
   long long o = 0;
 #pragma unroll

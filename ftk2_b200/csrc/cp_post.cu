@@ -540,93 +540,309 @@ static int grid_for(unsigned cap, int threads, int max_blocks) {
 
 // ---------------------------------------------------------------------------
 // Post-extraction for small feature counts (capacity <= kSmallPostCap): the
-// outputs of the general chain above in three launches.
-//   1. rank sort: every block holds all n keys in shared memory; the canonical
-//      position of a key is the number of keys below it (the keys of one
-//      extraction are distinct).  The block writes, at that position, its
-//      keys' sorted key, lambdas, float barycentrics, scalar and vertex ids.
-//   2. star edges: one warp per feature (edges_of_feature) with the sorted
-//      keys in shared memory.
-//   3. one block: exclusive scan of the edge counts, edge compaction, the
+// outputs of the general chain above in two launches.
+//   1. sort + star edges, one block of 1024 threads per SM, each block on all
+//      n keys in shared memory: a counting sort by the keys' top bits (bucket
+//      counts, their scan, every key scattered into its bucket), then each
+//      key's rank = its bucket's start + the keys of its bucket below it (the
+//      keys of one extraction are distinct, so every block finds the same
+//      order), and the sorted keys overwrite the buckets.  The block writes
+//      the outputs of features i with i mod gridDim == blockIdx at their
+//      ranks, and its warps find the star edges of the sorted features (one
+//      warp per feature) in the sorted keys.
+//   2. one block: exclusive scan of the edge counts, edge compaction, the
 //      union-find over the edges in shared memory, track ids and root count.
 
-constexpr int kRankThreads = 1024;
-constexpr int kRankMaxR = 8;  // keys per lane of a rank-sort block
+constexpr int kSortThreads = 1024;
+constexpr int kBucketBits = 13;
+constexpr int kBuckets = 1 << kBucketBits;
 
-template <int R>
-__device__ __forceinline__ void rank_keys(const unsigned long long* sk, unsigned n, unsigned base, int lane,
-                                          int warp, unsigned (*part)[kRankMaxR][32]) {
-  unsigned long long mine[R];
-  unsigned cnt[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const unsigned i = base + lane + 32u * r;
-    mine[r] = i < n ? sk[i] : ~0ull;
-    cnt[r] = 0;
+// Shared tables of the sort + edges kernel: the chain masks of the mesh's
+// dimension, 4 bits each with mk[0] = 0 in the lowest nibble, and the chain
+// rank by relative masks (c_rank3 / c_rank4).  Lane-dependent indices into
+// the constant bank would be serialised.
+struct StarTables {
+  unsigned mk[kMaxChains];
+  signed char rank[4096];
+};
+
+__device__ __forceinline__ void fill_star_tables(StarTables& T, int d) {
+  const ChainTable& CT = c_post_chains[d - 3];
+  for (int c = threadIdx.x; c < kMaxChains; c += blockDim.x) {
+    unsigned p = 0;
+    if (c < CT.n)
+      for (int k = 0; k < d - 1; ++k) p |= (unsigned)CT.mask[c][k] << (4 * (k + 1));
+    T.mk[c] = p;
   }
-  // warp w counts the keys of its segment below each of the lane's keys
-  const unsigned seg = (n + 31) / 32;
-  const unsigned j0 = min(n, warp * seg), j1 = min(n, j0 + seg);
-  for (unsigned j = j0; j < j1; ++j) {
-    const unsigned long long kj = sk[j];
-#pragma unroll
-    for (int r = 0; r < R; ++r) cnt[r] += kj < mine[r] ? 1u : 0u;
-  }
-#pragma unroll
-  for (int r = 0; r < R; ++r) part[warp][r][lane] = cnt[r];
+  for (int i = threadIdx.x; i < 4096; i += blockDim.x) T.rank[i] = d == 3 ? (i < 64 ? c_rank3[i] : -1) : c_rank4[i];
 }
 
-__global__ void __launch_bounds__(kRankThreads, 1)
-    small_rank_sort_kernel(RegularMesh mesh, int nch, PostBuffers B) {
-  pdl_enter();
-  extern __shared__ unsigned long long sk[];  // the n unsorted keys
-  __shared__ unsigned part[32][kRankMaxR][32];
-  const unsigned n = min(*B.count, B.cap);
-  const unsigned G = gridDim.x;
-  const unsigned R = (n + 32u * G - 1) / (32u * G);  // keys per lane
-  const unsigned base = blockIdx.x * 32u * R;
-  if (n == 0 || base >= n) return;
-  if (R > kRankMaxR) {  // the host sizes the grid so that this cannot happen
-    if (threadIdx.x == 0) atomicOr(B.err, 4u);
-    return;
+// a / b and a % b, in 32 bits when both fit
+__device__ __forceinline__ unsigned long long divmod_u64(unsigned long long a, unsigned long long b,
+                                                         unsigned long long& rem) {
+  if (((a | b) >> 32) == 0) {
+    const unsigned q = (unsigned)a / (unsigned)b;
+    rem = (unsigned)a - q * (unsigned)b;
+    return q;
   }
-  for (unsigned i = threadIdx.x; i < n; i += kRankThreads) sk[i] = B.key[i];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (R == 1) rank_keys<1>(sk, n, base, lane, warp, part);
-  else if (R == 2) rank_keys<2>(sk, n, base, lane, warp, part);
-  else if (R <= 4) rank_keys<4>(sk, n, base, lane, warp, part);
-  else rank_keys<8>(sk, n, base, lane, warp, part);
-  __syncthreads();
-  if (threadIdx.x >= 32u * R) return;
-  const int r = threadIdx.x >> 5, l = threadIdx.x & 31;
-  const unsigned i = base + l + 32u * r;
-  if (i >= n) return;
-  unsigned pos = 0;
-#pragma unroll 8
-  for (int w = 0; w < 32; ++w) pos += part[w][r][l];
-  const unsigned long long key = sk[i];
-  B.key_alt[pos] = key;
+  const unsigned long long q = a / b;
+  rem = a - q * b;
+  return q;
+}
+
+// Star edges of sorted feature i (one warp; key = kbase + local key): the two
+// Kuhn cofaces of its simplex inside the local box (the order of top_cells),
+// lane q * (d + 1) + r looks face r of coface q up in the sorted keys; when
+// feature i is the smallest active face of a coface it links to that coface's
+// other active faces.  Writes cnt[i] and the slots ascending.  Register-only
+// form of edges_of_feature.
+__device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch, const unsigned long long* keys,
+                                                unsigned n, unsigned i, unsigned long long local_key,
+                                                unsigned long long kbase, const StarTables& T, int lane,
+                                                unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+  const int d = mesh.d, m = d - 1, full = (1 << d) - 1;
+  unsigned long long rem;
+  unsigned long long vid = divmod_u64(local_key, (unsigned long long)nch, rem);
+  const int ch = (int)rem;
+  long long g[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    B.lam_sorted[4 * (size_t)pos + k] = B.lam[4 * (size_t)i + k];
-    B.bary4_sorted[4 * (size_t)pos + k] = B.bary4[4 * (size_t)i + k];
+    g[k] = 0;
+    if (k < d) {
+      vid = divmod_u64(vid, (unsigned long long)mesh.gd[k], rem);
+      g[k] = (long long)rem;
+    }
   }
-  B.scalar_sorted[pos] = B.scalar[i];
-  expand_feature(mesh, nch, key, pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
+  const unsigned mkp = T.mk[ch];  // masks of vertices 0..m, 4 bits each
+  const int mkm = (int)((mkp >> (4 * m)) & 15u);
+  const int missing = full & ~mkm;
+  const int q = lane > d ? 1 : 0, r = lane - q * (d + 1);
+  long long c[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c[k] = g[k];
+  unsigned cmp = 0;  // masks of the coface's d + 1 vertices, 4 bits each
+  int nc;
+  if (missing) {
+    // axis a never steps: prepend (corner - e_a) and / or append (full mask)
+    const int a = __ffs(missing) - 1;
+    long long ga = 0, la = 0;  // local coordinate and extent along a
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k == a) {
+        ga = g[k] - mesh.off[k];
+        la = mesh.ld[k];
+      }
+    const bool lo = ga >= 1, hi = ga + 1 < la;
+    nc = (int)lo + (int)hi;
+    if (lo && q == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k == a) c[k] -= 1;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j <= m) cmp |= ((((mkp >> (4 * j)) & 15u) | (1u << a)) << (4 * (j + 1)));
+    } else {
+      cmp = mkp | ((unsigned)full << (4 * (m + 1)));
+    }
+  } else {
+    // the one step of two axes, split in either order
+    int js = -1, ins_lo = 0, ins_hi = 0;
+#pragma unroll
+    for (int j = 1; j < 4; ++j)
+      if (j <= m && js < 0) {
+        const int step = (int)(((mkp >> (4 * j)) & 15u) & ~((mkp >> (4 * (j - 1))) & 15u));
+        if (__popc(step) == 2) {
+          js = j;
+          ins_lo = step & -step;
+          ins_hi = step & ~ins_lo;
+        }
+      }
+    nc = js < 0 ? 0 : 2;
+    if (js > 0) {
+      const unsigned ins = (unsigned)(q ? ins_hi : ins_lo);
+      const unsigned low = (1u << (4 * js)) - 1u;
+      cmp = (mkp & low) | ((((mkp >> (4 * (js - 1))) & 15u) | ins) << (4 * js)) | ((mkp & ~low) << 4);
+    }
+  }
+  long long idx = -1;
+  if (lane < nc * (d + 1)) {
+    // face without vertex r: based at vertex 1 when r == 0, else at vertex 0
+    const unsigned base = r == 0 ? ((cmp >> 4) & 15u) : 0u;
+    const int bits = d == 3 ? 3 : 4;
+    unsigned rel = 0;
+    int w = 0;
+#pragma unroll
+    for (int v = 1; v <= 4; ++v)
+      if (v <= d && v != r && !(r == 0 && v == 1)) {
+        rel |= (((cmp >> (4 * v)) & 15u) & ~base) << (bits * w);
+        ++w;
+      }
+    unsigned long long fvid = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < d) fvid += (unsigned long long)(c[k] + ((base >> k) & 1u)) * mesh.gstride[k];
+    idx = find_key(keys, n, kbase + fvid * (unsigned long long)nch + (unsigned long long)T.rank[rel]);
+  }
+  const unsigned act = __ballot_sync(0xFFFFFFFFu, idx >= 0);
+  bool qual[2] = {false, false};
+#pragma unroll
+  for (int qq = 0; qq < 2; ++qq)
+    if (qq < nc) {
+      const unsigned a = act & (((1u << (d + 1)) - 1u) << (qq * (d + 1)));
+      const unsigned v = ((a >> lane) & 1u) ? (unsigned)idx : 0xFFFFFFFFu;
+      const unsigned mn = __reduce_min_sync(0xFFFFFFFFu, v);
+      qual[qq] = __popc(a) >= 2 && mn == i;
+    }
+  // the other active faces of the qualifying cofaces are distinct (two top
+  // cells share only the feature), so each lane's slot is its rank among them
+  const bool valid = idx >= 0 && (q ? qual[1] : qual[0]) && (unsigned)idx != i;
+  const unsigned vm = __ballot_sync(0xFFFFFFFFu, valid);
+  unsigned rk = 0;
+  for (unsigned b = vm; b; b &= b - 1) {
+    const unsigned o = __shfl_sync(0xFFFFFFFFu, (unsigned)idx, __ffs(b) - 1);
+    rk += o < (unsigned)idx ? 1u : 0u;
+  }
+  if (valid) slots[(size_t)i * kEdgeSlots + rk] = (unsigned)idx;
+  if (lane == 0) cnt[i] = __popc(vm);
 }
 
-__global__ void __launch_bounds__(kRankThreads, 1)
-    small_edges_kernel(RegularMesh mesh, int nch, PostBuffers B) {
-  pdl_enter();
-  extern __shared__ unsigned long long sk[];  // the n sorted keys
-  const unsigned n = min(*B.count, B.cap);
-  for (unsigned i = threadIdx.x; i < n; i += kRankThreads) sk[i] = B.key_alt[i];
+// Exclusive scan over a block of 1024 threads, one value each; *total = sum.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* wsum /* 33 */, unsigned* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
   __syncthreads();
+  if (warp == 0) {
+    const unsigned w = wsum[lane];
+    unsigned wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    wsum[lane] = wi - w;
+    if (lane == 31) wsum[32] = wi;
+  }
+  __syncthreads();
+  *total = wsum[32];
+  return wsum[warp] + incl - v;
+}
+
+// The block's copy of the canonical order: keys i = threadIdx.x + 1024 k
+// (k < R) by bucket, rank within the bucket, sorted into sk.  rank[k]
+// receives the canonical position of the thread's k-th key.
+template <int R>
+__device__ __forceinline__ void block_sort_keys(const unsigned long long* __restrict__ key_in, unsigned n, int key_bits,
+                                                unsigned long long* sk, unsigned* bcnt, unsigned* wsum,
+                                                unsigned long long kv[R], unsigned rank[R]) {
+  const unsigned t = threadIdx.x;
+  const int shift = key_bits > kBucketBits ? key_bits - kBucketBits : 0;
+  // bucket of a key: its top bits (clamped, which keeps the order)
+  auto bucket = [shift](unsigned long long key) {
+    return (unsigned)min(key >> shift, (unsigned long long)(kBuckets - 1));
+  };
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const unsigned i = t + kSortThreads * k;
+    kv[k] = i < n ? key_in[i] : 0ull;
+  }
+#pragma unroll
+  for (int b = 0; b < kBuckets / kSortThreads; ++b) bcnt[t + kSortThreads * b] = 0;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    if (t + kSortThreads * k < n) atomicAdd(&bcnt[bucket(kv[k])], 1u);
+  __syncthreads();
+  // exclusive scan of the bucket counts: kBuckets / 1024 consecutive per thread
+  constexpr int kPerT = kBuckets / kSortThreads;
+  unsigned cb[kPerT], sum = 0;
+#pragma unroll
+  for (int b = 0; b < kPerT; ++b) {
+    cb[b] = bcnt[t * kPerT + b];
+    sum += cb[b];
+  }
+  unsigned total;
+  unsigned run = block_exclusive_scan(sum, wsum, &total);
+#pragma unroll
+  for (int b = 0; b < kPerT; ++b) {
+    bcnt[t * kPerT + b] = run;
+    run += cb[b];
+  }
+  __syncthreads();
+  // scatter; afterwards bcnt[b] = end of bucket b = start of bucket b + 1
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    if (t + kSortThreads * k < n) sk[atomicAdd(&bcnt[bucket(kv[k])], 1u)] = kv[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    rank[k] = 0;
+    if (t + kSortThreads * k < n) {
+      const unsigned b = bucket(kv[k]);
+      const unsigned b0 = b ? bcnt[b - 1] : 0u, b1 = bcnt[b];
+      unsigned below = 0;
+      for (unsigned j = b0; j < b1; ++j) below += sk[j] < kv[k] ? 1u : 0u;
+      rank[k] = b0 + below;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    if (t + kSortThreads * k < n) sk[rank[k]] = kv[k];
+  __syncthreads();
+}
+
+template <int R>
+__device__ __forceinline__ void sort_edges_body(const RegularMesh& mesh, int nch, const PostBuffers& B, unsigned n,
+                                                int want_edges, unsigned long long* sk, unsigned* bcnt,
+                                                unsigned* wsum, const StarTables& T) {
+  unsigned long long kv[R];
+  unsigned rank[R];
+  block_sort_keys<R>(B.key, n, B.key_bits, sk, bcnt, wsum, kv, rank);
+  const unsigned G = gridDim.x;
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const unsigned i = threadIdx.x + kSortThreads * k;
+    if (i < n && i % G == blockIdx.x) {
+      const unsigned pos = rank[k];
+      B.key_alt[pos] = kv[k];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        B.lam_sorted[4 * (size_t)pos + c] = B.lam[4 * (size_t)i + c];
+        B.bary4_sorted[4 * (size_t)pos + c] = B.bary4[4 * (size_t)i + c];
+      }
+      B.scalar_sorted[pos] = B.scalar[i];
+      expand_feature(mesh, nch, kv[k], pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
+    }
+  }
+  if (!want_edges) return;
   const int lane = threadIdx.x & 31;
-  const unsigned gw = (blockIdx.x * kRankThreads + threadIdx.x) >> 5;
-  const unsigned nw = (gridDim.x * kRankThreads) >> 5;
-  for (unsigned i = gw; i < n; i += nw) edges_of_feature(mesh, nch, sk, n, i, sk[i], 0ull, lane, B.edge_cnt, B.edge_slots);
+  const unsigned gw = (blockIdx.x * kSortThreads + threadIdx.x) >> 5;
+  const unsigned nw = (G * kSortThreads) >> 5;
+  for (unsigned i = gw; i < n; i += nw) star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots);
+}
+
+__global__ void __launch_bounds__(kSortThreads, 1)
+    small_sort_edges_kernel(RegularMesh mesh, int nch, PostBuffers B, int want_edges) {
+  extern __shared__ unsigned long long sk[];  // the n keys: by bucket, then sorted
+  __shared__ unsigned bcnt[kBuckets];
+  __shared__ unsigned wsum[33];
+  __shared__ StarTables T;
+  fill_star_tables(T, mesh.d);
+  pdl_enter();
+  const unsigned n = min(*B.count, B.cap);
+  if (n == 0) return;
+  const unsigned R = (n + kSortThreads - 1) / kSortThreads;
+  if (R <= 1) sort_edges_body<1>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
+  else if (R <= 2) sort_edges_body<2>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
+  else if (R <= 4) sort_edges_body<4>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
+  else if (R <= 8) sort_edges_body<8>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
+  else sort_edges_body<16>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
 }
 
 // union-find in shared memory: the global version's links (larger root under
@@ -741,22 +957,17 @@ static cudaError_t launch_post_small(const RegularMesh& mesh, int nch, const Pos
                                      cudaStream_t st, unsigned long long* launches) {
   const unsigned cap = B.cap;
   const size_t key_smem = sizeof(unsigned long long) * (size_t)(cap ? cap : 1);
-  int g1 = B.num_sms > 0 ? B.num_sms : 148;
-  const int need = (int)((cap + 32u * kRankMaxR - 1) / (32u * kRankMaxR));
-  if (g1 < need) g1 = need;
-  cudaError_t e = cudaFuncSetAttribute(small_rank_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const int g = B.num_sms > 0 ? B.num_sms : 148;
+  cudaError_t e = cudaFuncSetAttribute(small_sort_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)key_smem);
-  if (!e) e = launch_pdl(small_rank_sort_kernel, g1, kRankThreads, key_smem, st, mesh, nch, B);
+  if (!e) e = launch_pdl(small_sort_edges_kernel, g, kSortThreads, key_smem, st, mesh, nch, B, want_edges);
   if (e) return e;
   *launches += 1;
   if (!want_edges) return cudaGetLastError();
-  e = cudaFuncSetAttribute(small_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
-  if (!e) e = launch_pdl(small_edges_kernel, B.num_sms > 0 ? B.num_sms : 148, kRankThreads, key_smem, st, mesh, nch, B);
-  if (e) return e;
   const size_t uf_smem = sizeof(unsigned) * (2 * (size_t)cap + 1);
   e = cudaFuncSetAttribute(small_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uf_smem);
   if (!e) e = launch_pdl(small_finish_kernel, 1, 1024, uf_smem, st, B);
-  *launches += 2;
+  *launches += 1;
   return e ? e : cudaGetLastError();
 }
 

@@ -1325,7 +1325,7 @@ __device__ __forceinline__ void refine_candidate(const RegularMesh& mesh, const 
       }
     }
     T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
-    if (cfg.fiber) val = fp<T>::sub(val, (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
+    if (cfg.fiber) val = fp<T>::sub(val, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
     cube[v * M + j] = val;
   }
   __syncwarp();
@@ -1464,17 +1464,35 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 // integer SoS and the solve then keep every lane busy instead of the few
 // chains of a hypercube that survive its word test.
 
+// Masks of vertices 1..M of chain ch, a byte each (m1 | m2 << 8 | m3 << 16);
+// 0 past the table.  Kept in registers or shared memory by the exact-test
+// kernels: a constant-bank read indexed by a lane-dependent chain is
+// serialised over the distinct addresses of a warp.
+template <int D>
+__device__ __forceinline__ unsigned chain_packed(int ch) {
+  const ChainTable& CT = c_chains[D - 3];
+  unsigned p = 0;
+  if (ch < CT.n)
+#pragma unroll
+    for (int k = 0; k < D - 1; ++k) p |= (unsigned)CT.mask[ch][k] << (8 * k);
+  return p;
+}
+
 // One candidate by one warp: its vertex values into `out` (kStageVals values
-// per candidate) and the warp's shared cube, its vertex words, and the mask
-// of its surviving chains into rs.live[c].
+// per candidate) and the warp's shared cube, the values quantised for the
+// inside tests into `qout`, its vertex words, and the mask of its surviving
+// chains into rs.live[c] (or, when a value is off the fast path, into the
+// 128-bit list).  pk0 / pk1: chain_packed of chains lane and
+// 32 + lane.
 template <typename T, int D>
 __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const FieldAccess& fa,
                                                  const ExtractConfig& cfg, unsigned c, unsigned long long pc,
-                                                 unsigned long long chains, T* out, T* my, const unsigned* band_tbl,
+                                                 unsigned long long chains, T* out, int* qout, T* my,
+                                                 const unsigned* band_tbl, unsigned pk0, unsigned pk1,
                                                  const RefineStage& rs, int lane) {
   constexpr int M = D - 1;
   constexpr int NV = 1 << D;
-  const ChainTable& CT = c_chains[D - 3];
+  const int nch = c_chains[D - 3].n;
   const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
                           (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
   long long g0[4];
@@ -1483,6 +1501,7 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
     g0[k] = (k < D) ? lk + mesh.off[k] : 0;
   }
+  bool anybig = false;
   for (int e = lane; e < NV * M; e += 32) {
     const int v = e / M, j = e % M;
     long long g[4];
@@ -1497,11 +1516,14 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
       }
     }
     T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
-    if (cfg.fiber) val = fp<T>::sub(val, (T)cfg.fthr[j]);  // values[i][j] - thresholds[j]
+    if (cfg.fiber) val = fp<T>::sub(val, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
     my[e] = val;
     out[e] = val;
+    const int qv = quant_small<M>((double)val, cfg.Q);
+    qout[e] = qv;
+    anybig |= qv == kQBig;
   }
-  __syncwarp();
+  const bool big = __any_sync(0xFFFFFFFFu, anybig);
   unsigned vw = kAbsent;
   if (lane < NV) {
     unsigned h[M];
@@ -1512,17 +1534,32 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
     vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
   }
+  const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0);
   unsigned long long mask = 0;
-  for (int base = 0; base < CT.n; base += 32) {
-    const int ch = base + lane;
-    bool live = ch < CT.n && ((chains >> ch) & 1ull);
-    unsigned wacc = kAbsent;
 #pragma unroll
-    for (int i = 0; i <= M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, live ? (i ? CT.mask[ch][i - 1] : 0) : 0);
+  for (int half = 0; half < 2; ++half) {
+    if (half * 32 >= nch) break;
+    const int ch = half * 32 + lane;
+    const unsigned pk = half ? pk1 : pk0;
+    bool live = ch < nch && ((chains >> ch) & 1ull);
+    unsigned wacc = w0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pk >> (8 * i)) & 0xFF);
     live = live && (cfg.fiber || !word_culled(wacc));
-    mask |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, live) << base;
+    mask |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, live) << (half * 32);
   }
-  if (lane == 0) rs.live[c] = mask;
+  if (lane == 0) {
+    // a candidate holding a value off the fast path: every chain on the
+    // 128-bit path (at most one list entry per candidate)
+    unsigned long long fast = mask;
+    if (big && mask) {
+      const unsigned slot = atomicAdd(rs.big_count, 1u);
+      rs.big_list[slot] = c;
+      rs.big_live[slot] = mask;
+      fast = 0;
+    }
+    rs.live[c] = fast;
+  }
   __syncwarp();
 }
 
@@ -1535,39 +1572,60 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
   __shared__ T cube[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned pk0 = chain_packed<D>(lane), pk1 = chain_packed<D>(32 + lane);
   pdl_enter();
   __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const unsigned n = min(*cq.count, cq.cap);
   const unsigned gw = blockIdx.x * kRefineWarps + wib;
   const unsigned nw = gridDim.x * kRefineWarps;
   for (unsigned c = gw; c < n; c += nw)
     gather_candidate<T, D>(mesh, fa, cfg, c, cq.corner[c], cq.chains[c],
-                           static_cast<T*>(rs.vals) + (size_t)c * kStageVals, cube[wib], band_tbl, rs, lane);
+                           static_cast<T*>(rs.vals) + (size_t)c * kStageVals, rs.q + (size_t)c * kStageVals,
+                           cube[wib], band_tbl, pk0, pk1, rs, lane);
 }
 
 // One listed simplex (candidate c, chain ch) by one thread: the exact test
-// and, when accepted, its canonical key and reported values.
-template <typename T, int D>
+// and, when accepted, its canonical key and reported values.  src / qsrc:
+// the candidate's staged and quantised values; chain_pk: chain_packed of
+// every chain of the mesh's dimension.  BIG = false: every value of the
+// candidate takes the 64-bit fast path of the inside test (its quantised
+// form decides); BIG = true: the inside test from the field values.
+template <typename T, int D, bool BIG>
 __device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
-                                          unsigned long long pc, int ch, const T* src, unsigned long long key_base,
+                                          unsigned long long pc, int ch, const T* src, const int* qsrc,
+                                          const unsigned* chain_pk, unsigned long long key_base,
                                           unsigned long long& key, double lam_out[4], float bary_out[4],
                                           float& sc_out) {
   constexpr int M = D - 1;
   const ChainTable& CT = c_chains[D - 3];
   int mk[M + 1];
   mk[0] = 0;
+  const unsigned pk = chain_pk[ch];
 #pragma unroll
-  for (int k = 0; k < M; ++k) mk[k + 1] = CT.mask[ch][k];
+  for (int k = 0; k < M; ++k) mk[k + 1] = (pk >> (8 * k)) & 0xFF;
+  if constexpr (!BIG) {
+    int q[M + 1][M];
+#pragma unroll
+    for (int k = 0; k <= M; ++k)
+#pragma unroll
+      for (int j = 0; j < M; ++j) q[k][j] = qsrc[mk[k] * M + j];
+    bool inside;
+    if constexpr (M == 2) inside = sos_inside2_q(q);
+    else inside = sos_inside3_q(q);
+    if (!inside) return false;
+  }
   T vals[M + 1][M];
 #pragma unroll
   for (int k = 0; k <= M; ++k)
 #pragma unroll
     for (int j = 0; j < M; ++j) vals[k][j] = src[mk[k] * M + j];
-  bool inside;
-  if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
-  else inside = sos_inside3<T>(vals, cfg.Q);
-  if (!inside) return false;
+  if constexpr (BIG) {
+    bool inside;
+    if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
+    else inside = sos_inside3<T>(vals, cfg.Q);
+    if (!inside) return false;
+  }
   T lam[M + 1];
   bool solved = solve_exact<M, T>(vals, lam);
   if (!solved && cfg.fiber) {
@@ -1642,14 +1700,15 @@ __device__ __forceinline__ void sink_write(const FeatureSink& sink, bool acc, un
 
 constexpr int kPairCands = 64;  // candidates a block of the exact-test launch takes at a time
 
-// The block's next kPairCands candidates from `first`: masks and the prefix
-// counts of their set bits in shared memory; returns the number of simplices.
-__device__ __forceinline__ unsigned pairs_layout(const RefineStage& rs, unsigned first, unsigned n,
+// The block's next kPairCands entries of `live` from `first`: masks and the
+// prefix counts of their set bits in shared memory; returns the number of
+// simplices.
+__device__ __forceinline__ unsigned pairs_layout(const unsigned long long* live, unsigned first, unsigned n,
                                                  unsigned long long* msk, unsigned* off) {
   const int t = threadIdx.x;
   if (t < kPairCands) {
     const unsigned c = first + t;
-    msk[t] = c < n ? rs.live[c] : 0ull;
+    msk[t] = c < n ? live[c] : 0ull;
   }
   __syncthreads();
   if (t < 32) {
@@ -1685,17 +1744,22 @@ __device__ __forceinline__ void pairs_locate(unsigned p, const unsigned long lon
   ch = r < nlo ? (int)__fns(lo32, 0, (int)r + 1) : 32 + (int)__fns((unsigned)(m >> 32), 0, (int)(r - nlo) + 1);
 }
 
-template <typename T, int D>
-__global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
-                                                                            ExtractConfig cfg, CandidateQueue cq,
-                                                                            RefineStage rs, FeatureSink sink) {
+// BIG = false: the candidates of rs.live; true: those the gather listed for
+// the 128-bit path
+template <typename T, int D, bool BIG>
+__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
+                                                                                   ExtractConfig cfg, CandidateQueue cq,
+                                                                                   RefineStage rs, FeatureSink sink) {
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
+  __shared__ unsigned chain_pk[kMaxChains];
+  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
   pdl_enter();
   const int lane = threadIdx.x & 31;
-  const unsigned n = min(*cq.count, cq.cap);
+  const unsigned n = BIG ? *rs.big_count : min(*cq.count, cq.cap);
+  const unsigned long long* live = BIG ? rs.big_live : rs.live;
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
-    const unsigned P = pairs_layout(rs, first, n, msk, off);
+    const unsigned P = pairs_layout(live, first, n, msk, off);
     if (threadIdx.x == 0) atomicAdd(rs.count, P);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
@@ -1707,9 +1771,10 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_pairs_kernel(Regu
       if (p < P) {
         int k, ch;
         pairs_locate(p, msk, off, k, ch);
-        const unsigned c = first + k;
-        acc = test_pair<T, D>(mesh, fa, cfg, cq.corner[c], ch, static_cast<const T*>(rs.vals) + (size_t)c * kStageVals,
-                              0ull, key, lam_out, bary_out, sc_out);
+        const unsigned c = BIG ? rs.big_list[first + k] : first + k;
+        acc = test_pair<T, D, BIG>(mesh, fa, cfg, cq.corner[c], ch,
+                                   static_cast<const T*>(rs.vals) + (size_t)c * kStageVals,
+                                   rs.q + (size_t)c * kStageVals, chain_pk, 0ull, key, lam_out, bary_out, sc_out);
       }
       sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
@@ -1726,29 +1791,40 @@ __global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const B
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned pk3 = chain_packed<3>(lane);
+  const unsigned pk40 = chain_packed<4>(lane), pk41 = chain_packed<4>(32 + lane);
   const unsigned n = min(*cq.count, cq.cap);
   const unsigned gw = blockIdx.x * kRefineWarps + wib;
   const unsigned nw = gridDim.x * kRefineWarps;
   for (unsigned c = gw; c < n; c += nw) {
     const BatchField& F = fields[cq.field[c]];
     T* out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals;
+    int* qout = rs.q + (size_t)c * kStageVals;
     if (F.mesh.d == 4)
-      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, cube[wib], band_tbl, rs, lane);
+      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
+                             pk40, pk41, rs, lane);
     else
-      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, cube[wib], band_tbl, rs, lane);
+      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
+                             pk3, 0u, rs, lane);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kRefineWarps * 32, 2) batch_pairs_kernel(const BatchField* __restrict__ fields,
-                                                                           CandidateQueue cq, RefineStage rs,
-                                                                           FeatureSink sink) {
+template <typename T, bool BIG>
+__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) batch_pairs_kernel(const BatchField* __restrict__ fields,
+                                                                                  CandidateQueue cq, RefineStage rs,
+                                                                                  FeatureSink sink) {
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
+  __shared__ unsigned chain_pk[2][kMaxChains];
+  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
+    chain_pk[0][i] = chain_packed<3>(i);
+    chain_pk[1][i] = chain_packed<4>(i);
+  }
   const int lane = threadIdx.x & 31;
-  const unsigned n = min(*cq.count, cq.cap);
+  const unsigned n = BIG ? *rs.big_count : min(*cq.count, cq.cap);
+  const unsigned long long* live = BIG ? rs.big_live : rs.live;
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
-    const unsigned P = pairs_layout(rs, first, n, msk, off);
+    const unsigned P = pairs_layout(live, first, n, msk, off);
     if (threadIdx.x == 0) atomicAdd(rs.count, P);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
@@ -1760,15 +1836,16 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) batch_pairs_kernel(const
       if (p < P) {
         int k, ch;
         pairs_locate(p, msk, off, k, ch);
-        const unsigned c = first + k;
+        const unsigned c = BIG ? rs.big_list[first + k] : first + k;
         const BatchField& F = fields[cq.field[c]];
         const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
+        const int* qsrc = rs.q + (size_t)c * kStageVals;
         if (F.mesh.d == 4)
-          acc = test_pair<T, 4>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, F.key_base, key, lam_out, bary_out,
-                                sc_out);
+          acc = test_pair<T, 4, BIG>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, qsrc, chain_pk[1], F.key_base, key,
+                                     lam_out, bary_out, sc_out);
         else
-          acc = test_pair<T, 3>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, F.key_base, key, lam_out, bary_out,
-                                sc_out);
+          acc = test_pair<T, 3, BIG>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, qsrc, chain_pk[0], F.key_base, key,
+                                     lam_out, bary_out, sc_out);
       }
       sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
@@ -2206,32 +2283,27 @@ cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueu
   return cudaGetLastError();
 }
 
+template <typename T, int D>
+static cudaError_t launch_refine_staged_t(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                                          const CandidateQueue& cq, const RefineStage& rs, const FeatureSink& sink,
+                                          int num_sms, cudaStream_t st) {
+  const int thr = kRefineWarps * 32;
+  // programmatic dependent launches: each kernel waits for its predecessor
+  // at its start (pdl_enter), so its launch overlaps the predecessor's tail
+  cudaError_t e = launch_pdl(refine_gather_kernel<T, D>, num_sms * 16, thr, 0, st, mesh, fa, cfg, cq, rs);
+  if (!e) e = launch_pdl(refine_pairs_kernel<T, D, false>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
+  if (!e) e = launch_pdl(refine_pairs_kernel<T, D, true>, num_sms * 4, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
+  return e ? e : cudaGetLastError();
+}
+
 cudaError_t launch_refine_staged(int f64, const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                                  const CandidateQueue& cq, const RefineStage& rs, const FeatureSink& sink, int num_sms,
                                  cudaStream_t st) {
-  const int thr = kRefineWarps * 32;
-  const int g1 = num_sms * 16, g2 = num_sms * 4;
-  // programmatic dependent launches: each kernel waits for its predecessor
-  // at its start (pdl_enter), so its launch overlaps the predecessor's tail
-  cudaError_t e;
-  if (mesh.d == 4) {
-    if (f64) {
-      e = launch_pdl(refine_gather_kernel<double, 4>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
-      if (!e) e = launch_pdl(refine_pairs_kernel<double, 4>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-    } else {
-      e = launch_pdl(refine_gather_kernel<float, 4>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
-      if (!e) e = launch_pdl(refine_pairs_kernel<float, 4>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-    }
-  } else {
-    if (f64) {
-      e = launch_pdl(refine_gather_kernel<double, 3>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
-      if (!e) e = launch_pdl(refine_pairs_kernel<double, 3>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-    } else {
-      e = launch_pdl(refine_gather_kernel<float, 3>, g1, thr, 0, st, mesh, fa, cfg, cq, rs);
-      if (!e) e = launch_pdl(refine_pairs_kernel<float, 3>, g2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-    }
-  }
-  return e ? e : cudaGetLastError();
+  if (mesh.d == 4)
+    return f64 ? launch_refine_staged_t<double, 4>(mesh, fa, cfg, cq, rs, sink, num_sms, st)
+               : launch_refine_staged_t<float, 4>(mesh, fa, cfg, cq, rs, sink, num_sms, st);
+  return f64 ? launch_refine_staged_t<double, 3>(mesh, fa, cfg, cq, rs, sink, num_sms, st)
+             : launch_refine_staged_t<float, 3>(mesh, fa, cfg, cq, rs, sink, num_sms, st);
 }
 
 cudaError_t launch_refine_regular(int f64, const RegularMesh& mesh, const FieldAccess& fa,
@@ -2286,10 +2358,12 @@ cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const 
   const int thr = kRefineWarps * 32;
   if (f64) {
     batch_gather_kernel<double><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
-    batch_pairs_kernel<double><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<double, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<double, true><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
   } else {
     batch_gather_kernel<float><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
-    batch_pairs_kernel<float><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<float, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<float, true><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
   }
   return cudaGetLastError();
 }
