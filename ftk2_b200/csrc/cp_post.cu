@@ -24,6 +24,11 @@ namespace ftk2b {
 __constant__ ChainTable c_post_chains[2];
 __constant__ signed char c_rank3[64];     // (m1 | m2 << 3) -> chain rank, d = 3
 __constant__ signed char c_rank4[4096];   // (m1 | m2 << 4 | m3 << 8) -> chain rank, d = 4
+// the same tables for lane-dependent indices (the constant bank would
+// serialise them): chain masks of vertices 0..m, 4 bits each, and the rank
+// tables [0] = c_rank3 (64 entries, then -1), [1] = c_rank4
+__device__ unsigned g_star_mk[2][kMaxChains];
+__device__ __align__(16) signed char g_rank[2][4096];
 
 // ---------------------------------------------------------------------------
 // radix sort (keys u64, payload u32), stable, device-resident count
@@ -529,6 +534,17 @@ void upload_post_tables() {
     r4[h[1].mask[c][0] | (h[1].mask[c][1] << 4) | (h[1].mask[c][2] << 8)] = (signed char)c;
   cudaMemcpyToSymbol(c_rank3, r3, sizeof(r3));
   cudaMemcpyToSymbol(c_rank4, r4, sizeof(r4));
+  signed char gr[2][4096];
+  for (int i = 0; i < 4096; ++i) {
+    gr[0][i] = i < 64 ? r3[i] : (signed char)-1;
+    gr[1][i] = r4[i];
+  }
+  cudaMemcpyToSymbol(g_rank, gr, sizeof(gr));
+  unsigned mk[2][kMaxChains] = {};
+  for (int t = 0; t < 2; ++t)
+    for (int c = 0; c < h[t].n; ++c)
+      for (int k = 0; k < t + 2; ++k) mk[t][c] |= (unsigned)h[t].mask[c][k] << (4 * (k + 1));
+  cudaMemcpyToSymbol(g_star_mk, mk, sizeof(mk));
 }
 
 static int grid_for(unsigned cap, int threads, int max_blocks) {
@@ -561,20 +577,16 @@ constexpr int kBuckets = 1 << kBucketBits;
 // dimension, 4 bits each with mk[0] = 0 in the lowest nibble, and the chain
 // rank by relative masks (c_rank3 / c_rank4).  Lane-dependent indices into
 // the constant bank would be serialised.
-struct StarTables {
+struct __align__(16) StarTables {
   unsigned mk[kMaxChains];
   signed char rank[4096];
 };
 
 __device__ __forceinline__ void fill_star_tables(StarTables& T, int d) {
-  const ChainTable& CT = c_post_chains[d - 3];
-  for (int c = threadIdx.x; c < kMaxChains; c += blockDim.x) {
-    unsigned p = 0;
-    if (c < CT.n)
-      for (int k = 0; k < d - 1; ++k) p |= (unsigned)CT.mask[c][k] << (4 * (k + 1));
-    T.mk[c] = p;
-  }
-  for (int i = threadIdx.x; i < 4096; i += blockDim.x) T.rank[i] = d == 3 ? (i < 64 ? c_rank3[i] : -1) : c_rank4[i];
+  for (int c = threadIdx.x; c < kMaxChains; c += blockDim.x) T.mk[c] = g_star_mk[d - 3][c];
+  const unsigned* src = reinterpret_cast<const unsigned*>(g_rank[d - 3]);
+  unsigned* dst = reinterpret_cast<unsigned*>(T.rank);
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) dst[i] = src[i];
 }
 
 // a / b and a % b, in 32 bits when both fit
@@ -797,10 +809,22 @@ __device__ __forceinline__ void block_sort_keys(const unsigned long long* __rest
   __syncthreads();
 }
 
+// Outputs of feature i at its canonical position pos.
+static __device__ __noinline__ void write_sorted_feature(const RegularMesh& mesh, int nch, const PostBuffers& B,
+                                                         unsigned i, unsigned pos, unsigned long long key) {
+  B.key_alt[pos] = key;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    B.lam_sorted[4 * (size_t)pos + c] = B.lam[4 * (size_t)i + c];
+    B.bary4_sorted[4 * (size_t)pos + c] = B.bary4[4 * (size_t)i + c];
+  }
+  B.scalar_sorted[pos] = B.scalar[i];
+  expand_feature(mesh, nch, key, pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
+}
+
 template <int R>
-__device__ __forceinline__ void sort_edges_body(const RegularMesh& mesh, int nch, const PostBuffers& B, unsigned n,
-                                                int want_edges, unsigned long long* sk, unsigned* bcnt,
-                                                unsigned* wsum, const StarTables& T) {
+__device__ __forceinline__ void sort_and_write(const RegularMesh& mesh, int nch, const PostBuffers& B, unsigned n,
+                                               unsigned long long* sk, unsigned* bcnt, unsigned* wsum) {
   unsigned long long kv[R];
   unsigned rank[R];
   block_sort_keys<R>(B.key, n, B.key_bits, sk, bcnt, wsum, kv, rank);
@@ -808,23 +832,8 @@ __device__ __forceinline__ void sort_edges_body(const RegularMesh& mesh, int nch
 #pragma unroll
   for (int k = 0; k < R; ++k) {
     const unsigned i = threadIdx.x + kSortThreads * k;
-    if (i < n && i % G == blockIdx.x) {
-      const unsigned pos = rank[k];
-      B.key_alt[pos] = kv[k];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        B.lam_sorted[4 * (size_t)pos + c] = B.lam[4 * (size_t)i + c];
-        B.bary4_sorted[4 * (size_t)pos + c] = B.bary4[4 * (size_t)i + c];
-      }
-      B.scalar_sorted[pos] = B.scalar[i];
-      expand_feature(mesh, nch, kv[k], pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
-    }
+    if (i < n && i % G == blockIdx.x) write_sorted_feature(mesh, nch, B, i, rank[k], kv[k]);
   }
-  if (!want_edges) return;
-  const int lane = threadIdx.x & 31;
-  const unsigned gw = (blockIdx.x * kSortThreads + threadIdx.x) >> 5;
-  const unsigned nw = (G * kSortThreads) >> 5;
-  for (unsigned i = gw; i < n; i += nw) star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots);
 }
 
 __global__ void __launch_bounds__(kSortThreads, 1)
@@ -838,11 +847,15 @@ __global__ void __launch_bounds__(kSortThreads, 1)
   const unsigned n = min(*B.count, B.cap);
   if (n == 0) return;
   const unsigned R = (n + kSortThreads - 1) / kSortThreads;
-  if (R <= 1) sort_edges_body<1>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
-  else if (R <= 2) sort_edges_body<2>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
-  else if (R <= 4) sort_edges_body<4>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
-  else if (R <= 8) sort_edges_body<8>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
-  else sort_edges_body<16>(mesh, nch, B, n, want_edges, sk, bcnt, wsum, T);
+  if (R <= 2) sort_and_write<2>(mesh, nch, B, n, sk, bcnt, wsum);
+  else if (R <= 4) sort_and_write<4>(mesh, nch, B, n, sk, bcnt, wsum);
+  else if (R <= 8) sort_and_write<8>(mesh, nch, B, n, sk, bcnt, wsum);
+  else sort_and_write<16>(mesh, nch, B, n, sk, bcnt, wsum);
+  if (!want_edges) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned gw = (blockIdx.x * kSortThreads + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * kSortThreads) >> 5;
+  for (unsigned i = gw; i < n; i += nw) star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots);
 }
 
 // union-find in shared memory: the global version's links (larger root under
@@ -874,7 +887,7 @@ __device__ __forceinline__ void uf_unite_shared(unsigned* parent, unsigned a, un
 __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
   pdl_enter();
   extern __shared__ unsigned sh[];  // edge offsets of the n features (n + 1), then their union-find parents
-  __shared__ unsigned part[1024];
+  __shared__ unsigned wsum[33];
   __shared__ unsigned s_roots;
   constexpr int kPer = (int)(kSmallPostCap / 1024);  // features per thread, at most
   const unsigned n = min(*B.count, B.cap);
@@ -892,18 +905,10 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
     c[k] = (k < (int)seg && s0 + k < n) ? B.edge_cnt[s0 + k] : 0u;
     sum += c[k];
   }
-  part[t] = sum;
   for (unsigned i = t; i < n; i += 1024) sp[i] = i;
   if (t == 0) s_roots = 0;
-  __syncthreads();
-  for (unsigned o = 1; o < 1024; o <<= 1) {
-    const unsigned v = t >= o ? part[t - o] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
-  }
-  const unsigned total = part[1023];
-  unsigned run = part[t] - sum;
+  unsigned total;
+  unsigned run = block_exclusive_scan(sum, wsum, &total);
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
     if (k < (int)seg && s0 + k < n) off[s0 + k] = run;

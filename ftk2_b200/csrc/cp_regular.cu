@@ -40,6 +40,10 @@ __constant__ ChainTable c_chains[2];  // [0]: d=3, m=2 (12 chains); [1]: d=4, m=
 __constant__ unsigned long long c_chains_by_vmask[2][16];
 // chains whose last vertex steps along the time axis
 __constant__ unsigned long long c_time_chains[2];
+// masks of vertices 1..m of every chain, a byte each (m1 | m2 << 8 | m3 << 16),
+// 0 past the table: read with lane-dependent chain indices, which the
+// constant bank would serialise, so it lives in global memory
+__device__ unsigned g_chain_pk[2][kMaxChains];
 
 // ---------------------------------------------------------------------------
 // TMA / mbarrier primitives (inline PTX)
@@ -1465,17 +1469,10 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 // chains of a hypercube that survive its word test.
 
 // Masks of vertices 1..M of chain ch, a byte each (m1 | m2 << 8 | m3 << 16);
-// 0 past the table.  Kept in registers or shared memory by the exact-test
-// kernels: a constant-bank read indexed by a lane-dependent chain is
-// serialised over the distinct addresses of a warp.
+// 0 past the table.
 template <int D>
 __device__ __forceinline__ unsigned chain_packed(int ch) {
-  const ChainTable& CT = c_chains[D - 3];
-  unsigned p = 0;
-  if (ch < CT.n)
-#pragma unroll
-    for (int k = 0; k < D - 1; ++k) p |= (unsigned)CT.mask[ch][k] << (8 * k);
-  return p;
+  return g_chain_pk[D - 3][ch];
 }
 
 // One candidate by one warp: its vertex values into `out` (kStageVals values
@@ -1746,6 +1743,16 @@ __device__ __forceinline__ void pairs_locate(unsigned p, const unsigned long lon
 
 // BIG = false: the candidates of rs.live; true: those the gather listed for
 // the 128-bit path
+// The quantised values of the block's next kPairCands candidates (from
+// `first`, contiguous in rs.q) into shared memory, 16 bytes per copy.
+__device__ __forceinline__ void stage_quantised(const RefineStage& rs, unsigned first, unsigned n, int* sq) {
+  const unsigned nk = min(n - first, (unsigned)kPairCands);
+  const int4* src = reinterpret_cast<const int4*>(rs.q + (size_t)first * kStageVals);
+  int4* dst = reinterpret_cast<int4*>(sq);
+  for (unsigned e = threadIdx.x; e < nk * (kStageVals / 4); e += blockDim.x) dst[e] = src[e];
+  __syncthreads();
+}
+
 template <typename T, int D, bool BIG>
 __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
                                                                                    ExtractConfig cfg, CandidateQueue cq,
@@ -1753,6 +1760,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_k
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
   __shared__ unsigned chain_pk[kMaxChains];
+  __shared__ __align__(16) int sq[BIG ? 4 : kPairCands * kStageVals];  // the fast path's quantised values
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
   pdl_enter();
   const int lane = threadIdx.x & 31;
@@ -1761,6 +1769,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_k
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
     const unsigned P = pairs_layout(live, first, n, msk, off);
     if (threadIdx.x == 0) atomicAdd(rs.count, P);
+    if constexpr (!BIG) stage_quantised(rs, first, n, sq);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
       bool acc = false;
@@ -1773,8 +1782,8 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_k
         pairs_locate(p, msk, off, k, ch);
         const unsigned c = BIG ? rs.big_list[first + k] : first + k;
         acc = test_pair<T, D, BIG>(mesh, fa, cfg, cq.corner[c], ch,
-                                   static_cast<const T*>(rs.vals) + (size_t)c * kStageVals,
-                                   rs.q + (size_t)c * kStageVals, chain_pk, 0ull, key, lam_out, bary_out, sc_out);
+                                   static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, sq + k * kStageVals,
+                                   chain_pk, 0ull, key, lam_out, bary_out, sc_out);
       }
       sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
@@ -1816,6 +1825,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) batch_pairs_ke
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
   __shared__ unsigned chain_pk[2][kMaxChains];
+  __shared__ __align__(16) int sq[BIG ? 4 : kPairCands * kStageVals];
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
     chain_pk[0][i] = chain_packed<3>(i);
     chain_pk[1][i] = chain_packed<4>(i);
@@ -1826,6 +1836,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) batch_pairs_ke
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
     const unsigned P = pairs_layout(live, first, n, msk, off);
     if (threadIdx.x == 0) atomicAdd(rs.count, P);
+    if constexpr (!BIG) stage_quantised(rs, first, n, sq);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
       bool acc = false;
@@ -1839,7 +1850,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) batch_pairs_ke
         const unsigned c = BIG ? rs.big_list[first + k] : first + k;
         const BatchField& F = fields[cq.field[c]];
         const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
-        const int* qsrc = rs.q + (size_t)c * kStageVals;
+        const int* qsrc = sq + k * kStageVals;
         if (F.mesh.d == 4)
           acc = test_pair<T, 4, BIG>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, qsrc, chain_pk[1], F.key_base, key,
                                      lam_out, bary_out, sc_out);
@@ -2006,6 +2017,11 @@ void upload_chain_tables() {
       if (h[t].mask[c][t + 1] & tbit) tc[t] |= 1ull << c;
   }
   cudaMemcpyToSymbol(c_time_chains, tc, sizeof(tc));
+  unsigned pk[2][kMaxChains] = {};
+  for (int t = 0; t < 2; ++t)
+    for (int c = 0; c < h[t].n; ++c)
+      for (int k = 0; k < t + 2; ++k) pk[t][c] |= (unsigned)h[t].mask[c][k] << (8 * k);
+  cudaMemcpyToSymbol(g_chain_pk, pk, sizeof(pk));
 }
 
 
