@@ -201,19 +201,23 @@ __device__ bool sos_inside3(const T v[4][3], double Q) {
 
 // ---------------------------------------------------------------------------
 // The same inside tests from values quantised once per hypercube vertex: a
-// value enters as q when the fast path above would take it (|q| < 2^31 for
-// M = 2, 2^20 for M = 3, no overflow of the 64-bit conversion), else as
-// kQBig, and a simplex holding a kQBig value is tested by the functions above
-// from its field values.  Same signs, so the same decision.
+// value enters as q when |q| < 2^31 (and the 64-bit conversion did not
+// overflow), else as kQBig, and a simplex holding a kQBig value is tested by
+// the functions above from its field values.  Below 2^31 every 2x2 minor is
+// exact in 64 bits and a 3x3 determinant in 128, so the signs, and with them
+// the decision, are those of the functions above.
 
 constexpr int kQBig = -2147483647 - 1;
 
-template <int M>
-__device__ __forceinline__ int quant_small(double v, double Q) {
-  bool b;
-  const long long q = quant64(v, Q, b);
-  const long long lim = M == 3 ? (1ll << 20) : (1ll << 31);
-  return (b || q >= lim || q <= -lim) ? kQBig : (int)q;
+// p = (double)v * Q + (v > 0 ? 0.5 : -0.5), each operation rounded to
+// nearest; the quantised value is trunc(p)
+__device__ __forceinline__ double quant_p(double v, double Q) {
+  return __dadd_rn(__dmul_rn(v, Q), v > 0.0 ? 0.5 : -0.5);
+}
+
+__device__ __forceinline__ int quant_small_p(double p) {
+  if (!(fabs(p) < 2147483648.0)) return kQBig;  // |q| >= 2^31, or not finite
+  return (int)__double2ll_rz(p);
 }
 
 __device__ __forceinline__ bool sos_inside2_q(const int q[3][2]) {
@@ -228,44 +232,64 @@ __device__ __forceinline__ bool sos_inside2_q(const int q[3][2]) {
   return s[0] == s[1] && s[1] == s[2];
 }
 
-// det3 of rows with |entries| < 2^20: the 2x2 minors from 32-bit products
-// (< 2^41), the whole sum below 2^63
-__device__ __forceinline__ long long det3_q32(const int a[3], const int b[3], const int c[3]) {
-  const long long m0 = (long long)b[1] * c[2] - (long long)b[2] * c[1];
-  const long long m1 = (long long)b[0] * c[2] - (long long)b[2] * c[0];
-  const long long m2 = (long long)b[0] * c[1] - (long long)b[1] * c[0];
-  return a[0] * m0 - a[1] * m1 + a[2] * m2;
+// 2x2 minor x0*y1 - x1*y0 of entries below 2^31: each product below 2^62
+__device__ __forceinline__ long long minor2_q(int x0, int x1, int y0, int y1) {
+  return (long long)x0 * y1 - (long long)x1 * y0;
 }
 
-// sos_det3_levels for entries below 2^20 in magnitude: every level is a
-// 2x2 minor (< 2^41) or a single entry, exact in 64 bits
+// det3 of rows with entries below 2^20: minors below 2^41, the sum below 2^63
+__device__ __forceinline__ long long det3_q20(const int a[3], const int b[3], const int c[3]) {
+  return a[0] * minor2_q(b[1], b[2], c[1], c[2]) - a[1] * minor2_q(b[0], b[2], c[0], c[2]) +
+         a[2] * minor2_q(b[0], b[1], c[0], c[1]);
+}
+
+// det3 of rows with entries below 2^31: the sum below 2^96, in 128 bits
+__device__ __forceinline__ i128 det3_q31(const int a[3], const int b[3], const int c[3]) {
+  return (i128)a[0] * minor2_q(b[1], b[2], c[1], c[2]) - (i128)a[1] * minor2_q(b[0], b[2], c[0], c[2]) +
+         (i128)a[2] * minor2_q(b[0], b[1], c[0], c[1]);
+}
+
+// sos_det3_levels for entries below 2^31: every level is a 2x2 minor or a
+// single entry, exact in 64 bits
 static __device__ __noinline__ int sos_det3_levels_q(const int a[3], const int b[3], const int c[3]) {
   long long d;
-  auto m2 = [](int x0, int x1, int y0, int y1) { return (long long)x0 * y1 - (long long)x1 * y0; };
-  if ((d = m2(b[0], b[1], c[0], c[1]))) return sgn(d);    // 1
-  if ((d = -m2(b[0], b[2], c[0], c[2]))) return sgn(d);   // 2
-  if ((d = m2(b[1], b[2], c[1], c[2]))) return sgn(d);    // 3
-  if ((d = -m2(a[0], a[1], c[0], c[1]))) return sgn(d);   // 4
-  if ((d = c[0])) return sgn(d);                          // 5
-  if ((d = -(long long)c[1])) return sgn(d);              // 6
-  if ((d = m2(a[0], a[2], c[0], c[2]))) return sgn(d);    // 7
-  if ((d = c[2])) return sgn(d);                          // 8
-  if ((d = -m2(a[1], a[2], c[1], c[2]))) return sgn(d);   // 9
-  if ((d = m2(a[0], a[1], b[0], b[1]))) return sgn(d);    // 10
-  if ((d = -(long long)b[0])) return sgn(d);              // 11
-  if ((d = b[1])) return sgn(d);                          // 12
-  if ((d = a[0])) return sgn(d);                          // 13
-  return 1;                                               // 14
+  if ((d = minor2_q(b[0], b[1], c[0], c[1]))) return sgn(d);    // 1
+  if ((d = -minor2_q(b[0], b[2], c[0], c[2]))) return sgn(d);   // 2
+  if ((d = minor2_q(b[1], b[2], c[1], c[2]))) return sgn(d);    // 3
+  if ((d = -minor2_q(a[0], a[1], c[0], c[1]))) return sgn(d);   // 4
+  if ((d = c[0])) return sgn(d);                                // 5
+  if ((d = -(long long)c[1])) return sgn(d);                    // 6
+  if ((d = minor2_q(a[0], a[2], c[0], c[2]))) return sgn(d);    // 7
+  if ((d = c[2])) return sgn(d);                                // 8
+  if ((d = -minor2_q(a[1], a[2], c[1], c[2]))) return sgn(d);   // 9
+  if ((d = minor2_q(a[0], a[1], b[0], b[1]))) return sgn(d);    // 10
+  if ((d = -(long long)b[0])) return sgn(d);                    // 11
+  if ((d = b[1])) return sgn(d);                                // 12
+  if ((d = a[0])) return sgn(d);                                // 13
+  return 1;                                                     // 14
 }
 
 __device__ __forceinline__ bool sos_inside3_q(const int q[4][3]) {
+  // entries all below 2^20: the determinants in 64 bits
+  unsigned wide = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) wide |= ((unsigned)q[k][j] + (1u << 20)) >> 21;
   int s[4];
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     int r0, r1, r2;
     face_rows(f, r0, r1, r2);
-    const long long d = det3_q32(q[r0], q[r1], q[r2]);
-    s[f] = d ? sgn(d) : sos_det3_levels_q(q[r0], q[r1], q[r2]);
+    int sg;
+    if (!wide) {
+      const long long d = det3_q20(q[r0], q[r1], q[r2]);
+      sg = sgn(d);
+    } else {
+      const i128 d = det3_q31(q[r0], q[r1], q[r2]);
+      sg = sgn(d);
+    }
+    s[f] = sg ? sg : sos_det3_levels_q(q[r0], q[r1], q[r2]);
   }
   return s[0] == s[1] && s[1] == s[2] && s[2] == s[3];
 }

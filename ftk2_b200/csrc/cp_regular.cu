@@ -1479,14 +1479,20 @@ __device__ __forceinline__ unsigned chain_packed(int ch) {
 // per candidate) and the warp's shared cube, the values quantised for the
 // inside tests into `qout`, its vertex words, and the mask of its surviving
 // chains into rs.live[c] (or, when a value is off the fast path, into the
-// 128-bit list).  pk0 / pk1: chain_packed of chains lane and
-// 32 + lane.
+// 128-bit list).  pk0 / pk1: chain_packed of chains lane and 32 + lane;
+// qsg: the warp's kStageVals bytes of shared memory.
+//
+// A chain survives when its vertices' cull words do not prove that the solve
+// rejects it and when no component has quantised values of one strict sign
+// at all its vertices: q_j >= 1 everywhere (or <= -1) puts the origin at
+// least 1/2 away from the simplex's image in the lattice, so the inside test
+// (a symbolic perturbation of that image) answers "outside".
 template <typename T, int D>
 __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const FieldAccess& fa,
                                                  const ExtractConfig& cfg, unsigned c, unsigned long long pc,
                                                  unsigned long long chains, T* out, int* qout, T* my,
-                                                 const unsigned* band_tbl, unsigned pk0, unsigned pk1,
-                                                 const RefineStage& rs, int lane) {
+                                                 unsigned char* qsg, const unsigned* band_tbl, unsigned pk0,
+                                                 unsigned pk1, const RefineStage& rs, int lane) {
   constexpr int M = D - 1;
   constexpr int NV = 1 << D;
   const int nch = c_chains[D - 3].n;
@@ -1516,22 +1522,34 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     if (cfg.fiber) val = fp<T>::sub(val, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
     my[e] = val;
     out[e] = val;
-    const int qv = quant_small<M>((double)val, cfg.Q);
+    const double p = quant_p((double)val, cfg.Q);
+    const int qv = quant_small_p(p);
     qout[e] = qv;
     anybig |= qv == kQBig;
+    // strict sign of the quantised value (a value past 2^127 or not finite
+    // quantises to 0 in the reference's conversion)
+    qsg[e] = (unsigned char)((p >= 1.0 && p < 0x1p127) ? (1u << j) : ((p <= -1.0 && p > -0x1p127) ? (8u << j) : 0u));
   }
   const bool big = __any_sync(0xFFFFFFFFu, anybig);
-  unsigned vw = kAbsent;
+  __syncwarp();
+  unsigned vw = kAbsent, qw = 0x3Fu;  // absent vertices: neutral under AND
   if (lane < NV) {
     unsigned h[M];
+    unsigned qb = 0;
 #pragma unroll
-    for (int j = 0; j < M; ++j) h[j] = hi_word<T>(my[lane * M + j]);
+    for (int j = 0; j < M; ++j) {
+      h[j] = hi_word<T>(my[lane * M + j]);
+      qb |= qsg[lane * M + j];
+    }
     bool in = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
-    vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
+    if (in) {
+      vw = vertex_word_hi<T, M>(h, band_tbl);
+      qw = qb;
+    }
   }
-  const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0);
+  const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0), q0 = __shfl_sync(0xFFFFFFFFu, qw, 0);
   unsigned long long mask = 0;
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
@@ -1539,10 +1557,14 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     const int ch = half * 32 + lane;
     const unsigned pk = half ? pk1 : pk0;
     bool live = ch < nch && ((chains >> ch) & 1ull);
-    unsigned wacc = w0;
+    unsigned wacc = w0, qacc = q0;
 #pragma unroll
-    for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pk >> (8 * i)) & 0xFF);
-    live = live && (cfg.fiber || !word_culled(wacc));
+    for (int i = 0; i < M; ++i) {
+      const int src = (pk >> (8 * i)) & 0xFF;
+      wacc &= __shfl_sync(0xFFFFFFFFu, vw, src);
+      qacc &= __shfl_sync(0xFFFFFFFFu, qw, src);
+    }
+    live = live && qacc == 0 && (cfg.fiber || !word_culled(wacc));
     mask |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, live) << (half * 32);
   }
   if (lane == 0) {
@@ -1567,6 +1589,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
                                                                           ExtractConfig cfg, CandidateQueue cq,
                                                                           RefineStage rs) {
   __shared__ T cube[kRefineWarps][kStageVals];
+  __shared__ unsigned char qsg[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1579,7 +1602,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
   for (unsigned c = gw; c < n; c += nw)
     gather_candidate<T, D>(mesh, fa, cfg, c, cq.corner[c], cq.chains[c],
                            static_cast<T*>(rs.vals) + (size_t)c * kStageVals, rs.q + (size_t)c * kStageVals,
-                           cube[wib], band_tbl, pk0, pk1, rs, lane);
+                           cube[wib], qsg[wib], band_tbl, pk0, pk1, rs, lane);
 }
 
 // One listed simplex (candidate c, chain ch) by one thread: the exact test
@@ -1796,6 +1819,7 @@ template <typename T>
 __global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const BatchField* __restrict__ fields,
                                                                          CandidateQueue cq, RefineStage rs) {
   __shared__ T cube[kRefineWarps][kStageVals];
+  __shared__ unsigned char qsg[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   __syncthreads();
@@ -1810,11 +1834,11 @@ __global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const B
     T* out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals;
     int* qout = rs.q + (size_t)c * kStageVals;
     if (F.mesh.d == 4)
-      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
-                             pk40, pk41, rs, lane);
+      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], qsg[wib],
+                             band_tbl, pk40, pk41, rs, lane);
     else
-      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
-                             pk3, 0u, rs, lane);
+      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], qsg[wib],
+                             band_tbl, pk3, 0u, rs, lane);
   }
 }
 
