@@ -555,23 +555,28 @@ static int grid_for(unsigned cap, int threads, int max_blocks) {
 }
 
 // ---------------------------------------------------------------------------
-// Post-extraction for small feature counts (capacity <= kSmallPostCap): the
-// outputs of the general chain above in two launches.
-//   1. sort + star edges, one block of 1024 threads per SM, each block on all
-//      n keys in shared memory: a counting sort by the keys' top bits (bucket
-//      counts, their scan, every key scattered into its bucket), then each
-//      key's rank = its bucket's start + the keys of its bucket below it (the
-//      keys of one extraction are distinct, so every block finds the same
-//      order), and the sorted keys overwrite the buckets.  The block writes
-//      the outputs of features i with i mod gridDim == blockIdx at their
-//      ranks, and its warps find the star edges of the sorted features (one
-//      warp per feature) in the sorted keys.
-//   2. one block: exclusive scan of the edge counts, edge compaction, the
-//      union-find over the edges in shared memory, track ids and root count.
+// Post-extraction for small feature counts (capacity <= kSmallPostCap, keys
+// below 2^50): the outputs of the general chain above in three launches.
+//   1. sort, one block: a counting sort of the keys (each packed with its
+//      feature index in the low kIdxBits bits) by their top bits in shared
+//      memory, then each key's canonical position = its bucket's start + the
+//      keys of its bucket below it (the keys of one extraction are
+//      distinct); the packed keys land in key_alt in canonical order.
+//   2. star edges, one block of 1024 threads per SM: every block copies the
+//      sorted keys into shared memory, writes the outputs of positions p with
+//      p mod gridDim == blockIdx, and its warps find the star edges of the
+//      sorted features (one warp per feature) in the sorted keys and join
+//      each feature with its linked faces in a lock-free union-find (parents
+//      initialised by the sort).
+//   3. one block: exclusive scan of the edge counts, edge compaction, and
+//      every feature's root (the union-find's parents copied to shared
+//      memory): track ids and root count.
 
 constexpr int kSortThreads = 1024;
 constexpr int kBucketBits = 13;
 constexpr int kBuckets = 1 << kBucketBits;
+constexpr int kIdxBits = 14;  // feature index bits packed under a key (kSmallPostCap = 2^14)
+static_assert((1u << kIdxBits) >= kSmallPostCap, "feature indices of the short chain fit kIdxBits");
 
 // Shared tables of the sort + edges kernel: the chain masks of the mesh's
 // dimension, 4 bits each with mk[0] = 0 in the lowest nibble, and the chain
@@ -606,12 +611,14 @@ __device__ __forceinline__ unsigned long long divmod_u64(unsigned long long a, u
 // Kuhn cofaces of its simplex inside the local box (the order of top_cells),
 // lane q * (d + 1) + r looks face r of coface q up in the sorted keys; when
 // feature i is the smallest active face of a coface it links to that coface's
-// other active faces.  Writes cnt[i] and the slots ascending.  Register-only
-// form of edges_of_feature.
+// other active faces.  Writes cnt[i] and the slots ascending, and (parent not
+// null) joins i with every linked face in the union-find.  Register-only form
+// of edges_of_feature.
 __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch, const unsigned long long* keys,
                                                 unsigned n, unsigned i, unsigned long long local_key,
                                                 unsigned long long kbase, const StarTables& T, int lane,
-                                                unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+                                                unsigned* __restrict__ cnt, unsigned* __restrict__ slots,
+                                                unsigned* parent, unsigned* err) {
   const int d = mesh.d, m = d - 1, full = (1 << d) - 1;
   unsigned long long rem;
   unsigned long long vid = divmod_u64(local_key, (unsigned long long)nch, rem);
@@ -714,7 +721,10 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
     const unsigned o = __shfl_sync(0xFFFFFFFFu, (unsigned)idx, __ffs(b) - 1);
     rk += o < (unsigned)idx ? 1u : 0u;
   }
-  if (valid) slots[(size_t)i * kEdgeSlots + rk] = (unsigned)idx;
+  if (valid) {
+    slots[(size_t)i * kEdgeSlots + rk] = (unsigned)idx;
+    if (parent) uf_unite(parent, i, (unsigned)idx, err);
+  }
   if (lane == 0) cnt[i] = __popc(vm);
 }
 
@@ -745,32 +755,23 @@ __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* w
   return wsum[warp] + incl - v;
 }
 
-// The block's copy of the canonical order: keys i = threadIdx.x + 1024 k
-// (k < R) by bucket, rank within the bucket, sorted into sk.  rank[k]
-// receives the canonical position of the thread's k-th key.
-template <int R>
-__device__ __forceinline__ void block_sort_keys(const unsigned long long* __restrict__ key_in, unsigned n, int key_bits,
-                                                unsigned long long* sk, unsigned* bcnt, unsigned* wsum,
-                                                unsigned long long kv[R], unsigned rank[R]) {
+__global__ void __launch_bounds__(kSortThreads, 1) small_sort_kernel(PostBuffers B) {
+  extern __shared__ unsigned long long sk[];  // the n packed keys, by bucket
+  __shared__ unsigned bcnt[kBuckets];
+  __shared__ unsigned wsum[33];
   const unsigned t = threadIdx.x;
-  const int shift = key_bits > kBucketBits ? key_bits - kBucketBits : 0;
+  for (unsigned b = t; b < kBuckets; b += kSortThreads) bcnt[b] = 0;
+  pdl_enter();
+  const unsigned n = min(*B.count, B.cap);
+  const int shift = B.key_bits > kBucketBits ? B.key_bits - kBucketBits : 0;
   // bucket of a key: its top bits (clamped, which keeps the order)
   auto bucket = [shift](unsigned long long key) {
     return (unsigned)min(key >> shift, (unsigned long long)(kBuckets - 1));
   };
-#pragma unroll
-  for (int k = 0; k < R; ++k) {
-    const unsigned i = t + kSortThreads * k;
-    kv[k] = i < n ? key_in[i] : 0ull;
-  }
-#pragma unroll
-  for (int b = 0; b < kBuckets / kSortThreads; ++b) bcnt[t + kSortThreads * b] = 0;
   __syncthreads();
-#pragma unroll
-  for (int k = 0; k < R; ++k)
-    if (t + kSortThreads * k < n) atomicAdd(&bcnt[bucket(kv[k])], 1u);
+  for (unsigned i = t; i < n; i += kSortThreads) atomicAdd(&bcnt[bucket(B.key[i])], 1u);
   __syncthreads();
-  // exclusive scan of the bucket counts: kBuckets / 1024 consecutive per thread
+  // exclusive scan of the bucket counts, kBuckets / 1024 consecutive per thread
   constexpr int kPerT = kBuckets / kSortThreads;
   unsigned cb[kPerT], sum = 0;
 #pragma unroll
@@ -787,32 +788,27 @@ __device__ __forceinline__ void block_sort_keys(const unsigned long long* __rest
   }
   __syncthreads();
   // scatter; afterwards bcnt[b] = end of bucket b = start of bucket b + 1
-#pragma unroll
-  for (int k = 0; k < R; ++k)
-    if (t + kSortThreads * k < n) sk[atomicAdd(&bcnt[bucket(kv[k])], 1u)] = kv[k];
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < R; ++k) {
-    rank[k] = 0;
-    if (t + kSortThreads * k < n) {
-      const unsigned b = bucket(kv[k]);
-      const unsigned b0 = b ? bcnt[b - 1] : 0u, b1 = bcnt[b];
-      unsigned below = 0;
-      for (unsigned j = b0; j < b1; ++j) below += sk[j] < kv[k] ? 1u : 0u;
-      rank[k] = b0 + below;
-    }
+  for (unsigned i = t; i < n; i += kSortThreads) {
+    const unsigned long long key = B.key[i];
+    sk[atomicAdd(&bcnt[bucket(key)], 1u)] = (key << kIdxBits) | i;
   }
   __syncthreads();
-#pragma unroll
-  for (int k = 0; k < R; ++k)
-    if (t + kSortThreads * k < n) sk[rank[k]] = kv[k];
-  __syncthreads();
+  // union-find parents of the canonical positions (the edge kernel hooks)
+  for (unsigned p = t; p < n; p += kSortThreads) B.parent[p] = p;
+  // packed keys compare like their keys (distinct keys)
+  for (unsigned p = t; p < n; p += kSortThreads) {
+    const unsigned long long v = sk[p];
+    const unsigned b = bucket(v >> kIdxBits);
+    const unsigned b0 = b ? bcnt[b - 1] : 0u, b1 = bcnt[b];
+    unsigned below = 0;
+    for (unsigned j = b0; j < b1; ++j) below += sk[j] < v ? 1u : 0u;
+    B.key_alt[b0 + below] = v;
+  }
 }
 
 // Outputs of feature i at its canonical position pos.
-static __device__ __noinline__ void write_sorted_feature(const RegularMesh& mesh, int nch, const PostBuffers& B,
-                                                         unsigned i, unsigned pos, unsigned long long key) {
-  B.key_alt[pos] = key;
+__device__ __forceinline__ void write_sorted_feature(const RegularMesh& mesh, int nch, const PostBuffers& B,
+                                                     unsigned i, unsigned pos, unsigned long long key) {
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     B.lam_sorted[4 * (size_t)pos + c] = B.lam[4 * (size_t)i + c];
@@ -822,66 +818,27 @@ static __device__ __noinline__ void write_sorted_feature(const RegularMesh& mesh
   expand_feature(mesh, nch, key, pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
 }
 
-template <int R>
-__device__ __forceinline__ void sort_and_write(const RegularMesh& mesh, int nch, const PostBuffers& B, unsigned n,
-                                               unsigned long long* sk, unsigned* bcnt, unsigned* wsum) {
-  unsigned long long kv[R];
-  unsigned rank[R];
-  block_sort_keys<R>(B.key, n, B.key_bits, sk, bcnt, wsum, kv, rank);
-  const unsigned G = gridDim.x;
-#pragma unroll
-  for (int k = 0; k < R; ++k) {
-    const unsigned i = threadIdx.x + kSortThreads * k;
-    if (i < n && i % G == blockIdx.x) write_sorted_feature(mesh, nch, B, i, rank[k], kv[k]);
-  }
-}
-
 __global__ void __launch_bounds__(kSortThreads, 1)
-    small_sort_edges_kernel(RegularMesh mesh, int nch, PostBuffers B, int want_edges) {
-  extern __shared__ unsigned long long sk[];  // the n keys: by bucket, then sorted
-  __shared__ unsigned bcnt[kBuckets];
-  __shared__ unsigned wsum[33];
+    small_edges_kernel(RegularMesh mesh, int nch, PostBuffers B, int want_edges) {
+  extern __shared__ unsigned long long sk[];  // the n sorted keys
   __shared__ StarTables T;
   fill_star_tables(T, mesh.d);
   pdl_enter();
   const unsigned n = min(*B.count, B.cap);
-  if (n == 0) return;
-  const unsigned R = (n + kSortThreads - 1) / kSortThreads;
-  if (R <= 2) sort_and_write<2>(mesh, nch, B, n, sk, bcnt, wsum);
-  else if (R <= 4) sort_and_write<4>(mesh, nch, B, n, sk, bcnt, wsum);
-  else if (R <= 8) sort_and_write<8>(mesh, nch, B, n, sk, bcnt, wsum);
-  else sort_and_write<16>(mesh, nch, B, n, sk, bcnt, wsum);
+  const unsigned G = gridDim.x;
+  for (unsigned p = threadIdx.x; p < n; p += kSortThreads) {
+    const unsigned long long v = B.key_alt[p];
+    sk[p] = v >> kIdxBits;
+    if (p % G == blockIdx.x)
+      write_sorted_feature(mesh, nch, B, (unsigned)(v & ((1ull << kIdxBits) - 1)), p, v >> kIdxBits);
+  }
   if (!want_edges) return;
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned gw = (blockIdx.x * kSortThreads + threadIdx.x) >> 5;
-  const unsigned nw = (gridDim.x * kSortThreads) >> 5;
-  for (unsigned i = gw; i < n; i += nw) star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots);
-}
-
-// union-find in shared memory: the global version's links (larger root under
-// the smaller one) with shared-memory atomics
-__device__ __forceinline__ unsigned uf_root_shared(unsigned* parent, unsigned x) {
-  volatile unsigned* vp = parent;
-  unsigned p = vp[x];
-  while (p != x) {
-    const unsigned gp = vp[p];
-    if (gp < p) atomicMin(&parent[x], gp);
-    x = p;
-    p = gp;
-  }
-  return x;
-}
-
-__device__ __forceinline__ void uf_unite_shared(unsigned* parent, unsigned a, unsigned b, unsigned* err) {
-  for (int it = 0; it < (1 << 20); ++it) {
-    const unsigned ra = uf_root_shared(parent, a), rb = uf_root_shared(parent, b);
-    if (ra == rb) return;
-    const unsigned lo = min(ra, rb), hi = max(ra, rb);
-    if (atomicCAS(&parent[hi], hi, lo) == hi) return;
-    a = ra;
-    b = rb;
-  }
-  atomicOr(err, 1u);
+  const unsigned nw = (G * kSortThreads) >> 5;
+  for (unsigned i = gw; i < n; i += nw)
+    star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots, B.parent, B.err);
 }
 
 __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
@@ -905,7 +862,8 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
     c[k] = (k < (int)seg && s0 + k < n) ? B.edge_cnt[s0 + k] : 0u;
     sum += c[k];
   }
-  for (unsigned i = t; i < n; i += 1024) sp[i] = i;
+  // the edge kernel's union-find is complete: its parents into shared memory
+  for (unsigned i = t; i < n; i += 1024) sp[i] = __ldcg(&B.parent[i]);
   if (t == 0) s_roots = 0;
   unsigned total;
   unsigned run = block_exclusive_scan(sum, wsum, &total);
@@ -935,21 +893,14 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
       B.edges[2 * (size_t)e + 1] = other;
     }
   }
-  __syncthreads();
-  // hooks: each thread a contiguous run of edges (edges sorted by centre lie
-  // mostly within one track, runs of different threads mostly in different
-  // tracks, so few threads contend for the same root)
-  {
-    const unsigned ne = min(total, B.edge_cap);
-    const unsigned eseg = (ne + 1023) / 1024;
-    const unsigned e0 = min(t * eseg, ne), e1 = min(e0 + eseg, ne);
-    for (unsigned e = e0; e < e1; ++e)
-      uf_unite_shared(sp, B.edges[2 * (size_t)e], B.edges[2 * (size_t)e + 1], B.err);
-  }
-  __syncthreads();
+  // every feature's root: the minimum of its component
   unsigned roots = 0;
   for (unsigned i = t; i < n; i += 1024) {
-    const unsigned x = uf_root_shared(sp, i);
+    unsigned x = i, p = sp[x];
+    while (p != x) {
+      x = p;
+      p = sp[x];
+    }
     B.track[i] = x;
     roots += x == i ? 1u : 0u;
   }
@@ -963,11 +914,12 @@ static cudaError_t launch_post_small(const RegularMesh& mesh, int nch, const Pos
   const unsigned cap = B.cap;
   const size_t key_smem = sizeof(unsigned long long) * (size_t)(cap ? cap : 1);
   const int g = B.num_sms > 0 ? B.num_sms : 148;
-  cudaError_t e = cudaFuncSetAttribute(small_sort_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)key_smem);
-  if (!e) e = launch_pdl(small_sort_edges_kernel, g, kSortThreads, key_smem, st, mesh, nch, B, want_edges);
+  cudaError_t e = cudaFuncSetAttribute(small_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
+  if (!e) e = launch_pdl(small_sort_kernel, 1, kSortThreads, key_smem, st, B);
+  if (!e) e = cudaFuncSetAttribute(small_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
+  if (!e) e = launch_pdl(small_edges_kernel, g, kSortThreads, key_smem, st, mesh, nch, B, want_edges);
   if (e) return e;
-  *launches += 1;
+  *launches += 2;
   if (!want_edges) return cudaGetLastError();
   const size_t uf_smem = sizeof(unsigned) * (2 * (size_t)cap + 1);
   e = cudaFuncSetAttribute(small_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uf_smem);
@@ -979,7 +931,8 @@ static cudaError_t launch_post_small(const RegularMesh& mesh, int nch, const Pos
 cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuffers& B,
                                 int want_edges, cudaStream_t st, unsigned long long* launches) {
   const unsigned cap = B.cap;
-  if (cap <= kSmallPostCap) return launch_post_small(mesh, nch, B, want_edges, st, launches);
+  if (cap <= kSmallPostCap && B.key_bits <= 64 - kIdxBits)
+    return launch_post_small(mesh, nch, B, want_edges, st, launches);
   const int gsort = B.sort_grid;
   const int g = grid_for(cap, 256, 4096);
   // keys in canonical order: multi-block stable LSD radix passes

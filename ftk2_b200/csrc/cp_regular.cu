@@ -278,6 +278,28 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   for (int j = 0; j < (MULTI ? 1 : M); ++j)
     pbase |= (unsigned)(reinterpret_cast<uintptr_t>(fa.comp[j]) & 15) << (4 * j);
   const long long tstride = fa.estride[D - 1];
+  // bulk staging: warp 0's lanes issue box rows lane + 32 i; the source
+  // address of each row at array time 0 (0 for rows outside the mesh) and
+  // the bytes of a row's local vertices
+  constexpr int RPL = (G::ROWS + 31) / 32;
+  uintptr_t rsrc[RPL];
+  const int rbytes = min(VX, ldx - x0) * (MULTI ? M : 1) * (int)sizeof(T);
+#pragma unroll
+  for (int i = 0; i < RPL; ++i) {
+    rsrc[i] = 0;
+    const int r = lane + 32 * i;
+    if (bulk && warp == 0 && r < G::ROWS) {
+      const int rr = MULTI ? r : r % (VY * VZ);
+      const int j = MULTI ? 0 : r / (VY * VZ);
+      const int vy = rr % VY, vz = rr / VY;
+      if (y0 + vy < ldy && (D == 3 || z0 + vz < ldz)) {
+        long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
+        if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
+        rsrc[i] = reinterpret_cast<uintptr_t>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2])) +
+                  (uintptr_t)(e * (long long)sizeof(T));
+      }
+    }
+  }
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
@@ -309,41 +331,25 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       // bytes read around the row lie in pages the row occupies); the rows'
       // byte total goes to the mbarrier before any copy is issued
       if (warp == 0) {
-        const long long at = (long long)tcoord(s);
-        const int nvx = min(VX, ldx - x0);
-        const int rbytes = nvx * (MULTI ? M : 1) * (int)sizeof(T);
-        auto row_src = [&](int r, uintptr_t& lo, unsigned& n) {
-          const int rr = MULTI ? r : r % (VY * VZ);
-          const int j = MULTI ? 0 : r / (VY * VZ);
-          const int vy = rr % VY, vz = rr / VY;
-          n = 0;
-          lo = 0;
-          if (y0 + vy >= ldy || (D == 4 && z0 + vz >= ldz)) return;
-          long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
-          if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
-          e += at * tstride;
-          const uintptr_t src = reinterpret_cast<uintptr_t>(fa.comp[j]) + (uintptr_t)(e * (long long)sizeof(T));
-          lo = src & ~(uintptr_t)15;
-          n = (unsigned)(((src + (uintptr_t)rbytes + 15) & ~(uintptr_t)15) - lo);
-        };
+        const uintptr_t tb = (uintptr_t)((long long)tcoord(s) * tstride * (long long)sizeof(T));
         unsigned total = 0;
-        for (int r = lane; r < G::ROWS; r += 32) {
-          uintptr_t lo;
-          unsigned n;
-          row_src(r, lo, n);
-          total += n;
+        uintptr_t lo[RPL];
+        unsigned nb[RPL];
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          const uintptr_t src = rsrc[i] + tb;
+          lo[i] = src & ~(uintptr_t)15;
+          nb[i] = rsrc[i] ? (unsigned)(((src + (uintptr_t)rbytes + 15) & ~(uintptr_t)15) - lo[i]) : 0u;
+          total += nb[i];
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xFFFFFFFFu, total, o);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         if (lane == 0) mbar_expect_tx(&bar[buf], total);
         __syncwarp();
-        for (int r = lane; r < G::ROWS; r += 32) {
-          uintptr_t lo;
-          unsigned n;
-          row_src(r, lo, n);
-          if (n) bulk_load(dst0 + r * G::ROWB, reinterpret_cast<const void*>(lo), n, &bar[buf]);
-        }
+#pragma unroll
+        for (int i = 0; i < RPL; ++i)
+          if (nb[i]) bulk_load(dst0 + (lane + 32 * i) * G::ROWB, reinterpret_cast<const void*>(lo[i]), nb[i], &bar[buf]);
       }
     } else {
       // per-thread asynchronous element copies into the same layout (zeros
@@ -1453,20 +1459,25 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 }
 
 // ---------------------------------------------------------------------------
-// Exact test in two launches (the single-field path):
-//   refine_gather_kernel  one warp per candidate hypercube: its 2^D vertices'
-//                         values into a staging block (global memory, read
-//                         back from L2), their cull words, and the mask of
-//                         the chains whose words survive
+// Exact test in three launches:
+//   refine_gather_kernel  one lane per vertex of a candidate hypercube (32 /
+//                         2^D candidates per warp; batches: one warp per
+//                         candidate, batch_gather_kernel): the values into a
+//                         staging block (global memory, read back from L2),
+//                         quantised once for the inside tests, the vertices'
+//                         cull and sign words, and the mask of the chains
+//                         that survive them; a candidate holding a value
+//                         whose quantised form reaches 2^31 goes to a list
 //   refine_pairs_kernel   each block takes 64 candidates, lays their masks'
-//                         set bits out by a prefix count in shared memory, and
-//                         gives one thread to every (candidate, chain): the
-//                         exact SoS test, the solve, and the warp-ballot
-//                         compaction of the accepted simplices
-// No global counter is taken per candidate: the only atomics are the sink's.
-// The gather is latency-bound and light, so it runs at high occupancy; the
-// integer SoS and the solve then keep every lane busy instead of the few
-// chains of a hypercube that survive its word test.
+//                         set bits out by a prefix count in shared memory,
+//                         stages their quantised values there, and gives one
+//                         thread to every (candidate, chain): the exact inside
+//                         test, the solve, and the warp-ballot compaction of
+//                         the accepted simplices
+//   the same kernel over the listed candidates, with the 128-bit inside test
+// No global counter is taken per candidate: the only atomics are the sink's
+// and the list's.  The integer inside test and the solve keep every lane busy
+// instead of the few chains of a hypercube that survive the word tests.
 
 // Masks of vertices 1..M of chain ch, a byte each (m1 | m2 << 8 | m3 << 16);
 // 0 past the table.
@@ -1584,25 +1595,121 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
 
 constexpr int kStageVals = 48;  // 2^D * M values per candidate, D <= 4
 
+// The single-field gather with one lane per hypercube vertex: 32 / 2^D
+// candidates per warp, each lane loading its vertex's M components at once
+// and computing its cull word, sign word and quantised values in registers;
+// the chain test shuffles within the candidate's 2^D lanes.  Same staging
+// and chain masks as gather_candidate.
 template <typename T, int D>
 __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(RegularMesh mesh, FieldAccess fa,
                                                                           ExtractConfig cfg, CandidateQueue cq,
                                                                           RefineStage rs) {
-  __shared__ T cube[kRefineWarps][kStageVals];
-  __shared__ unsigned char qsg[kRefineWarps][kStageVals];
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;       // lanes per candidate
+  constexpr int CPW = 32 / NV;     // candidates per warp
+  constexpr int R = (D == 4) ? 4 : 2;  // chain rounds: ceil(chains / NV), 60 / 16 and 12 / 8
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const unsigned pk0 = chain_packed<D>(lane), pk1 = chain_packed<D>(32 + lane);
+  const int v = lane & (NV - 1), grp = lane / NV;
+  unsigned pkr[R];  // chain_packed of chains r * NV + v
+#pragma unroll
+  for (int r = 0; r < R; ++r) pkr[r] = r * NV + v < kMaxChains ? chain_packed<D>(r * NV + v) : 0u;
+  const int nch = c_chains[D - 3].n;
   pdl_enter();
   __syncthreads();
   const unsigned n = min(*cq.count, cq.cap);
   const unsigned gw = blockIdx.x * kRefineWarps + wib;
   const unsigned nw = gridDim.x * kRefineWarps;
-  for (unsigned c = gw; c < n; c += nw)
-    gather_candidate<T, D>(mesh, fa, cfg, c, cq.corner[c], cq.chains[c],
-                           static_cast<T*>(rs.vals) + (size_t)c * kStageVals, rs.q + (size_t)c * kStageVals,
-                           cube[wib], qsg[wib], band_tbl, pk0, pk1, rs, lane);
+  const unsigned lowmask = NV == 32 ? 0xFFFFFFFFu : ((1u << NV) - 1u);
+  for (unsigned base = gw * CPW; base < n; base += nw * CPW) {
+    const unsigned c = base + grp;
+    const bool has = c < n;
+    const unsigned long long pc = has ? cq.corner[c] : 0ull;
+    const unsigned long long chains = has ? cq.chains[c] : 0ull;
+    const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                            (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+    long long g[4];
+    bool in = has;
+    unsigned long long vid = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+      g[k] = (k < D) ? lk + mesh.off[k] + ((v >> k) & 1) : 0;
+      if (k < D) {
+        in &= g[k] - mesh.off[k] < mesh.ld[k];
+        vid += (unsigned long long)g[k] * mesh.gstride[k];
+      }
+    }
+    // the vertex's components: one array offset for all of them
+    long long o = 0;
+    if (!fa.per_vertex) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k < D) {
+          long long a = g[k] - fa.shift[k];
+          if (k == D - 1) a ^= fa.tflip;
+          o += a * fa.estride[k];
+        }
+    } else {
+      o = (long long)vid;
+    }
+    T val[M];
+    unsigned h[M];
+    unsigned qb = 0;
+    bool big = false;
+    T* const out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals + v * M;
+    int* const qout = rs.q + (size_t)c * kStageVals + v * M;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
+      T x = in ? src[o] : T(0);
+      if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
+      val[j] = x;
+      h[j] = hi_word<T>(x);
+      const double p = quant_p((double)x, cfg.Q);
+      const int qv = quant_small_p(p);
+      big |= qv == kQBig;
+      // strict sign of the quantised value (past 2^127 or not finite it is 0)
+      qb |= (p >= 1.0 && p < 0x1p127) ? (1u << j) : ((p <= -1.0 && p > -0x1p127) ? (8u << j) : 0u);
+      if (has) {
+        out[j] = x;
+        qout[j] = qv;
+      }
+    }
+    (void)val;
+    const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
+    const unsigned qw = in ? qb : 0x3Fu;  // absent vertices: neutral under AND
+    const bool gbig = ((__ballot_sync(0xFFFFFFFFu, big) >> (grp * NV)) & lowmask) != 0;
+    const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0, NV), q0 = __shfl_sync(0xFFFFFFFFu, qw, 0, NV);
+    unsigned long long mask = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ch = r * NV + v;
+      bool live = ch < nch && ((chains >> ch) & 1ull);
+      unsigned wacc = w0, qacc = q0;
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int srcl = (pkr[r] >> (8 * i)) & 0xFF;
+        wacc &= __shfl_sync(0xFFFFFFFFu, vw, srcl, NV);
+        qacc &= __shfl_sync(0xFFFFFFFFu, qw, srcl, NV);
+      }
+      live = live && qacc == 0 && (cfg.fiber || !word_culled(wacc));
+      mask |= (unsigned long long)((__ballot_sync(0xFFFFFFFFu, live) >> (grp * NV)) & lowmask) << (r * NV);
+    }
+    if (has && v == 0) {
+      // a candidate holding a value off the fast path: every chain on the
+      // 128-bit path (at most one list entry per candidate)
+      unsigned long long fast = mask;
+      if (gbig && mask) {
+        const unsigned slot = atomicAdd(rs.big_count, 1u);
+        rs.big_list[slot] = c;
+        rs.big_live[slot] = mask;
+        fast = 0;
+      }
+      rs.live[c] = fast;
+    }
+  }
 }
 
 // One listed simplex (candidate c, chain ch) by one thread: the exact test
@@ -2330,9 +2437,10 @@ static cudaError_t launch_refine_staged_t(const RegularMesh& mesh, const FieldAc
   const int thr = kRefineWarps * 32;
   // programmatic dependent launches: each kernel waits for its predecessor
   // at its start (pdl_enter), so its launch overlaps the predecessor's tail
-  cudaError_t e = launch_pdl(refine_gather_kernel<T, D>, num_sms * 16, thr, 0, st, mesh, fa, cfg, cq, rs);
+  cudaError_t e = launch_pdl(refine_gather_kernel<T, D>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs);
   if (!e) e = launch_pdl(refine_pairs_kernel<T, D, false>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-  if (!e) e = launch_pdl(refine_pairs_kernel<T, D, true>, num_sms * 4, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
+  // the 128-bit list is usually short or empty
+  if (!e) e = launch_pdl(refine_pairs_kernel<T, D, true>, num_sms, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
   return e ? e : cudaGetLastError();
 }
 
@@ -2399,11 +2507,11 @@ cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const 
   if (f64) {
     batch_gather_kernel<double><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
     batch_pairs_kernel<double, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
-    batch_pairs_kernel<double, true><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<double, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
   } else {
     batch_gather_kernel<float><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
     batch_pairs_kernel<float, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
-    batch_pairs_kernel<float, true><<<num_sms * 4, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_pairs_kernel<float, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
   }
   return cudaGetLastError();
 }
