@@ -699,7 +699,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->refine_vals.ensure(refine_stage_bytes(ccap, field->dtype == FTK2B_F64)));
-    CUDA_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap)));
+    CUDA_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap, cap)));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -714,9 +714,10 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cq.count = (unsigned*)ctx->counters.p + kCountCand;
     cq.cap = ccap;
     RefineStage rs;
-    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64);
+    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64, cap);
     rs.count = (unsigned*)ctx->counters.p + kCountPairs;
     rs.big_count = (unsigned*)ctx->counters.p + kCountBig;
+    rs.acc_count = (unsigned*)ctx->counters.p + kCountAcc;
     const int f64 = field->dtype == FTK2B_F64;
     // the device pipeline in two parts so that the fused cull kernel can be
     // timed on its own: [counters reset, cull] and [exact tests, canonical
@@ -737,7 +738,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e;
       if ((e = launch_refine_staged(f64, rm, fa, cfg, cq, rs, sink, ctx->num_sms, ctx->stream))) return e;
-      *nl += 3;
+      *nl += 4;
       if ((e = launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, nl))) return e;
       if (prm->classify && !cfg.fiber) {
         if ((e = launch_classify_regular(f64, rm, fa, nch, B, ctx->stream))) return e;

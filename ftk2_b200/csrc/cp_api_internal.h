@@ -33,7 +33,8 @@ enum {
   kCountItems = 5,  // batches: next cull item
   kCountPairs = 6,  // simplices the exact test ran on
   kCountBig = 7,    // candidates listed for the 128-bit inside test
-  kNumCounters = 8
+  kCountAcc = 8,    // simplices inside by the fast path (listed for the solve)
+  kNumCounters = 10
 };
 
 // Everything a regular-mesh run bakes into its kernel launches; a cached CUDA

@@ -280,7 +280,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     B_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     B_TRY(ctx, bc.cand_field.ensure(sizeof(unsigned) * (size_t)ccap));
     B_TRY(ctx, ctx->refine_vals.ensure(refine_stage_bytes(ccap, f64)));
-    B_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap)));
+    B_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap, cap)));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
     sink.key = B.key;
@@ -298,9 +298,10 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     unsigned* const counters = static_cast<unsigned*>(ctx->counters.p);
     unsigned* const dfbase = static_cast<unsigned*>(bc.fbase.p);
     RefineStage rs;
-    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, f64);
+    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, f64, cap);
     rs.count = counters + kCountPairs;
     rs.big_count = counters + kCountBig;
+    rs.acc_count = counters + kCountAcc;
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * kNumCounters, ctx->stream);
       if (!e)
@@ -311,7 +312,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     };
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = launch_batch_refine_staged(f64, dfields, cq, rs, sink, ctx->num_sms, ctx->stream);
-      *nl += 3;
+      *nl += 4;
       if (!e) e = launch_post_batch(dmeshes, dkb, (int)n, B, dfbase, ctx->stream, nl);
       if (!e)
         e = cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost,

@@ -116,11 +116,12 @@ void tile_scratch_size(const RegularMesh& mesh, size_t* stats_bytes, unsigned* r
 // chains (no cull)
 cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueue& cq, int num_sms,
                                     cudaStream_t st);
-// The exact test in three launches: a gather of each candidate's vertex
-// values, their quantised form and the mask of its surviving chains, then
-// one thread per surviving simplex of the candidates whose values all take
-// the inside tests' 64-bit fast path, then the same for the other
-// candidates (listed by the gather) with the 128-bit path.
+// The exact test in four launches: a gather of each candidate's vertex
+// values, their quantised form and the mask of its surviving chains; the
+// inside test of every surviving simplex of the candidates whose values all
+// take the 32-bit fast path, listing the simplices it accepts; the solve of
+// the listed simplices; and the whole test of the other candidates' simplices
+// (listed by the gather) with the 128-bit path.
 struct RefineStage {
   void* vals;        // 48 field values per candidate (2^D * M, D <= 4)
   int* q;            // the same 48 values quantised for the inside tests' fast path
@@ -128,18 +129,23 @@ struct RefineStage {
   unsigned long long* big_live;  // per listed candidate: chains to test on the 128-bit path
   unsigned* big_list;            // candidates listed for the 128-bit path
   unsigned* big_count;
+  unsigned long long* acc;       // simplices inside by the fast path: candidate << 8 | chain
+  unsigned* acc_count;           // may exceed acc_cap (then the call reports overflow)
+  unsigned acc_cap;
   unsigned* count;   // simplices tested (reported after the run)
 };
 // bytes of the staging buffers for `ccap` candidates: values, then quantised
-// values; the chain masks and the list
+// values; the chain masks, the inside list (acc_cap entries) and the list
 inline size_t refine_stage_bytes(size_t ccap, int f64) { return ccap * 48 * ((f64 ? 8 : 4) + 4); }
-inline size_t refine_mask_bytes(size_t ccap) { return ccap * (8 + 8 + 4); }
-inline void refine_stage_bind(RefineStage& rs, void* stage, void* masks, size_t ccap, int f64) {
+inline size_t refine_mask_bytes(size_t ccap, size_t acc_cap) { return ccap * (8 + 8 + 4) + acc_cap * 8; }
+inline void refine_stage_bind(RefineStage& rs, void* stage, void* masks, size_t ccap, int f64, unsigned acc_cap) {
   rs.vals = stage;
   rs.q = reinterpret_cast<int*>(static_cast<char*>(stage) + ccap * 48 * (f64 ? 8 : 4));
   rs.live = static_cast<unsigned long long*>(masks);
   rs.big_live = rs.live + ccap;
-  rs.big_list = reinterpret_cast<unsigned*>(rs.big_live + ccap);
+  rs.acc = rs.big_live + ccap;
+  rs.acc_cap = acc_cap;
+  rs.big_list = reinterpret_cast<unsigned*>(rs.acc + acc_cap);
 }
 cudaError_t launch_refine_staged(int f64, const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                                  const CandidateQueue& cq, const RefineStage& rs, const FeatureSink& sink, int num_sms,

@@ -563,11 +563,11 @@ static int grid_for(unsigned cap, int threads, int max_blocks) {
 //      keys of its bucket below it (the keys of one extraction are
 //      distinct); the packed keys land in key_alt in canonical order.
 //   2. star edges, one block of 1024 threads per SM: every block copies the
-//      sorted keys into shared memory, writes the outputs of positions p with
-//      p mod gridDim == blockIdx, and its warps find the star edges of the
+//      sorted keys into shared memory, its warps find the star edges of the
 //      sorted features (one warp per feature) in the sorted keys and join
 //      each feature with its linked faces in a lock-free union-find (parents
-//      initialised by the sort).
+//      initialised by the sort); then each block writes the outputs of its
+//      contiguous share of positions.
 //   3. one block: exclusive scan of the edge counts, edge compaction, and
 //      every feature's root (the union-find's parents copied to shared
 //      memory): track ids and root count.
@@ -826,19 +826,22 @@ __global__ void __launch_bounds__(kSortThreads, 1)
   pdl_enter();
   const unsigned n = min(*B.count, B.cap);
   const unsigned G = gridDim.x;
-  for (unsigned p = threadIdx.x; p < n; p += kSortThreads) {
-    const unsigned long long v = B.key_alt[p];
-    sk[p] = v >> kIdxBits;
-    if (p % G == blockIdx.x)
-      write_sorted_feature(mesh, nch, B, (unsigned)(v & ((1ull << kIdxBits) - 1)), p, v >> kIdxBits);
+  if (want_edges) {
+    for (unsigned p = threadIdx.x; p < n; p += kSortThreads) sk[p] = B.key_alt[p] >> kIdxBits;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const unsigned gw = (blockIdx.x * kSortThreads + threadIdx.x) >> 5;
+    const unsigned nw = (G * kSortThreads) >> 5;
+    for (unsigned i = gw; i < n; i += nw)
+      star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots, B.parent, B.err);
   }
-  if (!want_edges) return;
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const unsigned gw = (blockIdx.x * kSortThreads + threadIdx.x) >> 5;
-  const unsigned nw = (G * kSortThreads) >> 5;
-  for (unsigned i = gw; i < n; i += nw)
-    star_edges_warp(mesh, nch, sk, n, i, sk[i], 0ull, T, lane, B.edge_cnt, B.edge_slots, B.parent, B.err);
+  // the outputs of the block's contiguous share of positions (few warps,
+  // converged)
+  const unsigned share = (n + G - 1) / G, p0 = min(blockIdx.x * share, n), p1 = min(p0 + share, n);
+  for (unsigned p = p0 + threadIdx.x; p < p1; p += kSortThreads) {
+    const unsigned long long v = B.key_alt[p];
+    write_sorted_feature(mesh, nch, B, (unsigned)(v & ((1ull << kIdxBits) - 1)), p, v >> kIdxBits);
+  }
 }
 
 __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {

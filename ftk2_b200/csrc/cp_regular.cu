@@ -1465,8 +1465,8 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 //                         candidate, batch_gather_kernel): the values into a
 //                         staging block (global memory, read back from L2),
 //                         quantised once for the inside tests, the vertices'
-//                         cull and sign words, and the mask of the chains
-//                         that survive them; a candidate holding a value
+//                         cull words, and the mask of the chains that
+//                         survive them; a candidate holding a value
 //                         whose quantised form reaches 2^31 goes to a list
 //   refine_pairs_kernel   each block takes 64 candidates, lays their masks'
 //                         set bits out by a prefix count in shared memory,
@@ -1491,19 +1491,19 @@ __device__ __forceinline__ unsigned chain_packed(int ch) {
 // inside tests into `qout`, its vertex words, and the mask of its surviving
 // chains into rs.live[c] (or, when a value is off the fast path, into the
 // 128-bit list).  pk0 / pk1: chain_packed of chains lane and 32 + lane;
-// qsg: the warp's kStageVals bytes of shared memory.
 //
 // A chain survives when its vertices' cull words do not prove that the solve
-// rejects it and when no component has quantised values of one strict sign
-// at all its vertices: q_j >= 1 everywhere (or <= -1) puts the origin at
-// least 1/2 away from the simplex's image in the lattice, so the inside test
-// (a symbolic perturbation of that image) answers "outside".
+// rejects it.  (A test on the signs of the quantised values alone would not
+// do: when the quantised vertices and the origin are coplanar, the inside
+// test's fallback levels, which perturb by matrix row rather than by vertex,
+// can answer "inside" for a simplex whose quantised values keep one strict
+// sign, and the solve then decides.)
 template <typename T, int D>
 __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const FieldAccess& fa,
                                                  const ExtractConfig& cfg, unsigned c, unsigned long long pc,
                                                  unsigned long long chains, T* out, int* qout, T* my,
-                                                 unsigned char* qsg, const unsigned* band_tbl, unsigned pk0,
-                                                 unsigned pk1, const RefineStage& rs, int lane) {
+                                                 const unsigned* band_tbl, unsigned pk0, unsigned pk1,
+                                                 const RefineStage& rs, int lane) {
   constexpr int M = D - 1;
   constexpr int NV = 1 << D;
   const int nch = c_chains[D - 3].n;
@@ -1533,34 +1533,23 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     if (cfg.fiber) val = fp<T>::sub(val, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
     my[e] = val;
     out[e] = val;
-    const double p = quant_p((double)val, cfg.Q);
-    const int qv = quant_small_p(p);
+    const int qv = quant_small_p(quant_p((double)val, cfg.Q));
     qout[e] = qv;
     anybig |= qv == kQBig;
-    // strict sign of the quantised value (a value past 2^127 or not finite
-    // quantises to 0 in the reference's conversion)
-    qsg[e] = (unsigned char)((p >= 1.0 && p < 0x1p127) ? (1u << j) : ((p <= -1.0 && p > -0x1p127) ? (8u << j) : 0u));
   }
   const bool big = __any_sync(0xFFFFFFFFu, anybig);
   __syncwarp();
-  unsigned vw = kAbsent, qw = 0x3Fu;  // absent vertices: neutral under AND
+  unsigned vw = kAbsent;  // absent vertices: neutral under AND
   if (lane < NV) {
     unsigned h[M];
-    unsigned qb = 0;
 #pragma unroll
-    for (int j = 0; j < M; ++j) {
-      h[j] = hi_word<T>(my[lane * M + j]);
-      qb |= qsg[lane * M + j];
-    }
+    for (int j = 0; j < M; ++j) h[j] = hi_word<T>(my[lane * M + j]);
     bool in = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
-    if (in) {
-      vw = vertex_word_hi<T, M>(h, band_tbl);
-      qw = qb;
-    }
+    if (in) vw = vertex_word_hi<T, M>(h, band_tbl);
   }
-  const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0), q0 = __shfl_sync(0xFFFFFFFFu, qw, 0);
+  const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0);
   unsigned long long mask = 0;
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
@@ -1568,14 +1557,10 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
     const int ch = half * 32 + lane;
     const unsigned pk = half ? pk1 : pk0;
     bool live = ch < nch && ((chains >> ch) & 1ull);
-    unsigned wacc = w0, qacc = q0;
+    unsigned wacc = w0;
 #pragma unroll
-    for (int i = 0; i < M; ++i) {
-      const int src = (pk >> (8 * i)) & 0xFF;
-      wacc &= __shfl_sync(0xFFFFFFFFu, vw, src);
-      qacc &= __shfl_sync(0xFFFFFFFFu, qw, src);
-    }
-    live = live && qacc == 0 && (cfg.fiber || !word_culled(wacc));
+    for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pk >> (8 * i)) & 0xFF);
+    live = live && (cfg.fiber || !word_culled(wacc));
     mask |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, live) << (half * 32);
   }
   if (lane == 0) {
@@ -1597,7 +1582,7 @@ constexpr int kStageVals = 48;  // 2^D * M values per candidate, D <= 4
 
 // The single-field gather with one lane per hypercube vertex: 32 / 2^D
 // candidates per warp, each lane loading its vertex's M components at once
-// and computing its cull word, sign word and quantised values in registers;
+// and computing its cull word and quantised values in registers;
 // the chain test shuffles within the candidate's 2^D lanes.  Same staging
 // and chain masks as gather_candidate.
 template <typename T, int D>
@@ -1654,9 +1639,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
     } else {
       o = (long long)vid;
     }
-    T val[M];
     unsigned h[M];
-    unsigned qb = 0;
     bool big = false;
     T* const out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals + v * M;
     int* const qout = rs.q + (size_t)c * kStageVals + v * M;
@@ -1665,36 +1648,26 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
       const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
       T x = in ? src[o] : T(0);
       if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
-      val[j] = x;
       h[j] = hi_word<T>(x);
-      const double p = quant_p((double)x, cfg.Q);
-      const int qv = quant_small_p(p);
+      const int qv = quant_small_p(quant_p((double)x, cfg.Q));
       big |= qv == kQBig;
-      // strict sign of the quantised value (past 2^127 or not finite it is 0)
-      qb |= (p >= 1.0 && p < 0x1p127) ? (1u << j) : ((p <= -1.0 && p > -0x1p127) ? (8u << j) : 0u);
       if (has) {
         out[j] = x;
         qout[j] = qv;
       }
     }
-    (void)val;
-    const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;
-    const unsigned qw = in ? qb : 0x3Fu;  // absent vertices: neutral under AND
+    const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;  // absent: neutral under AND
     const bool gbig = ((__ballot_sync(0xFFFFFFFFu, big) >> (grp * NV)) & lowmask) != 0;
-    const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0, NV), q0 = __shfl_sync(0xFFFFFFFFu, qw, 0, NV);
+    const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0, NV);
     unsigned long long mask = 0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int ch = r * NV + v;
       bool live = ch < nch && ((chains >> ch) & 1ull);
-      unsigned wacc = w0, qacc = q0;
+      unsigned wacc = w0;
 #pragma unroll
-      for (int i = 0; i < M; ++i) {
-        const int srcl = (pkr[r] >> (8 * i)) & 0xFF;
-        wacc &= __shfl_sync(0xFFFFFFFFu, vw, srcl, NV);
-        qacc &= __shfl_sync(0xFFFFFFFFu, qw, srcl, NV);
-      }
-      live = live && qacc == 0 && (cfg.fiber || !word_culled(wacc));
+      for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pkr[r] >> (8 * i)) & 0xFF, NV);
+      live = live && (cfg.fiber || !word_culled(wacc));
       mask |= (unsigned long long)((__ballot_sync(0xFFFFFFFFu, live) >> (grp * NV)) & lowmask) << (r * NV);
     }
     if (has && v == 0) {
@@ -1712,18 +1685,36 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(Regula
   }
 }
 
-// One listed simplex (candidate c, chain ch) by one thread: the exact test
-// and, when accepted, its canonical key and reported values.  src / qsrc:
-// the candidate's staged and quantised values; chain_pk: chain_packed of
-// every chain of the mesh's dimension.  BIG = false: every value of the
-// candidate takes the 64-bit fast path of the inside test (its quantised
-// form decides); BIG = true: the inside test from the field values.
+// The fast-path inside test of listed simplex (candidate, chain ch) from the
+// candidate's quantised values qsrc; chain_pk: chain_packed of every chain of
+// the mesh's dimension.
+template <int D>
+__device__ __forceinline__ bool inside_pair_q(int ch, const int* qsrc, const unsigned* chain_pk) {
+  constexpr int M = D - 1;
+  int mk[M + 1];
+  mk[0] = 0;
+  const unsigned pk = chain_pk[ch];
+#pragma unroll
+  for (int k = 0; k < M; ++k) mk[k + 1] = (pk >> (8 * k)) & 0xFF;
+  int q[M + 1][M];
+#pragma unroll
+  for (int k = 0; k <= M; ++k)
+#pragma unroll
+    for (int j = 0; j < M; ++j) q[k][j] = qsrc[mk[k] * M + j];
+  if constexpr (M == 2) return sos_inside2_q(q);
+  else return sos_inside3_q(q);
+}
+
+// Listed simplex (candidate, chain ch) by one thread: BIG = true, the whole
+// exact test (inside test from the field values, 128-bit quantisation);
+// BIG = false, a simplex the fast-path inside test accepted.  Then the solve
+// and, when accepted, its canonical key and reported values.  src: the
+// candidate's staged values.
 template <typename T, int D, bool BIG>
 __device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
-                                          unsigned long long pc, int ch, const T* src, const int* qsrc,
-                                          const unsigned* chain_pk, unsigned long long key_base,
-                                          unsigned long long& key, double lam_out[4], float bary_out[4],
-                                          float& sc_out) {
+                                          unsigned long long pc, int ch, const T* src, const unsigned* chain_pk,
+                                          unsigned long long key_base, unsigned long long& key, double lam_out[4],
+                                          float bary_out[4], float& sc_out) {
   constexpr int M = D - 1;
   const ChainTable& CT = c_chains[D - 3];
   int mk[M + 1];
@@ -1731,17 +1722,6 @@ __device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAc
   const unsigned pk = chain_pk[ch];
 #pragma unroll
   for (int k = 0; k < M; ++k) mk[k + 1] = (pk >> (8 * k)) & 0xFF;
-  if constexpr (!BIG) {
-    int q[M + 1][M];
-#pragma unroll
-    for (int k = 0; k <= M; ++k)
-#pragma unroll
-      for (int j = 0; j < M; ++j) q[k][j] = qsrc[mk[k] * M + j];
-    bool inside;
-    if constexpr (M == 2) inside = sos_inside2_q(q);
-    else inside = sos_inside3_q(q);
-    if (!inside) return false;
-  }
   T vals[M + 1][M];
 #pragma unroll
   for (int k = 0; k <= M; ++k)
@@ -1827,11 +1807,12 @@ __device__ __forceinline__ void sink_write(const FeatureSink& sink, bool acc, un
 
 constexpr int kPairCands = 64;  // candidates a block of the exact-test launch takes at a time
 
-// The block's next kPairCands entries of `live` from `first`: masks and the
-// prefix counts of their set bits in shared memory; returns the number of
-// simplices.
+// The block's next kPairCands entries of `live` from `first` laid out as a
+// list of (slot, chain) pairs in shared memory (slot << 6 | chain), by a
+// prefix count of the masks' set bits; returns the number of simplices.
+// Shared: msk[kPairCands], off[kPairCands + 1], plist[kPairCands * 64].
 __device__ __forceinline__ unsigned pairs_layout(const unsigned long long* live, unsigned first, unsigned n,
-                                                 unsigned long long* msk, unsigned* off) {
+                                                 unsigned long long* msk, unsigned* off, unsigned short* plist) {
   const int t = threadIdx.x;
   if (t < kPairCands) {
     const unsigned c = first + t;
@@ -1852,44 +1833,48 @@ __device__ __forceinline__ unsigned pairs_layout(const unsigned long long* live,
     if (t == 31) off[kPairCands] = incl;
   }
   __syncthreads();
+  if (t < kPairCands) {
+    unsigned o = off[t];
+    for (unsigned long long m = msk[t]; m; m &= m - 1) plist[o++] = (unsigned short)((t << 6) | (__ffsll(m) - 1));
+  }
+  __syncthreads();
   return off[kPairCands];
 }
 
-// simplex p of the block's layout: its candidate slot k and chain
-__device__ __forceinline__ void pairs_locate(unsigned p, const unsigned long long* msk, const unsigned* off, int& k,
-                                             int& ch) {
-  int lo = 0, hi = kPairCands;  // the last k with off[k] <= p
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= p) lo = mid;
-    else hi = mid;
-  }
-  k = lo;
-  const unsigned r = p - off[k];
-  const unsigned long long m = msk[k];
-  const unsigned lo32 = (unsigned)m, nlo = __popc(lo32);
-  ch = r < nlo ? (int)__fns(lo32, 0, (int)r + 1) : 32 + (int)__fns((unsigned)(m >> 32), 0, (int)(r - nlo) + 1);
-}
-
-// BIG = false: the candidates of rs.live; true: those the gather listed for
-// the 128-bit path
 // The quantised values of the block's next kPairCands candidates (from
-// `first`, contiguous in rs.q) into shared memory, 16 bytes per copy.
+// `first`, contiguous in rs.q) into shared memory, 16 bytes per copy (made
+// visible by the layout's barriers).
 __device__ __forceinline__ void stage_quantised(const RefineStage& rs, unsigned first, unsigned n, int* sq) {
   const unsigned nk = min(n - first, (unsigned)kPairCands);
   const int4* src = reinterpret_cast<const int4*>(rs.q + (size_t)first * kStageVals);
   int4* dst = reinterpret_cast<int4*>(sq);
   for (unsigned e = threadIdx.x; e < nk * (kStageVals / 4); e += blockDim.x) dst[e] = src[e];
-  __syncthreads();
 }
 
+// warp-aggregated append of (candidate << 8 | chain) to the inside list
+__device__ __forceinline__ void acc_append(const RefineStage& rs, bool in, unsigned c, int ch, int lane) {
+  const unsigned ball = __ballot_sync(0xFFFFFFFFu, in);
+  if (!ball) return;
+  const int leader = __ffs(ball) - 1;
+  unsigned b0 = 0;
+  if (lane == leader) b0 = atomicAdd(rs.acc_count, (unsigned)__popc(ball));
+  b0 = __shfl_sync(0xFFFFFFFFu, b0, leader);
+  if (!in) return;
+  const unsigned idx = b0 + __popc(ball & ((1u << lane) - 1u));
+  if (idx < rs.acc_cap) rs.acc[idx] = ((unsigned long long)c << 8) | (unsigned)ch;
+}
+
+// BIG = false: the fast-path inside test of every surviving simplex of the
+// candidates of rs.live, listing the accepted ones; BIG = true: the whole
+// test of the candidates the gather listed for the 128-bit path.
 template <typename T, int D, bool BIG>
-__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
+__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 4) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
                                                                                    ExtractConfig cfg, CandidateQueue cq,
                                                                                    RefineStage rs, FeatureSink sink) {
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
   __shared__ unsigned chain_pk[kMaxChains];
+  __shared__ unsigned short plist[kPairCands * 64];
   __shared__ __align__(16) int sq[BIG ? 4 : kPairCands * kStageVals];  // the fast path's quantised values
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
   pdl_enter();
@@ -1897,27 +1882,66 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) refine_pairs_k
   const unsigned n = BIG ? *rs.big_count : min(*cq.count, cq.cap);
   const unsigned long long* live = BIG ? rs.big_live : rs.live;
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
-    const unsigned P = pairs_layout(live, first, n, msk, off);
-    if (threadIdx.x == 0) atomicAdd(rs.count, P);
     if constexpr (!BIG) stage_quantised(rs, first, n, sq);
+    const unsigned P = pairs_layout(live, first, n, msk, off, plist);
+    if (threadIdx.x == 0) atomicAdd(rs.count, P);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
-      bool acc = false;
-      double lam_out[4] = {0, 0, 0, 0};
-      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-      float sc_out = 0.f;
-      unsigned long long key = 0;
-      if (p < P) {
-        int k, ch;
-        pairs_locate(p, msk, off, k, ch);
-        const unsigned c = BIG ? rs.big_list[first + k] : first + k;
-        acc = test_pair<T, D, BIG>(mesh, fa, cfg, cq.corner[c], ch,
-                                   static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, sq + k * kStageVals,
-                                   chain_pk, 0ull, key, lam_out, bary_out, sc_out);
+      const unsigned e = p < P ? plist[p] : 0u;
+      const int k = (int)(e >> 6), ch = (int)(e & 63);
+      if constexpr (!BIG) {
+        const bool in = p < P && inside_pair_q<D>(ch, sq + k * kStageVals, chain_pk);
+        acc_append(rs, in, first + k, ch, lane);
+      } else {
+        bool acc = false;
+        double lam_out[4] = {0, 0, 0, 0};
+        float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+        float sc_out = 0.f;
+        unsigned long long key = 0;
+        if (p < P) {
+          const unsigned c = rs.big_list[first + k];
+          acc = test_pair<T, D, true>(mesh, fa, cfg, cq.corner[c], ch,
+                                      static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, chain_pk, 0ull, key,
+                                      lam_out, bary_out, sc_out);
+        }
+        sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
       }
-      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
     __syncthreads();  // the layout is rebuilt for the next candidates
+  }
+}
+
+// The solve of every simplex on the inside list, one thread each.  A list
+// longer than its capacity raises the sink count past the sink's capacity,
+// so that the call reports overflow and runs again with larger buffers.
+template <typename T, int D>
+__global__ void __launch_bounds__(kRefineWarps * 32) refine_solve_kernel(RegularMesh mesh, FieldAccess fa,
+                                                                         ExtractConfig cfg, CandidateQueue cq,
+                                                                         RefineStage rs, FeatureSink sink) {
+  __shared__ unsigned chain_pk[kMaxChains];
+  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
+  pdl_enter();
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned na = *rs.acc_count;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && na > rs.acc_cap) atomicMax(sink.count, na);
+  const unsigned n = min(na, rs.acc_cap);
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool acc = false;
+    double lam_out[4] = {0, 0, 0, 0};
+    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+    float sc_out = 0.f;
+    unsigned long long key = 0;
+    if (i < n) {
+      const unsigned long long e = rs.acc[i];
+      const unsigned c = (unsigned)(e >> 8);
+      acc = test_pair<T, D, false>(mesh, fa, cfg, cq.corner[c], (int)(e & 255),
+                                   static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, chain_pk, 0ull, key,
+                                   lam_out, bary_out, sc_out);
+    }
+    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
   }
 }
 
@@ -1926,7 +1950,6 @@ template <typename T>
 __global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const BatchField* __restrict__ fields,
                                                                          CandidateQueue cq, RefineStage rs) {
   __shared__ T cube[kRefineWarps][kStageVals];
-  __shared__ unsigned char qsg[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   __syncthreads();
@@ -1941,21 +1964,22 @@ __global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const B
     T* out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals;
     int* qout = rs.q + (size_t)c * kStageVals;
     if (F.mesh.d == 4)
-      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], qsg[wib],
-                             band_tbl, pk40, pk41, rs, lane);
+      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
+                             pk40, pk41, rs, lane);
     else
-      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], qsg[wib],
-                             band_tbl, pk3, 0u, rs, lane);
+      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
+                             pk3, 0u, rs, lane);
   }
 }
 
 template <typename T, bool BIG>
-__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) batch_pairs_kernel(const BatchField* __restrict__ fields,
+__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 4) batch_pairs_kernel(const BatchField* __restrict__ fields,
                                                                                   CandidateQueue cq, RefineStage rs,
                                                                                   FeatureSink sink) {
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
   __shared__ unsigned chain_pk[2][kMaxChains];
+  __shared__ unsigned short plist[kPairCands * 64];
   __shared__ __align__(16) int sq[BIG ? 4 : kPairCands * kStageVals];
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
     chain_pk[0][i] = chain_packed<3>(i);
@@ -1965,33 +1989,81 @@ __global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 3) batch_pairs_ke
   const unsigned n = BIG ? *rs.big_count : min(*cq.count, cq.cap);
   const unsigned long long* live = BIG ? rs.big_live : rs.live;
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
-    const unsigned P = pairs_layout(live, first, n, msk, off);
-    if (threadIdx.x == 0) atomicAdd(rs.count, P);
     if constexpr (!BIG) stage_quantised(rs, first, n, sq);
+    const unsigned P = pairs_layout(live, first, n, msk, off, plist);
+    if (threadIdx.x == 0) atomicAdd(rs.count, P);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
-      bool acc = false;
-      double lam_out[4] = {0, 0, 0, 0};
-      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-      float sc_out = 0.f;
-      unsigned long long key = 0;
-      if (p < P) {
-        int k, ch;
-        pairs_locate(p, msk, off, k, ch);
-        const unsigned c = BIG ? rs.big_list[first + k] : first + k;
-        const BatchField& F = fields[cq.field[c]];
-        const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
-        const int* qsrc = sq + k * kStageVals;
-        if (F.mesh.d == 4)
-          acc = test_pair<T, 4, BIG>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, qsrc, chain_pk[1], F.key_base, key,
-                                     lam_out, bary_out, sc_out);
-        else
-          acc = test_pair<T, 3, BIG>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, qsrc, chain_pk[0], F.key_base, key,
-                                     lam_out, bary_out, sc_out);
+      const unsigned e = p < P ? plist[p] : 0u;
+      const int k = (int)(e >> 6), ch = (int)(e & 63);
+      if constexpr (!BIG) {
+        bool in = false;
+        if (p < P) {
+          const int* qsrc = sq + k * kStageVals;
+          in = fields[cq.field[first + k]].mesh.d == 4 ? inside_pair_q<4>(ch, qsrc, chain_pk[1])
+                                                       : inside_pair_q<3>(ch, qsrc, chain_pk[0]);
+        }
+        acc_append(rs, in, first + k, ch, lane);
+      } else {
+        bool acc = false;
+        double lam_out[4] = {0, 0, 0, 0};
+        float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+        float sc_out = 0.f;
+        unsigned long long key = 0;
+        if (p < P) {
+          const unsigned c = rs.big_list[first + k];
+          const BatchField& F = fields[cq.field[c]];
+          const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
+          if (F.mesh.d == 4)
+            acc = test_pair<T, 4, true>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[1], F.key_base, key,
+                                        lam_out, bary_out, sc_out);
+          else
+            acc = test_pair<T, 3, true>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[0], F.key_base, key,
+                                        lam_out, bary_out, sc_out);
+        }
+        sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
       }
-      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
     __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRefineWarps * 32) batch_solve_kernel(const BatchField* __restrict__ fields,
+                                                                        CandidateQueue cq, RefineStage rs,
+                                                                        FeatureSink sink) {
+  __shared__ unsigned chain_pk[2][kMaxChains];
+  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
+    chain_pk[0][i] = chain_packed<3>(i);
+    chain_pk[1][i] = chain_packed<4>(i);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned na = *rs.acc_count;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && na > rs.acc_cap) atomicMax(sink.count, na);
+  const unsigned n = min(na, rs.acc_cap);
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool acc = false;
+    double lam_out[4] = {0, 0, 0, 0};
+    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+    float sc_out = 0.f;
+    unsigned long long key = 0;
+    if (i < n) {
+      const unsigned long long e = rs.acc[i];
+      const unsigned c = (unsigned)(e >> 8);
+      const int ch = (int)(e & 255);
+      const BatchField& F = fields[cq.field[c]];
+      const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
+      if (F.mesh.d == 4)
+        acc = test_pair<T, 4, false>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[1], F.key_base, key,
+                                     lam_out, bary_out, sc_out);
+      else
+        acc = test_pair<T, 3, false>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[0], F.key_base, key,
+                                     lam_out, bary_out, sc_out);
+    }
+    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
   }
 }
 
@@ -2439,6 +2511,7 @@ static cudaError_t launch_refine_staged_t(const RegularMesh& mesh, const FieldAc
   // at its start (pdl_enter), so its launch overlaps the predecessor's tail
   cudaError_t e = launch_pdl(refine_gather_kernel<T, D>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs);
   if (!e) e = launch_pdl(refine_pairs_kernel<T, D, false>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
+  if (!e) e = launch_pdl(refine_solve_kernel<T, D>, num_sms * 2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
   // the 128-bit list is usually short or empty
   if (!e) e = launch_pdl(refine_pairs_kernel<T, D, true>, num_sms, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
   return e ? e : cudaGetLastError();
@@ -2507,10 +2580,12 @@ cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const 
   if (f64) {
     batch_gather_kernel<double><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
     batch_pairs_kernel<double, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_solve_kernel<double><<<num_sms * 2, thr, 0, st>>>(fields, cq, rs, sink);
     batch_pairs_kernel<double, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
   } else {
     batch_gather_kernel<float><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
     batch_pairs_kernel<float, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
+    batch_solve_kernel<float><<<num_sms * 2, thr, 0, st>>>(fields, cq, rs, sink);
     batch_pairs_kernel<float, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
   }
   return cudaGetLastError();
