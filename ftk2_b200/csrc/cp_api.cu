@@ -512,6 +512,7 @@ PostBuffers ftk2b_ctx::post_buffers(unsigned cap_, unsigned edge_cap_, int key_b
   B.n_edges = c + kCountEdges;
   B.n_roots = c + kCountRoots;
   B.err = c + kCountErr;
+  B.done = c + kCountDone;
   B.key_alt = (unsigned long long*)key_alt.p;
   B.perm0 = (unsigned*)perm0.p;
   B.perm1 = (unsigned*)perm1.p;
@@ -698,7 +699,6 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     if (st) return st;
     CUDA_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     CUDA_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
-    CUDA_TRY(ctx, ctx->refine_vals.ensure(refine_stage_bytes(ccap, field->dtype == FTK2B_F64)));
     CUDA_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap, cap)));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
@@ -714,7 +714,9 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     cq.count = (unsigned*)ctx->counters.p + kCountCand;
     cq.cap = ccap;
     RefineStage rs;
-    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64, cap);
+    // the single-field test keeps values and quantised values in shared
+    // memory and reads the field again for the solve: no staging block
+    refine_stage_bind(rs, nullptr, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64, cap);
     rs.count = (unsigned*)ctx->counters.p + kCountPairs;
     rs.big_count = (unsigned*)ctx->counters.p + kCountBig;
     rs.acc_count = (unsigned*)ctx->counters.p + kCountAcc;
@@ -738,7 +740,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e;
       if ((e = launch_refine_staged(f64, rm, fa, cfg, cq, rs, sink, ctx->num_sms, ctx->stream))) return e;
-      *nl += 4;
+      *nl += 2;
       if ((e = launch_post_regular(rm, nch, B, prm->want_edges, ctx->stream, nl))) return e;
       if (prm->classify && !cfg.fiber) {
         if ((e = launch_classify_regular(f64, rm, fa, nch, B, ctx->stream))) return e;

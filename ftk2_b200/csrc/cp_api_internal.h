@@ -34,6 +34,7 @@ enum {
   kCountPairs = 6,  // simplices the exact test ran on
   kCountBig = 7,    // candidates listed for the 128-bit inside test
   kCountAcc = 8,    // simplices inside by the fast path (listed for the solve)
+  kCountDone = 9,   // blocks of the short chain's edge kernel that finished
   kNumCounters = 10
 };
 

@@ -116,12 +116,13 @@ void tile_scratch_size(const RegularMesh& mesh, size_t* stats_bytes, unsigned* r
 // chains (no cull)
 cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueue& cq, int num_sms,
                                     cudaStream_t st);
-// The exact test in four launches: a gather of each candidate's vertex
-// values, their quantised form and the mask of its surviving chains; the
-// inside test of every surviving simplex of the candidates whose values all
-// take the 32-bit fast path, listing the simplices it accepts; the solve of
-// the listed simplices; and the whole test of the other candidates' simplices
-// (listed by the gather) with the 128-bit path.
+// The exact test of the queued candidates: the fast-path inside test of
+// every surviving simplex of the candidates whose quantised values all stay
+// below 2^31, listing the simplices it accepts; the solve of the listed
+// simplices; and the whole test of the other candidates' simplices (listed)
+// with the 128-bit path.  Batches stage each candidate's values and their
+// quantised form in global memory between the launches (vals, q); the
+// single-field path keeps them in shared memory (vals = q = null).
 struct RefineStage {
   void* vals;        // 48 field values per candidate (2^D * M, D <= 4)
   int* q;            // the same 48 values quantised for the inside tests' fast path
@@ -140,7 +141,7 @@ inline size_t refine_stage_bytes(size_t ccap, int f64) { return ccap * 48 * ((f6
 inline size_t refine_mask_bytes(size_t ccap, size_t acc_cap) { return ccap * (8 + 8 + 4) + acc_cap * 8; }
 inline void refine_stage_bind(RefineStage& rs, void* stage, void* masks, size_t ccap, int f64, unsigned acc_cap) {
   rs.vals = stage;
-  rs.q = reinterpret_cast<int*>(static_cast<char*>(stage) + ccap * 48 * (f64 ? 8 : 4));
+  rs.q = stage ? reinterpret_cast<int*>(static_cast<char*>(stage) + ccap * 48 * (f64 ? 8 : 4)) : nullptr;
   rs.live = static_cast<unsigned long long*>(masks);
   rs.big_live = rs.live + ccap;
   rs.acc = rs.big_live + ccap;

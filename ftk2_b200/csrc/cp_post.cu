@@ -556,7 +556,7 @@ static int grid_for(unsigned cap, int threads, int max_blocks) {
 
 // ---------------------------------------------------------------------------
 // Post-extraction for small feature counts (capacity <= kSmallPostCap, keys
-// below 2^50): the outputs of the general chain above in three launches.
+// below 2^50): the outputs of the general chain above in two launches.
 //   1. sort, one block: a counting sort of the keys (each packed with its
 //      feature index in the low kIdxBits bits) by their top bits in shared
 //      memory, then each key's canonical position = its bucket's start + the
@@ -567,8 +567,8 @@ static int grid_for(unsigned cap, int threads, int max_blocks) {
 //      sorted features (one warp per feature) in the sorted keys and join
 //      each feature with its linked faces in a lock-free union-find (parents
 //      initialised by the sort); then each block writes the outputs of its
-//      contiguous share of positions.
-//   3. one block: exclusive scan of the edge counts, edge compaction, and
+//      contiguous share of positions, and the last block to finish runs the
+//      final step: exclusive scan of the edge counts, edge compaction, and
 //      every feature's root (the union-find's parents copied to shared
 //      memory): track ids and root count.
 
@@ -818,6 +818,8 @@ __device__ __forceinline__ void write_sorted_feature(const RegularMesh& mesh, in
   expand_feature(mesh, nch, key, pos, mesh.d, B.bary4_sorted, B.simplices, B.bary);
 }
 
+__device__ __forceinline__ void finish_block(const PostBuffers& B, unsigned* sh, unsigned* wsum, unsigned& s_roots);
+
 __global__ void __launch_bounds__(kSortThreads, 1)
     small_edges_kernel(RegularMesh mesh, int nch, PostBuffers B, int want_edges) {
   extern __shared__ unsigned long long sk[];  // the n sorted keys
@@ -842,13 +844,26 @@ __global__ void __launch_bounds__(kSortThreads, 1)
     const unsigned long long v = B.key_alt[p];
     write_sorted_feature(mesh, nch, B, (unsigned)(v & ((1ull << kIdxBits) - 1)), p, v >> kIdxBits);
   }
+  if (!want_edges) return;
+  // the last block to finish runs the final step: every block's edge
+  // counts, slots and union-find hooks are visible to it (each block fences
+  // its writes before counting itself done)
+  __shared__ unsigned s_last, s_roots;
+  __shared__ unsigned wsum[33];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(B.done, 1u) == G - 1 ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  finish_block(B, reinterpret_cast<unsigned*>(sk), wsum, s_roots);
 }
 
-__global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
-  pdl_enter();
-  extern __shared__ unsigned sh[];  // edge offsets of the n features (n + 1), then their union-find parents
-  __shared__ unsigned wsum[33];
-  __shared__ unsigned s_roots;
+// The short chain's last step, by one block of 1024 threads: exclusive scan
+// of the edge counts, edge compaction, every feature's root from the union-find
+// parents (copied to shared memory), track ids and root count.  sh: (2n + 1)
+// words of shared memory.
+__device__ __forceinline__ void finish_block(const PostBuffers& B, unsigned* sh, unsigned* wsum, unsigned& s_roots) {
   constexpr int kPer = (int)(kSmallPostCap / 1024);  // features per thread, at most
   const unsigned n = min(*B.count, B.cap);
   unsigned* const off = sh;
@@ -862,7 +877,7 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
   unsigned sum = 0;
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
-    c[k] = (k < (int)seg && s0 + k < n) ? B.edge_cnt[s0 + k] : 0u;
+    c[k] = (k < (int)seg && s0 + k < n) ? __ldcg(&B.edge_cnt[s0 + k]) : 0u;
     sum += c[k];
   }
   // the edge kernel's union-find is complete: its parents into shared memory
@@ -890,7 +905,7 @@ __global__ void __launch_bounds__(1024, 1) small_finish_kernel(PostBuffers B) {
       if (off[mid] <= e) lo = mid;
       else hi = mid;
     }
-    const unsigned other = B.edge_slots[(size_t)lo * kEdgeSlots + (e - off[lo])];
+    const unsigned other = __ldcg(&B.edge_slots[(size_t)lo * kEdgeSlots + (e - off[lo])]);
     if (e < B.edge_cap) {
       B.edges[2 * (size_t)e] = lo;
       B.edges[2 * (size_t)e + 1] = other;
@@ -916,19 +931,17 @@ static cudaError_t launch_post_small(const RegularMesh& mesh, int nch, const Pos
                                      cudaStream_t st, unsigned long long* launches) {
   const unsigned cap = B.cap;
   const size_t key_smem = sizeof(unsigned long long) * (size_t)(cap ? cap : 1);
+  // the edge kernel's last block reuses the keys' shared memory for the
+  // final step's 2n + 1 words
+  const size_t edge_smem = key_smem + 16;
   const int g = B.num_sms > 0 ? B.num_sms : 148;
   cudaError_t e = cudaFuncSetAttribute(small_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
   if (!e) e = launch_pdl(small_sort_kernel, 1, kSortThreads, key_smem, st, B);
-  if (!e) e = cudaFuncSetAttribute(small_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)key_smem);
-  if (!e) e = launch_pdl(small_edges_kernel, g, kSortThreads, key_smem, st, mesh, nch, B, want_edges);
+  if (!e) e = cudaFuncSetAttribute(small_edges_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)edge_smem);
+  if (!e) e = launch_pdl(small_edges_kernel, g, kSortThreads, edge_smem, st, mesh, nch, B, want_edges);
   if (e) return e;
   *launches += 2;
-  if (!want_edges) return cudaGetLastError();
-  const size_t uf_smem = sizeof(unsigned) * (2 * (size_t)cap + 1);
-  e = cudaFuncSetAttribute(small_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uf_smem);
-  if (!e) e = launch_pdl(small_finish_kernel, 1, 1024, uf_smem, st, B);
-  *launches += 1;
-  return e ? e : cudaGetLastError();
+  return cudaGetLastError();
 }
 
 cudaError_t launch_post_regular(const RegularMesh& mesh, int nch, const PostBuffers& B,

@@ -40,6 +40,7 @@ struct PostBuffers {
   unsigned* parent;
   unsigned* n_roots;
   unsigned* err;
+  unsigned* done;                   // short chain: edge-kernel blocks finished (zeroed per call)
   unsigned* cls;                    // per feature classification (FTK2B_CLASS_*)
 };
 

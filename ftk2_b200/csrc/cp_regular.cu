@@ -1459,25 +1459,23 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 }
 
 // ---------------------------------------------------------------------------
-// Exact test in three launches:
-//   refine_gather_kernel  one lane per vertex of a candidate hypercube (32 /
-//                         2^D candidates per warp; batches: one warp per
-//                         candidate, batch_gather_kernel): the values into a
-//                         staging block (global memory, read back from L2),
-//                         quantised once for the inside tests, the vertices'
-//                         cull words, and the mask of the chains that
-//                         survive them; a candidate holding a value
-//                         whose quantised form reaches 2^31 goes to a list
-//   refine_pairs_kernel   each block takes 64 candidates, lays their masks'
-//                         set bits out by a prefix count in shared memory,
-//                         stages their quantised values there, and gives one
-//                         thread to every (candidate, chain): the exact inside
-//                         test, the solve, and the warp-ballot compaction of
-//                         the accepted simplices
-//   the same kernel over the listed candidates, with the 128-bit inside test
-// No global counter is taken per candidate: the only atomics are the sink's
-// and the list's.  The integer inside test and the solve keep every lane busy
-// instead of the few chains of a hypercube that survive the word tests.
+// The exact test of the surviving hypercubes.
+//   single field, two launches:
+//     refine_test_kernel    64 candidates per block: one thread per vertex
+//                           gathers values, quantises them for the inside
+//                           tests and computes the cull words; the chains
+//                           that survive them are laid out as (candidate,
+//                           chain) pairs by a prefix count in shared memory
+//                           and each pair gets one thread for the fast-path
+//                           inside test; the accepted ones go to a list
+//     refine_accept_kernel  the solve of every listed simplex (one thread
+//                           each, values read from the field), and the whole
+//                           test with the 128-bit path for candidates holding
+//                           a quantised value past 2^31
+//   batches, four launches: the gather into a staging block in global memory
+//   (one warp per candidate, batch_gather_kernel), the fast-path inside test,
+//   the solve, and the 128-bit path, each reading the candidate's field record
+// The only atomics are the lists' and the sink's.
 
 // Masks of vertices 1..M of chain ch, a byte each (m1 | m2 << 8 | m3 << 16);
 // 0 past the table.
@@ -1580,111 +1578,6 @@ __device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const 
 
 constexpr int kStageVals = 48;  // 2^D * M values per candidate, D <= 4
 
-// The single-field gather with one lane per hypercube vertex: 32 / 2^D
-// candidates per warp, each lane loading its vertex's M components at once
-// and computing its cull word and quantised values in registers;
-// the chain test shuffles within the candidate's 2^D lanes.  Same staging
-// and chain masks as gather_candidate.
-template <typename T, int D>
-__global__ void __launch_bounds__(kRefineWarps * 32) refine_gather_kernel(RegularMesh mesh, FieldAccess fa,
-                                                                          ExtractConfig cfg, CandidateQueue cq,
-                                                                          RefineStage rs) {
-  constexpr int M = D - 1;
-  constexpr int NV = 1 << D;       // lanes per candidate
-  constexpr int CPW = 32 / NV;     // candidates per warp
-  constexpr int R = (D == 4) ? 4 : 2;  // chain rounds: ceil(chains / NV), 60 / 16 and 12 / 8
-  __shared__ unsigned band_tbl[kBandTable];
-  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int v = lane & (NV - 1), grp = lane / NV;
-  unsigned pkr[R];  // chain_packed of chains r * NV + v
-#pragma unroll
-  for (int r = 0; r < R; ++r) pkr[r] = r * NV + v < kMaxChains ? chain_packed<D>(r * NV + v) : 0u;
-  const int nch = c_chains[D - 3].n;
-  pdl_enter();
-  __syncthreads();
-  const unsigned n = min(*cq.count, cq.cap);
-  const unsigned gw = blockIdx.x * kRefineWarps + wib;
-  const unsigned nw = gridDim.x * kRefineWarps;
-  const unsigned lowmask = NV == 32 ? 0xFFFFFFFFu : ((1u << NV) - 1u);
-  for (unsigned base = gw * CPW; base < n; base += nw * CPW) {
-    const unsigned c = base + grp;
-    const bool has = c < n;
-    const unsigned long long pc = has ? cq.corner[c] : 0ull;
-    const unsigned long long chains = has ? cq.chains[c] : 0ull;
-    const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
-                            (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
-    long long g[4];
-    bool in = has;
-    unsigned long long vid = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
-      g[k] = (k < D) ? lk + mesh.off[k] + ((v >> k) & 1) : 0;
-      if (k < D) {
-        in &= g[k] - mesh.off[k] < mesh.ld[k];
-        vid += (unsigned long long)g[k] * mesh.gstride[k];
-      }
-    }
-    // the vertex's components: one array offset for all of them
-    long long o = 0;
-    if (!fa.per_vertex) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (k < D) {
-          long long a = g[k] - fa.shift[k];
-          if (k == D - 1) a ^= fa.tflip;
-          o += a * fa.estride[k];
-        }
-    } else {
-      o = (long long)vid;
-    }
-    unsigned h[M];
-    bool big = false;
-    T* const out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals + v * M;
-    int* const qout = rs.q + (size_t)c * kStageVals + v * M;
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
-      T x = in ? src[o] : T(0);
-      if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
-      h[j] = hi_word<T>(x);
-      const int qv = quant_small_p(quant_p((double)x, cfg.Q));
-      big |= qv == kQBig;
-      if (has) {
-        out[j] = x;
-        qout[j] = qv;
-      }
-    }
-    const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;  // absent: neutral under AND
-    const bool gbig = ((__ballot_sync(0xFFFFFFFFu, big) >> (grp * NV)) & lowmask) != 0;
-    const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0, NV);
-    unsigned long long mask = 0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int ch = r * NV + v;
-      bool live = ch < nch && ((chains >> ch) & 1ull);
-      unsigned wacc = w0;
-#pragma unroll
-      for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pkr[r] >> (8 * i)) & 0xFF, NV);
-      live = live && (cfg.fiber || !word_culled(wacc));
-      mask |= (unsigned long long)((__ballot_sync(0xFFFFFFFFu, live) >> (grp * NV)) & lowmask) << (r * NV);
-    }
-    if (has && v == 0) {
-      // a candidate holding a value off the fast path: every chain on the
-      // 128-bit path (at most one list entry per candidate)
-      unsigned long long fast = mask;
-      if (gbig && mask) {
-        const unsigned slot = atomicAdd(rs.big_count, 1u);
-        rs.big_list[slot] = c;
-        rs.big_live[slot] = mask;
-        fast = 0;
-      }
-      rs.live[c] = fast;
-    }
-  }
-}
-
 // The fast-path inside test of listed simplex (candidate, chain ch) from the
 // candidate's quantised values qsrc; chain_pk: chain_packed of every chain of
 // the mesh's dimension.
@@ -1709,7 +1602,8 @@ __device__ __forceinline__ bool inside_pair_q(int ch, const int* qsrc, const uns
 // exact test (inside test from the field values, 128-bit quantisation);
 // BIG = false, a simplex the fast-path inside test accepted.  Then the solve
 // and, when accepted, its canonical key and reported values.  src: the
-// candidate's staged values.
+// candidate's staged values, or null to read the simplex's values from the
+// field.
 template <typename T, int D, bool BIG>
 __device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                                           unsigned long long pc, int ch, const T* src, const unsigned* chain_pk,
@@ -1722,11 +1616,41 @@ __device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAc
   const unsigned pk = chain_pk[ch];
 #pragma unroll
   for (int k = 0; k < M; ++k) mk[k + 1] = (pk >> (8 * k)) & 0xFF;
+  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+  long long g0[4];
+  unsigned long long vid0 = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
+    g0[k] = (k < D) ? lk + mesh.off[k] : 0;
+    if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
+  }
   T vals[M + 1][M];
+  if (src) {
 #pragma unroll
-  for (int k = 0; k <= M; ++k)
+    for (int k = 0; k <= M; ++k)
 #pragma unroll
-    for (int j = 0; j < M; ++j) vals[k][j] = src[mk[k] * M + j];
+      for (int j = 0; j < M; ++j) vals[k][j] = src[mk[k] * M + j];
+  } else {
+    // a chain that survives lies inside the mesh
+#pragma unroll
+    for (int k = 0; k <= M; ++k) {
+      long long gv[4];
+      unsigned long long vid = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        gv[q] = (q < D) ? g0[q] + ((mk[k] >> q) & 1) : 0;
+        if (q < D) vid += (unsigned long long)gv[q] * mesh.gstride[q];
+      }
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        T x = field_at<T>(fa, j, gv, D, vid);
+        if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
+        vals[k][j] = x;
+      }
+    }
+  }
   if constexpr (BIG) {
     bool inside;
     if constexpr (M == 2) inside = sos_inside2<T>(vals, cfg.Q);
@@ -1742,16 +1666,6 @@ __device__ __forceinline__ bool test_pair(const RegularMesh& mesh, const FieldAc
     solved = true;
   }
   if (!solved) return false;
-  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
-                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
-  long long g0[4];
-  unsigned long long vid0 = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
-    g0[k] = (k < D) ? lk + mesh.off[k] : 0;
-    if (k < D) vid0 += (unsigned long long)g0[k] * mesh.gstride[k];
-  }
   key = key_base + vid0 * (unsigned long long)CT.n + (unsigned long long)ch;
 #pragma unroll
   for (int k = 0; k <= M; ++k) {
@@ -1811,6 +1725,8 @@ constexpr int kPairCands = 64;  // candidates a block of the exact-test launch t
 // list of (slot, chain) pairs in shared memory (slot << 6 | chain), by a
 // prefix count of the masks' set bits; returns the number of simplices.
 // Shared: msk[kPairCands], off[kPairCands + 1], plist[kPairCands * 64].
+__device__ __forceinline__ unsigned pairs_layout_smem(const unsigned long long* msk, unsigned* off,
+                                                      unsigned short* plist);
 __device__ __forceinline__ unsigned pairs_layout(const unsigned long long* live, unsigned first, unsigned n,
                                                  unsigned long long* msk, unsigned* off, unsigned short* plist) {
   const int t = threadIdx.x;
@@ -1819,6 +1735,13 @@ __device__ __forceinline__ unsigned pairs_layout(const unsigned long long* live,
     msk[t] = c < n ? live[c] : 0ull;
   }
   __syncthreads();
+  return pairs_layout_smem(msk, off, plist);
+}
+
+// The same from masks already in shared memory (visible to the block).
+__device__ __forceinline__ unsigned pairs_layout_smem(const unsigned long long* msk, unsigned* off,
+                                                      unsigned short* plist) {
+  const int t = threadIdx.x;
   if (t < 32) {
     // two candidates per lane, a warp-wide inclusive scan of their counts
     const unsigned a = __popcll(msk[2 * t]), b = __popcll(msk[2 * t + 1]);
@@ -1864,84 +1787,194 @@ __device__ __forceinline__ void acc_append(const RefineStage& rs, bool in, unsig
   if (idx < rs.acc_cap) rs.acc[idx] = ((unsigned long long)c << 8) | (unsigned)ch;
 }
 
-// BIG = false: the fast-path inside test of every surviving simplex of the
-// candidates of rs.live, listing the accepted ones; BIG = true: the whole
-// test of the candidates the gather listed for the 128-bit path.
-template <typename T, int D, bool BIG>
-__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 4) refine_pairs_kernel(RegularMesh mesh, FieldAccess fa,
-                                                                                   ExtractConfig cfg, CandidateQueue cq,
-                                                                                   RefineStage rs, FeatureSink sink) {
+// The single-field exact test, part 1: each block takes 64 candidates at a
+// time, gathers them with one thread per hypercube vertex (each loading its
+// vertex's M components at once, computing its cull word and quantised values
+// in registers; the chain test shuffles within the candidate's 2^D lanes),
+// keeps the quantised values and chain masks in shared memory, lays the
+// surviving (candidate, chain) pairs out, and runs the fast-path inside test
+// with one thread per pair, listing the accepted simplices.  Candidates with
+// a quantised value past 2^31 go to the 128-bit list instead.
+template <typename T, int D>
+__global__ void __launch_bounds__(kRefineWarps * 32, 4) refine_test_kernel(RegularMesh mesh, FieldAccess fa,
+                                                                          ExtractConfig cfg, CandidateQueue cq,
+                                                                          RefineStage rs) {
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;                 // threads per candidate
+  constexpr int kThr = kRefineWarps * 32;
+  constexpr int PER_PASS = kThr / NV;        // candidates per gather pass
+  constexpr int PASSES = kPairCands / PER_PASS;
+  constexpr int R = (D == 4) ? 4 : 2;        // chain rounds: ceil(chains / NV), 60 / 16 and 12 / 8
+  static_assert(PASSES * PER_PASS == kPairCands, "the gather passes cover the block's candidates");
+  __shared__ unsigned band_tbl[kBandTable];
+  __shared__ unsigned chain_pk[kMaxChains];
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
-  __shared__ unsigned chain_pk[kMaxChains];
   __shared__ unsigned short plist[kPairCands * 64];
-  __shared__ __align__(16) int sq[BIG ? 4 : kPairCands * kStageVals];  // the fast path's quantised values
+  __shared__ __align__(16) int sq[kPairCands * kStageVals];
+  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
-  pdl_enter();
   const int lane = threadIdx.x & 31;
-  const unsigned n = BIG ? *rs.big_count : min(*cq.count, cq.cap);
-  const unsigned long long* live = BIG ? rs.big_live : rs.live;
+  const int v = threadIdx.x & (NV - 1), grp = lane / NV, slot = threadIdx.x / NV;
+  unsigned pkr[R];  // chain_packed of chains r * NV + v
+#pragma unroll
+  for (int r = 0; r < R; ++r) pkr[r] = r * NV + v < kMaxChains ? chain_packed<D>(r * NV + v) : 0u;
+  const int nch = c_chains[D - 3].n;
+  const unsigned lowmask = NV == 32 ? 0xFFFFFFFFu : ((1u << NV) - 1u);
+  pdl_enter();
+  __syncthreads();
+  const unsigned n = min(*cq.count, cq.cap);
   for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
-    if constexpr (!BIG) stage_quantised(rs, first, n, sq);
-    const unsigned P = pairs_layout(live, first, n, msk, off, plist);
+#pragma unroll 1
+    for (int pass = 0; pass < PASSES; ++pass) {
+      const int k = pass * PER_PASS + slot;
+      const unsigned c = first + k;
+      const bool has = c < n;
+      const unsigned long long pc = has ? cq.corner[c] : 0ull;
+      const unsigned long long chains = has ? cq.chains[c] : 0ull;
+      const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                              (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+      long long g[4];
+      bool in = has;
+      unsigned long long vid = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const long long lq = (D == 4) ? l[q] : (q < 2 ? l[q] : (q == 2 ? l[3] : 0));
+        g[q] = (q < D) ? lq + mesh.off[q] + ((v >> q) & 1) : 0;
+        if (q < D) {
+          in &= g[q] - mesh.off[q] < mesh.ld[q];
+          vid += (unsigned long long)g[q] * mesh.gstride[q];
+        }
+      }
+      // the vertex's components: one array offset for all of them
+      long long o = 0;
+      if (!fa.per_vertex) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (q < D) {
+            long long a = g[q] - fa.shift[q];
+            if (q == D - 1) a ^= fa.tflip;
+            o += a * fa.estride[q];
+          }
+      } else {
+        o = (long long)vid;
+      }
+      unsigned h[M];
+      bool big = false;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
+        T x = in ? src[o] : T(0);
+        if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
+        h[j] = hi_word<T>(x);
+        const int qv = quant_small_p(quant_p((double)x, cfg.Q));
+        big |= qv == kQBig;
+        sq[k * kStageVals + v * M + j] = qv;
+      }
+      const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;  // absent: neutral under AND
+      const bool gbig = ((__ballot_sync(0xFFFFFFFFu, big) >> (grp * NV)) & lowmask) != 0;
+      const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0, NV);
+      unsigned long long mask = 0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int ch = r * NV + v;
+        bool live = ch < nch && ((chains >> ch) & 1ull);
+        unsigned wacc = w0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pkr[r] >> (8 * i)) & 0xFF, NV);
+        live = live && (cfg.fiber || !word_culled(wacc));
+        mask |= (unsigned long long)((__ballot_sync(0xFFFFFFFFu, live) >> (grp * NV)) & lowmask) << (r * NV);
+      }
+      if (v == 0) {
+        // a candidate holding a value off the fast path: every chain on the
+        // 128-bit path (at most one list entry per candidate)
+        unsigned long long fast = mask;
+        if (has && gbig && mask) {
+          const unsigned s2 = atomicAdd(rs.big_count, 1u);
+          rs.big_list[s2] = c;
+          rs.big_live[s2] = mask;
+          fast = 0;
+        }
+        msk[k] = fast;
+      }
+    }
+    __syncthreads();
+    const unsigned P = pairs_layout_smem(msk, off, plist);
     if (threadIdx.x == 0) atomicAdd(rs.count, P);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
       const unsigned e = p < P ? plist[p] : 0u;
       const int k = (int)(e >> 6), ch = (int)(e & 63);
-      if constexpr (!BIG) {
-        const bool in = p < P && inside_pair_q<D>(ch, sq + k * kStageVals, chain_pk);
-        acc_append(rs, in, first + k, ch, lane);
-      } else {
-        bool acc = false;
-        double lam_out[4] = {0, 0, 0, 0};
-        float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-        float sc_out = 0.f;
-        unsigned long long key = 0;
-        if (p < P) {
-          const unsigned c = rs.big_list[first + k];
-          acc = test_pair<T, D, true>(mesh, fa, cfg, cq.corner[c], ch,
-                                      static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, chain_pk, 0ull, key,
-                                      lam_out, bary_out, sc_out);
-        }
-        sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
-      }
+      const bool ins = p < P && inside_pair_q<D>(ch, sq + k * kStageVals, chain_pk);
+      acc_append(rs, ins, first + k, ch, lane);
     }
-    __syncthreads();  // the layout is rebuilt for the next candidates
+    __syncthreads();  // shared memory is rebuilt for the next candidates
   }
 }
 
-// The solve of every simplex on the inside list, one thread each.  A list
-// longer than its capacity raises the sink count past the sink's capacity,
-// so that the call reports overflow and runs again with larger buffers.
+// The single-field exact test, part 2: blocks below solve_blocks solve the
+// simplices on the inside list (one thread each; a list longer than its
+// capacity raises the sink count past the sink's capacity, so that the call
+// reports overflow and runs again with larger buffers); the others run the
+// whole test on the candidates listed for the 128-bit path.  Values are read
+// from the field.
 template <typename T, int D>
-__global__ void __launch_bounds__(kRefineWarps * 32) refine_solve_kernel(RegularMesh mesh, FieldAccess fa,
-                                                                         ExtractConfig cfg, CandidateQueue cq,
-                                                                         RefineStage rs, FeatureSink sink) {
+__global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_accept_kernel(RegularMesh mesh, FieldAccess fa,
+                                                                            ExtractConfig cfg, CandidateQueue cq,
+                                                                            RefineStage rs, FeatureSink sink,
+                                                                            int solve_blocks) {
+  __shared__ unsigned long long msk[kPairCands];
+  __shared__ unsigned off[kPairCands + 1];
   __shared__ unsigned chain_pk[kMaxChains];
+  __shared__ unsigned short plist[kPairCands * 64];
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
   pdl_enter();
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const unsigned na = *rs.acc_count;
-  if (blockIdx.x == 0 && threadIdx.x == 0 && na > rs.acc_cap) atomicMax(sink.count, na);
-  const unsigned n = min(na, rs.acc_cap);
-  const unsigned stride = gridDim.x * blockDim.x;
-  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
-    const unsigned i = base + threadIdx.x;
-    bool acc = false;
-    double lam_out[4] = {0, 0, 0, 0};
-    float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-    float sc_out = 0.f;
-    unsigned long long key = 0;
-    if (i < n) {
-      const unsigned long long e = rs.acc[i];
-      const unsigned c = (unsigned)(e >> 8);
-      acc = test_pair<T, D, false>(mesh, fa, cfg, cq.corner[c], (int)(e & 255),
-                                   static_cast<const T*>(rs.vals) + (size_t)c * kStageVals, chain_pk, 0ull, key,
-                                   lam_out, bary_out, sc_out);
+  if ((int)blockIdx.x < solve_blocks) {
+    const unsigned na = *rs.acc_count;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && na > rs.acc_cap) atomicMax(sink.count, na);
+    const unsigned n = min(na, rs.acc_cap);
+    const unsigned stride = solve_blocks * blockDim.x;
+    for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+      const unsigned i = base + threadIdx.x;
+      bool acc = false;
+      double lam_out[4] = {0, 0, 0, 0};
+      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+      float sc_out = 0.f;
+      unsigned long long key = 0;
+      if (i < n) {
+        const unsigned long long e = rs.acc[i];
+        const unsigned c = (unsigned)(e >> 8);
+        acc = test_pair<T, D, false>(mesh, fa, cfg, cq.corner[c], (int)(e & 255), (const T*)nullptr, chain_pk, 0ull,
+                                     key, lam_out, bary_out, sc_out);
+      }
+      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
-    sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
+    return;
+  }
+  const unsigned nb = *rs.big_count;
+  const unsigned bb = blockIdx.x - solve_blocks, nbb = gridDim.x - solve_blocks;
+  for (unsigned first = bb * kPairCands; first < nb; first += nbb * kPairCands) {
+    const unsigned P = pairs_layout(rs.big_live, first, nb, msk, off, plist);
+    if (threadIdx.x == 0) atomicAdd(rs.count, P);
+    for (unsigned base = 0; base < P; base += blockDim.x) {
+      const unsigned p = base + threadIdx.x;
+      const unsigned e = p < P ? plist[p] : 0u;
+      const int k = (int)(e >> 6), ch = (int)(e & 63);
+      bool acc = false;
+      double lam_out[4] = {0, 0, 0, 0};
+      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+      float sc_out = 0.f;
+      unsigned long long key = 0;
+      if (p < P) {
+        const unsigned c = rs.big_list[first + k];
+        acc = test_pair<T, D, true>(mesh, fa, cfg, cq.corner[c], ch, (const T*)nullptr, chain_pk, 0ull, key, lam_out,
+                                    bary_out, sc_out);
+      }
+      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
+    }
+    __syncthreads();
   }
 }
 
@@ -2509,11 +2542,9 @@ static cudaError_t launch_refine_staged_t(const RegularMesh& mesh, const FieldAc
   const int thr = kRefineWarps * 32;
   // programmatic dependent launches: each kernel waits for its predecessor
   // at its start (pdl_enter), so its launch overlaps the predecessor's tail
-  cudaError_t e = launch_pdl(refine_gather_kernel<T, D>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs);
-  if (!e) e = launch_pdl(refine_pairs_kernel<T, D, false>, num_sms * 8, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-  if (!e) e = launch_pdl(refine_solve_kernel<T, D>, num_sms * 2, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
-  // the 128-bit list is usually short or empty
-  if (!e) e = launch_pdl(refine_pairs_kernel<T, D, true>, num_sms, thr, 0, st, mesh, fa, cfg, cq, rs, sink);
+  cudaError_t e = launch_pdl(refine_test_kernel<T, D>, num_sms * 4, thr, 0, st, mesh, fa, cfg, cq, rs);
+  // solve blocks, then blocks for the (usually short or empty) 128-bit list
+  if (!e) e = launch_pdl(refine_accept_kernel<T, D>, num_sms * 2, thr, 0, st, mesh, fa, cfg, cq, rs, sink, num_sms);
   return e ? e : cudaGetLastError();
 }
 
