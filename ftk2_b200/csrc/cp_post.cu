@@ -911,14 +911,24 @@ __device__ __forceinline__ void finish_block(const PostBuffers& B, unsigned* sh,
       B.edges[2 * (size_t)e + 1] = other;
     }
   }
-  // every feature's root: the minimum of its component
+  // every feature's root (the minimum of its component) by pointer jumping:
+  // each round replaces every parent by its parent's parent, halving every
+  // path (reads may see this round's or the last round's values, both
+  // ancestors); a path of length L needs log2(L) rounds, at most 14 here
+  for (int round = 0; round < 16; ++round) {
+    bool changed = false;
+    for (unsigned i = t; i < n; i += 1024) {
+      const unsigned p = sp[i], pp = sp[p];
+      if (pp != p) {
+        sp[i] = pp;
+        changed = true;
+      }
+    }
+    if (!__syncthreads_or(changed)) break;
+  }
   unsigned roots = 0;
   for (unsigned i = t; i < n; i += 1024) {
-    unsigned x = i, p = sp[x];
-    while (p != x) {
-      x = p;
-      p = sp[x];
-    }
+    const unsigned x = sp[i];
     B.track[i] = x;
     roots += x == i ? 1u : 0u;
   }

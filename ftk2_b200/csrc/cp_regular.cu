@@ -1461,7 +1461,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 // ---------------------------------------------------------------------------
 // The exact test of the surviving hypercubes.
 //   single field, two launches:
-//     refine_test_kernel    64 candidates per block: one thread per vertex
+//     refine_test_kernel    32 candidates per block: one thread per vertex
 //                           gathers values, quantises them for the inside
 //                           tests and computes the cull words; the chains
 //                           that survive them are laid out as (candidate,
@@ -1720,6 +1720,9 @@ __device__ __forceinline__ void sink_write(const FeatureSink& sink, bool acc, un
 }
 
 constexpr int kPairCands = 64;  // candidates a block of the exact-test launch takes at a time
+// candidates a block of the single-field test takes at a time: small groups
+// balance the launch's few blocks across the SMs
+constexpr int kTestCands = 32;
 
 // The block's next kPairCands entries of `live` from `first` laid out as a
 // list of (slot, chain) pairs in shared memory (slot << 6 | chain), by a
@@ -1787,8 +1790,8 @@ __device__ __forceinline__ void acc_append(const RefineStage& rs, bool in, unsig
   if (idx < rs.acc_cap) rs.acc[idx] = ((unsigned long long)c << 8) | (unsigned)ch;
 }
 
-// The single-field exact test, part 1: each block takes 64 candidates at a
-// time, gathers them with one thread per hypercube vertex (each loading its
+// The single-field exact test, part 1: each block takes kTestCands
+// candidates at a time, gathers them with one thread per hypercube vertex (each loading its
 // vertex's M components at once, computing its cull word and quantised values
 // in registers; the chain test shuffles within the candidate's 2^D lanes),
 // keeps the quantised values and chain masks in shared memory, lays the
@@ -1803,17 +1806,19 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 4) refine_test_kernel(Regul
   constexpr int NV = 1 << D;                 // threads per candidate
   constexpr int kThr = kRefineWarps * 32;
   constexpr int PER_PASS = kThr / NV;        // candidates per gather pass
-  constexpr int PASSES = kPairCands / PER_PASS;
+  constexpr int PASSES = kTestCands / PER_PASS;
   constexpr int R = (D == 4) ? 4 : 2;        // chain rounds: ceil(chains / NV), 60 / 16 and 12 / 8
-  static_assert(PASSES * PER_PASS == kPairCands, "the gather passes cover the block's candidates");
+  static_assert(PASSES * PER_PASS == kTestCands, "the gather passes cover the block's candidates");
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned chain_pk[kMaxChains];
   __shared__ unsigned long long msk[kPairCands];
   __shared__ unsigned off[kPairCands + 1];
-  __shared__ unsigned short plist[kPairCands * 64];
-  __shared__ __align__(16) int sq[kPairCands * kStageVals];
+  __shared__ unsigned short plist[kTestCands * 64];
+  __shared__ __align__(16) int sq[kTestCands * kStageVals];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) chain_pk[i] = chain_packed<D>(i);
+  // the layout scans kPairCands masks; slots past the block's kTestCands stay empty
+  if (threadIdx.x >= kTestCands && threadIdx.x < kPairCands) msk[threadIdx.x] = 0ull;
   const int lane = threadIdx.x & 31;
   const int v = threadIdx.x & (NV - 1), grp = lane / NV, slot = threadIdx.x / NV;
   unsigned pkr[R];  // chain_packed of chains r * NV + v
@@ -1824,7 +1829,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 4) refine_test_kernel(Regul
   pdl_enter();
   __syncthreads();
   const unsigned n = min(*cq.count, cq.cap);
-  for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
+  for (unsigned first = blockIdx.x * kTestCands; first < n; first += gridDim.x * kTestCands) {
 #pragma unroll 1
     for (int pass = 0; pass < PASSES; ++pass) {
       const int k = pass * PER_PASS + slot;
@@ -2542,7 +2547,9 @@ static cudaError_t launch_refine_staged_t(const RegularMesh& mesh, const FieldAc
   const int thr = kRefineWarps * 32;
   // programmatic dependent launches: each kernel waits for its predecessor
   // at its start (pdl_enter), so its launch overlaps the predecessor's tail
-  cudaError_t e = launch_pdl(refine_test_kernel<T, D>, num_sms * 4, thr, 0, st, mesh, fa, cfg, cq, rs);
+  // more blocks than fit at once: each takes one group while the candidates
+  // last, and a block that finishes early makes room for the next
+  cudaError_t e = launch_pdl(refine_test_kernel<T, D>, num_sms * 16, thr, 0, st, mesh, fa, cfg, cq, rs);
   // solve blocks, then blocks for the (usually short or empty) 128-bit list
   if (!e) e = launch_pdl(refine_accept_kernel<T, D>, num_sms * 2, thr, 0, st, mesh, fa, cfg, cq, rs, sink, num_sms);
   return e ? e : cudaGetLastError();
