@@ -329,20 +329,6 @@ __device__ __forceinline__ unsigned batch_field_of(const unsigned long long* __r
   return lo;
 }
 
-__global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const unsigned long long* __restrict__ kb,
-                                        int nf, const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
-                                        unsigned cap, unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
-  const unsigned n = min(*n_ptr, cap);
-  const int lane = threadIdx.x & 31;
-  const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
-  for (unsigned i = gw; i < n; i += nw) {
-    const unsigned long long key = keys[i];
-    const unsigned f = batch_field_of(kb, nf, key);
-    edges_of_feature(fm[f].mesh, fm[f].nch, keys, n, i, key - kb[f], kb[f], lane, cnt, slots);
-  }
-}
-
 // After the exclusive scan of the counts (in place), copy every feature's
 // edges to their final positions: (centre, other) pairs, sorted and unique.
 __global__ void edges_compact_kernel(const unsigned* n_ptr, unsigned cap, const unsigned* __restrict__ off,
@@ -726,6 +712,28 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
     if (parent) uf_unite(parent, i, (unsigned)idx, err);
   }
   if (lane == 0) cnt[i] = __popc(vm);
+}
+
+// Batches: one warp per feature (the short chain's star_edges_warp with the
+// feature's field, found by its key).
+__global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const unsigned long long* __restrict__ kb,
+                                        int nf, const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
+                                        unsigned cap, unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+  __shared__ StarTables T[2];  // d = 3, d = 4
+  fill_star_tables(T[0], 3);
+  fill_star_tables(T[1], 4);
+  __syncthreads();
+  const unsigned n = min(*n_ptr, cap);
+  const int lane = threadIdx.x & 31;
+  const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned i = gw; i < n; i += nw) {
+    const unsigned long long key = keys[i];
+    const unsigned f = batch_field_of(kb, nf, key);
+    const RegularMesh mesh = fm[f].mesh;
+    star_edges_warp(mesh, fm[f].nch, keys, n, i, key - kb[f], kb[f], T[mesh.d - 3], lane, cnt, slots, nullptr,
+                    nullptr);
+  }
 }
 
 // Exclusive scan over a block of 1024 threads, one value each; *total = sum.

@@ -1484,98 +1484,6 @@ __device__ __forceinline__ unsigned chain_packed(int ch) {
   return g_chain_pk[D - 3][ch];
 }
 
-// One candidate by one warp: its vertex values into `out` (kStageVals values
-// per candidate) and the warp's shared cube, the values quantised for the
-// inside tests into `qout`, its vertex words, and the mask of its surviving
-// chains into rs.live[c] (or, when a value is off the fast path, into the
-// 128-bit list).  pk0 / pk1: chain_packed of chains lane and 32 + lane;
-//
-// A chain survives when its vertices' cull words do not prove that the solve
-// rejects it.  (A test on the signs of the quantised values alone would not
-// do: when the quantised vertices and the origin are coplanar, the inside
-// test's fallback levels, which perturb by matrix row rather than by vertex,
-// can answer "inside" for a simplex whose quantised values keep one strict
-// sign, and the solve then decides.)
-template <typename T, int D>
-__device__ __forceinline__ void gather_candidate(const RegularMesh& mesh, const FieldAccess& fa,
-                                                 const ExtractConfig& cfg, unsigned c, unsigned long long pc,
-                                                 unsigned long long chains, T* out, int* qout, T* my,
-                                                 const unsigned* band_tbl, unsigned pk0, unsigned pk1,
-                                                 const RefineStage& rs, int lane) {
-  constexpr int M = D - 1;
-  constexpr int NV = 1 << D;
-  const int nch = c_chains[D - 3].n;
-  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
-                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
-  long long g0[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const long long lk = (D == 4) ? l[k] : (k < 2 ? l[k] : (k == 2 ? l[3] : 0));
-    g0[k] = (k < D) ? lk + mesh.off[k] : 0;
-  }
-  bool anybig = false;
-  for (int e = lane; e < NV * M; e += 32) {
-    const int v = e / M, j = e % M;
-    long long g[4];
-    unsigned long long vid = 0;
-    bool in = true;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      g[k] = (k < D) ? g0[k] + ((v >> k) & 1) : 0;
-      if (k < D) {
-        in &= g[k] - mesh.off[k] < mesh.ld[k];
-        vid += (unsigned long long)g[k] * mesh.gstride[k];
-      }
-    }
-    T val = in ? field_at<T>(fa, j, g, D, vid) : T(0);
-    if (cfg.fiber) val = fp<T>::sub(val, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
-    my[e] = val;
-    out[e] = val;
-    const int qv = quant_small_p(quant_p((double)val, cfg.Q));
-    qout[e] = qv;
-    anybig |= qv == kQBig;
-  }
-  const bool big = __any_sync(0xFFFFFFFFu, anybig);
-  __syncwarp();
-  unsigned vw = kAbsent;  // absent vertices: neutral under AND
-  if (lane < NV) {
-    unsigned h[M];
-#pragma unroll
-    for (int j = 0; j < M; ++j) h[j] = hi_word<T>(my[lane * M + j]);
-    bool in = true;
-#pragma unroll
-    for (int k = 0; k < D; ++k) in &= g0[k] + ((lane >> k) & 1) - mesh.off[k] < mesh.ld[k];
-    if (in) vw = vertex_word_hi<T, M>(h, band_tbl);
-  }
-  const unsigned w0 = __shfl_sync(0xFFFFFFFFu, vw, 0);
-  unsigned long long mask = 0;
-#pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    if (half * 32 >= nch) break;
-    const int ch = half * 32 + lane;
-    const unsigned pk = half ? pk1 : pk0;
-    bool live = ch < nch && ((chains >> ch) & 1ull);
-    unsigned wacc = w0;
-#pragma unroll
-    for (int i = 0; i < M; ++i) wacc &= __shfl_sync(0xFFFFFFFFu, vw, (pk >> (8 * i)) & 0xFF);
-    live = live && (cfg.fiber || !word_culled(wacc));
-    mask |= (unsigned long long)__ballot_sync(0xFFFFFFFFu, live) << (half * 32);
-  }
-  if (lane == 0) {
-    // a candidate holding a value off the fast path: every chain on the
-    // 128-bit path (at most one list entry per candidate)
-    unsigned long long fast = mask;
-    if (big && mask) {
-      const unsigned slot = atomicAdd(rs.big_count, 1u);
-      rs.big_list[slot] = c;
-      rs.big_live[slot] = mask;
-      fast = 0;
-    }
-    rs.live[c] = fast;
-  }
-  __syncwarp();
-}
-
 constexpr int kStageVals = 48;  // 2^D * M values per candidate, D <= 4
 
 // The fast-path inside test of listed simplex (candidate, chain ch) from the
@@ -1984,29 +1892,117 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_accept_kernel(Reg
 }
 
 // the same two launches over a batch: each candidate reads its field's record
+// One candidate of a batch by a group of 16 lanes, one per hypercube vertex
+// (lanes 8-15 idle for a 2D+t field): its values and their quantised form
+// into the staging block, the vertices' cull words, and the mask of the
+// chains that survive them (or, with a quantised value past 2^31, the
+// 128-bit list).  gmask: the group's lanes; gshift: its first lane.
+template <typename T, int D>
+__device__ __forceinline__ void gather_group(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
+                                             unsigned c, unsigned long long pc, unsigned long long chains, int v,
+                                             unsigned gmask, int gshift, const unsigned* band_tbl,
+                                             const unsigned* chain_pk, const RefineStage& rs) {
+  constexpr int M = D - 1;
+  constexpr int NV = 1 << D;
+  constexpr int R = (D == 4) ? 4 : 1;  // chain rounds of 16: 60 and 12 chains
+  const int nch = c_chains[D - 3].n;
+  const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
+                          (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
+  long long g[4];
+  bool in = v < NV;
+  unsigned long long vid = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long lq = (D == 4) ? l[q] : (q < 2 ? l[q] : (q == 2 ? l[3] : 0));
+    g[q] = (q < D) ? lq + mesh.off[q] + ((v >> q) & 1) : 0;
+    if (q < D) {
+      in &= g[q] - mesh.off[q] < mesh.ld[q];
+      vid += (unsigned long long)g[q] * mesh.gstride[q];
+    }
+  }
+  long long o = 0;
+  if (!fa.per_vertex) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (q < D) {
+        long long a = g[q] - fa.shift[q];
+        if (q == D - 1) a ^= fa.tflip;
+        o += a * fa.estride[q];
+      }
+  } else {
+    o = (long long)vid;
+  }
+  unsigned h[M];
+  bool big = false;
+  T* const out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals + v * M;
+  int* const qout = rs.q + (size_t)c * kStageVals + v * M;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
+    T x = in ? src[o] : T(0);
+    if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
+    h[j] = hi_word<T>(x);
+    const int qv = quant_small_p(quant_p((double)x, cfg.Q));
+    big |= v < NV && qv == kQBig;
+    if (v < NV) {
+      out[j] = x;
+      qout[j] = qv;
+    }
+  }
+  const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;  // absent: neutral under AND
+  const bool gbig = ((__ballot_sync(gmask, big) >> gshift) & 0xFFFFu) != 0;
+  const unsigned w0 = __shfl_sync(gmask, vw, 0, 16);
+  unsigned long long mask = 0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int ch = r * 16 + v;
+    bool live = ch < nch && ((chains >> ch) & 1ull);
+    const unsigned pk = chain_pk[ch];
+    unsigned wacc = w0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) wacc &= __shfl_sync(gmask, vw, (pk >> (8 * i)) & 0xFF, 16);
+    live = live && (cfg.fiber || !word_culled(wacc));
+    mask |= (unsigned long long)((__ballot_sync(gmask, live) >> gshift) & 0xFFFFu) << (r * 16);
+  }
+  if (v == 0) {
+    unsigned long long fast = mask;
+    if (gbig && mask) {
+      const unsigned slot = atomicAdd(rs.big_count, 1u);
+      rs.big_list[slot] = c;
+      rs.big_live[slot] = mask;
+      fast = 0;
+    }
+    rs.live[c] = fast;
+  }
+}
+
+// the batch gather: two candidates per warp, 16 lanes each
 template <typename T>
 __global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const BatchField* __restrict__ fields,
                                                                          CandidateQueue cq, RefineStage rs) {
-  __shared__ T cube[kRefineWarps][kStageVals];
   __shared__ unsigned band_tbl[kBandTable];
+  __shared__ unsigned chain_pk[2][kMaxChains];
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
+  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
+    chain_pk[0][i] = chain_packed<3>(i);
+    chain_pk[1][i] = chain_packed<4>(i);
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const unsigned pk3 = chain_packed<3>(lane);
-  const unsigned pk40 = chain_packed<4>(lane), pk41 = chain_packed<4>(32 + lane);
+  const int v = lane & 15, grp = lane >> 4;
+  const unsigned gmask = 0xFFFFu << (16 * grp);
   const unsigned n = min(*cq.count, cq.cap);
   const unsigned gw = blockIdx.x * kRefineWarps + wib;
   const unsigned nw = gridDim.x * kRefineWarps;
-  for (unsigned c = gw; c < n; c += nw) {
+  for (unsigned base = gw * 2; base < n; base += nw * 2) {
+    const unsigned c = base + grp;
+    if (c >= n) continue;  // the whole group
     const BatchField& F = fields[cq.field[c]];
-    T* out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals;
-    int* qout = rs.q + (size_t)c * kStageVals;
+    const unsigned long long pc = cq.corner[c], chains = cq.chains[c];
     if (F.mesh.d == 4)
-      gather_candidate<T, 4>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
-                             pk40, pk41, rs, lane);
+      gather_group<T, 4>(F.mesh, F.fa, F.cfg, c, pc, chains, v, gmask, 16 * grp, band_tbl, chain_pk[1], rs);
     else
-      gather_candidate<T, 3>(F.mesh, F.fa, F.cfg, c, cq.corner[c], cq.chains[c], out, qout, cube[wib], band_tbl,
-                             pk3, 0u, rs, lane);
+      gather_group<T, 3>(F.mesh, F.fa, F.cfg, c, pc, chains, v, gmask, 16 * grp, band_tbl, chain_pk[0], rs);
   }
 }
 
@@ -2616,12 +2612,12 @@ cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const 
                                        const RefineStage& rs, const FeatureSink& sink, int num_sms, cudaStream_t st) {
   const int thr = kRefineWarps * 32;
   if (f64) {
-    batch_gather_kernel<double><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
+    batch_gather_kernel<double><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs);
     batch_pairs_kernel<double, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
     batch_solve_kernel<double><<<num_sms * 2, thr, 0, st>>>(fields, cq, rs, sink);
     batch_pairs_kernel<double, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
   } else {
-    batch_gather_kernel<float><<<num_sms * 16, thr, 0, st>>>(fields, cq, rs);
+    batch_gather_kernel<float><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs);
     batch_pairs_kernel<float, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
     batch_solve_kernel<float><<<num_sms * 2, thr, 0, st>>>(fields, cq, rs, sink);
     batch_pairs_kernel<float, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
