@@ -51,33 +51,81 @@ __global__ void rs_hist_kernel(const unsigned long long* __restrict__ keys, cons
   hist[threadIdx.x * G + b] = h[threadIdx.x];
 }
 
-// exclusive scan of `total` counters in place, one block of 1024 threads
+// Exclusive scan over a block of 1024 threads, one value each; *total = sum.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* wsum /* 33 */, unsigned* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned w = wsum[lane];
+    unsigned wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    wsum[lane] = wi - w;
+    if (lane == 31) wsum[32] = wi;
+  }
+  __syncthreads();
+  *total = wsum[32];
+  return wsum[warp] + incl - v;
+}
+
+// exclusive scan of `total` counters in place (clamped to *n_ptr), one block
+// of 1024 threads: tiles of 4096 counters, each thread 4 consecutive ones
+// (coalesced 16-byte loads), the next tile's loads issued before the current
+// tile is scanned, a running carry between tiles
 __global__ void scan_inplace_kernel(unsigned* __restrict__ a, unsigned total, unsigned* total_out,
                                     const unsigned* n_ptr, const unsigned* skip_small) {
   pdl_enter();
-  __shared__ unsigned part[1024];
+  constexpr int kPer = 4;
+  constexpr unsigned kTile = 1024u * kPer;
+  __shared__ unsigned wsum[33];
   const unsigned t = threadIdx.x;
   (void)skip_small;
   if (n_ptr) total = min(total, *n_ptr);
-  const unsigned seg = (total + 1023) / 1024;
-  const unsigned s0 = min(t * seg, total), s1 = min(s0 + seg, total);
-  unsigned sum = 0;
-  for (unsigned i = s0; i < s1; ++i) sum += a[i];
-  part[t] = sum;
-  __syncthreads();
-  for (unsigned off = 1; off < 1024; off <<= 1) {
-    unsigned v = (t >= off) ? part[t - off] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
+  const bool vec = (reinterpret_cast<uintptr_t>(a) & 15) == 0;  // 16-byte loads need an aligned array
+  auto load = [&](unsigned base, unsigned (&v)[kPer]) {
+    const unsigned i0 = base + t * kPer;
+    if (vec && base + kTile <= total) {
+      const uint4 q = *reinterpret_cast<const uint4*>(a + i0);
+      v[0] = q.x;
+      v[1] = q.y;
+      v[2] = q.z;
+      v[3] = q.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) v[j] = i0 + j < total ? a[i0 + j] : 0u;
+    }
+  };
+  unsigned nxt[kPer] = {0u, 0u, 0u, 0u};
+  if (total) load(0, nxt);
+  unsigned carry = 0;
+  for (unsigned base = 0; base < total; base += kTile) {
+    unsigned v[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) v[j] = nxt[j];
+    if (base + kTile < total) load(base + kTile, nxt);
+    const unsigned sum = v[0] + v[1] + v[2] + v[3];
+    unsigned tile_total;
+    unsigned run = carry + block_exclusive_scan(sum, wsum, &tile_total);
+    const unsigned i0 = base + t * kPer;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      if (i0 + j < total) a[i0 + j] = run;
+      run += v[j];
+    }
+    carry += tile_total;
+    __syncthreads();  // wsum is rewritten by the next tile's scan
   }
-  unsigned run = part[t] - sum;
-  for (unsigned i = s0; i < s1; ++i) {
-    unsigned v = a[i];
-    a[i] = run;
-    run += v;
-  }
-  if (total_out && t == 1023) *total_out = part[1023];
+  if (total_out && t == 0) *total_out = carry;
 }
 
 __global__ void rs_scatter_kernel(const unsigned long long* __restrict__ kin,
@@ -736,32 +784,6 @@ __global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const 
   }
 }
 
-// Exclusive scan over a block of 1024 threads, one value each; *total = sum.
-__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* wsum /* 33 */, unsigned* total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned incl = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  if (lane == 31) wsum[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    const unsigned w = wsum[lane];
-    unsigned wi = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-      if (lane >= o) wi += y;
-    }
-    wsum[lane] = wi - w;
-    if (lane == 31) wsum[32] = wi;
-  }
-  __syncthreads();
-  *total = wsum[32];
-  return wsum[warp] + incl - v;
-}
 
 __global__ void __launch_bounds__(kSortThreads, 1) small_sort_kernel(PostBuffers B) {
   extern __shared__ unsigned long long sk[];  // the n packed keys, by bucket
