@@ -1086,8 +1086,9 @@ cudaError_t launch_post_batch(const BatchMesh* fm, const unsigned long long* kb,
                                    B.bary4_sorted);
   expand_batch_kernel<<<g, 256, 0, st>>>(fm, kb, nf, skey, B.count, cap, B.bary4_sorted, B.simplices, B.bary);
   batch_bounds_kernel<<<(nf + 256) / 256, 256, 0, st>>>(kb, nf, skey, B.count, cap, fbase);
-  edges_batch_warp_kernel<<<grid_for(cap, 8, 8192), 256, 0, st>>>(fm, kb, nf, skey, B.count, cap, B.edge_cnt,
-                                                                 B.edge_slots);
+  // a persistent grid: every block copies the face tables into shared memory once
+  edges_batch_warp_kernel<<<(B.num_sms > 0 ? B.num_sms : 148) * 2, 512, 0, st>>>(fm, kb, nf, skey, B.count, cap,
+                                                                                  B.edge_cnt, B.edge_slots);
   scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count, nullptr);
   edges_compact_kernel<<<g, 256, 0, st>>>(B.count, cap, B.edge_cnt, B.n_edges, B.edge_slots, B.edges, B.edge_cap);
   uf_init_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap);

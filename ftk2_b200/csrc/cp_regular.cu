@@ -144,8 +144,10 @@ template <> struct Tile<4> {
   static constexpr int TX = 32, TY = 8, TZ = 4;
 };
 template <> struct Tile<3> {
-  // warp w owns corner rows cy = 2w, 2w + 1
-  static constexpr int TX = 32, TY = 32, TZ = 1;
+  // warp w < 15 owns corner rows cy = 2w, 2w + 1 (warp 15 none): 31 x 33
+  // vertex slots fit the block's 512 threads twice (32 rows would take 1089
+  // slots, a third pass over mostly empty slots)
+  static constexpr int TX = 32, TY = 30, TZ = 1;
 };
 
 constexpr int kThreads = 512;
@@ -217,7 +219,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   constexpr int VX = G::VX, VY = G::VY, VZ = G::VZ, VS = G::VS, VPT = G::VPT, VSP = G::VSP;
   constexpr int TBIT = 1 << (D - 1);  // mask bit of the time axis
   constexpr int HW = sizeof(T) / 4;   // the high 32-bit word of an element is its last
-  static_assert(D == 3 ? kWarps * kRows == TY : kWarps == TY * (TZ / kRows),
+  static_assert(D == 3 ? kWarps * kRows >= TY : kWarps == TY * (TZ / kRows),
                 "every corner row of the tile belongs to exactly one warp");
   unsigned* const Wb = reinterpret_cast<unsigned*>(smem + G::WORDS);
   const int tid = threadIdx.x;
@@ -491,8 +493,9 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   for (int q = 0; q < kRows; ++q) {
     const int cy = (D == 4) ? cyw : cyw + q;
     const int cz = (D == 4) ? czw + q : 0;
-    if (x0 + lane < ldx && y0 + cy < ldy && (D == 3 || z0 + cz < ldz)) row_valid |= 1u << q;
+    if (x0 + lane < ldx && cy < TY && y0 + cy < ldy && (D == 3 || z0 + cz < ldz)) row_valid |= 1u << q;
   }
+  const bool has_rows = D == 4 || cyw < TY;  // warp-uniform: the warp owns corner rows of the tile
 
   for (int ct = t0; ct < t1; ++ct) {
     const int s = ct + 1;
@@ -524,6 +527,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       return false;
     }
     if (s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
+    if (!has_rows) continue;
 
     // ---- hypercube cull: lanes along x, kRows corner rows per warp
     unsigned R[kRows + 1];
@@ -1055,7 +1059,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1)
   constexpr int VX = G::VX, VY = G::VY, VZ = G::VZ, VS = G::VS, VPT = G::VPT, VSP = G::VSP;
   constexpr int TBIT = 1 << (D - 1);
   constexpr int HW = sizeof(T) / 4;
-  static_assert(D == 3 ? kWarps * kRows == TY : kWarps == TY * (TZ / kRows),
+  static_assert(D == 3 ? kWarps * kRows >= TY : kWarps == TY * (TZ / kRows),
                 "every corner row of the tile belongs to exactly one warp");
 
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1213,7 +1217,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1)
     for (int q = 0; q < kRows; ++q) {
       const int cy = (D == 4) ? cyw : cyw + q;
       const int cz = (D == 4) ? czw + q : 0;
-      if (x0 + lane < ldx && y0 + cy < ldy && (D == 3 || z0 + cz < ldz)) row_valid |= 1u << q;
+      if (x0 + lane < ldx && cy < TY && y0 + cy < ldy && (D == 3 || z0 + cz < ldz)) row_valid |= 1u << q;
     }
     for (int c = t0; c < t1; ++c) {
       const int s = c + 1;
@@ -1240,6 +1244,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1)
         return;
       }
       if (TMA && tid == 0) produce_until(q_c + kNbuf - 1);
+      if (D == 3 && cyw >= TY) continue;  // warp-uniform: no corner rows of the tile
       const unsigned* A = wslot(q_c % kNbuf);
       const unsigned* B = has_s ? wslot((q_c + 1) % kNbuf) : wslot(kNbuf);
       unsigned R[kRows + 1];
@@ -2118,6 +2123,14 @@ __global__ void __launch_bounds__(kThreads, 2)
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned s_item, s_field;
   __shared__ unsigned s_ib[kBatchSmemFields];
+  __shared__ RegularMesh s_mesh;
+  __shared__ FieldAccess s_fa;
+  __shared__ ExtractConfig s_cfg;
+  __shared__ int s_tma;
+  __shared__ unsigned s_ibase;
+  static_assert(sizeof(RegularMesh) % 4 == 0 && sizeof(FieldAccess) % 4 == 0 && sizeof(ExtractConfig) % 4 == 0 &&
+                    (sizeof(RegularMesh) + sizeof(FieldAccess) + sizeof(ExtractConfig)) / 4 <= kThreads,
+                "one thread per word of a field record");
   const bool ib_smem = nf <= kBatchSmemFields;
   if (ib_smem)
     for (int i = threadIdx.x; i < nf; i += kThreads) s_ib[i] = item_base[i];
@@ -2153,23 +2166,40 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (it >= n_items) break;
     const unsigned f = s_field;
     const BatchField& F = fields[f];
-    const unsigned local = it - F.item_base;
-    const unsigned ntiles = (unsigned)F.cfg.tiles[0] * F.cfg.tiles[1] * F.cfg.tiles[2];
+    // the field's mesh, access and configuration into shared memory (the
+    // tensor maps stay in global memory, where TMA reads them)
+    {
+      constexpr int kMw = sizeof(RegularMesh) / 4, kFw = sizeof(FieldAccess) / 4, kCw = sizeof(ExtractConfig) / 4;
+      const unsigned* src_m = reinterpret_cast<const unsigned*>(&F.mesh);
+      const unsigned* src_f = reinterpret_cast<const unsigned*>(&F.fa);
+      const unsigned* src_c = reinterpret_cast<const unsigned*>(&F.cfg);
+      const int t = threadIdx.x;
+      if (t < kMw) reinterpret_cast<unsigned*>(&s_mesh)[t] = src_m[t];
+      else if (t < kMw + kFw) reinterpret_cast<unsigned*>(&s_fa)[t - kMw] = src_f[t - kMw];
+      else if (t < kMw + kFw + kCw) reinterpret_cast<unsigned*>(&s_cfg)[t - kMw - kFw] = src_c[t - kMw - kFw];
+      if (t == 0) {
+        s_tma = F.tma;
+        s_ibase = F.item_base;
+      }
+    }
+    __syncthreads();
+    const unsigned local = it - s_ibase;
+    const unsigned ntiles = (unsigned)s_cfg.tiles[0] * s_cfg.tiles[1] * s_cfg.tiles[2];
     CandidateQueue q = cq;
     q.field_id = f;
     bool ok;
-    if (F.mesh.d == 4) {
-      ok = F.tma ? cull_tile<T, 4, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+    if (s_mesh.d == 4) {
+      ok = s_tma ? cull_tile<T, 4, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
                                                 ph)
-                 : cull_tile<T, 4, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+                 : cull_tile<T, 4, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                  (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
                                                  ph);
     } else {
-      ok = F.tma ? cull_tile<T, 3, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+      ok = s_tma ? cull_tile<T, 3, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
                                                 ph)
-                 : cull_tile<T, 3, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], F.mesh, F.fa, F.cfg, q, err,
+                 : cull_tile<T, 3, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                  (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
                                                  ph);
     }
