@@ -207,21 +207,12 @@ __device__ __forceinline__ unsigned long long pack_corner(long long x, long long
 // (so that a persistent block can march many tiles) and is advanced past the
 // copies this call waits for.  Returns false when a bounded TMA wait gave up
 // (the error flag is set).
-//
-// A persistent block may pass the tile and time chunk of its next item of the
-// same field (next_tile >= 0): once the last slice of this item has been
-// turned into words, both slice buffers are free and the next item's first
-// two slices are issued into them (*did_prefetch = true, for every thread),
-// so that its prologue does not wait for a whole load; the next call then
-// passes prefetched = true and skips those two issues.  Only the mbarrier
-// stagings (TMA, bulk rows) prefetch.
 template <typename T, int D, bool MULTI, bool TMA>
 __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtensorMap* map1,
                                           const CUtensorMap* map2, const RegularMesh& mesh, const FieldAccess& fa,
                                           const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
                                           int tile, int chunk, unsigned char* smem, unsigned long long* bar,
-                                          const unsigned* band_tbl, unsigned ph[2], bool prefetched = false,
-                                          int next_tile = -1, int next_chunk = 0, bool* did_prefetch = nullptr) {
+                                          const unsigned* band_tbl, unsigned ph[2]) {
   using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
   constexpr int TX = G::TX, TY = G::TY, TZ = G::TZ;
@@ -293,50 +284,43 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // address of each row at array time 0 (0 for rows outside the mesh) and
   // the bytes of a row's local vertices
   constexpr int RPL = (G::ROWS + 31) / 32;
-  // row sources of a tile with origin (ox, oy, oz): warp 0's lanes only
-  auto row_sources = [&](int ox, int oy, int oz, uintptr_t (&out)[RPL]) {
-#pragma unroll
-    for (int i = 0; i < RPL; ++i) {
-      out[i] = 0;
-      const int r = lane + 32 * i;
-      if (bulk && warp == 0 && r < G::ROWS) {
-        const int rr = MULTI ? r : r % (VY * VZ);
-        const int j = MULTI ? 0 : r / (VY * VZ);
-        const int vy = rr % VY, vz = rr / VY;
-        if (oy + vy < ldy && (D == 3 || oz + vz < ldz)) {
-          long long e = (long long)(ox + aoff[0]) * fa.estride[0] + (long long)(oy + vy + aoff[1]) * fa.estride[1];
-          if (D == 4) e += (long long)(oz + vz + aoff[2]) * fa.estride[2];
-          out[i] = reinterpret_cast<uintptr_t>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2])) +
-                   (uintptr_t)(e * (long long)sizeof(T));
-        }
-      }
-    }
-  };
   uintptr_t rsrc[RPL];
   const int rbytes = min(VX, ldx - x0) * (MULTI ? M : 1) * (int)sizeof(T);
-  row_sources(x0, y0, z0, rsrc);
+#pragma unroll
+  for (int i = 0; i < RPL; ++i) {
+    rsrc[i] = 0;
+    const int r = lane + 32 * i;
+    if (bulk && warp == 0 && r < G::ROWS) {
+      const int rr = MULTI ? r : r % (VY * VZ);
+      const int j = MULTI ? 0 : r / (VY * VZ);
+      const int vy = rr % VY, vz = rr / VY;
+      if (y0 + vy < ldy && (D == 3 || z0 + vz < ldz)) {
+        long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
+        if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
+        rsrc[i] = reinterpret_cast<uintptr_t>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2])) +
+                  (uintptr_t)(e * (long long)sizeof(T));
+      }
+    }
+  }
 
   // ---- slice staging
-  // the mbarrier stagings of slice s of the tile at (ox, oy, oz) into buffer
-  // buf: one TMA box per array (thread 0), or bulk row copies (warp 0, row
-  // sources rs, rb bytes of local vertices per row)
-  auto mbar_issue = [&](int s, int buf, int ox, int oy, int oz, const uintptr_t (&rs)[RPL], int rb) {
+  auto issue = [&](int s, int buf) {
     unsigned char* dst0 = smem + buf * G::BYTES;
     if constexpr (TMA) {
       if (tid == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(&bar[buf], G::TX_BYTES);
-        const int cx = (ox + aoff[0]) * (MULTI ? M : 1);
-        const int cy = oy + aoff[1];
+        const int cx = (x0 + aoff[0]) * (MULTI ? M : 1);
+        const int cy = y0 + aoff[1];
         if constexpr (MULTI) {
-          if constexpr (D == 4) tma_load_4d(dst0, map0, cx, cy, oz + aoff[2], tcoord(s), &bar[buf]);
+          if constexpr (D == 4) tma_load_4d(dst0, map0, cx, cy, z0 + aoff[2], tcoord(s), &bar[buf]);
           else tma_load_3d(dst0, map0, cx, cy, tcoord(s), &bar[buf]);
         } else {
           const CUtensorMap* maps[3] = {map0, map1, map2};
 #pragma unroll
           for (int j = 0; j < M; ++j) {
             if constexpr (D == 4)
-              tma_load_4d(dst0 + j * G::COMP, maps[j], cx, cy, oz + aoff[2], tcoord(s), &bar[buf]);
+              tma_load_4d(dst0 + j * G::COMP, maps[j], cx, cy, z0 + aoff[2], tcoord(s), &bar[buf]);
             else
               tma_load_3d(dst0 + j * G::COMP, maps[j], cx, cy, tcoord(s), &bar[buf]);
           }
@@ -355,9 +339,9 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
         unsigned nb[RPL];
 #pragma unroll
         for (int i = 0; i < RPL; ++i) {
-          const uintptr_t src = rs[i] + tb;
+          const uintptr_t src = rsrc[i] + tb;
           lo[i] = src & ~(uintptr_t)15;
-          nb[i] = rs[i] ? (unsigned)(((src + (uintptr_t)rb + 15) & ~(uintptr_t)15) - lo[i]) : 0u;
+          nb[i] = rsrc[i] ? (unsigned)(((src + (uintptr_t)rbytes + 15) & ~(uintptr_t)15) - lo[i]) : 0u;
           total += nb[i];
         }
 #pragma unroll
@@ -369,15 +353,9 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
         for (int i = 0; i < RPL; ++i)
           if (nb[i]) bulk_load(dst0 + (lane + 32 * i) * G::ROWB, reinterpret_cast<const void*>(lo[i]), nb[i], &bar[buf]);
       }
-    }
-  };
-  auto issue = [&](int s, int buf) {
-    if (mbar) {
-      mbar_issue(s, buf, x0, y0, z0, rsrc, rbytes);
     } else {
       // per-thread asynchronous element copies into the same layout (zeros
       // outside the array), one commit group per slice
-      unsigned char* dst0 = smem + buf * G::BYTES;
       T* dst = reinterpret_cast<T*>(dst0);
       constexpr int NPER = G::VXBOX * VY * VZ;
       if (!fa.per_vertex) {
@@ -487,32 +465,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // hypercube's 2^D vertices then take 2^(D-1) shared-memory words.
   unsigned prev[VPT];
 
-  // the next item's first two slices into the free buffers (see above)
-  const bool can_prefetch = mbar && next_tile >= 0;
-  auto prefetch_next = [&]() {
-    if (!can_prefetch) return;
-    int nt = next_tile;
-    const int nx0 = (nt % cfg.tiles[0]) * TX;
-    nt /= cfg.tiles[0];
-    const int ny0 = (nt % cfg.tiles[1]) * TY;
-    nt /= cfg.tiles[1];
-    const int nz0 = (D == 4) ? nt * TZ : 0;
-    const int n_t0 = next_chunk * cfg.tchunk;
-    const int n_send = min(min(n_t0 + cfg.tchunk, lt), lt - 1);
-    uintptr_t nrs[RPL];
-    row_sources(nx0, ny0, nz0, nrs);
-    const int nrb = min(VX, ldx - nx0) * (MULTI ? M : 1) * (int)sizeof(T);
-    mbar_issue(n_t0, 0, nx0, ny0, nz0, nrs, nrb);
-    if (n_t0 + 1 <= n_send) mbar_issue(n_t0 + 1, 1, nx0, ny0, nz0, nrs, nrb);
-    if (did_prefetch) *did_prefetch = true;
-  };
-
   // the previous tile of a persistent block is done with every buffer
   __syncthreads();
-  if (!prefetched) {
-    issue(t0, 0);
-    if (t0 + 1 <= s_end) issue(t0 + 1, 1);
-  }
+  issue(t0, 0);
+  if (t0 + 1 <= s_end) issue(t0 + 1, 1);
   {
     bool ok = wait(t0, 0);
     // failure-path check (host option): after the first slice has landed,
@@ -528,7 +484,6 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     }
   }
   if (t0 + 2 <= s_end) issue(t0 + 2, 0);
-  if (s_end == t0) prefetch_next();  // one slice: its buffer is free already
 
   // corner validity per (lane, row) does not change along time
   const int cyw = (D == 4) ? warp % TY : warp * kRows;
@@ -572,7 +527,6 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       return false;
     }
     if (s + 2 <= s_end) issue(s + 2, (s - t0) & 1);
-    if (s == s_end) prefetch_next();  // the item's last slice is in words: both buffers are free
     if (!has_rows) continue;
 
     // ---- hypercube cull: lanes along x, kRows corner rows per warp
@@ -2189,32 +2143,32 @@ __global__ void __launch_bounds__(kThreads, 2)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   unsigned ph[2] = {0u, 0u};
-  // thread 0 takes the next item from the counter and finds its field (the
-  // last field whose first item is <= the item)
-  auto fetch = [&]() {
-    const unsigned it = atomicAdd(item_next, 1u);
-    unsigned f = 0;
-    if (it < n_items) {
-      unsigned lo = 0, hi = (unsigned)nf;
-      while (hi - lo > 1) {
-        const unsigned mid = (lo + hi) >> 1;
-        if (ib[mid] <= it) lo = mid;
-        else hi = mid;
+  for (;;) {
+    __syncthreads();  // s_item of the previous item has been read by every thread
+    if (threadIdx.x == 0) {
+      const unsigned it = atomicAdd(item_next, 1u);
+      unsigned f = 0;
+      if (it < n_items) {
+        // the last field whose first item is <= it
+        unsigned lo = 0, hi = (unsigned)nf;
+        while (hi - lo > 1) {
+          const unsigned mid = (lo + hi) >> 1;
+          if (ib[mid] <= it) lo = mid;
+          else hi = mid;
+        }
+        f = lo;
       }
-      f = lo;
+      s_item = it;
+      s_field = f;
     }
-    s_item = it;
-    s_field = f;
-  };
-  if (threadIdx.x == 0) fetch();
-  __syncthreads();
-  unsigned it = s_item, f = s_field, cur_f = 0xFFFFFFFFu;
-  bool prefetched = false;  // this item's first two slices were issued by the previous call
-  while (it < n_items) {
+    __syncthreads();
+    const unsigned it = s_item;
+    if (it >= n_items) break;
+    const unsigned f = s_field;
     const BatchField& F = fields[f];
-    if (f != cur_f) {
-      // the field's mesh, access and configuration into shared memory (the
-      // tensor maps stay in global memory, where TMA reads them)
+    // the field's mesh, access and configuration into shared memory (the
+    // tensor maps stay in global memory, where TMA reads them)
+    {
       constexpr int kMw = sizeof(RegularMesh) / 4, kFw = sizeof(FieldAccess) / 4, kCw = sizeof(ExtractConfig) / 4;
       const unsigned* src_m = reinterpret_cast<const unsigned*>(&F.mesh);
       const unsigned* src_f = reinterpret_cast<const unsigned*>(&F.fa);
@@ -2227,44 +2181,29 @@ __global__ void __launch_bounds__(kThreads, 2)
         s_tma = F.tma;
         s_ibase = F.item_base;
       }
-      cur_f = f;
     }
-    if (threadIdx.x == 0) fetch();  // the item after this one
-    __syncthreads();                 // the record and the next item are visible
-    const unsigned nit = s_item, nfld = s_field;
+    __syncthreads();
     const unsigned local = it - s_ibase;
     const unsigned ntiles = (unsigned)s_cfg.tiles[0] * s_cfg.tiles[1] * s_cfg.tiles[2];
-    // the next item's first slices are prefetched when it belongs to the same field
-    int next_tile = -1, next_chunk = 0;
-    if (nit < n_items && nfld == f) {
-      const unsigned nl = nit - s_ibase;
-      next_tile = (int)(nl % ntiles);
-      next_chunk = (int)(nl / ntiles);
-    }
     CandidateQueue q = cq;
     q.field_id = f;
-    const int tile = (int)(local % ntiles), chunk = (int)(local / ntiles);
-    bool ok, did = false;
+    bool ok;
     if (s_mesh.d == 4) {
       ok = s_tma ? cull_tile<T, 4, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
-                                                tile, chunk, smem, bar, band_tbl, ph, prefetched, next_tile,
-                                                next_chunk, &did)
+                                                (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                ph)
                  : cull_tile<T, 4, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
-                                                 tile, chunk, smem, bar, band_tbl, ph, prefetched, next_tile,
-                                                 next_chunk, &did);
+                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                 ph);
     } else {
       ok = s_tma ? cull_tile<T, 3, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
-                                                tile, chunk, smem, bar, band_tbl, ph, prefetched, next_tile,
-                                                next_chunk, &did)
+                                                (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                ph)
                  : cull_tile<T, 3, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
-                                                 tile, chunk, smem, bar, band_tbl, ph, prefetched, next_tile,
-                                                 next_chunk, &did);
+                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
+                                                 ph);
     }
     if (!ok) break;  // the whole block saw the failed wait
-    prefetched = did;
-    __syncthreads();  // every thread has read the item slots and the record
-    it = nit;
-    f = nfld;
   }
 }
 
