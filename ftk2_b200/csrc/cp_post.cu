@@ -257,6 +257,23 @@ __device__ __forceinline__ long long find_key(const unsigned long long* keys, un
   return -1;
 }
 
+// find_key over n sorted keys in global memory with a sample of every
+// 2^slog-th key in shared memory: the sample's binary search picks the run of
+// 2^slog keys that can hold k, then a binary search inside that run.
+__device__ __forceinline__ long long find_key_sampled(const unsigned long long* keys, unsigned n,
+                                                      const unsigned long long* sample, unsigned ns, int slog,
+                                                      unsigned long long k) {
+  unsigned lo = 0, hi = ns;  // the last run whose first key is <= k
+  while (hi - lo > 1) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (sample[mid] <= k) lo = mid;
+    else hi = mid;
+  }
+  const unsigned r0 = lo << slog, r1 = min(r0 + (1u << slog), n);
+  const long long j = find_key(keys + r0, r1 - r0, k);
+  return j < 0 ? -1 : (long long)r0 + j;
+}
+
 // Indices of the active faces of a top cell, ascending.
 __device__ int active_faces(const RegularMesh& mesh, int nch, const unsigned long long* keys,
                             unsigned n, const long long cc[4], const int cm[5], long long out[5]) {
@@ -652,7 +669,9 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
                                                 unsigned n, unsigned i, unsigned long long local_key,
                                                 unsigned long long kbase, const StarTables& T, int lane,
                                                 unsigned* __restrict__ cnt, unsigned* __restrict__ slots,
-                                                unsigned* parent, unsigned* err) {
+                                                unsigned* parent, unsigned* err,
+                                                const unsigned long long* sample = nullptr, unsigned ns = 0,
+                                                int slog = 0) {
   const int d = mesh.d, m = d - 1, full = (1 << d) - 1;
   unsigned long long rem;
   unsigned long long vid = divmod_u64(local_key, (unsigned long long)nch, rem);
@@ -734,7 +753,8 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       if (k < d) fvid += (unsigned long long)(c[k] + ((base >> k) & 1u)) * mesh.gstride[k];
-    idx = find_key(keys, n, kbase + fvid * (unsigned long long)nch + (unsigned long long)T.rank[rel]);
+    const unsigned long long fk = kbase + fvid * (unsigned long long)nch + (unsigned long long)T.rank[rel];
+    idx = sample ? find_key_sampled(keys, n, sample, ns, slog, fk) : find_key(keys, n, fk);
   }
   const unsigned act = __ballot_sync(0xFFFFFFFFu, idx >= 0);
   bool qual[2] = {false, false};
@@ -764,14 +784,20 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
 
 // Batches: one warp per feature (the short chain's star_edges_warp with the
 // feature's field, found by its key).
+// The keys live in global memory; every block keeps every 2^slog-th of them
+// in shared memory (dynamic, (n >> slog) + 1 entries) for the lookups.
 __global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const unsigned long long* __restrict__ kb,
                                         int nf, const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
-                                        unsigned cap, unsigned* __restrict__ cnt, unsigned* __restrict__ slots) {
+                                        unsigned cap, unsigned* __restrict__ cnt, unsigned* __restrict__ slots,
+                                        int slog) {
+  extern __shared__ unsigned long long sample[];
   __shared__ StarTables T[2];  // d = 3, d = 4
   fill_star_tables(T[0], 3);
   fill_star_tables(T[1], 4);
-  __syncthreads();
   const unsigned n = min(*n_ptr, cap);
+  const unsigned ns = (n + (1u << slog) - 1) >> slog;
+  for (unsigned j = threadIdx.x; j < ns; j += blockDim.x) sample[j] = keys[(size_t)j << slog];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned nw = (gridDim.x * blockDim.x) >> 5;
@@ -780,7 +806,7 @@ __global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const 
     const unsigned f = batch_field_of(kb, nf, key);
     const RegularMesh mesh = fm[f].mesh;
     star_edges_warp(mesh, fm[f].nch, keys, n, i, key - kb[f], kb[f], T[mesh.d - 3], lane, cnt, slots, nullptr,
-                    nullptr);
+                    nullptr, sample, ns, slog);
   }
 }
 
@@ -1086,9 +1112,16 @@ cudaError_t launch_post_batch(const BatchMesh* fm, const unsigned long long* kb,
                                    B.bary4_sorted);
   expand_batch_kernel<<<g, 256, 0, st>>>(fm, kb, nf, skey, B.count, cap, B.bary4_sorted, B.simplices, B.bary);
   batch_bounds_kernel<<<(nf + 256) / 256, 256, 0, st>>>(kb, nf, skey, B.count, cap, fbase);
-  // a persistent grid: every block copies the face tables into shared memory once
-  edges_batch_warp_kernel<<<(B.num_sms > 0 ? B.num_sms : 148) * 2, 512, 0, st>>>(fm, kb, nf, skey, B.count, cap,
-                                                                                  B.edge_cnt, B.edge_slots);
+  // a persistent grid: every block copies the face tables and a sample of
+  // the sorted keys (every 2^slog-th, at most 8192 entries) into shared memory once
+  {
+    int slog = 4;
+    while (((unsigned long long)cap >> slog) + 1 > 8192ull) ++slog;
+    const size_t smp = sizeof(unsigned long long) * (((size_t)cap >> slog) + 1);
+    cudaFuncSetAttribute(edges_batch_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
+    edges_batch_warp_kernel<<<(B.num_sms > 0 ? B.num_sms : 148) * 2, 512, smp, st>>>(fm, kb, nf, skey, B.count, cap,
+                                                                                      B.edge_cnt, B.edge_slots, slog);
+  }
   scan_inplace_kernel<<<1, 1024, 0, st>>>(B.edge_cnt, cap, B.n_edges, B.count, nullptr);
   edges_compact_kernel<<<g, 256, 0, st>>>(B.count, cap, B.edge_cnt, B.n_edges, B.edge_slots, B.edges, B.edge_cap);
   uf_init_kernel<<<g, 256, 0, st>>>(B.parent, B.count, cap);

@@ -151,6 +151,9 @@ template <> struct Tile<3> {
 };
 
 constexpr int kThreads = 512;
+// surviving hypercubes a block collects in shared memory before it reserves
+// queue space for all of them with one atomic (more go to the queue directly)
+constexpr int kCandBuf = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRows = 2;  // corner rows a warp culls per step
 
@@ -189,7 +192,9 @@ struct Geo {
   static constexpr int TX_BYTES = COMP_RAW * M;                          // bytes TMA delivers
   static constexpr int COMP_ELEMS = COMP / (int)sizeof(T);
   static constexpr int WORDS = 2 * BYTES;                                // offset of the word slots
-  static constexpr int SMEM = WORDS + 2 * VSP * 4;
+  // the block's candidate buffer (corner, chains) and its count, after the word slots
+  static constexpr int CAND = WORDS + 2 * VSP * 4;
+  static constexpr int SMEM = CAND + 16 * kCandBuf + 16;
 };
 
 __device__ __forceinline__ unsigned long long pack_corner(long long x, long long y, long long z,
@@ -465,6 +470,9 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // hypercube's 2^D vertices then take 2^(D-1) shared-memory words.
   unsigned prev[VPT];
 
+  unsigned long long* const cbuf = reinterpret_cast<unsigned long long*>(smem + G::CAND);
+  unsigned* const ccount = reinterpret_cast<unsigned*>(smem + G::CAND + 16 * kCandBuf);
+  if (tid == 0) ccount[0] = 0;
   // the previous tile of a persistent block is done with every buffer
   __syncthreads();
   issue(t0, 0);
@@ -554,29 +562,51 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       const unsigned ball = __ballot_sync(0xFFFFFFFFu, keep);
       if (ball) {
         // surviving hypercubes are queued with every chain that fits in the
-        // mesh; the exact-test kernel applies the per-simplex word test
+        // mesh (the exact-test kernel applies the per-simplex word test),
+        // first into the block's buffer
         unsigned basei = 0;
-        if (lane == 0) basei = atomicAdd(cq.count, (unsigned)__popc(ball));
+        if (lane == 0) basei = atomicAdd(ccount, (unsigned)__popc(ball));
         basei = __shfl_sync(0xFFFFFFFFu, basei, 0);
         if (keep) {
           const unsigned idx = basei + __popc(ball & ((1u << lane) - 1));
-          if (idx < cq.cap) {
-            const int l0 = x0 + lane, l1 = y0 + cy, l2 = (D == 4) ? z0 + cz : ct;
-            int vmask = 0;  // axes along which the corner can step by +1
-            if (l0 + 1 < ldx) vmask |= 1;
-            if (l1 + 1 < ldy) vmask |= 2;
-            if (D == 4 && l2 + 1 < ldz) vmask |= 4;
-            if (ct + 1 < lt) vmask |= TBIT;
-            cq.corner[idx] = pack_corner(l0, l1, (D == 4) ? l2 : 0, ct);
-            if (cq.field) cq.field[idx] = cq.field_id;
-            unsigned long long ch = c_chains_by_vmask[D - 3][vmask];
-            // a stream's window starts one slice before the new timestep: the
-            // purely spatial simplices of that slice were counted already
-            if (cfg.skip_first_spatial && ct == 0) ch &= c_time_chains[D - 3];
-            cq.chains[idx] = ch;
+          const int l0 = x0 + lane, l1 = y0 + cy, l2 = (D == 4) ? z0 + cz : ct;
+          int vmask = 0;  // axes along which the corner can step by +1
+          if (l0 + 1 < ldx) vmask |= 1;
+          if (l1 + 1 < ldy) vmask |= 2;
+          if (D == 4 && l2 + 1 < ldz) vmask |= 4;
+          if (ct + 1 < lt) vmask |= TBIT;
+          const unsigned long long corner = pack_corner(l0, l1, (D == 4) ? l2 : 0, ct);
+          unsigned long long ch = c_chains_by_vmask[D - 3][vmask];
+          // a stream's window starts one slice before the new timestep: the
+          // purely spatial simplices of that slice were counted already
+          if (cfg.skip_first_spatial && ct == 0) ch &= c_time_chains[D - 3];
+          if (idx < kCandBuf) {
+            cbuf[2 * idx] = corner;
+            cbuf[2 * idx + 1] = ch;
+          } else {
+            const unsigned gi = atomicAdd(cq.count, 1u);
+            if (gi < cq.cap) {
+              cq.corner[gi] = corner;
+              cq.chains[gi] = ch;
+              if (cq.field) cq.field[gi] = cq.field_id;
+            }
           }
         }
       }
+    }
+  }
+  // the block's buffered candidates into the queue: one reservation
+  __syncthreads();
+  const unsigned nc = min(ccount[0], (unsigned)kCandBuf);
+  if (tid == 0) ccount[1] = nc ? atomicAdd(cq.count, nc) : 0u;
+  __syncthreads();
+  const unsigned cbase = ccount[1];
+  for (unsigned i = tid; i < nc; i += kThreads) {
+    const unsigned gi = cbase + i;
+    if (gi < cq.cap) {
+      cq.corner[gi] = cbuf[2 * i];
+      cq.chains[gi] = cbuf[2 * i + 1];
+      if (cq.field) cq.field[gi] = cq.field_id;
     }
   }
   if (mbar) {
