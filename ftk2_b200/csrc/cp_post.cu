@@ -917,13 +917,12 @@ __global__ void __launch_bounds__(kSortThreads, 1)
 
 // The short chain's last step, by one block of 1024 threads: exclusive scan
 // of the edge counts, edge compaction, every feature's root from the union-find
-// parents (copied to shared memory), track ids and root count.  sh: (2n + 1)
-// words of shared memory.
+// parents (copied to shared memory), track ids and root count.  sh: n words
+// of shared memory.
 __device__ __forceinline__ void finish_block(const PostBuffers& B, unsigned* sh, unsigned* wsum, unsigned& s_roots) {
   constexpr int kPer = (int)(kSmallPostCap / 1024);  // features per thread, at most
   const unsigned n = min(*B.count, B.cap);
-  unsigned* const off = sh;
-  unsigned* const sp = sh + n + 1;
+  unsigned* const sp = sh;  // the union-find parents
   const unsigned t = threadIdx.x;
   // exclusive scan of the per-feature edge counts: each thread's contiguous
   // segment, its counts loaded first (independent loads)
@@ -941,31 +940,23 @@ __device__ __forceinline__ void finish_block(const PostBuffers& B, unsigned* sh,
   if (t == 0) s_roots = 0;
   unsigned total;
   unsigned run = block_exclusive_scan(sum, wsum, &total);
+  if (t == 0) *B.n_edges = total;
+  // the edges of each thread's contiguous run of features at their scanned
+  // offsets: the counts are in registers, the slots contiguous in memory
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
-    if (k < (int)seg && s0 + k < n) off[s0 + k] = run;
+    const unsigned i = s0 + k;
+    if (k < (int)seg && i < n) {
+      for (unsigned r = 0; r < c[k]; ++r) {
+        const unsigned other = __ldcg(&B.edge_slots[(size_t)i * kEdgeSlots + r]);
+        const unsigned e = run + r;
+        if (e < B.edge_cap) {
+          B.edges[2 * (size_t)e] = i;
+          B.edges[2 * (size_t)e + 1] = other;
+        }
+      }
+    }
     run += c[k];
-  }
-  if (t == 0) {
-    off[n] = total;
-    *B.n_edges = total;
-  }
-  __syncthreads();
-  // every edge by its own thread: the feature whose offset range holds it
-  // (binary search in shared memory), its slot, the output pair
-#pragma unroll 4
-  for (unsigned e = t; e < total; e += 1024) {
-    unsigned lo = 0, hi = n;  // the last i with off[i] <= e
-    while (hi - lo > 1) {
-      const unsigned mid = (lo + hi) >> 1;
-      if (off[mid] <= e) lo = mid;
-      else hi = mid;
-    }
-    const unsigned other = __ldcg(&B.edge_slots[(size_t)lo * kEdgeSlots + (e - off[lo])]);
-    if (e < B.edge_cap) {
-      B.edges[2 * (size_t)e] = lo;
-      B.edges[2 * (size_t)e + 1] = other;
-    }
   }
   // every feature's root (the minimum of its component) by pointer jumping:
   // each round replaces every parent by its parent's parent, halving every

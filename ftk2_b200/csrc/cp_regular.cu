@@ -1773,13 +1773,17 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 4) refine_test_kernel(Regul
   __syncthreads();
   const unsigned n = min(*cq.count, cq.cap);
   for (unsigned first = blockIdx.x * kTestCands; first < n; first += gridDim.x * kTestCands) {
-#pragma unroll 1
+    // every pass's loads first (corners, then the vertices' components, as
+    // read-only global loads), so that the passes' memory latencies overlap
+    unsigned long long chains_p[PASSES];
+    bool in_p[PASSES];
+    T x_p[PASSES][M];
+#pragma unroll
     for (int pass = 0; pass < PASSES; ++pass) {
-      const int k = pass * PER_PASS + slot;
-      const unsigned c = first + k;
+      const unsigned c = first + pass * PER_PASS + slot;
       const bool has = c < n;
-      const unsigned long long pc = has ? cq.corner[c] : 0ull;
-      const unsigned long long chains = has ? cq.chains[c] : 0ull;
+      const unsigned long long pc = has ? __ldg(&cq.corner[c]) : 0ull;
+      chains_p[pass] = has ? __ldg(&cq.chains[c]) : 0ull;
       const long long l[4] = {(long long)(pc & 0xFFFF), (long long)((pc >> 16) & 0xFFFF),
                               (long long)((pc >> 32) & 0xFFFF), (long long)(pc >> 48)};
       long long g[4];
@@ -1807,12 +1811,24 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 4) refine_test_kernel(Regul
       } else {
         o = (long long)vid;
       }
+      in_p[pass] = in;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
+        x_p[pass][j] = in ? __ldg(src + o) : T(0);
+      }
+    }
+#pragma unroll
+    for (int pass = 0; pass < PASSES; ++pass) {
+      const int k = pass * PER_PASS + slot;
+      const unsigned c = first + k;
+      const bool has = c < n, in = in_p[pass];
+      const unsigned long long chains = chains_p[pass];
       unsigned h[M];
       bool big = false;
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
-        T x = in ? src[o] : T(0);
+        T x = x_p[pass][j];
         if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
         h[j] = hi_word<T>(x);
         const int qv = quant_small_p(quant_p((double)x, cfg.Q));
