@@ -811,8 +811,29 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
         e.key = key;
         e.gen = gen;
         unsigned long long nl = 0;
+        // one graph for the whole pipeline, the call's three timing events
+        // captured as event-record nodes; two graphs with the events recorded
+        // between their launches when that capture fails
+        {
+          cudaGraph_t graph = nullptr;
+          CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+          cudaError_t ce = cudaEventRecordWithFlags(ctx->ev0, ctx->stream, cudaEventRecordExternal);
+          if (!ce) ce = enqueue1(&nl);
+          if (!ce) ce = cudaEventRecordWithFlags(ctx->ev_x, ctx->stream, cudaEventRecordExternal);
+          if (!ce) ce = enqueue2(&nl);
+          if (!ce) ce = cudaEventRecordWithFlags(ctx->ev1, ctx->stream, cudaEventRecordExternal);
+          const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
+          if (!ce && !ee && cudaGraphInstantiate(&e.g1, graph, 0) == cudaSuccess) {
+            cudaGraphDestroy(graph);
+          } else {
+            if (graph) cudaGraphDestroy(graph);
+            e.g1 = nullptr;
+            nl = 0;
+            cudaGetLastError();
+          }
+        }
         cudaGraphExec_t* slots[2] = {&e.g1, &e.g2};
-        for (int part = 0; part < 2; ++part) {
+        for (int part = 0; part < 2 && !(part == 0 && e.g1); ++part) {
           cudaGraph_t graph = nullptr;
           CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
           cudaError_t ce = part == 0 ? enqueue1(&nl) : enqueue2(&nl);
@@ -840,11 +861,15 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       ctx->last_used_tma = ent->used_tma;
       p2 = Clk::now();
       ctx->phase_ms[1] += msd(p1, p2);
-      CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-      CUDA_TRY(ctx, cudaGraphLaunch(ent->g1, ctx->stream));
-      CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
-      CUDA_TRY(ctx, cudaGraphLaunch(ent->g2, ctx->stream));
-      CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+      if (ent->g2) {
+        CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+        CUDA_TRY(ctx, cudaGraphLaunch(ent->g1, ctx->stream));
+        CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
+        CUDA_TRY(ctx, cudaGraphLaunch(ent->g2, ctx->stream));
+        CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+      } else {
+        CUDA_TRY(ctx, cudaGraphLaunch(ent->g1, ctx->stream));  // the event records are nodes of the graph
+      }
       ctx->launches += ent->launches;
     } else {
       unsigned long long nl = 0;
