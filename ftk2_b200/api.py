@@ -26,11 +26,13 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libftk2b.so")
+# the build with the device bounds checks compiled in (FTK2B_CHECKED=1 loads it)
+CHECKED_LIB_PATH = os.path.join(HERE, "_lib", "checked", "libftk2b.so")
 
 # enums of include/ftk2b.h
-OK, INVALID_ARG, OOM, CUDA_ERROR, TIMEOUT, OVERFLOW_RETRY, NO_DEVICE, UNSUPPORTED, BUSY = range(9)
+OK, INVALID_ARG, OOM, CUDA_ERROR, TIMEOUT, OVERFLOW_RETRY, NO_DEVICE, UNSUPPORTED, BUSY, INTERNAL = range(10)
 STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "CUDA_ERROR", "TIMEOUT", "OVERFLOW_RETRY", "NO_DEVICE",
-                "UNSUPPORTED", "BUSY"]
+                "UNSUPPORTED", "BUSY", "INTERNAL"]
 MESH_REGULAR, MESH_EXTRUDED = 0, 1
 F32, F64 = 0, 1
 LAYOUT_MULTICOMPONENT, LAYOUT_SEPARATE, LAYOUT_PER_VERTEX = 0, 1, 2
@@ -202,12 +204,15 @@ SIGNATURES = {
 _lib: Optional[C.CDLL] = None
 
 
-def load_library(path: str = LIB_PATH) -> C.CDLL:
-    """Load libftk2b.so and bind every exported entry point.  Raises if the
-    library has not been built: the path has no CPU fallback."""
+def load_library(path: Optional[str] = None) -> C.CDLL:
+    """Load libftk2b.so and bind every exported entry point (the checked build
+    when the environment sets FTK2B_CHECKED=1).  Raises if the library has
+    not been built: the path has no CPU fallback."""
     global _lib
     if _lib is not None:
         return _lib
+    if path is None:
+        path = CHECKED_LIB_PATH if os.environ.get("FTK2B_CHECKED") == "1" else LIB_PATH
     if not os.path.exists(path):
         raise RuntimeError(f"CUDA library not built: {path} (run __graft_entry__.build())")
     lib = C.CDLL(path)

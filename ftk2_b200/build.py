@@ -37,27 +37,38 @@ def _headers() -> list[str]:
         glob.glob(os.path.join(ROOT, "include", "*.h"))
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(OBJ_DIR, exist_ok=True)
+# The checked build: the same sources with the device bounds checks compiled
+# in (-DFTK2B_CHECKED: a failed index check sets an error bit and the call
+# returns FTK2B_INTERNAL), loaded instead of LIB when FTK2B_CHECKED=1.
+CHECKED_DIR = os.path.join(OUT_DIR, "checked")
+CHECKED_LIB = os.path.join(CHECKED_DIR, "libftk2b.so")
+
+
+def build(verbose: bool = False, checked: bool = False) -> str:
+    out_dir = CHECKED_DIR if checked else OUT_DIR
+    obj_dir = os.path.join(out_dir, "obj")
+    lib = CHECKED_LIB if checked else LIB
+    flags = NVCC_FLAGS + (["-DFTK2B_CHECKED"] if checked else [])
+    os.makedirs(obj_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdr_mtime = max((os.path.getmtime(h) for h in _headers()), default=0)
     objs = []
     for src in srcs:
-        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         objs.append(obj)
         if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_mtime):
             continue
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", src, "-o", obj]
+        cmd = [nvcc()] + ARCH + flags + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     newest = max(os.path.getmtime(o) for o in objs)
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if not os.path.exists(lib) or os.path.getmtime(lib) < newest:
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 DROPIN_SRC = os.path.join(ROOT, "tests", "cpp", "dropin_c1.cpp")

@@ -718,6 +718,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     // memory and reads the field again for the solve: no staging block
     refine_stage_bind(rs, nullptr, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64, cap);
     rs.count = (unsigned*)ctx->counters.p + kCountPairs;
+    rs.err = (unsigned*)ctx->counters.p + kCountErr;
     rs.big_count = (unsigned*)ctx->counters.p + kCountBig;
     rs.acc_count = (unsigned*)ctx->counters.p + kCountAcc;
     const int f64 = field->dtype == FTK2B_F64;
@@ -751,6 +752,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     };
     if (cfg.cull_mode == 2) {
       int mode = 0;
+      NvtxRange tune_range("ftk2b_tune_cull_mode");
       CUDA_TRY(ctx, resolve_cull_mode(ctx, rm, fa, f64, field->layout == FTK2B_LAYOUT_MULTICOMPONENT,
                                       [&](int md) -> cudaError_t {
                                         ExtractConfig c = cfg;
@@ -799,6 +801,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
         ++it;
       }
       if (!ent) {
+        NvtxRange capture_range("ftk2b_capture_pipeline");
         if (ctx->graphs.size() >= kMaxGraphs) {
           auto lru = ctx->graphs.begin();
           for (auto it = ctx->graphs.begin(); it != ctx->graphs.end(); ++it)
@@ -880,7 +883,10 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
       ctx->launches += nl;
     }
-    CUDA_TRY(ctx, ctx->sync());
+    {
+      NvtxRange wait_range("ftk2b_pipeline_wait");
+      CUDA_TRY(ctx, ctx->sync());
+    }
     ctx->phase_ms[2] += msd(p2, Clk::now());
     unsigned h[kNumCounters];
     memcpy(h, ctx->h_counters, sizeof(h));
@@ -891,6 +897,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     ctx->last_extract_ms = xms;
     ctx->last_candidates = h[kCountCand];
     ctx->last_tested = h[kCountPairs];
+    if (h[kCountErr] & kErrBounds) return fail(ctx, FTK2B_INTERNAL, "a device bounds check failed (checked build)");
     if (h[kCountErr] & 2u) return fail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return fail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
     if (h[kCountCand] > ccap) {
@@ -929,6 +936,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
 extern "C" ftk2b_status ftk2b_cp_run(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                      const ftk2b_field_desc* field, const ftk2b_cp_params* params,
                                      uint64_t* n_features, uint64_t* n_edges) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_cp_run");
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field) return fail(ctx, FTK2B_INVALID_ARG, "null descriptor");
   ftk2b_cp_params prm = params ? *params : ftk2b_cp_params_default();
@@ -946,6 +954,7 @@ extern "C" ftk2b_status ftk2b_cp_run(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh
 }
 
 extern "C" ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_cp_fetch");
   if (!ctx || !out) return FTK2B_INVALID_ARG;
   const auto f0 = std::chrono::steady_clock::now();
   struct PhaseTimer {
@@ -1010,6 +1019,7 @@ extern "C" ftk2b_status ftk2b_cp_fetch(ftk2b_ctx* ctx, ftk2b_cp_result** out) {
 extern "C" ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                             const ftk2b_field_desc* field, const double thresholds[2],
                                             double sos_q, ftk2b_cp_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_fiber_extract");
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field || !thresholds || !out) return fail(ctx, FTK2B_INVALID_ARG, "null argument");
   *out = nullptr;
@@ -1033,6 +1043,7 @@ extern "C" ftk2b_status ftk2b_fiber_extract(ftk2b_ctx* ctx, const ftk2b_mesh_des
 extern "C" ftk2b_status ftk2b_cp_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                          const ftk2b_field_desc* field, const ftk2b_cp_params* params,
                                          ftk2b_cp_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_cp_extract");
   if (!out) return ctx ? fail(ctx, FTK2B_INVALID_ARG, "null output") : FTK2B_INVALID_ARG;
   *out = nullptr;
   ftk2b_status st = ftk2b_cp_run(ctx, mesh, field, params, nullptr, nullptr);

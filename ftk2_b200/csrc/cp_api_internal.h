@@ -6,11 +6,23 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/ftk2b.h"
 #include "cp_internal.h"
 #include "cp_post.h"
 
 namespace ftk2b {
+
+// NVTX range over a scope (a profiler such as Nsight Systems shows the
+// library's stages on the host timeline; without one attached the calls do
+// nothing)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // grow-only device allocation owned by a context.  With `st` set, memory is
 // allocated and freed in stream order on that stream (the only stream that

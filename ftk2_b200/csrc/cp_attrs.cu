@@ -134,6 +134,7 @@ ftk2b_status afail(ftk2b_ctx* ctx, ftk2b_status st, const char* fmt, ...) {
 extern "C" ftk2b_status ftk2b_cp_attributes(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                             const uint64_t* base_grid_dims, uint32_t n_attrs,
                                             const ftk2b_attribute_desc* attrs, float* out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_cp_attributes");
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || (n_attrs && !attrs) || !out) return afail(ctx, FTK2B_INVALID_ARG, "null argument");
   if (n_attrs > 16) return afail(ctx, FTK2B_INVALID_ARG, "at most 16 attributes");

@@ -300,6 +300,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     RefineStage rs;
     refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, f64, cap);
     rs.count = counters + kCountPairs;
+    rs.err = counters + kCountErr;
     rs.big_count = counters + kCountBig;
     rs.acc_count = counters + kCountAcc;
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
@@ -383,6 +384,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     if (cudaEventElapsedTime(&xms, ctx->ev0, ctx->ev_x) != cudaSuccess) xms = 0.f;
     cudaGetLastError();
     ctx->last_extract_ms = xms;
+    if (h[kCountErr] & kErrBounds) return bfail(ctx, FTK2B_INTERNAL, "a device bounds check failed (checked build)");
     if (h[kCountErr] & 2u) return bfail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return bfail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");
     if (h[kCountCand] > ccap) {
@@ -417,6 +419,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
 extern "C" ftk2b_status ftk2b_cp_run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes,
                                            const ftk2b_field_desc* fields, const ftk2b_cp_params* params,
                                            uint64_t* n_features) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_cp_run_batch");
   if (!ctx) return FTK2B_INVALID_ARG;
   if (cudaSetDevice(ctx->device) != cudaSuccess) return bfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
   ctx->batch.nf = 0;
@@ -426,6 +429,7 @@ extern "C" ftk2b_status ftk2b_cp_run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk
 }
 
 extern "C" ftk2b_status ftk2b_cp_fetch_batch(ftk2b_ctx* ctx, ftk2b_cp_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_cp_fetch_batch");
   if (!ctx || !out) return FTK2B_INVALID_ARG;
   BatchCtx& bc = ctx->batch;
   if (bc.nf <= 0) return bfail(ctx, FTK2B_INVALID_ARG, "no batch has run on this context");

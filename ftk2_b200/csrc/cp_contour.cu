@@ -2296,6 +2296,7 @@ static ftk2b_status ct_geometry(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, con
 extern "C" ftk2b_status ftk2b_contour_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                               const ftk2b_field_desc* field, double threshold, double sos_q,
                                               ftk2b_contour_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_contour_extract");
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field || !out) return cfail(ctx, FTK2B_INVALID_ARG, "null argument");
   *out = nullptr;
@@ -2415,6 +2416,7 @@ static ftk2b_status ct_geometry(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh, con
 extern "C" ftk2b_status ftk2b_fiber_surface_extract(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
                                                     const ftk2b_field_desc* field, const double thresholds[2],
                                                     double sos_q, ftk2b_fiber_surface_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_fiber_surface_extract");
   if (!ctx) return FTK2B_INVALID_ARG;
   if (!mesh || !field || !thresholds || !out) return cfail(ctx, FTK2B_INVALID_ARG, "null argument");
   *out = nullptr;

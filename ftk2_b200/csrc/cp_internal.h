@@ -7,6 +7,22 @@
 
 namespace ftk2b {
 
+// Device bounds checks of the checked build (compiled with -DFTK2B_CHECKED):
+// FTK2B_CHECK(cond, err) is `cond`, and a failed check sets bit 3 of the
+// call's error word (the call then reports FTK2B_INTERNAL) so that the
+// caller can skip the access; never a trap.  In the normal build it is
+// `true` and the compiler drops the test.
+constexpr unsigned kErrBounds = 8u;
+#ifdef FTK2B_CHECKED
+__device__ __forceinline__ bool checked_bound(bool ok, unsigned* err) {
+  if (!ok && err) atomicOr(err, kErrBounds);
+  return ok;
+}
+#define FTK2B_CHECK(cond, err) (::ftk2b::checked_bound((cond), (err)))
+#else
+#define FTK2B_CHECK(cond, err) (true)
+#endif
+
 constexpr int kMaxChains = 64;
 
 // Value access for a field sampled on a regular grid or per vertex.
@@ -134,6 +150,7 @@ struct RefineStage {
   unsigned* acc_count;           // may exceed acc_cap (then the call reports overflow)
   unsigned acc_cap;
   unsigned* count;   // simplices tested (reported after the run)
+  unsigned* err;     // the call's error word (bounds checks of the checked build)
 };
 // bytes of the staging buffers for `ccap` candidates: values, then quantised
 // values; the chain masks, the inside list (acc_cap entries) and the list

@@ -685,7 +685,7 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
       g[k] = (long long)rem;
     }
   }
-  const unsigned mkp = T.mk[ch];  // masks of vertices 0..m, 4 bits each
+  const unsigned mkp = FTK2B_CHECK(ch >= 0 && ch < kMaxChains, err) ? T.mk[ch] : 0u;  // masks of vertices 0..m, 4 bits each
   const int mkm = (int)((mkp >> (4 * m)) & 15u);
   const int missing = full & ~mkm;
   const int q = lane > d ? 1 : 0, r = lane - q * (d + 1);
@@ -753,7 +753,8 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       if (k < d) fvid += (unsigned long long)(c[k] + ((base >> k) & 1u)) * mesh.gstride[k];
-    const unsigned long long fk = kbase + fvid * (unsigned long long)nch + (unsigned long long)T.rank[rel];
+    const int rk = FTK2B_CHECK(rel < 4096u, err) ? T.rank[rel] : -1;
+    const unsigned long long fk = kbase + fvid * (unsigned long long)nch + (unsigned long long)rk;
     idx = sample ? find_key_sampled(keys, n, sample, ns, slog, fk) : find_key(keys, n, fk);
   }
   const unsigned act = __ballot_sync(0xFFFFFFFFu, idx >= 0);
@@ -775,7 +776,7 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
     const unsigned o = __shfl_sync(0xFFFFFFFFu, (unsigned)idx, __ffs(b) - 1);
     rk += o < (unsigned)idx ? 1u : 0u;
   }
-  if (valid) {
+  if (valid && FTK2B_CHECK(rk < (unsigned)kEdgeSlots, err)) {
     slots[(size_t)i * kEdgeSlots + rk] = (unsigned)idx;
     if (parent) uf_unite(parent, i, (unsigned)idx, err);
   }
@@ -846,7 +847,8 @@ __global__ void __launch_bounds__(kSortThreads, 1) small_sort_kernel(PostBuffers
   // scatter; afterwards bcnt[b] = end of bucket b = start of bucket b + 1
   for (unsigned i = t; i < n; i += kSortThreads) {
     const unsigned long long key = B.key[i];
-    sk[atomicAdd(&bcnt[bucket(key)], 1u)] = (key << kIdxBits) | i;
+    const unsigned slot = atomicAdd(&bcnt[bucket(key)], 1u);
+    if (FTK2B_CHECK(slot < n, B.err)) sk[slot] = (key << kIdxBits) | i;
   }
   __syncthreads();
   // union-find parents of the canonical positions (the edge kernel hooks)
@@ -858,7 +860,7 @@ __global__ void __launch_bounds__(kSortThreads, 1) small_sort_kernel(PostBuffers
     const unsigned b0 = b ? bcnt[b - 1] : 0u, b1 = bcnt[b];
     unsigned below = 0;
     for (unsigned j = b0; j < b1; ++j) below += sk[j] < v ? 1u : 0u;
-    B.key_alt[b0 + below] = v;
+    if (FTK2B_CHECK(b0 + below < n, B.err)) B.key_alt[b0 + below] = v;
   }
 }
 
@@ -965,7 +967,9 @@ __device__ __forceinline__ void finish_block(const PostBuffers& B, unsigned* sh,
   for (int round = 0; round < 16; ++round) {
     bool changed = false;
     for (unsigned i = t; i < n; i += 1024) {
-      const unsigned p = sp[i], pp = sp[p];
+      const unsigned p = sp[i];
+      if (!FTK2B_CHECK(p < n, B.err)) continue;
+      const unsigned pp = sp[p];
       if (pp != p) {
         sp[i] = pp;
         changed = true;

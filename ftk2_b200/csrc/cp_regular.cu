@@ -449,7 +449,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
         for (int j = 0; j < M; ++j) {
           const unsigned sh = (su + (pbase >> (4 * (MULTI ? 0 : j)))) & 15u;
           const int o = voff[u] + (MULTI ? j * (int)sizeof(T) : j * VY * VZ * G::ROWB) + (int)sh;
-          h[j] = *reinterpret_cast<const unsigned*>(rb + o);
+          h[j] = FTK2B_CHECK(o >= 0 && o + 4 * HW <= G::BYTES, err) ? *reinterpret_cast<const unsigned*>(rb + o) : 0u;
         }
         const unsigned x = vertex_word_hi<T, M>(h, band_tbl);
         w[u] = x | vinv[u];
@@ -460,7 +460,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     for (int u = 0; u < VPT; ++u) {
       unsigned h[M];
 #pragma unroll
-      for (int j = 0; j < M; ++j) h[j] = r[HW * (MULTI ? voff[u] + j : voff[u] + j * G::COMP_ELEMS)];
+      for (int j = 0; j < M; ++j) {
+        const int ix = HW * (MULTI ? voff[u] + j : voff[u] + j * G::COMP_ELEMS);
+        h[j] = FTK2B_CHECK(ix >= 0 && 4 * (ix + HW) <= G::BYTES, err) ? r[ix] : 0u;
+      }
       const unsigned x = vertex_word_hi<T, M>(h, band_tbl);
       w[u] = x | vinv[u];
     }
@@ -544,12 +547,14 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       unsigned r, e;
       if constexpr (D == 4) {
         const int i0 = ((czw + q) * VY + cyw) * VX + lane, i1 = i0 + VX;
-        r = A[i0] & A[i1];
-        e = (lane == 31) ? (A[i0 + 1] & A[i1 + 1]) : kAbsent;
+        const bool okA = FTK2B_CHECK(i1 + 1 < VSP, err);
+        r = okA ? A[i0] & A[i1] : kAbsent;
+        e = (lane == 31 && okA) ? (A[i0 + 1] & A[i1 + 1]) : kAbsent;
       } else {
         const int i0 = (cyw + q) * VX + lane;
-        r = A[i0];
-        e = (lane == 31) ? A[i0 + 1] : kAbsent;
+        const bool okA = FTK2B_CHECK(i0 + 1 < VSP, err);
+        r = okA ? A[i0] : kAbsent;
+        e = (lane == 31 && okA) ? A[i0 + 1] : kAbsent;
       }
       const unsigned nb = __shfl_down_sync(0xFFFFFFFFu, r, 1);
       R[q] = r & (lane == 31 ? e : nb);
@@ -1833,7 +1838,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 4) refine_test_kernel(Regul
         h[j] = hi_word<T>(x);
         const int qv = quant_small_p(quant_p((double)x, cfg.Q));
         big |= qv == kQBig;
-        sq[k * kStageVals + v * M + j] = qv;
+        if (FTK2B_CHECK(k * kStageVals + v * M + j < kTestCands * kStageVals, rs.err)) sq[k * kStageVals + v * M + j] = qv;
       }
       const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;  // absent: neutral under AND
       const bool gbig = ((__ballot_sync(0xFFFFFFFFu, big) >> (grp * NV)) & lowmask) != 0;
@@ -1910,8 +1915,9 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_accept_kernel(Reg
       if (i < n) {
         const unsigned long long e = rs.acc[i];
         const unsigned c = (unsigned)(e >> 8);
-        acc = test_pair<T, D, false>(mesh, fa, cfg, cq.corner[c], (int)(e & 255), (const T*)nullptr, chain_pk, 0ull,
-                                     key, lam_out, bary_out, sc_out);
+        if (FTK2B_CHECK(c < min(*cq.count, cq.cap) && (e & 255) < kMaxChains, rs.err))
+          acc = test_pair<T, D, false>(mesh, fa, cfg, cq.corner[c], (int)(e & 255), (const T*)nullptr, chain_pk, 0ull,
+                                       key, lam_out, bary_out, sc_out);
       }
       sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }

@@ -568,6 +568,7 @@ extern "C" ftk2b_status ftk2b_stream_open(ftk2b_ctx* ctx, const ftk2b_mesh_desc*
 }
 
 extern "C" ftk2b_status ftk2b_stream_push(ftk2b_stream* s, const ftk2b_field_desc* step, uint64_t* n_new) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_stream_push");
   if (!s) return FTK2B_INVALID_ARG;
   ftk2b_ctx* ctx = s->ctx;
   if (!step) return sfail(ctx, FTK2B_INVALID_ARG, "null timestep");
@@ -608,6 +609,7 @@ extern "C" ftk2b_status ftk2b_stream_push(ftk2b_stream* s, const ftk2b_field_des
 }
 
 extern "C" ftk2b_status ftk2b_stream_result(ftk2b_stream* s, ftk2b_cp_result** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_stream_result");
   if (!s || !out) return FTK2B_INVALID_ARG;
   *out = nullptr;
   if (cudaSetDevice(s->ctx->device) != cudaSuccess) return sfail(s->ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");

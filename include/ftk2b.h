@@ -38,7 +38,8 @@ typedef enum {
   FTK2B_OVERFLOW_RETRY = 5,  /* an output buffer overflowed and retries were exhausted */
   FTK2B_NO_DEVICE = 6,       /* no usable CUDA device: there is no CPU fallback */
   FTK2B_UNSUPPORTED = 7,     /* a combination the path does not implement */
-  FTK2B_BUSY = 8             /* the serving queue is full */
+  FTK2B_BUSY = 8,            /* the serving queue is full */
+  FTK2B_INTERNAL = 9         /* a device self-check failed: a bounds check of the checked build (-DFTK2B_CHECKED) */
 } ftk2b_status;
 
 enum { FTK2B_MESH_REGULAR = 0, FTK2B_MESH_EXTRUDED = 1 };
