@@ -15,7 +15,7 @@ from ftk2_b200 import synthetic as S
 def cases():
     """(name, mesh dims, field array, components, Q) of every single-field case."""
     rng = np.random.default_rng(7)
-    noise3 = rng.standard_normal((3, 20, 18, 16, 4)).astype(np.float64)  # many features: the general post chain
+    noise3 = rng.standard_normal((4, 20, 18, 16, 3)).astype(np.float64)  # many features: the general post chain
     return [
         ("c1_2d", [64, 64, 10], S.analytic_2d(64, 64, 10), 2, 1e6),
         ("gauss3d_f64", [40, 36, 32, 6], S.gaussian_sum_gradient((40, 36, 32), 6, seed=5, n_blobs=12), 3, 2.0 ** 20),
