@@ -887,12 +887,14 @@ __global__ void __launch_bounds__(kStatsWarps * 32, 2)
     cp_async_commit();  // empty groups keep the count uniform
   };
 
-  int kmn[M], kmx[M], hmn[M], hmx[M];
+  // two accumulator sets, by the parity of the vector index, halve the
+  // dependent min / max chains of a row
+  int kmn[2][M], kmx[2][M], hmn[M], hmx[M];
   auto reset = [&]() {
 #pragma unroll
     for (int a = 0; a < M; ++a) {
-      kmn[a] = hmn[a] = 0x7FFFFFFF;
-      kmx[a] = hmx[a] = (int)0x80000000;
+      kmn[0][a] = kmn[1][a] = hmn[a] = 0x7FFFFFFF;
+      kmx[0][a] = kmx[1][a] = hmx[a] = (int)0x80000000;
     }
   };
   reset();
@@ -905,13 +907,15 @@ __global__ void __launch_bounds__(kStatsWarps * 32, 2)
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
       const uint4 w = *vslot(stage, j);
+      const int e0 = tb + LPT * V * j + V * q;
+      const bool full = e0 + V <= gc.ne;  // the whole vector lies in the row
 #pragma unroll
       for (int u = 0; u < V; ++u) {
         const int a = (LPT * V * j + u) % M;
-        if (tb + LPT * V * j + V * q + u < gc.ne) {
+        if (full || e0 + u < gc.ne) {
           const int key = ord_key(vec_hi_word<T>(w, u));
-          kmn[a] = min(kmn[a], key);
-          kmx[a] = max(kmx[a], key);
+          kmn[j & 1][a] = min(kmn[j & 1][a], key);
+          kmx[j & 1][a] = max(kmx[j & 1][a], key);
         }
       }
     }
@@ -937,8 +941,8 @@ __global__ void __launch_bounds__(kStatsWarps * 32, 2)
 #pragma unroll
       for (int a = 0; a < M; ++a)
         if ((a + rot) % M == c) {
-          rmn[c] = min(rmn[c], kmn[a]);
-          rmx[c] = max(rmx[c], kmx[a]);
+          rmn[c] = min(rmn[c], min(kmn[0][a], kmn[1][a]));
+          rmx[c] = max(rmx[c], max(kmx[0][a], kmx[1][a]));
         }
 #pragma unroll
       for (int o = 1; o < LPT; o <<= 1) {

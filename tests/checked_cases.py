@@ -34,7 +34,7 @@ def run_all(ctx) -> dict:
         out[f"{name}.lam"] = r.lam
         out[f"{name}.track"] = r.track_id
         out[f"{name}.edges"] = r.edges
-    cs = cases()[:3]
+    cs = cases()[:2]  # one dtype per batch: the 2D and the 3D+t float64 fields
     res = ctx.extract_batch([api.regular_mesh_desc(d) for _, d, _, _, _ in cs],
                             [api.field_desc(f, api.LAYOUT_MULTICOMPONENT, m) for _, _, f, m, _ in cs],
                             [api.params(q) for _, _, _, _, q in cs])
