@@ -786,27 +786,36 @@ __device__ __forceinline__ void star_edges_warp(const RegularMesh& mesh, int nch
 // Batches: one warp per feature (the short chain's star_edges_warp with the
 // feature's field, found by its key).
 // The keys live in global memory; every block keeps every 2^slog-th of them
-// in shared memory (dynamic, (n >> slog) + 1 entries) for the lookups.
+// in shared memory (dynamic, (cap >> slog) + 1 entries) for the lookups, and
+// the fields' first keys after them (up to kBatchKbSmem fields): a binary
+// search over global memory per feature would cost one dependent load a step.
+constexpr int kBatchKbSmem = 4096;
 __global__ void edges_batch_warp_kernel(const BatchMesh* __restrict__ fm, const unsigned long long* __restrict__ kb,
                                         int nf, const unsigned long long* __restrict__ keys, const unsigned* n_ptr,
                                         unsigned cap, unsigned* __restrict__ cnt, unsigned* __restrict__ slots,
                                         int slog) {
-  extern __shared__ unsigned long long sample[];
+  extern __shared__ unsigned long long sample[];  // then the fields' first keys, when kb_smem
   __shared__ StarTables T[2];  // d = 3, d = 4
   fill_star_tables(T[0], 3);
   fill_star_tables(T[1], 4);
   const unsigned n = min(*n_ptr, cap);
   const unsigned ns = (n + (1u << slog) - 1) >> slog;
+  const unsigned smax = (unsigned)((cap >> slog) + 1);
   for (unsigned j = threadIdx.x; j < ns; j += blockDim.x) sample[j] = keys[(size_t)j << slog];
+  const bool kb_smem = nf <= kBatchKbSmem;
+  unsigned long long* const skb = sample + smax;
+  if (kb_smem)
+    for (int f = threadIdx.x; f < nf; f += blockDim.x) skb[f] = kb[f];
+  const unsigned long long* fkb = kb_smem ? skb : kb;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned nw = (gridDim.x * blockDim.x) >> 5;
   for (unsigned i = gw; i < n; i += nw) {
     const unsigned long long key = keys[i];
-    const unsigned f = batch_field_of(kb, nf, key);
+    const unsigned f = batch_field_of(fkb, nf, key);
     const RegularMesh mesh = fm[f].mesh;
-    star_edges_warp(mesh, fm[f].nch, keys, n, i, key - kb[f], kb[f], T[mesh.d - 3], lane, cnt, slots, nullptr,
+    star_edges_warp(mesh, fm[f].nch, keys, n, i, key - fkb[f], fkb[f], T[mesh.d - 3], lane, cnt, slots, nullptr,
                     nullptr, sample, ns, slog);
   }
 }
@@ -1112,7 +1121,7 @@ cudaError_t launch_post_batch(const BatchMesh* fm, const unsigned long long* kb,
   {
     int slog = 4;
     while (((unsigned long long)cap >> slog) + 1 > 8192ull) ++slog;
-    const size_t smp = sizeof(unsigned long long) * (((size_t)cap >> slog) + 1);
+    const size_t smp = sizeof(unsigned long long) * (((size_t)cap >> slog) + 1 + (nf <= kBatchKbSmem ? nf : 0));
     cudaFuncSetAttribute(edges_batch_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
     edges_batch_warp_kernel<<<(B.num_sms > 0 ? B.num_sms : 148) * 2, 512, smp, st>>>(fm, kb, nf, skey, B.count, cap,
                                                                                       B.edge_cnt, B.edge_slots, slog);
