@@ -80,13 +80,10 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return false;
 }
 
-// Untiled bulk copy global -> shared (both addresses and the size multiples
-// of 16 bytes), completing on the mbarrier's transaction count.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
+// The mbarrier receives one arrival when every cp.async this thread issued
+// before has landed (.noinc: the barrier's expected count covers it).
+__device__ __forceinline__ void cp_async_mbar_arrive(unsigned long long* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
@@ -181,7 +178,7 @@ struct Geo {
   static constexpr int COMP_RAW = VXBOX * VY * VZ * (int)sizeof(T);  // bytes of one component box
   static constexpr int COMP = round128(COMP_RAW);
   static constexpr int BOX_BYTES = MULTI ? round128(COMP_RAW * M) : COMP * M;
-  // bulk row staging (arrays a TMA tensor map cannot describe): box row r of
+  // row staging (arrays a TMA tensor map cannot describe): box row r of
   // a slice goes to bytes [r * ROWB, (r + 1) * ROWB) of the buffer, its data
   // starting at the row's source address mod 16 (rows component-major for
   // separate arrays)
@@ -194,7 +191,9 @@ struct Geo {
   static constexpr int WORDS = 2 * BYTES;                                // offset of the word slots
   // the block's candidate buffer (corner, chains) and its count, after the word slots
   static constexpr int CAND = WORDS + 2 * VSP * 4;
-  static constexpr int SMEM = CAND + 16 * kCandBuf + 16;
+  // chunk staging: the source address of every box row
+  static constexpr int ROWSRC = CAND + 16 * kCandBuf + 16;
+  static constexpr int SMEM = ROWSRC + 8 * ROWS;
 };
 
 __device__ __forceinline__ unsigned long long pack_corner(long long x, long long y, long long z,
@@ -208,16 +207,19 @@ __device__ __forceinline__ unsigned long long pack_corner(long long x, long long
 //
 // cull_tile marches one tile over the corner time steps of one chunk.  The
 // block's two slice buffers, word slots, mbarriers and band table are the
-// caller's; ph[b] counts the phases mbarrier b has completed before this call
-// (so that a persistent block can march many tiles) and is advanced past the
-// copies this call waits for.  Returns false when a bounded TMA wait gave up
-// (the error flag is set).
+// caller's: bar[0..1] take TMA tensor copies (one arrival each), bar[2] is
+// the failure-path barrier that nothing completes, bar[3..4] take the chunk
+// copies of the block's threads (kThreads arrivals each).  ph[b] counts the
+// phases barrier b (b = 0, 1) or 3 + b - 2 (b = 2, 3) has completed before
+// this call (so that a persistent block can march many tiles) and is advanced
+// past the copies this call waits for.  Returns false when a bounded wait
+// gave up (the error flag is set).
 template <typename T, int D, bool MULTI, bool TMA>
 __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtensorMap* map1,
                                           const CUtensorMap* map2, const RegularMesh& mesh, const FieldAccess& fa,
                                           const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
                                           int tile, int chunk, unsigned char* smem, unsigned long long* bar,
-                                          const unsigned* band_tbl, unsigned ph[2]) {
+                                          const unsigned* band_tbl, unsigned ph[4]) {
   using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
   constexpr int TX = G::TX, TY = G::TY, TZ = G::TZ;
@@ -252,8 +254,9 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // two-slot ring stores timestep t in slot t & 1; tflip = 0 otherwise)
   auto tcoord = [&](int s) { return (s + aoff[D - 1]) ^ fa.tflip; };
 
-  // bulk row copies stage arrays that TMA cannot describe (rows not 16-byte
-  // multiples, misaligned offsets); per-vertex arrays keep element copies
+  // 16-byte chunk copies of the box rows stage arrays that TMA cannot
+  // describe (rows not 16-byte multiples, misaligned offsets); per-vertex
+  // arrays keep element copies
   const bool bulk = !TMA && !fa.per_vertex;
   const bool mbar = TMA || bulk;
 
@@ -285,28 +288,30 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   for (int j = 0; j < (MULTI ? 1 : M); ++j)
     pbase |= (unsigned)(reinterpret_cast<uintptr_t>(fa.comp[j]) & 15) << (4 * j);
   const long long tstride = fa.estride[D - 1];
-  // bulk staging: warp 0's lanes issue box rows lane + 32 i; the source
-  // address of each row at array time 0 (0 for rows outside the mesh) and
-  // the bytes of a row's local vertices
-  constexpr int RPL = (G::ROWS + 31) / 32;
-  uintptr_t rsrc[RPL];
+  // chunk staging: the source address of every box row at array time 0 (0
+  // for rows outside the mesh) in shared memory, and the bytes of a row's
+  // local vertices; the block's threads copy the rows in 16-byte blocks
+  unsigned long long* const rsrc = reinterpret_cast<unsigned long long*>(smem + G::ROWSRC);
   const int rbytes = min(VX, ldx - x0) * (MULTI ? M : 1) * (int)sizeof(T);
-#pragma unroll
-  for (int i = 0; i < RPL; ++i) {
-    rsrc[i] = 0;
-    const int r = lane + 32 * i;
-    if (bulk && warp == 0 && r < G::ROWS) {
+  if (bulk) {
+    for (int r = tid; r < G::ROWS; r += kThreads) {
       const int rr = MULTI ? r : r % (VY * VZ);
       const int j = MULTI ? 0 : r / (VY * VZ);
       const int vy = rr % VY, vz = rr / VY;
+      unsigned long long a = 0;
       if (y0 + vy < ldy && (D == 3 || z0 + vz < ldz)) {
         long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
         if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
-        rsrc[i] = reinterpret_cast<uintptr_t>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2])) +
-                  (uintptr_t)(e * (long long)sizeof(T));
+        a = (unsigned long long)(reinterpret_cast<uintptr_t>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2])) +
+                                 (uintptr_t)(e * (long long)sizeof(T)));
       }
+      rsrc[r] = a;
     }
   }
+  // chunk copies and TMA copies complete on separate barriers (different
+  // arrival counts); ph[2..3] count the phases of the chunk barriers
+  unsigned long long* const sb = bulk ? bar + 3 : bar;
+  unsigned* const sp = bulk ? ph + 2 : ph;
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
@@ -332,32 +337,28 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
         }
       }
     } else if (bulk) {
-      // warp 0: one bulk copy per box row holding vertices of the local
-      // mesh, from the 16-byte block of its first element to the block of
-      // its last (an aligned 16-byte block never crosses a page, so the
-      // bytes read around the row lie in pages the row occupies); the rows'
-      // byte total goes to the mbarrier before any copy is issued
-      if (warp == 0) {
-        const uintptr_t tb = (uintptr_t)((long long)tcoord(s) * tstride * (long long)sizeof(T));
-        unsigned total = 0;
-        uintptr_t lo[RPL];
-        unsigned nb[RPL];
+      // every thread: 16-byte blocks c = tid + k * kThreads of the box rows
+      // (CPR blocks per row slot), each row from the 16-byte block of its
+      // first element to the block of its last (an aligned 16-byte block
+      // never crosses a page, so the bytes read around the row lie in pages
+      // the row occupies); then one arrival on the slice's barrier once the
+      // thread's copies have landed
+      constexpr int CPR = G::ROWB / 16;
+      constexpr int CPT = (G::ROWS * CPR + kThreads - 1) / kThreads;
+      const uintptr_t tb = (uintptr_t)((long long)tcoord(s) * tstride * (long long)sizeof(T));
 #pragma unroll
-        for (int i = 0; i < RPL; ++i) {
-          const uintptr_t src = rsrc[i] + tb;
-          lo[i] = src & ~(uintptr_t)15;
-          nb[i] = rsrc[i] ? (unsigned)(((src + (uintptr_t)rbytes + 15) & ~(uintptr_t)15) - lo[i]) : 0u;
-          total += nb[i];
+      for (int k = 0; k < CPT; ++k) {
+        const int c = tid + k * kThreads;
+        if (c < G::ROWS * CPR) {
+          const int r = c / CPR, q = c - r * CPR;
+          const unsigned long long b = rsrc[r];
+          const uintptr_t src = (uintptr_t)b + tb;
+          const uintptr_t lo = (src & ~(uintptr_t)15) + 16 * (uintptr_t)q;
+          if (b && lo < src + (uintptr_t)rbytes && FTK2B_CHECK(r * G::ROWB + 16 * q + 16 <= G::BYTES, err))
+            cp_async_16(dst0 + r * G::ROWB + 16 * q, reinterpret_cast<const void*>(lo));
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xFFFFFFFFu, total, o);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (lane == 0) mbar_expect_tx(&bar[buf], total);
-        __syncwarp();
-#pragma unroll
-        for (int i = 0; i < RPL; ++i)
-          if (nb[i]) bulk_load(dst0 + (lane + 32 * i) * G::ROWB, reinterpret_cast<const void*>(lo[i]), nb[i], &bar[buf]);
       }
+      cp_async_mbar_arrive(&sb[buf]);
     } else {
       // per-thread asynchronous element copies into the same layout (zeros
       // outside the array), one commit group per slice
@@ -425,7 +426,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // in hardware); returns false when the bounded wait gave up
   auto wait = [&](int s, int buf) -> bool {
     if (mbar) {
-      return mbar_wait(&bar[buf], (ph[buf] + (unsigned)((s - t0) >> 1)) & 1u);
+      return mbar_wait(&sb[buf], (sp[buf] + (unsigned)((s - t0) >> 1)) & 1u);
     } else {
       // slice s + 1 (when it exists) was issued after s: one group may stay
       // in flight; then every thread's copies of slice s are visible
@@ -489,7 +490,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     if (ok) words(0, t0, prev);
     if (__syncthreads_or(!ok)) {
       // give the other copy in flight a bounded chance to land before leaving
-      if (mbar && t0 + 1 <= s_end) mbar_wait(&bar[1], ph[1] & 1u);
+      if (mbar && t0 + 1 <= s_end) mbar_wait(&sb[1], sp[1] & 1u);
       if (tid == 0) atomicOr(err, 2u);
       return false;
     }
@@ -533,7 +534,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     // s's raw buffer is free, and every warp has finished culling step ct - 1
     if (__syncthreads_or(!ok)) {
       const int ob = ((s - t0) & 1) ^ 1;
-      if (mbar && s + 1 <= s_end) mbar_wait(&bar[ob], (ph[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
+      if (mbar && s + 1 <= s_end) mbar_wait(&sb[ob], (sp[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
       if (tid == 0) atomicOr(err, 2u);
       return false;
     }
@@ -617,8 +618,8 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   if (mbar) {
     // slices t0 .. s_end alternate buffers 0, 1, 0, ...
     const unsigned nsl = (unsigned)(s_end - t0 + 1);
-    ph[0] += (nsl + 1) >> 1;
-    ph[1] += nsl >> 1;
+    sp[0] += (nsl + 1) >> 1;
+    sp[1] += nsl >> 1;
   }
   return true;
 }
@@ -630,18 +631,20 @@ __global__ void __launch_bounds__(kThreads, 2)
                            const __grid_constant__ CUtensorMap map2, RegularMesh mesh, FieldAccess fa,
                            ExtractConfig cfg, CandidateQueue cq, unsigned* err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ unsigned long long bar[3];
+  __shared__ unsigned long long bar[5];
   __shared__ unsigned band_tbl[kBandTable];
   fill_band_table<T>(band_tbl, threadIdx.x, kThreads);  // visible after the tile's first barrier
-  // TMA tensor copies and bulk row copies complete on bar[0..1]; bar[2] only
-  // serves the failure-path check and never completes
+  // TMA tensor copies complete on bar[0..1], the threads' chunk copies on
+  // bar[3..4]; bar[2] only serves the failure-path check and never completes
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     mbar_init(&bar[2], 1);
+    mbar_init(&bar[3], kThreads);
+    mbar_init(&bar[4], kThreads);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  unsigned ph[2] = {0u, 0u};
+  unsigned ph[4] = {0u, 0u, 0u, 0u};
   cull_tile<T, D, MULTI, TMA>(&map0, &map1, &map2, mesh, fa, cfg, cq, err, (int)blockIdx.x, (int)blockIdx.y, smem,
                               bar, band_tbl, ph);
 }
@@ -2175,7 +2178,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     batch_cull_kernel(const BatchField* __restrict__ fields, const unsigned* __restrict__ item_base, int nf,
                       unsigned n_items, unsigned* item_next, CandidateQueue cq, unsigned* err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ unsigned long long bar[3];
+  __shared__ unsigned long long bar[5];
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned s_item, s_field;
   __shared__ unsigned s_ib[kBatchSmemFields];
@@ -2196,9 +2199,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     mbar_init(&bar[2], 1);
+    mbar_init(&bar[3], kThreads);
+    mbar_init(&bar[4], kThreads);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  unsigned ph[2] = {0u, 0u};
+  unsigned ph[4] = {0u, 0u, 0u, 0u};
   for (;;) {
     __syncthreads();  // s_item of the previous item has been read by every thread
     if (threadIdx.x == 0) {
