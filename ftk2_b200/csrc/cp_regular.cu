@@ -202,6 +202,29 @@ __device__ __forceinline__ unsigned long long pack_corner(long long x, long long
          ((unsigned long long)t << 48);
 }
 
+// The block's buffered candidates into the queue with one reservation:
+// ccount[0] holds how many the block found (those past kCandBuf went to the
+// queue directly), cbuf their (corner, chains) pairs.  Every thread calls
+// it after a block barrier that follows the last candidate writes; it
+// leaves ccount[0] = 0, and the buffer may take new candidates after the
+// next block barrier.
+__device__ __forceinline__ void flush_candidates(const unsigned long long* cbuf, unsigned* ccount,
+                                                 const CandidateQueue& cq, unsigned field_id) {
+  const unsigned nc = min(ccount[0], (unsigned)kCandBuf);
+  if (threadIdx.x == 0) ccount[1] = nc ? atomicAdd(cq.count, nc) : 0u;
+  __syncthreads();
+  if (threadIdx.x == 0) ccount[0] = 0;
+  const unsigned cbase = ccount[1];
+  for (unsigned i = threadIdx.x; i < nc; i += kThreads) {
+    const unsigned gi = cbase + i;
+    if (gi < cq.cap) {
+      cq.corner[gi] = cbuf[2 * i];
+      cq.chains[gi] = cbuf[2 * i + 1];
+      if (cq.field) cq.field[gi] = field_id;
+    }
+  }
+}
+
 // Stage 1: stream the field through shared memory, cull hypercubes, queue
 // the survivors with the chains whose own vertices survive the cull.
 //
@@ -209,17 +232,23 @@ __device__ __forceinline__ unsigned long long pack_corner(long long x, long long
 // block's two slice buffers, word slots, mbarriers and band table are the
 // caller's: bar[0..1] take TMA tensor copies (one arrival each), bar[2] is
 // the failure-path barrier that nothing completes, bar[3..4] take the chunk
-// copies of the block's threads (kThreads arrivals each).  ph[b] counts the
-// phases barrier b (b = 0, 1) or 3 + b - 2 (b = 2, 3) has completed before
-// this call (so that a persistent block can march many tiles) and is advanced
-// past the copies this call waits for.  Returns false when a bounded wait
-// gave up (the error flag is set).
+// copies of the block's threads (kThreads arrivals each).  Bit b of ph is
+// the parity of the phases barrier b (b = 0, 1) or 3 + b - 2 (b = 2, 3) has
+// completed before this call (so that a persistent block can march many
+// tiles); it is advanced past the copies this call waits for.  Surviving
+// hypercubes go to the candidate buffer cbuf / ccount (flush_candidates);
+// with defer, the call first flushes what the block's previous tile left
+// there (as candidates of field pend_field) and leaves its own for the
+// next call, else it flushes its own at the end.  Returns false when a
+// bounded wait gave up (the error flag is set).
 template <typename T, int D, bool MULTI, bool TMA>
 __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtensorMap* map1,
                                           const CUtensorMap* map2, const RegularMesh& mesh, const FieldAccess& fa,
                                           const ExtractConfig& cfg, const CandidateQueue& cq, unsigned* err,
                                           int tile, int chunk, unsigned char* smem, unsigned long long* bar,
-                                          const unsigned* band_tbl, unsigned ph[4]) {
+                                          const unsigned* band_tbl, unsigned& ph,
+                                          unsigned long long* cbuf, unsigned* ccount, bool defer,
+                                          unsigned pend_field) {
   using G = Geo<T, D, MULTI>;
   constexpr int M = D - 1;
   constexpr int TX = G::TX, TY = G::TY, TZ = G::TZ;
@@ -263,25 +292,28 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // per-thread vertex slots of a slice, fixed for the whole time march:
   // element offset of component 0 in a slice buffer (bulk staging: byte
   // offset from the row's slot, and the row's source offset mod 16 without
-  // the time term, 4 bits per slot) and an absence mask
+  // the time term, 4 bits per slot) and an absence mask; set once the first
+  // slices' copies are in flight
   int voff[VPT];
   unsigned vshift = 0;
   unsigned vinv[VPT];  // ~0 for slots outside the mesh (absent under AND), else 0
+  auto set_slots = [&]() {
 #pragma unroll
-  for (int u = 0; u < VPT; ++u) {
-    const int i = tid + u * kThreads;
-    const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
-    const bool in = i < VS && x0 + vx < ldx && y0 + vy < ldy && (D == 3 || z0 + vz < ldz);
-    if (bulk) {
-      voff[u] = in ? (vz * VY + vy) * G::ROWB + vx * (MULTI ? M : 1) * (int)sizeof(T) : 0;
-      long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
-      if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
-      vshift |= (unsigned)((e * (long long)sizeof(T)) & 15) << (4 * u);
-    } else {
-      voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
+    for (int u = 0; u < VPT; ++u) {
+      const int i = tid + u * kThreads;
+      const int vx = i % VX, vy = (i / VX) % VY, vz = i / (VX * VY);
+      const bool in = i < VS && x0 + vx < ldx && y0 + vy < ldy && (D == 3 || z0 + vz < ldz);
+      if (bulk) {
+        voff[u] = in ? (vz * VY + vy) * G::ROWB + vx * (MULTI ? M : 1) * (int)sizeof(T) : 0;
+        long long e = (long long)(x0 + aoff[0]) * fa.estride[0] + (long long)(y0 + vy + aoff[1]) * fa.estride[1];
+        if (D == 4) e += (long long)(z0 + vz + aoff[2]) * fa.estride[2];
+        vshift |= (unsigned)((e * (long long)sizeof(T)) & 15) << (4 * u);
+      } else {
+        voff[u] = in ? (MULTI ? ((vz * VY + vy) * G::VXBOX + vx) * M : (vz * VY + vy) * G::VXBOX + vx) : 0;
+      }
+      vinv[u] = in ? 0u : kAbsent;
     }
-    vinv[u] = in ? 0u : kAbsent;
-  }
+  };
   // source address mod 16 of each array, and the time axis' element stride
   unsigned pbase = 0;
 #pragma unroll
@@ -309,9 +341,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     }
   }
   // chunk copies and TMA copies complete on separate barriers (different
-  // arrival counts); ph[2..3] count the phases of the chunk barriers
+  // arrival counts); bits 2..3 of ph hold the phase parities of the chunk
+  // barriers
   unsigned long long* const sb = bulk ? bar + 3 : bar;
-  unsigned* const sp = bulk ? ph + 2 : ph;
+  const int sp = bulk ? 2 : 0;
 
   // ---- slice staging
   auto issue = [&](int s, int buf) {
@@ -426,7 +459,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // in hardware); returns false when the bounded wait gave up
   auto wait = [&](int s, int buf) -> bool {
     if (mbar) {
-      return mbar_wait(&sb[buf], (sp[buf] + (unsigned)((s - t0) >> 1)) & 1u);
+      return mbar_wait(&sb[buf], ((ph >> (sp + buf)) + (unsigned)((s - t0) >> 1)) & 1u);
     } else {
       // slice s + 1 (when it exists) was issued after s: one group may stay
       // in flight; then every thread's copies of slice s are visible
@@ -474,13 +507,15 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
   // hypercube's 2^D vertices then take 2^(D-1) shared-memory words.
   unsigned prev[VPT];
 
-  unsigned long long* const cbuf = reinterpret_cast<unsigned long long*>(smem + G::CAND);
-  unsigned* const ccount = reinterpret_cast<unsigned*>(smem + G::CAND + 16 * kCandBuf);
-  if (tid == 0) ccount[0] = 0;
+  if (!defer && tid == 0) ccount[0] = 0;
   // the previous tile of a persistent block is done with every buffer
   __syncthreads();
   issue(t0, 0);
   if (t0 + 1 <= s_end) issue(t0 + 1, 1);
+  set_slots();
+  // a persistent block's previous tile left its candidates in the buffer:
+  // reserve their queue space while this tile's first slices are in flight
+  if (defer) flush_candidates(cbuf, ccount, cq, pend_field);
   {
     bool ok = wait(t0, 0);
     // failure-path check (host option): after the first slice has landed,
@@ -490,7 +525,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     if (ok) words(0, t0, prev);
     if (__syncthreads_or(!ok)) {
       // give the other copy in flight a bounded chance to land before leaving
-      if (mbar && t0 + 1 <= s_end) mbar_wait(&sb[1], sp[1] & 1u);
+      if (mbar && t0 + 1 <= s_end) mbar_wait(&sb[1], (ph >> (sp + 1)) & 1u);
       if (tid == 0) atomicOr(err, 2u);
       return false;
     }
@@ -534,7 +569,7 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     // s's raw buffer is free, and every warp has finished culling step ct - 1
     if (__syncthreads_or(!ok)) {
       const int ob = ((s - t0) & 1) ^ 1;
-      if (mbar && s + 1 <= s_end) mbar_wait(&sb[ob], (sp[ob] + (unsigned)((s + 1 - t0) >> 1)) & 1u);
+      if (mbar && s + 1 <= s_end) mbar_wait(&sb[ob], ((ph >> (sp + ob)) + (unsigned)((s + 1 - t0) >> 1)) & 1u);
       if (tid == 0) atomicOr(err, 2u);
       return false;
     }
@@ -601,25 +636,16 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       }
     }
   }
-  // the block's buffered candidates into the queue: one reservation
-  __syncthreads();
-  const unsigned nc = min(ccount[0], (unsigned)kCandBuf);
-  if (tid == 0) ccount[1] = nc ? atomicAdd(cq.count, nc) : 0u;
-  __syncthreads();
-  const unsigned cbase = ccount[1];
-  for (unsigned i = tid; i < nc; i += kThreads) {
-    const unsigned gi = cbase + i;
-    if (gi < cq.cap) {
-      cq.corner[gi] = cbuf[2 * i];
-      cq.chains[gi] = cbuf[2 * i + 1];
-      if (cq.field) cq.field[gi] = cq.field_id;
-    }
+  // the block's buffered candidates into the queue (deferred: by the
+  // block's next tile, or after its last)
+  if (!defer) {
+    __syncthreads();
+    flush_candidates(cbuf, ccount, cq, cq.field_id);
   }
   if (mbar) {
     // slices t0 .. s_end alternate buffers 0, 1, 0, ...
     const unsigned nsl = (unsigned)(s_end - t0 + 1);
-    sp[0] += (nsl + 1) >> 1;
-    sp[1] += nsl >> 1;
+    ph ^= ((((nsl + 1) >> 1) & 1u) << sp) | (((nsl >> 1) & 1u) << (sp + 1));
   }
   return true;
 }
@@ -644,9 +670,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     mbar_init(&bar[4], kThreads);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  unsigned ph[4] = {0u, 0u, 0u, 0u};
+  unsigned ph = 0;  // phase parities of bar[0], bar[1], bar[3], bar[4]
+  using G = Geo<T, D, MULTI>;
   cull_tile<T, D, MULTI, TMA>(&map0, &map1, &map2, mesh, fa, cfg, cq, err, (int)blockIdx.x, (int)blockIdx.y, smem,
-                              bar, band_tbl, ph);
+                              bar, band_tbl, ph, reinterpret_cast<unsigned long long*>(smem + G::CAND),
+                              reinterpret_cast<unsigned*>(smem + G::CAND + 16 * kCandBuf), false, 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -2182,6 +2210,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned s_item, s_field;
   __shared__ unsigned s_ib[kBatchSmemFields];
+  // candidate buffer shared by the items of every dimension: an item's
+  // candidates are flushed by the block's next item
+  __shared__ unsigned long long s_cbuf[2 * kCandBuf];
+  __shared__ unsigned s_ccount[2];
   __shared__ RegularMesh s_mesh;
   __shared__ FieldAccess s_fa;
   __shared__ ExtractConfig s_cfg;
@@ -2203,11 +2235,17 @@ __global__ void __launch_bounds__(kThreads, 2)
     mbar_init(&bar[4], kThreads);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  unsigned ph[4] = {0u, 0u, 0u, 0u};
+  unsigned ph = 0;  // phase parities of bar[0], bar[1], bar[3], bar[4]
+  // thread 0 takes the next item while the block works on the current one
+  unsigned next = threadIdx.x == 0 ? atomicAdd(item_next, 1u) : 0u;
+  unsigned cur_field = 0xFFFFFFFFu;  // field whose record is in shared memory
+  unsigned last_field = 0;           // field of the candidates in the buffer
+  if (threadIdx.x == 0) s_ccount[0] = 0;
   for (;;) {
     __syncthreads();  // s_item of the previous item has been read by every thread
     if (threadIdx.x == 0) {
-      const unsigned it = atomicAdd(item_next, 1u);
+      const unsigned it = next;
+      if (it < n_items) next = atomicAdd(item_next, 1u);
       unsigned f = 0;
       if (it < n_items) {
         // the last field whose first item is <= it
@@ -2227,9 +2265,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (it >= n_items) break;
     const unsigned f = s_field;
     const BatchField& F = fields[f];
-    // the field's mesh, access and configuration into shared memory (the
-    // tensor maps stay in global memory, where TMA reads them)
-    {
+    // the field's mesh, access and configuration into shared memory when the
+    // item belongs to another field than the previous one (the tensor maps
+    // stay in global memory, where TMA reads them)
+    if (f != cur_field) {
+      cur_field = f;
       constexpr int kMw = sizeof(RegularMesh) / 4, kFw = sizeof(FieldAccess) / 4, kCw = sizeof(ExtractConfig) / 4;
       const unsigned* src_m = reinterpret_cast<const unsigned*>(&F.mesh);
       const unsigned* src_f = reinterpret_cast<const unsigned*>(&F.fa);
@@ -2242,8 +2282,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         s_tma = F.tma;
         s_ibase = F.item_base;
       }
+      __syncthreads();
     }
-    __syncthreads();
     const unsigned local = it - s_ibase;
     const unsigned ntiles = (unsigned)s_cfg.tiles[0] * s_cfg.tiles[1] * s_cfg.tiles[2];
     CandidateQueue q = cq;
@@ -2252,20 +2292,24 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (s_mesh.d == 4) {
       ok = s_tma ? cull_tile<T, 4, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
-                                                ph)
+                                                ph, s_cbuf, s_ccount, true, last_field)
                  : cull_tile<T, 4, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                  (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
-                                                 ph);
+                                                 ph, s_cbuf, s_ccount, true, last_field);
     } else {
       ok = s_tma ? cull_tile<T, 3, MULTI, true>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                 (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
-                                                ph)
+                                                ph, s_cbuf, s_ccount, true, last_field)
                  : cull_tile<T, 3, MULTI, false>(&F.maps[0], &F.maps[1], &F.maps[2], s_mesh, s_fa, s_cfg, q, err,
                                                  (int)(local % ntiles), (int)(local / ntiles), smem, bar, band_tbl,
-                                                 ph);
+                                                 ph, s_cbuf, s_ccount, true, last_field);
     }
+    last_field = f;
     if (!ok) break;  // the whole block saw the failed wait
   }
+  // the last item's candidates
+  __syncthreads();
+  flush_candidates(s_cbuf, s_ccount, cq, last_field);
 }
 
 template <typename T>
