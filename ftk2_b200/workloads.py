@@ -47,6 +47,8 @@ def run_batch_case(args):
     """c3: the 256-field batch, one ftk2b_cp_run_batch per step."""
     import torch
     fields = generate.c3_batch(n=args.nfields)
+    if args.field_dims:
+        fields = [f for f in fields if len(f[0]) - 1 == args.field_dims]
     torch.cuda.synchronize()
     with api.Context(0) as ctx:
         if args.no_graphs:
@@ -91,6 +93,8 @@ def main():
     ap.add_argument("--tchunk", type=int, default=0, help="time steps per extraction block (0 = all)")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--nfields", type=int, default=256, help="c3: fields in the batch")
+    ap.add_argument("--field-dims", type=int, default=0, choices=(0, 2, 3),
+                    help="c3: keep only the batch's 2D or 3D fields (0: all)")
     ap.add_argument("--cull-mode", type=int, default=2,
                     help="0: per-vertex cull words only; 1: tile statistics first; 2: the faster, timed once (default)")
     args = ap.parse_args()
