@@ -260,8 +260,7 @@ std::vector<DevBuf*> ftk2b_ctx::all_bufs() {
   std::vector<DevBuf*> v = {&stage[0], &stage[1], &stage[2], &stage_scalar, &key, &lam, &bary4,
                             &scalar, &key_alt, &perm0, &perm1, &hist, &lam_s, &bary4_s, &scalar_s,
                             &simplices, &bary, &track, &edge_cnt, &edges, &parent, &counters,
-                            &cls, &cand_corner, &cand_chains, &edge_slots, &tstats, &runs, &refine_vals,
-                            &refine_pairs};
+                            &cls, &cand_corner, &cand_chains, &edge_slots, &tstats, &runs, &refine_pairs};
   for (auto& b : extra) v.push_back(&b);
   for (DevBuf* b : ext.bufs()) v.push_back(b);
   for (DevBuf* b : batch.bufs()) v.push_back(b);
@@ -716,7 +715,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     RefineStage rs;
     // the single-field test keeps values and quantised values in shared
     // memory and reads the field again for the solve: no staging block
-    refine_stage_bind(rs, nullptr, ctx->refine_pairs.p, ccap, field->dtype == FTK2B_F64, cap);
+    refine_stage_bind(rs, ctx->refine_pairs.p, ccap, cap);
     rs.count = (unsigned*)ctx->counters.p + kCountPairs;
     rs.err = (unsigned*)ctx->counters.p + kCountErr;
     rs.big_count = (unsigned*)ctx->counters.p + kCountBig;

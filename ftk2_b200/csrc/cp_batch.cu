@@ -279,7 +279,6 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     B_TRY(ctx, ctx->cand_corner.ensure(sizeof(unsigned long long) * (size_t)ccap));
     B_TRY(ctx, ctx->cand_chains.ensure(sizeof(unsigned long long) * (size_t)ccap));
     B_TRY(ctx, bc.cand_field.ensure(sizeof(unsigned) * (size_t)ccap));
-    B_TRY(ctx, ctx->refine_vals.ensure(refine_stage_bytes(ccap, f64)));
     B_TRY(ctx, ctx->refine_pairs.ensure(refine_mask_bytes(ccap, cap)));
     PostBuffers B = ctx->post_buffers(cap, edge_cap, key_bits);
     FeatureSink sink;
@@ -298,7 +297,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     unsigned* const counters = static_cast<unsigned*>(ctx->counters.p);
     unsigned* const dfbase = static_cast<unsigned*>(bc.fbase.p);
     RefineStage rs;
-    refine_stage_bind(rs, ctx->refine_vals.p, ctx->refine_pairs.p, ccap, f64, cap);
+    refine_stage_bind(rs, ctx->refine_pairs.p, ccap, cap);
     rs.count = counters + kCountPairs;
     rs.err = counters + kCountErr;
     rs.big_count = counters + kCountBig;
@@ -313,7 +312,7 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     };
     auto enqueue2 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e = launch_batch_refine_staged(f64, dfields, cq, rs, sink, ctx->num_sms, ctx->stream);
-      *nl += 4;
+      *nl += 3;
       if (!e) e = launch_post_batch(dmeshes, dkb, (int)n, B, dfbase, ctx->stream, nl);
       if (!e)
         e = cudaMemcpyAsync(ctx->h_counters, counters, sizeof(unsigned) * kNumCounters, cudaMemcpyDeviceToHost,
@@ -384,6 +383,8 @@ ftk2b_status run_batch(ftk2b_ctx* ctx, uint32_t n, const ftk2b_mesh_desc* meshes
     if (cudaEventElapsedTime(&xms, ctx->ev0, ctx->ev_x) != cudaSuccess) xms = 0.f;
     cudaGetLastError();
     ctx->last_extract_ms = xms;
+    ctx->last_candidates = h[kCountCand];
+    ctx->last_tested = h[kCountPairs];
     if (h[kCountErr] & kErrBounds) return bfail(ctx, FTK2B_INTERNAL, "a device bounds check failed (checked build)");
     if (h[kCountErr] & 2u) return bfail(ctx, FTK2B_TIMEOUT, "a TMA slice copy did not complete in time");
     if (h[kCountErr]) return bfail(ctx, FTK2B_TIMEOUT, "union-find retry bound reached");

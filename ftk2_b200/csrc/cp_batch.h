@@ -36,11 +36,10 @@ bool regular_tma_maps(int f64, const RegularMesh& mesh, const FieldAccess& fa, b
 cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, const unsigned* item_base, int nf,
                               unsigned n_items, unsigned* item_next, const CandidateQueue& cq, unsigned* err,
                               cudaStream_t st);
-// Exact tests of every queued candidate of the batch (cq.field names its field).
-cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
-                                int num_sms, cudaStream_t st);
-// The same in two launches: a gather of every candidate's vertex values and
-// surviving chains, then one thread per listed simplex.
+// Exact tests of every queued candidate of the batch (cq.field names its
+// field) in three launches: the fast-path inside test (values gathered and
+// quantised in shared memory), the solve of the accepted simplices, and the
+// 128-bit path; the last two read values from the fields.
 cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const CandidateQueue& cq,
                                        const RefineStage& rs, const FeatureSink& sink, int num_sms, cudaStream_t st);
 // Time chunk of a field of a batch: corner time steps per cull item.

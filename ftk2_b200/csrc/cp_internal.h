@@ -136,13 +136,9 @@ cudaError_t launch_fiber_candidates(const RegularMesh& mesh, const CandidateQueu
 // every surviving simplex of the candidates whose quantised values all stay
 // below 2^31, listing the simplices it accepts; the solve of the listed
 // simplices; and the whole test of the other candidates' simplices (listed)
-// with the 128-bit path.  Batches stage each candidate's values and their
-// quantised form in global memory between the launches (vals, q); the
-// single-field path keeps them in shared memory (vals = q = null).
+// with the 128-bit path.  Values and their quantised form stay in shared
+// memory; the solve and the 128-bit path read values from the field.
 struct RefineStage {
-  void* vals;        // 48 field values per candidate (2^D * M, D <= 4)
-  int* q;            // the same 48 values quantised for the inside tests' fast path
-  unsigned long long* live;      // per candidate: chains to test on the fast path
   unsigned long long* big_live;  // per listed candidate: chains to test on the 128-bit path
   unsigned* big_list;            // candidates listed for the 128-bit path
   unsigned* big_count;
@@ -152,15 +148,11 @@ struct RefineStage {
   unsigned* count;   // simplices tested (reported after the run)
   unsigned* err;     // the call's error word (bounds checks of the checked build)
 };
-// bytes of the staging buffers for `ccap` candidates: values, then quantised
-// values; the chain masks, the inside list (acc_cap entries) and the list
-inline size_t refine_stage_bytes(size_t ccap, int f64) { return ccap * 48 * ((f64 ? 8 : 4) + 4); }
-inline size_t refine_mask_bytes(size_t ccap, size_t acc_cap) { return ccap * (8 + 8 + 4) + acc_cap * 8; }
-inline void refine_stage_bind(RefineStage& rs, void* stage, void* masks, size_t ccap, int f64, unsigned acc_cap) {
-  rs.vals = stage;
-  rs.q = stage ? reinterpret_cast<int*>(static_cast<char*>(stage) + ccap * 48 * (f64 ? 8 : 4)) : nullptr;
-  rs.live = static_cast<unsigned long long*>(masks);
-  rs.big_live = rs.live + ccap;
+// bytes of the 128-bit list for `ccap` candidates (chain masks and
+// candidates) and of the inside list (acc_cap entries)
+inline size_t refine_mask_bytes(size_t ccap, size_t acc_cap) { return ccap * (8 + 4) + acc_cap * 8; }
+inline void refine_stage_bind(RefineStage& rs, void* masks, size_t ccap, unsigned acc_cap) {
+  rs.big_live = static_cast<unsigned long long*>(masks);
   rs.acc = rs.big_live + ccap;
   rs.acc_cap = acc_cap;
   rs.big_list = reinterpret_cast<unsigned*>(rs.acc + acc_cap);

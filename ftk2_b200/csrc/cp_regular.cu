@@ -1547,9 +1547,9 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2)
 //                           each, values read from the field), and the whole
 //                           test with the 128-bit path for candidates holding
 //                           a quantised value past 2^31
-//   batches, four launches: the gather into a staging block in global memory
-//   (one warp per candidate, batch_gather_kernel), the fast-path inside test,
-//   the solve, and the 128-bit path, each reading the candidate's field record
+//   batches, three launches: batch_test_kernel (refine_test_kernel with 16
+//   lanes per candidate and each candidate's field record), the solve, and
+//   the 128-bit path, the last two reading values from the fields
 // The only atomics are the lists' and the sink's.
 
 // Masks of vertices 1..M of chain ch, a byte each (m1 | m2 << 8 | m3 << 16);
@@ -1748,16 +1748,6 @@ __device__ __forceinline__ unsigned pairs_layout_smem(const unsigned long long* 
   }
   __syncthreads();
   return off[kPairCands];
-}
-
-// The quantised values of the block's next kPairCands candidates (from
-// `first`, contiguous in rs.q) into shared memory, 16 bytes per copy (made
-// visible by the layout's barriers).
-__device__ __forceinline__ void stage_quantised(const RefineStage& rs, unsigned first, unsigned n, int* sq) {
-  const unsigned nk = min(n - first, (unsigned)kPairCands);
-  const int4* src = reinterpret_cast<const int4*>(rs.q + (size_t)first * kStageVals);
-  int4* dst = reinterpret_cast<int4*>(sq);
-  for (unsigned e = threadIdx.x; e < nk * (kStageVals / 4); e += blockDim.x) dst[e] = src[e];
 }
 
 // warp-aggregated append of (candidate << 8 | chain) to the inside list
@@ -1983,17 +1973,18 @@ __global__ void __launch_bounds__(kRefineWarps * 32, 2) refine_accept_kernel(Reg
   }
 }
 
-// the same two launches over a batch: each candidate reads its field's record
 // One candidate of a batch by a group of 16 lanes, one per hypercube vertex
-// (lanes 8-15 idle for a 2D+t field): its values and their quantised form
-// into the staging block, the vertices' cull words, and the mask of the
-// chains that survive them (or, with a quantised value past 2^31, the
-// 128-bit list).  gmask: the group's lanes; gshift: its first lane.
+// (lanes 8-15 idle for a 2D+t field): the quantised form of its values into
+// qout (the vertex's M values at qout[v * M]), the vertices' cull words, and
+// the mask of the chains that survive them into *live_out (or, with a
+// quantised value past 2^31, the candidate onto the 128-bit list and 0 into
+// *live_out).  gmask: the group's lanes; gshift: its first lane.
 template <typename T, int D>
 __device__ __forceinline__ void gather_group(const RegularMesh& mesh, const FieldAccess& fa, const ExtractConfig& cfg,
                                              unsigned c, unsigned long long pc, unsigned long long chains, int v,
                                              unsigned gmask, int gshift, const unsigned* band_tbl,
-                                             const unsigned* chain_pk, const RefineStage& rs) {
+                                             const unsigned* chain_pk, const RefineStage& rs, int* qout,
+                                             unsigned long long* live_out) {
   constexpr int M = D - 1;
   constexpr int NV = 1 << D;
   constexpr int R = (D == 4) ? 4 : 1;  // chain rounds of 16: 60 and 12 chains
@@ -2026,20 +2017,19 @@ __device__ __forceinline__ void gather_group(const RegularMesh& mesh, const Fiel
   }
   unsigned h[M];
   bool big = false;
-  T* const out = static_cast<T*>(rs.vals) + (size_t)c * kStageVals + v * M;
-  int* const qout = rs.q + (size_t)c * kStageVals + v * M;
+  T x[M];
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     const T* src = static_cast<const T*>(j == 0 ? fa.comp[0] : (j == 1 ? fa.comp[1] : fa.comp[2]));
-    T x = in ? src[o] : T(0);
-    if (cfg.fiber) x = fp<T>::sub(x, (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
-    h[j] = hi_word<T>(x);
-    const int qv = quant_small_p(quant_p((double)x, cfg.Q));
+    x[j] = in ? __ldg(src + o) : T(0);
+  }
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    if (cfg.fiber) x[j] = fp<T>::sub(x[j], (T)(j ? cfg.fthr[1] : cfg.fthr[0]));  // values[i][j] - thresholds[j]
+    h[j] = hi_word<T>(x[j]);
+    const int qv = quant_small_p(quant_p((double)x[j], cfg.Q));
     big |= v < NV && qv == kQBig;
-    if (v < NV) {
-      out[j] = x;
-      qout[j] = qv;
-    }
+    if (v < NV) qout[v * M + j] = qv;
   }
   const unsigned vw = in ? vertex_word_hi<T, M>(h, band_tbl) : kAbsent;  // absent: neutral under AND
   const bool gbig = ((__ballot_sync(gmask, big) >> gshift) & 0xFFFFu) != 0;
@@ -2064,91 +2054,121 @@ __device__ __forceinline__ void gather_group(const RegularMesh& mesh, const Fiel
       rs.big_live[slot] = mask;
       fast = 0;
     }
-    rs.live[c] = fast;
+    *live_out = fast;
   }
 }
 
-// the batch gather: two candidates per warp, 16 lanes each
+// Batches, exact test part 1: refine_test_kernel with every candidate's own
+// field record.  A block takes kTestCands candidates at a time, 16 lanes per
+// candidate (two per warp), quantises their values into shared memory, lays
+// out the (candidate, chain) pairs that survive the cull words and runs the
+// fast-path inside test with one thread per pair, listing the accepted
+// simplices; candidates holding a quantised value past 2^31 go to the
+// 128-bit list.
 template <typename T>
-__global__ void __launch_bounds__(kRefineWarps * 32) batch_gather_kernel(const BatchField* __restrict__ fields,
+__global__ void __launch_bounds__(kRefineWarps * 32, 4) batch_test_kernel(const BatchField* __restrict__ fields,
                                                                          CandidateQueue cq, RefineStage rs) {
+  constexpr int PER_PASS = kRefineWarps * 2;  // candidates per gather pass
+  constexpr int PASSES = kTestCands / PER_PASS;
+  static_assert(PASSES * PER_PASS == kTestCands, "the gather passes cover the block's candidates");
   __shared__ unsigned band_tbl[kBandTable];
   __shared__ unsigned chain_pk[2][kMaxChains];
+  __shared__ unsigned long long msk[kPairCands];
+  __shared__ unsigned off[kPairCands + 1];
+  __shared__ unsigned short plist[kTestCands * 64];
+  __shared__ __align__(16) int sq[kTestCands * kStageVals];
+  __shared__ int sd[kTestCands];  // the dimension of each candidate's mesh
   fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
   for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
     chain_pk[0][i] = chain_packed<3>(i);
     chain_pk[1][i] = chain_packed<4>(i);
   }
-  __syncthreads();
+  // the layout scans kPairCands masks; slots past the block's kTestCands stay empty
+  if (threadIdx.x >= kTestCands && threadIdx.x < kPairCands) msk[threadIdx.x] = 0ull;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int v = lane & 15, grp = lane >> 4;
   const unsigned gmask = 0xFFFFu << (16 * grp);
+  pdl_enter();
+  __syncthreads();
   const unsigned n = min(*cq.count, cq.cap);
-  const unsigned gw = blockIdx.x * kRefineWarps + wib;
-  const unsigned nw = gridDim.x * kRefineWarps;
-  for (unsigned base = gw * 2; base < n; base += nw * 2) {
-    const unsigned c = base + grp;
-    if (c >= n) continue;  // the whole group
-    const BatchField& F = fields[cq.field[c]];
-    const unsigned long long pc = cq.corner[c], chains = cq.chains[c];
-    if (F.mesh.d == 4)
-      gather_group<T, 4>(F.mesh, F.fa, F.cfg, c, pc, chains, v, gmask, 16 * grp, band_tbl, chain_pk[1], rs);
-    else
-      gather_group<T, 3>(F.mesh, F.fa, F.cfg, c, pc, chains, v, gmask, 16 * grp, band_tbl, chain_pk[0], rs);
-  }
-}
-
-template <typename T, bool BIG>
-__global__ void __launch_bounds__(kRefineWarps * 32, BIG ? 2 : 4) batch_pairs_kernel(const BatchField* __restrict__ fields,
-                                                                                  CandidateQueue cq, RefineStage rs,
-                                                                                  FeatureSink sink) {
-  __shared__ unsigned long long msk[kPairCands];
-  __shared__ unsigned off[kPairCands + 1];
-  __shared__ unsigned chain_pk[2][kMaxChains];
-  __shared__ unsigned short plist[kPairCands * 64];
-  __shared__ __align__(16) int sq[BIG ? 4 : kPairCands * kStageVals];
-  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
-    chain_pk[0][i] = chain_packed<3>(i);
-    chain_pk[1][i] = chain_packed<4>(i);
-  }
-  const int lane = threadIdx.x & 31;
-  const unsigned n = BIG ? *rs.big_count : min(*cq.count, cq.cap);
-  const unsigned long long* live = BIG ? rs.big_live : rs.live;
-  for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
-    if constexpr (!BIG) stage_quantised(rs, first, n, sq);
-    const unsigned P = pairs_layout(live, first, n, msk, off, plist);
+  for (unsigned first = blockIdx.x * kTestCands; first < n; first += gridDim.x * kTestCands) {
+#pragma unroll
+    for (int pass = 0; pass < PASSES; ++pass) {
+      const int k = pass * PER_PASS + wib * 2 + grp;
+      const unsigned c = first + k;
+      if (c >= n) {  // the whole group
+        if (v == 0) msk[k] = 0ull;
+        continue;
+      }
+      const BatchField& F = fields[cq.field[c]];
+      const unsigned long long pc = __ldg(&cq.corner[c]), chains = __ldg(&cq.chains[c]);
+      const int d = F.mesh.d;
+      if (v == 0) sd[k] = d;
+      if (d == 4)
+        gather_group<T, 4>(F.mesh, F.fa, F.cfg, c, pc, chains, v, gmask, 16 * grp, band_tbl, chain_pk[1], rs,
+                           sq + k * kStageVals, &msk[k]);
+      else
+        gather_group<T, 3>(F.mesh, F.fa, F.cfg, c, pc, chains, v, gmask, 16 * grp, band_tbl, chain_pk[0], rs,
+                           sq + k * kStageVals, &msk[k]);
+    }
+    __syncthreads();
+    const unsigned P = pairs_layout_smem(msk, off, plist);
     if (threadIdx.x == 0) atomicAdd(rs.count, P);
     for (unsigned base = 0; base < P; base += blockDim.x) {
       const unsigned p = base + threadIdx.x;
       const unsigned e = p < P ? plist[p] : 0u;
       const int k = (int)(e >> 6), ch = (int)(e & 63);
-      if constexpr (!BIG) {
-        bool in = false;
-        if (p < P) {
-          const int* qsrc = sq + k * kStageVals;
-          in = fields[cq.field[first + k]].mesh.d == 4 ? inside_pair_q<4>(ch, qsrc, chain_pk[1])
-                                                       : inside_pair_q<3>(ch, qsrc, chain_pk[0]);
-        }
-        acc_append(rs, in, first + k, ch, lane);
-      } else {
-        bool acc = false;
-        double lam_out[4] = {0, 0, 0, 0};
-        float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
-        float sc_out = 0.f;
-        unsigned long long key = 0;
-        if (p < P) {
-          const unsigned c = rs.big_list[first + k];
-          const BatchField& F = fields[cq.field[c]];
-          const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
-          if (F.mesh.d == 4)
-            acc = test_pair<T, 4, true>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[1], F.key_base, key,
-                                        lam_out, bary_out, sc_out);
-          else
-            acc = test_pair<T, 3, true>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[0], F.key_base, key,
-                                        lam_out, bary_out, sc_out);
-        }
-        sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
+      bool ins = false;
+      if (p < P && FTK2B_CHECK(k < kTestCands, rs.err))
+        ins = sd[k] == 4 ? inside_pair_q<4>(ch, sq + k * kStageVals, chain_pk[1])
+                         : inside_pair_q<3>(ch, sq + k * kStageVals, chain_pk[0]);
+      acc_append(rs, ins, first + k, ch, lane);
+    }
+    __syncthreads();  // shared memory is rebuilt for the next candidates
+  }
+}
+
+// Batches, the whole test with the 128-bit path of the candidates on that
+// list, values read from each candidate's field.
+template <typename T>
+__global__ void __launch_bounds__(kRefineWarps * 32, 2) batch_big_kernel(const BatchField* __restrict__ fields,
+                                                                        CandidateQueue cq, RefineStage rs,
+                                                                        FeatureSink sink) {
+  __shared__ unsigned long long msk[kPairCands];
+  __shared__ unsigned off[kPairCands + 1];
+  __shared__ unsigned chain_pk[2][kMaxChains];
+  __shared__ unsigned short plist[kPairCands * 64];
+  for (int i = threadIdx.x; i < kMaxChains; i += blockDim.x) {
+    chain_pk[0][i] = chain_packed<3>(i);
+    chain_pk[1][i] = chain_packed<4>(i);
+  }
+  pdl_enter();
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned n = *rs.big_count;
+  for (unsigned first = blockIdx.x * kPairCands; first < n; first += gridDim.x * kPairCands) {
+    const unsigned P = pairs_layout(rs.big_live, first, n, msk, off, plist);
+    if (threadIdx.x == 0) atomicAdd(rs.count, P);
+    for (unsigned base = 0; base < P; base += blockDim.x) {
+      const unsigned p = base + threadIdx.x;
+      const unsigned e = p < P ? plist[p] : 0u;
+      const int k = (int)(e >> 6), ch = (int)(e & 63);
+      bool acc = false;
+      double lam_out[4] = {0, 0, 0, 0};
+      float bary_out[4] = {0.f, 0.f, 0.f, 0.f};
+      float sc_out = 0.f;
+      unsigned long long key = 0;
+      if (p < P) {
+        const unsigned c = rs.big_list[first + k];
+        const BatchField& F = fields[cq.field[c]];
+        if (F.mesh.d == 4)
+          acc = test_pair<T, 4, true>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, (const T*)nullptr, chain_pk[1],
+                                      F.key_base, key, lam_out, bary_out, sc_out);
+        else
+          acc = test_pair<T, 3, true>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, (const T*)nullptr, chain_pk[0],
+                                      F.key_base, key, lam_out, bary_out, sc_out);
       }
+      sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
     }
     __syncthreads();
   }
@@ -2163,6 +2183,7 @@ __global__ void __launch_bounds__(kRefineWarps * 32) batch_solve_kernel(const Ba
     chain_pk[0][i] = chain_packed<3>(i);
     chain_pk[1][i] = chain_packed<4>(i);
   }
+  pdl_enter();
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned na = *rs.acc_count;
@@ -2181,13 +2202,12 @@ __global__ void __launch_bounds__(kRefineWarps * 32) batch_solve_kernel(const Ba
       const unsigned c = (unsigned)(e >> 8);
       const int ch = (int)(e & 255);
       const BatchField& F = fields[cq.field[c]];
-      const T* src = static_cast<const T*>(rs.vals) + (size_t)c * kStageVals;
       if (F.mesh.d == 4)
-        acc = test_pair<T, 4, false>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[1], F.key_base, key,
-                                     lam_out, bary_out, sc_out);
+        acc = test_pair<T, 4, false>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, (const T*)nullptr, chain_pk[1],
+                                     F.key_base, key, lam_out, bary_out, sc_out);
       else
-        acc = test_pair<T, 3, false>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, src, chain_pk[0], F.key_base, key,
-                                     lam_out, bary_out, sc_out);
+        acc = test_pair<T, 3, false>(F.mesh, F.fa, F.cfg, cq.corner[c], ch, (const T*)nullptr, chain_pk[0],
+                                     F.key_base, key, lam_out, bary_out, sc_out);
     }
     sink_write(sink, acc, key, lam_out, bary_out, sc_out, lane);
   }
@@ -2312,27 +2332,6 @@ __global__ void __launch_bounds__(kThreads, 2)
   flush_candidates(s_cbuf, s_ccount, cq, last_field);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kRefineWarps * 32, 2)
-    batch_refine_kernel(const BatchField* __restrict__ fields, CandidateQueue cq, FeatureSink sink) {
-  __shared__ T cube[kRefineWarps][16 * 3];
-  __shared__ unsigned band_tbl[kBandTable];
-  fill_band_table<T>(band_tbl, threadIdx.x, blockDim.x);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const unsigned n = min(*cq.count, cq.cap);
-  const unsigned gw = blockIdx.x * kRefineWarps + wib;
-  const unsigned nw = gridDim.x * kRefineWarps;
-  for (unsigned c = gw; c < n; c += nw) {
-    const BatchField& F = fields[cq.field[c]];
-    if (F.mesh.d == 4)
-      refine_candidate<T, 4>(F.mesh, F.fa, F.cfg, cq.corner[c], cq.chains[c], sink, F.key_base, cube[wib], band_tbl,
-                             lane);
-    else
-      refine_candidate<T, 3>(F.mesh, F.fa, F.cfg, cq.corner[c], cq.chains[c], sink, F.key_base, cube[wib], band_tbl,
-                             lane);
-  }
-}
 
 // ---------------------------------------------------------------------------
 // host side
@@ -2743,29 +2742,21 @@ cudaError_t launch_batch_cull(int f64, int multi, const BatchField* fields, cons
                : launch_batch_cull_t<float, false>(fields, item_base, nf, n_items, item_next, cq, err, st);
 }
 
-cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const CandidateQueue& cq,
-                                       const RefineStage& rs, const FeatureSink& sink, int num_sms, cudaStream_t st) {
+template <typename T>
+static cudaError_t launch_batch_refine_t(const BatchField* fields, const CandidateQueue& cq, const RefineStage& rs,
+                                         const FeatureSink& sink, int num_sms, cudaStream_t st) {
   const int thr = kRefineWarps * 32;
-  if (f64) {
-    batch_gather_kernel<double><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs);
-    batch_pairs_kernel<double, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
-    batch_solve_kernel<double><<<num_sms * 2, thr, 0, st>>>(fields, cq, rs, sink);
-    batch_pairs_kernel<double, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
-  } else {
-    batch_gather_kernel<float><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs);
-    batch_pairs_kernel<float, false><<<num_sms * 8, thr, 0, st>>>(fields, cq, rs, sink);
-    batch_solve_kernel<float><<<num_sms * 2, thr, 0, st>>>(fields, cq, rs, sink);
-    batch_pairs_kernel<float, true><<<num_sms, thr, 0, st>>>(fields, cq, rs, sink);
-  }
-  return cudaGetLastError();
+  // programmatic dependent launches, as on the single-field path
+  cudaError_t e = launch_pdl(batch_test_kernel<T>, num_sms * 16, thr, 0, st, fields, cq, rs);
+  if (!e) e = launch_pdl(batch_solve_kernel<T>, num_sms * 2, thr, 0, st, fields, cq, rs, sink);
+  if (!e) e = launch_pdl(batch_big_kernel<T>, num_sms, thr, 0, st, fields, cq, rs, sink);
+  return e ? e : cudaGetLastError();
 }
 
-cudaError_t launch_batch_refine(int f64, const BatchField* fields, const CandidateQueue& cq, const FeatureSink& sink,
-                                int num_sms, cudaStream_t st) {
-  const int grid = num_sms * 8;
-  if (f64) batch_refine_kernel<double><<<grid, kRefineWarps * 32, 0, st>>>(fields, cq, sink);
-  else batch_refine_kernel<float><<<grid, kRefineWarps * 32, 0, st>>>(fields, cq, sink);
-  return cudaGetLastError();
+cudaError_t launch_batch_refine_staged(int f64, const BatchField* fields, const CandidateQueue& cq,
+                                       const RefineStage& rs, const FeatureSink& sink, int num_sms, cudaStream_t st) {
+  return f64 ? launch_batch_refine_t<double>(fields, cq, rs, sink, num_sms, st)
+             : launch_batch_refine_t<float>(fields, cq, rs, sink, num_sms, st);
 }
 
 int batch_time_chunk(long long lt, int pick) {

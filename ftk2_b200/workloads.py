@@ -66,7 +66,9 @@ def run_batch_case(args):
             n = ctx.run_batch(meshes, fds, prms)
             x, tot, _ = ctx.last_timing()
             print(f"step {i}: {n} features  cull {x:.3f} ms  pipeline {tot:.3f} ms  "
-                  f"host {1e3 * (time.perf_counter() - t):.3f} ms", flush=True)
+                  f"host {1e3 * (time.perf_counter() - t):.3f} ms  "
+                  f"candidates={ctx.get_option(api.INFO_LAST_CANDIDATES)}  "
+                  f"tested={ctx.get_option(api.INFO_LAST_TESTED)}", flush=True)
 
 
 def run_contour_case(args):

@@ -160,9 +160,9 @@ ftk2b_status ftk2b_ctx_set_option(ftk2b_ctx* ctx, int option, int64_t value);
  * FTK2B_INFO_LAST_CULL_MODE: the cull mode (0 or 1) it ran, or
  * FTK2B_INFO_LAST_BATCH_TIME_CHUNK: corner time steps per cull item of the
  * last batch (65535: each field's whole time range), or
- * FTK2B_INFO_LAST_CANDIDATES: hypercubes the last regular-mesh cull kept for
- * the exact test, or FTK2B_INFO_LAST_TESTED: simplices of those hypercubes
- * the exact test ran on. */
+ * FTK2B_INFO_LAST_CANDIDATES: hypercubes the last regular-mesh cull (one
+ * field or a batch) kept for the exact test, or FTK2B_INFO_LAST_TESTED:
+ * simplices of those hypercubes the exact test ran on. */
 enum { FTK2B_INFO_LAST_TMA = 100, FTK2B_INFO_LAST_CULL_MODE = 101, FTK2B_INFO_LAST_BATCH_TIME_CHUNK = 102,
        FTK2B_INFO_LAST_CANDIDATES = 103, FTK2B_INFO_LAST_TESTED = 104 };
 ftk2b_status ftk2b_ctx_get_option(ftk2b_ctx* ctx, int option, int64_t* value);
