@@ -7,6 +7,14 @@
 
 #include <cuda_runtime.h>
 
+// loop unrolling in device code only (the word is also compiled for the
+// host by its check)
+#ifdef __CUDA_ARCH__
+#define FTK2B_UNROLL _Pragma("unroll")
+#else
+#define FTK2B_UNROLL
+#endif
+
 namespace ftk2b {
 
 // ---------------------------------------------------------------------------
@@ -69,7 +77,7 @@ template <> __device__ __forceinline__ unsigned hi_word<float>(float v) {
 constexpr int kBandTable = 128;
 
 template <typename T>
-__device__ __forceinline__ void fill_band_table(unsigned* tbl, int tid, int nthreads) {
+__host__ __device__ __forceinline__ void fill_band_table(unsigned* tbl, int tid, int nthreads) {
   using P = CullParams<T>;
   for (int i = tid; i < kBandTable; i += nthreads) {
     const int rel = i - 1;
@@ -83,31 +91,33 @@ __device__ __forceinline__ void fill_band_table(unsigned* tbl, int tid, int nthr
 }
 
 template <typename T, int M>
-__device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M], const unsigned* band_tbl) {
+__host__ __device__ __forceinline__ unsigned vertex_word_hi(const unsigned h[M], const unsigned* band_tbl) {
   using P = CullParams<T>;
   unsigned a[M], b = 0;
-#pragma unroll
+FTK2B_UNROLL
   for (int j = 0; j < M; ++j) {
     a[j] = h[j] & 0x7FFFFFFFu;
-    b = max(b, a[j]);
+    b = b > a[j] ? b : a[j];
   }
   const unsigned kexp = (unsigned)P::kappa_exp << P::mant;
-  const unsigned thr = max(b, kexp) - kexp;  // high word of kappa' * b (0 below kappa')
-  // component j strong: |v_j| > thr; the sign bit then picks bit j
-  // (positive) or bit 3 + j (negative)
-  unsigned strong = 0, neg = 0;
-#pragma unroll
+  const unsigned thr = (b > kexp ? b : kexp) - kexp;  // high word of kappa' * b (0 below kappa')
+  // component j strong: |v_j| > thr, as the sign of thr - |v_j| (both below
+  // 2^31, so the difference does not overflow); the value's sign then picks
+  // bit j (positive) or bit 3 + j (negative)
+  unsigned w = 0;
+FTK2B_UNROLL
   for (int j = 0; j < M; ++j) {
-    strong |= (a[j] > thr ? 1u : 0u) << j;
-    neg |= (h[j] >> 31) << j;
+    const unsigned strong = (unsigned)((int)(thr - a[j]) >> 31);
+    const unsigned neg = (unsigned)((int)h[j] >> 31);
+    w |= strong & ((neg & (8u << j)) | (~neg & (1u << j)));
   }
-  unsigned w = (strong & ~neg) | ((strong & neg) << 3);
   w |= (b < P::tiny_hi ? 1u : 0u) << 6;
   const int rel1 = (int)(b >> P::mant) - P::bias - kElo + 1;
   // inf or nan somewhere: the exponent lies past the banded window, so the
   // word gets no band bit (and no tiny bit) and no set of vertices holding
   // it is ever culled
-  w |= band_tbl[min((unsigned)rel1, (unsigned)(kBandTable - 1))];
+  const unsigned ri = (unsigned)rel1 < (unsigned)(kBandTable - 1) ? (unsigned)rel1 : (unsigned)(kBandTable - 1);
+  w |= band_tbl[ri];
   return w;
 }
 
