@@ -170,6 +170,8 @@ SIGNATURES = {
     "ftk2b_ctx_last_phases": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "ftk2b_ctx_last_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(C.c_uint64)]),
+    "ftk2b_stream_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
+    "ftk2b_stream_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p)]),
     "ftk2b_stream_open": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(FieldDesc),
                                     C.POINTER(CPParams), C.POINTER(C.c_void_p)]),
     "ftk2b_stream_push": (C.c_int, [C.c_void_p, C.POINTER(FieldDesc), C.POINTER(C.c_uint64)]),
@@ -646,6 +648,26 @@ class Stream:
         t, n, ms = C.c_uint64(), C.c_uint64(), C.c_double()
         self.ctx._check(self.lib.ftk2b_stream_info(self.h, C.byref(t), C.byref(n), C.byref(ms)))
         return int(t.value), int(n.value), float(ms.value)
+
+    def checkpoint(self) -> bytes:
+        """The stream's whole state as bytes (ftk2b_stream_checkpoint)."""
+        n = C.c_uint64()
+        self.ctx._check(self.lib.ftk2b_stream_checkpoint(self.h, None, C.byref(n)))
+        buf = C.create_string_buffer(max(1, n.value))
+        self.ctx._check(self.lib.ftk2b_stream_checkpoint(self.h, buf, C.byref(n)))
+        return buf.raw[:n.value]
+
+    @classmethod
+    def restore(cls, ctx: Context, blob: bytes) -> "Stream":
+        """A stream on ctx resumed from checkpoint() bytes (ftk2b_stream_restore)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        data = C.create_string_buffer(bytes(blob), len(blob))
+        ctx._check(self.lib.ftk2b_stream_restore(ctx.h, data, len(blob), C.byref(h)))
+        self.h = h
+        return self
 
     def close(self):
         if getattr(self, "h", None):

@@ -635,3 +635,241 @@ extern "C" void ftk2b_stream_close(ftk2b_stream* s) {
     b->release();
   delete s;
 }
+
+// ---------------------------------------------------------------------------
+// Checkpoint / resume: everything a later push or result reads -- the
+// configuration, the ring's timesteps, the feature store, the star edges,
+// the union-find parents and the newest layer's ids -- as one host blob.
+// Per-push scratch and the context's caches are rebuilt on demand.
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'F', 'T', 'K', '2', 'B', 'S', 'T', 'R'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct StreamCkpt {
+  char magic[8];
+  uint32_t version, header_bytes;
+  int32_t kind, d, m, dtype, layout, ncomp, location, pad;
+  uint64_t es;
+  ftk2b_cp_params prm;
+  uint64_t ld[3], off[3], gd[3], adims[3];
+  ftk2b_mesh_desc emesh;  // base_cells stored as null; the cells follow the header
+  uint64_t n_ecells, ebase_hash;
+  uint64_t T, slice_elems;
+  uint32_t n, n_edges, n_prev, n_first;
+};
+
+// the device sections of a stream's state, in blob order
+std::vector<std::pair<ftk2b::DevBuf*, size_t>> ckpt_sections(ftk2b_stream* s) {
+  std::vector<std::pair<ftk2b::DevBuf*, size_t>> v;
+  const int narr = s->layout == FTK2B_LAYOUT_MULTICOMPONENT ? 1 : s->m;
+  for (int j = 0; j < narr; ++j) v.push_back({&s->ring[j], 2 * s->slice_elems * s->es});
+  const size_t n = s->n;
+  if (s->kind == FTK2B_MESH_REGULAR) {
+    v.push_back({&s->key, 8 * n});
+  } else {
+    v.push_back({&s->hi, 8 * n});
+    v.push_back({&s->lo, 8 * n});
+    v.push_back({&s->phase, 4 * n});
+  }
+  v.push_back({&s->lam, 32 * n});
+  v.push_back({&s->bary4, 16 * n});
+  v.push_back({&s->scalar, 4 * n});
+  v.push_back({&s->cls, 4 * n});
+  v.push_back({&s->parent, 4 * n});
+  v.push_back({&s->edges, 8 * (size_t)s->n_edges});
+  v.push_back({&s->prev_ids, 4 * (size_t)s->n_prev});
+  return v;
+}
+
+}  // namespace
+
+extern "C" ftk2b_status ftk2b_stream_checkpoint(ftk2b_stream* s, void* buf, uint64_t* bytes) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_stream_checkpoint");
+  if (!s || !bytes) return FTK2B_INVALID_ARG;
+  ftk2b_ctx* ctx = s->ctx;
+  const auto sec = ckpt_sections(s);
+  uint64_t total = sizeof(StreamCkpt) + 8 * (uint64_t)s->ecells.size();
+  for (const auto& x : sec) total += x.second;
+  if (!buf) {
+    *bytes = total;
+    return FTK2B_OK;
+  }
+  if (*bytes < total) {
+    *bytes = total;
+    return sfail(ctx, FTK2B_INVALID_ARG, "checkpoint buffer too small (%llu bytes needed)",
+                 (unsigned long long)total);
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return sfail(ctx, FTK2B_CUDA_ERROR, "cudaSetDevice failed");
+  StreamCkpt h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, kCkptMagic, 8);
+  h.version = kCkptVersion;
+  h.header_bytes = (uint32_t)sizeof(StreamCkpt);
+  h.kind = s->kind;
+  h.d = s->d;
+  h.m = s->m;
+  h.dtype = s->dtype;
+  h.layout = s->layout;
+  h.ncomp = s->ncomp;
+  h.location = s->location;
+  h.es = s->es;
+  h.prm = s->prm;
+  for (int k = 0; k < 3; ++k) {
+    h.ld[k] = s->ld[k];
+    h.off[k] = s->off[k];
+    h.gd[k] = s->gd[k];
+    h.adims[k] = s->adims[k];
+  }
+  h.emesh = s->emesh;
+  h.emesh.base_cells = nullptr;
+  h.n_ecells = s->ecells.size();
+  h.ebase_hash = s->ebase_hash;
+  h.T = s->T;
+  h.slice_elems = s->slice_elems;
+  h.n = s->n;
+  h.n_edges = s->n_edges;
+  h.n_prev = s->n_prev;
+  h.n_first = s->n_first;
+  char* p = static_cast<char*>(buf);
+  memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  if (!s->ecells.empty()) memcpy(p, s->ecells.data(), 8 * s->ecells.size());
+  p += 8 * s->ecells.size();
+  for (const auto& x : sec) {
+    if (x.second) S_TRY(ctx, cudaMemcpyAsync(p, x.first->p, x.second, cudaMemcpyDeviceToHost, ctx->stream));
+    p += x.second;
+  }
+  S_TRY(ctx, ctx->sync());
+  *bytes = total;
+  return FTK2B_OK;
+}
+
+extern "C" ftk2b_status ftk2b_stream_restore(ftk2b_ctx* ctx, const void* buf, uint64_t bytes, ftk2b_stream** out) {
+  ftk2b::NvtxRange nvtx_range("ftk2b_stream_restore");
+  if (!ctx || !out) return FTK2B_INVALID_ARG;
+  *out = nullptr;
+  if (!buf || bytes < sizeof(StreamCkpt)) return sfail(ctx, FTK2B_INVALID_ARG, "not a stream checkpoint (too short)");
+  StreamCkpt h;
+  memcpy(&h, buf, sizeof(h));
+  if (memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != kCkptVersion || h.header_bytes != sizeof(StreamCkpt))
+    return sfail(ctx, FTK2B_INVALID_ARG, "not a stream checkpoint of this library version");
+  // the configuration must be one that ftk2b_stream_open accepts
+  const bool regular = h.kind == FTK2B_MESH_REGULAR;
+  bool ok = (regular || h.kind == FTK2B_MESH_EXTRUDED) && (h.d == 3 || h.d == 4) && h.m == h.d - 1 &&
+            h.ncomp == h.m && (h.dtype == FTK2B_F32 || h.dtype == FTK2B_F64) &&
+            h.es == (h.dtype == FTK2B_F64 ? 8u : 4u) && (h.location == FTK2B_HOST || h.location == FTK2B_DEVICE) &&
+            h.prm.sos_q > 0 && h.T < (1ull << 30);
+  if (ok && regular) {
+    ok = (h.layout == FTK2B_LAYOUT_MULTICOMPONENT || h.layout == FTK2B_LAYOUT_SEPARATE) && h.n_ecells == 0;
+    uint64_t se = 1;
+    for (int k = 0; k < h.d - 1 && ok; ++k) {
+      const uint64_t need = h.layout == FTK2B_LAYOUT_SEPARATE ? h.ld[k] : h.off[k] + h.ld[k];
+      ok = h.ld[k] >= 1 && h.ld[k] < 65536 && h.off[k] + h.ld[k] <= h.gd[k] && h.adims[k] >= need &&
+           h.adims[k] < (1ull << 32);
+      se *= h.adims[k];
+    }
+    if (h.layout == FTK2B_LAYOUT_MULTICOMPONENT) se *= (uint64_t)h.m;
+    ok = ok && se == h.slice_elems;
+  } else if (ok) {
+    const int cd = h.emesh.base_cell_dim;
+    ok = cd == h.m && h.layout != FTK2B_LAYOUT_MULTICOMPONENT && h.emesh.n_base_cells > 0 &&
+         h.emesh.n_base_cells < (1ull << 40) && h.n_ecells == h.emesh.n_base_cells * (uint64_t)(cd + 1) &&
+         h.slice_elems == h.emesh.n_base_verts && h.slice_elems > 0;
+  }
+  if (!ok) return sfail(ctx, FTK2B_INVALID_ARG, "stream checkpoint holds an invalid configuration");
+
+  ftk2b_stream* s = new ftk2b_stream();
+  s->ctx = ctx;
+  s->kind = h.kind;
+  s->d = h.d;
+  s->m = h.m;
+  s->prm = h.prm;
+  s->dtype = h.dtype;
+  s->layout = h.layout;
+  s->ncomp = h.ncomp;
+  s->location = h.location;
+  s->es = h.es;
+  for (int k = 0; k < 3; ++k) {
+    s->ld[k] = h.ld[k];
+    s->off[k] = h.off[k];
+    s->gd[k] = h.gd[k];
+    s->adims[k] = h.adims[k];
+  }
+  s->slice_elems = h.slice_elems;
+  s->T = h.T;
+  const char* p = static_cast<const char*>(buf) + sizeof(h);
+  // the blob's size must be exactly what its counts say
+  s->n = h.n;
+  s->n_edges = h.n_edges;
+  s->n_prev = h.n_prev;
+  uint64_t total = sizeof(h) + 8 * h.n_ecells;
+  for (const auto& x : ckpt_sections(s)) total += x.second;
+  if (total != bytes || h.n_prev > h.n || (h.n && h.n_first > h.n)) {
+    delete s;
+    return sfail(ctx, FTK2B_INVALID_ARG, "stream checkpoint size does not match its contents");
+  }
+  if (!regular) {
+    s->emesh = h.emesh;
+    s->ecells.assign(reinterpret_cast<const uint64_t*>(p), reinterpret_cast<const uint64_t*>(p) + h.n_ecells);
+    s->emesh.base_cells = s->ecells.data();
+    s->ebase_hash = ftk2b::hash_base_cells(s->ecells.data(), (uint64_t)s->ecells.size());
+    if (s->ebase_hash != h.ebase_hash) {
+      delete s;
+      return sfail(ctx, FTK2B_INVALID_ARG, "stream checkpoint's base cells are damaged");
+    }
+  }
+  p += 8 * h.n_ecells;
+  auto release_all = [&]() {
+    for (DevBuf* b : {&s->ring[0], &s->ring[1], &s->ring[2], &s->key, &s->hi, &s->lo, &s->phase, &s->lam, &s->bary4,
+                      &s->scalar, &s->cls, &s->parent, &s->edges, &s->prev_ids, &s->prev_ids2})
+      b->release();
+  };
+  ftk2b_status st = FTK2B_OK;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) st = FTK2B_CUDA_ERROR;
+  for (DevBuf* b : {&s->ring[0], &s->ring[1], &s->ring[2], &s->key, &s->hi, &s->lo, &s->phase, &s->lam,
+                    &s->bary4, &s->scalar, &s->cls, &s->parent, &s->edges, &s->prev_ids, &s->prev_ids2, &s->s_key,
+                    &s->s_key2, &s->s_id, &s->s_id2, &s->s_hi, &s->s_lo, &s->s_phase, &s->wedges, &s->tmp_simp,
+                    &s->dummy})
+    b->st = ctx->stream;
+  const int narr = s->layout == FTK2B_LAYOUT_MULTICOMPONENT ? 1 : s->m;
+  for (int j = 0; j < narr && !st; ++j)
+    if (s->ring[j].ensure(2 * s->slice_elems * s->es) != cudaSuccess) st = FTK2B_OOM;
+  // an empty store grows to hold the checkpoint's features (nothing to keep)
+  if (!st) {
+    s->n = 0;
+    s->n_prev = 0;
+    st = ftk2b::ensure_stream_store(s, h.n > 0 ? h.n : 1);
+    s->n = h.n;
+    s->n_prev = h.n_prev;
+  }
+  if (!st && h.n_edges) {
+    unsigned nc = 262144u;
+    while (nc < h.n_edges) nc = nc * 2u > nc ? nc * 2u : 0xFFFFFFF0u;
+    if (s->edges.ensure(8 * (size_t)nc) != cudaSuccess) st = FTK2B_OOM;
+    else s->edge_cap = nc;
+  }
+  if (!st) {
+    s->n_edges = h.n_edges;
+    s->n_first = h.n_first;
+    for (const auto& x : ckpt_sections(s)) {
+      if (x.second &&
+          cudaMemcpyAsync(x.first->p, p, x.second, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+        st = FTK2B_CUDA_ERROR;
+        break;
+      }
+      p += x.second;
+    }
+  }
+  if (!st && ctx->sync() != cudaSuccess) st = FTK2B_CUDA_ERROR;
+  if (st) {
+    cudaGetLastError();
+    cudaStreamSynchronize(ctx->stream);
+    release_all();
+    delete s;
+    return sfail(ctx, st, "stream restore failed (device allocation or copy)");
+  }
+  *out = s;
+  return FTK2B_OK;
+}

@@ -271,6 +271,19 @@ ftk2b_status ftk2b_stream_push(ftk2b_stream* s, const ftk2b_field_desc* step, ui
 ftk2b_status ftk2b_stream_result(ftk2b_stream* s, ftk2b_cp_result** out);
 ftk2b_status ftk2b_stream_info(ftk2b_stream* s, uint64_t* timesteps, uint64_t* n_features, double* last_push_ms);
 void ftk2b_stream_close(ftk2b_stream* s);
+/* Checkpoint and resume (no reference counterpart: the reference's streaming
+ * drivers keep their state in one process).  ftk2b_stream_checkpoint writes
+ * everything later pushes and results read -- the configuration, the two
+ * newest timesteps, the features, star edges, union-find parents and the
+ * newest layer's ids -- to host memory: with buf = NULL it only stores the
+ * size needed in *bytes; with a buffer of *bytes bytes it writes the blob
+ * (FTK2B_INVALID_ARG, and the size in *bytes, when the buffer is too small).
+ * ftk2b_stream_restore opens a stream on ctx (any device) from such a blob;
+ * pushing the remaining timesteps to it gives what the original stream would
+ * have given.  The blob is checked (magic, version, configuration, sizes)
+ * before anything is allocated. */
+ftk2b_status ftk2b_stream_checkpoint(ftk2b_stream* s, void* buf, uint64_t* bytes);
+ftk2b_status ftk2b_stream_restore(ftk2b_ctx* ctx, const void* buf, uint64_t bytes, ftk2b_stream** out);
 
 /* --- serving ----------------------------------------------------------------
  * No counterpart in the reference (it has no request loop).  A server owns

@@ -204,3 +204,59 @@ def test_extruded_stream_matches_reference_fixture(ctx):
     ref = bridge.CPResult(simplices=z["simplices"], bary=z["bary"], lam=z["lam"], track_id=z["track_id"],
                           type=z["type"], scalar=z["scalar"], edges=z["edges"])
     assert_identical(r, ref)
+
+
+@pytest.mark.parametrize("cut", [1, 3])
+@pytest.mark.parametrize("which", [2, 3], ids=["g3d_f32_noise", "g2d_f32_sep_offset"])
+def test_stream_checkpoint_resume(ctx, which, cut):
+    """A stream checkpointed after `cut` pushes, closed, restored on another
+    context and fed the remaining timesteps gives the one-shot result."""
+    case = _cases()[which]
+    keep: list = []
+    nt = case.local_dims[-1]
+    mesh = api.regular_mesh_desc(case.local_dims, case.offset, case.global_dims)
+    tmpl = api.field_desc(steps_of(case, 0), case.layout, case.ncomp, keep=keep)
+    prm = api.params(case.sos_q)
+    with api.Stream(ctx, mesh, tmpl, prm) as st:
+        for t in range(cut):
+            st.push(api.field_desc(steps_of(case, t), case.layout, case.ncomp, keep=keep))
+        blob = st.checkpoint()
+    with api.Context(0) as ctx2, api.Stream.restore(ctx2, blob) as st2:
+        assert st2.info()[0] == cut
+        for t in range(cut, nt):
+            st2.push(api.field_desc(steps_of(case, t), case.layout, case.ncomp, keep=keep))
+        assert_identical(st2.result(), one_shot(ctx, case, nt, False))
+        # a checkpoint of the restored stream equals the original's layout
+        assert len(st2.checkpoint()) >= len(blob)
+
+
+def test_extruded_stream_checkpoint_resume(ctx):
+    case = _ext_cases()[2]
+    keep: list = []
+    nv = case.coords.shape[0]
+    nt = case.n_layers + 1
+    mesh = api.extruded_mesh_desc(nv, case.cells, case.n_layers, keep)
+    step = lambda t: [np.ascontiguousarray(a[t * nv:(t + 1) * nv]) for a in case.arrays]
+    tmpl = api.field_desc(step(0), case.layout, case.ncomp, keep=keep)
+    with api.Stream(ctx, mesh, tmpl, api.params(case.sos_q)) as st:
+        for t in range(3):
+            st.push(api.field_desc(step(t), case.layout, case.ncomp, keep=keep))
+        blob = st.checkpoint()
+    with api.Stream.restore(ctx, blob) as st2:
+        for t in range(3, nt):
+            st2.push(api.field_desc(step(t), case.layout, case.ncomp, keep=keep))
+        assert_identical(st2.result(), ext_one_shot(ctx, case, nt))
+
+
+def test_stream_restore_rejects_damaged_blobs(ctx):
+    case = _cases()[2]
+    keep: list = []
+    mesh = api.regular_mesh_desc(case.local_dims, case.offset, case.global_dims)
+    tmpl = api.field_desc(steps_of(case, 0), case.layout, case.ncomp, keep=keep)
+    with api.Stream(ctx, mesh, tmpl, api.params(case.sos_q)) as st:
+        st.push(api.field_desc(steps_of(case, 0), case.layout, case.ncomp, keep=keep))
+        blob = st.checkpoint()
+    for bad in (blob[:-1], b"XXXXXXXX" + blob[8:], blob[:64], blob + b"\0"):
+        with pytest.raises(api.Ftk2bError) as e:
+            api.Stream.restore(ctx, bad)
+        assert e.value.status == api.INVALID_ARG
