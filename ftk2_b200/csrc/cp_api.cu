@@ -721,12 +721,14 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
     rs.big_count = (unsigned*)ctx->counters.p + kCountBig;
     rs.acc_count = (unsigned*)ctx->counters.p + kCountAcc;
     const int f64 = field->dtype == FTK2B_F64;
-    // the device pipeline in two parts so that the fused cull kernel can be
-    // timed on its own: [counters reset, cull] and [exact tests, canonical
-    // order, star edges, trajectories, counters readback]
+    // the device pipeline after the counters' reset in two parts, so that the
+    // fused cull kernel can be timed on its own: [cull] and [exact tests,
+    // canonical order, star edges, trajectories, counters readback]
+    auto enqueue0 = [&]() -> cudaError_t {
+      return cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream);
+    };
     auto enqueue1 = [&](unsigned long long* nl) -> cudaError_t {
       cudaError_t e;
-      if ((e = cudaMemsetAsync(ctx->counters.p, 0, sizeof(unsigned) * kNumCounters, ctx->stream))) return e;
       int nk = 1;
       if (cfg.fiber) {
         if ((e = launch_fiber_candidates(rm, cq, ctx->num_sms, ctx->stream))) return e;
@@ -819,7 +821,8 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
         {
           cudaGraph_t graph = nullptr;
           CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-          cudaError_t ce = cudaEventRecordWithFlags(ctx->ev0, ctx->stream, cudaEventRecordExternal);
+          cudaError_t ce = enqueue0();
+          if (!ce) ce = cudaEventRecordWithFlags(ctx->ev0, ctx->stream, cudaEventRecordExternal);
           if (!ce) ce = enqueue1(&nl);
           if (!ce) ce = cudaEventRecordWithFlags(ctx->ev_x, ctx->stream, cudaEventRecordExternal);
           if (!ce) ce = enqueue2(&nl);
@@ -864,6 +867,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       p2 = Clk::now();
       ctx->phase_ms[1] += msd(p1, p2);
       if (ent->g2) {
+        CUDA_TRY(ctx, enqueue0());
         CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
         CUDA_TRY(ctx, cudaGraphLaunch(ent->g1, ctx->stream));
         CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));
@@ -875,6 +879,7 @@ static ftk2b_status run_regular(ftk2b_ctx* ctx, const ftk2b_mesh_desc* mesh,
       ctx->launches += ent->launches;
     } else {
       unsigned long long nl = 0;
+      CUDA_TRY(ctx, enqueue0());
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
       CUDA_TRY(ctx, enqueue1(&nl));
       CUDA_TRY(ctx, cudaEventRecord(ctx->ev_x, ctx->stream));

@@ -477,6 +477,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
       const unsigned ts = (unsigned)(((long long)tcoord(s) * tstride * (long long)sizeof(T)) & 15);
 #pragma unroll
       for (int u = 0; u < VPT; ++u) {
+        if (u == VPT - 1 && VS < VSP && tid + u * kThreads >= VS) {  // a padding slot: no vertex
+          w[u] = kAbsent;
+          continue;
+        }
         unsigned h[M];
         const unsigned su = (vshift >> (4 * u)) + ts;
 #pragma unroll
@@ -492,6 +496,10 @@ __device__ __forceinline__ bool cull_tile(const CUtensorMap* map0, const CUtenso
     }
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
+      if (u == VPT - 1 && VS < VSP && tid + u * kThreads >= VS) {  // a padding slot: no vertex
+        w[u] = kAbsent;
+        continue;
+      }
       unsigned h[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {

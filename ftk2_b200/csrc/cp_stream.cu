@@ -812,7 +812,8 @@ extern "C" ftk2b_status ftk2b_stream_restore(ftk2b_ctx* ctx, const void* buf, ui
   }
   if (!regular) {
     s->emesh = h.emesh;
-    s->ecells.assign(reinterpret_cast<const uint64_t*>(p), reinterpret_cast<const uint64_t*>(p) + h.n_ecells);
+    s->ecells.resize(h.n_ecells);  // the caller's blob need not be 8-byte aligned
+    memcpy(s->ecells.data(), p, 8 * h.n_ecells);
     s->emesh.base_cells = s->ecells.data();
     s->ebase_hash = ftk2b::hash_base_cells(s->ecells.data(), (uint64_t)s->ecells.size());
     if (s->ebase_hash != h.ebase_hash) {
