@@ -518,7 +518,7 @@ def batched_c3(ctx, steps=5, check=True):
     return out
 
 
-def north_star_summary(line):
+def targets_summary(line):
     """The targets of the workload set in one short object, printed last on
     the line: HBM roofline fractions of the plain FP64 drop-in (128^3 x 16)
     and of the 256^3 x 8 float32 workload (extraction kernels alone and whole
@@ -760,7 +760,7 @@ def main():
         line["contour"] = contour_c2(ctx)
         torch.cuda.empty_cache()
         line["fiber_surface"] = fiber_surface_bench(ctx)
-        line["north_star"] = north_star_summary(line)
+        line["targets"] = targets_summary(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
